@@ -1,0 +1,334 @@
+"""Particle-substeps/s of the plain PBF dam break (1,048,576 particles) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one frame of the scene: 2 substeps of predict -> cell-key sort -> 4 PBF iterations ->
+velocity update.  `value` times K frames replayed from one CUDA graph with the state resident in
+HBM (device time, CUDA events, max over ranks).  `e2e` times the same frames through the C ABI
+with the particle state uploaded from pinned host memory and read back every frame (the
+reference's enableBlockingReadback behaviour).  Under torchrun each rank steps its own replica
+of the scene (the single-scene substep does not shard), so `scaling` is "weak".
+
+--impl reference times the reference's CPU implementation of the same path.  The reference's
+own solver is Vulkan/D3D12 HLSL behind Diligent Engine and cannot run here, so its CPU
+restatement (the oracle under oracle/) is timed on the host cores, with every thread it can use,
+on a bounded lattice sample of the same scene.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "cressim-neo_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "particle-substeps/s"
+WORKLOAD = "pbf_dam_break_128x64x128"
+MEASURED_PEAKS = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except FileNotFoundError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            if self.uuid and self.uuid not in parts[0]:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        p = json.loads(MEASURED_PEAKS.read_text())
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# Algorithmic bytes per particle of one launch of each fluid kernel (compulsory traffic; neighbour
+# entries count 4 B).  Neighbour build + density: position P (16) + cell entry (16) + metadata (16)
+# + kind/material (4) + boundary mask (8), list writes 4*nbar, count (4), constraint write (16).
+# Delta + apply + clamp: P (16) + x (16) + accumulated delta r/w (32) + constraint (16) + list reads
+# 4*nbar + count (4) + kind/material (4) + boundary mask (8) + packed delta write (16 when kept).
+def kernel_bytes(name: str, nbar: float) -> float | None:
+    if name == "fluid_neighbors_density":
+        return 80.0 + 4.0 * nbar
+    if name == "fluid_delta_apply_clamp":
+        return 96.0 + 4.0 * nbar
+    if name == "fluid_gather":
+        return 4.0 + 16.0 + 16.0 + 16.0 + 16.0
+    if name == "predict_keys":
+        return 16 + 16 + 16 + 16 + 16 + 16 + 4 + 4 + 4  # x r/w, v r/w, x_prev w, entry w, key w, kinds
+    return None
+
+
+def substep_bytes(nbar: float, iters: int) -> float:
+    """The substep byte model: 232 + I * (140 + 12 nbar) bytes per particle."""
+    return 232.0 + iters * (140.0 + 12.0 * nbar)
+
+
+def traffic_from_profiles():
+    f = ROOT / "profiles" / "traffic.json"
+    try:
+        return json.loads(f.read_text())
+    except Exception:
+        return {}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from cn_physics import Solver, scenes
+
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    w, desc, dt = scenes.dam_break()
+    soa = w.soa()
+    n = soa.particle_count
+    solver = Solver(desc, device=local)
+    solver.sync_world(soa)
+    solver.set_timing(True)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    solver.step_many(dt, max(args.warmup, 0), sh)
+    torch.cuda.synchronize()
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    clocks = ClockSampler(uuid)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(args.steps):
+        solver.step_many(dt, 1, sh)
+    end.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = start.elapsed_time(end)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    substeps = desc.substeps
+    total_units = float(n) * substeps * args.steps * world
+    value = total_units / (ms / 1e3)
+    meta = solver.validate_gpu_meta()
+    ktimes = solver.kernel_times()
+    kernels_per_frame, _ = solver.graph_stats()
+    counts = solver_neighbor_mean(solver)
+
+    # e2e through the C ABI: pinned host state uploaded and read back every frame
+    xh = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
+    vh = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
+    x, v, _ = solver.read_particles()
+    xh.numpy()[:] = x
+    vh.numpy()[:] = v
+    lib = solver._lib
+    import ctypes as C
+    xp = C.cast(xh.data_ptr(), C.POINTER(C.c_float))
+    vp = C.cast(vh.data_ptr(), C.POINTER(C.c_float))
+    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        assert lib.cn_solver_write_particles(solver._h, xp, vp, n) == 0
+        solver.step_many(dt, 1, sh)
+        assert lib.cn_solver_read_particles(solver._h, xp, vp, None, n) == 0
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = float(n) * substeps * e2e_steps * world / e2e_s
+
+    hbm, peak_kind = peaks()
+    dominant = max((k for k in ktimes if kernel_bytes(k, counts) is not None), key=lambda k: ktimes[k][0], default=None)
+    roofline = None
+    if dominant:
+        tot_ms, launches = ktimes[dominant]
+        per_launch_s = tot_ms / launches / 1e3
+        algo = kernel_bytes(dominant, counts) * n
+        achieved = algo / per_launch_s / 1e9
+        tr = traffic_from_profiles().get(dominant)
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": hbm,
+                    "peak_kind": f"{peak_kind} copy bandwidth", "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                    "traffic": tr, "algorithmic_bytes_per_launch": algo, "launch_ms": round(tot_ms / launches, 4)}
+    frame_ms_device = sum(t for t, _ in ktimes.values())
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": "particle-substeps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles": n, "substeps": substeps, "fluid_iterations": desc.fluid_iterations,
+                   "frame_dt": dt, "parallelism": f"replicas{world}", "l2": "working set > L2 (~0.9 GB resident)",
+                   "mean_neighbors": round(counts, 2)},
+        "e2e": {"value": round(e2e_value, 1), "unit": "particle-substeps/s", "h2d_bytes_per_step": 32 * n,
+                "d2h_bytes_per_step": 32 * n, "steps": e2e_steps},
+        "gpu_launches": int(kernels_per_frame) * args.steps,
+        "roofline": roofline,
+        "kernel_ms_per_frame": {k: round(t, 4) for k, (t, _) in sorted(ktimes.items(), key=lambda kv: -kv[1][0])},
+        "substep_model_bytes_per_particle": substep_bytes(counts, desc.fluid_iterations),
+        "clocks": clk,
+        "meta_status": meta["status"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(budget_s=15.0)
+    if world > 1:
+        dist.barrier()
+        solver.close()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def solver_neighbor_mean(solver) -> float:
+    c = solver.debug_read("fluid_neighbor_counts").view(np.uint32)
+    return float(c.mean()) if c.size else 0.0
+
+
+def cpu_baseline(budget_s: float = 15.0, dims=(64, 32, 64), max_frames: int = 8):
+    """The oracle (CPU restatement, all host threads) on a lattice sample of the same scene."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import cn_oracle
+    from cn_physics import scenes
+
+    threads = cn_oracle.set_threads(os.cpu_count() or 1)
+    w, desc, dt = scenes.dam_break(nx=dims[0], ny=dims[1], nz=dims[2])
+    soa = w.soa()
+    ora = cn_oracle.Oracle(desc, soa)
+    frames, t0 = 0, time.perf_counter()
+    while frames < max_frames and (time.perf_counter() - t0) < budget_s:
+        ora.step(dt)
+        frames += 1
+    el = time.perf_counter() - t0
+    v = soa.particle_count * desc.substeps * frames / el
+    return {"value": round(v, 1), "unit": "particle-substeps/s", "cores": threads, "kind": "port",
+            "sample": f"{dims[0]}x{dims[1]}x{dims[2]} lattice ({soa.particle_count} particles) of the same dam break, "
+                      f"{frames} frames x {desc.substeps} substeps, {el:.1f} s"}
+
+
+def run_reference(args):
+    rank, local, world = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import cn_oracle
+    from cn_physics import scenes
+
+    threads = cn_oracle.set_threads(os.cpu_count() or 1)
+    dims = (48, 24, 48)
+    w, desc, dt = scenes.dam_break(nx=dims[0], ny=dims[1], nz=dims[2])
+    soa = w.soa()
+    ora = cn_oracle.Oracle(desc, soa)
+    for _ in range(max(args.warmup, 0)):
+        ora.step(dt)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ora.step(dt)
+    el = time.perf_counter() - t0
+    value = soa.particle_count * desc.substeps * args.steps / el
+    sample = (f"{dims[0]}x{dims[1]}x{dims[2]} lattice ({soa.particle_count} particles) of the dam break; "
+              "CPU restatement of the reference's HLSL passes (its Vulkan path cannot run here)")
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": "particle-substeps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(el * 1e3 / args.steps, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles": soa.particle_count, "substeps": desc.substeps,
+                       "fluid_iterations": desc.fluid_iterations, "frame_dt": dt},
+            "cpu_baseline": {"value": round(value, 1), "unit": "particle-substeps/s", "cores": threads,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": round(value, 1), "unit": "particle-substeps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,376 @@
+"""Python host mirror of the CRESSim-Neo particle substep (B200 build).
+
+The classes follow the reference's host API for this path:
+
+* ``World``  -- PhysicsWorld authoring (upsertSoftBody / fluids / cloth / strands / rigid bodies and
+  colliders, reference include/physics/physics_world.h) producing the particle/constraint SoA;
+* ``Solver`` -- PhysicsSolver (include/physics/physics_solver.h:150-205): ``sync_world``,
+  ``step``, ``validate_gpu_meta``, ``set_gravity``, ``gpu_scene_view``.
+
+Everything runs through the C ABI of ``libcn_physics.so`` (include/cn_physics.h); there is no
+Python or CPU implementation of the substep in this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+from ._abi import load
+
+__all__ = ["World", "Solver", "SolverDesc", "CNError", "load", "solver_desc", "DEBUG"]
+
+STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "CUDA", 3: "OUT_OF_MEMORY", 4: "NOT_INITIALIZED",
+          5: "CAPACITY", 6: "NO_DEVICE", 7: "DEVICE_TIMEOUT", 8: "UNSUPPORTED"}
+
+DEBUG = {"cell_entries": 0, "sorted_keys": 1, "cell_ranges": 2, "fluid_neighbor_counts": 3,
+         "fluid_neighbors": 4, "fluid_constraints": 5, "fluid_delta": 6, "rigid_contacts": 7}
+
+SolverDesc = _abi.SolverDesc
+
+
+class CNError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+def _check(status: int) -> None:
+    if status != 0:
+        raise CNError(status, load().cn_last_error().decode())
+
+
+def solver_desc(**overrides) -> _abi.SolverDesc:
+    """PhysicsSolverDesc with the reference defaults (physics_solver.h:22-143), then overrides.
+
+    Nested settings may be given as ``contact_slop=...``, ``soft_internal_relaxation=...``,
+    ``fluid_constraint_relaxation=...``; ``gravity=(x, y, z)``."""
+    d = _abi.SolverDesc()
+    load().cn_solver_desc_defaults(C.byref(d))
+    for key, value in overrides.items():
+        if key == "gravity":
+            d.gravity = (C.c_float * 3)(*value)
+        elif hasattr(d, key):
+            setattr(d, key, value)
+        else:
+            group, _, name = key.partition("_")
+            setattr(getattr(d, group), name, value)
+    return d
+
+
+def _f32(arr) -> C.POINTER(C.c_float):
+    return arr.ctypes.data_as(_abi.P_f32)
+
+
+def _u32(arr) -> C.POINTER(C.c_uint32):
+    return arr.ctypes.data_as(_abi.P_u32)
+
+
+def _view(ptr, count: int, dtype, cols: int = 1) -> np.ndarray:
+    if count == 0 or not ptr:
+        return np.zeros((count, cols) if cols > 1 else (count,), dtype=dtype)
+    ctype = C.c_float if dtype == np.float32 else C.c_uint32
+    base = C.cast(ptr, C.POINTER(ctype))
+    a = np.ctypeslib.as_array(base, shape=(count * cols,))
+    return a.reshape(count, cols) if cols > 1 else a
+
+
+class World:
+    """PhysicsWorld authoring mirror.  ``soa()`` packs the SoA the solver uploads; the position and
+    velocity arrays it exposes are views that may be edited in place before ``sync_world``."""
+
+    def __init__(self):
+        self._lib = load()
+        h = C.c_void_p()
+        _check(self._lib.cn_world_create(C.byref(h)))
+        self._h = h
+        self._soa: Optional[_abi.WorldSoA] = None
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cn_world_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _transform(t, position=(0, 0, 0), rotation=(0, 0, 0, 1), scale=(1, 1, 1)):
+        t.position = (C.c_float * 3)(*position)
+        t.rotation = (C.c_float * 4)(*rotation)
+        t.scale = (C.c_float * 3)(*scale)
+
+    @staticmethod
+    def _material(m, friction=0.0, restitution=0.0, damping=0.0, static_friction=-1.0):
+        m.friction, m.restitution, m.damping, m.static_friction = friction, restitution, damping, static_friction
+
+    def add_soft_body_grid(self, size, spacing, position=(0, 0, 0), rotation=(0, 0, 0, 1), *, mass=1.0,
+                           radius=0.125, edge_compliance=0.0, volume_compliance=0.0, self_collision=False,
+                           static_particles: Sequence[int] = (), environment=0, layer=1, mask=0xFFFFFFFF,
+                           friction=0.0, restitution=0.0, damping=0.0, static_friction=-1.0) -> int:
+        """SoftBodyState with a RegularGrid source (soft_body_authoring.cpp:81-176)."""
+        d = _abi.SoftBodyGridDesc()
+        self._lib.cn_soft_body_grid_desc_defaults(C.byref(d))
+        d.size = (C.c_float * 3)(*size)
+        d.target_particle_spacing = spacing
+        self._transform(d.rest_transform, position, rotation)
+        d.particle_mass, d.particle_radius = mass, radius
+        d.edge_compliance, d.volume_compliance = edge_compliance, volume_compliance
+        d.self_collision_enabled = int(self_collision)
+        d.environment_index, d.collision_layer, d.collision_mask = environment, layer, mask
+        self._material(d.material, friction, restitution, damping, static_friction)
+        st = np.ascontiguousarray(np.asarray(static_particles, dtype=np.uint32))
+        self._keep.append(st)
+        d.static_particle_indices = _u32(st) if st.size else None
+        d.static_particle_count = st.size
+        out = C.c_uint32()
+        _check(self._lib.cn_world_add_soft_body_grid(self._h, C.byref(d), C.byref(out)))
+        return out.value
+
+    def add_fluid_grid(self, size, spacing, position=(0, 0, 0), *, mass=1.0, radius=0.05, viscosity=0.01,
+                       cohesion=0.0, surface_tension=0.0, vorticity=0.0, gravity_scale=1.0, cfl=1.0,
+                       environment=0, layer=1, mask=0xFFFFFFFF, friction=0.0, restitution=0.0, damping=0.0,
+                       static_friction=-1.0) -> int:
+        """FluidState with a RegularGrid source (physics_world.cpp:6857-6891)."""
+        d = _abi.FluidGridDesc()
+        self._lib.cn_fluid_grid_desc_defaults(C.byref(d))
+        d.size = (C.c_float * 3)(*size)
+        d.target_particle_spacing = spacing
+        self._transform(d.rest_transform, position)
+        d.particle_mass, d.particle_radius = mass, radius
+        d.viscosity, d.cohesion, d.surface_tension = viscosity, cohesion, surface_tension
+        d.vorticity_confinement, d.gravity_scale, d.cfl_coefficient = vorticity, gravity_scale, cfl
+        d.environment_index, d.collision_layer, d.collision_mask = environment, layer, mask
+        self._material(d.material, friction, restitution, damping, static_friction)
+        out = C.c_uint32()
+        _check(self._lib.cn_world_add_fluid_grid(self._h, C.byref(d), C.byref(out)))
+        return out.value
+
+    def add_cloth_grid(self, resolution, size, position=(0, 0, 0), rotation=(0, 0, 0, 1), *, mass=1.0,
+                       radius=0.02, structural_compliance=0.0, bend_compliance=0.0, self_collision=False,
+                       static_particles: Sequence[int] = (), environment=0, layer=1, mask=0xFFFFFFFF,
+                       friction=0.0, restitution=0.0, damping=0.0, static_friction=-1.0) -> int:
+        """ClothState over a rectangular triangle grid (cloth_authoring.cpp:58-191)."""
+        d = _abi.ClothGridDesc()
+        self._lib.cn_cloth_grid_desc_defaults(C.byref(d))
+        d.resolution = (C.c_uint32 * 2)(*resolution)
+        d.size = (C.c_float * 2)(*size)
+        self._transform(d.rest_transform, position, rotation)
+        d.particle_mass, d.particle_radius = mass, radius
+        d.structural_compliance, d.bend_compliance = structural_compliance, bend_compliance
+        d.self_collision_enabled = int(self_collision)
+        d.environment_index, d.collision_layer, d.collision_mask = environment, layer, mask
+        self._material(d.material, friction, restitution, damping, static_friction)
+        st = np.ascontiguousarray(np.asarray(static_particles, dtype=np.uint32))
+        self._keep.append(st)
+        d.static_particle_indices = _u32(st) if st.size else None
+        d.static_particle_count = st.size
+        out = C.c_uint32()
+        _check(self._lib.cn_world_add_cloth_grid(self._h, C.byref(d), C.byref(out)))
+        return out.value
+
+    def add_strand(self, rest_positions, *, mass=1.0, radius=0.01, stretch_shear_compliance=0.0,
+                   bend_compliance=0.0, twist_compliance=0.0, distance_compliance=0.0, self_collision=False,
+                   static_particles: Sequence[int] = (), environment=0, layer=1, mask=0xFFFFFFFF,
+                   friction=0.0, restitution=0.0, damping=0.0, static_friction=-1.0) -> int:
+        """StrandState (physics_world.cpp:6893-6969)."""
+        d = _abi.StrandDesc()
+        self._lib.cn_strand_desc_defaults(C.byref(d))
+        pts = np.ascontiguousarray(np.asarray(rest_positions, dtype=np.float32).reshape(-1, 3))
+        self._keep.append(pts)
+        d.rest_positions = _f32(pts)
+        d.rest_position_count = pts.shape[0]
+        d.particle_mass, d.particle_radius = mass, radius
+        d.stretch_shear_compliance, d.bend_compliance = stretch_shear_compliance, bend_compliance
+        d.twist_compliance, d.distance_compliance = twist_compliance, distance_compliance
+        d.self_collision_enabled = int(self_collision)
+        d.environment_index, d.collision_layer, d.collision_mask = environment, layer, mask
+        self._material(d.material, friction, restitution, damping, static_friction)
+        st = np.ascontiguousarray(np.asarray(static_particles, dtype=np.uint32))
+        self._keep.append(st)
+        d.static_particle_indices = _u32(st) if st.size else None
+        d.static_particle_count = st.size
+        out = C.c_uint32()
+        _check(self._lib.cn_world_add_strand(self._h, C.byref(d), C.byref(out)))
+        return out.value
+
+    def add_rigid_body(self, body_type="static", position=(0, 0, 0), orientation=(0, 0, 0, 1),
+                       scale=(1, 1, 1)) -> int:
+        d = _abi.RigidBodyDesc()
+        self._lib.cn_rigid_body_desc_defaults(C.byref(d))
+        d.body_type = {"static": 0, "kinematic": 1, "dynamic": 2}[body_type]
+        d.position = (C.c_float * 3)(*position)
+        d.orientation = (C.c_float * 4)(*orientation)
+        d.scale = (C.c_float * 3)(*scale)
+        out = C.c_uint32()
+        _check(self._lib.cn_world_add_rigid_body(self._h, C.byref(d), C.byref(out)))
+        return out.value
+
+    def add_collider(self, body, shape, params, local_position=(0, 0, 0), local_orientation=(0, 0, 0, 1), *,
+                     friction=0.5, static_friction=-1.0, restitution=0.0, enabled=True, environment=0,
+                     layer=1, mask=0xFFFFFFFF) -> int:
+        d = _abi.ColliderDesc()
+        self._lib.cn_collider_desc_defaults(C.byref(d))
+        d.body = body
+        d.shape_type = {"sphere": 0, "box": 1, "capsule": 2}[shape]
+        p = list(params) + [0.0] * (4 - len(params))
+        d.shape_params = (C.c_float * 4)(*p)
+        d.local_position = (C.c_float * 3)(*local_position)
+        d.local_orientation = (C.c_float * 4)(*local_orientation)
+        d.enabled = int(enabled)
+        d.friction, d.static_friction, d.restitution = friction, static_friction, restitution
+        d.environment_index, d.collision_layer, d.collision_mask = environment, layer, mask
+        out = C.c_uint32()
+        _check(self._lib.cn_world_add_collider(self._h, C.byref(d), C.byref(out)))
+        return out.value
+
+    def soa(self) -> _abi.WorldSoA:
+        s = _abi.WorldSoA()
+        _check(self._lib.cn_world_get_soa(self._h, C.byref(s)))
+        self._soa = s
+        return s
+
+    # views into the packed SoA (valid until the next add_* call)
+    def positions(self) -> np.ndarray:
+        s = self._soa or self.soa()
+        return _view(s.positions_inv_mass, s.particle_count, np.float32, 4)
+
+    def velocities(self) -> np.ndarray:
+        s = self._soa or self.soa()
+        return _view(s.velocities, s.particle_count, np.float32, 4)
+
+    def counts(self) -> dict:
+        s = self._soa or self.soa()
+        return {"particles": s.particle_count, "edges": s.edge_count, "bends": s.bend_count,
+                "dihedrals": s.dihedral_count, "tets": s.tet_count, "segments": s.strand_segment_count,
+                "joints": s.strand_joint_count, "distances": s.strand_distance_count,
+                "bodies": s.rigid_body_count, "colliders": s.collider_count,
+                "fluid_materials": s.fluid_material_count}
+
+    def fluid_materials(self) -> np.ndarray:
+        s = self._soa or self.soa()
+        return _view(s.fluid_materials, s.fluid_material_count, np.float32, 12)
+
+    def array(self, name: str) -> np.ndarray:
+        """Raw view of one SoA array, e.g. ``array("kinds")`` or ``array("tets")``."""
+        s = self._soa or self.soa()
+        n = s.particle_count
+        spec = {"kinds": ("kinds", n, np.uint32, 1), "metadata": ("metadata", n, np.uint32, 4),
+                "radii": ("radii", n, np.float32, 1),
+                "tets": ("tets", s.tet_count, np.uint32, 8), "edges": ("edges", s.edge_count, np.uint32, 8),
+                "dihedrals": ("dihedrals", s.dihedral_count, np.uint32, 8),
+                "segments": ("strand_segments", s.strand_segment_count, np.uint32, 8),
+                "joints": ("strand_joints", s.strand_joint_count, np.uint32, 8)}[name]
+        return _view(getattr(s, spec[0]), spec[1], spec[2], spec[3])
+
+
+class Solver:
+    """PhysicsSolver mirror (include/physics/physics_solver.h:150-205) on one CUDA device."""
+
+    def __init__(self, desc: Optional[_abi.SolverDesc] = None, device: int = 0):
+        self._lib = load()
+        self.desc = desc if desc is not None else solver_desc()
+        h = C.c_void_p()
+        _check(self._lib.cn_solver_create(C.byref(self.desc), device, C.byref(h)))
+        self._h = h
+        self._n = 0
+        self._world = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cn_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync_world(self, world: "World | _abi.WorldSoA") -> None:
+        soa = world.soa() if isinstance(world, World) else world
+        if isinstance(world, World):
+            self._world = world
+        _check(self._lib.cn_solver_sync_world(self._h, C.byref(soa)))
+        self._n = soa.particle_count
+        self._segments = soa.strand_segment_count
+
+    def step(self, dt: float, stream: int = 0) -> None:
+        _check(self._lib.cn_solver_step(self._h, dt, C.c_void_p(stream) if stream else None))
+
+    def step_many(self, dt: float, steps: int, stream: int = 0) -> None:
+        _check(self._lib.cn_solver_step_many(self._h, dt, steps, C.c_void_p(stream) if stream else None))
+
+    def validate_gpu_meta(self) -> dict:
+        m = _abi.Meta()
+        status = self._lib.cn_solver_validate_meta(self._h, C.byref(m))
+        out = {name: getattr(m, name) for name, _ in _abi.Meta._fields_ if name != "reserved"}
+        out["status"] = STATUS.get(status, status)
+        return out
+
+    def set_gravity(self, g) -> None:
+        _check(self._lib.cn_solver_set_gravity(self._h, *map(float, g)))
+
+    def set_kinematic_target(self, body: int, position, orientation=(0, 0, 0, 1)) -> None:
+        p = (C.c_float * 3)(*position)
+        q = (C.c_float * 4)(*orientation)
+        _check(self._lib.cn_solver_set_kinematic_target(self._h, body, p, q))
+
+    def set_debug(self, keep_fluid_delta=False, post_update_neighbors=False, force_broadphase=False) -> None:
+        flags = (1 if keep_fluid_delta else 0) | (2 if post_update_neighbors else 0) | (4 if force_broadphase else 0)
+        _check(self._lib.cn_solver_set_debug(self._h, flags))
+
+    def set_timing(self, enable: bool = True) -> None:
+        _check(self._lib.cn_solver_set_timing(self._h, int(enable)))
+
+    def kernel_times(self) -> dict:
+        n = C.c_uint32()
+        _check(self._lib.cn_solver_kernel_times(self._h, None, 0, C.byref(n)))
+        arr = (_abi.KernelTime * max(n.value, 1))()
+        _check(self._lib.cn_solver_kernel_times(self._h, arr, n.value, C.byref(n)))
+        return {arr[i].name.decode(): (arr[i].milliseconds, arr[i].launches) for i in range(n.value)}
+
+    def graph_stats(self) -> tuple:
+        k, t = C.c_uint32(), C.c_uint32()
+        _check(self._lib.cn_solver_graph_stats(self._h, C.byref(k), C.byref(t)))
+        return k.value, t.value
+
+    def gpu_scene_view(self) -> dict:
+        v = _abi.SceneView()
+        _check(self._lib.cn_solver_scene_view(self._h, C.byref(v)))
+        return {name: getattr(v, name) for name, _ in _abi.SceneView._fields_ if name != "reserved"}
+
+    def read_particles(self):
+        x = np.zeros((self._n, 4), np.float32)
+        v = np.zeros((self._n, 4), np.float32)
+        xp = np.zeros((self._n, 4), np.float32)
+        _check(self._lib.cn_solver_read_particles(self._h, _f32(x), _f32(v), _f32(xp), self._n))
+        return x, v, xp
+
+    def write_particles(self, x: Optional[np.ndarray] = None, v: Optional[np.ndarray] = None) -> None:
+        xa = np.ascontiguousarray(x, dtype=np.float32) if x is not None else None
+        va = np.ascontiguousarray(v, dtype=np.float32) if v is not None else None
+        _check(self._lib.cn_solver_write_particles(self._h, _f32(xa) if xa is not None else None,
+                                                   _f32(va) if va is not None else None, self._n))
+
+    def read_strand_orientations(self) -> np.ndarray:
+        q = np.zeros((self._segments, 4), np.float32)
+        if self._segments:
+            _check(self._lib.cn_solver_read_strand_orientations(self._h, _f32(q), self._segments))
+        return q
+
+    def debug_read(self, name: str) -> np.ndarray:
+        which = DEBUG[name]
+        size = C.c_size_t()
+        _check(self._lib.cn_solver_debug_read(self._h, which, None, 0, C.byref(size)))
+        buf = np.zeros(size.value, np.uint8)
+        _check(self._lib.cn_solver_debug_read(self._h, which, buf.ctypes.data_as(C.c_void_p), size.value,
+                                              C.byref(size)))
+        return buf

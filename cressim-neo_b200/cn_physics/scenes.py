@@ -1,0 +1,124 @@
+"""Seeded synthetic scenes for the reference's benchmark configurations.
+
+No public dataset is involved: every scene is generated from its sizes and a seed, with the
+shapes and value ranges of the configurations it stands for.
+
+* ``xpbd_cube``   -- plain XPBD soft body: 16x16x16-vertex lattice split 5 tets per cell
+                     (16,875 tets), edge compliance 1e-5, volume compliance 1e-6, bottom face
+                     pinned, ground box with its top face at y = 0, jitter +-1e-3 of the edge length.
+* ``dam_break``   -- plain PBF dam break: 128x64x128 fluid lattice (1,048,576 particles) at spacing
+                     0.05 (h = 0.1, radius 0.03) in a 12.8 x 6.4 x 25.6 box of static walls,
+                     viscosity 0.01, vorticity off, jitter +-1e-4.
+* ``mixed_surgical`` -- tissue lattice + cloth + strands + fluid block + a kinematic capsule tool.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import World, solver_desc
+
+
+def _jitter(world: World, amplitude: float, seed: int) -> None:
+    x = world.positions()
+    rng = np.random.default_rng(seed)
+    movable = x[:, 3] > 0.0
+    j = rng.uniform(-amplitude, amplitude, size=(x.shape[0], 3)).astype(np.float32)
+    x[movable, :3] += j[movable]
+
+
+def ground(world: World, top_y: float = 0.0, half=(50.0, 0.5, 50.0), friction=0.5) -> int:
+    body = world.add_rigid_body("static", position=(0.0, top_y - half[1], 0.0))
+    world.add_collider(body, "box", half, friction=friction)
+    return body
+
+
+def xpbd_cube(n: int = 16, spacing: float = 1.0 / 16.0, seed: int = 0, radius: float | None = None,
+              pin_bottom: bool = True, lift: float = 0.0):
+    """Returns (world, desc, frame_dt).  n vertices per axis; cube bottom face sits on the ground."""
+    w = World()
+    size = (n - 1) * spacing
+    r = spacing * 0.5 if radius is None else radius
+    res = n
+    static = []
+    if pin_bottom:
+        for x in range(res):
+            for z in range(res):
+                static.append(x * res * res + 0 * res + z)
+    w.add_soft_body_grid((size, size, size), spacing, position=(0.0, size * 0.5 + r + lift, 0.0),
+                         radius=r, edge_compliance=1.0e-5, volume_compliance=1.0e-6,
+                         static_particles=static, friction=0.3)
+    ground(w)
+    w.soa()
+    _jitter(w, 1.0e-3 * spacing, seed)
+    desc = solver_desc(substeps=10, default_iterations=20, enable_blocking_readback=0)
+    return w, desc, 1.0 / 60.0
+
+
+def dam_break(nx: int = 128, ny: int = 64, nz: int = 128, spacing: float = 0.05, seed: int = 0,
+              box=(12.8, 6.4, 25.6)):
+    """Returns (world, desc, frame_dt)."""
+    w = World()
+    r = 0.6 * spacing  # h = max((2/0.6) r, 2r) = 2 * spacing
+    size = (nx * spacing, ny * spacing, nz * spacing)
+    offset = r - 0.5 * spacing
+    center = (size[0] * 0.5 + offset, size[1] * 0.5 + offset, size[2] * 0.5 + offset)
+    w.add_fluid_grid(size, spacing, position=center, radius=r, viscosity=0.01, vorticity=0.0)
+    body = w.add_rigid_body("static")
+    bx, by, bz = box
+    t = 0.5
+    w.add_collider(body, "box", (bx * 0.5 + 2 * t, t, bz * 0.5 + 2 * t), (bx * 0.5, -t, bz * 0.5))
+    w.add_collider(body, "box", (t, by * 0.5 + 2 * t, bz * 0.5 + 2 * t), (-t, by * 0.5, bz * 0.5))
+    w.add_collider(body, "box", (t, by * 0.5 + 2 * t, bz * 0.5 + 2 * t), (bx + t, by * 0.5, bz * 0.5))
+    w.add_collider(body, "box", (bx * 0.5 + 2 * t, by * 0.5 + 2 * t, t), (bx * 0.5, by * 0.5, -t))
+    w.add_collider(body, "box", (bx * 0.5 + 2 * t, by * 0.5 + 2 * t, t), (bx * 0.5, by * 0.5, bz + t))
+    w.soa()
+    _jitter(w, 1.0e-4, seed)
+    desc = solver_desc(substeps=2, fluid_iterations=4, enable_blocking_readback=0)
+    return w, desc, 1.0 / 120.0
+
+
+def tool_path(t: float, seed: int = 0, center=(0.0, 0.6, 0.0), amplitude=0.3):
+    """Seeded smooth random path: a sum of three sines per axis."""
+    rng = np.random.default_rng(seed)
+    freq = rng.uniform(0.3, 1.5, size=(3, 3))
+    phase = rng.uniform(0.0, 2.0 * math.pi, size=(3, 3))
+    amp = rng.uniform(0.3, 1.0, size=(3, 3))
+    amp = amp / amp.sum(axis=1, keepdims=True) * amplitude
+    p = [center[a] + float(np.sum(amp[a] * np.sin(freq[a] * t + phase[a]))) for a in range(3)]
+    return tuple(p)
+
+
+def mixed_surgical(tissue=(60, 30, 60), cloth=(256, 256), strands=(64, 129), fluid=(64, 64, 64),
+                   seed: int = 0):
+    """Tissue lattice + cloth sheet + strands + fluid block + kinematic capsule (r = 0.01).
+    Returns (world, desc, frame_dt, tool_body)."""
+    w = World()
+    sp = 0.02
+    tx, ty, tz = tissue
+    tsize = ((tx - 1) * sp, (ty - 1) * sp, (tz - 1) * sp)
+    w.add_soft_body_grid(tsize, sp, position=(0.0, tsize[1] * 0.5 + 0.01, 0.0), radius=0.01,
+                         edge_compliance=1.0e-5, volume_compliance=1.0e-6, friction=0.3)
+    cres = cloth
+    csize = (tsize[0] * 1.2, tsize[2] * 1.2)
+    w.add_cloth_grid(cres, csize, position=(0.0, tsize[1] + 0.05, 0.0), radius=0.004,
+                     structural_compliance=1.0e-6, bend_compliance=1.0e-3, friction=0.3)
+    ns, npts = strands
+    for k in range(ns):
+        x0 = -tsize[0] * 0.5 + (k + 0.5) * tsize[0] / ns
+        pts = [(x0, tsize[1] + 0.15, -tsize[2] * 0.5 + j * tsize[2] / (npts - 1)) for j in range(npts)]
+        w.add_strand(pts, radius=0.003, stretch_shear_compliance=1.0e-6, bend_compliance=1.0e-4,
+                     twist_compliance=1.0e-4, static_particles=[0])
+    fx, fy, fz = fluid
+    fsp = 0.01
+    w.add_fluid_grid((fx * fsp, fy * fsp, fz * fsp), fsp,
+                     position=(tsize[0] * 0.5 + 0.1 + fx * fsp * 0.5, fy * fsp * 0.5 + 0.01, 0.0),
+                     radius=0.6 * fsp)
+    ground(w)
+    tool = w.add_rigid_body("kinematic", position=tool_path(0.0, seed))
+    w.add_collider(tool, "capsule", (0.01, 0.1), friction=0.2)
+    w.soa()
+    _jitter(w, 1.0e-4, seed)
+    desc = solver_desc(substeps=8, enable_blocking_readback=0)
+    return w, desc, 1.0 / 60.0, tool

@@ -1,0 +1,197 @@
+// cn_device.h -- device-resident scene layout and kernel launchers of the particle substep.
+//
+// One Scene value holds every device pointer and count the kernels need; it is passed by
+// value to each launch so a captured CUDA graph replays with stable arguments.  Per-particle
+// state stays in the reference's particle order (float4 x/invMass, x_prev, v: the layout
+// PhysicsGpuSceneView exports, include/physics/physics_gpu_scene_view.h:114-169).  The fluid
+// solve runs in cell order: after the broadphase sort every fluid quantity of an iteration
+// (position, accumulated delta, density constraint, neighbour list) lives at the particle's
+// sorted slot, so neighbour gathers touch contiguous cell runs.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/cn_physics.h"
+
+namespace cn {
+
+// GpuParticleRigidContact (physics_particle_types.hlsli:74-83), 64 B.
+struct RigidContact {
+    uint32_t particle, body, collider, active;
+    float4 normalPenetration;
+    float4 rigidLocalPoint;
+    float4 material;
+};
+// GpuParticleContact (physics_particle_types.hlsli:85-92), 48 B.
+struct ParticleContact {
+    uint32_t a, b, active, reserved;
+    float4 normalPenetration;
+    float4 material;
+};
+
+// Device counters (mirrors GpuParticleNeighborMeta plus this build's own counters).
+struct DeviceMeta {
+    uint32_t rigidPairCount;          // min(required, capacity)
+    uint32_t requiredRigidPairs;
+    uint32_t particlePairCount;
+    uint32_t requiredParticlePairs;
+    uint32_t activeRigidContacts;
+    uint32_t activeParticleContacts;
+    uint32_t boundaryMaskOverflow;
+    uint32_t neighborTruncations;
+    uint32_t waitTimeouts;
+    uint32_t reserved[7];
+};
+
+constexpr uint32_t kMaxBoundaryColliders = 64u;  // bits of the per-particle boundary mask
+constexpr uint32_t kRigidDedup = 16u;            // kParticleRigidDedupCacheSize
+constexpr uint32_t kColliderIterationCap = 64u;  // kParticleRigidColliderIterationCap
+constexpr float kBroadPhaseMargin = 0.05f;       // physics_shape_common.hlsli:10
+
+struct Scene {
+    uint32_t N = 0;
+    // ---- particles (reference order) ----
+    float4 *x = nullptr, *xprev = nullptr, *v = nullptr;
+    const float *radii = nullptr;
+    const uint32_t *kinds = nullptr;
+    const uint4 *meta = nullptr;            // (environment, phase, layer, mask)
+    const uint32_t *matIdx = nullptr;
+    const uint32_t *fluidMatIdx = nullptr;
+    const uint32_t *ownerTypes = nullptr;
+    const uint32_t *ownerIdx = nullptr;
+    const uint32_t *adjOff = nullptr, *adjCnt = nullptr, *adjIdx = nullptr;
+    const float4 *contactMaterials = nullptr;
+    const cn_fluid_material *fluidMaterials = nullptr;
+    float cellSize = 1.0f;
+
+    // ---- soft constraints ----
+    uint32_t E = 0, Bn = 0, D = 0, T = 0, S = 0, J = 0, SD = 0;
+    const cn_soft_edge *edges = nullptr;
+    const cn_soft_bend *bends = nullptr;
+    const cn_cloth_dihedral *dihedrals = nullptr;
+    const cn_soft_tet *tets = nullptr;
+    const cn_strand_segment *segs = nullptr;
+    const cn_strand_joint *joints = nullptr;
+    const cn_strand_distance *dists = nullptr;
+    float4 *segOrient = nullptr;
+    // incidence: per-particle (start, count) and (constraint, slot) records, ascending
+    // constraint order (physics_scene_gpu_state.cpp:3255-3420)
+    const uint2 *edgeRanges = nullptr, *edgeInc = nullptr;
+    const uint2 *bendRanges = nullptr, *bendInc = nullptr;
+    const uint2 *tetRanges = nullptr, *tetInc = nullptr;
+    const uint2 *segRanges = nullptr, *segInc = nullptr;
+    const uint2 *segJointRanges = nullptr, *segJointInc = nullptr;
+    // lambdas and per-constraint correction records
+    float *edgeLambda = nullptr, *bendLambda = nullptr, *tetLambda = nullptr, *distLambda = nullptr;
+    float4 *segLambda = nullptr, *jointLambda = nullptr;
+    float4 *edgeCorr = nullptr;   // 2 per edge
+    float4 *bendCorr = nullptr;   // 4 per bend / dihedral
+    float4 *tetCorr = nullptr;    // 4 per tet
+    float4 *segCorr = nullptr;    // 3 per segment
+    float4 *jointCorr = nullptr;  // 2 per joint (twistRotationA, twistRotationB)
+    float4 *distCorr = nullptr;   // 2 per distance
+    float4 *posCorr = nullptr, *velCorr = nullptr;
+
+    // ---- rigid bodies / colliders ----
+    uint32_t B = 0, C = 0;
+    float4 *bodyPos = nullptr, *bodyRot = nullptr, *bodyLin = nullptr, *bodyAng = nullptr;
+    const float4 *bodyScale = nullptr, *bodyInvInertia = nullptr;
+    const uint32_t *bodyType = nullptr;
+    float4 *bodyKinPos = nullptr, *bodyKinRot = nullptr;
+    uint32_t *bodyKinFlags = nullptr;
+    const uint2 *bodyColRanges = nullptr;
+    const uint32_t *bodyColIdx = nullptr;
+    const cn_collider_geometry *colGeo = nullptr;
+    const cn_collider_broadphase *colBp = nullptr;
+    const float4 *colMat = nullptr;
+    float4 *prevBodyPos = nullptr, *prevBodyRot = nullptr;
+    float4 *predBodyPos = nullptr, *predBodyRot = nullptr, *predBodyLin = nullptr, *predBodyAng = nullptr;
+    float4 *colAabbMin = nullptr, *colAabbMax = nullptr;
+    const uint32_t *colQueryOrder = nullptr; // moving colliders first, then static
+    uint32_t colQueryCount = 0, activeMovingCount = 0;
+
+    // ---- broadphase ----
+    int4 *entries = nullptr;          // (cellX, cellY, cellZ, key) per particle
+    uint32_t *keysA = nullptr, *keysB = nullptr, *valsA = nullptr, *valsB = nullptr;
+    uint32_t *rank = nullptr;         // particle -> sorted slot
+    uint32_t tableMask = 0;           // cell hash table capacity - 1
+    uint32_t *tableKeys = nullptr, *tableStart = nullptr;
+    uint32_t *cellEnd = nullptr;      // at a run start: end | (mixed-coordinate flag << 31)
+
+    // ---- fluid (cell order) ----
+    uint32_t hasFluid = 0;
+    float4 *Xs = nullptr;             // x at the sorted slot (w = invMass)
+    float4 *P = nullptr;              // x + accumulated delta, w = invMass
+    float4 *Da = nullptr, *Db = nullptr; // accumulated delta ping-pong
+    float4 *Cs = nullptr;             // surface normal xyz, density constraint w
+    float4 *Dx = nullptr;             // packed delta + interaction weight (last iteration)
+    int4 *sCell = nullptr;            // cell entry at the sorted slot
+    uint4 *sMeta = nullptr;           // metadata at the sorted slot
+    uint32_t *sInfo = nullptr;        // kind (bit 31 = fluid) | fluid material index
+    unsigned long long *sBoundary = nullptr; // boundary-collider candidate mask (query order)
+    uint32_t maxNbr = 128;
+    uint32_t *nbr = nullptr;          // [N][maxNbr] sorted slots
+    uint32_t *nbrCount = nullptr;     // per sorted slot
+
+    // ---- contact candidates ----
+    uint32_t *candCount = nullptr, *candOffset = nullptr; // per particle
+    uint32_t *ppCount = nullptr, *ppOffset = nullptr;
+    uint2 *rigidPairs = nullptr;      // (particle, body)
+    uint32_t rigidPairCapacity = 0;
+    RigidContact *rigidContacts = nullptr;
+    uint2 *particlePairs = nullptr;   // (a, b)
+    uint32_t particlePairCapacity = 0;
+    ParticleContact *particleContacts = nullptr;
+    DeviceMeta *meta_ = nullptr;
+};
+
+// Settings the kernels read (PhysicsSolverConfigBuffer, physics_solver_config.hlsli:5-51).
+struct Config {
+    float slop, softContactRelaxation, softMaxCorrection, restitutionVelocityThreshold;
+    float restitutionPenetrationThreshold, positionFrictionMinDistance;
+    float softInternalRelaxation;
+    float fluidSolveCoefficient, fluidRelaxation, fluidBoundaryDensityScale, fluidBoundaryDeltaScale;
+    float fluidMaxUnderDensityRatio;
+    float gravity[3];
+};
+
+// ------------------------------------------------------------------ launchers (cn_kernels.cu)
+void launchRigidPredict(const Scene &s, float dt, float gx, float gy, float gz, cudaStream_t st);
+void launchPredictAndKeys(const Scene &s, float dt, const Config &c, cudaStream_t st);
+void launchCellSetup(const Scene &s, cudaStream_t st);
+void launchRigidCandidates(const Scene &s, uint32_t *scanTmp, size_t scanTmpBytes, cudaStream_t st);
+void launchParticleCandidates(const Scene &s, uint32_t *scanTmp, size_t scanTmpBytes, cudaStream_t st);
+void launchFluidIteration(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
+                          cudaStream_t st);
+void launchFluidGather(const Scene &s, uint32_t iter, cudaStream_t st);
+void launchFluidNeighborsDensity(const Scene &s, const Config &c, cudaStream_t st);
+void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
+                                cudaStream_t st);
+void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st);
+void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st);
+void launchContacts(const Scene &s, const Config &c, bool particleContacts, bool rigidContacts,
+                    cudaStream_t st);
+void launchUpdateVelocities(const Scene &s, float dt, const float4 *fluidDelta, cudaStream_t st);
+void launchFluidBoundaryVelocities(const Scene &s, float dt, const Config &c, cudaStream_t st);
+void launchRigidContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st);
+void launchParticleContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st);
+void launchCopyPredictedRigid(const Scene &s, cudaStream_t st);
+// debug export of the compacted cell-range table (reference layout)
+void launchExportCellRanges(const Scene &s, uint4 *out, uint32_t capacity, uint32_t *scanTmp,
+                            size_t scanTmpBytes, cudaStream_t st);
+
+// ------------------------------------------------------------------ sort / scan (cn_sort.cu)
+// Stable LSD radix sort of (key, index) pairs, 8-bit digits, onesweep passes with
+// decoupled look-back.  keys/vals A hold the input keys (vals ignored: the input index is
+// implied) and receive the sorted result; B is the ping-pong buffer.
+size_t radixSortScratchBytes(uint32_t n);
+void radixSortPairs(uint32_t *keysA, uint32_t *valsA, uint32_t *keysB, uint32_t *valsB, uint32_t n,
+                    void *scratch, uint32_t *waitTimeouts, cudaStream_t st);
+// Exclusive scan of n uint32 values; *total (device) receives the sum.
+size_t scanScratchBytes(uint32_t n);
+void exclusiveScan(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *total, void *scratch,
+                   cudaStream_t st);
+
+} // namespace cn

@@ -1,0 +1,1658 @@
+// cn_kernels.cu -- sm_100a kernels of the CRESSim-Neo particle physics substep.
+//
+// Each kernel cites the reference HLSL pass (paths relative to the reference project root)
+// whose result it reproduces.  The reference dispatches ~20 passes per solver iteration, each
+// a 64-thread-group 1-D dispatch over particles or constraints.  Here:
+//  * predict + cell key + sort key are one pass over particles;
+//  * the cell-range table is a hash map keyed by the reference's 32-bit cell key, with the
+//    reference's "skip a cell whose key is 0xffffffff" and coordinate-compare semantics;
+//  * the fluid solve runs in cell order (sorted slots): one kernel builds the neighbour list
+//    and the density constraint, one kernel computes the position delta, applies it and
+//    clamps against the boundary (the reference's four fluid passes per iteration);
+//  * particle-rigid contacts are generated, solved and summed per particle in candidate-pair
+//    order, so their sums are deterministic (the reference uses float atomics).
+// Arithmetic follows the reference's expression order; the library is built with
+// --fmad=false so float32 results match a CPU evaluation of the same order.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "cn_device.h"
+#include "cn_math.cuh"
+
+namespace cn {
+namespace {
+
+constexpr int kThreads = 256;
+inline unsigned blocksFor(uint32_t n) { return n == 0 ? 1u : (n + kThreads - 1) / kThreads; }
+constexpr uint32_t kFluidBit = 0x80000000u;
+
+__device__ __forceinline__ float4 ld4(const float4 *p) { return __ldg(p); }
+
+// ------------------------------------------------------------------------------------------
+// Rigid predict (static / kinematic; dynamic bodies are integrated without particle feedback)
+// physics_rigid_predict.cs.hlsl:20-81, collider world AABBs physics_rigid_update_world_aabbs.cs.hlsl
+// ------------------------------------------------------------------------------------------
+__device__ void computeBodyAabb(uint32_t shape, f3 pos, float4 q, float4 p, float4 sc, f3 &mnv, f3 &mxv)
+{
+    f3 e{0.f, 0.f, 0.f};
+    if (shape == CN_COLLIDER_SPHERE) {
+        const float r = sphereRadius(p, sc);
+        e = f3{r, r, r};
+    } else if (shape == CN_COLLIDER_BOX) {
+        const f3 h = boxHalfExtents(p, sc);
+        e = fabs3(qRotate(q, f3{1.f, 0.f, 0.f})) * h.x + fabs3(qRotate(q, f3{0.f, 1.f, 0.f})) * h.y +
+            fabs3(qRotate(q, f3{0.f, 0.f, 1.f})) * h.z;
+    } else {
+        f3 a, b;
+        float r = 0.0f;
+        capsuleSegment(pos, q, p, sc, a, b, r);
+        const f3 axis = fabs3(qRotate(q, f3{0.f, 1.f, 0.f}));
+        e = axis * (0.5f * length(b - a)) + f3{r, r, r};
+    }
+    mnv = pos - e;
+    mxv = pos + e;
+}
+
+__global__ void __launch_bounds__(kThreads) k_rigidPredict(Scene s, float dt, float gx, float gy, float gz)
+{
+    for (uint32_t b = threadIdx.x; b < s.B; b += blockDim.x) {
+        const float4 p = s.bodyPos[b];
+        const float4 q = qNormalize(s.bodyRot[b]);
+        const float4 lin = s.bodyLin[b], ang = s.bodyAng[b];
+        const bool kin = (s.bodyKinFlags[b] & 1u) != 0u;
+        const float4 kq = qNormalize(s.bodyKinRot[b]);
+        s.prevBodyPos[b] = p;
+        s.prevBodyRot[b] = q;
+        const uint32_t type = s.bodyType[b];
+        if (type == CN_BODY_STATIC) {
+            s.predBodyPos[b] = p;
+            s.predBodyRot[b] = q;
+            s.predBodyLin[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+            s.predBodyAng[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+        } else if (type == CN_BODY_KINEMATIC) {
+            const f3 pp = kin ? xyz(s.bodyKinPos[b]) : xyz(p);
+            const float4 pq = kin ? kq : q;
+            const f3 l = (pp - xyz(p)) / mx(dt, kEps);
+            const f3 a = angularVelocityFromQuaternionDelta(q, pq, mx(dt, kEps));
+            s.predBodyPos[b] = mk4(pp, p.w);
+            s.predBodyRot[b] = pq;
+            s.predBodyLin[b] = mk4(l, lin.w);
+            s.predBodyAng[b] = mk4(a, ang.w);
+        } else {
+            const f3 l = xyz(lin) + f3{gx, gy, gz} * dt;
+            s.predBodyPos[b] = mk4(xyz(p) + l * dt, p.w);
+            s.predBodyRot[b] = q;
+            s.predBodyLin[b] = mk4(l, lin.w);
+            s.predBodyAng[b] = ang;
+        }
+    }
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < s.C; c += blockDim.x) {
+        const cn_collider_broadphase bp = s.colBp[c];
+        const uint32_t ob = bp.owner_body;
+        if (ob >= s.B || bp.enabled_flag == 0u) {
+            s.colAabbMin[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+            s.colAabbMax[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+            continue;
+        }
+        const float4 sc = s.bodyScale[ob];
+        const cn_collider_geometry cg = s.colGeo[c];
+        const float4 params = make_float4(cg.shape_params[0], cg.shape_params[1], cg.shape_params[2],
+                                          cg.shape_params[3]);
+        const f3 lp = f3{cg.local_position[0], cg.local_position[1], cg.local_position[2]} * xyz(sc);
+        const float4 lq = qNormalize(make_float4(cg.local_orientation[0], cg.local_orientation[1],
+                                                 cg.local_orientation[2], cg.local_orientation[3]));
+        const float4 bq = qNormalize(s.predBodyRot[ob]);
+        const float4 pbq = qNormalize(s.prevBodyRot[ob]);
+        const f3 cp = xyz(s.predBodyPos[ob]) + qRotate(bq, lp);
+        const float4 cq = qNormalize(qMul(bq, lq));
+        const f3 pcp = xyz(s.prevBodyPos[ob]) + qRotate(pbq, lp);
+        const float4 pcq = qNormalize(qMul(pbq, lq));
+        f3 a0, a1, b0, b1;
+        computeBodyAabb(bp.shape_type, cp, cq, params, sc, a0, a1);
+        computeBodyAabb(bp.shape_type, pcp, pcq, params, sc, b0, b1);
+        const f3 lo = min3(a0, b0) - f3{kBroadPhaseMargin, kBroadPhaseMargin, kBroadPhaseMargin};
+        const f3 hi = max3(a1, b1) + f3{kBroadPhaseMargin, kBroadPhaseMargin, kBroadPhaseMargin};
+        s.colAabbMin[c] = mk4(lo, 0.f);
+        s.colAabbMax[c] = mk4(hi, 0.f);
+    }
+}
+
+// physics_rigid_update_velocities (copyPredictedRigidBodiesToPersistentState)
+__global__ void k_copyPredictedRigid(Scene s)
+{
+    for (uint32_t b = threadIdx.x; b < s.B; b += blockDim.x) {
+        s.bodyPos[b] = s.predBodyPos[b];
+        s.bodyRot[b] = s.predBodyRot[b];
+        s.bodyLin[b] = s.predBodyLin[b];
+        s.bodyAng[b] = s.predBodyAng[b];
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Predict + broadphase entry + sort key.
+// physics_soft_predict.cs.hlsl:12-47, physics_particle_build_broad_phase_entries.cs.hlsl:9-35,
+// physics_particle_build_broad_phase_keys.cs.hlsl:8-23
+// ------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_predictKeys(Scene s, float dt, float gx, float gy, float gz,
+                                                          bool writeKeys)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.N) return;
+    const float4 pim = s.x[i];
+    const f3 pos = xyz(pim);
+    s.xprev[i] = mk4(pos, 0.0f);
+    f3 pp = pos;
+    if (pim.w <= kEps) {
+        s.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+        f3 vel = xyz(s.v[i]);
+        float gs = 1.0f;
+        if (s.kinds[i] == CN_PARTICLE_FLUID) gs = s.fluidMaterials[s.fluidMatIdx[i]].gravity_scale;
+        vel = vel + f3{gx, gy, gz} * (dt * gs);
+        pp = pos + vel * dt;
+        s.v[i] = mk4(vel, 0.0f);
+        s.x[i] = mk4(pp, pim.w);
+    }
+    if (!writeKeys) return;
+    const float safe = mx(s.cellSize, 1.0e-4f);
+    const float inv = 1.0f / safe;
+    const int cx = int(floorf(pp.x * inv));
+    const int cy = int(floorf(pp.y * inv));
+    const int cz = int(floorf(pp.z * inv));
+    const uint32_t key = cellKey(cx, cy, cz);
+    s.entries[i] = make_int4(cx, cy, cz, int(key));
+    s.keysA[i] = key;
+}
+
+// ------------------------------------------------------------------------------------------
+// Cell table + cell-order gathers (one thread per sorted slot).
+// physics_particle_mark_cell_range_starts.cs.hlsl, physics_particle_build_cell_ranges.cs.hlsl
+// (the reference compacts runs into a sorted table searched by binary search; the same
+// (key -> run) mapping is stored here as an open-addressing hash map), plus the fluid
+// boundary candidate query (physics_particle_count/emit_fluid_boundary_candidates.cs.hlsl).
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t fluidBoundaryMaskFor(const Scene &s, uint32_t p, f3 pos,
+                                                         unsigned long long &mask)
+{
+    mask = 0ull;
+    const float pr = mx(s.radii[p], 0.0f);
+    const cn_fluid_material &fm = s.fluidMaterials[s.fluidMatIdx[p]];
+    const float support = mx(fm.smoothing_radius, pr);
+    const float reuse = mx(mx(fm.cfl_radius, pr), support);
+    const float qr = support + reuse;
+    const f3 qmin = pos - f3{qr, qr, qr}, qmax = pos + f3{qr, qr, qr};
+    const uint4 m = s.meta[p];
+    uint32_t overflow = 0;
+    for (uint32_t k = 0; k < s.colQueryCount; ++k) {
+        const uint32_t c = s.colQueryOrder[k];
+        if (!aabbOverlaps(qmin, qmax, xyz(s.colAabbMin[c]), xyz(s.colAabbMax[c]))) continue;
+        const cn_collider_broadphase bp = s.colBp[c];
+        const uint32_t bt = s.bodyType[bp.owner_body];
+        if (bp.enabled_flag != 0u && bp.environment_index == m.x && bt != CN_BODY_DYNAMIC &&
+            (m.w & bp.collision_layer) != 0u && (bp.collision_mask & m.z) != 0u) {
+            if (k < kMaxBoundaryColliders) mask |= 1ull << k;
+            else overflow = 1;
+        }
+    }
+    return overflow;
+}
+
+__global__ void __launch_bounds__(kThreads) k_cellSetup(Scene s)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= s.N) return;
+    const uint32_t p = s.valsA[slot];
+    const uint32_t key = s.keysA[slot];
+    s.rank[p] = slot;
+    const int4 e = s.entries[p];
+    s.sCell[slot] = e;
+    if (s.hasFluid) {
+        const uint32_t kind = s.kinds[p];
+        const bool fluid = kind == CN_PARTICLE_FLUID;
+        s.sMeta[slot] = s.meta[p];
+        s.sInfo[slot] = (fluid ? kFluidBit : 0u) | (s.fluidMatIdx[p] & 0x7fffffffu);
+        unsigned long long mask = 0ull;
+        if (fluid && s.colQueryCount > 0) {
+            if (fluidBoundaryMaskFor(s, p, xyz(s.x[p]), mask)) atomicAdd(&s.meta_->boundaryMaskOverflow, 1u);
+        }
+        s.sBoundary[slot] = mask;
+    }
+    if (slot != 0 && s.keysA[slot - 1] == key) return;
+    uint32_t end = slot + 1;
+    uint32_t mixed = 0;
+    while (end < s.N && s.keysA[end] == key) {
+        const int4 o = s.entries[s.valsA[end]];
+        if (o.x != e.x || o.y != e.y || o.z != e.z) mixed = 1;
+        ++end;
+    }
+    s.cellEnd[slot] = end | (mixed << 31);
+    if (key == kInvalid) return; // a run keyed 0xffffffff is never found by the reference lookup
+    uint32_t h = mixKey(key) & s.tableMask;
+    for (uint32_t probe = 0; probe <= s.tableMask; ++probe) {
+        const uint32_t prev = atomicCAS(&s.tableKeys[h], kInvalid, key);
+        if (prev == kInvalid || prev == key) {
+            s.tableStart[h] = slot;
+            return;
+        }
+        h = (h + 1) & s.tableMask;
+    }
+}
+
+// Returns the run [start, end) of cell key `key`, or false (FindCellRange semantics).
+__device__ __forceinline__ bool findRun(const Scene &s, uint32_t key, uint32_t &start, uint32_t &end,
+                                        bool &mixed)
+{
+    if (key == kInvalid) return false;
+    uint32_t h = mixKey(key) & s.tableMask;
+    for (uint32_t probe = 0; probe <= s.tableMask; ++probe) {
+        const uint32_t k = __ldg(&s.tableKeys[h]);
+        if (k == key) {
+            start = __ldg(&s.tableStart[h]);
+            const uint32_t ce = __ldg(&s.cellEnd[start]);
+            end = ce & 0x7fffffffu;
+            mixed = (ce >> 31) != 0u;
+            return true;
+        }
+        if (k == kInvalid) return false;
+        h = (h + 1) & s.tableMask;
+    }
+    return false;
+}
+
+// ------------------------------------------------------------------------------------------
+// Particle-rigid candidate pairs (solid particles vs static/kinematic bodies, dedup 16)
+// physics_particle_count_particle_rigid_candidates.cs.hlsl:113-151, emit, finalize.
+// ------------------------------------------------------------------------------------------
+template <bool kEmit>
+__global__ void __launch_bounds__(kThreads) k_rigidCandidates(Scene s, const uint32_t *total)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (kEmit && blockIdx.x == 0 && threadIdx.x == 0) {
+        s.meta_->requiredRigidPairs = *total;
+        s.meta_->rigidPairCount = min(*total, s.rigidPairCapacity);
+    }
+    if (i >= s.N) return;
+    if (kEmit && s.candCount[i] == 0u) return;
+    const f3 p = xyz(s.x[i]);
+    const float r = s.radii[i];
+    const f3 qmin = p - f3{r, r, r}, qmax = p + f3{r, r, r};
+    const uint4 m = s.meta[i];
+    const uint32_t kind = s.kinds[i];
+    const bool proxyOwner = s.ownerTypes[i] == CN_OWNER_RIGID_BODY;
+    const uint32_t owner = s.ownerIdx[i];
+    uint32_t seen[kRigidDedup];
+    uint32_t seenCount = 0, count = 0;
+    uint32_t write = kEmit ? s.candOffset[i] : 0u;
+    for (uint32_t k = 0; k < s.colQueryCount; ++k) {
+        const uint32_t c = s.colQueryOrder[k];
+        if (!aabbOverlaps(qmin, qmax, xyz(s.colAabbMin[c]), xyz(s.colAabbMax[c]))) continue;
+        const cn_collider_broadphase bp = s.colBp[c];
+        const uint32_t b = bp.owner_body;
+        if (proxyOwner && b == owner) continue;
+        const uint32_t bt = s.bodyType[b];
+        if (!(bp.enabled_flag != 0u && bp.environment_index == m.x && (m.w & bp.collision_layer) != 0u &&
+              (bp.collision_mask & m.z) != 0u && (kind == CN_PARTICLE_SOLID || bt == CN_BODY_DYNAMIC) &&
+              s.bodyColRanges[b].y > 0u))
+            continue;
+        bool fresh = true;
+        for (uint32_t q = 0; q < seenCount; ++q)
+            if (seen[q] == b) { fresh = false; break; }
+        if (!fresh) continue;
+        if (seenCount < kRigidDedup) seen[seenCount++] = b;
+        if (kEmit) {
+            if (write >= s.rigidPairCapacity) return;
+            s.rigidPairs[write++] = make_uint2(i, b);
+        } else {
+            ++count;
+        }
+    }
+    if (!kEmit) s.candCount[i] = count;
+}
+
+// ------------------------------------------------------------------------------------------
+// Particle-particle candidate pairs (cross-body / self collision)
+// physics_particle_count/emit_particle_particle_candidates.cs.hlsl,
+// physics_particle_broad_phase_query.hlsli:50-117
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool isAdjacent(const Scene &s, uint32_t p, uint32_t c)
+{
+    const uint32_t o = s.adjOff[p], n = s.adjCnt[p];
+    for (uint32_t k = 0; k < n; ++k)
+        if (s.adjIdx[o + k] == c) return true;
+    return false;
+}
+
+template <bool kEmit>
+__global__ void __launch_bounds__(kThreads) k_particleCandidates(Scene s, const uint32_t *total)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (kEmit && blockIdx.x == 0 && threadIdx.x == 0) {
+        s.meta_->requiredParticlePairs = *total;
+        s.meta_->particlePairCount = min(*total, s.particlePairCapacity);
+    }
+    if (i >= s.N) return;
+    if (kEmit && s.ppCount[i] == 0u) return;
+    const int4 e = s.entries[i];
+    const f3 pos = xyz(s.x[i]);
+    const float r = s.radii[i];
+    const uint4 m = s.meta[i];
+    const uint32_t kind = s.kinds[i];
+    uint32_t count = 0;
+    uint32_t write = kEmit ? s.ppOffset[i] : 0u;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int tx = e.x + dx, ty = e.y + dy, tz = e.z + dz;
+                uint32_t start, end;
+                bool mixed;
+                if (!findRun(s, cellKey(tx, ty, tz), start, end, mixed)) continue;
+                if (!mixed) {
+                    const int4 ce = s.sCell[start];
+                    if (ce.x != tx || ce.y != ty || ce.z != tz) continue;
+                }
+                for (uint32_t slot = start; slot < end; ++slot) {
+                    if (mixed) {
+                        const int4 ce = s.sCell[slot];
+                        if (ce.x != tx || ce.y != ty || ce.z != tz) continue;
+                    }
+                    const uint32_t c = s.valsA[slot];
+                    if (c <= i) continue;
+                    const uint4 om = s.meta[c];
+                    if (om.x != m.x) continue;
+                    if ((m.w & om.z) == 0u || (om.w & m.z) == 0u) continue;
+                    const uint32_t ok = s.kinds[c];
+                    if (kind == CN_PARTICLE_FLUID && ok == CN_PARTICLE_FLUID) continue;
+                    if (kind == CN_PARTICLE_SOLID && ok == CN_PARTICLE_SOLID &&
+                        (m.y & CN_PHASE_GROUP_MASK) == (om.y & CN_PHASE_GROUP_MASK)) {
+                        const bool a = (m.y & CN_PHASE_SELF_COLLIDE) != 0u;
+                        const bool b = (om.y & CN_PHASE_SELF_COLLIDE) != 0u;
+                        if (!a || !b || isAdjacent(s, i, c)) continue;
+                    }
+                    const f3 op = xyz(s.x[c]);
+                    const float cr = r + s.radii[c];
+                    const f3 d = op - pos;
+                    if (!(dot(d, d) <= cr * cr)) continue;
+                    if (kEmit) {
+                        if (write >= s.particlePairCapacity) return;
+                        s.particlePairs[write++] = make_uint2(i, c);
+                    } else {
+                        ++count;
+                    }
+                }
+            }
+    if (!kEmit) s.ppCount[i] = count;
+}
+
+// ------------------------------------------------------------------------------------------
+// Fluid solve (cell order).
+// ------------------------------------------------------------------------------------------
+// Position of this fluid iteration: x + accumulated delta (iteration > 0), in sorted slots.
+__global__ void __launch_bounds__(kThreads) k_fluidGather(Scene s, float4 *Xs, const float4 *Dcur,
+                                                          uint32_t iter)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= s.N) return;
+    const float4 xp = s.x[s.valsA[slot]];
+    const f3 d = iter > 0 ? xyz(Dcur[slot]) : f3{0.f, 0.f, 0.f};
+    Xs[slot] = xp;
+    s.P[slot] = mk4(xyz(xp) + d, xp.w);
+}
+
+// physics_fluid_boundary_common.hlsli:11-83
+__device__ bool fluidBoundaryContactInfo(const Scene &s, uint32_t c, f3 pos, float &sd, f3 &n)
+{
+    sd = 0.0f;
+    n = f3{0.f, 1.f, 0.f};
+    const cn_collider_broadphase bp = s.colBp[c];
+    if (bp.enabled_flag == 0u) return false;
+    const uint32_t b = bp.owner_body;
+    const f3 bpos = xyz(s.predBodyPos[b]);
+    const float4 bq = qNormalize(s.predBodyRot[b]);
+    const float4 sc = s.bodyScale[b];
+    const cn_collider_geometry cg = s.colGeo[c];
+    const f3 cwp = bpos + qRotate(bq, f3{cg.local_position[0], cg.local_position[1], cg.local_position[2]});
+    const float4 cwq = qNormalize(qMul(bq, qNormalize(make_float4(cg.local_orientation[0], cg.local_orientation[1],
+                                                                  cg.local_orientation[2], cg.local_orientation[3]))));
+    const float4 sp = make_float4(cg.shape_params[0], cg.shape_params[1], cg.shape_params[2], cg.shape_params[3]);
+    if (bp.shape_type == CN_COLLIDER_SPHERE) {
+        const f3 d = pos - cwp;
+        const float dist = length(d);
+        const float r = sphereRadius(sp, sc);
+        n = dist > kEps ? (d / dist) : f3{0.f, 1.f, 0.f};
+        sd = dist - r;
+    } else if (bp.shape_type == CN_COLLIDER_BOX) {
+        const f3 he = boxHalfExtents(sp, sc);
+        const f3 lp = qInvRotate(cwq, pos - cwp);
+        const f3 cl = clamp3(lp, -he, he);
+        const f3 d = lp - cl;
+        const float dl = length(d);
+        if (dl > kEps) {
+            n = qRotate(cwq, d / dl);
+            sd = dl;
+        } else {
+            const f3 ds = he - fabs3(lp);
+            n = qRotate(cwq, closestFaceNormalLocal(lp, he));
+            sd = -mn(ds.x, mn(ds.y, ds.z));
+        }
+    } else {
+        f3 a, b2;
+        float cr = 0.0f;
+        capsuleSegment(cwp, cwq, sp, sc, a, b2, cr);
+        const f3 seg = b2 - a;
+        const float l2 = dot(seg, seg);
+        float t = 0.0f;
+        if (l2 > kEps) t = saturate(dot(pos - a, seg) / l2);
+        const f3 cl = lerp3(a, b2, t);
+        const f3 d = pos - cl;
+        const float dist = length(d);
+        n = dist > kEps ? (d / dist) : f3{0.f, 1.f, 0.f};
+        sd = dist - cr;
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool fluidGhostDelta(const Scene &s, uint32_t c, f3 pos, float h, f3 &ghost)
+{
+    ghost = f3{0.f, 0.f, 0.f};
+    float sd = 0.0f;
+    f3 n{0.f, 1.f, 0.f};
+    if (!fluidBoundaryContactInfo(s, c, pos, sd, n)) return false;
+    if (sd < 0.0f || sd >= h) return false;
+    ghost = n * (2.0f * sd);
+    return true;
+}
+
+// Neighbour list + density constraint.
+// physics_fluid_build_neighbors.cs.hlsl:21-147 fused with
+// physics_fluid_compute_density_lambda.cs.hlsl:26-115.  The density sum runs over the list in
+// list order with the same distance values, so it equals the reference's second pass.
+__global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Config cfg, bool density)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= s.N) return;
+    const uint32_t info = s.sInfo[slot];
+    if ((info & kFluidBit) == 0u) {
+        if (density) s.Cs[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const float4 self = s.P[slot];
+    if (self.w <= kEps) {
+        if (density) s.Cs[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+        s.nbrCount[slot] = 0u;
+        return;
+    }
+    const uint32_t maxN = s.maxNbr;
+    if (maxN == 0u) {
+        s.nbrCount[slot] = 0u;
+        if (!density) return;
+    }
+    const cn_fluid_material &fm = s.fluidMaterials[info & 0x7fffffffu];
+    const float h = mx(fm.smoothing_radius, 1.0e-4f);
+    const float st = mx(fm.surface_tension, 0.0f);
+    const f3 sp = xyz(self);
+    const uint4 m = s.sMeta[slot];
+    const int4 e = s.sCell[slot];
+    uint32_t *out = s.nbr + size_t(slot) * maxN;
+    uint32_t count = 0, truncated = 0;
+    float rho = 0.0f;
+    f3 normal{0.f, 0.f, 0.f};
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int tx = e.x + dx, ty = e.y + dy, tz = e.z + dz;
+                uint32_t start, end;
+                bool mixed;
+                if (!findRun(s, cellKey(tx, ty, tz), start, end, mixed)) continue;
+                if (!mixed) {
+                    const int4 ce = __ldg(&s.sCell[start]);
+                    if (ce.x != tx || ce.y != ty || ce.z != tz) continue;
+                }
+                for (uint32_t c = start; c < end; ++c) {
+                    if (mixed) {
+                        const int4 ce = __ldg(&s.sCell[c]);
+                        if (ce.x != tx || ce.y != ty || ce.z != tz) continue;
+                    }
+                    // ShouldProcessFluidNeighbor (physics_fluid_neighbor_build.hlsli:48-69)
+                    if (c == slot) continue;
+                    if ((__ldg(&s.sInfo[c]) & kFluidBit) == 0u) continue;
+                    const uint4 om = __ldg(&s.sMeta[c]);
+                    if (om.x != m.x) continue;
+                    if (!((m.w & om.z) != 0u && (om.w & m.z) != 0u)) continue;
+                    const float4 np = ld4(&s.P[c]);
+                    if (np.w <= kEps) continue;
+                    const f3 delta = sp - xyz(np);
+                    const float dist = length(delta);
+                    if (dist >= h) continue;
+                    if (count >= maxN) { truncated = 1; continue; }
+                    out[count++] = c;
+                    if (density) {
+                        rho += spikyW(dist, h);
+                        if (st > kEps) normal += spikyGrad(delta, dist, h);
+                    }
+                }
+            }
+    s.nbrCount[slot] = count;
+    if (truncated) atomicAdd(&s.meta_->neighborTruncations, 1u);
+    if (!density) return;
+    unsigned long long bm = s.sBoundary[slot];
+    while (bm) {
+        const uint32_t k = __ffsll(bm) - 1;
+        bm &= bm - 1ull;
+        f3 ghost;
+        if (!fluidGhostDelta(s, s.colQueryOrder[k], sp, h, ghost)) continue;
+        const float dist = length(ghost);
+        if (dist >= h) continue;
+        rho += spikyW(dist, h) * cfg.fluidBoundaryDensityScale;
+    }
+    const float rho0 = mx(fm.rest_density, 1.0f);
+    const float C = mx(rho - rho0, -rho0 * mx(cfg.fluidMaxUnderDensityRatio, 0.0f)) * fm.density_constraint_scale;
+    if (st > kEps) {
+        normal = normal * st;
+        s.Cs[slot] = mk4(normal, C);
+    } else {
+        s.Cs[slot] = make_float4(0.f, 0.f, 0.f, C);
+    }
+}
+
+// Position delta, apply and boundary clamp.
+// physics_fluid_compute_delta_positions.cs.hlsl:27-157, physics_fluid_apply_delta_positions.cs.hlsl:11-31,
+// physics_fluid_clamp_boundary.cs.hlsl:23-80.  Reads the accumulated delta of iteration k (Dcur)
+// and writes that of iteration k+1 (Dnext), so the neighbours' deltas stay those of iteration k.
+__global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Config cfg, const float4 *Xs,
+                                                                   const float4 *Dcur, float4 *Dnext,
+                                                                   uint32_t iter, float dt, bool writeDx)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= s.N) return;
+    const uint32_t info = s.sInfo[slot];
+    if ((info & kFluidBit) == 0u) {
+        if (writeDx) s.Dx[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const float4 self = s.P[slot];
+    const f3 sdl = iter > 0 ? xyz(Dcur[slot]) : f3{0.f, 0.f, 0.f};
+    const cn_fluid_material &fm = s.fluidMaterials[info & 0x7fffffffu];
+    const uint32_t myMat = info & 0x7fffffffu;
+    f3 packed{0.f, 0.f, 0.f};
+    float weight = 0.0f;
+    if (self.w > kEps) {
+        const f3 sp = xyz(self);
+        const float4 snc = s.Cs[slot];
+        const float sC = snc.w;
+        const float h = mx(fm.smoothing_radius, 1.0e-4f);
+        const float cohesion = dt * mx(fm.cohesion, 0.0f);
+        const float visc = dt * mx(fm.viscosity, 0.0f);
+        const float st = mx(fm.surface_tension, 0.0f);
+        const float cfl = mx(fm.cfl_radius, 0.0f);
+        const f3 sn = st > kEps ? xyz(snc) : f3{0.f, 0.f, 0.f};
+        f3 dp{0.f, 0.f, 0.f};
+        const uint32_t cnt = s.nbrCount[slot];
+        const uint32_t *lst = s.nbr + size_t(slot) * s.maxNbr;
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t c = lst[k];
+            const float4 np = ld4(&s.P[c]);
+            if (np.w <= kEps) continue;
+            const f3 nd = iter > 0 ? xyz(ld4(&Dcur[c])) : f3{0.f, 0.f, 0.f};
+            const f3 delta = sp - xyz(np);
+            const float dist = length(delta);
+            if (dist >= h || dist <= kEps) continue;
+            const float4 nnc = ld4(&s.Cs[c]);
+            const f3 nij = delta / dist;
+            const float dw = spikyDW(dist, h);
+            f3 pd = -0.5f * (sC + nnc.w) * dw * nij;
+            if ((__ldg(&s.sInfo[c]) & 0x7fffffffu) == myMat) {
+                const f3 rel = sdl - nd;
+                if (cohesion > kEps) pd -= nij * (cohesion * cohesionW(dist, h, fm.cohesion1, fm.cohesion2));
+                if (visc > kEps) {
+                    const float vs = 1.0f - (1.0f / (1.0f + visc * spikyW(dist, h)));
+                    pd -= vs * rel;
+                }
+                if (cfl > kEps) {
+                    const float proj = dot(rel, nij);
+                    if (proj < -cfl) pd -= nij * (proj + cfl) * 0.5f;
+                }
+                if (st > kEps) pd -= dt * (sn - xyz(nnc));
+            }
+            dp += pd;
+            weight += 1.0f;
+        }
+        f3 bd{0.f, 0.f, 0.f};
+        unsigned long long bm = s.sBoundary[slot];
+        while (bm) {
+            const uint32_t k = __ffsll(bm) - 1;
+            bm &= bm - 1ull;
+            f3 ghost;
+            if (!fluidGhostDelta(s, s.colQueryOrder[k], sp, h, ghost)) continue;
+            const float dist = length(ghost);
+            if (dist <= kEps || dist >= h) continue;
+            const f3 nij = ghost / dist;
+            const float dw = spikyDW(dist, h);
+            bd += -mx(sC, 0.0f) * dw * nij;
+        }
+        bd = bd * cfg.fluidBoundaryDeltaScale;
+        packed = dp * cfg.fluidSolveCoefficient + bd;
+    }
+    if (writeDx) s.Dx[slot] = mk4(packed, weight);
+    // apply (physics_fluid_apply_delta_positions.cs.hlsl:21-30)
+    const float w = mx(weight * cfg.fluidRelaxation, 1.0f);
+    const f3 d = packed / w;
+    const f3 acc = sdl + d;
+    // clamp (physics_fluid_clamp_boundary.cs.hlsl:36-79)
+    const f3 base = xyz(Xs[slot]);
+    f3 cur = base + acc;
+    unsigned long long bm0 = s.sBoundary[slot];
+    if (bm0) {
+        const uint32_t p = s.valsA[slot];
+        const float pr = mx(s.radii[p], 0.0f);
+        for (uint32_t sweep = 0; sweep < 2u; ++sweep) {
+            bool changed = false;
+            unsigned long long bm = bm0;
+            while (bm) {
+                const uint32_t k = __ffsll(bm) - 1;
+                bm &= bm - 1ull;
+                float sd = 0.0f;
+                f3 n{0.f, 1.f, 0.f};
+                if (!fluidBoundaryContactInfo(s, s.colQueryOrder[k], cur, sd, n)) continue;
+                if (sd >= pr) continue;
+                cur += n * (pr - sd);
+                changed = true;
+            }
+            if (!changed) break;
+        }
+    }
+    Dnext[slot] = mk4(cur - base, 0.0f);
+}
+
+// ------------------------------------------------------------------------------------------
+// XPBD families: Jacobi solve writes per-constraint records, apply gathers them per particle in
+// ascending constraint order (the reference's incidence order).
+// ------------------------------------------------------------------------------------------
+// physics_soft_solve_edge_constraints.cs.hlsl:10-74
+__global__ void __launch_bounds__(kThreads) k_solveEdges(Scene s, float dt, float relax)
+{
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= s.E) return;
+    const cn_soft_edge ed = s.edges[e];
+    float4 cA = make_float4(0.f, 0.f, 0.f, 0.f), cB = cA;
+    if (ed.enabled != 0u) {
+        const float4 a = s.x[ed.particle_a], b = s.x[ed.particle_b];
+        const float wA = a.w, wB = b.w, wSum = wA + wB;
+        const f3 delta = xyz(b) - xyz(a);
+        const float l2 = dot(delta, delta);
+        if (wSum > kEps && l2 > kEps) {
+            const float len = sqrtf(l2);
+            const f3 gA = -delta / len;
+            const f3 gB = -gA;
+            const float alpha = mx(ed.compliance, 0.0f) / mx(dt * dt, kEps);
+            const float Cv = len - ed.rest_length;
+            const float lambda = s.edgeLambda[e];
+            const float den = wSum + alpha;
+            if (den > kEps) {
+                const float dl = -(Cv + alpha * lambda) / den;
+                s.edgeLambda[e] = lambda + dl;
+                cA = mk4(wA * dl * gA * relax, 0.0f);
+                cB = mk4(wB * dl * gB * relax, 0.0f);
+            }
+        }
+    }
+    s.edgeCorr[2 * e] = cA;
+    s.edgeCorr[2 * e + 1] = cB;
+}
+
+// physics_soft_apply_edge_corrections.cs.hlsl:9-35 (also the strand distance apply:
+// physics_strand_apply_distance_corrections.cs.hlsl:9-38)
+__global__ void __launch_bounds__(kThreads) k_applyPair(Scene s, const uint2 *ranges, const uint2 *inc,
+                                                        const float4 *corr)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.N) return;
+    const float4 p = s.x[i];
+    if (p.w <= kEps) return;
+    const uint2 r = ranges[i];
+    f3 total{0.f, 0.f, 0.f};
+    for (uint32_t k = 0; k < r.y; ++k) {
+        const uint2 ref = inc[r.x + k];
+        total += xyz(corr[2 * ref.x + (ref.y == 0u ? 0u : 1u)]);
+    }
+    s.x[i] = mk4(xyz(p) + total, p.w);
+}
+
+// physics_soft_apply_tet_corrections.cs.hlsl:9-50, physics_soft_apply_bend_corrections.cs.hlsl:9-51
+__global__ void __launch_bounds__(kThreads) k_applyQuad(Scene s, const uint2 *ranges, const uint2 *inc,
+                                                        const float4 *corr)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.N) return;
+    const float4 p = s.x[i];
+    if (p.w <= kEps) return;
+    const uint2 r = ranges[i];
+    f3 total{0.f, 0.f, 0.f};
+    for (uint32_t k = 0; k < r.y; ++k) {
+        const uint2 ref = inc[r.x + k];
+        total += xyz(corr[4 * ref.x + (ref.y > 3u ? 3u : ref.y)]);
+    }
+    s.x[i] = mk4(xyz(p) + total, p.w);
+}
+
+// physics_soft_solve_tet_constraints.cs.hlsl:15-87
+__global__ void __launch_bounds__(kThreads) k_solveTets(Scene s, float dt, float relax)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= s.T) return;
+    const cn_soft_tet tet = s.tets[t];
+    const float4 q0 = s.x[tet.particle_indices[0]], q1 = s.x[tet.particle_indices[1]];
+    const float4 q2 = s.x[tet.particle_indices[2]], q3 = s.x[tet.particle_indices[3]];
+    const float w0 = q0.w, w1 = q1.w, w2 = q2.w, w3 = q3.w;
+    if ((w0 + w1 + w2 + w3) <= kEps) return; // keeps the previous correction record
+    const f3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2), p3 = xyz(q3);
+    const float sv = dot(cross(p1 - p0, p2 - p0), p3 - p0) / 6.0f;
+    const float vs = (sv >= 0.0f) ? 1.0f : -1.0f;
+    const float Cv = fabsf(sv) - mx(tet.rest_volume, 0.0f);
+    const f3 g0 = cross(p3 - p1, p2 - p1) * (vs / 6.0f);
+    const f3 g1 = cross(p2 - p0, p3 - p0) * (vs / 6.0f);
+    const f3 g2 = cross(p3 - p0, p1 - p0) * (vs / 6.0f);
+    const f3 g3 = cross(p1 - p0, p2 - p0) * (vs / 6.0f);
+    const float sg = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
+    const float alpha = mx(tet.compliance, 0.0f) / mx(dt * dt, kEps);
+    const float lambda = s.tetLambda[t];
+    const float den = sg + alpha;
+    if (den <= kEps) return;
+    const float dl = -(Cv + alpha * lambda) / den;
+    s.tetLambda[t] = lambda + dl;
+    float4 *out = s.tetCorr + 4 * size_t(t);
+    out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
+    out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
+    out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
+    out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
+}
+
+// physics_soft_solve_bend_constraints.cs.hlsl:20-86
+__global__ void __launch_bounds__(kThreads) k_solveBends(Scene s, float dt, float relax)
+{
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.Bn) return;
+    const cn_soft_bend bd = s.bends[b];
+    float4 *out = s.bendCorr + 4 * size_t(b);
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 o0 = z, o1 = z, o2 = z;
+    const float4 q0 = s.x[bd.particle0], q1 = s.x[bd.particle1], q2 = s.x[bd.particle2];
+    const float w0 = q0.w, w1 = q1.w, w2 = q2.w;
+    const f3 e0 = xyz(q0) - xyz(q1), e1 = xyz(q2) - xyz(q1);
+    const float l0s = dot(e0, e0), l1s = dot(e1, e1);
+    if (w0 + w1 + w2 > kEps && l0s > kEps && l1s > kEps) {
+        const float l0 = sqrtf(l0s), l1 = sqrtf(l1s);
+        const f3 d0 = e0 / l0, d1 = e1 / l1;
+        const float ct = mn(mx(dot(d0, d1), -1.0f + 1.0e-4f), 1.0f - 1.0e-4f);
+        const float st2 = mx(1.0f - ct * ct, 1.0e-8f);
+        const float st = sqrtf(st2);
+        const float theta = acosf(ct);
+        const f3 g0 = -(d1 - ct * d0) / mx(l0 * st, kEps);
+        const f3 g2 = -(d0 - ct * d1) / mx(l1 * st, kEps);
+        const f3 g1 = -(g0 + g2);
+        const float den = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2);
+        const float alpha = mx(bd.compliance, 0.0f) / mx(dt * dt, kEps);
+        if (den + alpha > kEps) {
+            const float Cv = theta - bd.rest_angle;
+            const float lambda = s.bendLambda[b];
+            const float dl = -(Cv + alpha * lambda) / (den + alpha);
+            s.bendLambda[b] = lambda + dl;
+            o0 = mk4(w0 * dl * g0 * relax, 0.0f);
+            o1 = mk4(w1 * dl * g1 * relax, 0.0f);
+            o2 = mk4(w2 * dl * g2 * relax, 0.0f);
+        }
+    }
+    out[0] = o0; out[1] = o1; out[2] = o2; out[3] = z;
+}
+
+// physics_cloth_solve_dihedral_constraints.cs.hlsl:20-95
+__global__ void __launch_bounds__(kThreads) k_solveDihedrals(Scene s, float dt, float relax)
+{
+    const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d >= s.D) return;
+    const uint32_t ci = s.Bn + d;
+    const cn_cloth_dihedral h = s.dihedrals[d];
+    float4 *out = s.bendCorr + 4 * size_t(ci);
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 e0m = s.x[h.edge_particle0], e1m = s.x[h.edge_particle1];
+    const float4 o0m = s.x[h.opposite_particle0], o1m = s.x[h.opposite_particle1];
+    const f3 p0 = xyz(o0m), p1 = xyz(o1m), p2 = xyz(e0m), p3 = xyz(e1m);
+    const f3 edge = p3 - p2;
+    const float el2 = dot(edge, edge);
+    const f3 rn0 = cross(p2 - p0, p3 - p0);
+    const f3 rn1 = cross(p3 - p1, p2 - p1);
+    const float n0s = dot(rn0, rn0), n1s = dot(rn1, rn1);
+    if (el2 <= kEps || n0s <= kEps || n1s <= kEps) {
+        out[0] = z; out[1] = z; out[2] = z; out[3] = z;
+        return;
+    }
+    const float el = sqrtf(el2);
+    const float iel = 1.0f / el;
+    const f3 sn0 = rn0 / n0s, sn1 = rn1 / n1s;
+    const f3 dO0 = el * sn0, dO1 = el * sn1;
+    const f3 dE0 = dot(p0 - p3, edge) * iel * sn0 + dot(p1 - p3, edge) * iel * sn1;
+    const f3 dE1 = dot(p2 - p0, edge) * iel * sn0 + dot(p2 - p1, edge) * iel * sn1;
+    const f3 g0 = -dE0, g1 = -dE1, g2 = -dO0, g3 = -dO1;
+    const f3 n0 = rn0 / sqrtf(n0s), n1 = rn1 / sqrtf(n1s);
+    const float theta = atan2f(dot(edge * iel, cross(n0, n1)), mn(mx(dot(n0, n1), -1.0f), 1.0f));
+    const float twoPi = 6.283185307179586f;
+    float Cv = theta - h.rest_angle;
+    Cv = Cv - twoPi * floorf((Cv + 3.141592653589793f) / twoPi);
+    const float w0 = e0m.w, w1 = e1m.w, w2 = o0m.w, w3 = o1m.w;
+    const float den = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
+    const float alpha = mx(h.compliance, 0.0f) / mx(dt * dt, kEps);
+    if (den + alpha <= kEps) {
+        out[0] = z; out[1] = z; out[2] = z; out[3] = z;
+        return;
+    }
+    const float lambda = s.bendLambda[ci];
+    const float dl = -(Cv + alpha * lambda) / (den + alpha);
+    s.bendLambda[ci] = lambda + dl;
+    out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
+    out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
+    out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
+    out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
+}
+
+// 3x3 helpers of physics_strand_solve_{segment,joint}_constraints.cs.hlsl:12-64
+struct m3 { float m[3][3]; };
+__device__ __forceinline__ void addOuter(m3 &acc, float sc, f3 a, f3 b)
+{
+    const float o[3][3] = {{a.x * b.x, a.x * b.y, a.x * b.z}, {a.y * b.x, a.y * b.y, a.y * b.z},
+                           {a.z * b.x, a.z * b.y, a.z * b.z}};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc.m[r][c] = acc.m[r][c] + sc * o[r][c];
+}
+__device__ __forceinline__ f3 solve3(const m3 &M, f3 v)
+{
+    const float a00 = M.m[0][0], a01 = M.m[0][1], a02 = M.m[0][2];
+    const float a10 = M.m[1][0], a11 = M.m[1][1], a12 = M.m[1][2];
+    const float a20 = M.m[2][0], a21 = M.m[2][1], a22 = M.m[2][2];
+    const float c00 = a11 * a22 - a12 * a21, c01 = a02 * a21 - a01 * a22, c02 = a01 * a12 - a02 * a11;
+    const float c10 = a12 * a20 - a10 * a22, c11 = a00 * a22 - a02 * a20, c12 = a02 * a10 - a00 * a12;
+    const float c20 = a10 * a21 - a11 * a20, c21 = a01 * a20 - a00 * a21, c22 = a00 * a11 - a01 * a10;
+    const float det = a00 * c00 + a01 * c10 + a02 * c20;
+    if (fabsf(det) <= kEps) return f3{0.f, 0.f, 0.f} * v.x + f3{0.f, 0.f, 0.f}; // zero inverse
+    const float id = 1.0f / det;
+    const f3 r0{c00 * id, c01 * id, c02 * id}, r1{c10 * id, c11 * id, c12 * id}, r2{c20 * id, c21 * id, c22 * id};
+    return f3{dot(r0, v), dot(r1, v), dot(r2, v)};
+}
+__device__ __forceinline__ float strandOrientationInvMass(float wA, float wB, float rl)
+{
+    const float ws = mx(wA + wB, 0.0f);
+    if (ws <= kEps || rl <= kEps) return 0.0f;
+    const float avg = ws * 0.5f;
+    return 12.0f * avg / mx(rl * rl, kEps);
+}
+
+// physics_strand_solve_segment_constraints.cs.hlsl:66-147
+__global__ void __launch_bounds__(kThreads) k_solveSegments(Scene s, float dt, float relax)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= s.S) return;
+    const cn_strand_segment sg = s.segs[g];
+    const float4 a = s.x[sg.particle_a], b = s.x[sg.particle_b];
+    const float wA = a.w, wB = b.w, wSum = wA + wB;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 o0 = z, o1 = z, o2 = z;
+    const f3 delta = xyz(b) - xyz(a);
+    if (wSum > kEps && dot(delta, delta) > kEps) {
+        const float4 q = qNormalize(s.segOrient[g]);
+        const f3 axis = qRotate(q, f3{1.f, 0.f, 0.f});
+        const float irl = 1.0f / mx(sg.rest_length, kEps);
+        const float oim = strandOrientationInvMass(wA, wB, sg.rest_length);
+        const f3 Cv = delta * irl - axis;
+        const float alpha = mx(sg.stretch_shear_compliance, 0.0f) / mx(dt * dt, kEps);
+        const f3 lambda = xyz(s.segLambda[g]);
+        const f3 qv = xyz(q);
+        const float qw = q.w;
+        const f3 gQw = 2.0f * f3{qw, qv.z, -qv.y};
+        const f3 gQx = 2.0f * f3{0.0f, qv.y, qv.z};
+        const f3 gQy = 2.0f * f3{-qv.y, 0.0f, -qw};
+        const f3 gQz = 2.0f * f3{-qv.z, qw, 0.0f};
+        const float dg = wSum * irl * irl + alpha;
+        m3 sys{{{dg, 0.f, 0.f}, {0.f, dg, 0.f}, {0.f, 0.f, dg}}};
+        addOuter(sys, oim, gQx, gQx);
+        addOuter(sys, oim, gQy, gQy);
+        addOuter(sys, oim, gQz, gQz);
+        addOuter(sys, oim, gQw, gQw);
+        const f3 rhs = -(Cv + alpha * lambda);
+        const f3 dl = solve3(sys, rhs);
+        if (dot(dl, dl) > 0.0f) {
+            s.segLambda[g] = mk4(lambda + dl, 0.0f);
+            o0 = mk4(-wA * irl * dl * relax, 0.0f);
+            o1 = mk4(wB * irl * dl * relax, 0.0f);
+            o2 = scale4(make_float4(-dot(gQx, dl), -dot(gQy, dl), -dot(gQz, dl), -dot(gQw, dl)), oim * relax);
+        }
+    }
+    float4 *out = s.segCorr + 3 * size_t(g);
+    out[0] = o0; out[1] = o1; out[2] = o2;
+}
+
+// physics_strand_apply_segment_corrections.cs.hlsl:11-43
+__global__ void __launch_bounds__(kThreads) k_applySegments(Scene s)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < s.N) {
+        const float4 p = s.x[i];
+        if (p.w > kEps) {
+            const uint2 r = s.segRanges[i];
+            f3 total{0.f, 0.f, 0.f};
+            for (uint32_t k = 0; k < r.y; ++k) {
+                const uint2 ref = s.segInc[r.x + k];
+                total += xyz(s.segCorr[3 * ref.x + (ref.y == 0u ? 0u : 1u)]);
+            }
+            s.x[i] = mk4(xyz(p) + total, p.w);
+        }
+    }
+    if (i < s.S) s.segOrient[i] = qNormalize(add4(s.segOrient[i], s.segCorr[3 * size_t(i) + 2]));
+}
+
+// physics_strand_solve_joint_constraints.cs.hlsl:66-154
+__global__ void __launch_bounds__(kThreads) k_solveJoints(Scene s, float dt, float relax)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= s.J) return;
+    const cn_strand_joint jt = s.joints[j];
+    const cn_strand_segment sA = s.segs[jt.segment_a], sB = s.segs[jt.segment_b];
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 tA = z, tB = z;
+    const float4 oA = qNormalize(s.segOrient[jt.segment_a]);
+    const float4 oB = qNormalize(s.segOrient[jt.segment_b]);
+    const float imA = strandOrientationInvMass(s.x[sA.particle_a].w, s.x[sA.particle_b].w, sA.rest_length);
+    const float imB = strandOrientationInvMass(s.x[sB.particle_a].w, s.x[sB.particle_b].w, sB.rest_length);
+    const float4 rel = qNormalize(qMul(qConj(oA), oB));
+    float4 rr = qNormalize(make_float4(jt.rest_relative_orientation[0], jt.rest_relative_orientation[1],
+                                       jt.rest_relative_orientation[2], jt.rest_relative_orientation[3]));
+    if (dot4(rel, rr) < 0.0f) rr = make_float4(-rr.x, -rr.y, -rr.z, -rr.w);
+    const f3 Cv = xyz(rel) - xyz(rr);
+    const float4 lambda = s.jointLambda[j];
+    const float ba = mx(jt.bend_compliance, 0.0f) / mx(dt * dt, kEps);
+    const float ta = mx(jt.twist_compliance, 0.0f) / mx(dt * dt, kEps);
+    const f3 av{ta, ba, ba};
+    m3 sys{{{av.x, 0.f, 0.f}, {0.f, av.y, 0.f}, {0.f, 0.f, av.z}}};
+    const f3 va = xyz(oA), vb = xyz(oB);
+    const float wa = oA.w, wb = oB.w;
+    const f3 gAX{-wb, vb.z, -vb.y}, gAY{-vb.z, -wb, vb.x}, gAZ{vb.y, -vb.x, -wb}, gAW = vb;
+    const f3 gBX{wa, -va.z, va.y}, gBY{va.z, wa, -va.x}, gBZ{-va.y, va.x, wa}, gBW = -va;
+    addOuter(sys, imA, gAX, gAX);
+    addOuter(sys, imA, gAY, gAY);
+    addOuter(sys, imA, gAZ, gAZ);
+    addOuter(sys, imA, gAW, gAW);
+    addOuter(sys, imB, gBX, gBX);
+    addOuter(sys, imB, gBY, gBY);
+    addOuter(sys, imB, gBZ, gBZ);
+    addOuter(sys, imB, gBW, gBW);
+    const f3 rhs = -(Cv + av * xyz(lambda));
+    const f3 dl = solve3(sys, rhs);
+    if (dot(dl, dl) > 0.0f) {
+        s.jointLambda[j] = mk4(xyz(lambda) + dl, 0.0f);
+        tA = scale4(make_float4(dot(gAX, dl), dot(gAY, dl), dot(gAZ, dl), dot(gAW, dl)), imA * relax);
+        tB = scale4(make_float4(dot(gBX, dl), dot(gBY, dl), dot(gBZ, dl), dot(gBW, dl)), imB * relax);
+    }
+    s.jointCorr[2 * size_t(j)] = tA;
+    s.jointCorr[2 * size_t(j) + 1] = tB;
+}
+
+// physics_strand_apply_joint_corrections.cs.hlsl
+__global__ void __launch_bounds__(kThreads) k_applyJoints(Scene s)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= s.S) return;
+    const uint2 r = s.segJointRanges[g];
+    float4 total = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (uint32_t k = 0; k < r.y; ++k) {
+        const uint2 ref = s.segJointInc[r.x + k];
+        total = add4(total, s.jointCorr[2 * size_t(ref.x) + (ref.y == 0u ? 0u : 1u)]);
+    }
+    s.segOrient[g] = qNormalize(add4(s.segOrient[g], total));
+}
+
+// physics_strand_solve_distance_constraints.cs.hlsl:10-59
+__global__ void __launch_bounds__(kThreads) k_solveDistances(Scene s, float dt, float relax)
+{
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= s.SD) return;
+    const cn_strand_distance dc = s.dists[c];
+    float4 cA = make_float4(0.f, 0.f, 0.f, 0.f), cB = cA;
+    const float4 a = s.x[dc.particle_a], b = s.x[dc.particle_b];
+    const float wA = a.w, wB = b.w, wSum = wA + wB;
+    const f3 delta = xyz(b) - xyz(a);
+    const float l2 = dot(delta, delta);
+    if (wSum > kEps && l2 > kEps) {
+        const float len = sqrtf(l2);
+        const f3 grad = delta / len;
+        const float alpha = mx(dc.distance_compliance, 0.0f) / mx(dt * dt, kEps);
+        const float lambda = s.distLambda[c];
+        const float Cv = len - dc.rest_length;
+        const float den = wSum + alpha;
+        if (den > kEps) {
+            const float dl = -(Cv + alpha * lambda) / den;
+            s.distLambda[c] = lambda + dl;
+            cA = mk4(wA * dl * -grad * relax, 0.0f);
+            cB = mk4(wB * dl * grad * relax, 0.0f);
+        }
+    }
+    s.distCorr[2 * c] = cA;
+    s.distCorr[2 * c + 1] = cB;
+}
+
+// ------------------------------------------------------------------------------------------
+// Contacts
+// ------------------------------------------------------------------------------------------
+// physics_particle_generate_explicit_contacts.cs.hlsl (no suturing state, no rigid proxies)
+__global__ void __launch_bounds__(kThreads) k_particleContactGenerate(Scene s)
+{
+    const uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t count = s.meta_->particlePairCount;
+    if (pi == 0) s.meta_->activeParticleContacts = 0u;
+    if (pi >= count) return;
+    ParticleContact out{};
+    const uint2 pr = s.particlePairs[pi];
+    const uint32_t a = pr.x, b = pr.y;
+    out.material = mk4(combineContactMaterial(s.contactMaterials[s.matIdx[a]], s.contactMaterials[s.matIdx[b]]), 0.0f);
+    if (!(s.kinds[a] == CN_PARTICLE_FLUID && s.kinds[b] == CN_PARTICLE_FLUID)) {
+        const f3 pa = xyz(s.x[a]), pb = xyz(s.x[b]);
+        const float cr = s.radii[a] + s.radii[b];
+        const f3 delta = pb - pa;
+        const float d2 = dot(delta, delta);
+        if (d2 <= kEps) {
+            out.a = a; out.b = b; out.active = 1u;
+            out.normalPenetration = make_float4(0.f, 1.f, 0.f, cr);
+        } else {
+            const float dist = sqrtf(d2);
+            const float pen = cr - dist;
+            if (pen > 0.0f) {
+                out.a = a; out.b = b; out.active = 1u;
+                out.normalPenetration = mk4(delta / dist, pen);
+            }
+        }
+    }
+    s.particleContacts[pi] = out;
+}
+
+// physics_particle_solve_explicit_contacts.cs.hlsl (non-proxy branch); float atomics as in the
+// reference.
+__global__ void __launch_bounds__(kThreads) k_particleContactSolve(Scene s, Config cfg)
+{
+    const uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pi >= s.meta_->particlePairCount) return;
+    const ParticleContact c = s.particleContacts[pi];
+    if (c.active == 0u) return;
+    atomicAdd(&s.meta_->activeParticleContacts, 1u);
+    const float4 A = s.x[c.a], Bp = s.x[c.b];
+    const float iA = A.w, iB = Bp.w;
+    if (iA <= kEps && iB <= kEps) return;
+    const float pen = mn(mx(c.normalPenetration.w - cfg.slop, 0.0f), cfg.softMaxCorrection);
+    if (pen <= 0.0f) return;
+    const f3 mat = xyz(c.material);
+    const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
+    const f3 relDisp = (xyz(Bp) - xyz(s.xprev[c.b])) - (xyz(A) - xyz(s.xprev[c.a]));
+    const float denom = iA + iB;
+    if (denom <= kEps) return;
+    const float lambda = (pen / denom) * cfg.softContactRelaxation;
+    f3 cA = -n * (iA * lambda);
+    f3 cB = n * (iB * lambda);
+    const f3 fd = positionFrictionDelta(projectOntoTangent(relDisp, n), pen, mat.x, mat.z,
+                                        cfg.positionFrictionMinDistance);
+    const float fdist = length(fd);
+    if (fdist > 0.0f) {
+        const f3 t = fd / fdist;
+        const float tden = iA + iB;
+        if (tden > kEps) {
+            const float tl = (fdist / tden) * cfg.softContactRelaxation;
+            cA += t * (iA * tl);
+            cB -= t * (iB * tl);
+        }
+    }
+    if (iA > kEps) {
+        atomicAdd(&s.posCorr[c.a].x, cA.x);
+        atomicAdd(&s.posCorr[c.a].y, cA.y);
+        atomicAdd(&s.posCorr[c.a].z, cA.z);
+    }
+    if (iB > kEps) {
+        atomicAdd(&s.posCorr[c.b].x, cB.x);
+        atomicAdd(&s.posCorr[c.b].y, cB.y);
+        atomicAdd(&s.posCorr[c.b].z, cB.z);
+    }
+}
+
+// Particle-rigid contact for candidate pair `pi`: physics_particle_rigid_generate_contacts.cs.hlsl:29-210
+__device__ RigidContact generateRigidContact(const Scene &s, uint32_t i, uint32_t b)
+{
+    RigidContact out{};
+    if (s.ownerTypes[i] == CN_OWNER_RIGID_BODY) return out;
+    const f3 sp = xyz(s.x[i]);
+    const float sr = s.radii[i];
+    const uint4 m = s.meta[i];
+    const f3 bpos = xyz(s.predBodyPos[b]);
+    const float4 bq = qNormalize(s.predBodyRot[b]);
+    const float4 bsc = s.bodyScale[b];
+    const uint2 cr = s.bodyColRanges[b];
+    float bestPen = 0.0f;
+    uint32_t bestCol = 0;
+    f3 bestN{0.f, 1.f, 0.f}, bestW{0.f, 0.f, 0.f};
+    for (uint32_t k = 0; k < kColliderIterationCap; ++k) {
+        if (k >= cr.y) break;
+        const uint32_t c = s.bodyColIdx[cr.x + k];
+        const cn_collider_broadphase bp = s.colBp[c];
+        if (bp.enabled_flag == 0u || bp.environment_index != m.x) continue;
+        if ((m.w & bp.collision_layer) == 0u || (bp.collision_mask & m.z) == 0u) continue;
+        const cn_collider_geometry cg = s.colGeo[c];
+        const f3 clp{cg.local_position[0], cg.local_position[1], cg.local_position[2]};
+        const float4 clq = qNormalize(make_float4(cg.local_orientation[0], cg.local_orientation[1],
+                                                  cg.local_orientation[2], cg.local_orientation[3]));
+        const f3 cwp = bpos + qRotate(bq, clp);
+        const float4 cwq = qNormalize(qMul(bq, clq));
+        const f3 pl = qInvRotate(cwq, sp - cwp);
+        f3 nl{0.f, 1.f, 0.f}, cw{0.f, 0.f, 0.f};
+        float sd = 0.0f;
+        const float4 sp4 = make_float4(cg.shape_params[0], cg.shape_params[1], cg.shape_params[2], cg.shape_params[3]);
+        if (bp.shape_type == CN_COLLIDER_SPHERE) {
+            const float r = sphereRadius(sp4, bsc);
+            const float l = sqrtf(dot(pl, pl));
+            nl = l > kEps ? (pl / l) : f3{0.f, 1.f, 0.f};
+            sd = l - r;
+            cw = cwp + qRotate(cwq, nl * r);
+        } else if (bp.shape_type == CN_COLLIDER_BOX) {
+            const f3 he = boxHalfExtents(sp4, bsc);
+            const f3 cl = clamp3(pl, -he, he);
+            const f3 d = pl - cl;
+            const float dl = sqrtf(dot(d, d));
+            if (dl > kEps) {
+                nl = d / dl;
+                sd = dl;
+                cw = cwp + qRotate(cwq, cl);
+            } else {
+                nl = closestFaceNormalLocal(pl, he);
+                const f3 ds = he - fabs3(pl);
+                sd = -mn(ds.x, mn(ds.y, ds.z));
+                f3 cs = pl;
+                if (fabsf(nl.x) > 0.5f) cs.x = nl.x * he.x;
+                else if (fabsf(nl.y) > 0.5f) cs.y = nl.y * he.y;
+                else cs.z = nl.z * he.z;
+                cw = cwp + qRotate(cwq, cs);
+            }
+        } else {
+            f3 a, b2;
+            float cap = 0.0f;
+            capsuleSegment(cwp, cwq, sp4, bsc, a, b2, cap);
+            const f3 seg = b2 - a;
+            const float l2 = dot(seg, seg);
+            float t = 0.0f;
+            if (l2 > kEps) t = saturate(dot(sp - a, seg) / l2);
+            const f3 cl = lerp3(a, b2, t);
+            const f3 d = sp - cl;
+            const float l = sqrtf(dot(d, d));
+            const f3 wn = l > kEps ? (d / l) : f3{1.f, 0.f, 0.f};
+            sd = l - cap;
+            nl = qInvRotate(cwq, wn);
+            cw = cl + wn * cap;
+        }
+        const float pen = sr - sd;
+        if (pen <= 0.0f || pen <= bestPen) continue;
+        bestPen = pen;
+        bestCol = c;
+        bestN = safeNormalize(qRotate(cwq, nl), f3{0.f, 1.f, 0.f});
+        bestW = cw;
+    }
+    if (bestPen > 0.0f) {
+        out.particle = i; out.body = b; out.collider = bestCol; out.active = 1u;
+        out.normalPenetration = mk4(bestN, bestPen);
+        out.rigidLocalPoint = mk4(qInvRotate(bq, bestW - bpos), 0.0f);
+    }
+    return out;
+}
+
+// physics_particle_rigid_solve_contacts.cs.hlsl:27-141 for one contact (static/kinematic body:
+// only the particle moves).
+__device__ f3 solveRigidContact(const Scene &s, const Config &cfg, const RigidContact &c, float4 sp)
+{
+    const uint32_t i = c.particle, b = c.body;
+    const float iS = sp.w;
+    const f3 prevS = xyz(s.xprev[i]);
+    const float4 prevB = s.prevBodyPos[b], predB = s.predBodyPos[b];
+    const float4 prevQ = qNormalize(s.prevBodyRot[b]), predQ = qNormalize(s.predBodyRot[b]);
+    const float iR = s.bodyType[b] == CN_BODY_DYNAMIC ? predB.w : 0.0f;
+    if (iS <= kEps && iR <= kEps) return f3{0.f, 0.f, 0.f};
+    const float pen = mn(mx(c.normalPenetration.w - cfg.slop, 0.0f), cfg.softMaxCorrection);
+    if (pen <= 0.0f) return f3{0.f, 0.f, 0.f};
+    const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
+    f3 inI = xyz(s.bodyInvInertia[b]);
+    const f3 mat = combineContactMaterial(s.contactMaterials[s.matIdx[i]], s.colMat[c.collider]);
+    if (iR <= kEps) inI = f3{0.f, 0.f, 0.f};
+    const f3 prevCP = xyz(prevB) + qRotate(prevQ, xyz(c.rigidLocalPoint));
+    const f3 cp = xyz(predB) + qRotate(predQ, xyz(c.rigidLocalPoint));
+    const f3 rR = cp - xyz(predB);
+    const float nmR = contactEffectiveMass(iR, inI, predQ, rR, n);
+    const float denom = iS + nmR;
+    if (denom <= kEps) return f3{0.f, 0.f, 0.f};
+    const float lambda = (pen / denom) * cfg.softContactRelaxation;
+    f3 corr = n * (iS * lambda);
+    const f3 relDisp = (cp - prevCP) - (xyz(sp) - prevS);
+    const f3 fd = positionFrictionDelta(projectOntoTangent(relDisp, n), pen, mat.x, mat.z,
+                                        cfg.positionFrictionMinDistance);
+    const float fdist = length(fd);
+    if (fdist > 0.0f) {
+        const f3 t = fd / fdist;
+        const float tmR = contactEffectiveMass(iR, inI, predQ, rR, t);
+        const float tden = iS + tmR;
+        if (tden > kEps) {
+            const float tl = fdist / tden;
+            corr += t * (tl * iS * cfg.softContactRelaxation);
+        }
+    }
+    if (iS > kEps) return corr;
+    return f3{0.f, 0.f, 0.f};
+}
+
+// Generate + solve every candidate pair of particle i (pairs are particle-major), then either
+// accumulate into posCorr (explicit contacts present) or apply directly
+// (physics_particle_apply_position_corrections.cs.hlsl:8-30).
+__global__ void __launch_bounds__(kThreads) k_rigidContacts(Scene s, Config cfg, bool applyDirect)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.N) return;
+    const uint32_t cnt = s.candCount[i];
+    const float4 sp = s.x[i];
+    f3 corr{0.f, 0.f, 0.f};
+    bool any = false;
+    if (cnt) {
+        const uint32_t off = s.candOffset[i];
+        const uint32_t lim = s.meta_->rigidPairCount;
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t pi = off + k;
+            if (pi >= lim) break;
+            const uint2 pr = s.rigidPairs[pi];
+            const RigidContact c = generateRigidContact(s, pr.x, pr.y);
+            s.rigidContacts[pi] = c;
+            if (!c.active) continue;
+            const f3 d = solveRigidContact(s, cfg, c, sp);
+            // float atomic order of the reference == pair order here
+            if (sp.w > kEps) {
+                corr = corr + d;
+                any = true;
+            }
+        }
+    }
+    if (applyDirect) {
+        // applyParticlePositionCorrections with an accumulator that only this pass wrote
+        if (sp.w <= kEps) return;
+        s.x[i] = mk4(xyz(sp) + corr, sp.w);
+    } else if (any) {
+        float4 pc = s.posCorr[i];
+        pc = mk4(xyz(pc) + corr, pc.w);
+        s.posCorr[i] = pc;
+    }
+}
+
+// physics_particle_apply_position_corrections.cs.hlsl:8-30
+__global__ void __launch_bounds__(kThreads) k_applyPositionCorrections(Scene s)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.N) return;
+    const f3 c = xyz(s.posCorr[i]);
+    s.posCorr[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 p = s.x[i];
+    if (p.w <= kEps) return;
+    s.x[i] = mk4(xyz(p) + c, p.w);
+}
+
+// ------------------------------------------------------------------------------------------
+// Velocity update and velocity-level passes
+// ------------------------------------------------------------------------------------------
+// physics_particle_update_velocities.cs.hlsl:13-44 (the fluid accumulated delta lives at the
+// particle's sorted slot)
+__global__ void __launch_bounds__(kThreads) k_updateVelocities(Scene s, float dt, const float4 *Dfinal)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.N) return;
+    const float4 p = s.x[i];
+    if (p.w <= kEps || dt <= kEps) {
+        s.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const f3 pp = xyz(s.xprev[i]);
+    f3 pos = xyz(p);
+    if (Dfinal && s.kinds[i] == CN_PARTICLE_FLUID) {
+        pos += xyz(Dfinal[s.rank[i]]);
+        s.x[i] = mk4(pos, p.w);
+    }
+    const float damping = mx(s.contactMaterials[s.matIdx[i]].z, 0.0f);
+    const float ds = mx(1.0f - damping * dt, 0.0f);
+    s.v[i] = mk4(((pos - pp) / dt) * ds, 0.0f);
+}
+
+// physics_fluid_project_boundary_velocities.cs.hlsl:24-117
+__global__ void __launch_bounds__(kThreads) k_fluidBoundaryVelocities(Scene s, float dt, Config cfg)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.N || s.kinds[i] != CN_PARTICLE_FLUID) return;
+    unsigned long long bm = s.sBoundary[s.rank[i]];
+    if (!bm) return;
+    const f3 pos = xyz(s.x[i]);
+    const float pr = mx(s.radii[i], 0.0f);
+    const f3 vel = xyz(s.v[i]);
+    const float4 pm = s.contactMaterials[s.matIdx[i]];
+    const float pd = mx(pm.z, 0.0f);
+    float bestD = 3.402823466e+38f;
+    f3 bestN{0.f, 1.f, 0.f}, bestMat{0.f, 0.f, 0.f};
+    bool found = false;
+    while (bm) {
+        const uint32_t k = __ffsll(bm) - 1;
+        bm &= bm - 1ull;
+        const uint32_t c = s.colQueryOrder[k];
+        float sd = 0.0f;
+        f3 n{0.f, 1.f, 0.f};
+        if (!fluidBoundaryContactInfo(s, c, pos, sd, n)) continue;
+        const float cd = pr + 2.0f * cfg.slop;
+        if (sd > cd) continue;
+        if (sd < bestD) {
+            bestD = sd;
+            bestN = n;
+            bestMat = combineContactMaterial(pm, s.colMat[c]);
+            found = true;
+        }
+    }
+    if (!found) return;
+    const float pen = mx(pr - bestD, 0.0f);
+    const float cd = mx(pr + 2.0f * cfg.slop, 1.0e-5f);
+    const float cw = saturate((cd - bestD) / cd);
+    f3 rv = vel;
+    const float nv = dot(rv, bestN);
+    if (nv < 0.0f) rv -= bestN * nv;
+    f3 tv = projectOntoTangent(rv, bestN);
+    if (dt > kEps) {
+        const f3 fd = positionFrictionDelta(tv * dt, mx(pen, cfg.slop), bestMat.x, bestMat.z,
+                                            cfg.positionFrictionMinDistance);
+        tv -= fd / dt;
+    }
+    const float tds = mx(1.0f - pd * cw * dt, 0.0f);
+    tv = tv * tds;
+    rv = bestN * mx(dot(rv, bestN), 0.0f) + tv;
+    s.v[i] = mk4(rv, 0.0f);
+}
+
+// physics_particle_rigid_solve_contact_velocities.cs.hlsl + apply_contact_velocities.cs.hlsl for
+// all `iterations` at once: with static/kinematic bodies each particle's velocity only depends
+// on its own contacts, and the per-particle sum runs in contact order.
+__global__ void __launch_bounds__(kThreads) k_rigidContactVelocities(Scene s, uint32_t iterations, Config cfg)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.N) return;
+    const uint32_t cnt = s.candCount[i];
+    if (cnt == 0u) return;
+    const float iS = s.x[i].w;
+    if (iS <= kEps) return; // corrections are only applied to particles with mass
+    const uint32_t off = s.candOffset[i];
+    const uint32_t lim = s.meta_->rigidPairCount;
+    const float rpt = cfg.restitutionPenetrationThreshold;
+    f3 vel = xyz(s.v[i]);
+    const float vw = s.v[i].w;
+    for (uint32_t it = 0; it < iterations; ++it) {
+        f3 corr{0.f, 0.f, 0.f};
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t pi = off + k;
+            if (pi >= lim) break;
+            const RigidContact c = s.rigidContacts[pi];
+            if (!c.active) continue;
+            const uint32_t b = c.body;
+            const float4 rp = s.predBodyPos[b];
+            const float iR = s.bodyType[b] == CN_BODY_DYNAMIC ? rp.w : 0.0f;
+            const float4 rq = qNormalize(s.predBodyRot[b]);
+            const f3 rl = xyz(s.predBodyLin[b]), ra = xyz(s.predBodyAng[b]);
+            const f3 inI = xyz(s.bodyInvInertia[b]);
+            const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
+            const f3 cp = xyz(rp) + qRotate(rq, xyz(c.rigidLocalPoint));
+            const f3 rR = cp - xyz(rp);
+            const f3 rcv = rl + cross(ra, rR);
+            const f3 rel = vel - rcv;
+            const float nv = dot(rel, n);
+            if (nv >= 0.0f) continue;
+            const float nd = iS + contactEffectiveMass(iR, inI, rq, rR, n);
+            if (nd <= kEps) continue;
+            const f3 mat = combineContactMaterial(s.contactMaterials[s.matIdx[i]], s.colMat[c.collider]);
+            const bool er = (-nv > cfg.restitutionVelocityThreshold) && (c.normalPenetration.w <= rpt);
+            const float rest = er ? saturate(mat.y) : 0.0f;
+            const float dnv = er ? (-rest * nv) : 0.0f;
+            const float imp = mx(0.0f, (dnv - nv) / nd);
+            corr = corr + (n * imp) * iS;
+        }
+        vel = vel + corr;
+    }
+    s.v[i] = mk4(vel, vw);
+}
+
+// physics_particle_solve_contact_velocities.cs.hlsl (non-proxy) with float atomics.
+__global__ void __launch_bounds__(kThreads) k_particleContactVelocities(Scene s, Config cfg)
+{
+    const uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pi >= s.meta_->particlePairCount) return;
+    const ParticleContact c = s.particleContacts[pi];
+    if (c.active == 0u) return;
+    const float iA = s.x[c.a].w, iB = s.x[c.b].w;
+    if (iA <= kEps && iB <= kEps) return;
+    const f3 vA = xyz(s.v[c.a]), vB = xyz(s.v[c.b]);
+    const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
+    const float nv = dot(vB - vA, n);
+    if (nv >= 0.0f) return;
+    const float denom = iA + iB;
+    if (denom <= kEps) return;
+    const f3 mat = xyz(c.material);
+    const bool er = (-nv > cfg.restitutionVelocityThreshold) && (c.normalPenetration.w <= cfg.restitutionPenetrationThreshold);
+    const float rest = er ? saturate(mat.y) : 0.0f;
+    const float dnv = er ? (-rest * nv) : 0.0f;
+    const float imp = mx(0.0f, (dnv - nv) / denom);
+    const f3 ti = n * imp;
+    if (iA > kEps) {
+        const f3 d = -ti * iA;
+        atomicAdd(&s.velCorr[c.a].x, d.x);
+        atomicAdd(&s.velCorr[c.a].y, d.y);
+        atomicAdd(&s.velCorr[c.a].z, d.z);
+    }
+    if (iB > kEps) {
+        const f3 d = ti * iB;
+        atomicAdd(&s.velCorr[c.b].x, d.x);
+        atomicAdd(&s.velCorr[c.b].y, d.y);
+        atomicAdd(&s.velCorr[c.b].z, d.z);
+    }
+}
+
+// physics_particle_apply_contact_velocities.cs.hlsl
+__global__ void __launch_bounds__(kThreads) k_applyContactVelocities(Scene s)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.N) return;
+    float4 v = s.v[i];
+    const float im = s.x[i].w;
+    const f3 c = xyz(s.velCorr[i]);
+    if (im > kEps) v = mk4(xyz(v) + c, v.w);
+    s.v[i] = v;
+    s.velCorr[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Debug export: compacted (key, start, end, 0) runs in sorted order (reference table layout).
+__global__ void k_runFlags(Scene s, uint32_t *flags)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= s.N) return;
+    flags[slot] = (slot == 0 || s.keysA[slot - 1] != s.keysA[slot]) ? 1u : 0u;
+}
+__global__ void k_runCompact(Scene s, const uint32_t *flags, const uint32_t *offsets, uint4 *out, uint32_t cap)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= s.N || flags[slot] == 0u) return;
+    const uint32_t r = offsets[slot];
+    if (r >= cap) return;
+    out[r] = make_uint4(s.keysA[slot], slot, s.cellEnd[slot] & 0x7fffffffu, 0u);
+}
+
+} // namespace
+
+// ------------------------------------------------------------------------------ launchers
+void launchRigidPredict(const Scene &s, float dt, float gx, float gy, float gz, cudaStream_t st)
+{
+    if (s.B == 0 && s.C == 0) return;
+    k_rigidPredict<<<1, kThreads, 0, st>>>(s, dt, gx, gy, gz);
+}
+
+void launchCopyPredictedRigid(const Scene &s, cudaStream_t st)
+{
+    if (s.B == 0) return;
+    k_copyPredictedRigid<<<1, kThreads, 0, st>>>(s);
+}
+
+void launchPredictAndKeys(const Scene &s, float dt, const Config &c, cudaStream_t st)
+{
+    if (s.N == 0) return;
+    k_predictKeys<<<blocksFor(s.N), kThreads, 0, st>>>(s, dt, c.gravity[0], c.gravity[1], c.gravity[2],
+                                                       s.entries != nullptr);
+}
+
+void launchCellSetup(const Scene &s, cudaStream_t st)
+{
+    if (s.N == 0) return;
+    cudaMemsetAsync(s.tableKeys, 0xff, size_t(s.tableMask + 1) * sizeof(uint32_t), st);
+    k_cellSetup<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+}
+
+void launchRigidCandidates(const Scene &s, uint32_t *scanTmp, size_t, cudaStream_t st)
+{
+    if (s.N == 0) return;
+    k_rigidCandidates<false><<<blocksFor(s.N), kThreads, 0, st>>>(s, nullptr);
+    uint32_t *total = scanTmp;
+    exclusiveScan(s.candCount, s.candOffset, s.N, total, scanTmp + 1, st);
+    k_rigidCandidates<true><<<blocksFor(s.N), kThreads, 0, st>>>(s, total);
+}
+
+void launchParticleCandidates(const Scene &s, uint32_t *scanTmp, size_t, cudaStream_t st)
+{
+    if (s.N == 0) return;
+    k_particleCandidates<false><<<blocksFor(s.N), kThreads, 0, st>>>(s, nullptr);
+    uint32_t *total = scanTmp;
+    exclusiveScan(s.ppCount, s.ppOffset, s.N, total, scanTmp + 1, st);
+    k_particleCandidates<true><<<blocksFor(s.N), kThreads, 0, st>>>(s, total);
+}
+
+void launchFluidGather(const Scene &s, uint32_t iter, cudaStream_t st)
+{
+    if (s.N == 0) return;
+    const float4 *Dcur = (iter & 1u) ? s.Db : s.Da;
+    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, Dcur, iter);
+}
+
+void launchFluidNeighborsDensity(const Scene &s, const Config &c, cudaStream_t st)
+{
+    if (s.N == 0) return;
+    k_fluidNeighborsDensity<<<blocksFor(s.N), kThreads, 0, st>>>(s, c, true);
+}
+
+void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
+                                cudaStream_t st)
+{
+    if (s.N == 0) return;
+    const float4 *Dcur = (iter & 1u) ? s.Db : s.Da;
+    float4 *Dnext = (iter & 1u) ? s.Da : s.Db;
+    k_fluidDeltaApplyClamp<<<blocksFor(s.N), kThreads, 0, st>>>(s, c, s.Xs, Dcur, Dnext, iter, dt, writeDebug);
+}
+
+void launchFluidIteration(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
+                          cudaStream_t st)
+{
+    launchFluidGather(s, iter, st);
+    launchFluidNeighborsDensity(s, c, st);
+    launchFluidDeltaApplyClamp(s, iter, dt, c, writeDebug, st);
+}
+
+void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)
+{
+    if (s.N == 0) return;
+    // Positions after the velocity update; the accumulated delta was folded into x.
+    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, s.Da, 0u);
+    Config dummy{};
+    k_fluidNeighborsDensity<<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false);
+}
+
+void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st)
+{
+    const float relax = c.softInternalRelaxation;
+    if (s.E) {
+        k_solveEdges<<<blocksFor(s.E), kThreads, 0, st>>>(s, dt, relax);
+        k_applyPair<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.edgeRanges, s.edgeInc, s.edgeCorr);
+    }
+    if (s.S) {
+        k_solveSegments<<<blocksFor(s.S), kThreads, 0, st>>>(s, dt, relax);
+        k_applySegments<<<blocksFor(s.N > s.S ? s.N : s.S), kThreads, 0, st>>>(s);
+    }
+    if (s.Bn || s.D) {
+        if (s.Bn) k_solveBends<<<blocksFor(s.Bn), kThreads, 0, st>>>(s, dt, relax);
+        if (s.D) k_solveDihedrals<<<blocksFor(s.D), kThreads, 0, st>>>(s, dt, relax);
+        k_applyQuad<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.bendRanges, s.bendInc, s.bendCorr);
+    }
+    if (s.J) {
+        k_solveJoints<<<blocksFor(s.J), kThreads, 0, st>>>(s, dt, relax);
+        k_applyJoints<<<blocksFor(s.S), kThreads, 0, st>>>(s);
+    }
+    if (s.SD) {
+        k_solveDistances<<<blocksFor(s.SD), kThreads, 0, st>>>(s, dt, relax);
+        k_applyPair<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.segRanges, s.segInc, s.distCorr);
+    }
+    if (s.T) {
+        k_solveTets<<<blocksFor(s.T), kThreads, 0, st>>>(s, dt, relax);
+        k_applyQuad<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.tetRanges, s.tetInc, s.tetCorr);
+    }
+}
+
+void launchContacts(const Scene &s, const Config &c, bool particleContacts, bool rigidContacts,
+                    cudaStream_t st)
+{
+    if (particleContacts) {
+        const uint32_t cap = s.particlePairCapacity;
+        k_particleContactGenerate<<<blocksFor(cap), kThreads, 0, st>>>(s);
+        k_particleContactSolve<<<blocksFor(cap), kThreads, 0, st>>>(s, c);
+    }
+    if (rigidContacts) k_rigidContacts<<<blocksFor(s.N), kThreads, 0, st>>>(s, c, !particleContacts);
+    if (particleContacts) k_applyPositionCorrections<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+}
+
+void launchUpdateVelocities(const Scene &s, float dt, const float4 *fluidDelta, cudaStream_t st)
+{
+    if (s.N == 0) return;
+    k_updateVelocities<<<blocksFor(s.N), kThreads, 0, st>>>(s, dt, fluidDelta);
+}
+
+void launchFluidBoundaryVelocities(const Scene &s, float dt, const Config &c, cudaStream_t st)
+{
+    if (s.N == 0 || s.colQueryCount == 0) return;
+    k_fluidBoundaryVelocities<<<blocksFor(s.N), kThreads, 0, st>>>(s, dt, c);
+}
+
+void launchRigidContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st)
+{
+    if (s.N == 0 || iterations == 0) return;
+    k_rigidContactVelocities<<<blocksFor(s.N), kThreads, 0, st>>>(s, iterations, c);
+}
+
+void launchParticleContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st)
+{
+    for (uint32_t it = 0; it < iterations; ++it) {
+        k_particleContactVelocities<<<blocksFor(s.particlePairCapacity), kThreads, 0, st>>>(s, c);
+        k_applyContactVelocities<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+    }
+}
+
+void launchExportCellRanges(const Scene &s, uint4 *out, uint32_t capacity, uint32_t *scanTmp,
+                            size_t, cudaStream_t st)
+{
+    if (s.N == 0) return;
+    uint32_t *flags = scanTmp;
+    uint32_t *offsets = scanTmp + s.N;
+    uint32_t *total = scanTmp + 2 * size_t(s.N);
+    k_runFlags<<<blocksFor(s.N), kThreads, 0, st>>>(s, flags);
+    exclusiveScan(flags, offsets, s.N, total, total + 1, st);
+    k_runCompact<<<blocksFor(s.N), kThreads, 0, st>>>(s, flags, offsets, out, capacity);
+}
+
+} // namespace cn

@@ -1,0 +1,930 @@
+// cn_solver.cpp -- PhysicsSolver mirror behind the C ABI: device buffers, upload, the substep
+// schedule and its CUDA-graph replay.
+//
+// Reference: include/physics/physics_solver.h:150-205 (API), src/physics/physics_solver.cpp:173-1401
+// (syncWorldState + step), src/physics/physics_scene_gpu_state.cpp (buffers, incidence tables,
+// readback).  The pass order and gating flags of step() are reproduced; passes the reference
+// dispatches with provably empty inputs (for example particle-particle contacts in a scene
+// whose particles are all fluid) are not launched.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/cn_physics.h"
+#include "cn_device.h"
+#include "cn_internal.h"
+
+namespace cn {
+
+thread_local std::string g_lastError;
+
+inline uint32_t nextPow2(uint32_t v)
+{
+    if (v <= 1u) return 1u;
+    --v;
+    v |= v >> 1; v |= v >> 2; v |= v >> 4; v |= v >> 8; v |= v >> 16;
+    return v + 1u;
+}
+inline uint32_t resolveIter(uint32_t o, uint32_t d) { return o > 0u ? o : d; }
+
+cn_status setError(cn_status status, const std::string &message)
+{
+    g_lastError = message;
+    return status;
+}
+void clearError() { g_lastError.clear(); }
+
+// Bump allocator over one device allocation.  measure() runs the same layout code with a null
+// base to size the arena.
+class Arena {
+public:
+    void reset(uint8_t *base) { base_ = base; offset_ = 0; }
+    template <class T> T *take(size_t count)
+    {
+        const size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+        T *p = base_ ? reinterpret_cast<T *>(base_ + offset_) : nullptr;
+        offset_ += count ? bytes : 0;
+        return count ? p : nullptr;
+    }
+    size_t size() const { return offset_; }
+
+private:
+    uint8_t *base_ = nullptr;
+    size_t offset_ = 0;
+};
+
+} // namespace cn
+
+using cn::setError;
+
+struct cn_solver {
+    cn_solver_desc desc{};
+    int device = 0;
+    cudaStream_t ownStream = nullptr;
+    cn::Scene s{};
+    cn::Config cfg{};
+    void *arena = nullptr;
+    size_t arenaBytes = 0;
+    void *sortScratch = nullptr;
+    uint32_t *scanScratch = nullptr;
+    size_t scanScratchBytes = 0;
+    float *hostX = nullptr, *hostV = nullptr;
+    bool synced = false;
+    bool hasFluid = false, ppPossible = false, rigidPossible = false, hasBroadphase = false;
+    uint32_t substeps = 1, fluidIt = 1, softIt = 1, contactIt = 1, maxIt = 1;
+    bool postUpdateNeighbors = false, writeFluidDebug = false, forceBroadphase = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graphExec = nullptr;
+    float graphDt = -1.0f;
+    uint64_t bindingGeneration = 0;
+    // host-side sizes needed by debug reads
+    uint32_t cellRangeCapacity = 0;
+    // timing probes: event pairs recorded around kernel groups of the captured frame
+    bool timing = false;
+    struct Probe { const char *name; cudaEvent_t begin, end; };
+    std::vector<Probe> probes;
+    uint32_t graphKernelNodes = 0, graphNodes = 0;
+};
+
+namespace {
+
+#define CN_CUDA(call)                                                                                  \
+    do {                                                                                               \
+        const cudaError_t e__ = (call);                                                                \
+        if (e__ != cudaSuccess)                                                                        \
+            return setError(e__ == cudaErrorMemoryAllocation ? CN_ERR_OUT_OF_MEMORY : CN_ERR_CUDA,     \
+                            std::string(#call) + ": " + cudaGetErrorString(e__));                      \
+    } while (0)
+
+void releaseGraph(cn_solver *sv)
+{
+    if (sv->graphExec) cudaGraphExecDestroy(sv->graphExec);
+    if (sv->graph) cudaGraphDestroy(sv->graph);
+    sv->graphExec = nullptr;
+    sv->graph = nullptr;
+    sv->graphDt = -1.0f;
+    for (auto &p : sv->probes) {
+        cudaEventDestroy(p.begin);
+        cudaEventDestroy(p.end);
+    }
+    sv->probes.clear();
+}
+
+// Runs `fn` between two recorded events when timing is on (the events become graph nodes).
+template <class F> void probe(cn_solver *sv, const char *name, cudaStream_t st, F &&fn)
+{
+    if (!sv->timing) {
+        fn();
+        return;
+    }
+    cn_solver::Probe p{name, nullptr, nullptr};
+    cudaEventCreate(&p.begin);
+    cudaEventCreate(&p.end);
+    cudaEventRecord(p.begin, st);
+    fn();
+    cudaEventRecord(p.end, st);
+    sv->probes.push_back(p);
+}
+
+void releaseBuffers(cn_solver *sv)
+{
+    releaseGraph(sv);
+    if (sv->arena) cudaFree(sv->arena);
+    sv->arena = nullptr;
+    sv->arenaBytes = 0;
+    sv->s = cn::Scene{};
+    sv->synced = false;
+}
+
+struct Incidence {
+    std::vector<uint2> ranges, inc;
+};
+template <class F> Incidence buildIncidence(uint32_t n, uint32_t constraints, uint32_t perConstraint, F &&particlesOf)
+{
+    // physics_scene_gpu_state.cpp:3273-3420: per-particle lists in ascending constraint order
+    std::vector<uint32_t> counts(n, 0);
+    for (uint32_t c = 0; c < constraints; ++c)
+        for (uint32_t k = 0; k < perConstraint; ++k) {
+            const uint32_t p = particlesOf(c, k);
+            if (p < n) ++counts[p];
+        }
+    Incidence out;
+    out.ranges.resize(n);
+    uint32_t run = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        out.ranges[i] = make_uint2(run, counts[i]);
+        run += counts[i];
+    }
+    out.inc.resize(run);
+    std::vector<uint32_t> fill(n, 0);
+    for (uint32_t c = 0; c < constraints; ++c)
+        for (uint32_t k = 0; k < perConstraint; ++k) {
+            const uint32_t p = particlesOf(c, k);
+            if (p < n) out.inc[out.ranges[p].x + fill[p]++] = make_uint2(c, k);
+        }
+    return out;
+}
+
+// Lays out every device buffer; `upload` false only sizes the arena.
+void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const Incidence &edgeI, const Incidence &bendI,
+            const Incidence &tetI, const Incidence &segI, const Incidence &jointI)
+{
+    cn::Scene &s = sv->s;
+    const uint32_t N = w.particle_count;
+    s.N = N;
+    s.x = a.take<float4>(N); s.xprev = a.take<float4>(N); s.v = a.take<float4>(N);
+    s.radii = a.take<float>(N);
+    s.kinds = a.take<uint32_t>(N);
+    s.meta = a.take<uint4>(N);
+    s.matIdx = a.take<uint32_t>(N);
+    s.fluidMatIdx = a.take<uint32_t>(N);
+    s.ownerTypes = a.take<uint32_t>(N);
+    s.ownerIdx = a.take<uint32_t>(N);
+    s.adjOff = a.take<uint32_t>(N);
+    s.adjCnt = a.take<uint32_t>(N);
+    s.adjIdx = a.take<uint32_t>(std::max<uint32_t>(w.adjacency_index_count, 1u));
+    s.contactMaterials = a.take<float4>(std::max<uint32_t>(w.contact_material_count, 1u));
+    s.fluidMaterials = a.take<cn_fluid_material>(std::max<uint32_t>(w.fluid_material_count, 1u));
+    s.E = w.edge_count; s.Bn = w.bend_count; s.D = w.dihedral_count; s.T = w.tet_count;
+    s.S = w.strand_segment_count; s.J = w.strand_joint_count; s.SD = w.strand_distance_count;
+    s.edges = a.take<cn_soft_edge>(s.E);
+    s.bends = a.take<cn_soft_bend>(s.Bn);
+    s.dihedrals = a.take<cn_cloth_dihedral>(s.D);
+    s.tets = a.take<cn_soft_tet>(s.T);
+    s.segs = a.take<cn_strand_segment>(s.S);
+    s.joints = a.take<cn_strand_joint>(s.J);
+    s.dists = a.take<cn_strand_distance>(s.SD);
+    s.segOrient = a.take<float4>(s.S);
+    s.edgeRanges = a.take<uint2>(N); s.edgeInc = a.take<uint2>(edgeI.inc.size());
+    s.bendRanges = a.take<uint2>(N); s.bendInc = a.take<uint2>(bendI.inc.size());
+    s.tetRanges = a.take<uint2>(N); s.tetInc = a.take<uint2>(tetI.inc.size());
+    s.segRanges = a.take<uint2>(N); s.segInc = a.take<uint2>(segI.inc.size());
+    s.segJointRanges = a.take<uint2>(s.S); s.segJointInc = a.take<uint2>(jointI.inc.size());
+    s.edgeLambda = a.take<float>(s.E);
+    s.bendLambda = a.take<float>(s.Bn + s.D);
+    s.tetLambda = a.take<float>(s.T);
+    s.distLambda = a.take<float>(s.SD);
+    s.segLambda = a.take<float4>(s.S);
+    s.jointLambda = a.take<float4>(s.J);
+    s.edgeCorr = a.take<float4>(size_t(s.E) * 2);
+    s.bendCorr = a.take<float4>(size_t(s.Bn + s.D) * 4);
+    s.tetCorr = a.take<float4>(size_t(s.T) * 4);
+    s.segCorr = a.take<float4>(size_t(s.S) * 3);
+    s.jointCorr = a.take<float4>(size_t(s.J) * 2);
+    s.distCorr = a.take<float4>(size_t(s.SD) * 2);
+    s.posCorr = a.take<float4>(N);
+    s.velCorr = a.take<float4>(N);
+    s.B = w.rigid_body_count;
+    s.C = w.collider_count;
+    const uint32_t B = std::max<uint32_t>(s.B, 1u), C = std::max<uint32_t>(s.C, 1u);
+    s.bodyPos = a.take<float4>(B); s.bodyRot = a.take<float4>(B); s.bodyLin = a.take<float4>(B);
+    s.bodyAng = a.take<float4>(B); s.bodyScale = a.take<float4>(B); s.bodyInvInertia = a.take<float4>(B);
+    s.bodyType = a.take<uint32_t>(B);
+    s.bodyKinPos = a.take<float4>(B); s.bodyKinRot = a.take<float4>(B); s.bodyKinFlags = a.take<uint32_t>(B);
+    s.bodyColRanges = a.take<uint2>(B);
+    s.bodyColIdx = a.take<uint32_t>(std::max<uint32_t>(w.body_collider_index_count, 1u));
+    s.colGeo = a.take<cn_collider_geometry>(C);
+    s.colBp = a.take<cn_collider_broadphase>(C);
+    s.colMat = a.take<float4>(C);
+    s.prevBodyPos = a.take<float4>(B); s.prevBodyRot = a.take<float4>(B);
+    s.predBodyPos = a.take<float4>(B); s.predBodyRot = a.take<float4>(B);
+    s.predBodyLin = a.take<float4>(B); s.predBodyAng = a.take<float4>(B);
+    s.colAabbMin = a.take<float4>(C); s.colAabbMax = a.take<float4>(C);
+    s.colQueryOrder = a.take<uint32_t>(C);
+    if (sv->hasBroadphase) {
+        s.entries = a.take<int4>(N);
+        s.keysA = a.take<uint32_t>(N); s.keysB = a.take<uint32_t>(N);
+        s.valsA = a.take<uint32_t>(N); s.valsB = a.take<uint32_t>(N);
+        s.rank = a.take<uint32_t>(N);
+        const uint32_t cap = cn::nextPow2(std::max<uint32_t>(2u * N, 64u));
+        s.tableMask = cap - 1u;
+        s.tableKeys = a.take<uint32_t>(cap);
+        s.tableStart = a.take<uint32_t>(cap);
+        s.cellEnd = a.take<uint32_t>(N);
+        s.sCell = a.take<int4>(N);
+    }
+    s.hasFluid = sv->hasFluid ? 1u : 0u;
+    if (sv->hasFluid) {
+        s.Xs = a.take<float4>(N); s.P = a.take<float4>(N);
+        s.Da = a.take<float4>(N); s.Db = a.take<float4>(N);
+        s.Cs = a.take<float4>(N); s.Dx = a.take<float4>(N);
+        s.sMeta = a.take<uint4>(N);
+        s.sInfo = a.take<uint32_t>(N);
+        s.sBoundary = a.take<unsigned long long>(N);
+        s.maxNbr = sv->desc.max_fluid_neighborhood;
+        s.nbr = a.take<uint32_t>(std::max<size_t>(size_t(N) * s.maxNbr, 1));
+        s.nbrCount = a.take<uint32_t>(N);
+    }
+    if (sv->rigidPossible) {
+        s.candCount = a.take<uint32_t>(N);
+        s.candOffset = a.take<uint32_t>(N);
+        s.rigidPairCapacity = std::max<uint32_t>(N * 8u, 64u);
+        s.rigidPairs = a.take<uint2>(s.rigidPairCapacity);
+        s.rigidContacts = a.take<cn::RigidContact>(s.rigidPairCapacity);
+    }
+    if (sv->ppPossible) {
+        s.ppCount = a.take<uint32_t>(N);
+        s.ppOffset = a.take<uint32_t>(N);
+        s.particlePairCapacity = std::max<uint32_t>(N * 8u, 64u);
+        s.particlePairs = a.take<uint2>(s.particlePairCapacity);
+        s.particleContacts = a.take<cn::ParticleContact>(s.particlePairCapacity);
+    }
+    s.meta_ = a.take<cn::DeviceMeta>(1);
+    sv->sortScratch = a.take<uint8_t>(sv->hasBroadphase ? cn::radixSortScratchBytes(N) : 0);
+    sv->scanScratchBytes = (size_t(2) * N + 4) * sizeof(uint32_t) + cn::scanScratchBytes(std::max<uint32_t>(N, 1u));
+    sv->scanScratch = a.take<uint32_t>(sv->scanScratchBytes / sizeof(uint32_t));
+}
+
+template <class T> cudaError_t up(const T *dst, const void *src, size_t count, cudaStream_t st)
+{
+    if (!count || !src) return cudaSuccess;
+    return cudaMemcpyAsync(const_cast<T *>(dst), src, count * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
+{
+    const cn::Scene &s = sv->s;
+    const float dt = frameDt / float(sv->substeps);
+    const cn::Config &c = sv->cfg;
+    const uint32_t N = s.N;
+    for (uint32_t sub = 0; sub < sv->substeps; ++sub) {
+        probe(sv, "rigid_predict", st, [&] { cn::launchRigidPredict(s, dt, c.gravity[0], c.gravity[1], c.gravity[2], st); });
+        probe(sv, "predict_keys", st, [&] { cn::launchPredictAndKeys(s, dt, c, st); });
+        if (sv->hasBroadphase && (sv->hasFluid || sv->ppPossible || sv->forceBroadphase)) {
+            probe(sv, "radix_sort", st, [&] {
+                cn::radixSortPairs(s.keysA, s.valsA, s.keysB, s.valsB, N, sv->sortScratch, &s.meta_->waitTimeouts, st);
+            });
+            probe(sv, "cell_setup", st, [&] { cn::launchCellSetup(s, st); });
+        }
+        if (sv->ppPossible)
+            probe(sv, "particle_candidates", st, [&] { cn::launchParticleCandidates(s, sv->scanScratch, sv->scanScratchBytes, st); });
+        if (sv->rigidPossible)
+            probe(sv, "rigid_candidates", st, [&] { cn::launchRigidCandidates(s, sv->scanScratch, sv->scanScratchBytes, st); });
+        // clearSoftConstraintState (physics_clear_soft_constraint_state.cs.hlsl:14-54)
+        if (s.E) cudaMemsetAsync(s.edgeLambda, 0, sizeof(float) * s.E, st);
+        if (s.Bn + s.D) cudaMemsetAsync(s.bendLambda, 0, sizeof(float) * (s.Bn + s.D), st);
+        if (s.T) cudaMemsetAsync(s.tetLambda, 0, sizeof(float) * s.T, st);
+        if (s.SD) cudaMemsetAsync(s.distLambda, 0, sizeof(float) * s.SD, st);
+        if (s.S) cudaMemsetAsync(s.segLambda, 0, sizeof(float4) * s.S, st);
+        if (s.J) cudaMemsetAsync(s.jointLambda, 0, sizeof(float4) * s.J, st);
+        if (sv->ppPossible) {
+            cudaMemsetAsync(s.posCorr, 0, sizeof(float4) * N, st);
+            cudaMemsetAsync(s.velCorr, 0, sizeof(float4) * N, st);
+        }
+        const bool hasSoftInternal = N > 0 && (s.E || s.Bn || s.D || s.T || s.S || s.J || s.SD);
+        for (uint32_t it = 0; it < sv->maxIt; ++it) {
+            const bool runFluid = sv->hasFluid && it < sv->fluidIt;
+            const bool runSoft = hasSoftInternal && it < sv->softIt;
+            const bool runPP = sv->ppPossible && it < sv->contactIt;
+            const bool runRigid = sv->rigidPossible && it < sv->contactIt;
+            if (!runFluid && !runSoft && !runPP && !runRigid) break; // remaining iterations are empty
+            if (runFluid) {
+                probe(sv, "fluid_gather", st, [&] { cn::launchFluidGather(s, it, st); });
+                probe(sv, "fluid_neighbors_density", st, [&] { cn::launchFluidNeighborsDensity(s, c, st); });
+                probe(sv, "fluid_delta_apply_clamp", st,
+                      [&] { cn::launchFluidDeltaApplyClamp(s, it, dt, c, sv->writeFluidDebug, st); });
+            }
+            if (runSoft) probe(sv, "soft_constraints", st, [&] { cn::launchSoftIteration(s, dt, c, st); });
+            if (runPP || runRigid) probe(sv, "contacts", st, [&] { cn::launchContacts(s, c, runPP, runRigid, st); });
+        }
+        const float4 *fluidDelta = sv->hasFluid ? ((sv->fluidIt & 1u) ? s.Db : s.Da) : nullptr;
+        probe(sv, "update_velocities", st, [&] { cn::launchUpdateVelocities(s, dt, fluidDelta, st); });
+        if (sv->hasFluid) probe(sv, "fluid_boundary_velocities", st, [&] { cn::launchFluidBoundaryVelocities(s, dt, c, st); });
+        if (sv->hasFluid && sv->postUpdateNeighbors) cn::launchFluidNeighborsOnly(s, st);
+        if (sv->ppPossible && sv->contactIt)
+            probe(sv, "contact_velocities", st, [&] { cn::launchParticleContactVelocities(s, sv->contactIt, c, st); });
+        if (sv->rigidPossible && sv->contactIt)
+            probe(sv, "contact_velocities", st, [&] { cn::launchRigidContactVelocities(s, sv->contactIt, c, st); });
+        cn::launchCopyPredictedRigid(s, st);
+    }
+}
+
+cn_status runFrames(cn_solver *sv, float frameDt, uint32_t frames, cudaStream_t st)
+{
+    if (!sv->synced) return setError(CN_ERR_NOT_INITIALIZED, "cn_solver_step: no world synced");
+    if (sv->s.N == 0 && sv->s.B == 0) return CN_OK;
+    CN_CUDA(cudaSetDevice(sv->device));
+    if (sv->graphExec == nullptr || sv->graphDt != frameDt) {
+        releaseGraph(sv);
+        cudaStream_t cap = sv->ownStream;
+        CN_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+        enqueueFrame(sv, frameDt, cap);
+        const cudaError_t endErr = cudaStreamEndCapture(cap, &sv->graph);
+        if (endErr != cudaSuccess) {
+            cudaGetLastError();
+            return setError(CN_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(endErr));
+        }
+        CN_CUDA(cudaGraphInstantiate(&sv->graphExec, sv->graph, 0));
+        sv->graphDt = frameDt;
+        size_t count = 0;
+        cudaGraphGetNodes(sv->graph, nullptr, &count);
+        std::vector<cudaGraphNode_t> nodes(count);
+        cudaGraphGetNodes(sv->graph, nodes.data(), &count);
+        uint32_t kernels = 0;
+        for (cudaGraphNode_t n : nodes) {
+            cudaGraphNodeType type;
+            if (cudaGraphNodeGetType(n, &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) ++kernels;
+        }
+        sv->graphNodes = uint32_t(count);
+        sv->graphKernelNodes = kernels;
+    }
+    for (uint32_t f = 0; f < frames; ++f) CN_CUDA(cudaGraphLaunch(sv->graphExec, st));
+    CN_CUDA(cudaGetLastError());
+    return CN_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+CN_API const char *cn_last_error(void) { return cn::g_lastError.c_str(); }
+CN_API const char *cn_version(void) { return "cressim-neo-b200 0.1.0 (sm_100a)"; }
+
+CN_API void cn_solver_desc_defaults(cn_solver_desc *d)
+{
+    std::memset(d, 0, sizeof(*d));
+    d->gravity[1] = -9.81f;
+    d->substeps = 1;
+    d->default_iterations = 20;
+    d->contact = cn_contact_settings{1.0e-3f, 4.0f, 0.95f, 0.05f, 0.5f, 2.0f, 0.0f, 1.0e-5f};
+    d->rigid = cn_rigid_settings{0.25f, 0.90f, 0.10f, 1.0f, 0.01f, 0.10f, 0.8f, 0.5f};
+    d->joints = cn_joint_settings{0.95f, 0.7f, 0.05f, 0.02f, 0.12f, 1.0e-5f, 5.0e-5f, 1.0e-5f};
+    d->soft.internal_relaxation = 0.2f;
+    d->fluid.constraint_relaxation = 0.7f;
+    d->fluid.position_relaxation = 1.0f;
+    d->fluid.boundary_density_scale = 0.12f;
+    d->fluid.boundary_delta_scale = 0.08f;
+    d->fluid.max_under_density_ratio = 0.0f;
+    d->enable_blocking_readback = 1u;
+    d->max_fluid_neighborhood = 128u;
+}
+
+CN_API cn_status cn_solver_create(const cn_solver_desc *desc, int device, cn_solver **out)
+{
+    if (!desc || !out) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_create: null argument");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return setError(CN_ERR_NO_DEVICE, "cn_solver_create: no CUDA device");
+    }
+    if (device < 0 || device >= count) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_create: bad device");
+    CN_CUDA(cudaSetDevice(device));
+    cn_solver *sv = new cn_solver();
+    sv->desc = *desc;
+    sv->device = device;
+    const cudaError_t e = cudaStreamCreateWithFlags(&sv->ownStream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete sv;
+        return setError(CN_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+    }
+    *out = sv;
+    return CN_OK;
+}
+
+CN_API void cn_solver_destroy(cn_solver *sv)
+{
+    if (!sv) return;
+    cudaSetDevice(sv->device);
+    cudaStreamSynchronize(sv->ownStream);
+    releaseBuffers(sv);
+    cudaStreamDestroy(sv->ownStream);
+    delete sv;
+}
+
+CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
+{
+    if (!sv || !w) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_sync_world: null argument");
+    const uint32_t N = w->particle_count;
+    if (N && (!w->positions_inv_mass || !w->velocities || !w->radii || !w->kinds || !w->metadata ||
+              !w->material_indices || !w->fluid_material_indices || !w->owner_types || !w->owner_indices ||
+              !w->adjacency_offsets || !w->adjacency_counts))
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_sync_world: missing particle array");
+    if (N > (1u << 29)) return setError(CN_ERR_CAPACITY, "cn_solver_sync_world: more than 2^29 particles");
+    if (sv->desc.max_fluid_neighborhood > 1024u)
+        return setError(CN_ERR_INVALID_ARGUMENT, "max_fluid_neighborhood above 1024");
+    CN_CUDA(cudaSetDevice(sv->device));
+    CN_CUDA(cudaStreamSynchronize(sv->ownStream));
+    releaseBuffers(sv);
+
+    // Structural flags (physics_solver.cpp:472-496), plus which contact families can have pairs.
+    const cn_solver_desc &d = sv->desc;
+    sv->substeps = std::max<uint32_t>(d.substeps, 1u);
+    const uint32_t defIt = std::max<uint32_t>(d.default_iterations, 1u);
+    sv->fluidIt = cn::resolveIter(d.fluid_iterations, defIt);
+    sv->softIt = cn::resolveIter(d.soft_internal_iterations, defIt);
+    sv->contactIt = cn::resolveIter(d.soft_contact_iterations, defIt);
+    const uint32_t jointIt = cn::resolveIter(d.rigid_joint_iterations, defIt);
+    const uint32_t rrIt = cn::resolveIter(d.rigid_rigid_contact_iterations, defIt);
+    sv->maxIt = std::max(std::max(std::max(sv->fluidIt, sv->softIt), sv->contactIt), std::max(jointIt, rrIt));
+    bool anyFluid = false, anySolid = false, anySelf = false;
+    std::vector<uint32_t> solidGroups;
+    for (uint32_t i = 0; i < N; ++i) {
+        if (w->kinds[i] == CN_PARTICLE_FLUID) anyFluid = true;
+        else {
+            anySolid = true;
+            const uint32_t ph = w->metadata[4 * i + 1];
+            if (ph & CN_PHASE_SELF_COLLIDE) anySelf = true;
+            const uint32_t g = ph & CN_PHASE_GROUP_MASK;
+            if (solidGroups.size() < 2 && std::find(solidGroups.begin(), solidGroups.end(), g) == solidGroups.end())
+                solidGroups.push_back(g);
+        }
+    }
+    for (uint32_t b = 0; b < w->rigid_body_count; ++b)
+        if (w->body_types[b] == CN_BODY_DYNAMIC)
+            return setError(CN_ERR_UNSUPPORTED, "dynamic rigid bodies are outside the particle substep; use static or kinematic bodies");
+    for (uint32_t m = 0; m < w->fluid_material_count; ++m)
+        if (w->fluid_materials[m].vorticity_confinement > 1.0e-6f)
+            return setError(CN_ERR_UNSUPPORTED, "vorticity confinement is not implemented");
+    sv->hasFluid = anyFluid;
+    const bool contactWork = sv->contactIt > 0;
+    sv->ppPossible = contactWork && N > 1 && anySolid && (anyFluid || anySelf || solidGroups.size() > 1);
+    sv->rigidPossible = contactWork && N > 0 && w->collider_count > 0 && anySolid;
+    sv->hasBroadphase = N > 0 && ((contactWork && N > 1) || anyFluid || w->collider_count > 0);
+
+    // Collider query order: moving (kinematic) colliders, then static, ascending index.
+    std::vector<uint32_t> order, stat;
+    for (uint32_t c = 0; c < w->collider_count; ++c) {
+        const cn_collider_broadphase &bp = w->collider_broadphase[c];
+        if (bp.owner_body >= w->rigid_body_count || bp.enabled_flag == 0u) continue;
+        if (w->body_types[bp.owner_body] == CN_BODY_STATIC) stat.push_back(c);
+        else order.push_back(c);
+    }
+    const uint32_t moving = uint32_t(order.size());
+    order.insert(order.end(), stat.begin(), stat.end());
+    if (anyFluid && order.size() > cn::kMaxBoundaryColliders)
+        return setError(CN_ERR_UNSUPPORTED, "more than 64 colliders in a scene with fluid");
+
+    // Incidence tables.
+    const Incidence edgeI = buildIncidence(N, w->edge_count, 2, [&](uint32_t c, uint32_t k) {
+        return k == 0 ? w->edges[c].particle_a : w->edges[c].particle_b;
+    });
+    const uint32_t nb = w->bend_count;
+    const Incidence bendI = buildIncidence(N, nb + w->dihedral_count, 4, [&](uint32_t c, uint32_t k) -> uint32_t {
+        if (c < nb) {
+            if (k == 3) return 0xffffffffu;
+            const cn_soft_bend &b = w->bends[c];
+            return k == 0 ? b.particle0 : (k == 1 ? b.particle1 : b.particle2);
+        }
+        const cn_cloth_dihedral &h = w->dihedrals[c - nb];
+        const uint32_t p[4] = {h.edge_particle0, h.edge_particle1, h.opposite_particle0, h.opposite_particle1};
+        return p[k];
+    });
+    const Incidence tetI = buildIncidence(N, w->tet_count, 4, [&](uint32_t c, uint32_t k) {
+        return w->tets[c].particle_indices[k];
+    });
+    const Incidence segI = buildIncidence(N, w->strand_segment_count, 2, [&](uint32_t c, uint32_t k) {
+        return k == 0 ? w->strand_segments[c].particle_a : w->strand_segments[c].particle_b;
+    });
+    const uint32_t S = w->strand_segment_count;
+    const Incidence jointI = buildIncidence(S, w->strand_joint_count, 2, [&](uint32_t c, uint32_t k) -> uint32_t {
+        const cn_strand_joint &j = w->strand_joints[c];
+        if (j.segment_a >= S || j.segment_b >= S) return 0xffffffffu;
+        return k == 0 ? j.segment_a : j.segment_b;
+    });
+
+    cn::Arena a;
+    a.reset(nullptr);
+    layout(sv, a, *w, edgeI, bendI, tetI, segI, jointI);
+    sv->arenaBytes = a.size();
+    {
+        const cudaError_t e = cudaMalloc(&sv->arena, sv->arenaBytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            sv->arena = nullptr;
+            return setError(CN_ERR_OUT_OF_MEMORY, "cn_solver_sync_world: cannot allocate " +
+                                                      std::to_string(sv->arenaBytes) + " bytes");
+        }
+    }
+    a.reset(static_cast<uint8_t *>(sv->arena));
+    layout(sv, a, *w, edgeI, bendI, tetI, segI, jointI);
+    cn::Scene &s = sv->s;
+    s.cellSize = w->particle_grid_cell_size;
+    s.colQueryCount = uint32_t(order.size());
+    s.activeMovingCount = moving;
+    cudaStream_t st = sv->ownStream;
+    CN_CUDA(cudaMemsetAsync(sv->arena, 0, sv->arenaBytes, st));
+    CN_CUDA(up(s.x, w->positions_inv_mass, size_t(N) * 1, st));
+    CN_CUDA(up(s.v, w->velocities, N, st));
+    {
+        std::vector<float4> xp(N);
+        for (uint32_t i = 0; i < N; ++i)
+            xp[i] = make_float4(w->positions_inv_mass[4 * i], w->positions_inv_mass[4 * i + 1],
+                                w->positions_inv_mass[4 * i + 2], 0.0f);
+        CN_CUDA(up(s.xprev, xp.data(), N, st));
+        CN_CUDA(cudaStreamSynchronize(st));
+    }
+    CN_CUDA(up(s.radii, w->radii, N, st));
+    CN_CUDA(up(s.kinds, w->kinds, N, st));
+    CN_CUDA(up(s.meta, w->metadata, N, st));
+    CN_CUDA(up(s.matIdx, w->material_indices, N, st));
+    CN_CUDA(up(s.fluidMatIdx, w->fluid_material_indices, N, st));
+    CN_CUDA(up(s.ownerTypes, w->owner_types, N, st));
+    CN_CUDA(up(s.ownerIdx, w->owner_indices, N, st));
+    CN_CUDA(up(s.adjOff, w->adjacency_offsets, N, st));
+    CN_CUDA(up(s.adjCnt, w->adjacency_counts, N, st));
+    CN_CUDA(up(s.adjIdx, w->adjacency_indices, w->adjacency_index_count, st));
+    CN_CUDA(up(s.contactMaterials, w->contact_materials, w->contact_material_count, st));
+    CN_CUDA(up(s.fluidMaterials, w->fluid_materials, w->fluid_material_count, st));
+    CN_CUDA(up(s.edges, w->edges, s.E, st));
+    CN_CUDA(up(s.bends, w->bends, s.Bn, st));
+    CN_CUDA(up(s.dihedrals, w->dihedrals, s.D, st));
+    CN_CUDA(up(s.tets, w->tets, s.T, st));
+    CN_CUDA(up(s.segs, w->strand_segments, s.S, st));
+    CN_CUDA(up(s.joints, w->strand_joints, s.J, st));
+    CN_CUDA(up(s.dists, w->strand_distances, s.SD, st));
+    CN_CUDA(up(s.segOrient, w->strand_segment_orientations, s.S, st));
+    CN_CUDA(up(s.edgeRanges, edgeI.ranges.data(), edgeI.ranges.size(), st));
+    CN_CUDA(up(s.edgeInc, edgeI.inc.data(), edgeI.inc.size(), st));
+    CN_CUDA(up(s.bendRanges, bendI.ranges.data(), bendI.ranges.size(), st));
+    CN_CUDA(up(s.bendInc, bendI.inc.data(), bendI.inc.size(), st));
+    CN_CUDA(up(s.tetRanges, tetI.ranges.data(), tetI.ranges.size(), st));
+    CN_CUDA(up(s.tetInc, tetI.inc.data(), tetI.inc.size(), st));
+    CN_CUDA(up(s.segRanges, segI.ranges.data(), segI.ranges.size(), st));
+    CN_CUDA(up(s.segInc, segI.inc.data(), segI.inc.size(), st));
+    CN_CUDA(up(s.segJointRanges, jointI.ranges.data(), jointI.ranges.size(), st));
+    CN_CUDA(up(s.segJointInc, jointI.inc.data(), jointI.inc.size(), st));
+    CN_CUDA(up(s.bodyPos, w->body_positions_inv_mass, s.B, st));
+    CN_CUDA(up(s.bodyRot, w->body_orientations, s.B, st));
+    CN_CUDA(up(s.bodyLin, w->body_linear_velocities, s.B, st));
+    CN_CUDA(up(s.bodyAng, w->body_angular_velocities, s.B, st));
+    CN_CUDA(up(s.bodyScale, w->body_scales, s.B, st));
+    CN_CUDA(up(s.bodyInvInertia, w->body_inverse_inertia, s.B, st));
+    CN_CUDA(up(s.bodyType, w->body_types, s.B, st));
+    CN_CUDA(up(s.bodyKinPos, w->body_kinematic_target_positions, s.B, st));
+    CN_CUDA(up(s.bodyKinRot, w->body_kinematic_target_orientations, s.B, st));
+    CN_CUDA(up(s.bodyKinFlags, w->body_kinematic_target_flags, s.B, st));
+    CN_CUDA(up(s.bodyColRanges, w->body_collider_ranges, s.B, st));
+    CN_CUDA(up(s.bodyColIdx, w->body_collider_indices, w->body_collider_index_count, st));
+    CN_CUDA(up(s.colGeo, w->collider_geometry, s.C, st));
+    CN_CUDA(up(s.colBp, w->collider_broadphase, s.C, st));
+    CN_CUDA(up(s.colMat, w->collider_materials, s.C, st));
+    CN_CUDA(up(s.colQueryOrder, order.data(), order.size(), st));
+    CN_CUDA(cudaStreamSynchronize(st));
+
+    cn::Config &c = sv->cfg;
+    c.slop = d.contact.slop;
+    c.softContactRelaxation = d.contact.soft_relaxation;
+    c.softMaxCorrection = d.contact.soft_max_correction_per_iteration;
+    c.restitutionVelocityThreshold = d.contact.restitution_velocity_threshold;
+    c.restitutionPenetrationThreshold = d.contact.restitution_penetration_slop_multiplier * d.contact.slop;
+    c.positionFrictionMinDistance = d.contact.position_friction_min_distance;
+    c.softInternalRelaxation = d.soft.internal_relaxation;
+    c.fluidSolveCoefficient = d.fluid.constraint_relaxation;
+    c.fluidRelaxation = d.fluid.position_relaxation;
+    c.fluidBoundaryDensityScale = d.fluid.boundary_density_scale;
+    c.fluidBoundaryDeltaScale = d.fluid.boundary_delta_scale;
+    c.fluidMaxUnderDensityRatio = d.fluid.max_under_density_ratio;
+    c.gravity[0] = d.gravity[0]; c.gravity[1] = d.gravity[1]; c.gravity[2] = d.gravity[2];
+    sv->hostX = w->positions_inv_mass;
+    sv->hostV = w->velocities;
+    sv->cellRangeCapacity = cn::nextPow2(std::max<uint32_t>(N * 2u, 1u));
+    sv->synced = true;
+    ++sv->bindingGeneration;
+    cn::clearError();
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_step(cn_solver *sv, float frame_dt, void *stream)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_step: null solver");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : sv->ownStream;
+    const cn_status r = runFrames(sv, frame_dt, 1, st);
+    if (r != CN_OK) return r;
+    if (sv->desc.enable_blocking_readback && sv->hostX) {
+        CN_CUDA(cudaMemcpyAsync(sv->hostX, sv->s.x, sizeof(float4) * sv->s.N, cudaMemcpyDeviceToHost, st));
+        CN_CUDA(cudaMemcpyAsync(sv->hostV, sv->s.v, sizeof(float4) * sv->s.N, cudaMemcpyDeviceToHost, st));
+        CN_CUDA(cudaStreamSynchronize(st));
+    }
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_step_many(cn_solver *sv, float frame_dt, uint32_t steps, void *stream)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_step_many: null solver");
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : sv->ownStream;
+    return runFrames(sv, frame_dt, steps, st);
+}
+
+CN_API cn_status cn_solver_validate_meta(cn_solver *sv, cn_meta *out)
+{
+    if (!sv || !out) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_validate_meta: null argument");
+    if (!sv->synced) return setError(CN_ERR_NOT_INITIALIZED, "cn_solver_validate_meta: no world synced");
+    CN_CUDA(cudaSetDevice(sv->device));
+    CN_CUDA(cudaDeviceSynchronize());
+    cn::DeviceMeta m{};
+    CN_CUDA(cudaMemcpy(&m, sv->s.meta_, sizeof(m), cudaMemcpyDeviceToHost));
+    std::memset(out, 0, sizeof(*out));
+    out->particle_rigid_candidate_count = m.rigidPairCount;
+    out->required_particle_rigid_candidate_count = m.requiredRigidPairs;
+    out->particle_rigid_candidate_overflow = m.requiredRigidPairs > sv->s.rigidPairCapacity ? 1u : 0u;
+    out->particle_particle_candidate_count = m.particlePairCount;
+    out->required_particle_particle_candidate_count = m.requiredParticlePairs;
+    out->particle_particle_candidate_overflow = m.requiredParticlePairs > sv->s.particlePairCapacity ? 1u : 0u;
+    out->fluid_boundary_candidate_overflow = m.boundaryMaskOverflow;
+    out->active_particle_contact_count = m.activeParticleContacts;
+    out->fluid_neighbor_truncations = m.neighborTruncations;
+    out->device_wait_timeouts = m.waitTimeouts;
+    if (m.waitTimeouts) return setError(CN_ERR_DEVICE_TIMEOUT, "a bounded device wait gave up (sort look-back)");
+    if (out->particle_rigid_candidate_overflow || out->particle_particle_candidate_overflow ||
+        out->fluid_boundary_candidate_overflow)
+        return setError(CN_ERR_CAPACITY, "candidate buffer overflow");
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_set_gravity(cn_solver *sv, float x, float y, float z)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_set_gravity: null solver");
+    sv->desc.gravity[0] = x; sv->desc.gravity[1] = y; sv->desc.gravity[2] = z;
+    sv->cfg.gravity[0] = x; sv->cfg.gravity[1] = y; sv->cfg.gravity[2] = z;
+    releaseGraph(sv);
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_set_kinematic_target(cn_solver *sv, uint32_t body, const float position[3],
+                                                const float orientation[4])
+{
+    if (!sv || !position || !orientation) return setError(CN_ERR_INVALID_ARGUMENT, "set_kinematic_target: null argument");
+    if (!sv->synced || body >= sv->s.B) return setError(CN_ERR_INVALID_ARGUMENT, "set_kinematic_target: bad body");
+    const float4 p = make_float4(position[0], position[1], position[2], 0.0f);
+    const float4 q = make_float4(orientation[0], orientation[1], orientation[2], orientation[3]);
+    const uint32_t flag = 1u;
+    CN_CUDA(cudaSetDevice(sv->device));
+    CN_CUDA(cudaMemcpyAsync(sv->s.bodyKinPos + body, &p, sizeof(p), cudaMemcpyHostToDevice, sv->ownStream));
+    CN_CUDA(cudaMemcpyAsync(sv->s.bodyKinRot + body, &q, sizeof(q), cudaMemcpyHostToDevice, sv->ownStream));
+    CN_CUDA(cudaMemcpyAsync(sv->s.bodyKinFlags + body, &flag, sizeof(flag), cudaMemcpyHostToDevice, sv->ownStream));
+    CN_CUDA(cudaStreamSynchronize(sv->ownStream));
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_scene_view(cn_solver *sv, cn_scene_view *v)
+{
+    if (!sv || !v) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_scene_view: null argument");
+    std::memset(v, 0, sizeof(*v));
+    const cn::Scene &s = sv->s;
+    v->positions_inv_mass = s.x; v->previous_positions = s.xprev; v->velocities = s.v;
+    v->radii = const_cast<float *>(s.radii); v->kinds = const_cast<uint32_t *>(s.kinds);
+    v->edges = const_cast<cn_soft_edge *>(s.edges); v->bends = const_cast<cn_soft_bend *>(s.bends);
+    v->dihedrals = const_cast<cn_cloth_dihedral *>(s.dihedrals); v->tets = const_cast<cn_soft_tet *>(s.tets);
+    v->strand_segments = const_cast<cn_strand_segment *>(s.segs);
+    v->strand_joints = const_cast<cn_strand_joint *>(s.joints);
+    v->strand_distances = const_cast<cn_strand_distance *>(s.dists);
+    v->strand_segment_states = s.segOrient;
+    v->particle_count = s.N; v->edge_count = s.E; v->bend_count = s.Bn; v->dihedral_count = s.D;
+    v->tet_count = s.T; v->strand_segment_count = s.S; v->strand_joint_count = s.J; v->strand_distance_count = s.SD;
+    v->binding_generation = sv->bindingGeneration;
+    v->device = sv->device;
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_read_particles(cn_solver *sv, float *x, float *v, float *xprev, uint32_t count)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_read_particles: null solver");
+    if (count > sv->s.N) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_read_particles: count > particles");
+    CN_CUDA(cudaSetDevice(sv->device));
+    CN_CUDA(cudaDeviceSynchronize());
+    if (x) CN_CUDA(cudaMemcpy(x, sv->s.x, sizeof(float4) * count, cudaMemcpyDeviceToHost));
+    if (v) CN_CUDA(cudaMemcpy(v, sv->s.v, sizeof(float4) * count, cudaMemcpyDeviceToHost));
+    if (xprev) CN_CUDA(cudaMemcpy(xprev, sv->s.xprev, sizeof(float4) * count, cudaMemcpyDeviceToHost));
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_write_particles(cn_solver *sv, const float *x, const float *v, uint32_t count)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_write_particles: null solver");
+    if (count > sv->s.N) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_write_particles: count > particles");
+    CN_CUDA(cudaSetDevice(sv->device));
+    if (x) CN_CUDA(cudaMemcpyAsync(sv->s.x, x, sizeof(float4) * count, cudaMemcpyHostToDevice, sv->ownStream));
+    if (v) CN_CUDA(cudaMemcpyAsync(sv->s.v, v, sizeof(float4) * count, cudaMemcpyHostToDevice, sv->ownStream));
+    CN_CUDA(cudaStreamSynchronize(sv->ownStream));
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_read_strand_orientations(cn_solver *sv, float *q, uint32_t count)
+{
+    if (!sv || !q) return setError(CN_ERR_INVALID_ARGUMENT, "read_strand_orientations: null argument");
+    if (count > sv->s.S) return setError(CN_ERR_INVALID_ARGUMENT, "read_strand_orientations: count > segments");
+    CN_CUDA(cudaSetDevice(sv->device));
+    CN_CUDA(cudaDeviceSynchronize());
+    if (count) CN_CUDA(cudaMemcpy(q, sv->s.segOrient, sizeof(float4) * count, cudaMemcpyDeviceToHost));
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_set_debug(cn_solver *sv, uint32_t flags)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_set_debug: null solver");
+    sv->writeFluidDebug = (flags & 1u) != 0u;
+    sv->postUpdateNeighbors = (flags & 2u) != 0u;
+    sv->forceBroadphase = (flags & 4u) != 0u;
+    releaseGraph(sv);
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_set_timing(cn_solver *sv, uint32_t enable)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_set_timing: null solver");
+    sv->timing = enable != 0u;
+    releaseGraph(sv);
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_kernel_times(cn_solver *sv, cn_kernel_time *out, uint32_t capacity, uint32_t *count)
+{
+    if (!sv || !count) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_kernel_times: null argument");
+    CN_CUDA(cudaSetDevice(sv->device));
+    CN_CUDA(cudaDeviceSynchronize());
+    std::vector<cn_kernel_time> acc;
+    for (const auto &p : sv->probes) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, p.begin, p.end) != cudaSuccess) {
+            cudaGetLastError();
+            return setError(CN_ERR_CUDA, "cn_solver_kernel_times: events not recorded yet");
+        }
+        auto it = std::find_if(acc.begin(), acc.end(), [&](const cn_kernel_time &k) { return std::strcmp(k.name, p.name) == 0; });
+        if (it == acc.end()) {
+            cn_kernel_time k{};
+            std::strncpy(k.name, p.name, sizeof(k.name) - 1);
+            acc.push_back(k);
+            it = acc.end() - 1;
+        }
+        it->milliseconds += ms;
+        it->launches += 1;
+    }
+    *count = uint32_t(acc.size());
+    if (out)
+        for (uint32_t i = 0; i < capacity && i < acc.size(); ++i) out[i] = acc[i];
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_graph_stats(cn_solver *sv, uint32_t *kernel_nodes, uint32_t *nodes)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_graph_stats: null solver");
+    if (kernel_nodes) *kernel_nodes = sv->graphKernelNodes;
+    if (nodes) *nodes = sv->graphNodes;
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_debug_read(cn_solver *sv, cn_debug_buffer which, void *dst, size_t cap, size_t *outBytes)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_debug_read: null solver");
+    if (!sv->synced) return setError(CN_ERR_NOT_INITIALIZED, "cn_solver_debug_read: no world synced");
+    CN_CUDA(cudaSetDevice(sv->device));
+    CN_CUDA(cudaDeviceSynchronize());
+    const cn::Scene &s = sv->s;
+    const uint32_t N = s.N;
+    std::vector<uint8_t> buf;
+    auto fetch = [&](const void *src, size_t bytes, std::vector<uint8_t> &into) -> cudaError_t {
+        into.resize(bytes);
+        if (!bytes || !src) return cudaSuccess;
+        return cudaMemcpy(into.data(), src, bytes, cudaMemcpyDeviceToHost);
+    };
+    std::vector<uint8_t> rankB, valsB;
+    const bool needRank = which == CN_DEBUG_FLUID_NEIGHBOR_COUNTS || which == CN_DEBUG_FLUID_NEIGHBORS ||
+                          which == CN_DEBUG_FLUID_CONSTRAINTS || which == CN_DEBUG_FLUID_DELTA;
+    if (needRank) {
+        if (!s.rank || !s.hasFluid) return setError(CN_ERR_INVALID_ARGUMENT, "debug_read: scene has no fluid");
+        CN_CUDA(fetch(s.rank, sizeof(uint32_t) * N, rankB));
+        CN_CUDA(fetch(s.valsA, sizeof(uint32_t) * N, valsB));
+    }
+    const uint32_t *rank = reinterpret_cast<const uint32_t *>(rankB.data());
+    const uint32_t *vals = reinterpret_cast<const uint32_t *>(valsB.data());
+    std::vector<uint8_t> kindsB;
+    switch (which) {
+    case CN_DEBUG_CELL_ENTRIES:
+        if (!s.entries) return setError(CN_ERR_INVALID_ARGUMENT, "debug_read: no broadphase");
+        CN_CUDA(fetch(s.entries, sizeof(int4) * N, buf));
+        break;
+    case CN_DEBUG_SORTED_KEYS: {
+        if (!s.keysA) return setError(CN_ERR_INVALID_ARGUMENT, "debug_read: no broadphase");
+        std::vector<uint8_t> k, v;
+        CN_CUDA(fetch(s.keysA, sizeof(uint32_t) * N, k));
+        CN_CUDA(fetch(s.valsA, sizeof(uint32_t) * N, v));
+        buf.resize(size_t(N) * 8);
+        uint32_t *o = reinterpret_cast<uint32_t *>(buf.data());
+        for (uint32_t i = 0; i < N; ++i) {
+            o[2 * i] = reinterpret_cast<uint32_t *>(k.data())[i];
+            o[2 * i + 1] = reinterpret_cast<uint32_t *>(v.data())[i];
+        }
+        break;
+    }
+    case CN_DEBUG_CELL_RANGES: {
+        if (!s.keysA) return setError(CN_ERR_INVALID_ARGUMENT, "debug_read: no broadphase");
+        const uint32_t capR = sv->cellRangeCapacity;
+        uint4 *tmp = nullptr;
+        CN_CUDA(cudaMalloc(&tmp, sizeof(uint4) * capR));
+        std::vector<uint4> init(capR, make_uint4(0xffffffffu, 0u, 0u, 0u));
+        cudaMemcpy(tmp, init.data(), sizeof(uint4) * capR, cudaMemcpyHostToDevice);
+        cn::launchExportCellRanges(s, tmp, capR, sv->scanScratch, sv->scanScratchBytes, sv->ownStream);
+        cudaStreamSynchronize(sv->ownStream);
+        const cudaError_t e = fetch(tmp, sizeof(uint4) * capR, buf);
+        cudaFree(tmp);
+        CN_CUDA(e);
+        break;
+    }
+    case CN_DEBUG_FLUID_NEIGHBOR_COUNTS: {
+        std::vector<uint8_t> c;
+        CN_CUDA(fetch(s.nbrCount, sizeof(uint32_t) * N, c));
+        CN_CUDA(fetch(s.kinds, sizeof(uint32_t) * N, kindsB));
+        buf.assign(size_t(N) * 4, 0);
+        uint32_t *o = reinterpret_cast<uint32_t *>(buf.data());
+        const uint32_t *cc = reinterpret_cast<const uint32_t *>(c.data());
+        const uint32_t *kk = reinterpret_cast<const uint32_t *>(kindsB.data());
+        for (uint32_t p = 0; p < N; ++p) o[p] = kk[p] == CN_PARTICLE_FLUID ? cc[rank[p]] : 0u;
+        break;
+    }
+    case CN_DEBUG_FLUID_NEIGHBORS: {
+        std::vector<uint8_t> c, l;
+        CN_CUDA(fetch(s.nbrCount, sizeof(uint32_t) * N, c));
+        CN_CUDA(fetch(s.nbr, sizeof(uint32_t) * size_t(N) * s.maxNbr, l));
+        CN_CUDA(fetch(s.kinds, sizeof(uint32_t) * N, kindsB));
+        buf.assign(size_t(N) * s.maxNbr * 4, 0);
+        uint32_t *o = reinterpret_cast<uint32_t *>(buf.data());
+        const uint32_t *cc = reinterpret_cast<const uint32_t *>(c.data());
+        const uint32_t *ll = reinterpret_cast<const uint32_t *>(l.data());
+        const uint32_t *kk = reinterpret_cast<const uint32_t *>(kindsB.data());
+        for (uint32_t p = 0; p < N; ++p) {
+            if (kk[p] != CN_PARTICLE_FLUID) continue;
+            const uint32_t r = rank[p];
+            const uint32_t n = std::min(cc[r], s.maxNbr);
+            for (uint32_t k = 0; k < n; ++k) o[size_t(p) * s.maxNbr + k] = vals[ll[size_t(r) * s.maxNbr + k]];
+        }
+        break;
+    }
+    case CN_DEBUG_FLUID_CONSTRAINTS:
+    case CN_DEBUG_FLUID_DELTA: {
+        std::vector<uint8_t> c;
+        CN_CUDA(fetch(which == CN_DEBUG_FLUID_CONSTRAINTS ? s.Cs : s.Dx, sizeof(float4) * N, c));
+        buf.assign(size_t(N) * 16, 0);
+        float4 *o = reinterpret_cast<float4 *>(buf.data());
+        const float4 *cc = reinterpret_cast<const float4 *>(c.data());
+        for (uint32_t p = 0; p < N; ++p) o[p] = cc[rank[p]];
+        break;
+    }
+    case CN_DEBUG_RIGID_CONTACTS: {
+        if (!s.rigidContacts) { buf.clear(); break; }
+        cn::DeviceMeta m{};
+        CN_CUDA(cudaMemcpy(&m, s.meta_, sizeof(m), cudaMemcpyDeviceToHost));
+        std::vector<uint8_t> c;
+        CN_CUDA(fetch(s.rigidContacts, sizeof(cn::RigidContact) * m.rigidPairCount, c));
+        const cn::RigidContact *cc = reinterpret_cast<const cn::RigidContact *>(c.data());
+        for (uint32_t k = 0; k < m.rigidPairCount; ++k)
+            if (cc[k].active) {
+                const uint8_t *b = reinterpret_cast<const uint8_t *>(&cc[k]);
+                buf.insert(buf.end(), b, b + sizeof(cn::RigidContact));
+            }
+        break;
+    }
+    default:
+        return setError(CN_ERR_INVALID_ARGUMENT, "debug_read: unknown buffer");
+    }
+    if (outBytes) *outBytes = buf.size();
+    if (dst && cap) std::memcpy(dst, buf.data(), std::min(cap, buf.size()));
+    return CN_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,472 @@
+/*
+ * cn_physics.h -- C ABI of the B200-native CRESSim-Neo particle physics substep.
+ *
+ * This header is the drop-in boundary for the particle substep that
+ * cressim::neo::physics::PhysicsSolver runs
+ * (reference: include/physics/physics_solver.h:150-205,
+ *  src/physics/physics_solver.cpp:336-1401).  Every entry point takes plain
+ * pointers and sizes; no C++ or torch types cross it.  Every call returns a
+ * cn_status; cn_last_error() returns the message of the last failure on the
+ * calling thread.
+ *
+ * Record layouts (cn_soft_edge, cn_soft_tet, ...) are byte-compatible with the
+ * reference's GPU records (assets/shaders/include/physics/particle/
+ * physics_particle_types.hlsli:111-290) so a caller that already packs the
+ * reference's PhysicsWorld SoA can hand the same arrays over unchanged.
+ */
+#ifndef CN_PHYSICS_H
+#define CN_PHYSICS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define CN_API __declspec(dllexport)
+#else
+#define CN_API __attribute__((visibility("default")))
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum cn_status {
+    CN_OK = 0,
+    CN_ERR_INVALID_ARGUMENT = 1,
+    CN_ERR_CUDA = 2,
+    CN_ERR_OUT_OF_MEMORY = 3,
+    CN_ERR_NOT_INITIALIZED = 4,
+    CN_ERR_CAPACITY = 5,     /* a fixed-capacity table overflowed */
+    CN_ERR_NO_DEVICE = 6,
+    CN_ERR_DEVICE_TIMEOUT = 7, /* a bounded device-side wait gave up */
+    CN_ERR_UNSUPPORTED = 8
+} cn_status;
+
+/* Message of the last failing call on this thread ("" when none). */
+CN_API const char *cn_last_error(void);
+/* Library version string. */
+CN_API const char *cn_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Solver settings: field-for-field mirror of PhysicsSolverDesc and its five  */
+/* 32-byte settings structs (include/physics/physics_solver.h:22-143).        */
+/* ------------------------------------------------------------------------ */
+typedef struct cn_contact_settings {
+    float slop;                                 /* 1e-3  */
+    float manifold_merge_slop_multiplier;       /* 4     */
+    float soft_relaxation;                      /* 0.95  */
+    float soft_max_correction_per_iteration;    /* 0.05  */
+    float restitution_velocity_threshold;       /* 0.5   */
+    float restitution_penetration_slop_multiplier; /* 2  */
+    float rigid_restitution_velocity_threshold; /* 0     */
+    float position_friction_min_distance;       /* 1e-5  */
+} cn_contact_settings;
+
+typedef struct cn_rigid_settings {
+    float depenetration_baumgarte;
+    float depenetration_relaxation;
+    float depenetration_max_correction_per_iteration;
+    float velocity_penetration_stiffness;
+    float max_translation_correction_per_iteration;
+    float max_rotation_correction_per_iteration;
+    float max_linear_velocity_correction_per_iteration;
+    float max_angular_velocity_correction_per_iteration;
+} cn_rigid_settings;
+
+typedef struct cn_joint_settings {
+    float ball_relaxation;
+    float articulated_relaxation;
+    float max_error;
+    float max_translation_correction;
+    float max_angular_correction;
+    float regularization;
+    float angular_regularization;
+    float min_xpbd_dt;
+} cn_joint_settings;
+
+typedef struct cn_soft_settings {
+    float internal_relaxation; /* 0.2 */
+    float reserved[7];
+} cn_soft_settings;
+
+typedef struct cn_fluid_settings {
+    float constraint_relaxation;  /* 0.7  (kFluidSolveCoefficient) */
+    float position_relaxation;    /* 1.0  (kFluidRelaxationFactor) */
+    float boundary_density_scale; /* 0.12 */
+    float boundary_delta_scale;   /* 0.08 */
+    float max_under_density_ratio;/* 0.0  */
+    float reserved[3];
+} cn_fluid_settings;
+
+typedef struct cn_solver_desc {
+    float gravity[3];                 /* (0,-9.81,0) */
+    uint32_t substeps;                /* >= 1 */
+    uint32_t default_iterations;      /* 20 */
+    uint32_t fluid_iterations;        /* 0 = default_iterations */
+    uint32_t soft_internal_iterations;/* 0 = default_iterations */
+    uint32_t soft_contact_iterations; /* 0 = default_iterations */
+    uint32_t rigid_joint_iterations;  /* 0 = default_iterations */
+    uint32_t rigid_rigid_contact_iterations; /* 0 = default_iterations */
+    cn_contact_settings contact;
+    cn_rigid_settings rigid;
+    cn_joint_settings joints;
+    cn_soft_settings soft;
+    cn_fluid_settings fluid;
+    uint32_t enable_blocking_readback; /* 1: step() copies x and v back into the synced host arrays */
+    uint32_t max_fluid_neighborhood;   /* 128 (kDefaultFluidMaxNeighborhood) */
+} cn_solver_desc;
+
+/* Fills the reference's defaults (physics_solver.h:22-143). */
+CN_API void cn_solver_desc_defaults(cn_solver_desc *desc);
+
+/* ------------------------------------------------------------------------ */
+/* Device records (byte-compatible with physics_particle_types.hlsli and     */
+/* physics_rigid_types.hlsli).                                               */
+/* ------------------------------------------------------------------------ */
+typedef struct cn_soft_edge {          /* GpuSoftEdge, 32 B */
+    uint32_t particle_a, particle_b;
+    float rest_length, compliance;
+    uint32_t enabled, reserved0, reserved1, reserved2;
+} cn_soft_edge;
+
+typedef struct cn_soft_tet {           /* GpuSoftTet, 32 B */
+    uint32_t particle_indices[4];
+    float rest_volume, compliance;
+    uint32_t reserved0, reserved1;
+} cn_soft_tet;
+
+typedef struct cn_soft_bend {          /* GpuSoftBend, 32 B */
+    uint32_t particle0, particle1, particle2;
+    float rest_angle, compliance;
+    uint32_t reserved0, reserved1, reserved2;
+} cn_soft_bend;
+
+typedef struct cn_cloth_dihedral {     /* GpuClothDihedral, 32 B */
+    uint32_t edge_particle0, edge_particle1, opposite_particle0, opposite_particle1;
+    float rest_angle, compliance;
+    uint32_t reserved0, reserved1;
+} cn_cloth_dihedral;
+
+typedef struct cn_strand_segment {     /* GpuStrandSegment, 32 B */
+    uint32_t particle_a, particle_b;
+    float rest_length, stretch_shear_compliance;
+    float rest_orientation[4];         /* quaternion (x,y,z,w) */
+} cn_strand_segment;
+
+typedef struct cn_strand_joint {       /* GpuStrandJoint, 32 B */
+    uint32_t segment_a, segment_b;
+    float bend_compliance, twist_compliance;
+    float rest_relative_orientation[4];
+} cn_strand_joint;
+
+typedef struct cn_strand_distance {    /* GpuStrandDistanceConstraint, 16 B */
+    uint32_t particle_a, particle_b;
+    float rest_length, distance_compliance;
+} cn_strand_distance;
+
+typedef struct cn_fluid_material {     /* GpuFluidMaterial / FluidMaterialGpu, 48 B */
+    float rest_density, inv_rest_density, smoothing_radius, density_constraint_scale;
+    float viscosity, cohesion, cohesion1, cohesion2;
+    float surface_tension, vorticity_confinement, gravity_scale, cfl_radius;
+} cn_fluid_material;
+
+typedef struct cn_collider_geometry {  /* GpuColliderGeometryData, 48 B */
+    float shape_params[4];             /* sphere: r; box: half extents; capsule: r, half height */
+    float local_position[4];
+    float local_orientation[4];
+} cn_collider_geometry;
+
+typedef struct cn_collider_broadphase { /* GpuColliderBroadPhaseData, 32 B */
+    uint32_t owner_body, shape_type, environment_index, collision_layer;
+    uint32_t collision_mask, enabled_flag, reserved1, reserved2;
+} cn_collider_broadphase;
+
+enum { CN_COLLIDER_SPHERE = 0, CN_COLLIDER_BOX = 1, CN_COLLIDER_CAPSULE = 2 };
+enum { CN_BODY_STATIC = 0, CN_BODY_KINEMATIC = 1, CN_BODY_DYNAMIC = 2 };
+enum { CN_PARTICLE_SOLID = 0, CN_PARTICLE_FLUID = 1 };
+enum { CN_OWNER_NONE = 0, CN_OWNER_SOFT_BODY = 1, CN_OWNER_FLUID = 2, CN_OWNER_STRAND = 3,
+       CN_OWNER_RIGID_BODY = 4, CN_OWNER_CLOTH = 5 };
+#define CN_PHASE_GROUP_MASK 0x7fffffffu
+#define CN_PHASE_SELF_COLLIDE 0x80000000u
+
+/* ------------------------------------------------------------------------ */
+/* World SoA: the host arrays PhysicsSolver::syncWorldState uploads           */
+/* (reference: physics_types.h:696-920, physics_scene_gpu_state.cpp:2348).    */
+/* All pointers are host pointers; arrays of length 0 may be NULL.            */
+/* ------------------------------------------------------------------------ */
+typedef struct cn_world_soa {
+    /* particles */
+    uint32_t particle_count;
+    float *positions_inv_mass;      /* float4[N] xyz + invMass (read; written back on blocking readback) */
+    float *velocities;              /* float4[N] */
+    const float *radii;             /* float[N] */
+    const uint32_t *kinds;          /* uint[N]  CN_PARTICLE_* */
+    const uint32_t *metadata;       /* uint4[N] (environment, phase, collision layer, collision mask) */
+    const uint32_t *material_indices;       /* uint[N] -> contact_materials */
+    const uint32_t *fluid_material_indices; /* uint[N] -> fluid_materials (0xffffffff for solids) */
+    const uint32_t *owner_types;    /* uint[N] CN_OWNER_* */
+    const uint32_t *owner_indices;  /* uint[N] */
+    const uint32_t *adjacency_offsets; /* uint[N] */
+    const uint32_t *adjacency_counts;  /* uint[N] */
+    const uint32_t *adjacency_indices; /* uint[adjacency_index_count] */
+    uint32_t adjacency_index_count;
+    float particle_grid_cell_size;  /* PhysicsWorld::particleGridCellSize() */
+
+    uint32_t contact_material_count;
+    const float *contact_materials; /* float4[] (friction, restitution, damping, staticFriction) */
+    uint32_t fluid_material_count;
+    const cn_fluid_material *fluid_materials;
+
+    /* soft constraints */
+    uint32_t edge_count;         const cn_soft_edge *edges;
+    uint32_t bend_count;         const cn_soft_bend *bends;
+    uint32_t dihedral_count;     const cn_cloth_dihedral *dihedrals;
+    uint32_t tet_count;          const cn_soft_tet *tets;
+    uint32_t strand_segment_count; const cn_strand_segment *strand_segments;
+    float *strand_segment_orientations; /* float4[segments]: GpuStrandSegmentState */
+    uint32_t strand_joint_count; const cn_strand_joint *strand_joints;
+    uint32_t strand_distance_count; const cn_strand_distance *strand_distances;
+
+    /* rigid bodies (static and kinematic bodies take part in the particle path) */
+    uint32_t rigid_body_count;
+    const float *body_positions_inv_mass;   /* float4[B] */
+    const float *body_orientations;         /* float4[B] */
+    const float *body_linear_velocities;    /* float4[B] */
+    const float *body_angular_velocities;   /* float4[B] */
+    const float *body_scales;               /* float4[B] */
+    const float *body_inverse_inertia;      /* float4[B] */
+    const uint32_t *body_types;             /* uint[B] CN_BODY_* */
+    const float *body_kinematic_target_positions;    /* float4[B] */
+    const float *body_kinematic_target_orientations; /* float4[B] */
+    const uint32_t *body_kinematic_target_flags;     /* uint[B] bit0 = target enabled */
+    const uint32_t *body_collider_ranges;   /* uint2[B] (offset, count) into body_collider_indices */
+    const uint32_t *body_collider_indices;  /* uint[body_collider_index_count] */
+    uint32_t body_collider_index_count;
+
+    uint32_t collider_count;
+    const cn_collider_geometry *collider_geometry;
+    const cn_collider_broadphase *collider_broadphase;
+    const float *collider_materials;        /* float4[C] (friction, restitution, 0, staticFriction) */
+} cn_world_soa;
+
+/* ------------------------------------------------------------------------ */
+/* Host authoring (PhysicsWorld mirror): regular-grid soft bodies, fluid      */
+/* lattices, cloth grids, strands, rigid bodies and colliders.  The world     */
+/* derives the same state the reference derives at upload time.              */
+/* ------------------------------------------------------------------------ */
+typedef struct cn_world cn_world;
+
+typedef struct cn_transform { float position[3]; float rotation[4]; float scale[3]; } cn_transform;
+
+typedef struct cn_contact_material_desc {  /* ParticleContactMaterialDesc */
+    float friction, restitution, damping, static_friction; /* static < 0 reuses friction */
+} cn_contact_material_desc;
+
+typedef struct cn_soft_body_grid_desc {   /* SoftBodyState with a RegularGrid source */
+    float size[3];
+    float target_particle_spacing;
+    cn_transform rest_transform;
+    float particle_mass;          /* 1.0 */
+    float particle_radius;        /* 0.125 */
+    float edge_compliance;
+    float volume_compliance;
+    uint32_t self_collision_enabled;
+    uint32_t environment_index;
+    uint32_t collision_layer, collision_mask;
+    cn_contact_material_desc material;
+    const uint32_t *static_particle_indices; uint32_t static_particle_count;
+} cn_soft_body_grid_desc;
+
+typedef struct cn_fluid_grid_desc {       /* FluidState with a RegularGrid source */
+    float size[3];
+    float target_particle_spacing;
+    cn_transform rest_transform;
+    float particle_mass;
+    float particle_radius;
+    float viscosity, cohesion, surface_tension, vorticity_confinement, gravity_scale, cfl_coefficient;
+    uint32_t environment_index;
+    uint32_t collision_layer, collision_mask;
+    cn_contact_material_desc material;
+} cn_fluid_grid_desc;
+
+typedef struct cn_cloth_grid_desc {       /* ClothState with a rectangular grid source */
+    uint32_t resolution[2];
+    float size[2];
+    cn_transform rest_transform;
+    float particle_mass, particle_radius;
+    float structural_compliance, bend_compliance;
+    uint32_t self_collision_enabled, environment_index, collision_layer, collision_mask;
+    cn_contact_material_desc material;
+    const uint32_t *static_particle_indices; uint32_t static_particle_count;
+} cn_cloth_grid_desc;
+
+typedef struct cn_strand_desc {           /* StrandState */
+    const float *rest_positions; uint32_t rest_position_count; /* float3[] */
+    float particle_mass, particle_radius;
+    float stretch_shear_compliance, bend_compliance, twist_compliance, distance_compliance;
+    uint32_t self_collision_enabled, environment_index, collision_layer, collision_mask;
+    cn_contact_material_desc material;
+    const uint32_t *static_particle_indices; uint32_t static_particle_count;
+} cn_strand_desc;
+
+typedef struct cn_rigid_body_desc {
+    uint32_t body_type;           /* CN_BODY_* */
+    float position[3];
+    float orientation[4];
+    float scale[3];
+    float mass;
+    float inverse_inertia_local[3];
+} cn_rigid_body_desc;
+
+typedef struct cn_collider_desc {         /* ColliderState */
+    uint32_t body;
+    uint32_t shape_type;          /* CN_COLLIDER_* */
+    float shape_params[4];
+    float local_position[3];
+    float local_orientation[4];
+    uint32_t enabled;
+    float friction, static_friction, restitution;
+    uint32_t environment_index, collision_layer, collision_mask;
+} cn_collider_desc;
+
+CN_API void cn_soft_body_grid_desc_defaults(cn_soft_body_grid_desc *d);
+CN_API void cn_fluid_grid_desc_defaults(cn_fluid_grid_desc *d);
+CN_API void cn_cloth_grid_desc_defaults(cn_cloth_grid_desc *d);
+CN_API void cn_strand_desc_defaults(cn_strand_desc *d);
+CN_API void cn_rigid_body_desc_defaults(cn_rigid_body_desc *d);
+CN_API void cn_collider_desc_defaults(cn_collider_desc *d);
+
+CN_API cn_status cn_world_create(cn_world **out_world);
+CN_API void cn_world_destroy(cn_world *world);
+/* reference: PhysicsWorld::upsertSoftBody + buildRegularGridSource (soft_body_authoring.cpp:81-176) */
+CN_API cn_status cn_world_add_soft_body_grid(cn_world *w, const cn_soft_body_grid_desc *d, uint32_t *out_index);
+/* reference: prepareFluidStateForInsert (physics_world.cpp:6857-6891), toFluidSolverMaterial (:191-262) */
+CN_API cn_status cn_world_add_fluid_grid(cn_world *w, const cn_fluid_grid_desc *d, uint32_t *out_index);
+CN_API cn_status cn_world_add_cloth_grid(cn_world *w, const cn_cloth_grid_desc *d, uint32_t *out_index);
+CN_API cn_status cn_world_add_strand(cn_world *w, const cn_strand_desc *d, uint32_t *out_index);
+CN_API cn_status cn_world_add_rigid_body(cn_world *w, const cn_rigid_body_desc *d, uint32_t *out_body);
+CN_API cn_status cn_world_add_collider(cn_world *w, const cn_collider_desc *d, uint32_t *out_collider);
+/* Packs the SoA (PhysicsWorld::ensureDerivedStateUpToDate).  Pointers stay valid until the
+ * next mutating call on the world; positions and velocities may be edited in place. */
+CN_API cn_status cn_world_get_soa(cn_world *w, cn_world_soa *out);
+
+/* ------------------------------------------------------------------------ */
+/* Solver                                                                    */
+/* ------------------------------------------------------------------------ */
+typedef struct cn_solver cn_solver;
+
+/* Device-side counters read by cn_solver_validate_meta
+ * (reference: GpuParticleNeighborMeta, physics_particle_types.hlsli:49-64, and
+ *  PhysicsSolver::validateGpuMetaBlocking, physics_solver.cpp:1403-1491). */
+typedef struct cn_meta {
+    uint32_t particle_rigid_candidate_count;
+    uint32_t required_particle_rigid_candidate_count;
+    uint32_t particle_rigid_candidate_overflow;
+    uint32_t particle_particle_candidate_count;
+    uint32_t required_particle_particle_candidate_count;
+    uint32_t particle_particle_candidate_overflow;
+    uint32_t fluid_boundary_candidate_overflow;  /* more boundary colliders than the per-particle mask holds */
+    uint32_t active_particle_rigid_contact_count;
+    uint32_t active_particle_contact_count;
+    uint32_t fluid_neighbor_truncations;         /* particles whose neighbour list hit max_fluid_neighborhood */
+    uint32_t device_wait_timeouts;               /* bounded spins that gave up (sort look-back) */
+    uint32_t reserved[5];
+} cn_meta;
+
+/* Non-owning device pointers (reference: PhysicsGpuSceneView,
+ * include/physics/physics_gpu_scene_view.h:114-262).  Valid until
+ * binding_generation changes. */
+typedef struct cn_scene_view {
+    void *positions_inv_mass;   /* float4[N] */
+    void *previous_positions;   /* float4[N] */
+    void *velocities;           /* float4[N] */
+    void *radii;                /* float[N]  */
+    void *kinds;                /* uint[N]   */
+    void *edges; void *bends; void *dihedrals; void *tets;
+    void *strand_segments; void *strand_joints; void *strand_distances; void *strand_segment_states;
+    uint32_t particle_count, edge_count, bend_count, dihedral_count, tet_count;
+    uint32_t strand_segment_count, strand_joint_count, strand_distance_count;
+    uint64_t binding_generation;
+    int32_t device;
+    uint32_t reserved;
+} cn_scene_view;
+
+/* PhysicsSolver(GpuDevice&, const PhysicsSolverDesc&) + initialize().  device: CUDA ordinal. */
+CN_API cn_status cn_solver_create(const cn_solver_desc *desc, int device, cn_solver **out_solver);
+CN_API void cn_solver_destroy(cn_solver *solver);
+/* PhysicsSolver::syncWorldState: uploads the SoA, grows capacities, builds incidence tables. */
+CN_API cn_status cn_solver_sync_world(cn_solver *solver, const cn_world_soa *world);
+/* PhysicsSolver::step with FrameContext::deltaSeconds = frame_dt.  stream: cudaStream_t or NULL
+ * (the solver's own stream).  With enable_blocking_readback the call waits and writes x and v back
+ * into the synced host arrays. */
+CN_API cn_status cn_solver_step(cn_solver *solver, float frame_dt, void *stream);
+/* Runs `steps` frames back to back on the device (no per-frame host work when the scene is
+ * capture-stable: the whole frame is one CUDA graph launch). */
+CN_API cn_status cn_solver_step_many(cn_solver *solver, float frame_dt, uint32_t steps, void *stream);
+/* PhysicsSolver::validateGpuMetaBlocking: waits for the device and reads the counters. */
+CN_API cn_status cn_solver_validate_meta(cn_solver *solver, cn_meta *out_meta);
+CN_API cn_status cn_solver_set_gravity(cn_solver *solver, float x, float y, float z);
+/* Kinematic tool pose for the next step (reference: g_RigidBodyKinematicTarget*). */
+CN_API cn_status cn_solver_set_kinematic_target(cn_solver *solver, uint32_t body,
+                                                const float position[3], const float orientation[4]);
+/* PhysicsSolver::gpuSceneView / softPositionsInvMassSharedBuffer: the native device buffers. */
+CN_API cn_status cn_solver_scene_view(cn_solver *solver, cn_scene_view *out_view);
+/* Blocking copy of device particle state to host (readbackPredictedParticleStateBlocking).
+ * Any pointer may be NULL. */
+CN_API cn_status cn_solver_read_particles(cn_solver *solver, float *positions_inv_mass,
+                                          float *velocities, float *previous_positions,
+                                          uint32_t count);
+/* Uploads particle positions and velocities only (host -> device, on the solver stream). */
+CN_API cn_status cn_solver_write_particles(cn_solver *solver, const float *positions_inv_mass,
+                                           const float *velocities, uint32_t count);
+CN_API cn_status cn_solver_read_strand_orientations(cn_solver *solver, float *orientations,
+                                                    uint32_t count);
+
+/* Debug switches (no reference counterpart; all off by default):
+ *  CN_DEBUG_KEEP_FLUID_DELTA   keep the last iteration's packed fluid delta for cn_solver_debug_read;
+ *  CN_DEBUG_POST_UPDATE_NEIGHBORS  rebuild fluid neighbour lists after the velocity update, as the
+ *      reference does (physics_solver.cpp:1262-1268); the lists feed only vorticity confinement and
+ *      render anisotropy, so the default schedule skips the rebuild;
+ *  CN_DEBUG_FORCE_BROADPHASE   run the cell-key sort even when no consumer in the scene needs it
+ *      (the reference always runs it once any contact family is enabled). */
+enum { CN_DEBUG_KEEP_FLUID_DELTA = 1, CN_DEBUG_POST_UPDATE_NEIGHBORS = 2, CN_DEBUG_FORCE_BROADPHASE = 4 };
+CN_API cn_status cn_solver_set_debug(cn_solver *solver, uint32_t flags);
+
+/* Per-kernel-group device times of the last replayed frame (no reference counterpart: the
+ * reference records no GPU timestamps).  cn_solver_set_timing(1) records a CUDA event pair around
+ * each kernel group of the captured frame; cn_solver_kernel_times sums them by group name. */
+typedef struct cn_kernel_time {
+    char name[32];
+    float milliseconds;   /* summed over the group's launches in the last frame */
+    uint32_t launches;    /* instances of the group in one frame */
+} cn_kernel_time;
+CN_API cn_status cn_solver_set_timing(cn_solver *solver, uint32_t enable);
+CN_API cn_status cn_solver_kernel_times(cn_solver *solver, cn_kernel_time *out, uint32_t capacity,
+                                        uint32_t *count);
+/* Nodes of the captured frame graph: kernel launches and all nodes (launch count per frame). */
+CN_API cn_status cn_solver_graph_stats(cn_solver *solver, uint32_t *kernel_nodes, uint32_t *nodes);
+
+/* Intermediate buffers of the last substep, for parity checks.  Each is converted to the
+ * reference's layout and indexing (particle order, not cell order). */
+typedef enum cn_debug_buffer {
+    CN_DEBUG_CELL_ENTRIES = 0,     /* int4[N]: cellX, cellY, cellZ, cellKey (GpuParticleBroadPhaseEntry) */
+    CN_DEBUG_SORTED_KEYS = 1,      /* uint2[N]: (cellKey, elementIdx) after the stable sort */
+    CN_DEBUG_CELL_RANGES = 2,      /* uint4[nextPow2(2N)]: compacted (key, start, end, 0), rest key=0xffffffff */
+    CN_DEBUG_FLUID_NEIGHBOR_COUNTS = 3, /* uint[N] */
+    CN_DEBUG_FLUID_NEIGHBORS = 4,  /* uint[N * max_fluid_neighborhood]: neighbour particle indices */
+    CN_DEBUG_FLUID_CONSTRAINTS = 5,/* float4[N]: surface normal xyz, density constraint w */
+    CN_DEBUG_FLUID_DELTA = 6,      /* float4[N]: last packed delta + interaction weight */
+    CN_DEBUG_RIGID_CONTACTS = 7    /* 64 B records of the last iteration's particle-rigid contacts */
+} cn_debug_buffer;
+/* Copies at most capacity_bytes; *out_bytes receives the full size of the buffer. */
+CN_API cn_status cn_solver_debug_read(cn_solver *solver, cn_debug_buffer which, void *dst,
+                                      size_t capacity_bytes, size_t *out_bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CN_PHYSICS_H */

@@ -1,0 +1,2085 @@
+// cn_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of CRESSim-Neo's particle physics substep, used as the parity
+// checker for the CUDA path and as the timed CPU baseline ("port").  Nothing in
+// the product links, loads or calls this file; only tests/, __graft_entry__.smoke()
+// and bench.py's CPU-baseline leg do.
+//
+// Each pass restates one HLSL compute kernel of the reference and cites it
+// (paths are relative to the reference project root).  Passes run in the order
+// PhysicsSolver::step dispatches them (src/physics/physics_solver.cpp:336-1401).
+// Arithmetic is float32 with the reference's expression order; build with
+// -ffp-contract=off so no multiply-add is fused.
+//
+// Parity status: the reference's GPU path (Vulkan/D3D12 through Diligent + DXC)
+// cannot be built or run here, and its tests pin no numeric output of the
+// substep, so this restatement is pinned only by the known answers the
+// reference's tests hold for scene authoring (regular-grid counts) and by the
+// golden fixtures generated from it under tests/golden/ ("parity unpinned" for
+// substep numerics).
+//
+// Deliberate restatement choices (documented where they occur):
+//  * rigid-BVH traversal order is replaced by "moving colliders, then static
+//    colliders, each ascending by collider index"; the candidate SETS are the
+//    reference's (leaf AABB = union of previous/predicted collider AABB +/- 0.05).
+//  * float atomics are accumulated in contact-index order (the reference's order
+//    is whatever the GPU schedules).
+#include "../include/cn_physics.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr float kEps = 1.0e-6f;            // physics_base.hlsli:7
+constexpr uint32_t kInvalid = 0xffffffffu; // physics_base.hlsli:6
+constexpr uint32_t kRigidDedup = 16u;      // physics_particle_types.hlsli:23
+constexpr uint32_t kColliderCap = 64u;     // physics_particle_types.hlsli:24
+constexpr float kBroadPhaseMargin = 0.05f; // physics_shape_common.hlsli:10
+
+struct f3 { float x, y, z; };
+struct f4 { float x, y, z, w; };
+inline f3 mk(float x, float y, float z) { return f3{x, y, z}; }
+inline f3 xyz(const f4 &v) { return f3{v.x, v.y, v.z}; }
+inline f4 mk4(f3 v, float w) { return f4{v.x, v.y, v.z, w}; }
+inline f3 operator+(f3 a, f3 b) { return f3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline f3 operator-(f3 a, f3 b) { return f3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline f3 operator-(f3 a) { return f3{-a.x, -a.y, -a.z}; }
+inline f3 operator*(f3 a, float s) { return f3{a.x * s, a.y * s, a.z * s}; }
+inline f3 operator*(float s, f3 a) { return f3{s * a.x, s * a.y, s * a.z}; }
+inline f3 operator*(f3 a, f3 b) { return f3{a.x * b.x, a.y * b.y, a.z * b.z}; }
+inline f3 operator/(f3 a, float s) { return f3{a.x / s, a.y / s, a.z / s}; }
+inline f3 &operator+=(f3 &a, f3 b) { a = a + b; return a; }
+inline f3 &operator-=(f3 &a, f3 b) { a = a - b; return a; }
+inline f4 operator+(f4 a, f4 b) { return f4{a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; }
+inline f4 operator*(f4 a, float s) { return f4{a.x * s, a.y * s, a.z * s, a.w * s}; }
+inline float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline float dot4(f4 a, f4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+inline f3 cross(f3 a, f3 b)
+{
+    return f3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+inline float length(f3 v) { return std::sqrt(dot(v, v)); }
+inline float saturate(float v) { return std::min(std::max(v, 0.0f), 1.0f); }
+inline f3 fabs3(f3 v) { return f3{std::fabs(v.x), std::fabs(v.y), std::fabs(v.z)}; }
+inline f3 clamp3(f3 v, f3 lo, f3 hi)
+{
+    return f3{std::min(std::max(v.x, lo.x), hi.x), std::min(std::max(v.y, lo.y), hi.y),
+              std::min(std::max(v.z, lo.z), hi.z)};
+}
+inline f3 min3(f3 a, f3 b) { return f3{std::min(a.x, b.x), std::min(a.y, b.y), std::min(a.z, b.z)}; }
+inline f3 max3(f3 a, f3 b) { return f3{std::max(a.x, b.x), std::max(a.y, b.y), std::max(a.z, b.z)}; }
+inline f3 lerp3(f3 a, f3 b, float t) { return a + (b - a) * t; }
+
+// physics_math.hlsli:6-20
+inline f3 SafeNormalize(f3 v, f3 fallback)
+{
+    const float l2 = dot(v, v);
+    if (l2 <= kEps) return fallback;
+    return v * (1.0f / std::sqrt(l2));
+}
+inline f4 QNormalize(f4 q)
+{
+    const float l2 = dot4(q, q);
+    if (l2 <= kEps) return f4{0, 0, 0, 1};
+    return q * (1.0f / std::sqrt(l2));
+}
+inline f4 QConj(f4 q) { return f4{-q.x, -q.y, -q.z, q.w}; }
+// physics_math.hlsli:24-31
+inline f4 QMul(f4 a, f4 b)
+{
+    return f4{a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y,
+              a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
+              a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w,
+              a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z};
+}
+// physics_math.hlsli:33-37
+inline f3 QRotate(f4 q, f3 v)
+{
+    const f3 qv = xyz(q);
+    const f3 t = 2.0f * cross(qv, v);
+    return v + q.w * t + cross(qv, t);
+}
+inline f3 QInvRotate(f4 q, f3 v) { return QRotate(QConj(q), v); }
+// physics_math.hlsli:71-89
+inline f3 AngularVelocityFromQuaternionDelta(f4 prev, f4 cur, float dt)
+{
+    if (dt <= kEps) return f3{0, 0, 0};
+    f4 d = QMul(QNormalize(cur), QConj(QNormalize(prev)));
+    if (d.w < 0.0f) d = f4{-d.x, -d.y, -d.z, -d.w};
+    const f3 im = xyz(d);
+    const float l2 = dot(im, im);
+    if (l2 <= kEps) return im * (2.0f / dt);
+    const float l = std::sqrt(l2);
+    const float angle = 2.0f * std::atan2(l, d.w);
+    return im * (angle / (l * dt));
+}
+
+// physics_shape_common.hlsli:24-42
+inline float SphereRadius(f4 p, f4 s)
+{
+    const f3 a = fabs3(xyz(s));
+    return p.x * std::max(a.x, std::max(a.y, a.z));
+}
+inline f3 BoxHalfExtents(f4 p, f4 s) { return xyz(p) * fabs3(xyz(s)); }
+inline void CapsuleSegment(f3 pos, f4 q, f4 p, f4 s, f3 &a, f3 &b, float &r)
+{
+    const f3 as = fabs3(xyz(s));
+    r = p.x * std::max(as.x, as.z);
+    const float hh = p.y * as.y;
+    const f3 axis = QRotate(q, f3{0, 1, 0});
+    a = pos - axis * hh;
+    b = pos + axis * hh;
+}
+// physics_shape_common.hlsli:49-73
+inline void ComputeBodyAabb(uint32_t shape, f3 pos, f4 q, f4 p, f4 s, f3 &mn, f3 &mx)
+{
+    f3 e{0, 0, 0};
+    if (shape == CN_COLLIDER_SPHERE) {
+        const float r = SphereRadius(p, s);
+        e = f3{r, r, r};
+    } else if (shape == CN_COLLIDER_BOX) {
+        const f3 h = BoxHalfExtents(p, s);
+        e = fabs3(QRotate(q, f3{1, 0, 0})) * h.x + fabs3(QRotate(q, f3{0, 1, 0})) * h.y +
+            fabs3(QRotate(q, f3{0, 0, 1})) * h.z;
+    } else {
+        f3 a, b;
+        float r = 0.0f;
+        CapsuleSegment(pos, q, p, s, a, b, r);
+        const f3 axis = fabs3(QRotate(q, f3{0, 1, 0}));
+        e = axis * (0.5f * length(b - a)) + f3{r, r, r};
+    }
+    mn = pos - e;
+    mx = pos + e;
+}
+// physics_shape_common.hlsli:75-80
+inline bool AabbOverlaps(f3 minA, f3 maxA, f3 minB, f3 maxB)
+{
+    return minA.x <= maxB.x && maxA.x >= minB.x && minA.y <= maxB.y && maxA.y >= minB.y &&
+           minA.z <= maxB.z && maxA.z >= minB.z;
+}
+// physics_shape_common.hlsli:97-105
+inline f3 ClosestFaceNormalLocal(f3 lp, f3 h)
+{
+    const f3 d = h - fabs3(lp);
+    if (d.x <= d.y && d.x <= d.z) return f3{lp.x >= 0.0f ? 1.0f : -1.0f, 0, 0};
+    if (d.y <= d.z) return f3{0, lp.y >= 0.0f ? 1.0f : -1.0f, 0};
+    return f3{0, 0, lp.z >= 0.0f ? 1.0f : -1.0f};
+}
+
+// physics_rigid_solver_shared.hlsli:8-68
+inline f3 MulWorldInvInertia(f3 inv, f4 q, f3 v)
+{
+    const f3 ax = QRotate(q, f3{1, 0, 0});
+    const f3 ay = QRotate(q, f3{0, 1, 0});
+    const f3 az = QRotate(q, f3{0, 0, 1});
+    return ax * (inv.x * dot(ax, v)) + ay * (inv.y * dot(ay, v)) + az * (inv.z * dot(az, v));
+}
+inline float ContactEffectiveMass(float invMass, f3 inv, f4 q, f3 r, f3 dir)
+{
+    if (invMass <= kEps) return 0.0f;
+    const f3 am = MulWorldInvInertia(inv, q, cross(r, dir));
+    return invMass + dot(cross(am, r), dir);
+}
+inline f3 CombineContactMaterial(f4 a, f4 b)
+{
+    const float friction = std::sqrt(std::max(0.0f, a.x) * std::max(0.0f, b.x));
+    const float restitution = std::max(std::max(0.0f, a.y), std::max(0.0f, b.y));
+    const float stat = std::sqrt(std::max(0.0f, a.w) * std::max(0.0f, b.w));
+    return f3{friction, restitution, stat};
+}
+inline f3 ProjectOntoTangent(f3 v, f3 n) { return v - n * dot(v, n); }
+
+// physics_fluid_common.hlsli:17-41
+inline float SpikyW(float d, float h)
+{
+    if (d >= h) return 0.0f;
+    const float om = 1.0f - d / h;
+    const float h3 = h * h * h;
+    const float k = 15.0f / (3.14159265359f * h3);
+    return k * om * om;
+}
+inline float SpikyDW(float d, float h)
+{
+    if (d <= kEps || d >= h) return 0.0f;
+    const float om = 1.0f - d / h;
+    const float h3 = h * h * h;
+    const float k = 15.0f / (3.14159265359f * h3);
+    return -2.0f * k * om / h;
+}
+inline f3 SpikyGrad(f3 delta, float d, float h)
+{
+    if (d <= kEps || d >= h) return f3{0, 0, 0};
+    const float dw = SpikyDW(d, h);
+    return dw * (delta / d);
+}
+inline float CohesionW(float d, float h, float c1, float c2)
+{
+    if (d <= kEps || d >= h) return 0.0f;
+    const float q = d / h;
+    return c1 * q * q * q + c2 * q * q - 1.0f;
+}
+
+// physics_particle_grid.hlsli:4-10
+inline uint32_t CellKey(int gx, int gy, int gz)
+{
+    uint32_t seed = uint32_t(gx) * 73856093u;
+    seed ^= uint32_t(gy) * 19349663u;
+    seed ^= uint32_t(gz) * 83492791u;
+    return seed;
+}
+
+uint32_t nextPow2(uint32_t v)
+{
+    if (v <= 1u) return 1u;
+    --v;
+    v |= v >> 1; v |= v >> 2; v |= v >> 4; v |= v >> 8; v |= v >> 16;
+    return v + 1u;
+}
+
+struct Range { uint32_t start, count; };
+struct Incident { uint32_t index, slot; };
+struct CellRange { uint32_t key, start, end, pad; };
+struct RigidContact {   // GpuParticleRigidContact, physics_particle_types.hlsli:74-83
+    uint32_t particle, body, collider, active;
+    f4 normalPenetration, rigidLocalPoint, material;
+};
+struct ParticleContact { // GpuParticleContact
+    uint32_t a, b, active, pad;
+    f4 normalPenetration, material;
+};
+
+template <class T> void copyArr(std::vector<T> &dst, const void *src, size_t n)
+{
+    dst.resize(n);
+    if (n && src) std::memcpy(dst.data(), src, n * sizeof(T));
+}
+
+void buildIncidence(uint32_t n, const std::vector<std::vector<Incident>> &refs,
+                    std::vector<Range> &ranges, std::vector<Incident> &flat)
+{
+    // physics_scene_gpu_state.cpp:3255-3420: per-particle lists in ascending constraint order.
+    ranges.assign(n, Range{0, 0});
+    flat.clear();
+    for (uint32_t i = 0; i < n; ++i) {
+        ranges[i].start = uint32_t(flat.size());
+        ranges[i].count = uint32_t(refs[i].size());
+        flat.insert(flat.end(), refs[i].begin(), refs[i].end());
+    }
+}
+
+} // namespace
+
+struct cno_solver {
+    cn_solver_desc desc{};
+    uint32_t N = 0;
+    // particles
+    std::vector<f4> x, xprev, v;
+    std::vector<float> radii;
+    std::vector<uint32_t> kinds, matIdx, fluidMatIdx, ownerTypes, ownerIdx;
+    std::vector<uint32_t> meta; // uint4 per particle
+    std::vector<uint32_t> adjOff, adjCnt, adjIdx;
+    float cellSize = 1.0f;
+    std::vector<f4> contactMaterials;
+    std::vector<cn_fluid_material> fluidMaterials;
+    // constraints
+    std::vector<cn_soft_edge> edges;
+    std::vector<cn_soft_bend> bends;
+    std::vector<cn_cloth_dihedral> dihedrals;
+    std::vector<cn_soft_tet> tets;
+    std::vector<cn_strand_segment> segs;
+    std::vector<f4> segOrient;
+    std::vector<cn_strand_joint> joints;
+    std::vector<cn_strand_distance> dists;
+    // incidence
+    std::vector<Range> edgeRanges, bendRanges, tetRanges, segRanges, segJointRanges;
+    std::vector<Incident> edgeInc, bendInc, tetInc, segInc, segJointInc;
+    // rigid
+    uint32_t B = 0, C = 0;
+    std::vector<f4> bodyPos, bodyRot, bodyLin, bodyAng, bodyScale, bodyInvInertia;
+    std::vector<uint32_t> bodyType, bodyKinFlags;
+    std::vector<f4> bodyKinPos, bodyKinRot;
+    std::vector<uint32_t> bodyColRanges, bodyColIdx;
+    std::vector<cn_collider_geometry> colGeo;
+    std::vector<cn_collider_broadphase> colBp;
+    std::vector<f4> colMat;
+    std::vector<f4> prevBodyPos, prevBodyRot, predBodyPos, predBodyRot, predBodyLin, predBodyAng;
+    std::vector<f3> colAabbMin, colAabbMax;
+    std::vector<uint32_t> colliderQueryOrder; // moving colliders first, then static
+    uint32_t activeMovingCount = 0;
+    // transient state
+    std::vector<int32_t> entries;     // int4 per particle (cx, cy, cz, key)
+    std::vector<uint32_t> sortedKey, sortedIdx;
+    std::vector<CellRange> cellRanges;
+    uint32_t cellRangeCapacity = 0;
+    std::vector<uint32_t> nbrCount, nbrList;
+    std::vector<f4> fluidDelta, fluidNormalC, fluidDx;
+    std::vector<std::vector<uint32_t>> boundaryCand; // collider indices per particle (fluids)
+    std::vector<std::pair<uint32_t, uint32_t>> rigidPairs;    // (particle, body)
+    std::vector<std::pair<uint32_t, uint32_t>> particlePairs; // (a, b)
+    uint32_t requiredRigidPairs = 0, requiredParticlePairs = 0;
+    std::vector<RigidContact> rigidContacts, activeRigidContacts;
+    std::vector<ParticleContact> particleContacts, activeParticleContacts;
+    std::vector<f4> posCorr, velCorr;
+    std::vector<float> edgeLambda, bendLambda, tetLambda, distLambda;
+    std::vector<f4> segLambda, jointLambda;
+    std::vector<f4> edgeCorr;      // 2 per edge
+    std::vector<f4> bendCorr;      // 4 per bend/dihedral
+    std::vector<f4> tetCorr;       // 4 per tet
+    std::vector<f4> segCorr;       // 3 per segment
+    std::vector<f4> jointCorr;     // 5 per joint
+    std::vector<f4> distCorr;      // 2 per distance
+    uint32_t truncations = 0;
+
+    // settings shorthands (physics_solver_config.hlsli:27-62)
+    float slop() const { return desc.contact.slop; }
+};
+
+namespace {
+
+void setupWorld(cno_solver &s, const cn_world_soa &w)
+{
+    s.N = w.particle_count;
+    const uint32_t N = s.N;
+    copyArr(s.x, w.positions_inv_mass, N);
+    copyArr(s.v, w.velocities, N);
+    s.xprev.assign(N, f4{0, 0, 0, 0});
+    for (uint32_t i = 0; i < N; ++i) s.xprev[i] = mk4(xyz(s.x[i]), 0.0f);
+    copyArr(s.radii, w.radii, N);
+    copyArr(s.kinds, w.kinds, N);
+    copyArr(s.meta, w.metadata, size_t(N) * 4);
+    copyArr(s.matIdx, w.material_indices, N);
+    copyArr(s.fluidMatIdx, w.fluid_material_indices, N);
+    copyArr(s.ownerTypes, w.owner_types, N);
+    copyArr(s.ownerIdx, w.owner_indices, N);
+    copyArr(s.adjOff, w.adjacency_offsets, N);
+    copyArr(s.adjCnt, w.adjacency_counts, N);
+    copyArr(s.adjIdx, w.adjacency_indices, w.adjacency_index_count);
+    s.cellSize = w.particle_grid_cell_size;
+    copyArr(s.contactMaterials, w.contact_materials, w.contact_material_count);
+    copyArr(s.fluidMaterials, w.fluid_materials, w.fluid_material_count);
+    copyArr(s.edges, w.edges, w.edge_count);
+    copyArr(s.bends, w.bends, w.bend_count);
+    copyArr(s.dihedrals, w.dihedrals, w.dihedral_count);
+    copyArr(s.tets, w.tets, w.tet_count);
+    copyArr(s.segs, w.strand_segments, w.strand_segment_count);
+    copyArr(s.segOrient, w.strand_segment_orientations, w.strand_segment_count);
+    copyArr(s.joints, w.strand_joints, w.strand_joint_count);
+    copyArr(s.dists, w.strand_distances, w.strand_distance_count);
+    s.B = w.rigid_body_count;
+    s.C = w.collider_count;
+    copyArr(s.bodyPos, w.body_positions_inv_mass, s.B);
+    copyArr(s.bodyRot, w.body_orientations, s.B);
+    copyArr(s.bodyLin, w.body_linear_velocities, s.B);
+    copyArr(s.bodyAng, w.body_angular_velocities, s.B);
+    copyArr(s.bodyScale, w.body_scales, s.B);
+    copyArr(s.bodyInvInertia, w.body_inverse_inertia, s.B);
+    copyArr(s.bodyType, w.body_types, s.B);
+    copyArr(s.bodyKinPos, w.body_kinematic_target_positions, s.B);
+    copyArr(s.bodyKinRot, w.body_kinematic_target_orientations, s.B);
+    copyArr(s.bodyKinFlags, w.body_kinematic_target_flags, s.B);
+    copyArr(s.bodyColRanges, w.body_collider_ranges, size_t(s.B) * 2);
+    copyArr(s.bodyColIdx, w.body_collider_indices, w.body_collider_index_count);
+    copyArr(s.colGeo, w.collider_geometry, s.C);
+    copyArr(s.colBp, w.collider_broadphase, s.C);
+    copyArr(s.colMat, w.collider_materials, s.C);
+
+    // Incidence tables (physics_scene_gpu_state.cpp:3273-3420).
+    std::vector<std::vector<Incident>> refs(N);
+    for (uint32_t e = 0; e < s.edges.size(); ++e) {
+        if (s.edges[e].particle_a < N) refs[s.edges[e].particle_a].push_back({e, 0});
+        if (s.edges[e].particle_b < N) refs[s.edges[e].particle_b].push_back({e, 1});
+    }
+    buildIncidence(N, refs, s.edgeRanges, s.edgeInc);
+    refs.assign(N, {});
+    for (uint32_t b = 0; b < s.bends.size(); ++b) {
+        const uint32_t p[3] = {s.bends[b].particle0, s.bends[b].particle1, s.bends[b].particle2};
+        for (uint32_t k = 0; k < 3; ++k)
+            if (p[k] < N) refs[p[k]].push_back({b, k});
+    }
+    const uint32_t off = uint32_t(s.bends.size());
+    for (uint32_t d = 0; d < s.dihedrals.size(); ++d) {
+        const cn_cloth_dihedral &h = s.dihedrals[d];
+        const uint32_t p[4] = {h.edge_particle0, h.edge_particle1, h.opposite_particle0,
+                               h.opposite_particle1};
+        for (uint32_t k = 0; k < 4; ++k)
+            if (p[k] < N) refs[p[k]].push_back({off + d, k});
+    }
+    buildIncidence(N, refs, s.bendRanges, s.bendInc);
+    refs.assign(N, {});
+    for (uint32_t t = 0; t < s.tets.size(); ++t)
+        for (uint32_t k = 0; k < 4; ++k) {
+            const uint32_t p = s.tets[t].particle_indices[k];
+            if (p < N) refs[p].push_back({t, k});
+        }
+    buildIncidence(N, refs, s.tetRanges, s.tetInc);
+    refs.assign(N, {});
+    for (uint32_t g = 0; g < s.segs.size(); ++g) {
+        if (s.segs[g].particle_a < N) refs[s.segs[g].particle_a].push_back({g, 0});
+        if (s.segs[g].particle_b < N) refs[s.segs[g].particle_b].push_back({g, 1});
+    }
+    buildIncidence(N, refs, s.segRanges, s.segInc);
+    std::vector<std::vector<Incident>> srefs(s.segs.size());
+    for (uint32_t j = 0; j < s.joints.size(); ++j) {
+        if (s.joints[j].segment_a >= s.segs.size() || s.joints[j].segment_b >= s.segs.size())
+            continue;
+        srefs[s.joints[j].segment_a].push_back({j, 0});
+        srefs[s.joints[j].segment_b].push_back({j, 1});
+    }
+    buildIncidence(uint32_t(s.segs.size()), srefs, s.segJointRanges, s.segJointInc);
+
+    // Transient buffers start zeroed (fresh allocations).
+    s.entries.assign(size_t(N) * 4, 0);
+    s.sortedKey.assign(N, 0);
+    s.sortedIdx.assign(N, 0);
+    s.cellRangeCapacity = nextPow2(std::max<uint32_t>(N * 2u, 1u));
+    s.cellRanges.assign(s.cellRangeCapacity, CellRange{kInvalid, 0, 0, 0});
+    s.nbrCount.assign(N, 0);
+    s.nbrList.assign(size_t(N) * s.desc.max_fluid_neighborhood, 0);
+    s.fluidDelta.assign(N, f4{0, 0, 0, 0});
+    s.fluidNormalC.assign(N, f4{0, 0, 0, 0});
+    s.fluidDx.assign(N, f4{0, 0, 0, 0});
+    s.boundaryCand.assign(N, {});
+    s.posCorr.assign(N, f4{0, 0, 0, 0});
+    s.velCorr.assign(N, f4{0, 0, 0, 0});
+    s.edgeLambda.assign(s.edges.size(), 0.0f);
+    s.bendLambda.assign(s.bends.size() + s.dihedrals.size(), 0.0f);
+    s.tetLambda.assign(s.tets.size(), 0.0f);
+    s.distLambda.assign(s.dists.size(), 0.0f);
+    s.segLambda.assign(s.segs.size(), f4{0, 0, 0, 0});
+    s.jointLambda.assign(s.joints.size(), f4{0, 0, 0, 0});
+    s.edgeCorr.assign(s.edges.size() * 2, f4{0, 0, 0, 0});
+    s.bendCorr.assign((s.bends.size() + s.dihedrals.size()) * 4, f4{0, 0, 0, 0});
+    s.tetCorr.assign(s.tets.size() * 4, f4{0, 0, 0, 0});
+    s.segCorr.assign(s.segs.size() * 3, f4{0, 0, 0, 0});
+    s.jointCorr.assign(s.joints.size() * 5, f4{0, 0, 0, 0});
+    s.distCorr.assign(s.dists.size() * 2, f4{0, 0, 0, 0});
+    s.prevBodyPos = s.bodyPos; s.prevBodyRot = s.bodyRot;
+    s.predBodyPos = s.bodyPos; s.predBodyRot = s.bodyRot;
+    s.predBodyLin = s.bodyLin; s.predBodyAng = s.bodyAng;
+    s.colAabbMin.assign(s.C, f3{0, 0, 0});
+    s.colAabbMax.assign(s.C, f3{0, 0, 0});
+}
+
+// ---------------------------------------------------------------------------
+// Rigid predict (static / kinematic branches): physics_rigid_predict.cs.hlsl:20-81,
+// then the collider world AABBs: physics_rigid_update_world_aabbs.cs.hlsl:23-100.
+// ---------------------------------------------------------------------------
+void predictRigid(cno_solver &s, float dt)
+{
+    const f3 g{s.desc.gravity[0], s.desc.gravity[1], s.desc.gravity[2]};
+    for (uint32_t b = 0; b < s.B; ++b) {
+        const f4 p = s.bodyPos[b];
+        const f4 q = QNormalize(s.bodyRot[b]);
+        f4 lin = s.bodyLin[b], ang = s.bodyAng[b];
+        const bool kinEnabled = (s.bodyKinFlags[b] & 1u) != 0u;
+        const f4 kq = QNormalize(s.bodyKinRot[b]);
+        s.prevBodyPos[b] = p;
+        s.prevBodyRot[b] = q;
+        if (s.bodyType[b] == CN_BODY_STATIC) {
+            s.predBodyPos[b] = p; s.predBodyRot[b] = q;
+            s.predBodyLin[b] = f4{0, 0, 0, 0}; s.predBodyAng[b] = f4{0, 0, 0, 0};
+            continue;
+        }
+        if (s.bodyType[b] == CN_BODY_KINEMATIC) {
+            const f3 pp = kinEnabled ? xyz(s.bodyKinPos[b]) : xyz(p);
+            const f4 pq = kinEnabled ? kq : q;
+            const f3 l = (pp - xyz(p)) / std::max(dt, kEps);
+            const f3 a = AngularVelocityFromQuaternionDelta(q, pq, std::max(dt, kEps));
+            s.predBodyPos[b] = mk4(pp, p.w); s.predBodyRot[b] = pq;
+            s.predBodyLin[b] = mk4(l, lin.w); s.predBodyAng[b] = mk4(a, ang.w);
+            continue;
+        }
+        // Dynamic bodies are integrated but receive no particle feedback in this restatement.
+        f3 l = xyz(lin) + g * dt;
+        s.predBodyPos[b] = mk4(xyz(p) + l * dt, p.w);
+        s.predBodyRot[b] = q;
+        s.predBodyLin[b] = mk4(l, lin.w);
+        s.predBodyAng[b] = ang;
+    }
+    s.activeMovingCount = 0;
+    std::vector<uint32_t> moving, stat;
+    for (uint32_t c = 0; c < s.C; ++c) {
+        const cn_collider_broadphase &bp = s.colBp[c];
+        const uint32_t ob = bp.owner_body;
+        if (ob >= s.B || bp.enabled_flag == 0u) {
+            s.colAabbMin[c] = f3{0, 0, 0}; s.colAabbMax[c] = f3{0, 0, 0};
+            continue;
+        }
+        const f4 sc = s.bodyScale[ob];
+        const cn_collider_geometry &cg = s.colGeo[c];
+        const f4 params{cg.shape_params[0], cg.shape_params[1], cg.shape_params[2], cg.shape_params[3]};
+        const f3 lp = f3{cg.local_position[0], cg.local_position[1], cg.local_position[2]} * xyz(sc);
+        const f4 lq = QNormalize(f4{cg.local_orientation[0], cg.local_orientation[1],
+                                    cg.local_orientation[2], cg.local_orientation[3]});
+        const f4 bq = QNormalize(s.predBodyRot[ob]);
+        const f4 pbq = QNormalize(s.prevBodyRot[ob]);
+        const f3 cp = xyz(s.predBodyPos[ob]) + QRotate(bq, lp);
+        const f4 cq = QNormalize(QMul(bq, lq));
+        const f3 pcp = xyz(s.prevBodyPos[ob]) + QRotate(pbq, lp);
+        const f4 pcq = QNormalize(QMul(pbq, lq));
+        f3 mn, mx, pmn, pmx;
+        ComputeBodyAabb(bp.shape_type, cp, cq, params, sc, mn, mx);
+        ComputeBodyAabb(bp.shape_type, pcp, pcq, params, sc, pmn, pmx);
+        mn = min3(mn, pmn);
+        mx = max3(mx, pmx);
+        s.colAabbMin[c] = mn - f3{kBroadPhaseMargin, kBroadPhaseMargin, kBroadPhaseMargin};
+        s.colAabbMax[c] = mx + f3{kBroadPhaseMargin, kBroadPhaseMargin, kBroadPhaseMargin};
+        if (s.bodyType[ob] == CN_BODY_STATIC) stat.push_back(c);
+        else moving.push_back(c);
+    }
+    s.activeMovingCount = uint32_t(moving.size());
+    s.colliderQueryOrder = moving;
+    s.colliderQueryOrder.insert(s.colliderQueryOrder.end(), stat.begin(), stat.end());
+}
+
+// physics_soft_predict.cs.hlsl:12-47
+void predictSoft(cno_solver &s, float dt)
+{
+    const f3 g{s.desc.gravity[0], s.desc.gravity[1], s.desc.gravity[2]};
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        const f4 pim = s.x[i];
+        s.xprev[i] = mk4(xyz(pim), 0.0f);
+        if (pim.w <= kEps) {
+            s.v[i] = f4{0, 0, 0, 0};
+            continue;
+        }
+        f3 vel = xyz(s.v[i]);
+        float gs = 1.0f;
+        if (s.kinds[i] == CN_PARTICLE_FLUID) gs = s.fluidMaterials[s.fluidMatIdx[i]].gravity_scale;
+        vel = vel + g * (dt * gs);
+        const f3 pp = xyz(pim) + vel * dt;
+        s.v[i] = mk4(vel, 0.0f);
+        s.x[i] = mk4(pp, pim.w);
+    }
+}
+
+// physics_particle_build_broad_phase_entries.cs.hlsl:9-35 + _keys.cs.hlsl:8-23 +
+// the stable 32-pass split radix sort (physics_pass_dispatcher.cpp:3963-4057) +
+// cell ranges (mark_cell_range_starts / clear_cell_ranges / build_cell_ranges).
+void broadphase(cno_solver &s)
+{
+    const uint32_t N = s.N;
+    const float safe = std::max(s.cellSize, 1.0e-4f);
+    const float inv = 1.0f / safe;
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        const f3 p = xyz(s.x[i]);
+        const int gx = int(std::floor(p.x * inv));
+        const int gy = int(std::floor(p.y * inv));
+        const int gz = int(std::floor(p.z * inv));
+        s.entries[4 * i + 0] = gx;
+        s.entries[4 * i + 1] = gy;
+        s.entries[4 * i + 2] = gz;
+        s.entries[4 * i + 3] = int32_t(CellKey(gx, gy, gz));
+    }
+    std::vector<uint64_t> kv(N);
+    for (uint32_t i = 0; i < N; ++i) kv[i] = (uint64_t(uint32_t(s.entries[4 * i + 3])) << 32) | i;
+    // Sorting (key, index) lexicographically is the permutation of a stable sort by key.
+    std::sort(kv.begin(), kv.end());
+    for (uint32_t i = 0; i < N; ++i) {
+        s.sortedKey[i] = uint32_t(kv[i] >> 32);
+        s.sortedIdx[i] = uint32_t(kv[i] & 0xffffffffu);
+    }
+    s.cellRangeCapacity = nextPow2(std::max<uint32_t>(N * 2u, 1u));
+    s.cellRanges.assign(s.cellRangeCapacity, CellRange{kInvalid, 0, 0, 0});
+    uint32_t rangeIndex = 0;
+    for (uint32_t i = 0; i < N; ++i) {
+        if (i != 0 && s.sortedKey[i - 1] == s.sortedKey[i]) continue;
+        uint32_t end = i + 1;
+        while (end < N && s.sortedKey[end] == s.sortedKey[i]) ++end;
+        if (rangeIndex < s.cellRangeCapacity)
+            s.cellRanges[rangeIndex] = CellRange{s.sortedKey[i], i, end, 0};
+        ++rangeIndex;
+    }
+}
+
+// physics_fluid_neighbor_build.hlsli:6-46 (identical to FindCellRange in
+// physics_particle_broad_phase_query.hlsli:8-48)
+inline CellRange FindCellRange(const cno_solver &s, uint32_t key)
+{
+    const CellRange missing{kInvalid, 0, 0, 0};
+    if (s.cellRangeCapacity == 0) return missing;
+    uint32_t lo = 0, hi = s.cellRangeCapacity;
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        if (s.cellRanges[mid].key < key) lo = mid + 1u;
+        else hi = mid;
+    }
+    if (lo < s.cellRangeCapacity && s.cellRanges[lo].key == key) return s.cellRanges[lo];
+    return missing;
+}
+
+// physics_particle_broad_phase_query.hlsli:50-117
+bool IsAdjacent(const cno_solver &s, uint32_t p, uint32_t c)
+{
+    const uint32_t o = s.adjOff[p], n = s.adjCnt[p];
+    for (uint32_t i = 0; i < n; ++i)
+        if (s.adjIdx[o + i] == c) return true;
+    return false;
+}
+bool ValidParticleParticleCandidate(const cno_solver &s, uint32_t p, f3 pos, float r, uint32_t kind,
+                                    uint32_t env, uint32_t phase, uint32_t layer, uint32_t mask,
+                                    uint32_t other)
+{
+    if (other <= p) return false;
+    const uint32_t *om = &s.meta[4 * other];
+    if (om[0] != env) return false;
+    if ((mask & om[2]) == 0u || (om[3] & layer) == 0u) return false;
+    const uint32_t ok = s.kinds[other];
+    if (kind == CN_PARTICLE_FLUID && ok == CN_PARTICLE_FLUID) return false;
+    if (kind == CN_PARTICLE_SOLID && ok == CN_PARTICLE_SOLID &&
+        (phase & CN_PHASE_GROUP_MASK) == (om[1] & CN_PHASE_GROUP_MASK)) {
+        const bool a = (phase & CN_PHASE_SELF_COLLIDE) != 0u;
+        const bool b = (om[1] & CN_PHASE_SELF_COLLIDE) != 0u;
+        if (!a || !b || IsAdjacent(s, p, other)) return false;
+    }
+    const f3 op = xyz(s.x[other]);
+    const float cr = r + s.radii[other];
+    const f3 d = op - pos;
+    return dot(d, d) <= cr * cr;
+}
+
+// count/finalize/emit_particle_particle_candidates.cs.hlsl
+void buildParticleParticleCandidates(cno_solver &s)
+{
+    const uint32_t N = s.N;
+    std::vector<std::vector<uint32_t>> per(N);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t ii = 0; ii < int64_t(N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        const int32_t *e = &s.entries[4 * i];
+        const f3 pos = xyz(s.x[i]);
+        const float r = s.radii[i];
+        const uint32_t *m = &s.meta[4 * i];
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const CellRange rg = FindCellRange(s, CellKey(e[0] + dx, e[1] + dy, e[2] + dz));
+                    if (rg.key == kInvalid) continue;
+                    for (uint32_t si = rg.start; si < rg.end; ++si) {
+                        const uint32_t c = s.sortedIdx[si];
+                        const int32_t *ce = &s.entries[4 * c];
+                        if (ce[0] != e[0] + dx || ce[1] != e[1] + dy || ce[2] != e[2] + dz) continue;
+                        if (ValidParticleParticleCandidate(s, i, pos, r, s.kinds[i], m[0], m[1], m[2],
+                                                           m[3], c))
+                            per[i].push_back(c);
+                    }
+                }
+    }
+    const uint32_t cap = std::max<uint32_t>(N * 8u, 64u);
+    s.particlePairs.clear();
+    uint64_t required = 0;
+    for (uint32_t i = 0; i < N; ++i) {
+        for (uint32_t c : per[i]) {
+            if (required < cap) s.particlePairs.push_back({i, c});
+            ++required;
+        }
+    }
+    s.requiredParticlePairs = uint32_t(required);
+}
+
+// count/finalize/emit_particle_rigid_candidates.cs.hlsl:113-151 (BVH replaced by the
+// collider query order; TryAppendRigidBody dedup cache of 16 bodies kept).
+void buildParticleRigidCandidates(cno_solver &s)
+{
+    const uint32_t N = s.N;
+    std::vector<std::vector<uint32_t>> per(N);
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        const f3 p = xyz(s.x[i]);
+        const float r = s.radii[i];
+        const f3 qmin = p - f3{r, r, r}, qmax = p + f3{r, r, r};
+        const uint32_t *m = &s.meta[4 * i];
+        const bool proxyOwner = s.ownerTypes[i] == CN_OWNER_RIGID_BODY;
+        uint32_t seen[kRigidDedup];
+        uint32_t seenCount = 0;
+        for (uint32_t k = 0; k < s.colliderQueryOrder.size(); ++k) {
+            const uint32_t c = s.colliderQueryOrder[k];
+            const bool isMoving = k < s.activeMovingCount;
+            if (isMoving && s.activeMovingCount == 0) continue;
+            if (!AabbOverlaps(qmin, qmax, s.colAabbMin[c], s.colAabbMax[c])) continue;
+            const cn_collider_broadphase &bp = s.colBp[c];
+            const uint32_t b = bp.owner_body;
+            if (proxyOwner && b == s.ownerIdx[i]) continue;
+            const uint32_t bt = s.bodyType[b];
+            if (!(bp.enabled_flag != 0u && bp.environment_index == m[0] &&
+                  (m[3] & bp.collision_layer) != 0u && (bp.collision_mask & m[2]) != 0u &&
+                  (s.kinds[i] == CN_PARTICLE_SOLID || bt == CN_BODY_DYNAMIC) &&
+                  s.bodyColRanges[2 * b + 1] > 0u))
+                continue;
+            bool fresh = true;
+            for (uint32_t q = 0; q < seenCount; ++q)
+                if (seen[q] == b) { fresh = false; break; }
+            if (!fresh) continue;
+            if (seenCount < kRigidDedup) seen[seenCount++] = b;
+            per[i].push_back(b);
+        }
+    }
+    const uint32_t cap = std::max<uint32_t>(N * 8u, 64u);
+    s.rigidPairs.clear();
+    uint64_t required = 0;
+    for (uint32_t i = 0; i < N; ++i)
+        for (uint32_t b : per[i]) {
+            if (required < cap) s.rigidPairs.push_back({i, b});
+            ++required;
+        }
+    s.requiredRigidPairs = uint32_t(required);
+}
+
+// count/emit_fluid_boundary_candidates.cs.hlsl (per-particle candidate lists)
+void buildFluidBoundaryCandidates(cno_solver &s)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        s.boundaryCand[i].clear();
+        if (s.kinds[i] != CN_PARTICLE_FLUID) continue;
+        const f3 p = xyz(s.x[i]);
+        const float pr = std::max(s.radii[i], 0.0f);
+        const cn_fluid_material &fm = s.fluidMaterials[s.fluidMatIdx[i]];
+        const float support = std::max(fm.smoothing_radius, pr);
+        const float reuse = std::max(std::max(fm.cfl_radius, pr), support);
+        const float qr = support + reuse;
+        const f3 qmin = p - f3{qr, qr, qr}, qmax = p + f3{qr, qr, qr};
+        const uint32_t *m = &s.meta[4 * i];
+        for (uint32_t k = 0; k < s.colliderQueryOrder.size(); ++k) {
+            const uint32_t c = s.colliderQueryOrder[k];
+            if (!AabbOverlaps(qmin, qmax, s.colAabbMin[c], s.colAabbMax[c])) continue;
+            const cn_collider_broadphase &bp = s.colBp[c];
+            const uint32_t bt = s.bodyType[bp.owner_body];
+            if (bp.enabled_flag != 0u && bp.environment_index == m[0] && bt != CN_BODY_DYNAMIC &&
+                (m[3] & bp.collision_layer) != 0u && (bp.collision_mask & m[2]) != 0u)
+                s.boundaryCand[i].push_back(c);
+        }
+    }
+}
+
+// physics_fluid_boundary_common.hlsli:11-83
+bool FluidBoundaryContactInfo(const cno_solver &s, uint32_t c, f3 pos, float &sd, f3 &n)
+{
+    sd = 0.0f;
+    n = f3{0, 1, 0};
+    const cn_collider_broadphase &bp = s.colBp[c];
+    if (bp.enabled_flag == 0u) return false;
+    const uint32_t b = bp.owner_body;
+    const f3 bpos = xyz(s.predBodyPos[b]);
+    const f4 bq = QNormalize(s.predBodyRot[b]);
+    const f4 sc = s.bodyScale[b];
+    const cn_collider_geometry &cg = s.colGeo[c];
+    const f3 cwp = bpos + QRotate(bq, f3{cg.local_position[0], cg.local_position[1], cg.local_position[2]});
+    const f4 cwq = QNormalize(QMul(bq, QNormalize(f4{cg.local_orientation[0], cg.local_orientation[1],
+                                                      cg.local_orientation[2], cg.local_orientation[3]})));
+    const f4 sp{cg.shape_params[0], cg.shape_params[1], cg.shape_params[2], cg.shape_params[3]};
+    if (bp.shape_type == CN_COLLIDER_SPHERE) {
+        const f3 d = pos - cwp;
+        const float dist = length(d);
+        const float r = SphereRadius(sp, sc);
+        n = dist > kEps ? (d / dist) : f3{0, 1, 0};
+        sd = dist - r;
+    } else if (bp.shape_type == CN_COLLIDER_BOX) {
+        const f3 he = BoxHalfExtents(sp, sc);
+        const f3 lp = QInvRotate(cwq, pos - cwp);
+        const f3 cl = clamp3(lp, -he, he);
+        const f3 d = lp - cl;
+        const float dl = length(d);
+        if (dl > kEps) {
+            n = QRotate(cwq, d / dl);
+            sd = dl;
+        } else {
+            const f3 ds = he - fabs3(lp);
+            n = QRotate(cwq, ClosestFaceNormalLocal(lp, he));
+            sd = -std::min(ds.x, std::min(ds.y, ds.z));
+        }
+    } else {
+        f3 a, b2;
+        float cr = 0.0f;
+        CapsuleSegment(cwp, cwq, sp, sc, a, b2, cr);
+        const f3 seg = b2 - a;
+        const float l2 = dot(seg, seg);
+        float t = 0.0f;
+        if (l2 > kEps) t = saturate(dot(pos - a, seg) / l2);
+        const f3 cl = lerp3(a, b2, t);
+        const f3 d = pos - cl;
+        const float dist = length(d);
+        n = dist > kEps ? (d / dist) : f3{0, 1, 0};
+        sd = dist - cr;
+    }
+    return true;
+}
+bool FluidGhostDelta(const cno_solver &s, uint32_t c, f3 pos, float h, f3 &ghost)
+{
+    ghost = f3{0, 0, 0};
+    float sd = 0.0f;
+    f3 n{0, 1, 0};
+    if (!FluidBoundaryContactInfo(s, c, pos, sd, n)) return false;
+    if (sd < 0.0f || sd >= h) return false;
+    ghost = n * (2.0f * sd);
+    return true;
+}
+
+// physics_fluid_build_neighbors.cs.hlsl:21-147
+void buildFluidNeighbors(cno_solver &s, uint32_t iter)
+{
+    const uint32_t maxN = s.desc.max_fluid_neighborhood;
+    uint32_t trunc = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : trunc)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        if (s.kinds[i] != CN_PARTICLE_FLUID) continue;
+        const f4 self = s.x[i];
+        if (self.w <= kEps) continue;
+        if (maxN == 0) { s.nbrCount[i] = 0; continue; }
+        const f3 sd = iter > 0 ? xyz(s.fluidDelta[i]) : f3{0, 0, 0};
+        const f3 sp = xyz(self) + sd;
+        const float h = std::max(s.fluidMaterials[s.fluidMatIdx[i]].smoothing_radius, 1.0e-4f);
+        const uint32_t *m = &s.meta[4 * i];
+        const int32_t *e = &s.entries[4 * i];
+        uint32_t count = 0;
+        bool truncated = false;
+        uint32_t *out = &s.nbrList[size_t(i) * maxN];
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int tx = e[0] + dx, ty = e[1] + dy, tz = e[2] + dz;
+                    const CellRange rg = FindCellRange(s, CellKey(tx, ty, tz));
+                    if (rg.key == kInvalid) continue;
+                    for (uint32_t si = rg.start; si < rg.end; ++si) {
+                        const uint32_t c = s.sortedIdx[si];
+                        const int32_t *ce = &s.entries[4 * c];
+                        if (ce[0] != tx || ce[1] != ty || ce[2] != tz) continue;
+                        // ShouldProcessFluidNeighbor (physics_fluid_neighbor_build.hlsli:48-69)
+                        if (c == i || s.kinds[c] != CN_PARTICLE_FLUID) continue;
+                        const uint32_t *om = &s.meta[4 * c];
+                        if (om[0] != m[0]) continue;
+                        if (!((m[3] & om[2]) != 0u && (om[3] & m[2]) != 0u)) continue;
+                        const f4 np = s.x[c];
+                        if (np.w <= kEps) continue;
+                        const f3 nd = iter > 0 ? xyz(s.fluidDelta[c]) : f3{0, 0, 0};
+                        const f3 delta = sp - (xyz(np) + nd);
+                        if (length(delta) >= h) continue;
+                        if (count >= maxN) { truncated = true; continue; }
+                        out[count++] = c;
+                    }
+                }
+        s.nbrCount[i] = count;
+        trunc += truncated ? 1u : 0u;
+    }
+    s.truncations += trunc;
+}
+
+// physics_fluid_compute_density_lambda.cs.hlsl:26-115
+void fluidDensity(cno_solver &s, uint32_t iter)
+{
+    const uint32_t maxN = s.desc.max_fluid_neighborhood;
+    const float bds = s.desc.fluid.boundary_density_scale;
+    const float maxUnder = s.desc.fluid.max_under_density_ratio;
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        if (s.kinds[i] != CN_PARTICLE_FLUID) { s.fluidNormalC[i] = f4{0, 0, 0, 0}; continue; }
+        const f4 self = s.x[i];
+        if (self.w <= kEps) { s.fluidNormalC[i] = f4{0, 0, 0, 0}; continue; }
+        const f3 sdl = iter > 0 ? xyz(s.fluidDelta[i]) : f3{0, 0, 0};
+        const f3 sp = xyz(self) + sdl;
+        const cn_fluid_material &fm = s.fluidMaterials[s.fluidMatIdx[i]];
+        const float rho0 = std::max(fm.rest_density, 1.0f);
+        const float scale = fm.density_constraint_scale;
+        const float h = std::max(fm.smoothing_radius, 1.0e-4f);
+        const float st = std::max(fm.surface_tension, 0.0f);
+        float density = 0.0f;
+        f3 normal{0, 0, 0};
+        const uint32_t cnt = s.nbrCount[i];
+        const uint32_t *lst = &s.nbrList[size_t(i) * maxN];
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t c = lst[k];
+            const f3 nd = iter > 0 ? xyz(s.fluidDelta[c]) : f3{0, 0, 0};
+            const f3 delta = sp - (xyz(s.x[c]) + nd);
+            const float dist = length(delta);
+            if (dist >= h) continue;
+            density += SpikyW(dist, h);
+            if (st > kEps) normal += SpikyGrad(delta, dist, h);
+        }
+        for (uint32_t c : s.boundaryCand[i]) {
+            f3 ghost;
+            if (!FluidGhostDelta(s, c, sp, h, ghost)) continue;
+            const float dist = length(ghost);
+            if (dist >= h) continue;
+            density += SpikyW(dist, h) * bds;
+        }
+        const float C = std::max(density - rho0, -rho0 * std::max(maxUnder, 0.0f)) * scale;
+        if (st > kEps) {
+            normal = normal * st;
+            s.fluidNormalC[i] = mk4(normal, C);
+        } else {
+            s.fluidNormalC[i] = f4{0, 0, 0, C};
+        }
+    }
+}
+
+// physics_fluid_compute_delta_positions.cs.hlsl:27-157
+void fluidDeltaPositions(cno_solver &s, uint32_t iter, float dt)
+{
+    const uint32_t maxN = s.desc.max_fluid_neighborhood;
+    const float coef = s.desc.fluid.constraint_relaxation;
+    const float bdelta = s.desc.fluid.boundary_delta_scale;
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        if (s.kinds[i] != CN_PARTICLE_FLUID) { s.fluidDx[i] = f4{0, 0, 0, 0}; continue; }
+        const f4 self = s.x[i];
+        if (self.w <= kEps) { s.fluidDx[i] = f4{0, 0, 0, 0}; continue; }
+        const f3 sdl = iter > 0 ? xyz(s.fluidDelta[i]) : f3{0, 0, 0};
+        const f3 sp = xyz(self) + sdl;
+        const f4 snc = s.fluidNormalC[i];
+        const float sC = snc.w;
+        const cn_fluid_material &fm = s.fluidMaterials[s.fluidMatIdx[i]];
+        const float h = std::max(fm.smoothing_radius, 1.0e-4f);
+        const float cohesion = dt * std::max(fm.cohesion, 0.0f);
+        const float visc = dt * std::max(fm.viscosity, 0.0f);
+        const float st = std::max(fm.surface_tension, 0.0f);
+        const float cfl = std::max(fm.cfl_radius, 0.0f);
+        f3 dp{0, 0, 0};
+        float weight = 0.0f;
+        const f3 sn = st > kEps ? xyz(snc) : f3{0, 0, 0};
+        const uint32_t cnt = s.nbrCount[i];
+        const uint32_t *lst = &s.nbrList[size_t(i) * maxN];
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t c = lst[k];
+            const f4 np = s.x[c];
+            if (np.w <= kEps) continue;
+            const f3 nd = iter > 0 ? xyz(s.fluidDelta[c]) : f3{0, 0, 0};
+            const f3 npos = xyz(np) + nd;
+            const f3 delta = sp - npos;
+            const float dist = length(delta);
+            if (dist >= h || dist <= kEps) continue;
+            const f4 nnc = s.fluidNormalC[c];
+            const f3 nij = delta / dist;
+            const float dw = SpikyDW(dist, h);
+            f3 pd = -0.5f * (sC + nnc.w) * dw * nij;
+            if (s.fluidMatIdx[i] == s.fluidMatIdx[c]) {
+                const f3 rel = sdl - nd;
+                if (cohesion > kEps) pd -= nij * (cohesion * CohesionW(dist, h, fm.cohesion1, fm.cohesion2));
+                if (visc > kEps) {
+                    const float vs = 1.0f - (1.0f / (1.0f + visc * SpikyW(dist, h)));
+                    pd -= vs * rel;
+                }
+                if (cfl > kEps) {
+                    const float proj = dot(rel, nij);
+                    if (proj < -cfl) pd -= nij * (proj + cfl) * 0.5f;
+                }
+                if (st > kEps) pd -= dt * (sn - xyz(nnc));
+            }
+            dp += pd;
+            weight += 1.0f;
+        }
+        f3 bd{0, 0, 0};
+        for (uint32_t c : s.boundaryCand[i]) {
+            f3 ghost;
+            if (!FluidGhostDelta(s, c, sp, h, ghost)) continue;
+            const float dist = length(ghost);
+            if (dist <= kEps || dist >= h) continue;
+            const f3 nij = ghost / dist;
+            const float dw = SpikyDW(dist, h);
+            bd += -std::max(sC, 0.0f) * dw * nij;
+        }
+        bd = bd * bdelta;
+        const f3 packed = dp * coef + bd;
+        s.fluidDx[i] = mk4(packed, weight);
+    }
+}
+
+// physics_fluid_apply_delta_positions.cs.hlsl:11-31 + physics_fluid_clamp_boundary.cs.hlsl:23-80
+void fluidApplyAndClamp(cno_solver &s, uint32_t iter)
+{
+    const float relax = s.desc.fluid.position_relaxation;
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        if (s.kinds[i] != CN_PARTICLE_FLUID) continue;
+        const f4 dw = s.fluidDx[i];
+        const float weight = std::max(dw.w * relax, 1.0f);
+        const f3 d = xyz(dw) / weight;
+        const f3 prev = iter > 0 ? xyz(s.fluidDelta[i]) : f3{0, 0, 0};
+        s.fluidDelta[i] = mk4(prev + d, 0.0f);
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        if (s.kinds[i] != CN_PARTICLE_FLUID) continue;
+        const f3 base = xyz(s.x[i]);
+        const float pr = std::max(s.radii[i], 0.0f);
+        f3 cur = base + xyz(s.fluidDelta[i]);
+        for (uint32_t sweep = 0; sweep < 2u; ++sweep) {
+            bool changed = false;
+            for (uint32_t c : s.boundaryCand[i]) {
+                float sd = 0.0f;
+                f3 n{0, 1, 0};
+                if (!FluidBoundaryContactInfo(s, c, cur, sd, n)) continue;
+                if (sd >= pr) continue;
+                cur += n * (pr - sd);
+                changed = true;
+            }
+            if (!changed) break;
+        }
+        s.fluidDelta[i] = mk4(cur - base, 0.0f);
+    }
+}
+
+// ---- XPBD families (Jacobi: solve writes per-constraint records, apply gathers) ----
+// physics_soft_solve_edge_constraints.cs.hlsl:10-74
+void solveEdges(cno_solver &s, float dt)
+{
+    const float relax = s.desc.soft.internal_relaxation;
+#pragma omp parallel for schedule(static)
+    for (int64_t ee = 0; ee < int64_t(s.edges.size()); ++ee) {
+        const uint32_t e = uint32_t(ee);
+        const cn_soft_edge &ed = s.edges[e];
+        f4 &cA = s.edgeCorr[2 * e], &cB = s.edgeCorr[2 * e + 1];
+        cA = f4{0, 0, 0, 0}; cB = f4{0, 0, 0, 0};
+        if (ed.enabled == 0u) continue;
+        const f4 a = s.x[ed.particle_a], b = s.x[ed.particle_b];
+        const float wA = a.w, wB = b.w, wSum = wA + wB;
+        if (wSum <= kEps) continue;
+        const f3 delta = xyz(b) - xyz(a);
+        const float l2 = dot(delta, delta);
+        if (l2 <= kEps) continue;
+        const float len = std::sqrt(l2);
+        const f3 gA = -delta / len;
+        const f3 gB = -gA;
+        const float compliance = std::max(ed.compliance, 0.0f);
+        const float alpha = compliance / std::max(dt * dt, kEps);
+        const float Cv = len - ed.rest_length;
+        const float lambda = s.edgeLambda[e];
+        const float den = wSum + alpha;
+        if (den <= kEps) continue;
+        const float dl = -(Cv + alpha * lambda) / den;
+        s.edgeLambda[e] = lambda + dl;
+        cA = mk4(wA * dl * gA * relax, 0.0f);
+        cB = mk4(wB * dl * gB * relax, 0.0f);
+    }
+}
+// physics_soft_apply_edge_corrections.cs.hlsl:9-35 (and the strand distance apply, which
+// indexes its correction records through the strand-segment incidence table,
+// physics_strand_apply_distance_corrections.cs.hlsl:9-38)
+void applyPairCorrections(cno_solver &s, const std::vector<Range> &ranges,
+                          const std::vector<Incident> &inc, const std::vector<f4> &corr)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        const f4 p = s.x[i];
+        if (p.w <= kEps) continue;
+        const Range r = ranges[i];
+        f3 total{0, 0, 0};
+        for (uint32_t k = 0; k < r.count; ++k) {
+            const Incident &ref = inc[r.start + k];
+            total += ref.slot == 0u ? xyz(corr[2 * ref.index]) : xyz(corr[2 * ref.index + 1]);
+        }
+        s.x[i] = mk4(xyz(p) + total, p.w);
+    }
+}
+// physics_soft_apply_tet_corrections.cs.hlsl:9-50, physics_soft_apply_bend_corrections.cs.hlsl:9-51
+void applyQuadCorrections(cno_solver &s, const std::vector<Range> &ranges,
+                          const std::vector<Incident> &inc, const std::vector<f4> &corr)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        const f4 p = s.x[i];
+        if (p.w <= kEps) continue;
+        const Range r = ranges[i];
+        f3 total{0, 0, 0};
+        for (uint32_t k = 0; k < r.count; ++k) {
+            const Incident &ref = inc[r.start + k];
+            const uint32_t slot = ref.slot > 3u ? 3u : ref.slot;
+            total += xyz(corr[4 * ref.index + slot]);
+        }
+        s.x[i] = mk4(xyz(p) + total, p.w);
+    }
+}
+// physics_soft_solve_tet_constraints.cs.hlsl:15-87
+void solveTets(cno_solver &s, float dt)
+{
+    const float relax = s.desc.soft.internal_relaxation;
+#pragma omp parallel for schedule(static)
+    for (int64_t tt = 0; tt < int64_t(s.tets.size()); ++tt) {
+        const uint32_t t = uint32_t(tt);
+        const cn_soft_tet &tet = s.tets[t];
+        const f4 q0 = s.x[tet.particle_indices[0]], q1 = s.x[tet.particle_indices[1]];
+        const f4 q2 = s.x[tet.particle_indices[2]], q3 = s.x[tet.particle_indices[3]];
+        const float w0 = q0.w, w1 = q1.w, w2 = q2.w, w3 = q3.w;
+        if ((w0 + w1 + w2 + w3) <= kEps) continue; // keeps the previous correction record
+        const f3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2), p3 = xyz(q3);
+        const float sv = dot(cross(p1 - p0, p2 - p0), p3 - p0) / 6.0f;
+        const float vs = (sv >= 0.0f) ? 1.0f : -1.0f;
+        const float vol = std::fabs(sv);
+        const float rv = std::max(tet.rest_volume, 0.0f);
+        const float Cv = vol - rv;
+        const f3 g0 = cross(p3 - p1, p2 - p1) * (vs / 6.0f);
+        const f3 g1 = cross(p2 - p0, p3 - p0) * (vs / 6.0f);
+        const f3 g2 = cross(p3 - p0, p1 - p0) * (vs / 6.0f);
+        const f3 g3 = cross(p1 - p0, p2 - p0) * (vs / 6.0f);
+        const float sg = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
+        const float compliance = std::max(tet.compliance, 0.0f);
+        const float alpha = compliance / std::max(dt * dt, kEps);
+        const float lambda = s.tetLambda[t];
+        const float den = sg + alpha;
+        if (den <= kEps) continue;
+        const float dl = -(Cv + alpha * lambda) / den;
+        s.tetLambda[t] = lambda + dl;
+        s.tetCorr[4 * t + 0] = mk4(w0 * dl * g0 * relax, 0.0f);
+        s.tetCorr[4 * t + 1] = mk4(w1 * dl * g1 * relax, 0.0f);
+        s.tetCorr[4 * t + 2] = mk4(w2 * dl * g2 * relax, 0.0f);
+        s.tetCorr[4 * t + 3] = mk4(w3 * dl * g3 * relax, 0.0f);
+    }
+}
+// physics_soft_solve_bend_constraints.cs.hlsl:20-86
+void solveBends(cno_solver &s, float dt)
+{
+    const float relax = s.desc.soft.internal_relaxation;
+#pragma omp parallel for schedule(static)
+    for (int64_t bb = 0; bb < int64_t(s.bends.size()); ++bb) {
+        const uint32_t b = uint32_t(bb);
+        const cn_soft_bend &bd = s.bends[b];
+        f4 *out = &s.bendCorr[4 * b];
+        out[0] = out[1] = out[2] = out[3] = f4{0, 0, 0, 0};
+        const f4 q0 = s.x[bd.particle0], q1 = s.x[bd.particle1], q2 = s.x[bd.particle2];
+        const float w0 = q0.w, w1 = q1.w, w2 = q2.w;
+        if (w0 + w1 + w2 <= kEps) continue;
+        const f3 e0 = xyz(q0) - xyz(q1), e1 = xyz(q2) - xyz(q1);
+        const float l0s = dot(e0, e0), l1s = dot(e1, e1);
+        if (l0s <= kEps || l1s <= kEps) continue;
+        const float l0 = std::sqrt(l0s), l1 = std::sqrt(l1s);
+        const f3 d0 = e0 / l0, d1 = e1 / l1;
+        const float ct = std::min(std::max(dot(d0, d1), -1.0f + 1.0e-4f), 1.0f - 1.0e-4f);
+        const float st2 = std::max(1.0f - ct * ct, 1.0e-8f);
+        const float st = std::sqrt(st2);
+        const float theta = std::acos(ct);
+        const f3 g0 = -(d1 - ct * d0) / std::max(l0 * st, kEps);
+        const f3 g2 = -(d0 - ct * d1) / std::max(l1 * st, kEps);
+        const f3 g1 = -(g0 + g2);
+        const float den = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2);
+        const float alpha = std::max(bd.compliance, 0.0f) / std::max(dt * dt, kEps);
+        if (den + alpha <= kEps) continue;
+        const float Cv = theta - bd.rest_angle;
+        const float lambda = s.bendLambda[b];
+        const float dl = -(Cv + alpha * lambda) / (den + alpha);
+        s.bendLambda[b] = lambda + dl;
+        out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
+        out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
+        out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
+    }
+}
+// physics_cloth_solve_dihedral_constraints.cs.hlsl:20-95
+void solveDihedrals(cno_solver &s, float dt)
+{
+    const float relax = s.desc.soft.internal_relaxation;
+    const uint32_t off = uint32_t(s.bends.size());
+#pragma omp parallel for schedule(static)
+    for (int64_t dd = 0; dd < int64_t(s.dihedrals.size()); ++dd) {
+        const uint32_t d = uint32_t(dd);
+        const uint32_t ci = off + d;
+        const cn_cloth_dihedral &h = s.dihedrals[d];
+        f4 *out = &s.bendCorr[4 * ci];
+        out[0] = out[1] = out[2] = out[3] = f4{0, 0, 0, 0};
+        const f4 e0m = s.x[h.edge_particle0], e1m = s.x[h.edge_particle1];
+        const f4 o0m = s.x[h.opposite_particle0], o1m = s.x[h.opposite_particle1];
+        const f3 p0 = xyz(o0m), p1 = xyz(o1m), p2 = xyz(e0m), p3 = xyz(e1m);
+        const f3 edge = p3 - p2;
+        const float el2 = dot(edge, edge);
+        const f3 rn0 = cross(p2 - p0, p3 - p0);
+        const f3 rn1 = cross(p3 - p1, p2 - p1);
+        const float n0s = dot(rn0, rn0), n1s = dot(rn1, rn1);
+        if (el2 <= kEps || n0s <= kEps || n1s <= kEps) continue;
+        const float el = std::sqrt(el2);
+        const float iel = 1.0f / el;
+        const f3 sn0 = rn0 / n0s, sn1 = rn1 / n1s;
+        const f3 dO0 = el * sn0, dO1 = el * sn1;
+        const f3 dE0 = dot(p0 - p3, edge) * iel * sn0 + dot(p1 - p3, edge) * iel * sn1;
+        const f3 dE1 = dot(p2 - p0, edge) * iel * sn0 + dot(p2 - p1, edge) * iel * sn1;
+        const f3 g0 = -dE0, g1 = -dE1, g2 = -dO0, g3 = -dO1;
+        const f3 n0 = rn0 / std::sqrt(n0s), n1 = rn1 / std::sqrt(n1s);
+        const float theta = std::atan2(dot(edge * iel, cross(n0, n1)),
+                                       std::min(std::max(dot(n0, n1), -1.0f), 1.0f));
+        const float twoPi = 6.283185307179586f;
+        float Cv = theta - h.rest_angle;
+        Cv = Cv - twoPi * std::floor((Cv + 3.141592653589793f) / twoPi);
+        const float w0 = e0m.w, w1 = e1m.w, w2 = o0m.w, w3 = o1m.w;
+        const float den = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
+        const float alpha = std::max(h.compliance, 0.0f) / std::max(dt * dt, kEps);
+        if (den + alpha <= kEps) continue;
+        const float lambda = s.bendLambda[ci];
+        const float dl = -(Cv + alpha * lambda) / (den + alpha);
+        s.bendLambda[ci] = lambda + dl;
+        out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
+        out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
+        out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
+        out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
+    }
+}
+
+// 3x3 helpers of physics_strand_solve_{segment,joint}_constraints.cs.hlsl:12-64
+struct m3 { float m[3][3]; };
+inline m3 outer(f3 a, f3 b)
+{
+    return m3{{{a.x * b.x, a.x * b.y, a.x * b.z}, {a.y * b.x, a.y * b.y, a.y * b.z},
+               {a.z * b.x, a.z * b.y, a.z * b.z}}};
+}
+inline void addScaled(m3 &acc, float s, const m3 &o)
+{
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) acc.m[r][c] = acc.m[r][c] + s * o.m[r][c];
+}
+inline f3 mul3(const m3 &m, f3 v)
+{
+    return f3{dot(f3{m.m[0][0], m.m[0][1], m.m[0][2]}, v), dot(f3{m.m[1][0], m.m[1][1], m.m[1][2]}, v),
+              dot(f3{m.m[2][0], m.m[2][1], m.m[2][2]}, v)};
+}
+inline m3 inverse3(const m3 &M)
+{
+    const float a00 = M.m[0][0], a01 = M.m[0][1], a02 = M.m[0][2];
+    const float a10 = M.m[1][0], a11 = M.m[1][1], a12 = M.m[1][2];
+    const float a20 = M.m[2][0], a21 = M.m[2][1], a22 = M.m[2][2];
+    const float c00 = a11 * a22 - a12 * a21, c01 = a02 * a21 - a01 * a22, c02 = a01 * a12 - a02 * a11;
+    const float c10 = a12 * a20 - a10 * a22, c11 = a00 * a22 - a02 * a20, c12 = a02 * a10 - a00 * a12;
+    const float c20 = a10 * a21 - a11 * a20, c21 = a01 * a20 - a00 * a21, c22 = a00 * a11 - a01 * a10;
+    const float det = a00 * c00 + a01 * c10 + a02 * c20;
+    if (std::fabs(det) <= kEps) return m3{{{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}};
+    const float id = 1.0f / det;
+    return m3{{{c00 * id, c01 * id, c02 * id}, {c10 * id, c11 * id, c12 * id},
+               {c20 * id, c21 * id, c22 * id}}};
+}
+inline float StrandOrientationInvMass(float wA, float wB, float rl)
+{
+    const float ws = std::max(wA + wB, 0.0f);
+    if (ws <= kEps || rl <= kEps) return 0.0f;
+    const float avg = ws * 0.5f;
+    return 12.0f * avg / std::max(rl * rl, kEps);
+}
+// physics_strand_solve_segment_constraints.cs.hlsl:66-147
+void solveSegments(cno_solver &s, float dt)
+{
+    const float relax = s.desc.soft.internal_relaxation;
+#pragma omp parallel for schedule(static)
+    for (int64_t gg = 0; gg < int64_t(s.segs.size()); ++gg) {
+        const uint32_t g = uint32_t(gg);
+        const cn_strand_segment &sg = s.segs[g];
+        const f4 a = s.x[sg.particle_a], b = s.x[sg.particle_b];
+        const float wA = a.w, wB = b.w, wSum = wA + wB;
+        f4 *out = &s.segCorr[3 * g];
+        out[0] = out[1] = out[2] = f4{0, 0, 0, 0};
+        if (wSum <= kEps) continue;
+        const f3 delta = xyz(b) - xyz(a);
+        if (dot(delta, delta) <= kEps) continue;
+        const f4 q = QNormalize(s.segOrient[g]);
+        const f3 axis = QRotate(q, f3{1, 0, 0});
+        const float irl = 1.0f / std::max(sg.rest_length, kEps);
+        const float oim = StrandOrientationInvMass(wA, wB, sg.rest_length);
+        const f3 Cv = delta * irl - axis;
+        const float alpha = std::max(sg.stretch_shear_compliance, 0.0f) / std::max(dt * dt, kEps);
+        const f3 lambda = xyz(s.segLambda[g]);
+        const f3 qv = xyz(q);
+        const float qw = q.w;
+        const f3 gQw = 2.0f * f3{qw, qv.z, -qv.y};
+        const f3 gQx = 2.0f * f3{0.0f, qv.y, qv.z};
+        const f3 gQy = 2.0f * f3{-qv.y, 0.0f, -qw};
+        const f3 gQz = 2.0f * f3{-qv.z, qw, 0.0f};
+        const float dg = wSum * irl * irl + alpha;
+        m3 sys{{{dg, 0, 0}, {0, dg, 0}, {0, 0, dg}}};
+        addScaled(sys, oim, outer(gQx, gQx));
+        addScaled(sys, oim, outer(gQy, gQy));
+        addScaled(sys, oim, outer(gQz, gQz));
+        addScaled(sys, oim, outer(gQw, gQw));
+        const f3 rhs = -(Cv + alpha * lambda);
+        const f3 dl = mul3(inverse3(sys), rhs);
+        if (dot(dl, dl) > 0.0f) {
+            s.segLambda[g] = mk4(lambda + dl, 0.0f);
+            out[0] = mk4(-wA * irl * dl * relax, 0.0f);
+            out[1] = mk4(wB * irl * dl * relax, 0.0f);
+            const f4 qg{-dot(gQx, dl), -dot(gQy, dl), -dot(gQz, dl), -dot(gQw, dl)};
+            out[2] = qg * (oim * relax);
+        }
+    }
+}
+// physics_strand_apply_segment_corrections.cs.hlsl:11-43
+void applySegments(cno_solver &s)
+{
+    const uint32_t n = std::max<uint32_t>(s.N, uint32_t(s.segs.size()));
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(n); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        if (i < s.N) {
+            const f4 p = s.x[i];
+            if (p.w > kEps) {
+                const Range r = s.segRanges[i];
+                f3 total{0, 0, 0};
+                for (uint32_t k = 0; k < r.count; ++k) {
+                    const Incident &ref = s.segInc[r.start + k];
+                    total += ref.slot == 0u ? xyz(s.segCorr[3 * ref.index]) : xyz(s.segCorr[3 * ref.index + 1]);
+                }
+                s.x[i] = mk4(xyz(p) + total, p.w);
+            }
+        }
+        if (i < s.segs.size()) s.segOrient[i] = QNormalize(s.segOrient[i] + s.segCorr[3 * i + 2]);
+    }
+}
+// physics_strand_solve_joint_constraints.cs.hlsl:66-154
+void solveJoints(cno_solver &s, float dt)
+{
+    const float relax = s.desc.soft.internal_relaxation;
+#pragma omp parallel for schedule(static)
+    for (int64_t jj = 0; jj < int64_t(s.joints.size()); ++jj) {
+        const uint32_t j = uint32_t(jj);
+        const cn_strand_joint &jt = s.joints[j];
+        const cn_strand_segment &sA = s.segs[jt.segment_a], &sB = s.segs[jt.segment_b];
+        f4 *out = &s.jointCorr[5 * j];
+        for (int k = 0; k < 5; ++k) out[k] = f4{0, 0, 0, 0};
+        const f4 oA = QNormalize(s.segOrient[jt.segment_a]);
+        const f4 oB = QNormalize(s.segOrient[jt.segment_b]);
+        const float wA0 = s.x[sA.particle_a].w, wA1 = s.x[sA.particle_b].w;
+        const float wB0 = s.x[sB.particle_a].w, wB1 = s.x[sB.particle_b].w;
+        const float imA = StrandOrientationInvMass(wA0, wA1, sA.rest_length);
+        const float imB = StrandOrientationInvMass(wB0, wB1, sB.rest_length);
+        const f4 rel = QNormalize(QMul(QConj(oA), oB));
+        f4 rr = QNormalize(f4{jt.rest_relative_orientation[0], jt.rest_relative_orientation[1],
+                              jt.rest_relative_orientation[2], jt.rest_relative_orientation[3]});
+        if (dot4(rel, rr) < 0.0f) rr = f4{-rr.x, -rr.y, -rr.z, -rr.w};
+        const f3 Cv = xyz(rel) - xyz(rr);
+        const f4 lambda = s.jointLambda[j];
+        const float ba = std::max(jt.bend_compliance, 0.0f) / std::max(dt * dt, kEps);
+        const float ta = std::max(jt.twist_compliance, 0.0f) / std::max(dt * dt, kEps);
+        const f3 av{ta, ba, ba};
+        m3 sys{{{av.x, 0, 0}, {0, av.y, 0}, {0, 0, av.z}}};
+        const f3 va = xyz(oA), vb = xyz(oB);
+        const float wa = oA.w, wb = oB.w;
+        const f3 gAX{-wb, vb.z, -vb.y}, gAY{-vb.z, -wb, vb.x}, gAZ{vb.y, -vb.x, -wb}, gAW = vb;
+        const f3 gBX{wa, -va.z, va.y}, gBY{va.z, wa, -va.x}, gBZ{-va.y, va.x, wa}, gBW = -va;
+        addScaled(sys, imA, outer(gAX, gAX));
+        addScaled(sys, imA, outer(gAY, gAY));
+        addScaled(sys, imA, outer(gAZ, gAZ));
+        addScaled(sys, imA, outer(gAW, gAW));
+        addScaled(sys, imB, outer(gBX, gBX));
+        addScaled(sys, imB, outer(gBY, gBY));
+        addScaled(sys, imB, outer(gBZ, gBZ));
+        addScaled(sys, imB, outer(gBW, gBW));
+        const f3 rhs = -(Cv + av * xyz(lambda));
+        const f3 dl = mul3(inverse3(sys), rhs);
+        if (dot(dl, dl) > 0.0f) {
+            s.jointLambda[j] = mk4(xyz(lambda) + dl, 0.0f);
+            out[3] = f4{dot(gAX, dl), dot(gAY, dl), dot(gAZ, dl), dot(gAW, dl)} * (imA * relax);
+            out[4] = f4{dot(gBX, dl), dot(gBY, dl), dot(gBZ, dl), dot(gBW, dl)} * (imB * relax);
+        }
+    }
+}
+// physics_strand_apply_joint_corrections.cs.hlsl
+void applyJoints(cno_solver &s)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t gg = 0; gg < int64_t(s.segs.size()); ++gg) {
+        const uint32_t g = uint32_t(gg);
+        const Range r = s.segJointRanges[g];
+        f4 total{0, 0, 0, 0};
+        for (uint32_t k = 0; k < r.count; ++k) {
+            const Incident &ref = s.segJointInc[r.start + k];
+            total = total + (ref.slot == 0u ? s.jointCorr[5 * ref.index + 3] : s.jointCorr[5 * ref.index + 4]);
+        }
+        s.segOrient[g] = QNormalize(s.segOrient[g] + total);
+    }
+}
+// physics_strand_solve_distance_constraints.cs.hlsl:10-59
+void solveDistances(cno_solver &s, float dt)
+{
+    const float relax = s.desc.soft.internal_relaxation;
+#pragma omp parallel for schedule(static)
+    for (int64_t cc = 0; cc < int64_t(s.dists.size()); ++cc) {
+        const uint32_t c = uint32_t(cc);
+        const cn_strand_distance &dc = s.dists[c];
+        f4 &cA = s.distCorr[2 * c], &cB = s.distCorr[2 * c + 1];
+        cA = cB = f4{0, 0, 0, 0};
+        const f4 a = s.x[dc.particle_a], b = s.x[dc.particle_b];
+        const float wA = a.w, wB = b.w, wSum = wA + wB;
+        if (wSum <= kEps) continue;
+        const f3 delta = xyz(b) - xyz(a);
+        const float l2 = dot(delta, delta);
+        if (l2 <= kEps) continue;
+        const float len = std::sqrt(l2);
+        const f3 grad = delta / len;
+        const float alpha = std::max(dc.distance_compliance, 0.0f) / std::max(dt * dt, kEps);
+        const float lambda = s.distLambda[c];
+        const float Cv = len - dc.rest_length;
+        const float den = wSum + alpha;
+        if (den > kEps) {
+            const float dl = -(Cv + alpha * lambda) / den;
+            s.distLambda[c] = lambda + dl;
+            cA = mk4(wA * dl * -grad * relax, 0.0f);
+            cB = mk4(wB * dl * grad * relax, 0.0f);
+        }
+    }
+}
+
+// physics_particle_generate_explicit_contacts.cs.hlsl (no suturing / proxies) +
+// compact + physics_particle_solve_explicit_contacts.cs.hlsl (non-proxy branch).
+void particleParticleContacts(cno_solver &s)
+{
+    const size_t P = s.particlePairs.size();
+    s.particleContacts.assign(P, ParticleContact{});
+#pragma omp parallel for schedule(static)
+    for (int64_t pp = 0; pp < int64_t(P); ++pp) {
+        ParticleContact out{};
+        const uint32_t a = s.particlePairs[pp].first, b = s.particlePairs[pp].second;
+        out.material = mk4(CombineContactMaterial(s.contactMaterials[s.matIdx[a]],
+                                                  s.contactMaterials[s.matIdx[b]]), 0.0f);
+        if (s.kinds[a] == CN_PARTICLE_FLUID && s.kinds[b] == CN_PARTICLE_FLUID) {
+            s.particleContacts[pp] = out;
+            continue;
+        }
+        const f3 pa = xyz(s.x[a]), pb = xyz(s.x[b]);
+        const float cr = s.radii[a] + s.radii[b];
+        const f3 delta = pb - pa;
+        const float d2 = dot(delta, delta);
+        if (d2 <= kEps) {
+            out.a = a; out.b = b; out.active = 1;
+            out.normalPenetration = f4{0, 1, 0, cr};
+            s.particleContacts[pp] = out;
+            continue;
+        }
+        const float dist = std::sqrt(d2);
+        const float pen = cr - dist;
+        if (pen > 0.0f) {
+            out.a = a; out.b = b; out.active = 1;
+            out.normalPenetration = mk4(delta / dist, pen);
+        }
+        s.particleContacts[pp] = out;
+    }
+    s.activeParticleContacts.clear();
+    for (const ParticleContact &c : s.particleContacts)
+        if (c.active) s.activeParticleContacts.push_back(c);
+    const float relax = s.desc.contact.soft_relaxation;
+    const float maxCorr = s.desc.contact.soft_max_correction_per_iteration;
+    const float minFric = s.desc.contact.position_friction_min_distance;
+    for (const ParticleContact &c : s.activeParticleContacts) { // float atomics in contact order
+        const f4 A = s.x[c.a], Bp = s.x[c.b];
+        const float iA = A.w, iB = Bp.w;
+        if (iA <= kEps && iB <= kEps) continue;
+        const float pen = std::min(std::max(c.normalPenetration.w - s.slop(), 0.0f), maxCorr);
+        if (pen <= 0.0f) continue;
+        const f3 mat = xyz(c.material);
+        const f3 n = SafeNormalize(xyz(c.normalPenetration), f3{0, 1, 0});
+        const f3 relDisp = (xyz(Bp) - xyz(s.xprev[c.b])) - (xyz(A) - xyz(s.xprev[c.a]));
+        const float denom = iA + iB;
+        if (denom <= kEps) continue;
+        const float lambda = (pen / denom) * relax;
+        f3 cA = -n * (iA * lambda);
+        f3 cB = n * (iB * lambda);
+        const f3 tdisp = ProjectOntoTangent(relDisp, n);
+        // ComputePositionFrictionDelta (physics_rigid_solver_shared.hlsli:50-68)
+        f3 fd{0, 0, 0};
+        const float td = length(tdisp);
+        if (!(td <= minFric || pen <= kEps)) {
+            const float sl = saturate(mat.z) * pen;
+            if (td <= sl) fd = tdisp;
+            else fd = tdisp * std::min(saturate(mat.x) * pen / td, 1.0f);
+        }
+        const float fdist = length(fd);
+        if (fdist > 0.0f) {
+            const f3 t = fd / fdist;
+            const float tden = iA + iB;
+            if (tden > kEps) {
+                const float tl = (fdist / tden) * relax;
+                cA += t * (iA * tl);
+                cB -= t * (iB * tl);
+            }
+        }
+        if (iA > kEps) s.posCorr[c.a] = mk4(xyz(s.posCorr[c.a]) + cA, s.posCorr[c.a].w);
+        if (iB > kEps) s.posCorr[c.b] = mk4(xyz(s.posCorr[c.b]) + cB, s.posCorr[c.b].w);
+    }
+}
+
+// physics_particle_rigid_generate_contacts.cs.hlsl:29-210 + compact_active_rigid_contacts +
+// physics_particle_rigid_solve_contacts.cs.hlsl:27-141 (static / kinematic bodies).
+void particleRigidContacts(cno_solver &s)
+{
+    const size_t P = s.rigidPairs.size();
+    s.rigidContacts.assign(P, RigidContact{});
+#pragma omp parallel for schedule(static)
+    for (int64_t pp = 0; pp < int64_t(P); ++pp) {
+        RigidContact out{};
+        const uint32_t i = s.rigidPairs[pp].first, b = s.rigidPairs[pp].second;
+        if (s.ownerTypes[i] == CN_OWNER_RIGID_BODY) { s.rigidContacts[pp] = out; continue; }
+        const f3 sp = xyz(s.x[i]);
+        const float sr = s.radii[i];
+        const uint32_t *m = &s.meta[4 * i];
+        const f3 bpos = xyz(s.predBodyPos[b]);
+        const f4 bq = QNormalize(s.predBodyRot[b]);
+        const f4 bsc = s.bodyScale[b];
+        const uint32_t co = s.bodyColRanges[2 * b], cc = s.bodyColRanges[2 * b + 1];
+        float bestPen = 0.0f;
+        uint32_t bestCol = 0;
+        f3 bestN{0, 1, 0}, bestW{0, 0, 0};
+        for (uint32_t k = 0; k < kColliderCap; ++k) {
+            if (k >= cc) break;
+            const uint32_t c = s.bodyColIdx[co + k];
+            const cn_collider_broadphase &bp = s.colBp[c];
+            if (bp.enabled_flag == 0u || bp.environment_index != m[0]) continue;
+            if ((m[3] & bp.collision_layer) == 0u || (bp.collision_mask & m[2]) == 0u) continue;
+            const cn_collider_geometry &cg = s.colGeo[c];
+            const f3 clp{cg.local_position[0], cg.local_position[1], cg.local_position[2]};
+            const f4 clq = QNormalize(f4{cg.local_orientation[0], cg.local_orientation[1],
+                                         cg.local_orientation[2], cg.local_orientation[3]});
+            const f3 cwp = bpos + QRotate(bq, clp);
+            const f4 cwq = QNormalize(QMul(bq, clq));
+            const f3 pl = QInvRotate(cwq, sp - cwp);
+            f3 nl{0, 1, 0}, cw{0, 0, 0};
+            float sd = 0.0f;
+            const f4 sp4{cg.shape_params[0], cg.shape_params[1], cg.shape_params[2], cg.shape_params[3]};
+            if (bp.shape_type == CN_COLLIDER_SPHERE) {
+                const float r = SphereRadius(sp4, bsc);
+                const float l = std::sqrt(dot(pl, pl));
+                nl = l > kEps ? (pl / l) : f3{0, 1, 0};
+                sd = l - r;
+                cw = cwp + QRotate(cwq, nl * r);
+            } else if (bp.shape_type == CN_COLLIDER_BOX) {
+                const f3 he = BoxHalfExtents(sp4, bsc);
+                const f3 cl = clamp3(pl, -he, he);
+                const f3 d = pl - cl;
+                const float dl = std::sqrt(dot(d, d));
+                if (dl > kEps) {
+                    nl = d / dl;
+                    sd = dl;
+                    cw = cwp + QRotate(cwq, cl);
+                } else {
+                    nl = ClosestFaceNormalLocal(pl, he);
+                    const f3 ds = he - fabs3(pl);
+                    sd = -std::min(ds.x, std::min(ds.y, ds.z));
+                    f3 cs = pl;
+                    if (std::fabs(nl.x) > 0.5f) cs.x = nl.x * he.x;
+                    else if (std::fabs(nl.y) > 0.5f) cs.y = nl.y * he.y;
+                    else cs.z = nl.z * he.z;
+                    cw = cwp + QRotate(cwq, cs);
+                }
+            } else {
+                f3 a, b2;
+                float cr = 0.0f;
+                CapsuleSegment(cwp, cwq, sp4, bsc, a, b2, cr);
+                const f3 seg = b2 - a;
+                const float l2 = dot(seg, seg);
+                float t = 0.0f;
+                if (l2 > kEps) t = saturate(dot(sp - a, seg) / l2);
+                const f3 cl = lerp3(a, b2, t);
+                const f3 d = sp - cl;
+                const float l = std::sqrt(dot(d, d));
+                const f3 wn = l > kEps ? (d / l) : f3{1, 0, 0};
+                sd = l - cr;
+                nl = QInvRotate(cwq, wn);
+                cw = cl + wn * cr;
+            }
+            const float pen = sr - sd;
+            if (pen <= 0.0f || pen <= bestPen) continue;
+            bestPen = pen;
+            bestCol = c;
+            bestN = SafeNormalize(QRotate(cwq, nl), f3{0, 1, 0});
+            bestW = cw;
+        }
+        if (bestPen > 0.0f) {
+            out.particle = i; out.body = b; out.collider = bestCol; out.active = 1;
+            out.normalPenetration = mk4(bestN, bestPen);
+            out.rigidLocalPoint = mk4(QInvRotate(bq, bestW - bpos), 0.0f);
+        }
+        s.rigidContacts[pp] = out;
+    }
+    s.activeRigidContacts.clear();
+    for (const RigidContact &c : s.rigidContacts)
+        if (c.active) s.activeRigidContacts.push_back(c);
+    const float relax = s.desc.contact.soft_relaxation;
+    const float maxCorr = s.desc.contact.soft_max_correction_per_iteration;
+    const float minFric = s.desc.contact.position_friction_min_distance;
+    for (const RigidContact &c : s.activeRigidContacts) {
+        const uint32_t i = c.particle, b = c.body;
+        const f4 sp = s.x[i];
+        const float iS = sp.w;
+        const f3 prevS = xyz(s.xprev[i]);
+        const f4 prevB = s.prevBodyPos[b], predB = s.predBodyPos[b];
+        const f4 prevQ = QNormalize(s.prevBodyRot[b]), predQ = QNormalize(s.predBodyRot[b]);
+        const float iR = s.bodyType[b] == CN_BODY_DYNAMIC ? predB.w : 0.0f;
+        if (iS <= kEps && iR <= kEps) continue;
+        const float pen = std::min(std::max(c.normalPenetration.w - s.slop(), 0.0f), maxCorr);
+        if (pen <= 0.0f) continue;
+        const f3 n = SafeNormalize(xyz(c.normalPenetration), f3{0, 1, 0});
+        f3 inI = xyz(s.bodyInvInertia[b]);
+        const f3 mat = CombineContactMaterial(s.contactMaterials[s.matIdx[i]], s.colMat[c.collider]);
+        if (iR <= kEps) inI = f3{0, 0, 0};
+        const f3 prevCP = xyz(prevB) + QRotate(prevQ, xyz(c.rigidLocalPoint));
+        const f3 cp = xyz(predB) + QRotate(predQ, xyz(c.rigidLocalPoint));
+        const f3 rR = cp - xyz(predB);
+        const float nmR = ContactEffectiveMass(iR, inI, predQ, rR, n);
+        const float denom = iS + nmR;
+        if (denom <= kEps) continue;
+        const float lambda = (pen / denom) * relax;
+        f3 corr = n * (iS * lambda);
+        const f3 relDisp = (cp - prevCP) - (xyz(sp) - prevS);
+        const f3 tdisp = ProjectOntoTangent(relDisp, n);
+        f3 fd{0, 0, 0};
+        const float td = length(tdisp);
+        if (!(td <= minFric || pen <= kEps)) {
+            const float sl = saturate(mat.z) * pen;
+            if (td <= sl) fd = tdisp;
+            else fd = tdisp * std::min(saturate(mat.x) * pen / td, 1.0f);
+        }
+        const float fdist = length(fd);
+        if (fdist > 0.0f) {
+            const f3 t = fd / fdist;
+            const float tmR = ContactEffectiveMass(iR, inI, predQ, rR, t);
+            const float tden = iS + tmR;
+            if (tden > kEps) {
+                const float tl = fdist / tden;
+                corr += t * (tl * iS * relax);
+            }
+        }
+        if (iS > kEps) s.posCorr[i] = mk4(xyz(s.posCorr[i]) + corr, s.posCorr[i].w);
+    }
+}
+
+// physics_particle_apply_position_corrections.cs.hlsl:8-30
+void applyPositionCorrections(cno_solver &s)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        const f3 c = xyz(s.posCorr[i]);
+        s.posCorr[i] = f4{0, 0, 0, 0};
+        const f4 p = s.x[i];
+        if (p.w <= kEps) continue;
+        s.x[i] = mk4(xyz(p) + c, p.w);
+    }
+}
+
+// physics_particle_update_velocities.cs.hlsl:13-44
+void updateVelocities(cno_solver &s, float dt)
+{
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        const f4 p = s.x[i];
+        if (p.w <= kEps || dt <= kEps) { s.v[i] = f4{0, 0, 0, 0}; continue; }
+        const f3 pp = xyz(s.xprev[i]);
+        f3 pos = xyz(p);
+        if (s.kinds[i] == CN_PARTICLE_FLUID) {
+            pos += xyz(s.fluidDelta[i]);
+            s.x[i] = mk4(pos, p.w);
+            s.fluidDelta[i] = f4{0, 0, 0, 0};
+        }
+        const float damping = std::max(s.contactMaterials[s.matIdx[i]].z, 0.0f);
+        const float ds = std::max(1.0f - damping * dt, 0.0f);
+        s.v[i] = mk4(((pos - pp) / dt) * ds, 0.0f);
+    }
+}
+
+// physics_fluid_project_boundary_velocities.cs.hlsl:24-117
+void projectFluidBoundaryVelocities(cno_solver &s, float dt)
+{
+    const float slop = s.slop();
+    const float minFric = s.desc.contact.position_friction_min_distance;
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        if (s.kinds[i] != CN_PARTICLE_FLUID) continue;
+        const f3 pos = xyz(s.x[i]);
+        const float pr = std::max(s.radii[i], 0.0f);
+        f3 vel = xyz(s.v[i]);
+        const f4 pm = s.contactMaterials[s.matIdx[i]];
+        const float pd = std::max(pm.z, 0.0f);
+        float bestD = 3.402823466e+38f;
+        f3 bestN{0, 1, 0}, bestMat{0, 0, 0};
+        bool found = false;
+        for (uint32_t c : s.boundaryCand[i]) {
+            float sd = 0.0f;
+            f3 n{0, 1, 0};
+            if (!FluidBoundaryContactInfo(s, c, pos, sd, n)) continue;
+            const float cd = pr + 2.0f * slop;
+            if (sd > cd) continue;
+            if (sd < bestD) {
+                bestD = sd; bestN = n;
+                bestMat = CombineContactMaterial(pm, s.colMat[c]);
+                found = true;
+            }
+        }
+        if (!found) continue;
+        const float pen = std::max(pr - bestD, 0.0f);
+        const float cd = std::max(pr + 2.0f * slop, 1.0e-5f);
+        const float cw = saturate((cd - bestD) / cd);
+        f3 rv = vel;
+        const float nv = dot(rv, bestN);
+        if (nv < 0.0f) rv -= bestN * nv;
+        f3 tv = ProjectOntoTangent(rv, bestN);
+        if (dt > kEps) {
+            const f3 tdisp = tv * dt;
+            const float p2 = std::max(pen, slop);
+            f3 fd{0, 0, 0};
+            const float td = length(tdisp);
+            if (!(td <= minFric || p2 <= kEps)) {
+                const float sl = saturate(bestMat.z) * p2;
+                if (td <= sl) fd = tdisp;
+                else fd = tdisp * std::min(saturate(bestMat.x) * p2 / td, 1.0f);
+            }
+            tv -= fd / dt;
+        }
+        const float tds = std::max(1.0f - pd * cw * dt, 0.0f);
+        tv = tv * tds;
+        rv = bestN * std::max(dot(rv, bestN), 0.0f) + tv;
+        s.v[i] = mk4(rv, 0.0f);
+    }
+}
+
+// physics_particle_rigid_solve_contact_velocities.cs.hlsl + apply_contact_velocities.cs.hlsl,
+// repeated softContactIterations times (physics_pass_dispatcher.cpp:3338-3410).
+void particleRigidContactVelocities(cno_solver &s, uint32_t iterations)
+{
+    const float rvt = s.desc.contact.restitution_velocity_threshold;
+    const float rpt = s.desc.contact.restitution_penetration_slop_multiplier * s.slop();
+    for (uint32_t it = 0; it < iterations; ++it) {
+        for (const RigidContact &c : s.activeRigidContacts) {
+            const uint32_t i = c.particle, b = c.body;
+            const float iS = s.x[i].w;
+            const f3 sv = xyz(s.v[i]);
+            const f4 rp = s.predBodyPos[b];
+            const float iR = s.bodyType[b] == CN_BODY_DYNAMIC ? rp.w : 0.0f;
+            if (iS <= kEps && iR <= kEps) continue;
+            const f4 rq = QNormalize(s.predBodyRot[b]);
+            const f3 rl = xyz(s.predBodyLin[b]), ra = xyz(s.predBodyAng[b]);
+            const f3 inI = xyz(s.bodyInvInertia[b]);
+            const f3 n = SafeNormalize(xyz(c.normalPenetration), f3{0, 1, 0});
+            const f3 cp = xyz(rp) + QRotate(rq, xyz(c.rigidLocalPoint));
+            const f3 rR = cp - xyz(rp);
+            const f3 rcv = rl + cross(ra, rR);
+            const f3 rel = sv - rcv;
+            const float nv = dot(rel, n);
+            if (nv >= 0.0f) continue;
+            const float rnd = ContactEffectiveMass(iR, inI, rq, rR, n);
+            const float nd = iS + rnd;
+            if (nd <= kEps) continue;
+            const f3 mat = CombineContactMaterial(s.contactMaterials[s.matIdx[i]], s.colMat[c.collider]);
+            const bool er = (-nv > rvt) && (c.normalPenetration.w <= rpt);
+            const float rest = er ? saturate(mat.y) : 0.0f;
+            const float dnv = er ? (-rest * nv) : 0.0f;
+            const float imp = std::max(0.0f, (dnv - nv) / nd);
+            const f3 ti = n * imp;
+            if (iS > kEps) s.velCorr[i] = mk4(xyz(s.velCorr[i]) + ti * iS, s.velCorr[i].w);
+        }
+        for (uint32_t i = 0; i < s.N; ++i) {
+            f4 vel = s.v[i];
+            const float im = s.x[i].w;
+            const f3 c = xyz(s.velCorr[i]);
+            if (im > kEps) vel = mk4(xyz(vel) + c, vel.w);
+            s.v[i] = vel;
+            s.velCorr[i] = f4{0, 0, 0, 0};
+        }
+    }
+}
+
+// physics_particle_solve_contact_velocities.cs.hlsl (non-proxy branch) +
+// apply_contact_velocities.cs.hlsl, repeated softContactIterations times
+// (physics_pass_dispatcher.cpp:3201-3273).
+void particleContactVelocities(cno_solver &s, uint32_t iterations)
+{
+    const float rvt = s.desc.contact.restitution_velocity_threshold;
+    const float rpt = s.desc.contact.restitution_penetration_slop_multiplier * s.slop();
+    for (uint32_t it = 0; it < iterations; ++it) {
+        for (const ParticleContact &c : s.activeParticleContacts) {
+            const float iA = s.x[c.a].w, iB = s.x[c.b].w;
+            const f3 vA = xyz(s.v[c.a]), vB = xyz(s.v[c.b]);
+            if (iA <= kEps && iB <= kEps) continue;
+            const f3 n = SafeNormalize(xyz(c.normalPenetration), f3{0, 1, 0});
+            const f3 rel = vB - vA;
+            const float nv = dot(rel, n);
+            if (nv >= 0.0f) continue;
+            const float denom = iA + iB;
+            if (denom <= kEps) continue;
+            const f3 mat = xyz(c.material);
+            const bool er = (-nv > rvt) && (c.normalPenetration.w <= rpt);
+            const float rest = er ? saturate(mat.y) : 0.0f;
+            const float dnv = er ? (-rest * nv) : 0.0f;
+            const float imp = std::max(0.0f, (dnv - nv) / denom);
+            const f3 ti = n * imp;
+            if (iA > kEps) s.velCorr[c.a] = mk4(xyz(s.velCorr[c.a]) + (-ti * iA), s.velCorr[c.a].w);
+            if (iB > kEps) s.velCorr[c.b] = mk4(xyz(s.velCorr[c.b]) + ti * iB, s.velCorr[c.b].w);
+        }
+        for (uint32_t i = 0; i < s.N; ++i) {
+            f4 vel = s.v[i];
+            const float im = s.x[i].w;
+            const f3 c = xyz(s.velCorr[i]);
+            if (im > kEps) vel = mk4(xyz(vel) + c, vel.w);
+            s.v[i] = vel;
+            s.velCorr[i] = f4{0, 0, 0, 0};
+        }
+    }
+}
+
+uint32_t resolveIter(uint32_t o, uint32_t d) { return o > 0u ? o : d; }
+
+void stepFrame(cno_solver &s, float frameDt)
+{
+    const cn_solver_desc &d = s.desc;
+    const uint32_t substeps = std::max<uint32_t>(d.substeps, 1u);
+    const uint32_t defIt = std::max<uint32_t>(d.default_iterations, 1u);
+    const uint32_t fluidIt = resolveIter(d.fluid_iterations, defIt);
+    const uint32_t softIt = resolveIter(d.soft_internal_iterations, defIt);
+    const uint32_t contactIt = resolveIter(d.soft_contact_iterations, defIt);
+    const uint32_t jointIt = resolveIter(d.rigid_joint_iterations, defIt);
+    const uint32_t rrIt = resolveIter(d.rigid_rigid_contact_iterations, defIt);
+    const uint32_t maxIt = std::max(std::max(std::max(fluidIt, softIt), contactIt), std::max(jointIt, rrIt));
+    const float dt = frameDt / float(substeps);
+    uint32_t fluidCount = 0;
+    for (uint32_t k : s.kinds) fluidCount += k == CN_PARTICLE_FLUID ? 1u : 0u;
+    const uint32_t N = s.N;
+
+    for (uint32_t sub = 0; sub < substeps; ++sub) {
+        // physics_solver.cpp:472-496 gating flags
+        const bool hasFluidWork = fluidCount > 0 && N > 0;
+        const bool hasSoftInternal = N > 0 && (!s.edges.empty() || !s.bends.empty() ||
+                                               !s.dihedrals.empty() || !s.tets.empty() ||
+                                               !s.segs.empty() || !s.joints.empty() || !s.dists.empty());
+        const bool hasSoftSoftContact = contactIt > 0 && N > 1;
+        const bool hasRigidCand = N > 0 && s.C > 0;
+        const bool hasSoftRigidContact = contactIt > 0 && hasRigidCand;
+        const bool hasBroadphase = hasSoftSoftContact || hasFluidWork || hasRigidCand;
+
+        predictRigid(s, dt);
+        predictSoft(s, dt);
+        if (hasBroadphase) broadphase(s);
+        s.particlePairs.clear();
+        s.rigidPairs.clear();
+        s.requiredParticlePairs = s.requiredRigidPairs = 0;
+        if (N > 0) {
+            if (hasSoftSoftContact) buildParticleParticleCandidates(s);
+            if (hasRigidCand) buildParticleRigidCandidates(s);
+            if (hasFluidWork && s.C > 0) buildFluidBoundaryCandidates(s);
+        }
+        // clearSoftConstraintState (physics_clear_soft_constraint_state.cs.hlsl:14-54)
+        std::fill(s.posCorr.begin(), s.posCorr.end(), f4{0, 0, 0, 0});
+        std::fill(s.velCorr.begin(), s.velCorr.end(), f4{0, 0, 0, 0});
+        std::fill(s.edgeLambda.begin(), s.edgeLambda.end(), 0.0f);
+        std::fill(s.bendLambda.begin(), s.bendLambda.end(), 0.0f);
+        std::fill(s.tetLambda.begin(), s.tetLambda.end(), 0.0f);
+        std::fill(s.distLambda.begin(), s.distLambda.end(), 0.0f);
+        std::fill(s.segLambda.begin(), s.segLambda.end(), f4{0, 0, 0, 0});
+        std::fill(s.jointLambda.begin(), s.jointLambda.end(), f4{0, 0, 0, 0});
+
+        for (uint32_t it = 0; it < maxIt; ++it) {
+            const bool runSoft = hasSoftInternal && it < softIt;
+            const bool runContacts = hasSoftSoftContact && it < contactIt;
+            const bool runRigid = hasSoftRigidContact && it < contactIt;
+            const bool runFluid = hasFluidWork && it < fluidIt;
+            if (runFluid) {
+                buildFluidNeighbors(s, it);
+                fluidDensity(s, it);
+                fluidDeltaPositions(s, it, dt);
+                fluidApplyAndClamp(s, it);
+            }
+            if (runSoft) {
+                solveEdges(s, dt);
+                applyPairCorrections(s, s.edgeRanges, s.edgeInc, s.edgeCorr);
+                solveSegments(s, dt);
+                applySegments(s);
+                solveBends(s, dt);
+                solveDihedrals(s, dt);
+                applyQuadCorrections(s, s.bendRanges, s.bendInc, s.bendCorr);
+                solveJoints(s, dt);
+                applyJoints(s);
+                solveDistances(s, dt);
+                applyPairCorrections(s, s.segRanges, s.segInc, s.distCorr);
+                solveTets(s, dt);
+                applyQuadCorrections(s, s.tetRanges, s.tetInc, s.tetCorr);
+            }
+            if (runContacts) particleParticleContacts(s);
+            if (runRigid) particleRigidContacts(s);
+            if (runContacts || runRigid) applyPositionCorrections(s);
+        }
+        updateVelocities(s, dt);
+        if (hasFluidWork) projectFluidBoundaryVelocities(s, dt);
+        if (hasFluidWork) {
+            // post-update neighbour rebuild (physics_solver.cpp:1262-1268); its lists feed only
+            // vorticity confinement and render anisotropy.
+            buildFluidNeighbors(s, maxIt > 0 ? maxIt - 1 : 0);
+        }
+        if (hasSoftSoftContact && contactIt > 0) particleContactVelocities(s, contactIt);
+        if (hasSoftRigidContact && contactIt > 0) particleRigidContactVelocities(s, contactIt);
+        // copyPredictedRigidBodiesToPersistentState
+        for (uint32_t b = 0; b < s.B; ++b) {
+            s.bodyPos[b] = s.predBodyPos[b];
+            s.bodyRot[b] = s.predBodyRot[b];
+            s.bodyLin[b] = s.predBodyLin[b];
+            s.bodyAng[b] = s.predBodyAng[b];
+        }
+    }
+}
+
+thread_local std::string g_err;
+
+} // namespace
+
+extern "C" {
+
+CN_API const char *cno_last_error(void) { return g_err.c_str(); }
+
+CN_API int cno_set_threads(int n)
+{
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+    return omp_get_max_threads();
+#else
+    (void)n;
+    return 1;
+#endif
+}
+
+CN_API cno_solver *cno_create(const cn_solver_desc *desc, const cn_world_soa *world)
+{
+    if (!desc || !world) { g_err = "null argument"; return nullptr; }
+    cno_solver *s = new cno_solver();
+    s->desc = *desc;
+    setupWorld(*s, *world);
+    return s;
+}
+
+CN_API void cno_destroy(cno_solver *s) { delete s; }
+
+CN_API int cno_step(cno_solver *s, float frame_dt)
+{
+    if (!s) return CN_ERR_INVALID_ARGUMENT;
+    stepFrame(*s, frame_dt);
+    return CN_OK;
+}
+
+CN_API int cno_set_kinematic_target(cno_solver *s, uint32_t body, const float *pos, const float *rot)
+{
+    if (!s || body >= s->B) return CN_ERR_INVALID_ARGUMENT;
+    s->bodyKinPos[body] = f4{pos[0], pos[1], pos[2], 0.0f};
+    s->bodyKinRot[body] = f4{rot[0], rot[1], rot[2], rot[3]};
+    s->bodyKinFlags[body] |= 1u;
+    return CN_OK;
+}
+
+CN_API int cno_read_particles(cno_solver *s, float *x, float *v, float *xprev)
+{
+    if (!s) return CN_ERR_INVALID_ARGUMENT;
+    if (x) std::memcpy(x, s->x.data(), s->x.size() * sizeof(f4));
+    if (v) std::memcpy(v, s->v.data(), s->v.size() * sizeof(f4));
+    if (xprev) std::memcpy(xprev, s->xprev.data(), s->xprev.size() * sizeof(f4));
+    return CN_OK;
+}
+
+CN_API int cno_read_strand_orientations(cno_solver *s, float *q)
+{
+    if (!s) return CN_ERR_INVALID_ARGUMENT;
+    std::memcpy(q, s->segOrient.data(), s->segOrient.size() * sizeof(f4));
+    return CN_OK;
+}
+
+// Same buffer ids and layouts as cn_solver_debug_read.
+CN_API size_t cno_debug_read(cno_solver *s, int which, void *dst, size_t cap)
+{
+    if (!s) return 0;
+    std::vector<uint8_t> buf;
+    auto put = [&](const void *p, size_t n) { buf.assign((const uint8_t *)p, (const uint8_t *)p + n); };
+    switch (which) {
+    case CN_DEBUG_CELL_ENTRIES: put(s->entries.data(), s->entries.size() * 4); break;
+    case CN_DEBUG_SORTED_KEYS: {
+        std::vector<uint32_t> kv(size_t(s->N) * 2);
+        for (uint32_t i = 0; i < s->N; ++i) { kv[2 * i] = s->sortedKey[i]; kv[2 * i + 1] = s->sortedIdx[i]; }
+        put(kv.data(), kv.size() * 4);
+        break;
+    }
+    case CN_DEBUG_CELL_RANGES: put(s->cellRanges.data(), s->cellRanges.size() * sizeof(CellRange)); break;
+    case CN_DEBUG_FLUID_NEIGHBOR_COUNTS: put(s->nbrCount.data(), s->nbrCount.size() * 4); break;
+    case CN_DEBUG_FLUID_NEIGHBORS: put(s->nbrList.data(), s->nbrList.size() * 4); break;
+    case CN_DEBUG_FLUID_CONSTRAINTS: put(s->fluidNormalC.data(), s->fluidNormalC.size() * 16); break;
+    case CN_DEBUG_FLUID_DELTA: put(s->fluidDx.data(), s->fluidDx.size() * 16); break;
+    case CN_DEBUG_RIGID_CONTACTS: put(s->activeRigidContacts.data(), s->activeRigidContacts.size() * sizeof(RigidContact)); break;
+    default: return 0;
+    }
+    if (dst) std::memcpy(dst, buf.data(), std::min(cap, buf.size()));
+    return buf.size();
+}
+
+CN_API uint32_t cno_meta(cno_solver *s, uint32_t *out, uint32_t n)
+{
+    // (required rigid pairs, rigid pair count, required particle pairs, particle pair count,
+    //  active rigid contacts, active particle contacts, neighbour-list truncations)
+    const uint32_t vals[7] = {s->requiredRigidPairs, uint32_t(s->rigidPairs.size()),
+                              s->requiredParticlePairs, uint32_t(s->particlePairs.size()),
+                              uint32_t(s->activeRigidContacts.size()),
+                              uint32_t(s->activeParticleContacts.size()), s->truncations};
+    for (uint32_t i = 0; i < n && i < 7; ++i) out[i] = vals[i];
+    return 7;
+}
+
+// Host derivations restated for cross-checking the product's authoring code:
+// toFluidSolverMaterial / calculateFluidSolveScales (physics_world.cpp:150-262).
+CN_API void cno_fluid_material(float particle_radius, float viscosity, float cohesion,
+                               float surface_tension, float vorticity, float gravity_scale,
+                               float cfl, cn_fluid_material *out)
+{
+    const float pi = 3.14159265358979323846f;
+    const float restDist = std::max(2.0f * particle_radius, 1.0e-4f);
+    const float h = std::max((2.0f / 0.6f) * particle_radius, restDist);
+    // tightPack3D (physics_world.cpp:150-182)
+    const int dim = int(std::ceil(h / restDist));
+    const float rowScale = std::sqrt(0.75f) * restDist;
+    float rho = 0.0f, scale = 0.0f, a = 0.0f, b = 0.0f;
+    uint32_t count = 0;
+    for (int z = -dim; z <= dim && count < 2048; ++z)
+        for (int y = -dim; y <= dim && count < 2048; ++y)
+            for (int x = -dim; x <= dim && count < 2048; ++x) {
+                const float xp = x * restDist + (((y + z) & 1) != 0 ? restDist * 0.5f : 0.0f);
+                const f3 smp{xp, y * rowScale, z * rowScale};
+                const float m2 = smp.x * smp.x + smp.y * smp.y + smp.z * smp.z;
+                if (m2 == 0.0f) continue;
+                if (std::sqrt(m2) <= h) {
+                    ++count;
+                    const float dist = std::sqrt(smp.x * smp.x + smp.y * smp.y + smp.z * smp.z);
+                    const float om = 1.0f - dist / h;
+                    const float k = 15.0f / (pi * h * h * h);
+                    rho += k * om * om;
+                    const float dw = -k * 2.0f * om / h;
+                    scale += dw * dw;
+                    if (smp.y <= 0.0f && dist > 0.0f) {
+                        const float ct = smp.y / dist;
+                        a += dw * ct;
+                        b -= dist * ct;
+                    }
+                }
+            }
+    if (rho <= 1.0e-6f) rho = 1.0f;
+    if (scale <= 1.0e-6f) scale = 1.0f;
+    const float surf = (std::fabs(b) > 1.0e-6f && std::fabs(a) > 1.0e-6f) ? std::fabs(a / b) : 1.0f;
+    const float inv = 1.0f / rho;
+    const float rr = std::min(std::max(restDist / h, 1.0e-3f), 0.999f);
+    const float rr2 = rr * rr;
+    out->rest_density = rho;
+    out->inv_rest_density = inv;
+    out->smoothing_radius = h;
+    out->density_constraint_scale = 1.0f / std::max(scale, 1.0e-6f);
+    out->viscosity = viscosity * inv;
+    out->cohesion = cohesion * h;
+    out->cohesion1 = -(1.0f + rr) / rr2;
+    out->cohesion2 = (rr2 + rr + 1.0f) / rr2;
+    out->surface_tension = (surface_tension * inv) / surf;
+    out->vorticity_confinement = vorticity * inv * h;
+    out->gravity_scale = gravity_scale;
+    out->cfl_radius = cfl * h;
+}
+
+} // extern "C"
