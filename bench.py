@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dims", type=str, default="128,64,128", help="fluid lattice (profiling runs use smaller ones)")
     return ap.parse_args()
 
 
@@ -154,7 +155,8 @@ def run_ours(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    w, desc, dt = scenes.dam_break()
+    dims = tuple(int(v) for v in args.dims.split(","))
+    w, desc, dt = scenes.dam_break(nx=dims[0], ny=dims[1], nz=dims[2])
     soa = w.soa()
     n = soa.particle_count
     solver = Solver(desc, device=local)
@@ -240,7 +242,8 @@ def run_ours(args):
         "metric": METRIC, "value": round(value, 1), "unit": "particle-substeps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "particles": n, "substeps": substeps, "fluid_iterations": desc.fluid_iterations,
+        "config": {"workload": WORKLOAD if dims == (128, 64, 128) else f"pbf_dam_break_{dims[0]}x{dims[1]}x{dims[2]}",
+                   "particles": n, "substeps": substeps, "fluid_iterations": desc.fluid_iterations,
                    "frame_dt": dt, "parallelism": f"replicas{world}", "l2": "working set > L2 (~0.9 GB resident)",
                    "mean_neighbors": round(counts, 2)},
         "e2e": {"value": round(e2e_value, 1), "unit": "particle-substeps/s", "h2d_bytes_per_step": 32 * n,

@@ -125,9 +125,11 @@ template <class F> void probe(cn_solver *sv, const char *name, cudaStream_t st, 
     cn_solver::Probe p{name, nullptr, nullptr};
     cudaEventCreate(&p.begin);
     cudaEventCreate(&p.end);
-    cudaEventRecord(p.begin, st);
+    // External records become event-record nodes of the captured graph (plain records inside a
+    // capture only express ordering).
+    cudaEventRecordWithFlags(p.begin, st, cudaEventRecordExternal);
     fn();
-    cudaEventRecord(p.end, st);
+    cudaEventRecordWithFlags(p.end, st, cudaEventRecordExternal);
     sv->probes.push_back(p);
 }
 

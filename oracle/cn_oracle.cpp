@@ -338,6 +338,7 @@ struct cno_solver {
     std::vector<f4> jointCorr;     // 5 per joint
     std::vector<f4> distCorr;      // 2 per distance
     uint32_t truncations = 0;
+    bool postUpdateNeighbors = true; // physics_solver.cpp:1262-1268
 
     // settings shorthands (physics_solver_config.hlsli:27-62)
     float slop() const { return desc.contact.slop; }
@@ -1909,7 +1910,7 @@ void stepFrame(cno_solver &s, float frameDt)
         }
         updateVelocities(s, dt);
         if (hasFluidWork) projectFluidBoundaryVelocities(s, dt);
-        if (hasFluidWork) {
+        if (hasFluidWork && s.postUpdateNeighbors) {
             // post-update neighbour rebuild (physics_solver.cpp:1262-1268); its lists feed only
             // vorticity confinement and render anisotropy.
             buildFluidNeighbors(s, maxIt > 0 ? maxIt - 1 : 0);
@@ -1955,6 +1956,10 @@ CN_API cno_solver *cno_create(const cn_solver_desc *desc, const cn_world_soa *wo
 }
 
 CN_API void cno_destroy(cno_solver *s) { delete s; }
+
+// Switches the reference's post-update neighbour rebuild off (lists then hold the last
+// iteration's build), for comparisons with a GPU schedule that skips it.
+CN_API void cno_set_post_update_neighbors(cno_solver *s, int enable) { s->postUpdateNeighbors = enable != 0; }
 
 CN_API int cno_step(cno_solver *s, float frame_dt)
 {

@@ -41,6 +41,7 @@ def load() -> C.CDLL:
         lib.cno_debug_read.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
         lib.cno_set_kinematic_target.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
         lib.cno_set_threads.argtypes = [C.c_int]
+        lib.cno_set_post_update_neighbors.argtypes = [C.c_void_p, C.c_int]
         lib.cno_meta.restype = C.c_uint32
         lib.cno_meta.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
         lib.cno_fluid_material.argtypes = [C.c_float] * 7 + [C.c_void_p]
@@ -73,6 +74,9 @@ class Oracle:
             self.close()
         except Exception:
             pass
+
+    def set_post_update_neighbors(self, enable: bool) -> None:
+        self._lib.cno_set_post_update_neighbors(self._h, int(enable))
 
     def step(self, dt: float) -> None:
         self._lib.cno_step(self._h, dt)
