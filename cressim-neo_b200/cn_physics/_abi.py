@@ -196,6 +196,7 @@ SIGNATURES = [
     ("cn_solver_set_timing", C.c_int, [C.c_void_p, u32]),
     ("cn_solver_kernel_times", C.c_int, [C.c_void_p, C.c_void_p, u32, P_u32]),
     ("cn_solver_graph_stats", C.c_int, [C.c_void_p, P_u32, P_u32]),
+    ("cn_sort_cell_keys_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, u32, C.c_void_p]),
     ("cn_solver_debug_read", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
 ]
 

@@ -465,6 +465,20 @@ typedef enum cn_debug_buffer {
 CN_API cn_status cn_solver_debug_read(cn_solver *solver, cn_debug_buffer which, void *dst,
                                       size_t capacity_bytes, size_t *out_bytes);
 
+/* Allocation-free broadphase sort (no counterpart in the reference).
+ * For callers that must not allocate device memory while they run -- engines whose device memory
+ * belongs to their own pool, frame loops that cannot afford the allocator's implicit
+ * synchronisation, real-time code that reserves everything up front.  Sorts `count` cell keys
+ * stably (the permutation equals a stable sort by key, as the broadphase's) into caller-owned
+ * device buffers: sorted_keys[i] is the i-th key, sorted_indices[i] its input position.
+ * Limit: count <= 1048576; larger counts return CN_ERR_CAPACITY.  Scratch lives in a ~10 MiB
+ * file-scope device array that every GPU loading the library keeps until exit; the first call on
+ * a device looks its address up (cudaGetSymbolAddress), so make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU (different streams or
+ * threads without ordering) race.  `keys` is not modified; `stream` may be NULL. */
+CN_API cn_status cn_sort_cell_keys_noalloc(const uint32_t *keys, uint32_t *sorted_keys,
+                                           uint32_t *sorted_indices, uint32_t count, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
