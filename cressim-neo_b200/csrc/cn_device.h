@@ -61,6 +61,7 @@ struct Scene {
     const uint32_t *fluidMatIdx = nullptr;
     const uint32_t *ownerTypes = nullptr;
     const uint32_t *ownerIdx = nullptr;
+    const uint32_t *fluidGroup = nullptr;   // dense id of (environment, layer, mask) for fluid particles
     const uint32_t *adjOff = nullptr, *adjCnt = nullptr, *adjIdx = nullptr;
     const float4 *contactMaterials = nullptr;
     const cn_fluid_material *fluidMaterials = nullptr;
@@ -119,6 +120,10 @@ struct Scene {
     uint32_t tableMask = 0;           // cell hash table capacity - 1
     uint32_t *tableKeys = nullptr, *tableStart = nullptr;
     uint32_t *cellEnd = nullptr;      // at a run start: end | (mixed-coordinate flag << 31)
+    uint32_t *runFlag = nullptr;      // 1 at a run start (fluid scenes)
+    uint32_t *runIdx = nullptr;       // exclusive scan of runFlag
+    uint32_t *runStartOf = nullptr;   // per run: start slot | (mixed << 31)
+    uint2 *runNbr = nullptr;          // per run: 27 neighbour runs (start | check << 31, end)
 
     // ---- fluid (cell order) ----
     uint32_t hasFluid = 0;
@@ -134,6 +139,11 @@ struct Scene {
     uint32_t maxNbr = 128;
     uint32_t *nbr = nullptr;          // [N][maxNbr] sorted slots
     uint32_t *nbrCount = nullptr;     // per sorted slot
+    uint32_t supCap = 0;              // superset list slots per particle (0: superset lists off)
+    float supMargin = 0.2f;           // superset radius = h * (1 + supMargin)
+    uint32_t *sup = nullptr;          // [N][supCap] candidates within the superset radius, traversal order
+    uint32_t *supCount = nullptr;     // per sorted slot (> supCap: overflowed)
+    uint32_t *fluidMaxDelta = nullptr; // [64] float bits of max |accumulated delta| per iteration
 
     // ---- contact candidates ----
     uint32_t *candCount = nullptr, *candOffset = nullptr; // per particle
@@ -160,13 +170,13 @@ struct Config {
 // ------------------------------------------------------------------ launchers (cn_kernels.cu)
 void launchRigidPredict(const Scene &s, float dt, float gx, float gy, float gz, cudaStream_t st);
 void launchPredictAndKeys(const Scene &s, float dt, const Config &c, cudaStream_t st);
-void launchCellSetup(const Scene &s, cudaStream_t st);
+void launchCellSetup(const Scene &s, uint32_t *scanTmp, cudaStream_t st);
 void launchRigidCandidates(const Scene &s, uint32_t *scanTmp, size_t scanTmpBytes, cudaStream_t st);
 void launchParticleCandidates(const Scene &s, uint32_t *scanTmp, size_t scanTmpBytes, cudaStream_t st);
 void launchFluidIteration(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
                           cudaStream_t st);
 void launchFluidGather(const Scene &s, uint32_t iter, cudaStream_t st);
-void launchFluidNeighborsDensity(const Scene &s, const Config &c, cudaStream_t st);
+void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter, cudaStream_t st);
 void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
                                 cudaStream_t st);
 void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st);

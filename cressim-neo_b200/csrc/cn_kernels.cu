@@ -24,7 +24,13 @@ namespace {
 
 constexpr int kThreads = 256;
 inline unsigned blocksFor(uint32_t n) { return n == 0 ? 1u : (n + kThreads - 1) / kThreads; }
+// Per-slot fluid word: bit 31 = fluid particle, bits 16..30 = fluid material, bits 0..15 = filter
+// group (a dense id of the particle's (environment, layer, mask) triple).  P.w carries the same
+// word with bit 31 meaning "fluid and invMass > kEps" (the neighbour candidate filter).
 constexpr uint32_t kFluidBit = 0x80000000u;
+constexpr uint32_t kMaxTrackedIterations = 64u; // fluid iterations whose max |delta| is tracked
+__host__ __device__ __forceinline__ uint32_t infoMaterial(uint32_t info) { return (info >> 16) & 0x7fffu; }
+__host__ __device__ __forceinline__ uint32_t infoGroup(uint32_t info) { return info & 0xffffu; }
 
 __device__ __forceinline__ float4 ld4(const float4 *p) { return __ldg(p); }
 
@@ -211,14 +217,16 @@ __global__ void __launch_bounds__(kThreads) k_cellSetup(Scene s)
         const uint32_t kind = s.kinds[p];
         const bool fluid = kind == CN_PARTICLE_FLUID;
         s.sMeta[slot] = s.meta[p];
-        s.sInfo[slot] = (fluid ? kFluidBit : 0u) | (s.fluidMatIdx[p] & 0x7fffffffu);
+        s.sInfo[slot] = fluid ? (kFluidBit | ((s.fluidMatIdx[p] & 0x7fffu) << 16) | (s.fluidGroup[p] & 0xffffu)) : 0u;
         unsigned long long mask = 0ull;
         if (fluid && s.colQueryCount > 0) {
             if (fluidBoundaryMaskFor(s, p, xyz(s.x[p]), mask)) atomicAdd(&s.meta_->boundaryMaskOverflow, 1u);
         }
         s.sBoundary[slot] = mask;
     }
-    if (slot != 0 && s.keysA[slot - 1] == key) return;
+    const bool start = slot == 0 || s.keysA[slot - 1] != key;
+    if (s.runFlag) s.runFlag[slot] = start ? 1u : 0u;
+    if (!start) return;
     uint32_t end = slot + 1;
     uint32_t mixed = 0;
     while (end < s.N && s.keysA[end] == key) {
@@ -258,6 +266,38 @@ __device__ __forceinline__ bool findRun(const Scene &s, uint32_t key, uint32_t &
         h = (h + 1) & s.tableMask;
     }
     return false;
+}
+
+// Per cell run: the 27 neighbour runs in the reference's traversal order (dz, dy, dx), looked up
+// once per substep.  Entry k = (start | checkCoordinates << 31, end); empty when the target cell
+// has no run or its (uniform) run holds another cell that hashes to the same key.
+__global__ void __launch_bounds__(kThreads) k_runNeighbors(Scene s)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= s.N || s.runFlag[slot] == 0u) return;
+    const uint32_t r = s.runIdx[slot];
+    const uint32_t mixedHere = s.cellEnd[slot] >> 31;
+    s.runStartOf[r] = slot | (mixedHere << 31);
+    const int4 e = s.sCell[slot];
+    uint2 *out = s.runNbr + size_t(r) * 27u;
+    int k = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx, ++k) {
+                const int tx = e.x + dx, ty = e.y + dy, tz = e.z + dz;
+                uint32_t start = 0, end = 0;
+                bool mixed = false;
+                uint2 rg = make_uint2(0u, 0u);
+                if (findRun(s, cellKey(tx, ty, tz), start, end, mixed)) {
+                    if (mixed) {
+                        rg = make_uint2(start | 0x80000000u, end);
+                    } else {
+                        const int4 ce = s.sCell[start];
+                        if (ce.x == tx && ce.y == ty && ce.z == tz) rg = make_uint2(start, end);
+                    }
+                }
+                out[k] = rg;
+            }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -392,11 +432,22 @@ __global__ void __launch_bounds__(kThreads) k_fluidGather(Scene s, float4 *Xs, c
                                                           uint32_t iter)
 {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= s.N) return;
-    const float4 xp = s.x[s.valsA[slot]];
-    const f3 d = iter > 0 ? xyz(Dcur[slot]) : f3{0.f, 0.f, 0.f};
-    Xs[slot] = xp;
-    s.P[slot] = mk4(xyz(xp) + d, xp.w);
+    float largest = 0.0f;
+    if (slot < s.N) {
+        const float4 xp = s.x[s.valsA[slot]];
+        const f3 d = iter > 0 ? xyz(Dcur[slot]) : f3{0.f, 0.f, 0.f};
+        const uint32_t info = s.sInfo[slot];
+        const uint32_t tag = (info & 0x7fffffffu) | ((info & kFluidBit) && xp.w > kEps ? kFluidBit : 0u);
+        Xs[slot] = xp;
+        s.P[slot] = mk4(xyz(xp) + d, __uint_as_float(tag));
+        if (info & kFluidBit) largest = sqrtf(dot(d, d));
+    }
+    // largest accumulated delta of this iteration: validity of the superset lists
+    if (s.fluidMaxDelta && iter > 0 && iter < kMaxTrackedIterations) {
+        for (int o = 16; o > 0; o >>= 1) largest = fmaxf(largest, __shfl_xor_sync(0xffffffffu, largest, o));
+        if ((threadIdx.x & 31) == 0 && largest > 0.0f)
+            atomicMax(&s.fluidMaxDelta[iter], __float_as_uint(largest));
+    }
 }
 
 // physics_fluid_boundary_common.hlsli:11-83
@@ -463,11 +514,45 @@ __device__ __forceinline__ bool fluidGhostDelta(const Scene &s, uint32_t c, f3 p
     return true;
 }
 
+// Smallest float t with sqrtf(t) >= h: `length(d) >= h` (the reference's neighbour test) is exactly
+// `dot(d, d) >= t` because the IEEE square root is correctly rounded and monotonic, so the square
+// root is only taken for accepted neighbours.
+__device__ __forceinline__ float sqrtThreshold(float h)
+{
+    float t = h * h;
+    for (int k = 0; k < 4 && sqrtf(t) >= h; ++k) t = __uint_as_float(__float_as_uint(t) - 1u);
+    for (int k = 0; k < 8 && sqrtf(t) < h; ++k) t = __uint_as_float(__float_as_uint(t) + 1u);
+    return t;
+}
+
+// Candidate filter of physics_fluid_neighbor_build.hlsli:48-69 on the packed tag: fluid with
+// invMass > kEps (bit 31), then environment / layer / mask.  Same-group candidates share the
+// self particle's (environment, layer, mask), so the answer is the self-compatibility bit.
+__device__ __forceinline__ bool neighborAllowed(const Scene &s, uint32_t tag, uint32_t myGroup, bool selfCompat,
+                                                uint4 m, uint32_t c)
+{
+    if ((tag & kFluidBit) == 0u) return false;
+    if ((tag & 0xffffu) == myGroup) return selfCompat;
+    const uint4 om = __ldg(&s.sMeta[c]);
+    return om.x == m.x && (m.w & om.z) != 0u && (om.w & m.z) != 0u;
+}
+
 // Neighbour list + density constraint.
 // physics_fluid_build_neighbors.cs.hlsl:21-147 fused with
 // physics_fluid_compute_density_lambda.cs.hlsl:26-115.  The density sum runs over the list in
 // list order with the same distance values, so it equals the reference's second pass.
-__global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Config cfg, bool density)
+//
+// mode 0: walk the 27 cells (runs from the per-run table of k_runNeighbors; a particle whose run
+//         mixes several cells looks its runs up itself);
+// mode 1: as mode 0, and also record every candidate within h * (1 + margin) ("superset", in
+//         traversal order) for the later iterations of this substep;
+// mode 2: filter the superset instead of walking the cells.  Cells are fixed for the substep and
+//         positions move only by the accumulated delta, so while 2 * max|delta| < margin * h every
+//         neighbour of this iteration is in the superset, and filtering it in order yields exactly
+//         the list the cell walk would build.  Otherwise (or if this particle's superset
+//         overflowed) the particle walks the cells.
+__global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Config cfg, bool density,
+                                                                    uint32_t mode, uint32_t iter)
 {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= s.N) return;
@@ -477,73 +562,123 @@ __global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Con
         return;
     }
     const float4 self = s.P[slot];
-    if (self.w <= kEps) {
+    if ((__float_as_uint(self.w) & kFluidBit) == 0u) { // invMass <= kEps
         if (density) s.Cs[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
         s.nbrCount[slot] = 0u;
+        if (mode == 1u) s.supCount[slot] = 0u;
         return;
     }
     const uint32_t maxN = s.maxNbr;
-    if (maxN == 0u) {
-        s.nbrCount[slot] = 0u;
-        if (!density) return;
-    }
-    const cn_fluid_material &fm = s.fluidMaterials[info & 0x7fffffffu];
+    const cn_fluid_material &fm = s.fluidMaterials[infoMaterial(info)];
     const float h = mx(fm.smoothing_radius, 1.0e-4f);
+    const float h2 = sqrtThreshold(h);
+    const float kW = spikyK(h);
     const float st = mx(fm.surface_tension, 0.0f);
     const f3 sp = xyz(self);
-    const uint4 m = s.sMeta[slot];
-    const int4 e = s.sCell[slot];
     uint32_t *out = s.nbr + size_t(slot) * maxN;
     uint32_t count = 0, truncated = 0;
     float rho = 0.0f;
     f3 normal{0.f, 0.f, 0.f};
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int tx = e.x + dx, ty = e.y + dy, tz = e.z + dz;
-                uint32_t start, end;
-                bool mixed;
-                if (!findRun(s, cellKey(tx, ty, tz), start, end, mixed)) continue;
-                if (!mixed) {
-                    const int4 ce = __ldg(&s.sCell[start]);
-                    if (ce.x != tx || ce.y != ty || ce.z != tz) continue;
-                }
-                for (uint32_t c = start; c < end; ++c) {
-                    if (mixed) {
-                        const int4 ce = __ldg(&s.sCell[c]);
-                        if (ce.x != tx || ce.y != ty || ce.z != tz) continue;
-                    }
-                    // ShouldProcessFluidNeighbor (physics_fluid_neighbor_build.hlsli:48-69)
-                    if (c == slot) continue;
-                    if ((__ldg(&s.sInfo[c]) & kFluidBit) == 0u) continue;
-                    const uint4 om = __ldg(&s.sMeta[c]);
-                    if (om.x != m.x) continue;
-                    if (!((m.w & om.z) != 0u && (om.w & m.z) != 0u)) continue;
-                    const float4 np = ld4(&s.P[c]);
-                    if (np.w <= kEps) continue;
-                    const f3 delta = sp - xyz(np);
-                    const float dist = length(delta);
-                    if (dist >= h) continue;
-                    if (count >= maxN) { truncated = 1; continue; }
-                    out[count++] = c;
-                    if (density) {
-                        rho += spikyW(dist, h);
-                        if (st > kEps) normal += spikyGrad(delta, dist, h);
-                    }
-                }
+
+    bool useSuperset = false;
+    if (mode == 2u) {
+        const float maxDelta = __uint_as_float(s.fluidMaxDelta[iter < kMaxTrackedIterations ? iter : 0u]);
+        useSuperset = iter < kMaxTrackedIterations && 2.0f * maxDelta < 0.99f * s.supMargin * h &&
+                      s.supCount[slot] <= s.supCap;
+    }
+    if (useSuperset) {
+        const uint32_t n = s.supCount[slot];
+        const uint32_t *sup = s.sup + size_t(slot) * s.supCap;
+        uint32_t cN = n > 0 ? sup[0] : 0u;
+        uint32_t cNN = n > 1 ? sup[1] : 0u;
+        float4 qN = n > 0 ? ld4(&s.P[cN]) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t c = cN;
+            const float4 q = qN;
+            if (k + 1 < n) {
+                cN = cNN;
+                if (k + 2 < n) cNN = sup[k + 2];
+                qN = ld4(&s.P[cN]);
             }
+            const f3 delta = sp - xyz(q);
+            const float d2 = dot(delta, delta);
+            if (d2 >= h2) continue;
+            if (count >= maxN) { truncated = 1; continue; }
+            out[count++] = c;
+            if (density) {
+                const float dist = sqrtf(d2);
+                rho += spikyWk(dist, h, kW);
+                if (st > kEps) normal += spikyGradK(delta, dist, h, kW);
+            }
+        }
+    } else {
+        const uint4 m = s.sMeta[slot];
+        const uint32_t myGroup = infoGroup(info);
+        const bool selfCompat = (m.w & m.z) != 0u;
+        const int4 e = s.sCell[slot];
+        const bool buildSup = mode == 1u;
+        const float supR = h * (1.0f + s.supMargin);
+        const float sup2 = supR * supR;
+        uint32_t *sup = buildSup ? s.sup + size_t(slot) * s.supCap : nullptr;
+        uint32_t supN = 0;
+        const uint32_t run = s.runIdx[slot] + s.runFlag[slot] - 1u;
+        const uint32_t runStart = s.runStartOf[run];
+        const bool ownLookups = (runStart >> 31) != 0u;
+        const uint2 *ranges = s.runNbr + size_t(run) * 27u;
+        int k = 0;
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx, ++k) {
+                    const int tx = e.x + dx, ty = e.y + dy, tz = e.z + dz;
+                    uint32_t start, end;
+                    bool check;
+                    if (!ownLookups) {
+                        const uint2 rg = __ldg(&ranges[k]);
+                        start = rg.x & 0x7fffffffu;
+                        end = rg.y;
+                        check = (rg.x >> 31) != 0u;
+                    } else {
+                        bool mixed;
+                        if (!findRun(s, cellKey(tx, ty, tz), start, end, mixed)) continue;
+                        check = true;
+                    }
+                    for (uint32_t c = start; c < end; ++c) {
+                        if (check) {
+                            const int4 ce = __ldg(&s.sCell[c]);
+                            if (ce.x != tx || ce.y != ty || ce.z != tz) continue;
+                        }
+                        const float4 q = ld4(&s.P[c]);
+                        if (c == slot || !neighborAllowed(s, __float_as_uint(q.w), myGroup, selfCompat, m, c)) continue;
+                        const f3 delta = sp - xyz(q);
+                        const float d2 = dot(delta, delta);
+                        if (buildSup && d2 < sup2) {
+                            if (supN < s.supCap) sup[supN] = c;
+                            ++supN;
+                        }
+                        if (d2 >= h2) continue;
+                        if (count >= maxN) { truncated = 1; continue; }
+                        out[count++] = c;
+                        if (density) {
+                            const float dist = sqrtf(d2);
+                            rho += spikyWk(dist, h, kW);
+                            if (st > kEps) normal += spikyGradK(delta, dist, h, kW);
+                        }
+                    }
+                }
+        if (buildSup) s.supCount[slot] = supN; // > supCap marks an overflowed superset
+    }
     s.nbrCount[slot] = count;
     if (truncated) atomicAdd(&s.meta_->neighborTruncations, 1u);
     if (!density) return;
     unsigned long long bm = s.sBoundary[slot];
     while (bm) {
-        const uint32_t k = __ffsll(bm) - 1;
+        const uint32_t kk = __ffsll(bm) - 1;
         bm &= bm - 1ull;
         f3 ghost;
-        if (!fluidGhostDelta(s, s.colQueryOrder[k], sp, h, ghost)) continue;
+        if (!fluidGhostDelta(s, s.colQueryOrder[kk], sp, h, ghost)) continue;
         const float dist = length(ghost);
         if (dist >= h) continue;
-        rho += spikyW(dist, h) * cfg.fluidBoundaryDensityScale;
+        rho += spikyWk(dist, h, kW) * cfg.fluidBoundaryDensityScale;
     }
     const float rho0 = mx(fm.rest_density, 1.0f);
     const float C = mx(rho - rho0, -rho0 * mx(cfg.fluidMaxUnderDensityRatio, 0.0f)) * fm.density_constraint_scale;
@@ -572,47 +707,71 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
     }
     const float4 self = s.P[slot];
     const f3 sdl = iter > 0 ? xyz(Dcur[slot]) : f3{0.f, 0.f, 0.f};
-    const cn_fluid_material &fm = s.fluidMaterials[info & 0x7fffffffu];
-    const uint32_t myMat = info & 0x7fffffffu;
+    const uint32_t myMat = infoMaterial(info);
+    const cn_fluid_material &fm = s.fluidMaterials[myMat];
     f3 packed{0.f, 0.f, 0.f};
     float weight = 0.0f;
-    if (self.w > kEps) {
+    if (__float_as_uint(self.w) & kFluidBit) {
         const f3 sp = xyz(self);
         const float4 snc = s.Cs[slot];
         const float sC = snc.w;
         const float h = mx(fm.smoothing_radius, 1.0e-4f);
+        const float kW = spikyK(h);
         const float cohesion = dt * mx(fm.cohesion, 0.0f);
         const float visc = dt * mx(fm.viscosity, 0.0f);
         const float st = mx(fm.surface_tension, 0.0f);
         const float cfl = mx(fm.cfl_radius, 0.0f);
+        const bool needRel = visc > kEps || cfl > kEps;
         const f3 sn = st > kEps ? xyz(snc) : f3{0.f, 0.f, 0.f};
         f3 dp{0.f, 0.f, 0.f};
         const uint32_t cnt = s.nbrCount[slot];
         const uint32_t *lst = s.nbr + size_t(slot) * s.maxNbr;
+        // Software-pipelined over the list: the next neighbour's slot, position word, constraint
+        // and accumulated delta are in flight while the current pair term is computed.
+        const bool relLoads = needRel && iter > 0;
+        const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t cN = cnt > 0 ? lst[0] : 0u;
+        uint32_t cNN = cnt > 1 ? lst[1] : 0u;
+        float4 npN = cnt > 0 ? ld4(&s.P[cN]) : zero4;
+        float cwN = cnt > 0 ? __ldg(&s.Cs[cN].w) : 0.0f;
+        float4 dN = (cnt > 0 && relLoads) ? ld4(&Dcur[cN]) : zero4;
         for (uint32_t k = 0; k < cnt; ++k) {
-            const uint32_t c = lst[k];
-            const float4 np = ld4(&s.P[c]);
-            if (np.w <= kEps) continue;
-            const f3 nd = iter > 0 ? xyz(ld4(&Dcur[c])) : f3{0.f, 0.f, 0.f};
+            const uint32_t c = cN;
+            const float4 np = npN;
+            const float ncw = cwN;
+            const float4 nd4 = dN;
+            if (k + 1 < cnt) {
+                cN = cNN;
+                if (k + 2 < cnt) cNN = lst[k + 2];
+                npN = ld4(&s.P[cN]);
+                cwN = __ldg(&s.Cs[cN].w);
+                if (relLoads) dN = ld4(&Dcur[cN]);
+            }
+            const uint32_t tag = __float_as_uint(np.w);
+            if ((tag & kFluidBit) == 0u) continue;
             const f3 delta = sp - xyz(np);
             const float dist = length(delta);
             if (dist >= h || dist <= kEps) continue;
-            const float4 nnc = ld4(&s.Cs[c]);
             const f3 nij = delta / dist;
-            const float dw = spikyDW(dist, h);
-            f3 pd = -0.5f * (sC + nnc.w) * dw * nij;
-            if ((__ldg(&s.sInfo[c]) & 0x7fffffffu) == myMat) {
-                const f3 rel = sdl - nd;
+            // spikyDW / spikyW of physics_fluid_common.hlsli:17-41 sharing 1 - dist / h
+            const float om = 1.0f - dist / h;
+            const float dw = -2.0f * kW * om / h;
+            f3 pd = -0.5f * (sC + ncw) * dw * nij;
+            if (infoMaterial(tag) == myMat) {
                 if (cohesion > kEps) pd -= nij * (cohesion * cohesionW(dist, h, fm.cohesion1, fm.cohesion2));
-                if (visc > kEps) {
-                    const float vs = 1.0f - (1.0f / (1.0f + visc * spikyW(dist, h)));
-                    pd -= vs * rel;
+                if (needRel) {
+                    const f3 nd = iter > 0 ? xyz(nd4) : f3{0.f, 0.f, 0.f};
+                    const f3 rel = sdl - nd;
+                    if (visc > kEps) {
+                        const float vs = 1.0f - (1.0f / (1.0f + visc * (kW * om * om)));
+                        pd -= vs * rel;
+                    }
+                    if (cfl > kEps) {
+                        const float proj = dot(rel, nij);
+                        if (proj < -cfl) pd -= nij * (proj + cfl) * 0.5f;
+                    }
                 }
-                if (cfl > kEps) {
-                    const float proj = dot(rel, nij);
-                    if (proj < -cfl) pd -= nij * (proj + cfl) * 0.5f;
-                }
-                if (st > kEps) pd -= dt * (sn - xyz(nnc));
+                if (st > kEps) pd -= dt * (sn - xyz(ld4(&s.Cs[c])));
             }
             dp += pd;
             weight += 1.0f;
@@ -627,7 +786,7 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
             const float dist = length(ghost);
             if (dist <= kEps || dist >= h) continue;
             const f3 nij = ghost / dist;
-            const float dw = spikyDW(dist, h);
+            const float dw = spikyDWk(dist, h, kW);
             bd += -mx(sC, 0.0f) * dw * nij;
         }
         bd = bd * cfg.fluidBoundaryDeltaScale;
@@ -1511,11 +1670,15 @@ void launchPredictAndKeys(const Scene &s, float dt, const Config &c, cudaStream_
                                                        s.entries != nullptr);
 }
 
-void launchCellSetup(const Scene &s, cudaStream_t st)
+void launchCellSetup(const Scene &s, uint32_t *scanTmp, cudaStream_t st)
 {
     if (s.N == 0) return;
     cudaMemsetAsync(s.tableKeys, 0xff, size_t(s.tableMask + 1) * sizeof(uint32_t), st);
     k_cellSetup<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+    if (s.runFlag) {
+        exclusiveScan(s.runFlag, s.runIdx, s.N, scanTmp, scanTmp + 1, st);
+        k_runNeighbors<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+    }
 }
 
 void launchRigidCandidates(const Scene &s, uint32_t *scanTmp, size_t, cudaStream_t st)
@@ -1543,10 +1706,11 @@ void launchFluidGather(const Scene &s, uint32_t iter, cudaStream_t st)
     k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, Dcur, iter);
 }
 
-void launchFluidNeighborsDensity(const Scene &s, const Config &c, cudaStream_t st)
+void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter, cudaStream_t st)
 {
     if (s.N == 0) return;
-    k_fluidNeighborsDensity<<<blocksFor(s.N), kThreads, 0, st>>>(s, c, true);
+    const uint32_t mode = s.sup == nullptr ? 0u : (iter == 0 ? 1u : 2u);
+    k_fluidNeighborsDensity<<<blocksFor(s.N), kThreads, 0, st>>>(s, c, true, mode, iter);
 }
 
 void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
@@ -1562,7 +1726,7 @@ void launchFluidIteration(const Scene &s, uint32_t iter, float dt, const Config 
                           cudaStream_t st)
 {
     launchFluidGather(s, iter, st);
-    launchFluidNeighborsDensity(s, c, st);
+    launchFluidNeighborsDensity(s, c, iter, st);
     launchFluidDeltaApplyClamp(s, iter, dt, c, writeDebug, st);
 }
 
@@ -1572,7 +1736,7 @@ void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)
     // Positions after the velocity update; the accumulated delta was folded into x.
     k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, s.Da, 0u);
     Config dummy{};
-    k_fluidNeighborsDensity<<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false);
+    k_fluidNeighborsDensity<<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u, 0u);
 }
 
 void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st)

@@ -193,6 +193,31 @@ __host__ __device__ __forceinline__ f3 spikyGrad(f3 delta, float d, float h)
     const float dw = spikyDW(d, h);
     return dw * (delta / d);
 }
+// The same kernels with the normalisation 15 / (pi h^3) passed in: a per-material constant whose
+// value does not depend on the neighbour, so computing it once per particle changes no bits.
+__host__ __device__ __forceinline__ float spikyK(float h)
+{
+    const float h3 = h * h * h;
+    return 15.0f / (3.14159265359f * h3);
+}
+__host__ __device__ __forceinline__ float spikyWk(float d, float h, float k)
+{
+    if (d >= h) return 0.0f;
+    const float om = 1.0f - d / h;
+    return k * om * om;
+}
+__host__ __device__ __forceinline__ float spikyDWk(float d, float h, float k)
+{
+    if (d <= kEps || d >= h) return 0.0f;
+    const float om = 1.0f - d / h;
+    return -2.0f * k * om / h;
+}
+__host__ __device__ __forceinline__ f3 spikyGradK(f3 delta, float d, float h, float k)
+{
+    if (d <= kEps || d >= h) return f3{0.f, 0.f, 0.f};
+    const float dw = spikyDWk(d, h, k);
+    return dw * (delta / d);
+}
 __host__ __device__ __forceinline__ float cohesionW(float d, float h, float c1, float c2)
 {
     if (d <= kEps || d >= h) return 0.0f;

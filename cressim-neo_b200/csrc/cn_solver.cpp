@@ -7,6 +7,7 @@
 // dispatches with provably empty inputs (for example particle-particle contacts in a scene
 // whose particles are all fluid) are not launched.
 #include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -187,6 +188,7 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const Incidence 
     s.fluidMatIdx = a.take<uint32_t>(N);
     s.ownerTypes = a.take<uint32_t>(N);
     s.ownerIdx = a.take<uint32_t>(N);
+    s.fluidGroup = a.take<uint32_t>(N);
     s.adjOff = a.take<uint32_t>(N);
     s.adjCnt = a.take<uint32_t>(N);
     s.adjIdx = a.take<uint32_t>(std::max<uint32_t>(w.adjacency_index_count, 1u));
@@ -258,6 +260,16 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const Incidence 
         s.sMeta = a.take<uint4>(N);
         s.sInfo = a.take<uint32_t>(N);
         s.sBoundary = a.take<unsigned long long>(N);
+        s.runFlag = a.take<uint32_t>(N);
+        s.runIdx = a.take<uint32_t>(N);
+        s.runStartOf = a.take<uint32_t>(N);
+        s.runNbr = a.take<uint2>(size_t(N) * 27u);
+        s.fluidMaxDelta = a.take<uint32_t>(64);
+        if (!sv->ppPossible) { // fluid x is fixed during the iterations: superset lists are exact
+            s.supCap = 160u;
+            s.sup = a.take<uint32_t>(size_t(N) * s.supCap);
+            s.supCount = a.take<uint32_t>(N);
+        }
         s.maxNbr = sv->desc.max_fluid_neighborhood;
         s.nbr = a.take<uint32_t>(std::max<size_t>(size_t(N) * s.maxNbr, 1));
         s.nbrCount = a.take<uint32_t>(N);
@@ -301,7 +313,7 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             probe(sv, "radix_sort", st, [&] {
                 cn::radixSortPairs(s.keysA, s.valsA, s.keysB, s.valsB, N, sv->sortScratch, &s.meta_->waitTimeouts, st);
             });
-            probe(sv, "cell_setup", st, [&] { cn::launchCellSetup(s, st); });
+            probe(sv, "cell_setup", st, [&] { cn::launchCellSetup(s, sv->scanScratch, st); });
         }
         if (sv->ppPossible)
             probe(sv, "particle_candidates", st, [&] { cn::launchParticleCandidates(s, sv->scanScratch, sv->scanScratchBytes, st); });
@@ -314,6 +326,7 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
         if (s.SD) cudaMemsetAsync(s.distLambda, 0, sizeof(float) * s.SD, st);
         if (s.S) cudaMemsetAsync(s.segLambda, 0, sizeof(float4) * s.S, st);
         if (s.J) cudaMemsetAsync(s.jointLambda, 0, sizeof(float4) * s.J, st);
+        if (s.fluidMaxDelta) cudaMemsetAsync(s.fluidMaxDelta, 0, sizeof(uint32_t) * 64, st);
         if (sv->ppPossible) {
             cudaMemsetAsync(s.posCorr, 0, sizeof(float4) * N, st);
             cudaMemsetAsync(s.velCorr, 0, sizeof(float4) * N, st);
@@ -327,7 +340,7 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             if (!runFluid && !runSoft && !runPP && !runRigid) break; // remaining iterations are empty
             if (runFluid) {
                 probe(sv, "fluid_gather", st, [&] { cn::launchFluidGather(s, it, st); });
-                probe(sv, "fluid_neighbors_density", st, [&] { cn::launchFluidNeighborsDensity(s, c, st); });
+                probe(sv, "fluid_neighbors_density", st, [&] { cn::launchFluidNeighborsDensity(s, c, it, st); });
                 probe(sv, "fluid_delta_apply_clamp", st,
                       [&] { cn::launchFluidDeltaApplyClamp(s, it, dt, c, sv->writeFluidDebug, st); });
             }
@@ -489,6 +502,27 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     sv->rigidPossible = contactWork && N > 0 && w->collider_count > 0 && anySolid;
     sv->hasBroadphase = N > 0 && ((contactWork && N > 1) || anyFluid || w->collider_count > 0);
 
+    // Fluid filter groups: dense ids of the distinct (environment, layer, mask) triples.
+    std::vector<uint32_t> fluidGroup(N, 0u);
+    {
+        std::vector<std::array<uint32_t, 3>> groups;
+        for (uint32_t i = 0; i < N; ++i) {
+            if (w->kinds[i] != CN_PARTICLE_FLUID) continue;
+            const std::array<uint32_t, 3> key{w->metadata[4 * i], w->metadata[4 * i + 2], w->metadata[4 * i + 3]};
+            auto it = std::find(groups.begin(), groups.end(), key);
+            if (it == groups.end()) {
+                if (groups.size() >= 0xffffu)
+                    return setError(CN_ERR_UNSUPPORTED, "more than 65535 fluid (environment, layer, mask) groups");
+                groups.push_back(key);
+                it = groups.end() - 1;
+            }
+            fluidGroup[i] = uint32_t(it - groups.begin());
+        }
+        for (uint32_t m = 0; m < N; ++m)
+            if (w->kinds[m] == CN_PARTICLE_FLUID && w->fluid_material_indices[m] > 0x7fffu)
+                return setError(CN_ERR_UNSUPPORTED, "fluid material index above 32767");
+    }
+
     // Collider query order: moving (kinematic) colliders, then static, ascending index.
     std::vector<uint32_t> order, stat;
     for (uint32_t c = 0; c < w->collider_count; ++c) {
@@ -568,6 +602,7 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     CN_CUDA(up(s.fluidMatIdx, w->fluid_material_indices, N, st));
     CN_CUDA(up(s.ownerTypes, w->owner_types, N, st));
     CN_CUDA(up(s.ownerIdx, w->owner_indices, N, st));
+    CN_CUDA(up(s.fluidGroup, fluidGroup.data(), N, st));
     CN_CUDA(up(s.adjOff, w->adjacency_offsets, N, st));
     CN_CUDA(up(s.adjCnt, w->adjacency_counts, N, st));
     CN_CUDA(up(s.adjIdx, w->adjacency_indices, w->adjacency_index_count, st));
