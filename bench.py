@@ -118,11 +118,14 @@ def peaks():
 # Algorithmic bytes per particle of one launch of each fluid kernel (compulsory traffic; neighbour
 # entries count 4 B).  Neighbour build + density: position P (16) + cell entry (16) + metadata (16)
 # + kind/material (4) + boundary mask (8), list writes 4*nbar, count (4), constraint write (16).
+# The first iteration of a substep also writes the superset list (4*nsup + 4 for its count).
 # Delta + apply + clamp: P (16) + x (16) + accumulated delta r/w (32) + constraint (16) + list reads
 # 4*nbar + count (4) + kind/material (4) + boundary mask (8) + packed delta write (16 when kept).
-def kernel_bytes(name: str, nbar: float) -> float | None:
+def kernel_bytes(name: str, nbar: float, nsup: float = 0.0) -> float | None:
     if name == "fluid_neighbors_density":
         return 80.0 + 4.0 * nbar
+    if name == "fluid_neighbors_superset":
+        return 84.0 + 4.0 * nbar + 4.0 * nsup
     if name == "fluid_delta_apply_clamp":
         return 96.0 + 4.0 * nbar
     if name == "fluid_gather":
@@ -161,11 +164,14 @@ def run_ours(args):
     n = soa.particle_count
     solver = Solver(desc, device=local)
     solver.sync_world(soa)
-    solver.set_timing(True)
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: the C ABI reads a NULL stream as "the solver's own stream", and torch's
+    # default stream has handle 0, so stepping on it would leave the events below unordered.
+    stream = torch.cuda.Stream(device=local)
     sh = stream.cuda_stream
+    assert sh != 0
     solver.step_many(dt, max(args.warmup, 0), sh)
     torch.cuda.synchronize()
+    x0, v0, _ = solver.read_particles()  # the timed frames are replayed below for the kernel split
     uuid = None
     try:
         uuid = str(torch.cuda.get_device_properties(local).uuid)
@@ -176,12 +182,14 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record(stream)
-    for _ in range(args.steps):
+    marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    marks[0].record(stream)
+    for i in range(args.steps):
         solver.step_many(dt, 1, sh)
-    end.record(stream)
+        marks[i + 1].record(stream)
     torch.cuda.synchronize()
+    start, end = marks[0], marks[-1]
+    step_ms = sorted(marks[i].elapsed_time(marks[i + 1]) for i in range(args.steps))
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
@@ -194,9 +202,22 @@ def run_ours(args):
     total_units = float(n) * substeps * args.steps * world
     value = total_units / (ms / 1e3)
     meta = solver.validate_gpu_meta()
-    ktimes = solver.kernel_times()
     kernels_per_frame, _ = solver.graph_stats()
-    counts = solver_neighbor_mean(solver)
+    counts, sup_counts = solver_neighbor_mean(solver)
+
+    # Kernel split: the same frames again from the same state, with event probes around every
+    # kernel group of the captured frame, read back after each frame and averaged.
+    solver.write_particles(x0, v0)
+    solver.set_timing(True)
+    ktimes = {}
+    for _ in range(args.steps):
+        solver.step_many(dt, 1, sh)
+        for k, (t, launches) in solver.kernel_times().items():
+            acc = ktimes.setdefault(k, [0.0, 0])
+            acc[0] += t / args.steps
+            acc[1] += launches / args.steps
+    solver.set_timing(False)
+    probe_frame_ms = sum(t for t, _ in ktimes.values())
 
     # e2e through the C ABI: pinned host state uploaded and read back every frame
     xh = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
@@ -225,32 +246,43 @@ def run_ours(args):
         e2e_s = float(t.item())
     e2e_value = float(n) * substeps * e2e_steps * world / e2e_s
 
+    def pct(q):
+        return round(step_ms[min(len(step_ms) - 1, int(q * len(step_ms)))], 4)
+
     hbm, peak_kind = peaks()
     dominant = max((k for k in ktimes if kernel_bytes(k, counts) is not None), key=lambda k: ktimes[k][0], default=None)
     roofline = None
     if dominant:
         tot_ms, launches = ktimes[dominant]
         per_launch_s = tot_ms / launches / 1e3
-        algo = kernel_bytes(dominant, counts) * n
+        algo = kernel_bytes(dominant, counts, sup_counts) * n
         achieved = algo / per_launch_s / 1e9
         tr = traffic_from_profiles().get(dominant)
         roofline = {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": hbm,
                     "peak_kind": f"{peak_kind} copy bandwidth", "unit": "GB/s", "frac": round(achieved / hbm, 4),
                     "traffic": tr, "algorithmic_bytes_per_launch": algo, "launch_ms": round(tot_ms / launches, 4)}
-    frame_ms_device = sum(t for t, _ in ktimes.values())
+    per_kernel = {}
+    for k, (tot_ms, launches) in ktimes.items():
+        b = kernel_bytes(k, counts, sup_counts)
+        if b is not None and tot_ms > 0:
+            per_kernel[k] = {"launch_ms": round(tot_ms / launches, 4),
+                             "achieved_gbs": round(b * n / (tot_ms / launches / 1e3) / 1e9, 1)}
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": "particle-substeps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "step_latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "max": round(step_ms[-1], 4)},
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD if dims == (128, 64, 128) else f"pbf_dam_break_{dims[0]}x{dims[1]}x{dims[2]}",
                    "particles": n, "substeps": substeps, "fluid_iterations": desc.fluid_iterations,
                    "frame_dt": dt, "parallelism": f"replicas{world}", "l2": "working set > L2 (~0.9 GB resident)",
-                   "mean_neighbors": round(counts, 2)},
+                   "mean_neighbors": round(counts, 2), "mean_superset": round(sup_counts, 2)},
         "e2e": {"value": round(e2e_value, 1), "unit": "particle-substeps/s", "h2d_bytes_per_step": 32 * n,
                 "d2h_bytes_per_step": 32 * n, "steps": e2e_steps},
         "gpu_launches": int(kernels_per_frame) * args.steps,
         "roofline": roofline,
         "kernel_ms_per_frame": {k: round(t, 4) for k, (t, _) in sorted(ktimes.items(), key=lambda kv: -kv[1][0])},
+        "kernel_split_frame_ms": round(probe_frame_ms, 4),
+        "kernel_roofline": per_kernel,
         "substep_model_bytes_per_particle": substep_bytes(counts, desc.fluid_iterations),
         "clocks": clk,
         "meta_status": meta["status"],
@@ -265,9 +297,10 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
-def solver_neighbor_mean(solver) -> float:
+def solver_neighbor_mean(solver) -> tuple:
     c = solver.debug_read("fluid_neighbor_counts").view(np.uint32)
-    return float(c.mean()) if c.size else 0.0
+    sc = solver.debug_read("fluid_superset_counts").view(np.uint32)
+    return (float(c.mean()) if c.size else 0.0), (float(sc.mean()) if sc.size else 0.0)
 
 
 def cpu_baseline(budget_s: float = 15.0, dims=(64, 32, 64), max_frames: int = 8):

@@ -27,7 +27,8 @@ STATUS = {0: "OK", 1: "INVALID_ARGUMENT", 2: "CUDA", 3: "OUT_OF_MEMORY", 4: "NOT
           5: "CAPACITY", 6: "NO_DEVICE", 7: "DEVICE_TIMEOUT", 8: "UNSUPPORTED"}
 
 DEBUG = {"cell_entries": 0, "sorted_keys": 1, "cell_ranges": 2, "fluid_neighbor_counts": 3,
-         "fluid_neighbors": 4, "fluid_constraints": 5, "fluid_delta": 6, "rigid_contacts": 7}
+         "fluid_neighbors": 4, "fluid_constraints": 5, "fluid_delta": 6, "rigid_contacts": 7,
+         "fluid_superset_counts": 8}
 
 SolverDesc = _abi.SolverDesc
 

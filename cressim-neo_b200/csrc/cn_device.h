@@ -110,6 +110,9 @@ struct Scene {
     float4 *prevBodyPos = nullptr, *prevBodyRot = nullptr;
     float4 *predBodyPos = nullptr, *predBodyRot = nullptr, *predBodyLin = nullptr, *predBodyAng = nullptr;
     float4 *colAabbMin = nullptr, *colAabbMax = nullptr;
+    // Per collider, the world frame the fluid boundary queries use this substep (4 float4:
+    // centre + shape/enabled word, orientation, shape extents, capsule end).
+    float4 *colFrame = nullptr;
     const uint32_t *colQueryOrder = nullptr; // moving colliders first, then static
     uint32_t colQueryCount = 0, activeMovingCount = 0;
 
@@ -122,8 +125,21 @@ struct Scene {
     uint32_t *cellEnd = nullptr;      // at a run start: end | (mixed-coordinate flag << 31)
     uint32_t *runFlag = nullptr;      // 1 at a run start (fluid scenes)
     uint32_t *runIdx = nullptr;       // exclusive scan of runFlag
-    uint32_t *runStartOf = nullptr;   // per run: start slot | (mixed << 31)
-    uint2 *runNbr = nullptr;          // per run: 27 neighbour runs (start | check << 31, end)
+    // Fluid scenes solve in "compute order": the runs of the key sort re-ordered along a Morton
+    // curve of their cells, each run's particles kept in sorted order.  Runs are numbered r in
+    // key order and j in compute order.
+    uint32_t *runStartOf = nullptr;   // per run j: compute start | (mixed << 31)
+    uint2 *runNbr = nullptr;          // per run j: 27 neighbour runs (compute start | check << 31, end)
+    uint32_t *runKey = nullptr, *runVal = nullptr, *runKeyB = nullptr, *runValB = nullptr; // run sort (j -> r)
+    uint32_t *runHashStart = nullptr; // per run r: key-order start | (mixed << 31)
+    uint32_t *runLen = nullptr;       // per run r: particle count
+    uint32_t *runLenSorted = nullptr; // per run j: particle count (0 past the last run)
+    uint32_t *runCompStart = nullptr; // per run j: compute start (exclusive scan of runLenSorted)
+    uint32_t *runComp = nullptr;      // per run r: compute start
+    uint32_t *runPos = nullptr;       // per run r: j
+    uint32_t *cvals = nullptr;        // compute slot -> particle
+    int4 *cCell = nullptr;            // compute slot -> cell coordinates
+    uint32_t *cRun = nullptr;         // compute slot -> run j
 
     // ---- fluid (cell order) ----
     uint32_t hasFluid = 0;
@@ -170,7 +186,9 @@ struct Config {
 // ------------------------------------------------------------------ launchers (cn_kernels.cu)
 void launchRigidPredict(const Scene &s, float dt, float gx, float gy, float gz, cudaStream_t st);
 void launchPredictAndKeys(const Scene &s, float dt, const Config &c, cudaStream_t st);
-void launchCellSetup(const Scene &s, uint32_t *scanTmp, cudaStream_t st);
+void launchCellSetup(const Scene &s, uint32_t *scanTmp, void *sortScratch, cudaStream_t st);
+// Neighbour and superset lists: entry k of compute slot i at k * N + i (true) or i * cap + k.
+bool fluidListsInterleaved();
 void launchRigidCandidates(const Scene &s, uint32_t *scanTmp, size_t scanTmpBytes, cudaStream_t st);
 void launchParticleCandidates(const Scene &s, uint32_t *scanTmp, size_t scanTmpBytes, cudaStream_t st);
 void launchFluidIteration(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,

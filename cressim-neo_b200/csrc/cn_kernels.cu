@@ -23,6 +23,11 @@ namespace cn {
 namespace {
 
 constexpr int kThreads = 256;
+#ifndef CN_LIST_ROW_MAJOR
+constexpr bool kInterleavedLists = true;
+#else
+constexpr bool kInterleavedLists = false;
+#endif
 inline unsigned blocksFor(uint32_t n) { return n == 0 ? 1u : (n + kThreads - 1) / kThreads; }
 // Per-slot fluid word: bit 31 = fluid particle, bits 16..30 = fluid material, bits 0..15 = filter
 // group (a dense id of the particle's (environment, layer, mask) triple).  P.w carries the same
@@ -122,6 +127,41 @@ __global__ void __launch_bounds__(kThreads) k_rigidPredict(Scene s, float dt, fl
         s.colAabbMin[c] = mk4(lo, 0.f);
         s.colAabbMax[c] = mk4(hi, 0.f);
     }
+    // Collider frames for the fluid boundary queries, with the arithmetic of
+    // physics_fluid_boundary_common.hlsli:11-40 (unscaled local offset), done once per collider.
+    for (uint32_t c = threadIdx.x; c < s.C; c += blockDim.x) {
+        const cn_collider_broadphase bp = s.colBp[c];
+        float4 *fr = s.colFrame + size_t(c) * 4;
+        const uint32_t b = bp.owner_body;
+        if (bp.enabled_flag == 0u || b >= s.B) {
+            fr[0] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0u));
+            continue;
+        }
+        const f3 bpos = xyz(s.predBodyPos[b]);
+        const float4 bq = qNormalize(s.predBodyRot[b]);
+        const float4 sc = s.bodyScale[b];
+        const cn_collider_geometry cg = s.colGeo[c];
+        const f3 cwp = bpos + qRotate(bq, f3{cg.local_position[0], cg.local_position[1], cg.local_position[2]});
+        const float4 cwq = qNormalize(qMul(bq, qNormalize(make_float4(cg.local_orientation[0], cg.local_orientation[1],
+                                                                      cg.local_orientation[2], cg.local_orientation[3]))));
+        const float4 sp = make_float4(cg.shape_params[0], cg.shape_params[1], cg.shape_params[2], cg.shape_params[3]);
+        float4 e0 = make_float4(0.f, 0.f, 0.f, 0.f), e1 = e0;
+        if (bp.shape_type == CN_COLLIDER_SPHERE) {
+            e0.x = sphereRadius(sp, sc);
+        } else if (bp.shape_type == CN_COLLIDER_BOX) {
+            e0 = mk4(boxHalfExtents(sp, sc), 0.f);
+        } else {
+            f3 a, b2;
+            float cr = 0.0f;
+            capsuleSegment(cwp, cwq, sp, sc, a, b2, cr);
+            e0 = mk4(a, cr);
+            e1 = mk4(b2, 0.f);
+        }
+        fr[0] = mk4(cwp, __uint_as_float(1u | (bp.shape_type << 8)));
+        fr[1] = cwq;
+        fr[2] = e0;
+        fr[3] = e1;
+    }
 }
 
 // physics_rigid_update_velocities (copyPredictedRigidBodiesToPersistentState)
@@ -210,20 +250,9 @@ __global__ void __launch_bounds__(kThreads) k_cellSetup(Scene s)
     if (slot >= s.N) return;
     const uint32_t p = s.valsA[slot];
     const uint32_t key = s.keysA[slot];
-    s.rank[p] = slot;
+    if (!s.hasFluid) s.rank[p] = slot; // fluid scenes rank particles in compute order
     const int4 e = s.entries[p];
     s.sCell[slot] = e;
-    if (s.hasFluid) {
-        const uint32_t kind = s.kinds[p];
-        const bool fluid = kind == CN_PARTICLE_FLUID;
-        s.sMeta[slot] = s.meta[p];
-        s.sInfo[slot] = fluid ? (kFluidBit | ((s.fluidMatIdx[p] & 0x7fffu) << 16) | (s.fluidGroup[p] & 0xffffu)) : 0u;
-        unsigned long long mask = 0ull;
-        if (fluid && s.colQueryCount > 0) {
-            if (fluidBoundaryMaskFor(s, p, xyz(s.x[p]), mask)) atomicAdd(&s.meta_->boundaryMaskOverflow, 1u);
-        }
-        s.sBoundary[slot] = mask;
-    }
     const bool start = slot == 0 || s.keysA[slot - 1] != key;
     if (s.runFlag) s.runFlag[slot] = start ? 1u : 0u;
     if (!start) return;
@@ -268,32 +297,122 @@ __device__ __forceinline__ bool findRun(const Scene &s, uint32_t key, uint32_t &
     return false;
 }
 
-// Per cell run: the 27 neighbour runs in the reference's traversal order (dz, dy, dx), looked up
-// once per substep.  Entry k = (start | checkCoordinates << 31, end); empty when the target cell
-// has no run or its (uniform) run holds another cell that hashes to the same key.
-__global__ void __launch_bounds__(kThreads) k_runNeighbors(Scene s)
+// Compute order (fluid scenes).  The key sort groups each cell's particles into a run but
+// scatters neighbouring cells over the whole array (the key is a hash).  The fluid kernels
+// instead walk the runs along a Morton curve of their cells, so a warp's particles share
+// neighbour cells and their gathers hit in L1.  Inside a run the particles keep their sorted
+// order, which is all the reference's neighbour order depends on (cells in (dz, dy, dx) order,
+// each cell's particles in sorted order), so results are unchanged.
+__device__ __forceinline__ uint32_t spreadBits3(uint32_t v)
+{
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+// 30-bit Morton code of the low 10 bits of each cell coordinate (wrapping only costs locality).
+__device__ __forceinline__ uint32_t cellMorton(int4 e)
+{
+    return spreadBits3(uint32_t(e.x)) | (spreadBits3(uint32_t(e.y)) << 1) | (spreadBits3(uint32_t(e.z)) << 2);
+}
+
+__device__ __forceinline__ uint32_t runOfSlot(const Scene &s, uint32_t slot)
+{
+    return s.runIdx[slot] + s.runFlag[slot] - 1u;
+}
+
+// Per run r (at its key-order start): sort key, start and length.
+__global__ void __launch_bounds__(kThreads) k_runKeys(Scene s)
 {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= s.N || s.runFlag[slot] == 0u) return;
     const uint32_t r = s.runIdx[slot];
-    const uint32_t mixedHere = s.cellEnd[slot] >> 31;
-    s.runStartOf[r] = slot | (mixedHere << 31);
-    const int4 e = s.sCell[slot];
-    uint2 *out = s.runNbr + size_t(r) * 27u;
+    const uint32_t ce = s.cellEnd[slot];
+    s.runKey[r] = cellMorton(s.sCell[slot]);
+    s.runHashStart[r] = slot | (ce & 0x80000000u);
+    s.runLen[r] = (ce & 0x7fffffffu) - slot;
+}
+
+// Per sorted run j: its length (0 for the padding past the last run).
+__global__ void __launch_bounds__(kThreads) k_runLengths(Scene s)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= s.N) return;
+    s.runLenSorted[j] = s.runKey[j] != kInvalid ? s.runLen[s.runVal[j]] : 0u;
+}
+
+// Per sorted run j: compute start, and the r -> (compute start, j) maps.
+__global__ void __launch_bounds__(kThreads) k_runPlace(Scene s)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= s.N || s.runKey[j] == kInvalid) return;
+    const uint32_t r = s.runVal[j];
+    const uint32_t cs = s.runCompStart[j];
+    s.runComp[r] = cs;
+    s.runPos[r] = j;
+    s.runStartOf[j] = cs | (s.runHashStart[r] & 0x80000000u);
+}
+
+// Per key-order slot: its compute slot, and the per-particle data the fluid kernels read there.
+__global__ void __launch_bounds__(kThreads) k_computeOrderSetup(Scene s)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= s.N) return;
+    const uint32_t r = runOfSlot(s, slot);
+    const uint32_t cslot = s.runComp[r] + (slot - (s.runHashStart[r] & 0x7fffffffu));
+    const uint32_t p = s.valsA[slot];
+    s.cvals[cslot] = p;
+    s.rank[p] = cslot;
+    s.cCell[cslot] = s.sCell[slot];
+    s.cRun[cslot] = s.runPos[r];
+    const bool fluid = s.kinds[p] == CN_PARTICLE_FLUID;
+    s.sMeta[cslot] = s.meta[p];
+    s.sInfo[cslot] = fluid ? (kFluidBit | ((s.fluidMatIdx[p] & 0x7fffu) << 16) | (s.fluidGroup[p] & 0xffffu)) : 0u;
+    unsigned long long mask = 0ull;
+    if (fluid && s.colQueryCount > 0) {
+        if (fluidBoundaryMaskFor(s, p, xyz(s.x[p]), mask)) atomicAdd(&s.meta_->boundaryMaskOverflow, 1u);
+    }
+    s.sBoundary[cslot] = mask;
+}
+
+// The run of cell key `key` in compute slots (FindCellRange semantics).
+__device__ __forceinline__ bool findRunCompute(const Scene &s, uint32_t key, uint32_t &start, uint32_t &end,
+                                               bool &mixed)
+{
+    uint32_t hs, he;
+    if (!findRun(s, key, hs, he, mixed)) return false;
+    start = __ldg(&s.runComp[__ldg(&s.runIdx[hs])]);
+    end = start + (he - hs);
+    return true;
+}
+
+// Per run j: the 27 neighbour runs in the reference's traversal order (dz, dy, dx), looked up
+// once per substep.  Entry k = (compute start | checkCoordinates << 31, end); empty when the
+// target cell has no run or its (uniform) run holds another cell that hashes to the same key.
+__global__ void __launch_bounds__(kThreads) k_runNeighbors(Scene s)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= s.N || s.runKey[j] == kInvalid) return;
+    const uint32_t r = s.runVal[j];
+    const int4 e = s.sCell[s.runHashStart[r] & 0x7fffffffu];
+    uint2 *out = s.runNbr + size_t(j) * 27u;
     int k = 0;
     for (int dz = -1; dz <= 1; ++dz)
         for (int dy = -1; dy <= 1; ++dy)
             for (int dx = -1; dx <= 1; ++dx, ++k) {
                 const int tx = e.x + dx, ty = e.y + dy, tz = e.z + dz;
-                uint32_t start = 0, end = 0;
+                uint32_t hs = 0, he = 0;
                 bool mixed = false;
                 uint2 rg = make_uint2(0u, 0u);
-                if (findRun(s, cellKey(tx, ty, tz), start, end, mixed)) {
+                if (findRun(s, cellKey(tx, ty, tz), hs, he, mixed)) {
+                    const uint32_t cs = s.runComp[s.runIdx[hs]];
                     if (mixed) {
-                        rg = make_uint2(start | 0x80000000u, end);
+                        rg = make_uint2(cs | 0x80000000u, cs + (he - hs));
                     } else {
-                        const int4 ce = s.sCell[start];
-                        if (ce.x == tx && ce.y == ty && ce.z == tz) rg = make_uint2(start, end);
+                        const int4 ce = s.sCell[hs];
+                        if (ce.x == tx && ce.y == ty && ce.z == tz) rg = make_uint2(cs, cs + (he - hs));
                     }
                 }
                 out[k] = rg;
@@ -434,7 +553,7 @@ __global__ void __launch_bounds__(kThreads) k_fluidGather(Scene s, float4 *Xs, c
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     float largest = 0.0f;
     if (slot < s.N) {
-        const float4 xp = s.x[s.valsA[slot]];
+        const float4 xp = s.x[s.cvals[slot]];
         const f3 d = iter > 0 ? xyz(Dcur[slot]) : f3{0.f, 0.f, 0.f};
         const uint32_t info = s.sInfo[slot];
         const uint32_t tag = (info & 0x7fffffffu) | ((info & kFluidBit) && xp.w > kEps ? kFluidBit : 0u);
@@ -455,25 +574,21 @@ __device__ bool fluidBoundaryContactInfo(const Scene &s, uint32_t c, f3 pos, flo
 {
     sd = 0.0f;
     n = f3{0.f, 1.f, 0.f};
-    const cn_collider_broadphase bp = s.colBp[c];
-    if (bp.enabled_flag == 0u) return false;
-    const uint32_t b = bp.owner_body;
-    const f3 bpos = xyz(s.predBodyPos[b]);
-    const float4 bq = qNormalize(s.predBodyRot[b]);
-    const float4 sc = s.bodyScale[b];
-    const cn_collider_geometry cg = s.colGeo[c];
-    const f3 cwp = bpos + qRotate(bq, f3{cg.local_position[0], cg.local_position[1], cg.local_position[2]});
-    const float4 cwq = qNormalize(qMul(bq, qNormalize(make_float4(cg.local_orientation[0], cg.local_orientation[1],
-                                                                  cg.local_orientation[2], cg.local_orientation[3]))));
-    const float4 sp = make_float4(cg.shape_params[0], cg.shape_params[1], cg.shape_params[2], cg.shape_params[3]);
-    if (bp.shape_type == CN_COLLIDER_SPHERE) {
+    const float4 *fr = s.colFrame + size_t(c) * 4;
+    const float4 f0 = __ldg(&fr[0]);
+    const uint32_t word = __float_as_uint(f0.w);
+    if ((word & 1u) == 0u) return false; // disabled collider
+    const uint32_t shape = word >> 8;
+    const f3 cwp = xyz(f0);
+    if (shape == CN_COLLIDER_SPHERE) {
+        const float r = __ldg(&fr[2].x);
         const f3 d = pos - cwp;
         const float dist = length(d);
-        const float r = sphereRadius(sp, sc);
         n = dist > kEps ? (d / dist) : f3{0.f, 1.f, 0.f};
         sd = dist - r;
-    } else if (bp.shape_type == CN_COLLIDER_BOX) {
-        const f3 he = boxHalfExtents(sp, sc);
+    } else if (shape == CN_COLLIDER_BOX) {
+        const float4 cwq = __ldg(&fr[1]);
+        const f3 he = xyz(__ldg(&fr[2]));
         const f3 lp = qInvRotate(cwq, pos - cwp);
         const f3 cl = clamp3(lp, -he, he);
         const f3 d = lp - cl;
@@ -487,9 +602,9 @@ __device__ bool fluidBoundaryContactInfo(const Scene &s, uint32_t c, f3 pos, flo
             sd = -mn(ds.x, mn(ds.y, ds.z));
         }
     } else {
-        f3 a, b2;
-        float cr = 0.0f;
-        capsuleSegment(cwp, cwq, sp, sc, a, b2, cr);
+        const float4 e0 = __ldg(&fr[2]);
+        const f3 a = xyz(e0), b2 = xyz(__ldg(&fr[3]));
+        const float cr = e0.w;
         const f3 seg = b2 - a;
         const float l2 = dot(seg, seg);
         float t = 0.0f;
@@ -575,7 +690,9 @@ __global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Con
     const float kW = spikyK(h);
     const float st = mx(fm.surface_tension, 0.0f);
     const f3 sp = xyz(self);
-    uint32_t *out = s.nbr + size_t(slot) * maxN;
+    // Lists are interleaved (entry k of slot i at k * N + i): a warp's k-th entries share lines.
+    uint32_t *out = kInterleavedLists ? s.nbr + slot : s.nbr + size_t(slot) * maxN;
+    const size_t lstr = kInterleavedLists ? size_t(s.N) : 1u;
     uint32_t count = 0, truncated = 0;
     float rho = 0.0f;
     f3 normal{0.f, 0.f, 0.f};
@@ -588,23 +705,23 @@ __global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Con
     }
     if (useSuperset) {
         const uint32_t n = s.supCount[slot];
-        const uint32_t *sup = s.sup + size_t(slot) * s.supCap;
+        const uint32_t *sup = kInterleavedLists ? s.sup + slot : s.sup + size_t(slot) * s.supCap;
         uint32_t cN = n > 0 ? sup[0] : 0u;
-        uint32_t cNN = n > 1 ? sup[1] : 0u;
+        uint32_t cNN = n > 1 ? sup[lstr] : 0u;
         float4 qN = n > 0 ? ld4(&s.P[cN]) : make_float4(0.f, 0.f, 0.f, 0.f);
         for (uint32_t k = 0; k < n; ++k) {
             const uint32_t c = cN;
             const float4 q = qN;
             if (k + 1 < n) {
                 cN = cNN;
-                if (k + 2 < n) cNN = sup[k + 2];
+                if (k + 2 < n) cNN = sup[(k + 2) * lstr];
                 qN = ld4(&s.P[cN]);
             }
             const f3 delta = sp - xyz(q);
             const float d2 = dot(delta, delta);
             if (d2 >= h2) continue;
             if (count >= maxN) { truncated = 1; continue; }
-            out[count++] = c;
+            out[count++ * lstr] = c;
             if (density) {
                 const float dist = sqrtf(d2);
                 rho += spikyWk(dist, h, kW);
@@ -615,13 +732,13 @@ __global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Con
         const uint4 m = s.sMeta[slot];
         const uint32_t myGroup = infoGroup(info);
         const bool selfCompat = (m.w & m.z) != 0u;
-        const int4 e = s.sCell[slot];
+        const int4 e = s.cCell[slot];
         const bool buildSup = mode == 1u;
         const float supR = h * (1.0f + s.supMargin);
         const float sup2 = supR * supR;
-        uint32_t *sup = buildSup ? s.sup + size_t(slot) * s.supCap : nullptr;
+        uint32_t *sup = buildSup ? (kInterleavedLists ? s.sup + slot : s.sup + size_t(slot) * s.supCap) : nullptr;
         uint32_t supN = 0;
-        const uint32_t run = s.runIdx[slot] + s.runFlag[slot] - 1u;
+        const uint32_t run = s.cRun[slot];
         const uint32_t runStart = s.runStartOf[run];
         const bool ownLookups = (runStart >> 31) != 0u;
         const uint2 *ranges = s.runNbr + size_t(run) * 27u;
@@ -639,12 +756,12 @@ __global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Con
                         check = (rg.x >> 31) != 0u;
                     } else {
                         bool mixed;
-                        if (!findRun(s, cellKey(tx, ty, tz), start, end, mixed)) continue;
+                        if (!findRunCompute(s, cellKey(tx, ty, tz), start, end, mixed)) continue;
                         check = true;
                     }
                     for (uint32_t c = start; c < end; ++c) {
                         if (check) {
-                            const int4 ce = __ldg(&s.sCell[c]);
+                            const int4 ce = __ldg(&s.cCell[c]);
                             if (ce.x != tx || ce.y != ty || ce.z != tz) continue;
                         }
                         const float4 q = ld4(&s.P[c]);
@@ -652,12 +769,12 @@ __global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Con
                         const f3 delta = sp - xyz(q);
                         const float d2 = dot(delta, delta);
                         if (buildSup && d2 < sup2) {
-                            if (supN < s.supCap) sup[supN] = c;
+                            if (supN < s.supCap) sup[supN * lstr] = c;
                             ++supN;
                         }
                         if (d2 >= h2) continue;
                         if (count >= maxN) { truncated = 1; continue; }
-                        out[count++] = c;
+                        out[count++ * lstr] = c;
                         if (density) {
                             const float dist = sqrtf(d2);
                             rho += spikyWk(dist, h, kW);
@@ -725,13 +842,14 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
         const f3 sn = st > kEps ? xyz(snc) : f3{0.f, 0.f, 0.f};
         f3 dp{0.f, 0.f, 0.f};
         const uint32_t cnt = s.nbrCount[slot];
-        const uint32_t *lst = s.nbr + size_t(slot) * s.maxNbr;
+        const uint32_t *lst = kInterleavedLists ? s.nbr + slot : s.nbr + size_t(slot) * s.maxNbr;
+        const size_t lstr = kInterleavedLists ? size_t(s.N) : 1u;
         // Software-pipelined over the list: the next neighbour's slot, position word, constraint
         // and accumulated delta are in flight while the current pair term is computed.
         const bool relLoads = needRel && iter > 0;
         const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
         uint32_t cN = cnt > 0 ? lst[0] : 0u;
-        uint32_t cNN = cnt > 1 ? lst[1] : 0u;
+        uint32_t cNN = cnt > 1 ? lst[lstr] : 0u;
         float4 npN = cnt > 0 ? ld4(&s.P[cN]) : zero4;
         float cwN = cnt > 0 ? __ldg(&s.Cs[cN].w) : 0.0f;
         float4 dN = (cnt > 0 && relLoads) ? ld4(&Dcur[cN]) : zero4;
@@ -742,7 +860,7 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
             const float4 nd4 = dN;
             if (k + 1 < cnt) {
                 cN = cNN;
-                if (k + 2 < cnt) cNN = lst[k + 2];
+                if (k + 2 < cnt) cNN = lst[(k + 2) * lstr];
                 npN = ld4(&s.P[cN]);
                 cwN = __ldg(&s.Cs[cN].w);
                 if (relLoads) dN = ld4(&Dcur[cN]);
@@ -802,7 +920,7 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
     f3 cur = base + acc;
     unsigned long long bm0 = s.sBoundary[slot];
     if (bm0) {
-        const uint32_t p = s.valsA[slot];
+        const uint32_t p = s.cvals[slot];
         const float pr = mx(s.radii[p], 0.0f);
         for (uint32_t sweep = 0; sweep < 2u; ++sweep) {
             bool changed = false;
@@ -1670,13 +1788,20 @@ void launchPredictAndKeys(const Scene &s, float dt, const Config &c, cudaStream_
                                                        s.entries != nullptr);
 }
 
-void launchCellSetup(const Scene &s, uint32_t *scanTmp, cudaStream_t st)
+void launchCellSetup(const Scene &s, uint32_t *scanTmp, void *sortScratch, cudaStream_t st)
 {
     if (s.N == 0) return;
     cudaMemsetAsync(s.tableKeys, 0xff, size_t(s.tableMask + 1) * sizeof(uint32_t), st);
     k_cellSetup<<<blocksFor(s.N), kThreads, 0, st>>>(s);
     if (s.runFlag) {
         exclusiveScan(s.runFlag, s.runIdx, s.N, scanTmp, scanTmp + 1, st);
+        cudaMemsetAsync(s.runKey, 0xff, size_t(s.N) * sizeof(uint32_t), st);
+        k_runKeys<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+        radixSortPairs(s.runKey, s.runVal, s.runKeyB, s.runValB, s.N, sortScratch, &s.meta_->waitTimeouts, st);
+        k_runLengths<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+        exclusiveScan(s.runLenSorted, s.runCompStart, s.N, scanTmp, scanTmp + 1, st);
+        k_runPlace<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+        k_computeOrderSetup<<<blocksFor(s.N), kThreads, 0, st>>>(s);
         k_runNeighbors<<<blocksFor(s.N), kThreads, 0, st>>>(s);
     }
 }
@@ -1705,6 +1830,8 @@ void launchFluidGather(const Scene &s, uint32_t iter, cudaStream_t st)
     const float4 *Dcur = (iter & 1u) ? s.Db : s.Da;
     k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, Dcur, iter);
 }
+
+bool fluidListsInterleaved() { return kInterleavedLists; }
 
 void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter, cudaStream_t st)
 {

@@ -239,6 +239,7 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const Incidence 
     s.predBodyPos = a.take<float4>(B); s.predBodyRot = a.take<float4>(B);
     s.predBodyLin = a.take<float4>(B); s.predBodyAng = a.take<float4>(B);
     s.colAabbMin = a.take<float4>(C); s.colAabbMax = a.take<float4>(C);
+    s.colFrame = a.take<float4>(size_t(C) * 4);
     s.colQueryOrder = a.take<uint32_t>(C);
     if (sv->hasBroadphase) {
         s.entries = a.take<int4>(N);
@@ -264,6 +265,12 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const Incidence 
         s.runIdx = a.take<uint32_t>(N);
         s.runStartOf = a.take<uint32_t>(N);
         s.runNbr = a.take<uint2>(size_t(N) * 27u);
+        s.runKey = a.take<uint32_t>(N); s.runVal = a.take<uint32_t>(N);
+        s.runKeyB = a.take<uint32_t>(N); s.runValB = a.take<uint32_t>(N);
+        s.runHashStart = a.take<uint32_t>(N); s.runLen = a.take<uint32_t>(N);
+        s.runLenSorted = a.take<uint32_t>(N); s.runCompStart = a.take<uint32_t>(N);
+        s.runComp = a.take<uint32_t>(N); s.runPos = a.take<uint32_t>(N);
+        s.cvals = a.take<uint32_t>(N); s.cCell = a.take<int4>(N); s.cRun = a.take<uint32_t>(N);
         s.fluidMaxDelta = a.take<uint32_t>(64);
         if (!sv->ppPossible) { // fluid x is fixed during the iterations: superset lists are exact
             s.supCap = 160u;
@@ -313,7 +320,7 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             probe(sv, "radix_sort", st, [&] {
                 cn::radixSortPairs(s.keysA, s.valsA, s.keysB, s.valsB, N, sv->sortScratch, &s.meta_->waitTimeouts, st);
             });
-            probe(sv, "cell_setup", st, [&] { cn::launchCellSetup(s, sv->scanScratch, st); });
+            probe(sv, "cell_setup", st, [&] { cn::launchCellSetup(s, sv->scanScratch, sv->sortScratch, st); });
         }
         if (sv->ppPossible)
             probe(sv, "particle_candidates", st, [&] { cn::launchParticleCandidates(s, sv->scanScratch, sv->scanScratchBytes, st); });
@@ -340,7 +347,9 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             if (!runFluid && !runSoft && !runPP && !runRigid) break; // remaining iterations are empty
             if (runFluid) {
                 probe(sv, "fluid_gather", st, [&] { cn::launchFluidGather(s, it, st); });
-                probe(sv, "fluid_neighbors_density", st, [&] { cn::launchFluidNeighborsDensity(s, c, it, st); });
+                // the first iteration of a substep also records the superset lists when they are on
+                probe(sv, (it == 0 && s.sup) ? "fluid_neighbors_superset" : "fluid_neighbors_density", st,
+                      [&] { cn::launchFluidNeighborsDensity(s, c, it, st); });
                 probe(sv, "fluid_delta_apply_clamp", st,
                       [&] { cn::launchFluidDeltaApplyClamp(s, it, dt, c, sv->writeFluidDebug, st); });
             }
@@ -776,6 +785,7 @@ CN_API cn_status cn_solver_write_particles(cn_solver *sv, const float *x, const 
     if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_write_particles: null solver");
     if (count > sv->s.N) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_write_particles: count > particles");
     CN_CUDA(cudaSetDevice(sv->device));
+    CN_CUDA(cudaDeviceSynchronize()); // frames stepped on a caller stream may still be running
     if (x) CN_CUDA(cudaMemcpyAsync(sv->s.x, x, sizeof(float4) * count, cudaMemcpyHostToDevice, sv->ownStream));
     if (v) CN_CUDA(cudaMemcpyAsync(sv->s.v, v, sizeof(float4) * count, cudaMemcpyHostToDevice, sv->ownStream));
     CN_CUDA(cudaStreamSynchronize(sv->ownStream));
@@ -862,11 +872,12 @@ CN_API cn_status cn_solver_debug_read(cn_solver *sv, cn_debug_buffer which, void
     };
     std::vector<uint8_t> rankB, valsB;
     const bool needRank = which == CN_DEBUG_FLUID_NEIGHBOR_COUNTS || which == CN_DEBUG_FLUID_NEIGHBORS ||
+                          which == CN_DEBUG_FLUID_SUPERSET_COUNTS ||
                           which == CN_DEBUG_FLUID_CONSTRAINTS || which == CN_DEBUG_FLUID_DELTA;
     if (needRank) {
         if (!s.rank || !s.hasFluid) return setError(CN_ERR_INVALID_ARGUMENT, "debug_read: scene has no fluid");
         CN_CUDA(fetch(s.rank, sizeof(uint32_t) * N, rankB));
-        CN_CUDA(fetch(s.valsA, sizeof(uint32_t) * N, valsB));
+        CN_CUDA(fetch(s.cvals, sizeof(uint32_t) * N, valsB));
     }
     const uint32_t *rank = reinterpret_cast<const uint32_t *>(rankB.data());
     const uint32_t *vals = reinterpret_cast<const uint32_t *>(valsB.data());
@@ -914,6 +925,18 @@ CN_API cn_status cn_solver_debug_read(cn_solver *sv, cn_debug_buffer which, void
         for (uint32_t p = 0; p < N; ++p) o[p] = kk[p] == CN_PARTICLE_FLUID ? cc[rank[p]] : 0u;
         break;
     }
+    case CN_DEBUG_FLUID_SUPERSET_COUNTS: {
+        buf.assign(size_t(N) * 4, 0);
+        if (!s.supCount) break;
+        std::vector<uint8_t> c;
+        CN_CUDA(fetch(s.supCount, sizeof(uint32_t) * N, c));
+        CN_CUDA(fetch(s.kinds, sizeof(uint32_t) * N, kindsB));
+        uint32_t *o = reinterpret_cast<uint32_t *>(buf.data());
+        const uint32_t *cc = reinterpret_cast<const uint32_t *>(c.data());
+        const uint32_t *kk = reinterpret_cast<const uint32_t *>(kindsB.data());
+        for (uint32_t p = 0; p < N; ++p) o[p] = kk[p] == CN_PARTICLE_FLUID ? cc[rank[p]] : 0u;
+        break;
+    }
     case CN_DEBUG_FLUID_NEIGHBORS: {
         std::vector<uint8_t> c, l;
         CN_CUDA(fetch(s.nbrCount, sizeof(uint32_t) * N, c));
@@ -928,7 +951,9 @@ CN_API cn_status cn_solver_debug_read(cn_solver *sv, cn_debug_buffer which, void
             if (kk[p] != CN_PARTICLE_FLUID) continue;
             const uint32_t r = rank[p];
             const uint32_t n = std::min(cc[r], s.maxNbr);
-            for (uint32_t k = 0; k < n; ++k) o[size_t(p) * s.maxNbr + k] = vals[ll[size_t(r) * s.maxNbr + k]];
+            const bool inter = cn::fluidListsInterleaved();
+            for (uint32_t k = 0; k < n; ++k)
+                o[size_t(p) * s.maxNbr + k] = vals[ll[inter ? size_t(k) * N + r : size_t(r) * s.maxNbr + k]];
         }
         break;
     }
