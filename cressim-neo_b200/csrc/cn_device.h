@@ -131,6 +131,7 @@ struct Scene {
     uint32_t *runStartOf = nullptr;   // per run j: compute start | (mixed << 31)
     uint2 *runNbr = nullptr;          // per run j: 27 neighbour runs (compute start | check << 31, end)
     uint32_t *runKey = nullptr, *runVal = nullptr, *runKeyB = nullptr, *runValB = nullptr; // run sort (j -> r)
+    uint32_t *runTotal = nullptr;     // number of runs (device word)
     uint32_t *runHashStart = nullptr; // per run r: key-order start | (mixed << 31)
     uint32_t *runLen = nullptr;       // per run r: particle count
     uint32_t *runLenSorted = nullptr; // per run j: particle count (0 past the last run)
@@ -215,8 +216,10 @@ void launchExportCellRanges(const Scene &s, uint4 *out, uint32_t capacity, uint3
 // decoupled look-back.  keys/vals A hold the input keys (vals ignored: the input index is
 // implied) and receive the sorted result; B is the ping-pong buffer.
 size_t radixSortScratchBytes(uint32_t n);
+// With `count` (device word), only the first min(n, *count) pairs are sorted; the rest of A is
+// left as it was.
 void radixSortPairs(uint32_t *keysA, uint32_t *valsA, uint32_t *keysB, uint32_t *valsB, uint32_t n,
-                    void *scratch, uint32_t *waitTimeouts, cudaStream_t st);
+                    void *scratch, uint32_t *waitTimeouts, cudaStream_t st, const uint32_t *count = nullptr);
 // Exclusive scan of n uint32 values; *total (device) receives the sum.
 size_t scanScratchBytes(uint32_t n);
 void exclusiveScan(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *total, void *scratch,

@@ -28,7 +28,7 @@ constexpr bool kInterleavedLists = true;
 #else
 constexpr bool kInterleavedLists = false;
 #endif
-inline unsigned blocksFor(uint32_t n) { return n == 0 ? 1u : (n + kThreads - 1) / kThreads; }
+inline unsigned blocksFor(size_t n) { return n == 0 ? 1u : unsigned((n + kThreads - 1) / kThreads); }
 // Per-slot fluid word: bit 31 = fluid particle, bits 16..30 = fluid material, bits 0..15 = filter
 // group (a dense id of the particle's (environment, layer, mask) triple).  P.w carries the same
 // word with bit 31 meaning "fluid and invMass > kEps" (the neighbour candidate filter).
@@ -393,30 +393,27 @@ __device__ __forceinline__ bool findRunCompute(const Scene &s, uint32_t key, uin
 // target cell has no run or its (uniform) run holds another cell that hashes to the same key.
 __global__ void __launch_bounds__(kThreads) k_runNeighbors(Scene s)
 {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= s.N || s.runKey[j] == kInvalid) return;
+    // one thread per (run j, neighbour k): the 27 hash probes of a run proceed in parallel
+    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const uint32_t j = uint32_t(t / 27u), k = uint32_t(t % 27u);
+    if (j >= __ldg(s.runTotal)) return;
     const uint32_t r = s.runVal[j];
     const int4 e = s.sCell[s.runHashStart[r] & 0x7fffffffu];
-    uint2 *out = s.runNbr + size_t(j) * 27u;
-    int k = 0;
-    for (int dz = -1; dz <= 1; ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx, ++k) {
-                const int tx = e.x + dx, ty = e.y + dy, tz = e.z + dz;
-                uint32_t hs = 0, he = 0;
-                bool mixed = false;
-                uint2 rg = make_uint2(0u, 0u);
-                if (findRun(s, cellKey(tx, ty, tz), hs, he, mixed)) {
-                    const uint32_t cs = s.runComp[s.runIdx[hs]];
-                    if (mixed) {
-                        rg = make_uint2(cs | 0x80000000u, cs + (he - hs));
-                    } else {
-                        const int4 ce = s.sCell[hs];
-                        if (ce.x == tx && ce.y == ty && ce.z == tz) rg = make_uint2(cs, cs + (he - hs));
-                    }
-                }
-                out[k] = rg;
-            }
+    const int dz = int(k / 9u) - 1, dy = int((k / 3u) % 3u) - 1, dx = int(k % 3u) - 1;
+    const int tx = e.x + dx, ty = e.y + dy, tz = e.z + dz;
+    uint32_t hs = 0, he = 0;
+    bool mixed = false;
+    uint2 rg = make_uint2(0u, 0u);
+    if (findRun(s, cellKey(tx, ty, tz), hs, he, mixed)) {
+        const uint32_t cs = s.runComp[s.runIdx[hs]];
+        if (mixed) {
+            rg = make_uint2(cs | 0x80000000u, cs + (he - hs));
+        } else {
+            const int4 ce = s.sCell[hs];
+            if (ce.x == tx && ce.y == ty && ce.z == tz) rg = make_uint2(cs, cs + (he - hs));
+        }
+    }
+    s.runNbr[size_t(j) * 27u + k] = rg;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1794,15 +1791,16 @@ void launchCellSetup(const Scene &s, uint32_t *scanTmp, void *sortScratch, cudaS
     cudaMemsetAsync(s.tableKeys, 0xff, size_t(s.tableMask + 1) * sizeof(uint32_t), st);
     k_cellSetup<<<blocksFor(s.N), kThreads, 0, st>>>(s);
     if (s.runFlag) {
-        exclusiveScan(s.runFlag, s.runIdx, s.N, scanTmp, scanTmp + 1, st);
+        exclusiveScan(s.runFlag, s.runIdx, s.N, s.runTotal, scanTmp + 1, st);
         cudaMemsetAsync(s.runKey, 0xff, size_t(s.N) * sizeof(uint32_t), st);
         k_runKeys<<<blocksFor(s.N), kThreads, 0, st>>>(s);
-        radixSortPairs(s.runKey, s.runVal, s.runKeyB, s.runValB, s.N, sortScratch, &s.meta_->waitTimeouts, st);
+        radixSortPairs(s.runKey, s.runVal, s.runKeyB, s.runValB, s.N, sortScratch, &s.meta_->waitTimeouts, st,
+                       s.runTotal);
         k_runLengths<<<blocksFor(s.N), kThreads, 0, st>>>(s);
         exclusiveScan(s.runLenSorted, s.runCompStart, s.N, scanTmp, scanTmp + 1, st);
         k_runPlace<<<blocksFor(s.N), kThreads, 0, st>>>(s);
         k_computeOrderSetup<<<blocksFor(s.N), kThreads, 0, st>>>(s);
-        k_runNeighbors<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+        k_runNeighbors<<<blocksFor(size_t(s.N) * 27u), kThreads, 0, st>>>(s);
     }
 }
 

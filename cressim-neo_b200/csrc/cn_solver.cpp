@@ -268,6 +268,7 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const Incidence 
         s.runKey = a.take<uint32_t>(N); s.runVal = a.take<uint32_t>(N);
         s.runKeyB = a.take<uint32_t>(N); s.runValB = a.take<uint32_t>(N);
         s.runHashStart = a.take<uint32_t>(N); s.runLen = a.take<uint32_t>(N);
+        s.runTotal = a.take<uint32_t>(1);
         s.runLenSorted = a.take<uint32_t>(N); s.runCompStart = a.take<uint32_t>(N);
         s.runComp = a.take<uint32_t>(N); s.runPos = a.take<uint32_t>(N);
         s.cvals = a.take<uint32_t>(N); s.cCell = a.take<int4>(N); s.cRun = a.take<uint32_t>(N);

@@ -51,9 +51,16 @@ SortScratch carve(void *scratch, uint32_t n)
 }
 
 // One pass over the keys builds all four digit histograms.
-__global__ void __launch_bounds__(256) k_radixHistogram(const uint32_t *__restrict__ keys, uint32_t n,
+__device__ __forceinline__ uint32_t liveCount(uint32_t n, const uint32_t *count)
+{
+    return count ? min(n, *count) : n;
+}
+
+__global__ void __launch_bounds__(256) k_radixHistogram(const uint32_t *__restrict__ keys, uint32_t capacity,
+                                                        const uint32_t *__restrict__ count,
                                                         uint32_t *__restrict__ hist)
 {
+    const uint32_t n = liveCount(capacity, count);
     __shared__ uint32_t sh[4][kRadix];
     for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) (&sh[0][0])[i] = 0u;
     __syncthreads();
@@ -107,8 +114,8 @@ template <bool kFirstPass>
 __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint32_t *__restrict__ keysIn,
                                                            const uint32_t *__restrict__ valsIn,
                                                            uint32_t *__restrict__ keysOut,
-                                                           uint32_t *__restrict__ valsOut, uint32_t n,
-                                                           uint32_t shift,
+                                                           uint32_t *__restrict__ valsOut, uint32_t capacity,
+                                                           const uint32_t *__restrict__ count, uint32_t shift,
                                                            const uint32_t *__restrict__ digitOffsets,
                                                            uint32_t *lookback, uint32_t *tileCounter,
                                                            uint32_t *waitTimeouts)
@@ -126,6 +133,10 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint32_t *__res
     for (int i = threadIdx.x; i < kSortWarps * kRadix; i += kSortThreads) (&warpHist[0][0])[i] = 0u;
     __syncthreads();
     const uint32_t tile = tileId;
+    const uint32_t n = liveCount(capacity, count);
+    // Tiles past a device-side count have nothing to sort.  Tickets are handed out in order, so
+    // every tile a live tile looks back on is live too.
+    if (tile >= numTiles(n)) return;
     const uint32_t warpBase = tile * kTile + warp * kWarpTile;
 
     uint32_t key[kItems], val[kItems], rnk[kItems];
@@ -324,29 +335,29 @@ size_t radixSortScratchBytes(uint32_t n)
 }
 
 void radixSortPairs(uint32_t *keysA, uint32_t *valsA, uint32_t *keysB, uint32_t *valsB, uint32_t n,
-                    void *scratch, uint32_t *waitTimeouts, cudaStream_t st)
+                    void *scratch, uint32_t *waitTimeouts, cudaStream_t st, const uint32_t *count)
 {
     if (n == 0) return;
     const SortScratch s = carve(scratch, n);
     const uint32_t tiles = numTiles(n);
     cudaMemsetAsync(scratch, 0, radixSortScratchBytes(n), st);
     const uint32_t histBlocks = min(tiles * 4u, 148u * 4u);
-    k_radixHistogram<<<histBlocks, 256, 0, st>>>(keysA, n, s.hist);
+    k_radixHistogram<<<histBlocks, 256, 0, st>>>(keysA, n, count, s.hist);
     k_radixHistogramScan<<<1, 256, 0, st>>>(s.hist);
     uint32_t *kin = keysA, *vin = valsA, *kout = keysB, *vout = valsB;
     for (int pass = 0; pass < 4; ++pass) {
         uint32_t *look = s.lookback + size_t(pass) * tiles * kRadix;
         if (pass == 0)
-            k_onesweep<true><<<tiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, 0u, s.hist, look,
+            k_onesweep<true><<<tiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, count, 0u, s.hist, look,
                                                              s.counters + 0, waitTimeouts);
         else
-            k_onesweep<false><<<tiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, 8u * pass,
+            k_onesweep<false><<<tiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, count, 8u * pass,
                                                               s.hist + pass * kRadix, look,
                                                               s.counters + pass, waitTimeouts);
         uint32_t *tk = kin, *tv = vin;
         kin = kout; vin = vout; kout = tk; vout = tv;
     }
-    // After four passes the result is back in (keysA, valsA).
+    // After four passes the result is back in (keysA, valsA); with a count, only [0, count).
 }
 
 size_t scanScratchBytes(uint32_t n)
