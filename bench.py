@@ -53,6 +53,22 @@ def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
 
 
+def max_over_ranks(value: float, world: int, device="cuda") -> float:
+    """The largest `value` over all ranks (the slowest rank's time); identity for one rank."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(particles: int, substeps: int, steps: int, world: int, seconds: float) -> float:
+    """Particle-substeps/s of the whole job: every rank steps its own replica of the scene."""
+    return float(particles) * substeps * steps * world / seconds
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons during the timed region."""
 
@@ -193,14 +209,9 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
     clk = clocks.stop()
-    ms = start.elapsed_time(end)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(start.elapsed_time(end), world)
     substeps = desc.substeps
-    total_units = float(n) * substeps * args.steps * world
-    value = total_units / (ms / 1e3)
+    value = whole_job_rate(n, substeps, args.steps, world, ms / 1e3)
     meta = solver.validate_gpu_meta()
     kernels_per_frame, _ = solver.graph_stats()
     counts, sup_counts = solver_neighbor_mean(solver)
@@ -239,12 +250,8 @@ def run_ours(args):
         solver.step_many(dt, 1, sh)
         assert lib.cn_solver_read_particles(solver._h, xp, vp, None, n) == 0
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = float(n) * substeps * e2e_steps * world / e2e_s
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = whole_job_rate(n, substeps, e2e_steps, world, e2e_s)
 
     def pct(q):
         return round(step_ms[min(len(step_ms) - 1, int(q * len(step_ms)))], 4)
@@ -324,7 +331,7 @@ def cpu_baseline(budget_s: float = 15.0, dims=(64, 32, 64), max_frames: int = 8)
                       f"{frames} frames x {desc.substeps} substeps, {el:.1f} s"}
 
 
-def run_reference(args):
+def run_reference(args, dims=(48, 24, 48)):
     rank, local, world = dist_env()
     if rank != 0:
         return
@@ -333,7 +340,6 @@ def run_reference(args):
     from cn_physics import scenes
 
     threads = cn_oracle.set_threads(os.cpu_count() or 1)
-    dims = (48, 24, 48)
     w, desc, dt = scenes.dam_break(nx=dims[0], ny=dims[1], nz=dims[2])
     soa = w.soa()
     ora = cn_oracle.Oracle(desc, soa)

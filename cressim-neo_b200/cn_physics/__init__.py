@@ -117,10 +117,56 @@ class World:
                            static_particles: Sequence[int] = (), environment=0, layer=1, mask=0xFFFFFFFF,
                            friction=0.0, restitution=0.0, damping=0.0, static_friction=-1.0) -> int:
         """SoftBodyState with a RegularGrid source (soft_body_authoring.cpp:81-176)."""
-        d = _abi.SoftBodyGridDesc()
-        self._lib.cn_soft_body_grid_desc_defaults(C.byref(d))
+        d = self._soft_desc(position, rotation, mass, radius, edge_compliance, volume_compliance, self_collision,
+                            static_particles, environment, layer, mask, friction, restitution, damping,
+                            static_friction)
         d.size = (C.c_float * 3)(*size)
         d.target_particle_spacing = spacing
+        out = C.c_uint32()
+        _check(self._lib.cn_world_add_soft_body_grid(self._h, C.byref(d), C.byref(out)))
+        return out.value
+
+    def add_soft_body_tet_mesh(self, positions, tets, position=(0, 0, 0), rotation=(0, 0, 0, 1), **kw) -> int:
+        """SoftBodyState with a TetMesh source: object-space (V, 3) positions, (T, 4) indices."""
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float32).reshape(-1, 3))
+        idx = np.ascontiguousarray(np.asarray(tets, dtype=np.uint32).reshape(-1, 4))
+        d = self._soft_desc(position, rotation, **self._soft_kw(kw))
+        out = C.c_uint32()
+        _check(self._lib.cn_world_add_soft_body_tet_mesh(self._h, C.byref(d), _f32(pos), pos.shape[0], _u32(idx),
+                                                         idx.shape[0], C.byref(out)))
+        return out.value
+
+    def add_soft_body_tetgen(self, node_file, ele_file, position=(0, 0, 0), rotation=(0, 0, 0, 1), **kw) -> int:
+        """SoftBodyState with a TetGenFiles source (.node / .ele pair)."""
+        d = self._soft_desc(position, rotation, **self._soft_kw(kw))
+        out = C.c_uint32()
+        _check(self._lib.cn_world_add_soft_body_tetgen(self._h, C.byref(d), str(node_file).encode(),
+                                                       str(ele_file).encode(), C.byref(out)))
+        return out.value
+
+    def add_soft_body_meshfree(self, positions, neighbours, position=(0, 0, 0), rotation=(0, 0, 0, 1), **kw) -> int:
+        """SoftBodyState with a MeshfreeParticles source (k-nearest distance graph)."""
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float32).reshape(-1, 3))
+        d = self._soft_desc(position, rotation, **self._soft_kw(kw))
+        out = C.c_uint32()
+        _check(self._lib.cn_world_add_soft_body_meshfree(self._h, C.byref(d), _f32(pos), pos.shape[0], neighbours,
+                                                         C.byref(out)))
+        return out.value
+
+    @staticmethod
+    def _soft_kw(kw):
+        names = ("mass", "radius", "edge_compliance", "volume_compliance", "self_collision", "static_particles",
+                 "environment", "layer", "mask", "friction", "restitution", "damping", "static_friction")
+        defaults = (1.0, 0.125, 0.0, 0.0, False, (), 0, 1, 0xFFFFFFFF, 0.0, 0.0, 0.0, -1.0)
+        unknown = set(kw) - set(names)
+        if unknown:
+            raise TypeError(f"unknown soft body arguments: {sorted(unknown)}")
+        return {n: kw.get(n, dv) for n, dv in zip(names, defaults)}
+
+    def _soft_desc(self, position, rotation, mass, radius, edge_compliance, volume_compliance, self_collision,
+                   static_particles, environment, layer, mask, friction, restitution, damping, static_friction):
+        d = _abi.SoftBodyGridDesc()
+        self._lib.cn_soft_body_grid_desc_defaults(C.byref(d))
         self._transform(d.rest_transform, position, rotation)
         d.particle_mass, d.particle_radius = mass, radius
         d.edge_compliance, d.volume_compliance = edge_compliance, volume_compliance
@@ -131,9 +177,7 @@ class World:
         self._keep.append(st)
         d.static_particle_indices = _u32(st) if st.size else None
         d.static_particle_count = st.size
-        out = C.c_uint32()
-        _check(self._lib.cn_world_add_soft_body_grid(self._h, C.byref(d), C.byref(out)))
-        return out.value
+        return d
 
     def add_fluid_grid(self, size, spacing, position=(0, 0, 0), *, mass=1.0, radius=0.05, viscosity=0.01,
                        cohesion=0.0, surface_tension=0.0, vorticity=0.0, gravity_scale=1.0, cfl=1.0,

@@ -174,6 +174,12 @@ SIGNATURES = [
     ("cn_world_create", C.c_int, [C.POINTER(C.c_void_p)]),
     ("cn_world_destroy", None, [C.c_void_p]),
     ("cn_world_add_soft_body_grid", C.c_int, [C.c_void_p, C.POINTER(SoftBodyGridDesc), P_u32]),
+    ("cn_world_add_soft_body_tet_mesh", C.c_int, [C.c_void_p, C.POINTER(SoftBodyGridDesc), P_f32, C.c_uint32,
+                                                  P_u32, C.c_uint32, P_u32]),
+    ("cn_world_add_soft_body_tetgen", C.c_int, [C.c_void_p, C.POINTER(SoftBodyGridDesc), C.c_char_p, C.c_char_p,
+                                                P_u32]),
+    ("cn_world_add_soft_body_meshfree", C.c_int, [C.c_void_p, C.POINTER(SoftBodyGridDesc), P_f32, C.c_uint32,
+                                                  C.c_uint32, P_u32]),
     ("cn_world_add_fluid_grid", C.c_int, [C.c_void_p, C.POINTER(FluidGridDesc), P_u32]),
     ("cn_world_add_cloth_grid", C.c_int, [C.c_void_p, C.POINTER(ClothGridDesc), P_u32]),
     ("cn_world_add_strand", C.c_int, [C.c_void_p, C.POINTER(StrandDesc), P_u32]),

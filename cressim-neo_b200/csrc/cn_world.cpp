@@ -8,7 +8,9 @@
 #include <cmath>
 #include <cstring>
 #include <map>
+#include <fstream>
 #include <set>
+#include <sstream>
 #include <string>
 #include <unordered_map>
 #include <unordered_set>
@@ -124,8 +126,13 @@ uint32_t packPhase(uint32_t group, bool selfCollide)
     return (group & CN_PHASE_GROUP_MASK) | (selfCollide ? CN_PHASE_SELF_COLLIDE : 0u);
 }
 
+enum class SoftSource { RegularGrid, TetMesh, Meshfree };
 struct SoftBody {
     cn_soft_body_grid_desc desc;
+    SoftSource source = SoftSource::RegularGrid;
+    std::vector<v3> srcPositions;     // object space (TetMesh / TetGen / meshfree sources)
+    std::vector<uint32_t> srcTets;    // 4 indices per tetrahedron (TetMesh / TetGen sources)
+    uint32_t neighbourCount = 0;      // meshfree k-nearest graph
     std::vector<uint32_t> staticIdx;
     std::vector<v3> rest;
     std::vector<std::array<uint32_t, 4>> tets;
@@ -183,11 +190,10 @@ struct cn_world {
 
 namespace {
 
-// soft_body_authoring.cpp:81-176 (buildRegularGridSource) + :296-434 (tets, edges, adjacency)
-cn_status buildSoftBody(SoftBody &sb)
+// soft_body_authoring.cpp:81-176 (buildRegularGridSource): object-space lattice and 5-tet split.
+void regularGridSource(const cn_soft_body_grid_desc &d, std::vector<v3> &pos, std::vector<uint32_t> &idx)
 {
-    const cn_soft_body_grid_desc &d = sb.desc;
-    const float kMinExtent = 1.0e-4f, kMinSpacing = 1.0e-4f, kMinRestVolume = 1.0e-8f;
+    const float kMinExtent = 1.0e-4f, kMinSpacing = 1.0e-4f;
     const v3 size{std::max(d.size[0], kMinExtent), std::max(d.size[1], kMinExtent), std::max(d.size[2], kMinExtent)};
     const float spacing = std::max(d.target_particle_spacing, kMinSpacing);
     auto res = [spacing](float extent) {
@@ -195,19 +201,18 @@ cn_status buildSoftBody(SoftBody &sb)
     };
     const uint32_t rx = res(size.x), ry = res(size.y), rz = res(size.z);
     auto flat = [&](uint32_t x, uint32_t y, uint32_t z) { return x * ry * rz + y * rz + z; };
-    sb.rest.clear();
+    pos.clear();
+    idx.clear();
     for (uint32_t x = 0; x < rx; ++x) {
         const float tx = rx > 1u ? float(x) / float(rx - 1u) : 0.0f;
         for (uint32_t y = 0; y < ry; ++y) {
             const float ty = ry > 1u ? float(y) / float(ry - 1u) : 0.0f;
             for (uint32_t z = 0; z < rz; ++z) {
                 const float tz = rz > 1u ? float(z) / float(rz - 1u) : 0.0f;
-                sb.rest.push_back(applyTransform(d.rest_transform, v3{(tx - 0.5f) * size.x, (ty - 0.5f) * size.y,
-                                                                      (tz - 0.5f) * size.z}));
+                pos.push_back(v3{(tx - 0.5f) * size.x, (ty - 0.5f) * size.y, (tz - 0.5f) * size.z});
             }
         }
     }
-    std::vector<uint32_t> idx;
     for (uint32_t x = 0; x + 1u < rx; ++x)
         for (uint32_t y = 0; y + 1u < ry; ++y)
             for (uint32_t z = 0; z + 1u < rz; ++z) {
@@ -219,32 +224,178 @@ cn_status buildSoftBody(SoftBody &sb)
                 const auto &split = (((x + y + z) & 1u) != 0u) ? odd : even;
                 for (int t = 0; t < 5; ++t) idx.insert(idx.end(), split[t], split[t] + 4);
             }
+}
+
+// soft_body_authoring.cpp:179-226 (buildMeshfreeKNearestGraph): each particle links to its k
+// nearest others (ties by index); edges are unique (min, max) pairs in discovery order.
+void meshfreeGraph(SoftBody &sb, uint32_t k)
+{
+    const uint32_t n = uint32_t(sb.rest.size());
+    if (n < 2u) return;
+    k = std::min(k, n - 1u);
+    std::set<uint64_t> unique;
+    std::vector<std::pair<float, uint32_t>> nearest;
+    nearest.reserve(n - 1u);
+    for (uint32_t i = 0; i < n; ++i) {
+        nearest.clear();
+        for (uint32_t c = 0; c < n; ++c) {
+            if (c == i) continue;
+            const v3 d = sb.rest[c] - sb.rest[i];
+            nearest.emplace_back(dot(d, d), c);
+        }
+        std::sort(nearest.begin(), nearest.end(), [](const auto &a, const auto &b) {
+            return a.first != b.first ? a.first < b.first : a.second < b.second;
+        });
+        for (uint32_t slot = 0; slot < k; ++slot) {
+            const uint32_t j = nearest[slot].second;
+            sb.adjacency[i].push_back(j);
+            sb.adjacency[j].push_back(i);
+            const uint32_t lo = std::min(i, j), hi = std::max(i, j);
+            if (unique.insert((uint64_t(lo) << 32) | hi).second) sb.edges.push_back({lo, hi});
+        }
+    }
+}
+
+// soft_body_authoring.cpp:235-434 (resolveSoftBodyTopology): rest positions through the rest
+// transform, then per tetrahedron the range / repeated-vertex / degenerate-volume checks, the
+// tetrahedron itself, its 6 edges (unique, in discovery order) and adjacency; static indices are
+// sorted, deduplicated and range-checked.  Returns an error text, empty on success.
+std::string buildSoftBody(SoftBody &sb)
+{
+    const cn_soft_body_grid_desc &d = sb.desc;
+    const float kMinRestVolume = 1.0e-8f;
+    std::vector<v3> src;
+    std::vector<uint32_t> idx;
+    if (sb.source == SoftSource::RegularGrid) {
+        regularGridSource(d, src, idx);
+    } else {
+        src = sb.srcPositions;
+        idx = sb.srcTets;
+    }
+    if (src.empty()) return "Soft body source does not contain any rest positions.";
+    const bool meshfree = sb.source == SoftSource::Meshfree;
+    if (!meshfree && idx.empty()) return "Soft body source does not contain any tetrahedra.";
+    if (!meshfree && (idx.size() % 4u) != 0u) return "Soft body tetrahedron index buffer size must be divisible by 4.";
+    sb.rest.clear();
+    for (const v3 &p : src) sb.rest.push_back(applyTransform(d.rest_transform, p));
     const uint32_t n = uint32_t(sb.rest.size());
     sb.adjacency.assign(n, {});
     sb.tets.clear();
     sb.edges.clear();
-    std::set<uint64_t> unique;
-    for (size_t b = 0; b < idx.size(); b += 4) {
-        const std::array<uint32_t, 4> t{idx[b], idx[b + 1], idx[b + 2], idx[b + 3]};
-        const v3 a0 = sb.rest[t[0]], a1 = sb.rest[t[1]], a2 = sb.rest[t[2]], a3 = sb.rest[t[3]];
-        const float vol = std::fabs(dot(cross(a1 - a0, a2 - a0), a3 - a0) / 6.0f);
-        if (vol <= kMinRestVolume) return CN_ERR_INVALID_ARGUMENT; // degenerate tetrahedron
-        sb.tets.push_back(t);
-        const uint32_t pairs[6][2] = {{t[0], t[1]}, {t[0], t[2]}, {t[0], t[3]}, {t[1], t[2]}, {t[1], t[3]}, {t[2], t[3]}};
-        for (const auto &e : pairs) {
-            sb.adjacency[e[0]].push_back(e[1]);
-            sb.adjacency[e[1]].push_back(e[0]);
-            const uint32_t lo = std::min(e[0], e[1]), hi = std::max(e[0], e[1]);
-            if (unique.insert((uint64_t(lo) << 32) | hi).second) sb.edges.push_back({lo, hi});
+    if (meshfree) {
+        meshfreeGraph(sb, sb.neighbourCount);
+    } else {
+        std::set<uint64_t> unique;
+        for (size_t b = 0; b < idx.size(); b += 4) {
+            const std::array<uint32_t, 4> t{idx[b], idx[b + 1], idx[b + 2], idx[b + 3]};
+            for (uint32_t v : t)
+                if (v >= n)
+                    return "Tet vertex index " + std::to_string(v) + " is out of range for " + std::to_string(n) +
+                           " particles.";
+            if (t[0] == t[1] || t[0] == t[2] || t[0] == t[3] || t[1] == t[2] || t[1] == t[3] || t[2] == t[3])
+                return "Soft body tetrahedra must not repeat a vertex index.";
+            const v3 a0 = sb.rest[t[0]], a1 = sb.rest[t[1]], a2 = sb.rest[t[2]], a3 = sb.rest[t[3]];
+            const float vol = std::fabs(dot(cross(a1 - a0, a2 - a0), a3 - a0) / 6.0f);
+            if (vol <= kMinRestVolume) return "Soft body source contains a degenerate tetrahedron.";
+            sb.tets.push_back(t);
+            const uint32_t pairs[6][2] = {{t[0], t[1]}, {t[0], t[2]}, {t[0], t[3]}, {t[1], t[2]}, {t[1], t[3]}, {t[2], t[3]}};
+            for (const auto &e : pairs) {
+                sb.adjacency[e[0]].push_back(e[1]);
+                sb.adjacency[e[1]].push_back(e[0]);
+                const uint32_t lo = std::min(e[0], e[1]), hi = std::max(e[0], e[1]);
+                if (unique.insert((uint64_t(lo) << 32) | hi).second) sb.edges.push_back({lo, hi});
+            }
         }
     }
     for (auto &a : sb.adjacency) {
         std::sort(a.begin(), a.end());
         a.erase(std::unique(a.begin(), a.end()), a.end());
     }
-    for (uint32_t s : sb.staticIdx)
-        if (s >= n) return CN_ERR_INVALID_ARGUMENT;
-    return CN_OK;
+    for (uint32_t st : sb.staticIdx)
+        if (st >= n)
+            return "Static particle index " + std::to_string(st) + " is out of range for " + std::to_string(n) +
+                   " particles.";
+    return std::string();
+}
+
+// tetgen_loader.cpp:68-215 (loadTetGenFiles).  '#' starts a comment, blank lines are skipped.
+// .node: "count 3 attributes markers" then "id x y z" rows (ids unique); .ele: "count 4 attributes"
+// then "id i0 i1 i2 i3" rows whose indices must be ids of the .node table -- dense 0- or
+// 1-based renumberings that do not match the ids are rejected rather than guessed.
+bool nextMeaningfulLine(std::istream &in, std::string &line)
+{
+    while (std::getline(in, line)) {
+        const size_t hash = line.find('#');
+        if (hash != std::string::npos) line.erase(hash);
+        const size_t b = line.find_first_not_of(" \t\r\n");
+        if (b == std::string::npos) continue;
+        const size_t e = line.find_last_not_of(" \t\r\n");
+        line = line.substr(b, e - b + 1);
+        return true;
+    }
+    return false;
+}
+
+std::string loadTetGen(const char *nodeFile, const char *eleFile, std::vector<v3> &pos, std::vector<uint32_t> &idx)
+{
+    pos.clear();
+    idx.clear();
+    const std::string nf = nodeFile ? nodeFile : "", ef = eleFile ? eleFile : "";
+    std::ifstream ns(nf);
+    if (!ns.is_open()) return "Unable to open TetGen node file '" + nf + "'.";
+    std::ifstream es(ef);
+    if (!es.is_open()) return "Unable to open TetGen ele file '" + ef + "'.";
+    std::string line;
+    if (!nextMeaningfulLine(ns, line)) return "TetGen node file '" + nf + "' is empty.";
+    uint32_t nodeCount = 0;
+    int dim = 0, attrs = 0, markers = 0;
+    {
+        std::istringstream h(line);
+        if (!(h >> nodeCount >> dim >> attrs >> markers)) return "TetGen node file '" + nf + "' has an invalid header.";
+    }
+    if (dim != 3) return "TetGen node file '" + nf + "' must describe 3D vertices.";
+    std::unordered_map<int64_t, uint32_t> idToDense;
+    pos.resize(nodeCount);
+    for (uint32_t i = 0; i < nodeCount; ++i) {
+        if (!nextMeaningfulLine(ns, line))
+            return "TetGen node file '" + nf + "' ended before all declared vertices were read.";
+        std::istringstream r(line);
+        int64_t id = 0;
+        v3 p{};
+        if (!(r >> id >> p.x >> p.y >> p.z)) return "TetGen node file '" + nf + "' contains an invalid vertex row.";
+        if (!idToDense.emplace(id, i).second) return "TetGen node file '" + nf + "' contains duplicate node ids.";
+        pos[i] = p;
+    }
+    if (!nextMeaningfulLine(es, line)) return "TetGen ele file '" + ef + "' is empty.";
+    uint32_t tetCount = 0;
+    int perTet = 0, eattrs = 0;
+    {
+        std::istringstream h(line);
+        if (!(h >> tetCount >> perTet >> eattrs)) return "TetGen ele file '" + ef + "' has an invalid header.";
+    }
+    if (perTet != 4) return "TetGen ele file '" + ef + "' must contain tetrahedra with exactly 4 vertices.";
+    std::vector<int64_t> raw;
+    raw.reserve(size_t(tetCount) * 4u);
+    for (uint32_t i = 0; i < tetCount; ++i) {
+        if (!nextMeaningfulLine(es, line))
+            return "TetGen ele file '" + ef + "' ended before all declared tetrahedra were read.";
+        std::istringstream r(line);
+        int64_t id = 0, a = 0, b = 0, c = 0, dd = 0;
+        if (!(r >> id >> a >> b >> c >> dd)) return "TetGen ele file '" + ef + "' contains an invalid tetrahedron row.";
+        raw.insert(raw.end(), {a, b, c, dd});
+    }
+    idx.reserve(raw.size());
+    for (int64_t v : raw) {
+        const auto it = idToDense.find(v);
+        if (it == idToDense.end()) {
+            pos.clear();
+            idx.clear();
+            return "TetGen ele file '" + ef + "' references node ids missing from '" + nf +
+                   "' (dense re-indexed element files are rejected).";
+        }
+        idx.push_back(it->second);
+    }
+    return std::string();
 }
 
 // physics_world.cpp:6857-6891
@@ -733,21 +884,70 @@ CN_API cn_status cn_world_create(cn_world **out)
 
 CN_API void cn_world_destroy(cn_world *w) { delete w; }
 
-CN_API cn_status cn_world_add_soft_body_grid(cn_world *w, const cn_soft_body_grid_desc *d, uint32_t *out)
+namespace {
+cn_status addSoftBody(cn_world *w, SoftBody &&sb, const cn_soft_body_grid_desc *d, uint32_t *out, const char *what)
 {
-    if (!w || !d) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_soft_body_grid: null argument");
-    SoftBody sb;
-    sb.desc = *d;
     if (d->static_particle_indices && d->static_particle_count)
         sb.staticIdx.assign(d->static_particle_indices, d->static_particle_indices + d->static_particle_count);
     std::sort(sb.staticIdx.begin(), sb.staticIdx.end());
     sb.staticIdx.erase(std::unique(sb.staticIdx.begin(), sb.staticIdx.end()), sb.staticIdx.end());
     sb.desc.static_particle_indices = nullptr;
-    if (buildSoftBody(sb) != CN_OK)
-        return cn::setError(CN_ERR_INVALID_ARGUMENT, "soft body: degenerate tetrahedron or static index out of range");
+    const std::string err = buildSoftBody(sb);
+    if (!err.empty()) return cn::setError(CN_ERR_INVALID_ARGUMENT, std::string(what) + ": " + err);
     if (out) *out = uint32_t(w->softBodies.size());
     w->softBodies.push_back(std::move(sb));
     return CN_OK;
+}
+} // namespace
+
+CN_API cn_status cn_world_add_soft_body_grid(cn_world *w, const cn_soft_body_grid_desc *d, uint32_t *out)
+{
+    if (!w || !d) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_soft_body_grid: null argument");
+    SoftBody sb;
+    sb.desc = *d;
+    sb.source = SoftSource::RegularGrid;
+    return addSoftBody(w, std::move(sb), d, out, "cn_world_add_soft_body_grid");
+}
+
+CN_API cn_status cn_world_add_soft_body_tet_mesh(cn_world *w, const cn_soft_body_grid_desc *d, const float *positions,
+                                                 uint32_t vertex_count, const uint32_t *tet_indices,
+                                                 uint32_t tet_count, uint32_t *out)
+{
+    if (!w || !d || (vertex_count && !positions) || (tet_count && !tet_indices))
+        return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_soft_body_tet_mesh: null argument");
+    SoftBody sb;
+    sb.desc = *d;
+    sb.source = SoftSource::TetMesh;
+    for (uint32_t i = 0; i < vertex_count; ++i)
+        sb.srcPositions.push_back(v3{positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]});
+    sb.srcTets.assign(tet_indices, tet_indices + size_t(tet_count) * 4u);
+    return addSoftBody(w, std::move(sb), d, out, "cn_world_add_soft_body_tet_mesh");
+}
+
+CN_API cn_status cn_world_add_soft_body_tetgen(cn_world *w, const cn_soft_body_grid_desc *d, const char *node_file,
+                                               const char *ele_file, uint32_t *out)
+{
+    if (!w || !d) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_soft_body_tetgen: null argument");
+    SoftBody sb;
+    sb.desc = *d;
+    sb.source = SoftSource::TetMesh;
+    const std::string err = loadTetGen(node_file, ele_file, sb.srcPositions, sb.srcTets);
+    if (!err.empty()) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_soft_body_tetgen: " + err);
+    return addSoftBody(w, std::move(sb), d, out, "cn_world_add_soft_body_tetgen");
+}
+
+CN_API cn_status cn_world_add_soft_body_meshfree(cn_world *w, const cn_soft_body_grid_desc *d, const float *positions,
+                                                 uint32_t particle_count, uint32_t neighbour_count, uint32_t *out)
+{
+    if (!w || !d || (particle_count && !positions))
+        return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_soft_body_meshfree: null argument");
+    SoftBody sb;
+    sb.desc = *d;
+    sb.source = SoftSource::Meshfree;
+    sb.neighbourCount = neighbour_count;
+    for (uint32_t i = 0; i < particle_count; ++i)
+        sb.srcPositions.push_back(v3{positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]});
+    return addSoftBody(w, std::move(sb), d, out, "cn_world_add_soft_body_meshfree");
 }
 
 CN_API cn_status cn_world_add_fluid_grid(cn_world *w, const cn_fluid_grid_desc *d, uint32_t *out)

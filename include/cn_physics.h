@@ -343,6 +343,20 @@ CN_API cn_status cn_world_create(cn_world **out_world);
 CN_API void cn_world_destroy(cn_world *world);
 /* reference: PhysicsWorld::upsertSoftBody + buildRegularGridSource (soft_body_authoring.cpp:81-176) */
 CN_API cn_status cn_world_add_soft_body_grid(cn_world *w, const cn_soft_body_grid_desc *d, uint32_t *out_index);
+/* SoftBodyState with a TetMesh source (soft_body_authoring.cpp:254-258): object-space positions
+ * (xyz per vertex) and 4 indices per tetrahedron.  The grid fields size / target_particle_spacing
+ * of `d` are ignored; transform, mass, radius, compliances, collision and static indices apply. */
+CN_API cn_status cn_world_add_soft_body_tet_mesh(cn_world *w, const cn_soft_body_grid_desc *d, const float *positions,
+                                                 uint32_t vertex_count, const uint32_t *tet_indices,
+                                                 uint32_t tet_count, uint32_t *out_index);
+/* SoftBodyState with a TetGenFiles source: the .node / .ele pair read as loadTetGenFiles does
+ * (tetgen_loader.cpp:68-215); element rows must name node ids of the .node file. */
+CN_API cn_status cn_world_add_soft_body_tetgen(cn_world *w, const cn_soft_body_grid_desc *d, const char *node_file,
+                                               const char *ele_file, uint32_t *out_index);
+/* SoftBodyState with a MeshfreeParticles source: distance edges to each particle's
+ * neighbour_count nearest particles (buildMeshfreeKNearestGraph, soft_body_authoring.cpp:179-226). */
+CN_API cn_status cn_world_add_soft_body_meshfree(cn_world *w, const cn_soft_body_grid_desc *d, const float *positions,
+                                                 uint32_t particle_count, uint32_t neighbour_count, uint32_t *out_index);
 /* reference: prepareFluidStateForInsert (physics_world.cpp:6857-6891), toFluidSolverMaterial (:191-262) */
 CN_API cn_status cn_world_add_fluid_grid(cn_world *w, const cn_fluid_grid_desc *d, uint32_t *out_index);
 CN_API cn_status cn_world_add_cloth_grid(cn_world *w, const cn_cloth_grid_desc *d, uint32_t *out_index);

@@ -1,7 +1,10 @@
 """Host authoring against the reference's known answers (no GPU)."""
-import numpy as np
+from pathlib import Path
 
-from cn_physics import World
+import numpy as np
+import pytest
+
+from cn_physics import CNError, World
 import cn_oracle
 
 
@@ -66,3 +69,97 @@ def test_grid_cell_size_is_max_of_diameter_and_support():
     w.add_soft_body_grid((1, 1, 1), 0.25, radius=0.2)
     w.add_fluid_grid((0.4, 0.4, 0.4), 0.05, radius=0.03)
     assert abs(w.soa().particle_grid_cell_size - 0.4) < 1e-7
+
+
+# A 5-vertex, 2-tetrahedron mesh with TetGen-style node ids 10..50 (the shape of the reference's
+# tests/physics/fixtures/soft_body_simple.node / soft_body_simple_ids.ele), written by this test.
+_MESH_POS = [(-0.5, 0.0, 0.0), (0.5, 0.0, 0.0), (0.0, 0.75, 0.0), (0.0, 0.0, 0.75), (0.0, 0.0, -0.75)]
+_MESH_TETS = [(0, 1, 2, 3), (0, 1, 4, 2)]
+_SOFT_KW = dict(mass=2.0, radius=0.1, edge_compliance=0.01, volume_compliance=0.02, static_particles=[1])
+
+
+def _write_tetgen(tmp_path, ids=(10, 20, 30, 40, 50), ele_ids=None):
+    node = tmp_path / "mesh.node"
+    ele = tmp_path / "mesh.ele"
+    rows = [f"{ids[i]} {p[0]} {p[1]} {p[2]}" for i, p in enumerate(_MESH_POS)]
+    node.write_text("# nodes\n5 3 0 0\n" + "\n".join(rows) + "\n")
+    ele_ids = ele_ids or ids
+    trows = [f"{k + 1} " + " ".join(str(ele_ids[v]) for v in t) for k, t in enumerate(_MESH_TETS)]
+    ele.write_text("2 4 0\n" + "\n".join(trows) + "  # trailing comment\n")
+    return node, ele
+
+
+def _soft_state(w):
+    s = w.soa()
+    return (w.positions().copy(), w.array("edges")[:, :2].copy(), w.array("edges").view(np.float32)[:, 2].copy(),
+            w.array("tets")[:, :4].copy(), w.array("tets").view(np.float32)[:, 4].copy())
+
+
+def _assert_same_soft(a, b):
+    for x, y in zip(a, b):
+        assert x.shape == y.shape
+        assert np.allclose(x, y, atol=1e-6) if x.dtype.kind == "f" else np.array_equal(x, y)
+
+
+def test_tet_mesh_source_topology():
+    # soft_body_authoring.cpp:235-434: edges unique in discovery order, rest volume |det| / 6
+    w = World()
+    w.add_soft_body_tet_mesh(_MESH_POS, _MESH_TETS, **_SOFT_KW)
+    x, edges, rest, tets, vol = _soft_state(w)
+    assert x.shape == (5, 4) and np.allclose(x[:, 3], [0.5, 0.0, 0.5, 0.5, 0.5])  # index 1 static
+    assert tets.tolist() == [list(t) for t in _MESH_TETS]
+    assert edges.tolist() == [[0, 1], [0, 2], [0, 3], [1, 2], [1, 3], [2, 3], [0, 4], [1, 4], [2, 4]]
+    p = np.asarray(_MESH_POS, np.float32)
+    assert np.allclose(rest, np.linalg.norm(p[edges[:, 1]] - p[edges[:, 0]], axis=1), atol=1e-6)
+    assert np.allclose(vol, [0.09375, 0.09375], atol=1e-7)  # |((1,0,0) x (.5,.75,0)) . (.5,0,.75)| / 6
+
+
+def test_tetgen_round_trip_matches_tet_mesh(tmp_path):
+    # tests/physics/physics_soft_body_authoring_tetgen_roundtrip.cpp: node-id-mapped files give the
+    # same world as the equivalent TetMesh source; a dense 1-based element file is rejected
+    ref = World()
+    ref.add_soft_body_tet_mesh(_MESH_POS, _MESH_TETS, **_SOFT_KW)
+    node, ele = _write_tetgen(tmp_path)
+    w = World()
+    w.add_soft_body_tetgen(node, ele, **_SOFT_KW)
+    _assert_same_soft(_soft_state(ref), _soft_state(w))
+    node, dense = _write_tetgen(tmp_path, ele_ids=(1, 2, 3, 4, 5))
+    bad = World()
+    with pytest.raises(CNError):
+        bad.add_soft_body_tetgen(node, dense, **_SOFT_KW)
+
+
+def test_tetgen_reference_fixtures(tmp_path):
+    # The reference's own fixture files, read as text where the reference tree is present.
+    fx = Path("/root/reference/tests/physics/fixtures")
+    if not (fx / "soft_body_simple.node").exists():
+        pytest.skip("reference fixtures not present")
+    ref = World()
+    ref.add_soft_body_tet_mesh(_MESH_POS, _MESH_TETS, **_SOFT_KW)
+    w = World()
+    w.add_soft_body_tetgen(fx / "soft_body_simple.node", fx / "soft_body_simple_ids.ele", **_SOFT_KW)
+    _assert_same_soft(_soft_state(ref), _soft_state(w))
+    with pytest.raises(CNError):
+        World().add_soft_body_tetgen(fx / "soft_body_simple.node", fx / "soft_body_simple_dense1.ele", **_SOFT_KW)
+
+
+def test_soft_body_source_errors():
+    # soft_body_authoring.cpp:336-360: out-of-range index, repeated vertex, degenerate volume
+    for tets in ([(0, 1, 2, 7)], [(0, 1, 1, 2)], [(0, 1, 2, 2)]):
+        with pytest.raises(CNError):
+            World().add_soft_body_tet_mesh(_MESH_POS, tets)
+    flat = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 0)]
+    with pytest.raises(CNError):
+        World().add_soft_body_tet_mesh(flat, [(0, 1, 2, 3)])
+    with pytest.raises(CNError):
+        World().add_soft_body_tet_mesh(_MESH_POS, _MESH_TETS, static_particles=[9])
+
+
+def test_meshfree_knn_graph():
+    # soft_body_authoring.cpp:179-226: k nearest (ties by index), unique (min, max) edges
+    pts = np.array([(0, 0, 0), (1, 0, 0), (3, 0, 0), (0, 2, 0)], np.float32)
+    w = World()
+    w.add_soft_body_meshfree(pts, 1)
+    _, edges, rest, _, _ = _soft_state(w)
+    assert edges.tolist() == [[0, 1], [1, 2], [0, 3]]
+    assert np.allclose(rest, [1.0, 2.0, 2.0])
