@@ -134,12 +134,13 @@ def peaks():
 # Algorithmic bytes per particle of one launch of each fluid kernel (compulsory traffic; neighbour
 # entries count 4 B).  Neighbour build + density: position P (16) + cell entry (16) + metadata (16)
 # + kind/material (4) + boundary mask (8), list writes 4*nbar, count (4), constraint write (16).
-# The first iteration of a substep also writes the superset list (4*nsup + 4 for its count).
+# The first iteration of a substep also writes the superset list (4*nsup + 4 for its count);
+# the later iterations read it back instead of walking the cells (4*nsup + 4).
 # Delta + apply + clamp: P (16) + x (16) + accumulated delta r/w (32) + constraint (16) + list reads
 # 4*nbar + count (4) + kind/material (4) + boundary mask (8) + packed delta write (16 when kept).
 def kernel_bytes(name: str, nbar: float, nsup: float = 0.0) -> float | None:
     if name == "fluid_neighbors_density":
-        return 80.0 + 4.0 * nbar
+        return 80.0 + 4.0 * nbar + (4.0 * nsup + 4.0 if nsup > 0 else 0.0)
     if name == "fluid_neighbors_superset":
         return 84.0 + 4.0 * nbar + 4.0 * nsup
     if name == "fluid_delta_apply_clamp":
