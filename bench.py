@@ -46,6 +46,11 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dims", type=str, default="128,64,128", help="fluid lattice (profiling runs use smaller ones)")
+    ap.add_argument("--serve-scenes", type=int, default=512, help="tissue scenes of the served/batched pool (0: skip)")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="Poisson arrival window of the served run")
+    ap.add_argument("--serve-rate", type=float, default=20000.0, help="offered frames per second")
+    ap.add_argument("--serve-substeps", type=int, default=1)
+    ap.add_argument("--serve-iterations", type=int, default=20)
     return ap.parse_args()
 
 
@@ -295,6 +300,8 @@ def run_ours(args):
         "clocks": clk,
         "meta_status": meta["status"],
     }
+    if args.serve_scenes > 0:
+        line["served"] = run_served(args, stream, sh)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(budget_s=15.0)
     if world > 1:
@@ -303,6 +310,101 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def run_served(args, stream, sh) -> dict:
+    """The batched and served forms on a pool of soft-tissue scenes (2K-60K tets, log-uniform),
+    against the plain per-scene drop-in (one cn_solver per scene) on the same pool.
+
+    plain: one frame of every scene, scene after scene, each through its own solver;
+    batched: one tick stepping every scene together (saturated);
+    served: Poisson arrivals of 1-8-frame requests with drifting tool poses, replayed in real
+    time through the server (admission by a device-memory budget, continuous batching)."""
+    import torch
+    from cn_physics import Batch, Server, Solver, batch_desc, serving
+
+    pool = serving.tissue_pool(args.serve_scenes, seed=0)
+    P = sum(sc.particles for sc in pool)
+    T = sum(sc.tets for sc in pool)
+    E = sum(sc.world.counts()["edges"] for sc in pool)
+    desc = serving.serving_solver_desc(args.serve_substeps, args.serve_iterations)
+    sub = desc.substeps
+    dt = 1.0 / 60.0
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    # plain per-scene drop-in
+    solvers = []
+    for sc in pool:
+        sv = Solver(desc)
+        sv.sync_world(sc.world.soa())
+        solvers.append(sv)
+    serving.plain_round(pool, solvers, dt, sh)  # graph capture + warm-up
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    serving.plain_round(pool, solvers, dt, sh)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    plain_ms = ev[0].elapsed_time(ev[1])
+    for sv in solvers:
+        sv.close()
+    del solvers
+
+    # batched: every scene resident, autotuned schedule, saturated ticks
+    budget = 120 << 30
+    bd = batch_desc(desc, memory_budget_bytes=budget, max_scenes=len(pool) + 8, particle_capacity=P + 4096,
+                    edge_capacity=E + 4096, tet_capacity=T + 4096)
+    b = Batch(bd)
+    ids = [b.add_scene(sc.world.soa()) for sc in pool]
+    tune = b.autotune(ids, dt)
+    b.step(ids, dt, sh)
+    torch.cuda.synchronize()
+    ticks = []
+    for _ in range(5):
+        ev[0].record(stream)
+        b.step(ids, dt, sh)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        ticks.append(ev[0].elapsed_time(ev[1]))
+    tick_ms = float(np.median(ticks))
+    b.close()
+
+    # served: a fresh batch (same schedule) behind the server, Poisson load in real time
+    bd.tile_elements, bd.blocks_per_sm = tune["tile_elements"], tune["blocks_per_sm"]
+    b = Batch(bd)
+    srv = Server(b, dt)
+    sids = [srv.register(sc.world.soa()) for sc in pool]
+    prefetched = sum(1 for k in sids if srv.admit(k))  # warm start: resident before the clock starts
+    reqs = serving.poisson_requests(pool, steps_per_second=args.serve_rate, duration_s=args.serve_seconds, seed=1)
+    out = serving.serve(srv, pool, sids, reqs, sh)
+    st = out["stats"]
+    bstats = b.stats()
+    srv.close()
+    b.close()
+    plain_rate = P * sub / (plain_ms / 1e3)
+    batched_rate = P * sub / (tick_ms / 1e3)
+    served_rate = st["particle_substeps"] / out["elapsed_s"]
+    return {
+        "workload": f"tissue_pool_{len(pool)}: XPBD tissue blocks, tets log-uniform 2K-60K, per-tet compliance "
+                    f"log-normal (sigma 0.5), kinematic capsule tool, dt 1/60, {sub} substep x "
+                    f"{desc.default_iterations} iterations",
+        "scenes": len(pool), "particles": P, "tets": T, "edges": E, "unit": "particle-substeps/s",
+        "plain": {"value": round(plain_rate, 1), "round_ms": round(plain_ms, 3),
+                  "method": "one cn_solver per scene, one frame of every scene in turn (CUDA-graph replays)"},
+        "batched": {"value": round(batched_rate, 1), "tick_ms_p50": round(tick_ms, 3),
+                    "tick_ms_max": round(max(ticks), 3), "schedule": {"tile_elements": tune["tile_elements"],
+                                                                      "blocks_per_sm": tune["blocks_per_sm"]},
+                    "autotune_candidates": tune["candidates"]},
+        "batched_over_plain": round(batched_rate / plain_rate, 2),
+        "served": {"offered_frames_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds,
+                   "requests": out["requests"], "frames": st["scene_steps"], "value": round(served_rate, 1),
+                   "frames_per_s": round(st["scene_steps"] / out["elapsed_s"], 1),
+                   "elapsed_s": round(out["elapsed_s"], 3),
+                   "request_latency_ms": {"p50": round(out["latency_ms_p50"], 3), "p99": round(out["latency_ms_p99"], 3)},
+                   "step_latency_ms": {"p50": round(st["tick_ms_p50"], 3), "p99": round(st["tick_ms_p99"], 3)},
+                   "ticks": st["ticks"], "prefetched_scenes": prefetched,
+                   "admissions_during_run": st["admissions"] - prefetched, "evictions": st["evictions"],
+                   "budget_bytes": bstats["budget_bytes"], "budget_used_bytes": bstats["budget_used_bytes"]},
+    }
 
 
 def solver_neighbor_mean(solver) -> tuple:

@@ -419,3 +419,167 @@ class Solver:
         _check(self._lib.cn_solver_debug_read(self._h, which, buf.ctypes.data_as(C.c_void_p), size.value,
                                               C.byref(size)))
         return buf
+
+
+def batch_desc(solver: Optional[_abi.SolverDesc] = None, **fields) -> _abi.BatchDesc:
+    """cn_batch_desc with defaults, the shared solver settings and field overrides."""
+    d = _abi.BatchDesc()
+    load().cn_batch_desc_defaults(C.byref(d))
+    if solver is not None:
+        d.solver = solver
+    for key, value in fields.items():
+        setattr(d, key, value)
+    return d
+
+
+def _stream(stream) -> Optional[C.c_void_p]:
+    return C.c_void_p(stream) if stream else None
+
+
+class Batch:
+    """Independent soft-tissue scenes resident in one device pool, stepped together (cn_batch_*)."""
+
+    def __init__(self, desc: Optional[_abi.BatchDesc] = None, device: int = 0):
+        self._lib = load()
+        self.desc = desc if desc is not None else batch_desc()
+        h = C.c_void_p()
+        _check(self._lib.cn_batch_create(C.byref(self.desc), device, C.byref(h)))
+        self._h = h
+        self._sizes = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cn_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_scene(self, world: "World | _abi.WorldSoA") -> int:
+        soa = world.soa() if isinstance(world, World) else world
+        out = C.c_uint32()
+        _check(self._lib.cn_batch_add_scene(self._h, C.byref(soa), C.byref(out)))
+        self._sizes[out.value] = soa.particle_count
+        return out.value
+
+    def remove_scene(self, scene: int) -> None:
+        _check(self._lib.cn_batch_remove_scene(self._h, scene))
+        self._sizes.pop(scene, None)
+
+    def set_kinematic_target(self, scene: int, body: int, position, orientation=(0, 0, 0, 1)) -> None:
+        p = (C.c_float * 3)(*position)
+        q = (C.c_float * 4)(*orientation)
+        _check(self._lib.cn_batch_set_kinematic_target(self._h, scene, body, p, q))
+
+    def step(self, scenes: Sequence[int], dt: float, stream: int = 0) -> None:
+        ids = np.ascontiguousarray(np.asarray(scenes, dtype=np.uint32))
+        _check(self._lib.cn_batch_step(self._h, _u32(ids), ids.size, dt, _stream(stream)))
+
+    def read_particles(self, scene: int):
+        n = self._sizes[scene]
+        x = np.zeros((n, 4), np.float32)
+        v = np.zeros((n, 4), np.float32)
+        _check(self._lib.cn_batch_read_particles(self._h, scene, _f32(x), _f32(v), n))
+        return x, v
+
+    def stats(self) -> dict:
+        s = _abi.BatchStats()
+        _check(self._lib.cn_batch_get_stats(self._h, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in _abi.BatchStats._fields_ if not name.startswith("reserved")}
+
+    def set_schedule(self, tile_elements: int, blocks_per_sm: int) -> None:
+        _check(self._lib.cn_batch_set_schedule(self._h, tile_elements, blocks_per_sm))
+
+    def autotune(self, scenes: Sequence[int], dt: float) -> dict:
+        ids = np.ascontiguousarray(np.asarray(scenes, dtype=np.uint32))
+        t = _abi.BatchTuning()
+        _check(self._lib.cn_batch_autotune(self._h, _u32(ids), ids.size, dt, C.byref(t)))
+        return {"tile_elements": t.tile_elements, "blocks_per_sm": t.blocks_per_sm, "tick_ms": t.tick_ms,
+                "candidates": [(t.candidates[k].tile_elements, t.candidates[k].blocks_per_sm,
+                                round(t.candidates[k].tick_ms, 4)) for k in range(t.candidate_count)]}
+
+
+class Server:
+    """Serving loop over a Batch (cn_server_*): registration, admission by the memory budget,
+    continuous batching of pending requests, per-request latency."""
+
+    def __init__(self, batch: Batch, frame_dt: float, max_scenes_per_tick: int = 0):
+        self._lib = load()
+        self.batch = batch
+        d = _abi.ServerDesc()
+        self._lib.cn_server_desc_defaults(C.byref(d))
+        d.frame_dt = frame_dt
+        d.max_scenes_per_tick = max_scenes_per_tick
+        h = C.c_void_p()
+        _check(self._lib.cn_server_create(batch._h, C.byref(d), batch.desc.solver.substeps, C.byref(h)))
+        self._h = h
+        self._sizes = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.cn_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def register(self, world: "World | _abi.WorldSoA") -> int:
+        soa = world.soa() if isinstance(world, World) else world
+        out = C.c_uint32()
+        _check(self._lib.cn_server_register_scene(self._h, C.byref(soa), C.byref(out)))
+        self._sizes.append(soa.particle_count)
+        return out.value
+
+    def admit(self, scene: int) -> bool:
+        """Makes a scene resident ahead of its requests; False when the budget has no room."""
+        st = self._lib.cn_server_admit(self._h, scene)
+        if st == 5:  # CN_ERR_CAPACITY
+            return False
+        _check(st)
+        return True
+
+    def submit(self, scene: int, steps: int, tool_body: int = 0, targets=None) -> int:
+        rid = C.c_uint64()
+        tp = None
+        if targets is not None:
+            arr = np.ascontiguousarray(np.asarray(targets, dtype=np.float32).reshape(steps, 7))
+            tp = _f32(arr)
+        _check(self._lib.cn_server_submit(self._h, scene, steps, tool_body, tp, C.byref(rid)))
+        return rid.value
+
+    def tick(self, stream: int = 0) -> int:
+        n = C.c_uint32()
+        _check(self._lib.cn_server_tick(self._h, _stream(stream), C.byref(n)))
+        return n.value
+
+    def drain(self, stream: int = 0) -> None:
+        _check(self._lib.cn_server_drain(self._h, _stream(stream)))
+
+    def poll(self) -> list:
+        out = (_abi.RequestDone * 4096)()
+        got, n = [], C.c_uint32()
+        while True:
+            _check(self._lib.cn_server_poll(self._h, out, 4096, C.byref(n)))
+            got += [{"request": out[k].request_id, "scene": out[k].scene, "steps": out[k].steps,
+                     "submit_s": out[k].submit_s, "first_tick_s": out[k].first_tick_s, "done_s": out[k].done_s}
+                    for k in range(n.value)]
+            if n.value < 4096:
+                return got
+
+    def stats(self) -> dict:
+        s = _abi.ServerStats()
+        _check(self._lib.cn_server_get_stats(self._h, C.byref(s)))
+        return {name: getattr(s, name) for name, _ in _abi.ServerStats._fields_}
+
+    def read_particles(self, scene: int):
+        n = self._sizes[scene]
+        x = np.zeros((n, 4), np.float32)
+        v = np.zeros((n, 4), np.float32)
+        _check(self._lib.cn_server_read_particles(self._h, scene, _f32(x), _f32(v), n))
+        return x, v

@@ -161,6 +161,47 @@ class KernelTime(C.Structure):
 
 
 # Exported entry points and their signatures: (name, restype, argtypes).
+u64 = C.c_uint64
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [("solver", SolverDesc), ("memory_budget_bytes", u64), ("max_scenes", u32),
+                ("particle_capacity", u32), ("edge_capacity", u32), ("tet_capacity", u32),
+                ("body_capacity", u32), ("collider_capacity", u32), ("tile_elements", u32),
+                ("blocks_per_sm", u32), ("rigid_pairs_per_particle", u32), ("reserved", u32 * 3)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("resident_scenes", u32), ("particles_used", u32), ("particle_capacity", u32),
+                ("edges_used", u32), ("edge_capacity", u32), ("tets_used", u32), ("tet_capacity", u32),
+                ("tile_elements", u32), ("grid_blocks", u32), ("reserved0", u32), ("budget_bytes", u64),
+                ("budget_used_bytes", u64), ("pool_bytes", u64), ("ticks", u64)]
+
+
+class BatchCandidate(C.Structure):
+    _fields_ = [("tile_elements", u32), ("blocks_per_sm", u32), ("tick_ms", f32), ("reserved", u32)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("tile_elements", u32), ("blocks_per_sm", u32), ("tick_ms", f32), ("candidate_count", u32),
+                ("candidates", BatchCandidate * 16)]
+
+
+class ServerDesc(C.Structure):
+    _fields_ = [("frame_dt", f32), ("max_scenes_per_tick", u32), ("reserved", u32 * 6)]
+
+
+class RequestDone(C.Structure):
+    _fields_ = [("request_id", u64), ("scene", u32), ("steps", u32), ("submit_s", C.c_double),
+                ("first_tick_s", C.c_double), ("done_s", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("ticks", u64), ("scene_steps", u64), ("particle_substeps", u64), ("admissions", u64),
+                ("evictions", u64), ("completed", u64), ("pending", u64), ("resident_scenes", u32),
+                ("registered_scenes", u32), ("gpu_ms", C.c_double), ("tick_ms_p50", f32), ("tick_ms_p99", f32)]
+
+
 SIGNATURES = [
     ("cn_last_error", C.c_char_p, []),
     ("cn_version", C.c_char_p, []),
@@ -204,6 +245,29 @@ SIGNATURES = [
     ("cn_solver_graph_stats", C.c_int, [C.c_void_p, P_u32, P_u32]),
     ("cn_sort_cell_keys_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, u32, C.c_void_p]),
     ("cn_solver_debug_read", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+    ("cn_batch_desc_defaults", None, [C.POINTER(BatchDesc)]),
+    ("cn_batch_create", C.c_int, [C.POINTER(BatchDesc), C.c_int, C.POINTER(C.c_void_p)]),
+    ("cn_batch_destroy", None, [C.c_void_p]),
+    ("cn_batch_add_scene", C.c_int, [C.c_void_p, C.POINTER(WorldSoA), P_u32]),
+    ("cn_batch_remove_scene", C.c_int, [C.c_void_p, u32]),
+    ("cn_batch_set_kinematic_target", C.c_int, [C.c_void_p, u32, u32, P_f32, P_f32]),
+    ("cn_batch_step", C.c_int, [C.c_void_p, P_u32, u32, f32, C.c_void_p]),
+    ("cn_batch_read_particles", C.c_int, [C.c_void_p, u32, P_f32, P_f32, u32]),
+    ("cn_batch_export_scene", C.c_int, [C.c_void_p, u32, C.POINTER(WorldSoA)]),
+    ("cn_batch_get_stats", C.c_int, [C.c_void_p, C.POINTER(BatchStats)]),
+    ("cn_batch_set_schedule", C.c_int, [C.c_void_p, u32, u32]),
+    ("cn_batch_autotune", C.c_int, [C.c_void_p, P_u32, u32, f32, C.POINTER(BatchTuning)]),
+    ("cn_server_desc_defaults", None, [C.POINTER(ServerDesc)]),
+    ("cn_server_create", C.c_int, [C.c_void_p, C.POINTER(ServerDesc), u32, C.POINTER(C.c_void_p)]),
+    ("cn_server_destroy", None, [C.c_void_p]),
+    ("cn_server_register_scene", C.c_int, [C.c_void_p, C.POINTER(WorldSoA), P_u32]),
+    ("cn_server_admit", C.c_int, [C.c_void_p, u32]),
+    ("cn_server_submit", C.c_int, [C.c_void_p, u32, u32, u32, P_f32, C.POINTER(u64)]),
+    ("cn_server_tick", C.c_int, [C.c_void_p, C.c_void_p, P_u32]),
+    ("cn_server_drain", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("cn_server_poll", C.c_int, [C.c_void_p, C.POINTER(RequestDone), u32, P_u32]),
+    ("cn_server_get_stats", C.c_int, [C.c_void_p, C.POINTER(ServerStats)]),
+    ("cn_server_read_particles", C.c_int, [C.c_void_p, u32, P_f32, P_f32, u32]),
 ]
 
 _lib = None

@@ -50,7 +50,19 @@ constexpr uint32_t kRigidDedup = 16u;            // kParticleRigidDedupCacheSize
 constexpr uint32_t kColliderIterationCap = 64u;  // kParticleRigidColliderIterationCap
 constexpr float kBroadPhaseMargin = 0.05f;       // physics_shape_common.hlsli:10
 
+// A batch's per-tick work: `tiles` are element ranges [x, y) of the scenes stepped this tick,
+// `count` the number of tiles (device word); kernels launched with a work list run `grid` blocks
+// that stride over the tiles.  A null list means "all elements [0, n)" (a single world).
+struct WorkList {
+    const uint2 *tiles = nullptr;
+    const uint32_t *count = nullptr;
+    uint32_t grid = 0;
+};
+
 struct Scene {
+    // per-tick work lists of a batch (all null for a single world)
+    WorkList wP, wE, wT, wB, wC;      // particles, edges, tets, rigid bodies, colliders
+    const uint2 *pColRange = nullptr; // per particle: its scene's range of colQueryOrder
     uint32_t N = 0;
     // ---- particles (reference order) ----
     float4 *x = nullptr, *xprev = nullptr, *v = nullptr;
@@ -184,7 +196,16 @@ struct Config {
     float gravity[3];
 };
 
+// A kinematic target staged for a batch tick: pos.xyz, pos.w = the body index (bits); rot = xyzw.
+struct BodyTarget {
+    float4 pos;
+    float4 rot;
+};
+
 // ------------------------------------------------------------------ launchers (cn_kernels.cu)
+// Writes `*count` staged kinematic targets (what cn_solver_set_kinematic_target writes for one).
+void launchApplyBodyTargets(const Scene &s, const BodyTarget *list, const uint32_t *count, uint32_t capacity,
+                            cudaStream_t st);
 void launchRigidPredict(const Scene &s, float dt, float gx, float gy, float gz, cudaStream_t st);
 void launchPredictAndKeys(const Scene &s, float dt, const Config &c, cudaStream_t st);
 void launchCellSetup(const Scene &s, uint32_t *scanTmp, void *sortScratch, cudaStream_t st);

@@ -1,14 +1,115 @@
-// cn_internal.h -- error reporting shared by the C ABI translation units.
+// cn_internal.h -- helpers shared by the host translation units behind the C ABI: error
+// reporting, the device arena, incidence tables and the solver constants.
 #pragma once
 
+#include <cstdint>
 #include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
 
 #include "../../include/cn_physics.h"
+#include "cn_device.h"
 
 namespace cn {
 
 // Records `message` as this thread's last error and returns `status`.
 cn_status setError(cn_status status, const std::string &message);
 void clearError();
+
+
+inline uint32_t nextPow2(uint32_t v)
+{
+    if (v <= 1u) return 1u;
+    --v;
+    v |= v >> 1; v |= v >> 2; v |= v >> 4; v |= v >> 8; v |= v >> 16;
+    return v + 1u;
+}
+inline uint32_t resolveIter(uint32_t o, uint32_t d) { return o > 0u ? o : d; }
+
+// Bump allocator over one device allocation.  Running a layout with a null base sizes it.
+class Arena {
+public:
+    void reset(uint8_t *base) { base_ = base; offset_ = 0; }
+    template <class T> T *take(size_t count)
+    {
+        const size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+        T *p = base_ ? reinterpret_cast<T *>(base_ + offset_) : nullptr;
+        offset_ += count ? bytes : 0;
+        return count ? p : nullptr;
+    }
+    size_t size() const { return offset_; }
+
+private:
+    uint8_t *base_ = nullptr;
+    size_t offset_ = 0;
+};
+
+// Per-particle incidence lists in ascending constraint order
+// (physics_scene_gpu_state.cpp:3273-3420): ranges[p] = (start, count), inc = (constraint, slot).
+struct Incidence {
+    std::vector<uint2> ranges, inc;
+};
+template <class F> Incidence buildIncidence(uint32_t n, uint32_t constraints, uint32_t perConstraint, F &&particlesOf)
+{
+    std::vector<uint32_t> counts(n, 0);
+    for (uint32_t c = 0; c < constraints; ++c)
+        for (uint32_t k = 0; k < perConstraint; ++k) {
+            const uint32_t p = particlesOf(c, k);
+            if (p < n) ++counts[p];
+        }
+    Incidence out;
+    out.ranges.resize(n);
+    uint32_t run = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        out.ranges[i] = make_uint2(run, counts[i]);
+        run += counts[i];
+    }
+    out.inc.resize(run);
+    std::vector<uint32_t> fill(n, 0);
+    for (uint32_t c = 0; c < constraints; ++c)
+        for (uint32_t k = 0; k < perConstraint; ++k) {
+            const uint32_t p = particlesOf(c, k);
+            if (p < n) out.inc[out.ranges[p].x + fill[p]++] = make_uint2(c, k);
+        }
+    return out;
+}
+
+// Solver constants of one substep, from the PhysicsSolverDesc mirror.
+inline Config configFromDesc(const cn_solver_desc &d)
+{
+    Config c{};
+    c.slop = d.contact.slop;
+    c.softContactRelaxation = d.contact.soft_relaxation;
+    c.softMaxCorrection = d.contact.soft_max_correction_per_iteration;
+    c.restitutionVelocityThreshold = d.contact.restitution_velocity_threshold;
+    c.restitutionPenetrationThreshold = d.contact.restitution_penetration_slop_multiplier * d.contact.slop;
+    c.positionFrictionMinDistance = d.contact.position_friction_min_distance;
+    c.softInternalRelaxation = d.soft.internal_relaxation;
+    c.fluidSolveCoefficient = d.fluid.constraint_relaxation;
+    c.fluidRelaxation = d.fluid.position_relaxation;
+    c.fluidBoundaryDensityScale = d.fluid.boundary_density_scale;
+    c.fluidBoundaryDeltaScale = d.fluid.boundary_delta_scale;
+    c.fluidMaxUnderDensityRatio = d.fluid.max_under_density_ratio;
+    c.gravity[0] = d.gravity[0]; c.gravity[1] = d.gravity[1]; c.gravity[2] = d.gravity[2];
+    return c;
+}
+
+// Moving (kinematic) colliders, then static ones, each ascending by index; disabled colliders
+// and colliders of missing bodies are left out.  Returns the number of moving colliders.
+inline uint32_t colliderQueryOrder(const cn_world_soa &w, std::vector<uint32_t> &order)
+{
+    order.clear();
+    std::vector<uint32_t> stat;
+    for (uint32_t c = 0; c < w.collider_count; ++c) {
+        const cn_collider_broadphase &bp = w.collider_broadphase[c];
+        if (bp.owner_body >= w.rigid_body_count || bp.enabled_flag == 0u) continue;
+        if (w.body_types[bp.owner_body] == CN_BODY_STATIC) stat.push_back(c);
+        else order.push_back(c);
+    }
+    const uint32_t moving = uint32_t(order.size());
+    order.insert(order.end(), stat.begin(), stat.end());
+    return moving;
+}
 
 } // namespace cn

@@ -39,6 +39,38 @@ __host__ __device__ __forceinline__ uint32_t infoGroup(uint32_t info) { return i
 
 __device__ __forceinline__ float4 ld4(const float4 *p) { return __ldg(p); }
 
+// One element per thread over [0, n) (a single world), or -- with a work list -- a fixed grid
+// striding over the list's tiles: each tile is an element range [x, y) of one resident scene of
+// a batch, so a launch covers exactly the scenes stepped this tick.
+template <class F> __device__ __forceinline__ void forEachElem(const WorkList &w, uint32_t n, F &&f)
+{
+    if (w.tiles == nullptr) {
+        const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i < n) f(i);
+        return;
+    }
+    const uint32_t count = *w.count;
+    for (uint32_t t = blockIdx.x; t < count; t += gridDim.x) {
+        const uint2 r = w.tiles[t];
+        for (uint32_t i = r.x + threadIdx.x; i < r.y; i += blockDim.x) f(i);
+    }
+}
+inline unsigned gridFor(const WorkList &w, size_t n) { return w.tiles ? w.grid : blocksFor(n); }
+// The same for loops that one block runs over a small family (rigid bodies, colliders).
+template <class F> __device__ __forceinline__ void forEachInBlock(const WorkList &w, uint32_t n, F &&f)
+{
+    if (w.tiles == nullptr) {
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) f(i);
+        return;
+    }
+    // body / collider tiles are one scene's few elements: one thread per tile
+    const uint32_t count = *w.count;
+    for (uint32_t t = threadIdx.x; t < count; t += blockDim.x) {
+        const uint2 r = w.tiles[t];
+        for (uint32_t i = r.x; i < r.y; ++i) f(i);
+    }
+}
+
 // ------------------------------------------------------------------------------------------
 // Rigid predict (static / kinematic; dynamic bodies are integrated without particle feedback)
 // physics_rigid_predict.cs.hlsl:20-81, collider world AABBs physics_rigid_update_world_aabbs.cs.hlsl
@@ -66,7 +98,7 @@ __device__ void computeBodyAabb(uint32_t shape, f3 pos, float4 q, float4 p, floa
 
 __global__ void __launch_bounds__(kThreads) k_rigidPredict(Scene s, float dt, float gx, float gy, float gz)
 {
-    for (uint32_t b = threadIdx.x; b < s.B; b += blockDim.x) {
+    forEachInBlock(s.wB, s.B, [&](uint32_t b) {
         const float4 p = s.bodyPos[b];
         const float4 q = qNormalize(s.bodyRot[b]);
         const float4 lin = s.bodyLin[b], ang = s.bodyAng[b];
@@ -96,15 +128,15 @@ __global__ void __launch_bounds__(kThreads) k_rigidPredict(Scene s, float dt, fl
             s.predBodyLin[b] = mk4(l, lin.w);
             s.predBodyAng[b] = ang;
         }
-    }
+    });
     __syncthreads();
-    for (uint32_t c = threadIdx.x; c < s.C; c += blockDim.x) {
+    forEachInBlock(s.wC, s.C, [&](uint32_t c) {
         const cn_collider_broadphase bp = s.colBp[c];
         const uint32_t ob = bp.owner_body;
         if (ob >= s.B || bp.enabled_flag == 0u) {
             s.colAabbMin[c] = make_float4(0.f, 0.f, 0.f, 0.f);
             s.colAabbMax[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-            continue;
+            return;
         }
         const float4 sc = s.bodyScale[ob];
         const cn_collider_geometry cg = s.colGeo[c];
@@ -126,16 +158,16 @@ __global__ void __launch_bounds__(kThreads) k_rigidPredict(Scene s, float dt, fl
         const f3 hi = max3(a1, b1) + f3{kBroadPhaseMargin, kBroadPhaseMargin, kBroadPhaseMargin};
         s.colAabbMin[c] = mk4(lo, 0.f);
         s.colAabbMax[c] = mk4(hi, 0.f);
-    }
+    });
     // Collider frames for the fluid boundary queries, with the arithmetic of
     // physics_fluid_boundary_common.hlsli:11-40 (unscaled local offset), done once per collider.
-    for (uint32_t c = threadIdx.x; c < s.C; c += blockDim.x) {
+    forEachInBlock(s.wC, s.C, [&](uint32_t c) {
         const cn_collider_broadphase bp = s.colBp[c];
         float4 *fr = s.colFrame + size_t(c) * 4;
         const uint32_t b = bp.owner_body;
         if (bp.enabled_flag == 0u || b >= s.B) {
             fr[0] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0u));
-            continue;
+            return;
         }
         const f3 bpos = xyz(s.predBodyPos[b]);
         const float4 bq = qNormalize(s.predBodyRot[b]);
@@ -161,18 +193,31 @@ __global__ void __launch_bounds__(kThreads) k_rigidPredict(Scene s, float dt, fl
         fr[1] = cwq;
         fr[2] = e0;
         fr[3] = e1;
+    });
+}
+
+__global__ void k_applyBodyTargets(Scene s, const BodyTarget *list, const uint32_t *count)
+{
+    const uint32_t n = *count;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const BodyTarget bt = list[t];
+        const uint32_t b = __float_as_uint(bt.pos.w);
+        if (b >= s.B) continue;
+        s.bodyKinPos[b] = make_float4(bt.pos.x, bt.pos.y, bt.pos.z, 0.0f);
+        s.bodyKinRot[b] = bt.rot;
+        s.bodyKinFlags[b] = 1u;
     }
 }
 
 // physics_rigid_update_velocities (copyPredictedRigidBodiesToPersistentState)
 __global__ void k_copyPredictedRigid(Scene s)
 {
-    for (uint32_t b = threadIdx.x; b < s.B; b += blockDim.x) {
+    forEachInBlock(s.wB, s.B, [&](uint32_t b) {
         s.bodyPos[b] = s.predBodyPos[b];
         s.bodyRot[b] = s.predBodyRot[b];
         s.bodyLin[b] = s.predBodyLin[b];
         s.bodyAng[b] = s.predBodyAng[b];
-    }
+    });
 }
 
 // ------------------------------------------------------------------------------------------
@@ -183,32 +228,32 @@ __global__ void k_copyPredictedRigid(Scene s)
 __global__ void __launch_bounds__(kThreads) k_predictKeys(Scene s, float dt, float gx, float gy, float gz,
                                                           bool writeKeys)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.N) return;
-    const float4 pim = s.x[i];
-    const f3 pos = xyz(pim);
-    s.xprev[i] = mk4(pos, 0.0f);
-    f3 pp = pos;
-    if (pim.w <= kEps) {
-        s.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    } else {
-        f3 vel = xyz(s.v[i]);
-        float gs = 1.0f;
-        if (s.kinds[i] == CN_PARTICLE_FLUID) gs = s.fluidMaterials[s.fluidMatIdx[i]].gravity_scale;
-        vel = vel + f3{gx, gy, gz} * (dt * gs);
-        pp = pos + vel * dt;
-        s.v[i] = mk4(vel, 0.0f);
-        s.x[i] = mk4(pp, pim.w);
-    }
-    if (!writeKeys) return;
-    const float safe = mx(s.cellSize, 1.0e-4f);
-    const float inv = 1.0f / safe;
-    const int cx = int(floorf(pp.x * inv));
-    const int cy = int(floorf(pp.y * inv));
-    const int cz = int(floorf(pp.z * inv));
-    const uint32_t key = cellKey(cx, cy, cz);
-    s.entries[i] = make_int4(cx, cy, cz, int(key));
-    s.keysA[i] = key;
+    forEachElem(s.wP, s.N, [&](uint32_t i) {
+        const float4 pim = s.x[i];
+        const f3 pos = xyz(pim);
+        s.xprev[i] = mk4(pos, 0.0f);
+        f3 pp = pos;
+        if (pim.w <= kEps) {
+            s.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        } else {
+            f3 vel = xyz(s.v[i]);
+            float gs = 1.0f;
+            if (s.kinds[i] == CN_PARTICLE_FLUID) gs = s.fluidMaterials[s.fluidMatIdx[i]].gravity_scale;
+            vel = vel + f3{gx, gy, gz} * (dt * gs);
+            pp = pos + vel * dt;
+            s.v[i] = mk4(vel, 0.0f);
+            s.x[i] = mk4(pp, pim.w);
+        }
+        if (!writeKeys) return;
+        const float safe = mx(s.cellSize, 1.0e-4f);
+        const float inv = 1.0f / safe;
+        const int cx = int(floorf(pp.x * inv));
+        const int cy = int(floorf(pp.y * inv));
+        const int cz = int(floorf(pp.z * inv));
+        const uint32_t key = cellKey(cx, cy, cz);
+        s.entries[i] = make_int4(cx, cy, cz, int(key));
+        s.keysA[i] = key;
+    });
 }
 
 // ------------------------------------------------------------------------------------------
@@ -423,47 +468,48 @@ __global__ void __launch_bounds__(kThreads) k_runNeighbors(Scene s)
 template <bool kEmit>
 __global__ void __launch_bounds__(kThreads) k_rigidCandidates(Scene s, const uint32_t *total)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (kEmit && blockIdx.x == 0 && threadIdx.x == 0) {
         s.meta_->requiredRigidPairs = *total;
         s.meta_->rigidPairCount = min(*total, s.rigidPairCapacity);
     }
-    if (i >= s.N) return;
-    if (kEmit && s.candCount[i] == 0u) return;
-    const f3 p = xyz(s.x[i]);
-    const float r = s.radii[i];
-    const f3 qmin = p - f3{r, r, r}, qmax = p + f3{r, r, r};
-    const uint4 m = s.meta[i];
-    const uint32_t kind = s.kinds[i];
-    const bool proxyOwner = s.ownerTypes[i] == CN_OWNER_RIGID_BODY;
-    const uint32_t owner = s.ownerIdx[i];
-    uint32_t seen[kRigidDedup];
-    uint32_t seenCount = 0, count = 0;
-    uint32_t write = kEmit ? s.candOffset[i] : 0u;
-    for (uint32_t k = 0; k < s.colQueryCount; ++k) {
-        const uint32_t c = s.colQueryOrder[k];
-        if (!aabbOverlaps(qmin, qmax, xyz(s.colAabbMin[c]), xyz(s.colAabbMax[c]))) continue;
-        const cn_collider_broadphase bp = s.colBp[c];
-        const uint32_t b = bp.owner_body;
-        if (proxyOwner && b == owner) continue;
-        const uint32_t bt = s.bodyType[b];
-        if (!(bp.enabled_flag != 0u && bp.environment_index == m.x && (m.w & bp.collision_layer) != 0u &&
-              (bp.collision_mask & m.z) != 0u && (kind == CN_PARTICLE_SOLID || bt == CN_BODY_DYNAMIC) &&
-              s.bodyColRanges[b].y > 0u))
-            continue;
-        bool fresh = true;
-        for (uint32_t q = 0; q < seenCount; ++q)
-            if (seen[q] == b) { fresh = false; break; }
-        if (!fresh) continue;
-        if (seenCount < kRigidDedup) seen[seenCount++] = b;
-        if (kEmit) {
-            if (write >= s.rigidPairCapacity) return;
-            s.rigidPairs[write++] = make_uint2(i, b);
-        } else {
-            ++count;
+    forEachElem(s.wP, s.N, [&](uint32_t i) {
+        if (kEmit && s.candCount[i] == 0u) return;
+        const f3 p = xyz(s.x[i]);
+        const float r = s.radii[i];
+        const f3 qmin = p - f3{r, r, r}, qmax = p + f3{r, r, r};
+        const uint4 m = s.meta[i];
+        const uint32_t kind = s.kinds[i];
+        const bool proxyOwner = s.ownerTypes[i] == CN_OWNER_RIGID_BODY;
+        const uint32_t owner = s.ownerIdx[i];
+        uint32_t seen[kRigidDedup];
+        uint32_t seenCount = 0, count = 0;
+        uint32_t write = kEmit ? s.candOffset[i] : 0u;
+        const uint2 cq = s.pColRange ? s.pColRange[i] : make_uint2(0u, s.colQueryCount);
+        for (uint32_t k = cq.x; k < cq.y; ++k) {
+            const uint32_t c = s.colQueryOrder[k];
+            if (!aabbOverlaps(qmin, qmax, xyz(s.colAabbMin[c]), xyz(s.colAabbMax[c]))) continue;
+            const cn_collider_broadphase bp = s.colBp[c];
+            const uint32_t b = bp.owner_body;
+            if (proxyOwner && b == owner) continue;
+            const uint32_t bt = s.bodyType[b];
+            if (!(bp.enabled_flag != 0u && bp.environment_index == m.x && (m.w & bp.collision_layer) != 0u &&
+                  (bp.collision_mask & m.z) != 0u && (kind == CN_PARTICLE_SOLID || bt == CN_BODY_DYNAMIC) &&
+                  s.bodyColRanges[b].y > 0u))
+                continue;
+            bool fresh = true;
+            for (uint32_t q = 0; q < seenCount; ++q)
+                if (seen[q] == b) { fresh = false; break; }
+            if (!fresh) continue;
+            if (seenCount < kRigidDedup) seen[seenCount++] = b;
+            if (kEmit) {
+                if (write >= s.rigidPairCapacity) return;
+                s.rigidPairs[write++] = make_uint2(i, b);
+            } else {
+                ++count;
+            }
         }
-    }
-    if (!kEmit) s.candCount[i] = count;
+        if (!kEmit) s.candCount[i] = count;
+    });
 }
 
 // ------------------------------------------------------------------------------------------
@@ -945,33 +991,33 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
 // physics_soft_solve_edge_constraints.cs.hlsl:10-74
 __global__ void __launch_bounds__(kThreads) k_solveEdges(Scene s, float dt, float relax)
 {
-    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= s.E) return;
-    const cn_soft_edge ed = s.edges[e];
-    float4 cA = make_float4(0.f, 0.f, 0.f, 0.f), cB = cA;
-    if (ed.enabled != 0u) {
-        const float4 a = s.x[ed.particle_a], b = s.x[ed.particle_b];
-        const float wA = a.w, wB = b.w, wSum = wA + wB;
-        const f3 delta = xyz(b) - xyz(a);
-        const float l2 = dot(delta, delta);
-        if (wSum > kEps && l2 > kEps) {
-            const float len = sqrtf(l2);
-            const f3 gA = -delta / len;
-            const f3 gB = -gA;
-            const float alpha = mx(ed.compliance, 0.0f) / mx(dt * dt, kEps);
-            const float Cv = len - ed.rest_length;
-            const float lambda = s.edgeLambda[e];
-            const float den = wSum + alpha;
-            if (den > kEps) {
-                const float dl = -(Cv + alpha * lambda) / den;
-                s.edgeLambda[e] = lambda + dl;
-                cA = mk4(wA * dl * gA * relax, 0.0f);
-                cB = mk4(wB * dl * gB * relax, 0.0f);
+    forEachElem(s.wE, s.E, [&](uint32_t e) {
+        const cn_soft_edge ed = s.edges[e];
+        float4 cA = make_float4(0.f, 0.f, 0.f, 0.f), cB = cA;
+        if (ed.enabled != 0u) {
+            const float4 a = s.x[ed.particle_a], b = s.x[ed.particle_b];
+            const float wA = a.w, wB = b.w, wSum = wA + wB;
+            const f3 delta = xyz(b) - xyz(a);
+            const float l2 = dot(delta, delta);
+            if (wSum > kEps && l2 > kEps) {
+                const float len = sqrtf(l2);
+                const f3 gA = -delta / len;
+                const f3 gB = -gA;
+                const float alpha = mx(ed.compliance, 0.0f) / mx(dt * dt, kEps);
+                const float Cv = len - ed.rest_length;
+                const float lambda = s.edgeLambda[e];
+                const float den = wSum + alpha;
+                if (den > kEps) {
+                    const float dl = -(Cv + alpha * lambda) / den;
+                    s.edgeLambda[e] = lambda + dl;
+                    cA = mk4(wA * dl * gA * relax, 0.0f);
+                    cB = mk4(wB * dl * gB * relax, 0.0f);
+                }
             }
         }
-    }
-    s.edgeCorr[2 * e] = cA;
-    s.edgeCorr[2 * e + 1] = cB;
+        s.edgeCorr[2 * e] = cA;
+        s.edgeCorr[2 * e + 1] = cB;
+    });
 }
 
 // physics_soft_apply_edge_corrections.cs.hlsl:9-35 (also the strand distance apply:
@@ -979,66 +1025,66 @@ __global__ void __launch_bounds__(kThreads) k_solveEdges(Scene s, float dt, floa
 __global__ void __launch_bounds__(kThreads) k_applyPair(Scene s, const uint2 *ranges, const uint2 *inc,
                                                         const float4 *corr)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.N) return;
-    const float4 p = s.x[i];
-    if (p.w <= kEps) return;
-    const uint2 r = ranges[i];
-    f3 total{0.f, 0.f, 0.f};
-    for (uint32_t k = 0; k < r.y; ++k) {
-        const uint2 ref = inc[r.x + k];
-        total += xyz(corr[2 * ref.x + (ref.y == 0u ? 0u : 1u)]);
-    }
-    s.x[i] = mk4(xyz(p) + total, p.w);
+    forEachElem(s.wP, s.N, [&](uint32_t i) {
+        const float4 p = s.x[i];
+        if (p.w <= kEps) return;
+        const uint2 r = ranges[i];
+        f3 total{0.f, 0.f, 0.f};
+        for (uint32_t k = 0; k < r.y; ++k) {
+            const uint2 ref = inc[r.x + k];
+            total += xyz(corr[2 * ref.x + (ref.y == 0u ? 0u : 1u)]);
+        }
+        s.x[i] = mk4(xyz(p) + total, p.w);
+    });
 }
 
 // physics_soft_apply_tet_corrections.cs.hlsl:9-50, physics_soft_apply_bend_corrections.cs.hlsl:9-51
 __global__ void __launch_bounds__(kThreads) k_applyQuad(Scene s, const uint2 *ranges, const uint2 *inc,
                                                         const float4 *corr)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.N) return;
-    const float4 p = s.x[i];
-    if (p.w <= kEps) return;
-    const uint2 r = ranges[i];
-    f3 total{0.f, 0.f, 0.f};
-    for (uint32_t k = 0; k < r.y; ++k) {
-        const uint2 ref = inc[r.x + k];
-        total += xyz(corr[4 * ref.x + (ref.y > 3u ? 3u : ref.y)]);
-    }
-    s.x[i] = mk4(xyz(p) + total, p.w);
+    forEachElem(s.wP, s.N, [&](uint32_t i) {
+        const float4 p = s.x[i];
+        if (p.w <= kEps) return;
+        const uint2 r = ranges[i];
+        f3 total{0.f, 0.f, 0.f};
+        for (uint32_t k = 0; k < r.y; ++k) {
+            const uint2 ref = inc[r.x + k];
+            total += xyz(corr[4 * ref.x + (ref.y > 3u ? 3u : ref.y)]);
+        }
+        s.x[i] = mk4(xyz(p) + total, p.w);
+    });
 }
 
 // physics_soft_solve_tet_constraints.cs.hlsl:15-87
 __global__ void __launch_bounds__(kThreads) k_solveTets(Scene s, float dt, float relax)
 {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= s.T) return;
-    const cn_soft_tet tet = s.tets[t];
-    const float4 q0 = s.x[tet.particle_indices[0]], q1 = s.x[tet.particle_indices[1]];
-    const float4 q2 = s.x[tet.particle_indices[2]], q3 = s.x[tet.particle_indices[3]];
-    const float w0 = q0.w, w1 = q1.w, w2 = q2.w, w3 = q3.w;
-    if ((w0 + w1 + w2 + w3) <= kEps) return; // keeps the previous correction record
-    const f3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2), p3 = xyz(q3);
-    const float sv = dot(cross(p1 - p0, p2 - p0), p3 - p0) / 6.0f;
-    const float vs = (sv >= 0.0f) ? 1.0f : -1.0f;
-    const float Cv = fabsf(sv) - mx(tet.rest_volume, 0.0f);
-    const f3 g0 = cross(p3 - p1, p2 - p1) * (vs / 6.0f);
-    const f3 g1 = cross(p2 - p0, p3 - p0) * (vs / 6.0f);
-    const f3 g2 = cross(p3 - p0, p1 - p0) * (vs / 6.0f);
-    const f3 g3 = cross(p1 - p0, p2 - p0) * (vs / 6.0f);
-    const float sg = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
-    const float alpha = mx(tet.compliance, 0.0f) / mx(dt * dt, kEps);
-    const float lambda = s.tetLambda[t];
-    const float den = sg + alpha;
-    if (den <= kEps) return;
-    const float dl = -(Cv + alpha * lambda) / den;
-    s.tetLambda[t] = lambda + dl;
-    float4 *out = s.tetCorr + 4 * size_t(t);
-    out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
-    out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
-    out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
-    out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
+    forEachElem(s.wT, s.T, [&](uint32_t t) {
+        const cn_soft_tet tet = s.tets[t];
+        const float4 q0 = s.x[tet.particle_indices[0]], q1 = s.x[tet.particle_indices[1]];
+        const float4 q2 = s.x[tet.particle_indices[2]], q3 = s.x[tet.particle_indices[3]];
+        const float w0 = q0.w, w1 = q1.w, w2 = q2.w, w3 = q3.w;
+        if ((w0 + w1 + w2 + w3) <= kEps) return; // keeps the previous correction record
+        const f3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2), p3 = xyz(q3);
+        const float sv = dot(cross(p1 - p0, p2 - p0), p3 - p0) / 6.0f;
+        const float vs = (sv >= 0.0f) ? 1.0f : -1.0f;
+        const float Cv = fabsf(sv) - mx(tet.rest_volume, 0.0f);
+        const f3 g0 = cross(p3 - p1, p2 - p1) * (vs / 6.0f);
+        const f3 g1 = cross(p2 - p0, p3 - p0) * (vs / 6.0f);
+        const f3 g2 = cross(p3 - p0, p1 - p0) * (vs / 6.0f);
+        const f3 g3 = cross(p1 - p0, p2 - p0) * (vs / 6.0f);
+        const float sg = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
+        const float alpha = mx(tet.compliance, 0.0f) / mx(dt * dt, kEps);
+        const float lambda = s.tetLambda[t];
+        const float den = sg + alpha;
+        if (den <= kEps) return;
+        const float dl = -(Cv + alpha * lambda) / den;
+        s.tetLambda[t] = lambda + dl;
+        float4 *out = s.tetCorr + 4 * size_t(t);
+        out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
+        out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
+        out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
+        out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
+    });
 }
 
 // physics_soft_solve_bend_constraints.cs.hlsl:20-86
@@ -1527,39 +1573,39 @@ __device__ f3 solveRigidContact(const Scene &s, const Config &cfg, const RigidCo
 // (physics_particle_apply_position_corrections.cs.hlsl:8-30).
 __global__ void __launch_bounds__(kThreads) k_rigidContacts(Scene s, Config cfg, bool applyDirect)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.N) return;
-    const uint32_t cnt = s.candCount[i];
-    const float4 sp = s.x[i];
-    f3 corr{0.f, 0.f, 0.f};
-    bool any = false;
-    if (cnt) {
-        const uint32_t off = s.candOffset[i];
-        const uint32_t lim = s.meta_->rigidPairCount;
-        for (uint32_t k = 0; k < cnt; ++k) {
-            const uint32_t pi = off + k;
-            if (pi >= lim) break;
-            const uint2 pr = s.rigidPairs[pi];
-            const RigidContact c = generateRigidContact(s, pr.x, pr.y);
-            s.rigidContacts[pi] = c;
-            if (!c.active) continue;
-            const f3 d = solveRigidContact(s, cfg, c, sp);
-            // float atomic order of the reference == pair order here
-            if (sp.w > kEps) {
-                corr = corr + d;
-                any = true;
+    forEachElem(s.wP, s.N, [&](uint32_t i) {
+        const uint32_t cnt = s.candCount[i];
+        const float4 sp = s.x[i];
+        f3 corr{0.f, 0.f, 0.f};
+        bool any = false;
+        if (cnt) {
+            const uint32_t off = s.candOffset[i];
+            const uint32_t lim = s.meta_->rigidPairCount;
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const uint32_t pi = off + k;
+                if (pi >= lim) break;
+                const uint2 pr = s.rigidPairs[pi];
+                const RigidContact c = generateRigidContact(s, pr.x, pr.y);
+                s.rigidContacts[pi] = c;
+                if (!c.active) continue;
+                const f3 d = solveRigidContact(s, cfg, c, sp);
+                // float atomic order of the reference == pair order here
+                if (sp.w > kEps) {
+                    corr = corr + d;
+                    any = true;
+                }
             }
         }
-    }
-    if (applyDirect) {
-        // applyParticlePositionCorrections with an accumulator that only this pass wrote
-        if (sp.w <= kEps) return;
-        s.x[i] = mk4(xyz(sp) + corr, sp.w);
-    } else if (any) {
-        float4 pc = s.posCorr[i];
-        pc = mk4(xyz(pc) + corr, pc.w);
-        s.posCorr[i] = pc;
-    }
+        if (applyDirect) {
+            // applyParticlePositionCorrections with an accumulator that only this pass wrote
+            if (sp.w <= kEps) return;
+            s.x[i] = mk4(xyz(sp) + corr, sp.w);
+        } else if (any) {
+            float4 pc = s.posCorr[i];
+            pc = mk4(xyz(pc) + corr, pc.w);
+            s.posCorr[i] = pc;
+        }
+    });
 }
 
 // physics_particle_apply_position_corrections.cs.hlsl:8-30
@@ -1581,22 +1627,22 @@ __global__ void __launch_bounds__(kThreads) k_applyPositionCorrections(Scene s)
 // particle's sorted slot)
 __global__ void __launch_bounds__(kThreads) k_updateVelocities(Scene s, float dt, const float4 *Dfinal)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.N) return;
-    const float4 p = s.x[i];
-    if (p.w <= kEps || dt <= kEps) {
-        s.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        return;
-    }
-    const f3 pp = xyz(s.xprev[i]);
-    f3 pos = xyz(p);
-    if (Dfinal && s.kinds[i] == CN_PARTICLE_FLUID) {
-        pos += xyz(Dfinal[s.rank[i]]);
-        s.x[i] = mk4(pos, p.w);
-    }
-    const float damping = mx(s.contactMaterials[s.matIdx[i]].z, 0.0f);
-    const float ds = mx(1.0f - damping * dt, 0.0f);
-    s.v[i] = mk4(((pos - pp) / dt) * ds, 0.0f);
+    forEachElem(s.wP, s.N, [&](uint32_t i) {
+        const float4 p = s.x[i];
+        if (p.w <= kEps || dt <= kEps) {
+            s.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            return;
+        }
+        const f3 pp = xyz(s.xprev[i]);
+        f3 pos = xyz(p);
+        if (Dfinal && s.kinds[i] == CN_PARTICLE_FLUID) {
+            pos += xyz(Dfinal[s.rank[i]]);
+            s.x[i] = mk4(pos, p.w);
+        }
+        const float damping = mx(s.contactMaterials[s.matIdx[i]].z, 0.0f);
+        const float ds = mx(1.0f - damping * dt, 0.0f);
+        s.v[i] = mk4(((pos - pp) / dt) * ds, 0.0f);
+    });
 }
 
 // physics_fluid_project_boundary_velocities.cs.hlsl:24-117
@@ -1654,49 +1700,49 @@ __global__ void __launch_bounds__(kThreads) k_fluidBoundaryVelocities(Scene s, f
 // on its own contacts, and the per-particle sum runs in contact order.
 __global__ void __launch_bounds__(kThreads) k_rigidContactVelocities(Scene s, uint32_t iterations, Config cfg)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.N) return;
-    const uint32_t cnt = s.candCount[i];
-    if (cnt == 0u) return;
-    const float iS = s.x[i].w;
-    if (iS <= kEps) return; // corrections are only applied to particles with mass
-    const uint32_t off = s.candOffset[i];
-    const uint32_t lim = s.meta_->rigidPairCount;
-    const float rpt = cfg.restitutionPenetrationThreshold;
-    f3 vel = xyz(s.v[i]);
-    const float vw = s.v[i].w;
-    for (uint32_t it = 0; it < iterations; ++it) {
-        f3 corr{0.f, 0.f, 0.f};
-        for (uint32_t k = 0; k < cnt; ++k) {
-            const uint32_t pi = off + k;
-            if (pi >= lim) break;
-            const RigidContact c = s.rigidContacts[pi];
-            if (!c.active) continue;
-            const uint32_t b = c.body;
-            const float4 rp = s.predBodyPos[b];
-            const float iR = s.bodyType[b] == CN_BODY_DYNAMIC ? rp.w : 0.0f;
-            const float4 rq = qNormalize(s.predBodyRot[b]);
-            const f3 rl = xyz(s.predBodyLin[b]), ra = xyz(s.predBodyAng[b]);
-            const f3 inI = xyz(s.bodyInvInertia[b]);
-            const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
-            const f3 cp = xyz(rp) + qRotate(rq, xyz(c.rigidLocalPoint));
-            const f3 rR = cp - xyz(rp);
-            const f3 rcv = rl + cross(ra, rR);
-            const f3 rel = vel - rcv;
-            const float nv = dot(rel, n);
-            if (nv >= 0.0f) continue;
-            const float nd = iS + contactEffectiveMass(iR, inI, rq, rR, n);
-            if (nd <= kEps) continue;
-            const f3 mat = combineContactMaterial(s.contactMaterials[s.matIdx[i]], s.colMat[c.collider]);
-            const bool er = (-nv > cfg.restitutionVelocityThreshold) && (c.normalPenetration.w <= rpt);
-            const float rest = er ? saturate(mat.y) : 0.0f;
-            const float dnv = er ? (-rest * nv) : 0.0f;
-            const float imp = mx(0.0f, (dnv - nv) / nd);
-            corr = corr + (n * imp) * iS;
+    forEachElem(s.wP, s.N, [&](uint32_t i) {
+        const uint32_t cnt = s.candCount[i];
+        if (cnt == 0u) return;
+        const float iS = s.x[i].w;
+        if (iS <= kEps) return; // corrections are only applied to particles with mass
+        const uint32_t off = s.candOffset[i];
+        const uint32_t lim = s.meta_->rigidPairCount;
+        const float rpt = cfg.restitutionPenetrationThreshold;
+        f3 vel = xyz(s.v[i]);
+        const float vw = s.v[i].w;
+        for (uint32_t it = 0; it < iterations; ++it) {
+            f3 corr{0.f, 0.f, 0.f};
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const uint32_t pi = off + k;
+                if (pi >= lim) break;
+                const RigidContact c = s.rigidContacts[pi];
+                if (!c.active) continue;
+                const uint32_t b = c.body;
+                const float4 rp = s.predBodyPos[b];
+                const float iR = s.bodyType[b] == CN_BODY_DYNAMIC ? rp.w : 0.0f;
+                const float4 rq = qNormalize(s.predBodyRot[b]);
+                const f3 rl = xyz(s.predBodyLin[b]), ra = xyz(s.predBodyAng[b]);
+                const f3 inI = xyz(s.bodyInvInertia[b]);
+                const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
+                const f3 cp = xyz(rp) + qRotate(rq, xyz(c.rigidLocalPoint));
+                const f3 rR = cp - xyz(rp);
+                const f3 rcv = rl + cross(ra, rR);
+                const f3 rel = vel - rcv;
+                const float nv = dot(rel, n);
+                if (nv >= 0.0f) continue;
+                const float nd = iS + contactEffectiveMass(iR, inI, rq, rR, n);
+                if (nd <= kEps) continue;
+                const f3 mat = combineContactMaterial(s.contactMaterials[s.matIdx[i]], s.colMat[c.collider]);
+                const bool er = (-nv > cfg.restitutionVelocityThreshold) && (c.normalPenetration.w <= rpt);
+                const float rest = er ? saturate(mat.y) : 0.0f;
+                const float dnv = er ? (-rest * nv) : 0.0f;
+                const float imp = mx(0.0f, (dnv - nv) / nd);
+                corr = corr + (n * imp) * iS;
+            }
+            vel = vel + corr;
         }
-        vel = vel + corr;
-    }
-    s.v[i] = mk4(vel, vw);
+        s.v[i] = mk4(vel, vw);
+    });
 }
 
 // physics_particle_solve_contact_velocities.cs.hlsl (non-proxy) with float atomics.
@@ -1772,6 +1818,13 @@ void launchRigidPredict(const Scene &s, float dt, float gx, float gy, float gz, 
     k_rigidPredict<<<1, kThreads, 0, st>>>(s, dt, gx, gy, gz);
 }
 
+void launchApplyBodyTargets(const Scene &s, const BodyTarget *list, const uint32_t *count, uint32_t capacity,
+                            cudaStream_t st)
+{
+    if (capacity == 0) return;
+    k_applyBodyTargets<<<blocksFor(capacity) < 64u ? blocksFor(capacity) : 64u, kThreads, 0, st>>>(s, list, count);
+}
+
 void launchCopyPredictedRigid(const Scene &s, cudaStream_t st)
 {
     if (s.B == 0) return;
@@ -1781,7 +1834,7 @@ void launchCopyPredictedRigid(const Scene &s, cudaStream_t st)
 void launchPredictAndKeys(const Scene &s, float dt, const Config &c, cudaStream_t st)
 {
     if (s.N == 0) return;
-    k_predictKeys<<<blocksFor(s.N), kThreads, 0, st>>>(s, dt, c.gravity[0], c.gravity[1], c.gravity[2],
+    k_predictKeys<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, dt, c.gravity[0], c.gravity[1], c.gravity[2],
                                                        s.entries != nullptr);
 }
 
@@ -1807,10 +1860,11 @@ void launchCellSetup(const Scene &s, uint32_t *scanTmp, void *sortScratch, cudaS
 void launchRigidCandidates(const Scene &s, uint32_t *scanTmp, size_t, cudaStream_t st)
 {
     if (s.N == 0) return;
-    k_rigidCandidates<false><<<blocksFor(s.N), kThreads, 0, st>>>(s, nullptr);
+    if (s.wP.tiles) cudaMemsetAsync(s.candCount, 0, sizeof(uint32_t) * s.N, st); // scenes not stepped: none
+    k_rigidCandidates<false><<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, nullptr);
     uint32_t *total = scanTmp;
     exclusiveScan(s.candCount, s.candOffset, s.N, total, scanTmp + 1, st);
-    k_rigidCandidates<true><<<blocksFor(s.N), kThreads, 0, st>>>(s, total);
+    k_rigidCandidates<true><<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, total);
 }
 
 void launchParticleCandidates(const Scene &s, uint32_t *scanTmp, size_t, cudaStream_t st)
@@ -1868,8 +1922,8 @@ void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t
 {
     const float relax = c.softInternalRelaxation;
     if (s.E) {
-        k_solveEdges<<<blocksFor(s.E), kThreads, 0, st>>>(s, dt, relax);
-        k_applyPair<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.edgeRanges, s.edgeInc, s.edgeCorr);
+        k_solveEdges<<<gridFor(s.wE, s.E), kThreads, 0, st>>>(s, dt, relax);
+        k_applyPair<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, s.edgeRanges, s.edgeInc, s.edgeCorr);
     }
     if (s.S) {
         k_solveSegments<<<blocksFor(s.S), kThreads, 0, st>>>(s, dt, relax);
@@ -1889,8 +1943,8 @@ void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t
         k_applyPair<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.segRanges, s.segInc, s.distCorr);
     }
     if (s.T) {
-        k_solveTets<<<blocksFor(s.T), kThreads, 0, st>>>(s, dt, relax);
-        k_applyQuad<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.tetRanges, s.tetInc, s.tetCorr);
+        k_solveTets<<<gridFor(s.wT, s.T), kThreads, 0, st>>>(s, dt, relax);
+        k_applyQuad<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, s.tetRanges, s.tetInc, s.tetCorr);
     }
 }
 
@@ -1902,14 +1956,14 @@ void launchContacts(const Scene &s, const Config &c, bool particleContacts, bool
         k_particleContactGenerate<<<blocksFor(cap), kThreads, 0, st>>>(s);
         k_particleContactSolve<<<blocksFor(cap), kThreads, 0, st>>>(s, c);
     }
-    if (rigidContacts) k_rigidContacts<<<blocksFor(s.N), kThreads, 0, st>>>(s, c, !particleContacts);
+    if (rigidContacts) k_rigidContacts<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, c, !particleContacts);
     if (particleContacts) k_applyPositionCorrections<<<blocksFor(s.N), kThreads, 0, st>>>(s);
 }
 
 void launchUpdateVelocities(const Scene &s, float dt, const float4 *fluidDelta, cudaStream_t st)
 {
     if (s.N == 0) return;
-    k_updateVelocities<<<blocksFor(s.N), kThreads, 0, st>>>(s, dt, fluidDelta);
+    k_updateVelocities<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, dt, fluidDelta);
 }
 
 void launchFluidBoundaryVelocities(const Scene &s, float dt, const Config &c, cudaStream_t st)
@@ -1921,7 +1975,7 @@ void launchFluidBoundaryVelocities(const Scene &s, float dt, const Config &c, cu
 void launchRigidContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st)
 {
     if (s.N == 0 || iterations == 0) return;
-    k_rigidContactVelocities<<<blocksFor(s.N), kThreads, 0, st>>>(s, iterations, c);
+    k_rigidContactVelocities<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, iterations, c);
 }
 
 void launchParticleContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st)

@@ -24,40 +24,12 @@ namespace cn {
 
 thread_local std::string g_lastError;
 
-inline uint32_t nextPow2(uint32_t v)
-{
-    if (v <= 1u) return 1u;
-    --v;
-    v |= v >> 1; v |= v >> 2; v |= v >> 4; v |= v >> 8; v |= v >> 16;
-    return v + 1u;
-}
-inline uint32_t resolveIter(uint32_t o, uint32_t d) { return o > 0u ? o : d; }
-
 cn_status setError(cn_status status, const std::string &message)
 {
     g_lastError = message;
     return status;
 }
 void clearError() { g_lastError.clear(); }
-
-// Bump allocator over one device allocation.  measure() runs the same layout code with a null
-// base to size the arena.
-class Arena {
-public:
-    void reset(uint8_t *base) { base_ = base; offset_ = 0; }
-    template <class T> T *take(size_t count)
-    {
-        const size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
-        T *p = base_ ? reinterpret_cast<T *>(base_ + offset_) : nullptr;
-        offset_ += count ? bytes : 0;
-        return count ? p : nullptr;
-    }
-    size_t size() const { return offset_; }
-
-private:
-    uint8_t *base_ = nullptr;
-    size_t offset_ = 0;
-};
 
 } // namespace cn
 
@@ -144,38 +116,9 @@ void releaseBuffers(cn_solver *sv)
     sv->synced = false;
 }
 
-struct Incidence {
-    std::vector<uint2> ranges, inc;
-};
-template <class F> Incidence buildIncidence(uint32_t n, uint32_t constraints, uint32_t perConstraint, F &&particlesOf)
-{
-    // physics_scene_gpu_state.cpp:3273-3420: per-particle lists in ascending constraint order
-    std::vector<uint32_t> counts(n, 0);
-    for (uint32_t c = 0; c < constraints; ++c)
-        for (uint32_t k = 0; k < perConstraint; ++k) {
-            const uint32_t p = particlesOf(c, k);
-            if (p < n) ++counts[p];
-        }
-    Incidence out;
-    out.ranges.resize(n);
-    uint32_t run = 0;
-    for (uint32_t i = 0; i < n; ++i) {
-        out.ranges[i] = make_uint2(run, counts[i]);
-        run += counts[i];
-    }
-    out.inc.resize(run);
-    std::vector<uint32_t> fill(n, 0);
-    for (uint32_t c = 0; c < constraints; ++c)
-        for (uint32_t k = 0; k < perConstraint; ++k) {
-            const uint32_t p = particlesOf(c, k);
-            if (p < n) out.inc[out.ranges[p].x + fill[p]++] = make_uint2(c, k);
-        }
-    return out;
-}
-
 // Lays out every device buffer; `upload` false only sizes the arena.
-void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const Incidence &edgeI, const Incidence &bendI,
-            const Incidence &tetI, const Incidence &segI, const Incidence &jointI)
+void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incidence &edgeI, const cn::Incidence &bendI,
+            const cn::Incidence &tetI, const cn::Incidence &segI, const cn::Incidence &jointI)
 {
     cn::Scene &s = sv->s;
     const uint32_t N = w.particle_count;
@@ -534,24 +477,17 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     }
 
     // Collider query order: moving (kinematic) colliders, then static, ascending index.
-    std::vector<uint32_t> order, stat;
-    for (uint32_t c = 0; c < w->collider_count; ++c) {
-        const cn_collider_broadphase &bp = w->collider_broadphase[c];
-        if (bp.owner_body >= w->rigid_body_count || bp.enabled_flag == 0u) continue;
-        if (w->body_types[bp.owner_body] == CN_BODY_STATIC) stat.push_back(c);
-        else order.push_back(c);
-    }
-    const uint32_t moving = uint32_t(order.size());
-    order.insert(order.end(), stat.begin(), stat.end());
+    std::vector<uint32_t> order;
+    const uint32_t moving = cn::colliderQueryOrder(*w, order);
     if (anyFluid && order.size() > cn::kMaxBoundaryColliders)
         return setError(CN_ERR_UNSUPPORTED, "more than 64 colliders in a scene with fluid");
 
     // Incidence tables.
-    const Incidence edgeI = buildIncidence(N, w->edge_count, 2, [&](uint32_t c, uint32_t k) {
+    const cn::Incidence edgeI = cn::buildIncidence(N, w->edge_count, 2, [&](uint32_t c, uint32_t k) {
         return k == 0 ? w->edges[c].particle_a : w->edges[c].particle_b;
     });
     const uint32_t nb = w->bend_count;
-    const Incidence bendI = buildIncidence(N, nb + w->dihedral_count, 4, [&](uint32_t c, uint32_t k) -> uint32_t {
+    const cn::Incidence bendI = cn::buildIncidence(N, nb + w->dihedral_count, 4, [&](uint32_t c, uint32_t k) -> uint32_t {
         if (c < nb) {
             if (k == 3) return 0xffffffffu;
             const cn_soft_bend &b = w->bends[c];
@@ -561,14 +497,14 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
         const uint32_t p[4] = {h.edge_particle0, h.edge_particle1, h.opposite_particle0, h.opposite_particle1};
         return p[k];
     });
-    const Incidence tetI = buildIncidence(N, w->tet_count, 4, [&](uint32_t c, uint32_t k) {
+    const cn::Incidence tetI = cn::buildIncidence(N, w->tet_count, 4, [&](uint32_t c, uint32_t k) {
         return w->tets[c].particle_indices[k];
     });
-    const Incidence segI = buildIncidence(N, w->strand_segment_count, 2, [&](uint32_t c, uint32_t k) {
+    const cn::Incidence segI = cn::buildIncidence(N, w->strand_segment_count, 2, [&](uint32_t c, uint32_t k) {
         return k == 0 ? w->strand_segments[c].particle_a : w->strand_segments[c].particle_b;
     });
     const uint32_t S = w->strand_segment_count;
-    const Incidence jointI = buildIncidence(S, w->strand_joint_count, 2, [&](uint32_t c, uint32_t k) -> uint32_t {
+    const cn::Incidence jointI = cn::buildIncidence(S, w->strand_joint_count, 2, [&](uint32_t c, uint32_t k) -> uint32_t {
         const cn_strand_joint &j = w->strand_joints[c];
         if (j.segment_a >= S || j.segment_b >= S) return 0xffffffffu;
         return k == 0 ? j.segment_a : j.segment_b;
@@ -654,20 +590,7 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     CN_CUDA(up(s.colQueryOrder, order.data(), order.size(), st));
     CN_CUDA(cudaStreamSynchronize(st));
 
-    cn::Config &c = sv->cfg;
-    c.slop = d.contact.slop;
-    c.softContactRelaxation = d.contact.soft_relaxation;
-    c.softMaxCorrection = d.contact.soft_max_correction_per_iteration;
-    c.restitutionVelocityThreshold = d.contact.restitution_velocity_threshold;
-    c.restitutionPenetrationThreshold = d.contact.restitution_penetration_slop_multiplier * d.contact.slop;
-    c.positionFrictionMinDistance = d.contact.position_friction_min_distance;
-    c.softInternalRelaxation = d.soft.internal_relaxation;
-    c.fluidSolveCoefficient = d.fluid.constraint_relaxation;
-    c.fluidRelaxation = d.fluid.position_relaxation;
-    c.fluidBoundaryDensityScale = d.fluid.boundary_density_scale;
-    c.fluidBoundaryDeltaScale = d.fluid.boundary_delta_scale;
-    c.fluidMaxUnderDensityRatio = d.fluid.max_under_density_ratio;
-    c.gravity[0] = d.gravity[0]; c.gravity[1] = d.gravity[1]; c.gravity[2] = d.gravity[2];
+    sv->cfg = cn::configFromDesc(d);
     sv->hostX = w->positions_inv_mass;
     sv->hostV = w->velocities;
     sv->cellRangeCapacity = cn::nextPow2(std::max<uint32_t>(N * 2u, 1u));

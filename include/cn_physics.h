@@ -481,6 +481,112 @@ typedef enum cn_debug_buffer {
 CN_API cn_status cn_solver_debug_read(cn_solver *solver, cn_debug_buffer which, void *dst,
                                       size_t capacity_bytes, size_t *out_bytes);
 
+/* ------------------------------------------------------------------------ */
+/* Batched scenes (no counterpart in the reference, which steps one          */
+/* PhysicsWorld per PhysicsSolver).  Independent soft-tissue scenes (XPBD     */
+/* edges + tets, static / kinematic colliders) live in one device pool, each  */
+/* in its own index ranges, and any subset of them is stepped by one tick:    */
+/* one CUDA graph whose kernels stride over per-scene work tiles.  A scene    */
+/* stepped in a batch gets the same bits as in a cn_solver of its own.       */
+/* ------------------------------------------------------------------------ */
+typedef struct cn_batch cn_batch;
+
+typedef struct cn_batch_desc {
+    cn_solver_desc solver;          /* substeps, iterations and settings shared by all scenes */
+    uint64_t memory_budget_bytes;   /* admission bound: device bytes the admitted scenes may use */
+    uint32_t max_scenes;            /* resident scenes at most (sizes the per-tick work lists) */
+    uint32_t particle_capacity;     /* pool sizes; 0 = split from the budget by a soft-tissue mix */
+    uint32_t edge_capacity, tet_capacity, body_capacity, collider_capacity;
+    uint32_t tile_elements;         /* elements per work tile (autotuned by cn_batch_autotune) */
+    uint32_t blocks_per_sm;         /* grid of the tile kernels = SMs x this */
+    uint32_t rigid_pairs_per_particle;
+    uint32_t reserved[3];
+} cn_batch_desc;
+
+typedef struct cn_batch_stats {
+    uint32_t resident_scenes;
+    uint32_t particles_used, particle_capacity, edges_used, edge_capacity, tets_used, tet_capacity;
+    uint32_t tile_elements, grid_blocks, reserved0;
+    uint64_t budget_bytes, budget_used_bytes, pool_bytes, ticks;
+} cn_batch_stats;
+
+typedef struct cn_batch_candidate { uint32_t tile_elements, blocks_per_sm; float tick_ms; uint32_t reserved; } cn_batch_candidate;
+typedef struct cn_batch_tuning {
+    uint32_t tile_elements, blocks_per_sm;
+    float tick_ms;
+    uint32_t candidate_count;
+    cn_batch_candidate candidates[16];
+} cn_batch_tuning;
+
+CN_API void cn_batch_desc_defaults(cn_batch_desc *desc);
+CN_API cn_status cn_batch_create(const cn_batch_desc *desc, int cuda_device, cn_batch **out_batch);
+CN_API void cn_batch_destroy(cn_batch *batch);
+/* Admits one scene (a world SoA with 0-based indices).  CN_ERR_CAPACITY when the budget or the
+ * pool has no room; CN_ERR_UNSUPPORTED for fluid, cloth, strand, self-colliding or dynamic-body
+ * content. */
+CN_API cn_status cn_batch_add_scene(cn_batch *batch, const cn_world_soa *world, uint32_t *out_scene);
+CN_API cn_status cn_batch_remove_scene(cn_batch *batch, uint32_t scene);
+/* Staged until the next cn_batch_step, as cn_solver_set_kinematic_target for one scene's body. */
+CN_API cn_status cn_batch_set_kinematic_target(cn_batch *batch, uint32_t scene, uint32_t body,
+                                               const float position[3], const float orientation[4]);
+/* One frame of every listed scene (the others do not move), asynchronous on `stream`. */
+CN_API cn_status cn_batch_step(cn_batch *batch, const uint32_t *scenes, uint32_t count, float frame_dt,
+                               void *stream);
+CN_API cn_status cn_batch_read_particles(cn_batch *batch, uint32_t scene, float *positions_inv_mass,
+                                         float *velocities, uint32_t count);
+/* Writes a scene's particle and rigid-body state back into its SoA (before evicting it). */
+CN_API cn_status cn_batch_export_scene(cn_batch *batch, uint32_t scene, cn_world_soa *world);
+CN_API cn_status cn_batch_get_stats(cn_batch *batch, cn_batch_stats *out);
+CN_API cn_status cn_batch_set_schedule(cn_batch *batch, uint32_t tile_elements, uint32_t blocks_per_sm);
+/* Times a tick of `scenes` for each (tile size, blocks per SM) candidate, keeps the fastest and
+ * restores the scenes' state. */
+CN_API cn_status cn_batch_autotune(cn_batch *batch, const uint32_t *scenes, uint32_t count, float frame_dt,
+                                   cn_batch_tuning *out);
+
+/* Serving loop over a batch (no counterpart in the reference).  Scenes are registered once (a
+ * host copy is kept) and admitted to the batch's pool when a request needs them and the memory
+ * budget allows, evicting idle scenes (least recently stepped first) when it does not.  Each
+ * tick steps one frame of every resident scene with pending work; requests that arrive while
+ * ticks run join the next tick.  Times are seconds on the server's steady clock. */
+typedef struct cn_server cn_server;
+typedef struct cn_server_desc {
+    float frame_dt;
+    uint32_t max_scenes_per_tick;   /* 0 = every scene with pending work */
+    uint32_t reserved[6];
+} cn_server_desc;
+typedef struct cn_request_done {
+    uint64_t request_id;
+    uint32_t scene, steps;
+    double submit_s, first_tick_s, done_s;
+} cn_request_done;
+typedef struct cn_server_stats {
+    uint64_t ticks, scene_steps, particle_substeps, admissions, evictions, completed, pending;
+    uint32_t resident_scenes, registered_scenes;
+    double gpu_ms;
+    float tick_ms_p50, tick_ms_p99;
+} cn_server_stats;
+
+CN_API void cn_server_desc_defaults(cn_server_desc *desc);
+/* `substeps` is the batch's substep count (used for the particle-substep count). */
+CN_API cn_status cn_server_create(cn_batch *batch, const cn_server_desc *desc, uint32_t substeps, cn_server **out);
+CN_API void cn_server_destroy(cn_server *server);
+CN_API cn_status cn_server_register_scene(cn_server *server, const cn_world_soa *world, uint32_t *out_scene);
+/* Makes a registered scene resident ahead of its requests (evicting idle scenes if needed);
+ * CN_ERR_CAPACITY when the budget has no room. */
+CN_API cn_status cn_server_admit(cn_server *server, uint32_t scene);
+/* k frames of one scene; tool_targets (k x 7 floats: position xyz, orientation xyzw) drive the
+ * kinematic body `tool_body` frame by frame, or NULL. */
+CN_API cn_status cn_server_submit(cn_server *server, uint32_t scene, uint32_t steps, uint32_t tool_body,
+                                  const float *tool_targets, uint64_t *out_request);
+/* Launches one tick (asynchronous on `stream`), then waits for the tick before it. */
+CN_API cn_status cn_server_tick(cn_server *server, void *stream, uint32_t *out_stepped_scenes);
+/* Ticks until no request is pending and every tick has finished. */
+CN_API cn_status cn_server_drain(cn_server *server, void *stream);
+CN_API cn_status cn_server_poll(cn_server *server, cn_request_done *out, uint32_t capacity, uint32_t *out_count);
+CN_API cn_status cn_server_get_stats(cn_server *server, cn_server_stats *out);
+CN_API cn_status cn_server_read_particles(cn_server *server, uint32_t scene, float *positions_inv_mass,
+                                          float *velocities, uint32_t count);
+
 /* Allocation-free broadphase sort (no counterpart in the reference).
  * For callers that must not allocate device memory while they run -- engines whose device memory
  * belongs to their own pool, frame loops that cannot afford the allocator's implicit

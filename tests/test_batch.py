@@ -1,0 +1,142 @@
+"""Batched and served forms: scenes in one pool, stepped together, equal scenes stepped alone.
+
+The per-element arithmetic of a batch tick is that of a solver of its own (the scene's indices
+are only rebased), so every comparison below is bit for bit.
+"""
+import numpy as np
+import pytest
+
+from cn_physics import Batch, Server, Solver, batch_desc, serving
+from conftest import has_gpu
+
+DT = 1.0 / 60.0
+
+
+def small_pool(n=4, seed=3):
+    return [serving.tissue_scene(dims, seed=seed + k) for k, dims in
+            enumerate([(6, 4, 6), (9, 3, 5), (4, 4, 4), (7, 5, 8), (5, 6, 3), (8, 4, 6)][:n])]
+
+
+def targets_for(scene, frames, seed):
+    rng = np.random.default_rng(seed)
+    pose = scene.tool_pose.copy()
+    out = []
+    for _ in range(frames):
+        pose = pose + rng.normal(0.0, 0.002, 3).astype(np.float32)
+        pose[1] = max(pose[1] - 0.002, 0.0)   # press down into the tissue
+        out.append(np.concatenate([pose, [0.0, 0.0, 0.7071068, 0.7071068]]).astype(np.float32))
+    return np.stack(out)
+
+
+def own_solver_run(scene, targets):
+    sv = Solver(serving.serving_solver_desc())
+    sv.sync_world(scene.world.soa())
+    for tg in targets:
+        sv.set_kinematic_target(scene.tool, tg[:3], tg[3:])
+        sv.step(DT)
+    x, v, _ = sv.read_particles()
+    sv.close()
+    return x, v
+
+
+def test_pool_generator_counts():
+    pool = serving.tissue_pool(6, seed=1, tet_range=(2000, 8000))
+    for sc in pool:
+        cx, cy, cz = sc.cells
+        assert sc.tets == 5 * cx * cy * cz and sc.particles == (cx + 1) * (cy + 1) * (cz + 1)
+        assert 1000 <= sc.tets <= 12000
+    req = serving.poisson_requests(pool, steps_per_second=20000.0, duration_s=0.5, seed=2)
+    frames = sum(r.steps for r in req)
+    assert 8000 < frames < 12000 and all(1 <= r.steps <= 8 for r in req)
+    assert all(a.arrival <= b.arrival for a, b in zip(req, req[1:]))
+
+
+def test_batch_desc_defaults():
+    d = batch_desc()
+    assert d.max_scenes == 1024 and d.tile_elements == 256 and d.blocks_per_sm == 8
+    assert d.solver.default_iterations == 20 and d.solver.enable_blocking_readback == 0
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device error path")
+def test_batch_create_fails_without_device():
+    from cn_physics import CNError
+    with pytest.raises(CNError):
+        Batch(batch_desc(serving.serving_solver_desc()))
+
+
+@pytest.mark.gpu
+def test_batched_scene_equals_its_own_solver_and_is_independent_of_the_mix():
+    pool = small_pool(4)
+    frames = 6
+    tg = [targets_for(sc, frames, seed=10 + k) for k, sc in enumerate(pool)]
+    ref = [own_solver_run(sc, tg[k]) for k, sc in enumerate(pool)]
+    b = Batch(batch_desc(serving.serving_solver_desc(), memory_budget_bytes=1 << 30, particle_capacity=20000))
+    ids = [b.add_scene(sc.world.soa()) for sc in pool]
+    # scenes 0 and 2 stepped every tick; 1 and 3 only on some ticks (they catch up afterwards)
+    done = [0] * len(pool)
+    schedule = [[0, 1, 2, 3], [0, 2], [0, 2, 3], [0, 1, 2], [0, 2], [0, 1, 2, 3], [1, 3], [1, 3], [1, 3], [1]]
+    for tick in schedule:
+        step = [k for k in tick if done[k] < frames]
+        for k in step:
+            t = tg[k][done[k]]
+            b.set_kinematic_target(ids[k], pool[k].tool, t[:3], t[3:])
+        b.step([ids[k] for k in step], DT)
+        for k in step:
+            done[k] += 1
+    assert done == [frames] * len(pool)
+    for k in range(len(pool)):
+        x, v = b.read_particles(ids[k])
+        assert np.array_equal(x, ref[k][0]) and np.array_equal(v, ref[k][1]), f"scene {k}"
+    b.close()
+
+
+@pytest.mark.gpu
+def test_autotune_keeps_state_and_results():
+    pool = small_pool(3)
+    tg = [targets_for(sc, 3, seed=20 + k) for k, sc in enumerate(pool)]
+    ref = [own_solver_run(sc, tg[k]) for k, sc in enumerate(pool)]
+    b = Batch(batch_desc(serving.serving_solver_desc(), memory_budget_bytes=1 << 30, particle_capacity=10000))
+    ids = [b.add_scene(sc.world.soa()) for sc in pool]
+    tune = b.autotune(ids, DT)
+    assert tune["candidates"] and tune["tick_ms"] > 0
+    for f in range(3):
+        for k in range(len(pool)):
+            b.set_kinematic_target(ids[k], pool[k].tool, tg[k][f][:3], tg[k][f][3:])
+        b.step(ids, DT)
+    for k in range(len(pool)):
+        x, v = b.read_particles(ids[k])
+        assert np.array_equal(x, ref[k][0]) and np.array_equal(v, ref[k][1])
+    b.close()
+
+
+@pytest.mark.gpu
+def test_server_results_equal_alone_and_in_the_mix_with_evictions():
+    pool = small_pool(6)
+    # a budget that holds two or three of the six scenes: admissions must evict idle scenes
+    # (the batch charges 120 + 4 x 72 B per particle, 84 B per edge, 132 B per tet, 272 B per
+    # body and 216 B per collider)
+    def scene_bytes(sc):
+        c = sc.world.counts()
+        return c["particles"] * (120 + 288) + c["edges"] * 84 + c["tets"] * 132 + 2 * 272 + 2 * 216
+    largest = max(scene_bytes(sc) for sc in pool)
+    b = Batch(batch_desc(serving.serving_solver_desc(), memory_budget_bytes=int(2.5 * largest),
+                         particle_capacity=20000))
+    srv = Server(b, DT)
+    ids = [srv.register(sc.world.soa()) for sc in pool]
+    req = serving.poisson_requests(pool, steps_per_second=600.0, duration_s=0.15, seed=5)
+    per_scene = {k: [] for k in range(len(pool))}
+    for r in req:
+        per_scene[r.scene].append(r.targets)
+    out = serving.serve(srv, pool, ids, req)
+    st = out["stats"]
+    assert out["requests"] == len(req) and st["pending"] == 0 and st["completed"] == len(req)
+    assert st["evictions"] > 0, st
+    for k, sc in enumerate(pool):
+        if not per_scene[k]:
+            continue
+        tg = np.concatenate(per_scene[k])
+        x_ref, v_ref = own_solver_run(sc, tg)
+        x, v = srv.read_particles(ids[k])
+        assert np.array_equal(x, x_ref) and np.array_equal(v, v_ref), f"scene {k}"
+    srv.close()
+    b.close()
