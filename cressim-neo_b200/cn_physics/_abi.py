@@ -202,6 +202,11 @@ class ServerStats(C.Structure):
                 ("registered_scenes", u32), ("gpu_ms", C.c_double), ("tick_ms_p50", f32), ("tick_ms_p99", f32)]
 
 
+class DiffDesc(C.Structure):
+    _fields_ = [("gravity", f32 * 3), ("substeps", u32), ("iterations", u32), ("substep_dt", f32),
+                ("relaxation", f32), ("checkpoint_interval", u32), ("precision", u32), ("reserved", u32 * 4)]
+
+
 SIGNATURES = [
     ("cn_last_error", C.c_char_p, []),
     ("cn_version", C.c_char_p, []),
@@ -257,6 +262,13 @@ SIGNATURES = [
     ("cn_batch_get_stats", C.c_int, [C.c_void_p, C.POINTER(BatchStats)]),
     ("cn_batch_set_schedule", C.c_int, [C.c_void_p, u32, u32]),
     ("cn_batch_autotune", C.c_int, [C.c_void_p, P_u32, u32, f32, C.POINTER(BatchTuning)]),
+    ("cn_diff_desc_defaults", None, [C.POINTER(DiffDesc)]),
+    ("cn_diff_create", C.c_int, [C.POINTER(DiffDesc), C.c_int, C.POINTER(C.c_void_p)]),
+    ("cn_diff_destroy", None, [C.c_void_p]),
+    ("cn_diff_set_scene", C.c_int, [C.c_void_p, C.POINTER(WorldSoA)]),
+    ("cn_diff_forward", C.c_int, [C.c_void_p] + [C.c_void_p] * 6),
+    ("cn_diff_backward", C.c_int, [C.c_void_p] + [C.c_void_p] * 6),
+    ("cn_diff_memory", C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     ("cn_server_desc_defaults", None, [C.POINTER(ServerDesc)]),
     ("cn_server_create", C.c_int, [C.c_void_p, C.POINTER(ServerDesc), u32, C.POINTER(C.c_void_p)]),
     ("cn_server_destroy", None, [C.c_void_p]),

@@ -587,6 +587,39 @@ CN_API cn_status cn_server_get_stats(cn_server *server, cn_server_stats *out);
 CN_API cn_status cn_server_read_particles(cn_server *server, uint32_t scene, float *positions_inv_mass,
                                           float *velocities, uint32_t count);
 
+/* ------------------------------------------------------------------------ */
+/* Differentiable XPBD rollout (no counterpart in the reference).  The soft   */
+/* substep (predict, Jacobi edge + tet iterations, velocity update) of a      */
+/* scene without colliders, forward with checkpoints every                    */
+/* checkpoint_interval substeps and a hand-written adjoint giving d loss /    */
+/* d (per-tet compliance, initial positions, initial velocities).  Buffers are*/
+/* device pointers of float (precision 4) or double (precision 8); positions  */
+/* and velocities are 4 values per particle (xyz + invMass / unused).         */
+/* ------------------------------------------------------------------------ */
+typedef struct cn_diff cn_diff;
+typedef struct cn_diff_desc {
+    float gravity[3];
+    uint32_t substeps;              /* substeps of one rollout */
+    uint32_t iterations;            /* Jacobi iterations per substep */
+    float substep_dt;
+    float relaxation;               /* softInternalRelaxation (0.2) */
+    uint32_t checkpoint_interval;   /* substeps between saved (x, v) states */
+    uint32_t precision;             /* 4 = float, 8 = double */
+    uint32_t reserved[4];
+} cn_diff_desc;
+CN_API void cn_diff_desc_defaults(cn_diff_desc *desc);
+CN_API cn_status cn_diff_create(const cn_diff_desc *desc, int cuda_device, cn_diff **out);
+CN_API void cn_diff_destroy(cn_diff *diff);
+CN_API cn_status cn_diff_set_scene(cn_diff *diff, const cn_world_soa *world);
+CN_API cn_status cn_diff_forward(cn_diff *diff, const void *tet_compliance, const void *x0, const void *v0,
+                                 void *x_out, void *v_out, void *stream);
+/* Adjoint of the last forward: grad_x_out / grad_v_out (either may be NULL = zero) in, the
+ * gradients with respect to the forward's inputs out (grad_x0 / grad_v0 may be NULL). */
+CN_API cn_status cn_diff_backward(cn_diff *diff, const void *grad_x_out, const void *grad_v_out,
+                                  void *grad_tet_compliance, void *grad_x0, void *grad_v0, void *stream);
+/* Device bytes of the state the adjoint keeps (checkpoints, one segment, one substep). */
+CN_API cn_status cn_diff_memory(cn_diff *diff, uint64_t *bytes);
+
 /* Allocation-free broadphase sort (no counterpart in the reference).
  * For callers that must not allocate device memory while they run -- engines whose device memory
  * belongs to their own pool, frame loops that cannot afford the allocator's implicit

@@ -37,11 +37,11 @@ def test_struct_sizes_match_header():
     src = r'''
 #include <stdio.h>
 #include "cn_physics.h"
-int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(cn_solver_desc),
+int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(cn_solver_desc),
  sizeof(cn_world_soa), sizeof(cn_soft_body_grid_desc), sizeof(cn_fluid_grid_desc), sizeof(cn_cloth_grid_desc),
  sizeof(cn_strand_desc), sizeof(cn_rigid_body_desc), sizeof(cn_collider_desc), sizeof(cn_meta), sizeof(cn_scene_view),
  sizeof(cn_batch_desc), sizeof(cn_batch_stats), sizeof(cn_batch_tuning), sizeof(cn_server_desc),
- sizeof(cn_request_done), sizeof(cn_server_stats)); return 0;}
+ sizeof(cn_request_done), sizeof(cn_server_stats), sizeof(cn_diff_desc)); return 0;}
 '''
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "s.c")
@@ -53,7 +53,7 @@ int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %
     want = [C.sizeof(t) for t in (_abi.SolverDesc, _abi.WorldSoA, _abi.SoftBodyGridDesc, _abi.FluidGridDesc,
                                   _abi.ClothGridDesc, _abi.StrandDesc, _abi.RigidBodyDesc, _abi.ColliderDesc,
                                   _abi.Meta, _abi.SceneView, _abi.BatchDesc, _abi.BatchStats, _abi.BatchTuning,
-                                  _abi.ServerDesc, _abi.RequestDone, _abi.ServerStats)]
+                                  _abi.ServerDesc, _abi.RequestDone, _abi.ServerStats, _abi.DiffDesc)]
     assert got == want
 
 
