@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--serve-scenes", type=int, default=512, help="tissue scenes of the served/batched pool (0: skip)")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="Poisson arrival window of the served run")
     ap.add_argument("--serve-rate", type=float, default=20000.0, help="offered frames per second")
+    ap.add_argument("--no-diff", action="store_true", help="skip the differentiable-rollout measurement")
     ap.add_argument("--serve-substeps", type=int, default=1)
     ap.add_argument("--serve-iterations", type=int, default=20)
     return ap.parse_args()
@@ -302,6 +303,8 @@ def run_ours(args):
     }
     if args.serve_scenes > 0:
         line["served"] = run_served(args, stream, sh)
+    if not args.no_diff:
+        line["differentiation"] = run_diff(stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(budget_s=15.0)
     if world > 1:
@@ -405,6 +408,111 @@ def run_served(args, stream, sh) -> dict:
                    "admissions_during_run": st["admissions"] - prefetched, "evictions": st["evictions"],
                    "budget_bytes": bstats["budget_bytes"], "budget_used_bytes": bstats["budget_used_bytes"]},
     }
+
+
+def _diff_block(dims, spacing=0.1, base=1e-11, seed=0):
+    """Pinned soft block whose per-tet compliances (log-normal, sigma 0.5) carry its stiffness."""
+    from cn_physics import World
+    rx, ry, rz = dims
+    w = World()
+    size = ((rx - 1.25) * spacing, (ry - 1.25) * spacing, (rz - 1.25) * spacing)
+    pinned = [x * ry * rz + z for x in range(rx) for z in range(rz)]
+    w.add_soft_body_grid(size, spacing, position=(0.0, size[1] * 0.5, 0.0), radius=0.4 * spacing,
+                         edge_compliance=1e-4, volume_compliance=base, static_particles=pinned)
+    w.soa()
+    comp = w.array("tets").view(np.float32)[:, 5]
+    comp[:] = (base * np.random.default_rng(seed).lognormal(0.0, 0.5, comp.shape[0])).astype(np.float32)
+    return w
+
+
+def run_diff(stream) -> dict:
+    """Differentiation: a 28x14x28-vertex block (47,385 tets), 32 substeps x 20 iterations,
+    surface-vertex MSE against a target rolled out with log-normal (sigma 0.3) per-tet stiffness;
+    gradient with respect to per-tet compliance and initial velocities, checkpoint every 8
+    substeps.  The adjoint is checked against FP64 central differences (eps 1e-6) on a
+    9x8x8-vertex (1,960-tet) instance."""
+    import torch
+    from cn_physics import diff
+
+    def inputs(w, dtype):
+        x0 = torch.as_tensor(w.positions().copy(), device="cuda", dtype=dtype)
+        comp = torch.as_tensor(w.array("tets").view(np.float32)[:, 5].copy(), device="cuda", dtype=dtype)
+        v = np.zeros((x0.shape[0], 4))
+        v[:, :3] = np.random.default_rng(1).normal(0.0, 0.05, (x0.shape[0], 3))
+        v0 = torch.as_tensor(v, device="cuda", dtype=dtype)
+        v0[x0[:, 3] <= 0] = 0
+        return comp, x0, v0
+
+    def loss_grad(r, comp, x0, v0, target, surf):
+        out = torch.empty_like(x0)
+        r.forward(comp, x0, v0, out)
+        d = out[surf, :3] - target[surf, :3]
+        g = torch.zeros_like(out)
+        g[surf, :3] = 2.0 * d / d.numel()
+        gc, gv = torch.zeros_like(comp), torch.zeros_like(v0)
+        r.backward(g, None, gc, None, gv)
+        return float((d * d).mean()), gc, gv
+
+    dims = (28, 14, 28)
+    w = _diff_block(dims)
+    surf = torch.as_tensor(diff.lattice_surface(dims), device="cuda")
+    kw = dict(substeps=32, iterations=20, substep_dt=1.0 / 480.0, checkpoint_interval=8)
+    r = diff.Rollout(w, **kw)
+    comp, x0, v0 = inputs(w, torch.float32)
+    true = comp * torch.as_tensor(np.random.default_rng(2).lognormal(0.0, 0.3, comp.shape[0]), device="cuda",
+                                  dtype=torch.float32)
+    target = torch.empty_like(x0)
+    r.forward(true, x0, v0, target)
+    loss_grad(r, comp, x0, v0, target, surf)  # warm-up
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    out = torch.empty_like(x0)
+    g = torch.zeros_like(x0)
+    g[surf, :3] = 1e-3
+    gc, gv = torch.zeros_like(comp), torch.zeros_like(v0)
+    ev[0].record(stream)
+    r.forward(comp, x0, v0, out)
+    ev[1].record(stream)
+    r.backward(g, None, gc, None, gv)
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    fwd_ms, bwd_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    kept = r.memory_bytes()
+    n, t = w.counts()["particles"], w.counts()["tets"]
+    e = w.counts()["edges"]
+    tape = 32 * 20 * (2 * n * 16 + (e + t) * 4) + 32 * 2 * n * 16   # every iteration state of every substep
+    r.close()
+
+    # FD check on the small instance in FP64
+    sd = (9, 8, 8)
+    ws = _diff_block(sd)
+    ssurf = torch.as_tensor(diff.lattice_surface(sd), device="cuda")
+    kws = dict(substeps=32, iterations=10, substep_dt=1.0 / 480.0, checkpoint_interval=8)
+    r64 = diff.Rollout(ws, precision=8, **kws)
+    c64, x64, v64 = inputs(ws, torch.float64)
+    rng = np.random.default_rng(7)
+    t64 = torch.empty_like(x64)
+    r64.forward(c64 * torch.as_tensor(rng.lognormal(0.0, 0.3, c64.shape[0]), device="cuda"), x64, v64, t64)
+    _, g64, _ = loss_grad(r64, c64, x64, v64, t64, ssurf)
+    u = torch.as_tensor(rng.normal(0.0, 1.0, c64.shape[0]), device="cuda") * c64
+    eps = 1e-6
+
+    def L(c):
+        o = torch.empty_like(x64)
+        r64.forward(c, x64, v64, o)
+        d = o[ssurf, :3] - t64[ssurf, :3]
+        return float((d * d).mean())
+    fd = (L(c64 + eps * u) - L(c64 - eps * u)) / (2 * eps)
+    an = float((g64 * u).sum())
+    r64.close()
+    return {"workload": f"XPBD block {dims[0]}x{dims[1]}x{dims[2]} vertices ({t} tets, {n} particles), 32 substeps x "
+                        f"20 iterations, checkpoint every 8 substeps, surface MSE vs a log-normal (sigma 0.3) "
+                        f"stiffness target; gradients w.r.t. per-tet compliance and initial velocities",
+            "forward_ms": round(fwd_ms, 3), "backward_ms": round(bwd_ms, 3),
+            "particle_substeps_per_s_forward": round(n * 32 / (fwd_ms / 1e3), 1),
+            "adjoint_state_bytes": kept, "full_tape_bytes": tape,
+            "fd_check": {"instance": "9x8x8 vertices (1,960 tets), FP64, eps 1e-6, random log-space direction",
+                         "adjoint": an, "central_difference": fd, "relative_error": abs(an - fd) / abs(fd)}}
 
 
 def solver_neighbor_mean(solver) -> tuple:
