@@ -157,7 +157,8 @@ struct Scene {
     // ---- fluid (cell order) ----
     uint32_t hasFluid = 0;
     float4 *Xs = nullptr;             // x at the sorted slot (w = invMass)
-    float4 *P = nullptr;              // x + accumulated delta, w = invMass
+    float4 *P = nullptr;              // x + accumulated delta, w = tag word (fluid bit, material, group)
+    float4 *Pb = nullptr;             // second position buffer (odd iterations) when x is fixed over them
     float4 *Da = nullptr, *Db = nullptr; // accumulated delta ping-pong
     float4 *Cs = nullptr;             // surface normal xyz, density constraint w
     float4 *Dx = nullptr;             // packed delta + interaction weight (last iteration)
@@ -216,6 +217,8 @@ void launchParticleCandidates(const Scene &s, uint32_t *scanTmp, size_t scanTmpB
 void launchFluidIteration(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
                           cudaStream_t st);
 void launchFluidGather(const Scene &s, uint32_t iter, cudaStream_t st);
+// False when the positions are double-buffered: the gather then runs at the first iteration only.
+bool fluidGatherEachIteration(const Scene &s);
 void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter, cudaStream_t st);
 void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
                                 cudaStream_t st);

@@ -590,8 +590,10 @@ __global__ void __launch_bounds__(kThreads) k_particleCandidates(Scene s, const 
 // Fluid solve (cell order).
 // ------------------------------------------------------------------------------------------
 // Position of this fluid iteration: x + accumulated delta (iteration > 0), in sorted slots.
+// With `P2` (double-buffered positions, see k_fluidDeltaApplyClamp) the first iteration writes
+// both buffers, so the tags of slots the iterations never rewrite are valid in each.
 __global__ void __launch_bounds__(kThreads) k_fluidGather(Scene s, float4 *Xs, const float4 *Dcur,
-                                                          uint32_t iter)
+                                                          uint32_t iter, float4 *P2)
 {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     float largest = 0.0f;
@@ -602,6 +604,7 @@ __global__ void __launch_bounds__(kThreads) k_fluidGather(Scene s, float4 *Xs, c
         const uint32_t tag = (info & 0x7fffffffu) | ((info & kFluidBit) && xp.w > kEps ? kFluidBit : 0u);
         Xs[slot] = xp;
         s.P[slot] = mk4(xyz(xp) + d, __uint_as_float(tag));
+        if (P2) P2[slot] = mk4(xyz(xp) + d, __uint_as_float(tag));
         if (info & kFluidBit) largest = sqrtf(dot(d, d));
     }
     // largest accumulated delta of this iteration: validity of the superset lists
@@ -854,9 +857,15 @@ __global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Con
 // physics_fluid_compute_delta_positions.cs.hlsl:27-157, physics_fluid_apply_delta_positions.cs.hlsl:11-31,
 // physics_fluid_clamp_boundary.cs.hlsl:23-80.  Reads the accumulated delta of iteration k (Dcur)
 // and writes that of iteration k+1 (Dnext), so the neighbours' deltas stay those of iteration k.
+//
+// With `Pnext` (fluid x fixed over the iterations: no particle-particle contacts) the kernel also
+// writes the next iteration's position x + accumulated delta -- what k_fluidGather would compute
+// -- into the other position buffer, and records the largest accumulated delta for the superset
+// test of the next iteration, so the gather runs once per substep.
 __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Config cfg, const float4 *Xs,
                                                                    const float4 *Dcur, float4 *Dnext,
-                                                                   uint32_t iter, float dt, bool writeDx)
+                                                                   uint32_t iter, float dt, bool writeDx,
+                                                                   float4 *Pnext)
 {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= s.N) return;
@@ -981,7 +990,18 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
             if (!changed) break;
         }
     }
-    Dnext[slot] = mk4(cur - base, 0.0f);
+    const f3 dn = cur - base;
+    Dnext[slot] = mk4(dn, 0.0f);
+    if (Pnext) {
+        Pnext[slot] = mk4(base + dn, self.w);
+        const uint32_t next = iter + 1u;
+        if (next < kMaxTrackedIterations) {
+            // lanes that returned early are not in the mask; diverged groups reduce separately
+            const unsigned mask = __activemask();
+            const uint32_t big = __reduce_max_sync(mask, __float_as_uint(sqrtf(dot(dn, dn))));
+            if (int(threadIdx.x & 31u) == __ffs(mask) - 1 && big > 0u) atomicMax(&s.fluidMaxDelta[next], big);
+        }
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1876,12 +1896,23 @@ void launchParticleCandidates(const Scene &s, uint32_t *scanTmp, size_t, cudaStr
     k_particleCandidates<true><<<blocksFor(s.N), kThreads, 0, st>>>(s, total);
 }
 
+// Positions of iteration k: buffer A (s.P) for even k, B (s.Pb) for odd k when double-buffered.
+inline Scene withPositions(const Scene &s, uint32_t iter)
+{
+    Scene c = s;
+    if (s.Pb && (iter & 1u)) c.P = s.Pb;
+    return c;
+}
+
 void launchFluidGather(const Scene &s, uint32_t iter, cudaStream_t st)
 {
     if (s.N == 0) return;
     const float4 *Dcur = (iter & 1u) ? s.Db : s.Da;
-    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, Dcur, iter);
+    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), s.Xs, Dcur, iter,
+                                                       (s.Pb && iter == 0) ? s.Pb : nullptr);
 }
+
+bool fluidGatherEachIteration(const Scene &s) { return s.Pb == nullptr; }
 
 bool fluidListsInterleaved() { return kInterleavedLists; }
 
@@ -1889,7 +1920,7 @@ void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter,
 {
     if (s.N == 0) return;
     const uint32_t mode = s.sup == nullptr ? 0u : (iter == 0 ? 1u : 2u);
-    k_fluidNeighborsDensity<<<blocksFor(s.N), kThreads, 0, st>>>(s, c, true, mode, iter);
+    k_fluidNeighborsDensity<<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), c, true, mode, iter);
 }
 
 void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
@@ -1898,13 +1929,15 @@ void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const C
     if (s.N == 0) return;
     const float4 *Dcur = (iter & 1u) ? s.Db : s.Da;
     float4 *Dnext = (iter & 1u) ? s.Da : s.Db;
-    k_fluidDeltaApplyClamp<<<blocksFor(s.N), kThreads, 0, st>>>(s, c, s.Xs, Dcur, Dnext, iter, dt, writeDebug);
+    float4 *Pnext = s.Pb ? ((iter & 1u) ? s.P : s.Pb) : nullptr;
+    k_fluidDeltaApplyClamp<<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), c, s.Xs, Dcur, Dnext, iter,
+                                                                dt, writeDebug, Pnext);
 }
 
 void launchFluidIteration(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
                           cudaStream_t st)
 {
-    launchFluidGather(s, iter, st);
+    if (iter == 0 || fluidGatherEachIteration(s)) launchFluidGather(s, iter, st);
     launchFluidNeighborsDensity(s, c, iter, st);
     launchFluidDeltaApplyClamp(s, iter, dt, c, writeDebug, st);
 }
@@ -1913,7 +1946,7 @@ void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)
 {
     if (s.N == 0) return;
     // Positions after the velocity update; the accumulated delta was folded into x.
-    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, s.Da, 0u);
+    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, s.Da, 0u, nullptr);
     Config dummy{};
     k_fluidNeighborsDensity<<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u, 0u);
 }

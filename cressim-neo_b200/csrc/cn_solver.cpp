@@ -220,6 +220,7 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
             s.supCap = 160u;
             s.sup = a.take<uint32_t>(size_t(N) * s.supCap);
             s.supCount = a.take<uint32_t>(N);
+            s.Pb = a.take<float4>(N);
         }
         s.maxNbr = sv->desc.max_fluid_neighborhood;
         s.nbr = a.take<uint32_t>(std::max<size_t>(size_t(N) * s.maxNbr, 1));
@@ -290,7 +291,8 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             const bool runRigid = sv->rigidPossible && it < sv->contactIt;
             if (!runFluid && !runSoft && !runPP && !runRigid) break; // remaining iterations are empty
             if (runFluid) {
-                probe(sv, "fluid_gather", st, [&] { cn::launchFluidGather(s, it, st); });
+                if (it == 0 || cn::fluidGatherEachIteration(s))
+                    probe(sv, "fluid_gather", st, [&] { cn::launchFluidGather(s, it, st); });
                 // the first iteration of a substep also records the superset lists when they are on
                 probe(sv, (it == 0 && s.sup) ? "fluid_neighbors_superset" : "fluid_neighbors_density", st,
                       [&] { cn::launchFluidNeighborsDensity(s, c, it, st); });
