@@ -712,8 +712,9 @@ __device__ __forceinline__ bool neighborAllowed(const Scene &s, uint32_t tag, ui
 //         neighbour of this iteration is in the superset, and filtering it in order yields exactly
 //         the list the cell walk would build.  Otherwise (or if this particle's superset
 //         overflowed) the particle walks the cells.
-__global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Config cfg, bool density,
-                                                                    uint32_t mode, uint32_t iter)
+// One instantiation per mode, so the cell walk's register needs do not set the filter's occupancy.
+template <uint32_t mode>
+__global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighborsDensity(Scene s, Config cfg, bool density, uint32_t iter)
 {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= s.N) return;
@@ -752,26 +753,28 @@ __global__ void __launch_bounds__(kThreads) k_fluidNeighborsDensity(Scene s, Con
     if (useSuperset) {
         const uint32_t n = s.supCount[slot];
         const uint32_t *sup = kInterleavedLists ? s.sup + slot : s.sup + size_t(slot) * s.supCap;
-        uint32_t cN = n > 0 ? sup[0] : 0u;
-        uint32_t cNN = n > 1 ? sup[lstr] : 0u;
-        float4 qN = n > 0 ? ld4(&s.P[cN]) : make_float4(0.f, 0.f, 0.f, 0.f);
-        for (uint32_t k = 0; k < n; ++k) {
-            const uint32_t c = cN;
-            const float4 q = qN;
-            if (k + 1 < n) {
-                cN = cNN;
-                if (k + 2 < n) cNN = sup[(k + 2) * lstr];
-                qN = ld4(&s.P[cN]);
-            }
-            const f3 delta = sp - xyz(q);
-            const float d2 = dot(delta, delta);
-            if (d2 >= h2) continue;
-            if (count >= maxN) { truncated = 1; continue; }
-            out[count++ * lstr] = c;
-            if (density) {
-                const float dist = sqrtf(d2);
-                rho += spikyWk(dist, h, kW);
-                if (st > kEps) normal += spikyGradK(delta, dist, h, kW);
+        // Four entries in flight: their list words, then their positions, load before any is
+        // used (the loop is bound by gather latency); they are consumed in list order.
+        for (uint32_t k = 0; k < n; k += 4u) {
+            uint32_t cc[4];
+            float4 qq[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) cc[j] = (k + j < n) ? sup[(k + j) * lstr] : slot;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) qq[j] = ld4(&s.P[cc[j]]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (k + j >= n) break;
+                const f3 delta = sp - xyz(qq[j]);
+                const float d2 = dot(delta, delta);
+                if (d2 >= h2) continue;
+                if (count >= maxN) { truncated = 1; continue; }
+                out[count++ * lstr] = cc[j];
+                if (density) {
+                    const float dist = sqrtf(d2);
+                    rho += spikyWk(dist, h, kW);
+                    if (st > kEps) normal += spikyGradK(delta, dist, h, kW);
+                }
             }
         }
     } else {
@@ -1919,8 +1922,13 @@ bool fluidListsInterleaved() { return kInterleavedLists; }
 void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter, cudaStream_t st)
 {
     if (s.N == 0) return;
-    const uint32_t mode = s.sup == nullptr ? 0u : (iter == 0 ? 1u : 2u);
-    k_fluidNeighborsDensity<<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), c, true, mode, iter);
+    const Scene sp = withPositions(s, iter);
+    if (s.sup == nullptr)
+        k_fluidNeighborsDensity<0u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter);
+    else if (iter == 0)
+        k_fluidNeighborsDensity<1u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter);
+    else
+        k_fluidNeighborsDensity<2u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter);
 }
 
 void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
@@ -1948,7 +1956,7 @@ void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)
     // Positions after the velocity update; the accumulated delta was folded into x.
     k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, s.Da, 0u, nullptr);
     Config dummy{};
-    k_fluidNeighborsDensity<<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u, 0u);
+    k_fluidNeighborsDensity<0u><<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u);
 }
 
 void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st)
