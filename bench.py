@@ -301,9 +301,11 @@ def run_ours(args):
         "clocks": clk,
         "meta_status": meta["status"],
     }
-    if args.serve_scenes > 0:
+    # the batched / served and differentiable forms are single-GPU workloads of their own: they
+    # run once, in single-GPU runs, rather than on every rank of a scaling run
+    if world == 1 and args.serve_scenes > 0:
         line["served"] = run_served(args, stream, sh)
-    if not args.no_diff:
+    if world == 1 and not args.no_diff:
         line["differentiation"] = run_diff(stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(budget_s=15.0)
