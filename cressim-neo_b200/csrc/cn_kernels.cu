@@ -713,8 +713,11 @@ __device__ __forceinline__ bool neighborAllowed(const Scene &s, uint32_t tag, ui
 //         the list the cell walk would build.  Otherwise (or if this particle's superset
 //         overflowed) the particle walks the cells.
 // One instantiation per mode, so the cell walk's register needs do not set the filter's occupancy.
+// With `Dk` (the accumulated delta this iteration starts from) the density constraint is also
+// stored in Dk.w, so the delta kernel reads a neighbour's delta and constraint in one load.
 template <uint32_t mode>
-__global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighborsDensity(Scene s, Config cfg, bool density, uint32_t iter)
+__global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighborsDensity(Scene s, Config cfg, bool density,
+                                                                                    uint32_t iter, float4 *Dk)
 {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= s.N) return;
@@ -854,6 +857,7 @@ __global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighbors
     } else {
         s.Cs[slot] = make_float4(0.f, 0.f, 0.f, C);
     }
+    if (Dk) reinterpret_cast<float *>(Dk + slot)[3] = C;
 }
 
 // Position delta, apply and boundary clamp.
@@ -901,24 +905,23 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
         const size_t lstr = kInterleavedLists ? size_t(s.N) : 1u;
         // Software-pipelined over the list: the next neighbour's slot, position word, constraint
         // and accumulated delta are in flight while the current pair term is computed.
-        const bool relLoads = needRel && iter > 0;
+        // A neighbour's accumulated delta (xyz, used from the second iteration on) and density
+        // constraint (w, stored there by the density kernel) come in one load.
         const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
         uint32_t cN = cnt > 0 ? lst[0] : 0u;
         uint32_t cNN = cnt > 1 ? lst[lstr] : 0u;
         float4 npN = cnt > 0 ? ld4(&s.P[cN]) : zero4;
-        float cwN = cnt > 0 ? __ldg(&s.Cs[cN].w) : 0.0f;
-        float4 dN = (cnt > 0 && relLoads) ? ld4(&Dcur[cN]) : zero4;
+        float4 dN = cnt > 0 ? ld4(&Dcur[cN]) : zero4;
         for (uint32_t k = 0; k < cnt; ++k) {
             const uint32_t c = cN;
             const float4 np = npN;
-            const float ncw = cwN;
+            const float ncw = dN.w;
             const float4 nd4 = dN;
             if (k + 1 < cnt) {
                 cN = cNN;
                 if (k + 2 < cnt) cNN = lst[(k + 2) * lstr];
                 npN = ld4(&s.P[cN]);
-                cwN = __ldg(&s.Cs[cN].w);
-                if (relLoads) dN = ld4(&Dcur[cN]);
+                dN = ld4(&Dcur[cN]);
             }
             const uint32_t tag = __float_as_uint(np.w);
             if ((tag & kFluidBit) == 0u) continue;
@@ -1923,12 +1926,13 @@ void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter,
 {
     if (s.N == 0) return;
     const Scene sp = withPositions(s, iter);
+    float4 *Dk = (iter & 1u) ? s.Db : s.Da;
     if (s.sup == nullptr)
-        k_fluidNeighborsDensity<0u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter);
+        k_fluidNeighborsDensity<0u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter, Dk);
     else if (iter == 0)
-        k_fluidNeighborsDensity<1u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter);
+        k_fluidNeighborsDensity<1u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter, Dk);
     else
-        k_fluidNeighborsDensity<2u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter);
+        k_fluidNeighborsDensity<2u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter, Dk);
 }
 
 void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
@@ -1956,7 +1960,7 @@ void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)
     // Positions after the velocity update; the accumulated delta was folded into x.
     k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, s.Da, 0u, nullptr);
     Config dummy{};
-    k_fluidNeighborsDensity<0u><<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u);
+    k_fluidNeighborsDensity<0u><<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u, nullptr);
 }
 
 void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st)
