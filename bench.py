@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="Poisson arrival window of the served run")
     ap.add_argument("--serve-rate", type=float, default=20000.0, help="offered frames per second")
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiable-rollout measurement")
+    ap.add_argument("--no-configs", action="store_true", help="skip the XPBD cube / mixed scene measurements")
     ap.add_argument("--serve-substeps", type=int, default=1)
     ap.add_argument("--serve-iterations", type=int, default=20)
     return ap.parse_args()
@@ -307,6 +308,8 @@ def run_ours(args):
         line["served"] = run_served(args, stream, sh)
     if world == 1 and not args.no_diff:
         line["differentiation"] = run_diff(stream)
+    if world == 1 and not args.no_configs:
+        line["other_configs"] = run_other_configs(stream, sh, cpu=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(budget_s=15.0)
     if world > 1:
@@ -410,6 +413,78 @@ def run_served(args, stream, sh) -> dict:
                    "admissions_during_run": st["admissions"] - prefetched, "evictions": st["evictions"],
                    "budget_bytes": bstats["budget_bytes"], "budget_used_bytes": bstats["budget_used_bytes"]},
     }
+
+
+def run_other_configs(stream, sh, cpu: bool = True) -> dict:
+    """The plain XPBD cube (16^3 vertices, 16,875 tets, 10 substeps x 20 iterations, ground) and the
+    mixed surgical scene (60x30x60 tissue, 256^2 cloth, 64 strands of 129, 64^3 fluid, kinematic
+    capsule on a seeded path, 8 substeps), each timed over frames replayed from its CUDA graph;
+    the cube also beside the oracle on the host cores (the reference's CPU-runnable case)."""
+    import torch
+    from cn_physics import Solver, scenes
+    out = {}
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def timed(solver, dt, frames, tool=None):
+        for k in range(3):
+            if tool is not None:
+                solver.set_kinematic_target(tool, scenes.tool_path(dt * (k + 1)))
+            solver.step_many(dt, 1, sh)
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        if tool is None:
+            solver.step_many(dt, frames, sh)
+        else:
+            for k in range(frames):
+                solver.set_kinematic_target(tool, scenes.tool_path(dt * (k + 4)))
+                solver.step_many(dt, 1, sh)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        return ev[0].elapsed_time(ev[1]) / frames
+
+    w, desc, dt = scenes.xpbd_cube()
+    soa = w.soa()
+    sv = Solver(desc)
+    sv.sync_world(soa)
+    ms = timed(sv, dt, 100)
+    kernels, _ = sv.graph_stats()
+    n = soa.particle_count
+    cube = {"workload": "xpbd_cube_16: 4,096 particles, 16,875 tets, 10 substeps x 20 iterations, dt 1/60, ground",
+            "value": round(n * desc.substeps / (ms / 1e3), 1), "unit": "particle-substeps/s",
+            "ms_per_frame": round(ms, 4), "kernels_per_frame": kernels,
+            "us_per_kernel": round(ms * 1e3 / max(kernels, 1), 3)}
+    sv.close()
+    if cpu:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import cn_oracle
+        threads = cn_oracle.set_threads(os.cpu_count() or 1)
+        w2, d2, dt2 = scenes.xpbd_cube()
+        o = cn_oracle.Oracle(d2, w2.soa())
+        t0, frames = time.perf_counter(), 0
+        while frames < 50 and time.perf_counter() - t0 < 10.0:
+            o.step(dt2)
+            frames += 1
+        el = time.perf_counter() - t0
+        cube["cpu_baseline"] = {"value": round(n * d2.substeps * frames / el, 1), "unit": "particle-substeps/s",
+                                "cores": threads, "kind": "port", "sample": f"{frames} frames of the same cube"}
+    out["xpbd_cube"] = cube
+
+    w, desc, dt, tool = scenes.mixed_surgical()
+    soa = w.soa()
+    c = w.counts()
+    sv = Solver(desc)
+    sv.sync_world(soa)
+    ms = timed(sv, dt, 10, tool)
+    meta = sv.validate_gpu_meta()
+    n = soa.particle_count
+    out["mixed_surgical"] = {
+        "workload": f"mixed: {c['tets']} tets, {c['dihedrals']} dihedrals, {c['segments']} "
+                    f"strand segments, {n} particles in all (tissue, cloth, strands, 64^3 fluid), kinematic capsule, "
+                    f"{desc.substeps} substeps x {desc.default_iterations} iterations, dt 1/60",
+        "value": round(n * desc.substeps / (ms / 1e3), 1), "unit": "particle-substeps/s",
+        "ms_per_frame": round(ms, 3), "meta_status": meta["status"]}
+    sv.close()
+    return out
 
 
 def _diff_block(dims, spacing=0.1, base=1e-11, seed=0):
