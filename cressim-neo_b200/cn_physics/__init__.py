@@ -392,6 +392,28 @@ class Solver:
         _check(self._lib.cn_solver_scene_view(self._h, C.byref(v)))
         return {name: getattr(v, name) for name, _ in _abi.SceneView._fields_ if name != "reserved"}
 
+    def export_dlpack(self, buffer: str = "positions_inv_mass"):
+        """A torch tensor viewing one device buffer of the scene (no copy; the reference's
+        shared_buffer_to_dlpack).  Valid while gpu_scene_view()["binding_generation"] is unchanged."""
+        import torch
+        ptr = C.c_void_p()
+        _check(self._lib.cn_solver_export_dlpack(self._h, buffer.encode(), C.byref(ptr)))
+        new_capsule = C.pythonapi.PyCapsule_New
+        new_capsule.restype = C.py_object
+        new_capsule.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
+        return torch.utils.dlpack.from_dlpack(new_capsule(ptr, b"dltensor", None))
+
+    SYNC = {"particle_state": 1, "particle_attributes": 2, "constraints": 4, "rigid_bodies": 8, "colliders": 16}
+
+    def update_world(self, world: "World | _abi.WorldSoA", *categories: str) -> None:
+        """Uploads the named categories (SYNC keys; all when none is named) into the existing
+        buffers: the element counts must be the synced ones."""
+        soa = world.soa() if isinstance(world, World) else world
+        flags = 0
+        for c in categories or tuple(self.SYNC):
+            flags |= self.SYNC[c]
+        _check(self._lib.cn_solver_update_world(self._h, C.byref(soa), flags))
+
     def read_particles(self):
         x = np.zeros((self._n, 4), np.float32)
         v = np.zeros((self._n, 4), np.float32)

@@ -262,6 +262,8 @@ SIGNATURES = [
     ("cn_batch_get_stats", C.c_int, [C.c_void_p, C.POINTER(BatchStats)]),
     ("cn_batch_set_schedule", C.c_int, [C.c_void_p, u32, u32]),
     ("cn_batch_autotune", C.c_int, [C.c_void_p, P_u32, u32, f32, C.POINTER(BatchTuning)]),
+    ("cn_solver_export_dlpack", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p)]),
+    ("cn_solver_update_world", C.c_int, [C.c_void_p, C.POINTER(WorldSoA), u32]),
     ("cn_diff_desc_defaults", None, [C.POINTER(DiffDesc)]),
     ("cn_diff_create", C.c_int, [C.POINTER(DiffDesc), C.c_int, C.POINTER(C.c_void_p)]),
     ("cn_diff_destroy", None, [C.c_void_p]),

@@ -62,6 +62,7 @@ struct cn_solver {
     struct Probe { const char *name; cudaEvent_t begin, end; };
     std::vector<Probe> probes;
     uint32_t graphKernelNodes = 0, graphNodes = 0;
+    uint32_t contactMaterialCapacity = 0, fluidMaterialCapacity = 0;
 };
 
 namespace {
@@ -595,6 +596,8 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     sv->cfg = cn::configFromDesc(d);
     sv->hostX = w->positions_inv_mass;
     sv->hostV = w->velocities;
+    sv->contactMaterialCapacity = w->contact_material_count;
+    sv->fluidMaterialCapacity = w->fluid_material_count;
     sv->cellRangeCapacity = cn::nextPow2(std::max<uint32_t>(N * 2u, 1u));
     sv->synced = true;
     ++sv->bindingGeneration;
@@ -691,6 +694,110 @@ CN_API cn_status cn_solver_scene_view(cn_solver *sv, cn_scene_view *v)
     v->tet_count = s.T; v->strand_segment_count = s.S; v->strand_joint_count = s.J; v->strand_distance_count = s.SD;
     v->binding_generation = sv->bindingGeneration;
     v->device = sv->device;
+    return CN_OK;
+}
+
+namespace {
+struct DlHolder {
+    cn_dl_managed_tensor t{};
+    int64_t shape[2] = {0, 0};
+};
+void dlDelete(cn_dl_managed_tensor *self)
+{
+    delete static_cast<DlHolder *>(self->manager_ctx);
+}
+} // namespace
+
+CN_API cn_status cn_solver_export_dlpack(cn_solver *sv, const char *buffer, cn_dl_managed_tensor **out)
+{
+    if (!sv || !buffer || !out) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_export_dlpack: null argument");
+    if (!sv->synced) return setError(CN_ERR_NOT_INITIALIZED, "cn_solver_export_dlpack: no world synced");
+    const cn::Scene &s = sv->s;
+    const std::string name(buffer);
+    void *data = nullptr;
+    int64_t rows = s.N, cols = 4;
+    uint8_t code = 2; // float
+    if (name == "positions_inv_mass") data = s.x;
+    else if (name == "previous_positions") data = s.xprev;
+    else if (name == "velocities") data = s.v;
+    else if (name == "radii") { data = const_cast<float *>(s.radii); cols = 1; }
+    else if (name == "kinds") { data = const_cast<uint32_t *>(s.kinds); cols = 1; code = 1; }
+    else if (name == "strand_segment_states") { data = s.segOrient; rows = s.S; }
+    else return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_export_dlpack: unknown buffer '" + name + "'");
+    auto *h = new DlHolder();
+    h->shape[0] = rows;
+    h->shape[1] = cols;
+    cn_dl_tensor &t = h->t.dl_tensor;
+    t.data = data;
+    t.device_type = 2; // kDLCUDA
+    t.device_id = sv->device;
+    t.ndim = cols == 1 ? 1 : 2;
+    t.dtype_code = code;
+    t.dtype_bits = 32;
+    t.dtype_lanes = 1;
+    t.shape = h->shape;
+    t.strides = nullptr;
+    t.byte_offset = 0;
+    h->t.manager_ctx = h;
+    h->t.deleter = dlDelete;
+    *out = &h->t;
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, uint32_t flags)
+{
+    if (!sv || !w) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: null argument");
+    if (!sv->synced) return setError(CN_ERR_NOT_INITIALIZED, "cn_solver_update_world: no world synced");
+    const cn::Scene &s = sv->s;
+    if (w->particle_count != s.N || w->edge_count != s.E || w->bend_count != s.Bn || w->dihedral_count != s.D ||
+        w->tet_count != s.T || w->strand_segment_count != s.S || w->strand_joint_count != s.J ||
+        w->strand_distance_count != s.SD || w->rigid_body_count != s.B || w->collider_count != s.C)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: element counts changed; use cn_solver_sync_world");
+    CN_CUDA(cudaSetDevice(sv->device));
+    CN_CUDA(cudaDeviceSynchronize()); // frames in flight read these buffers
+    cudaStream_t st = sv->ownStream;
+    const uint32_t N = s.N;
+    if (flags & CN_SYNC_PARTICLE_STATE) {
+        CN_CUDA(up(s.x, w->positions_inv_mass, N, st));
+        CN_CUDA(up(s.v, w->velocities, N, st));
+    }
+    if (flags & CN_SYNC_PARTICLE_ATTRIBUTES) {
+        CN_CUDA(up(s.radii, w->radii, N, st));
+        CN_CUDA(up(s.meta, w->metadata, N, st));
+        CN_CUDA(up(s.matIdx, w->material_indices, N, st));
+        CN_CUDA(up(s.fluidMatIdx, w->fluid_material_indices, N, st));
+        if (w->contact_material_count > std::max<uint32_t>(sv->contactMaterialCapacity, 1u) ||
+            w->fluid_material_count > std::max<uint32_t>(sv->fluidMaterialCapacity, 1u))
+            return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: more materials than synced; use cn_solver_sync_world");
+        CN_CUDA(up(s.contactMaterials, w->contact_materials, w->contact_material_count, st));
+        CN_CUDA(up(s.fluidMaterials, w->fluid_materials, w->fluid_material_count, st));
+    }
+    if (flags & CN_SYNC_CONSTRAINTS) {
+        // records only: incidence tables depend on the particle indices, which must not change
+        CN_CUDA(up(s.edges, w->edges, s.E, st));
+        CN_CUDA(up(s.bends, w->bends, s.Bn, st));
+        CN_CUDA(up(s.dihedrals, w->dihedrals, s.D, st));
+        CN_CUDA(up(s.tets, w->tets, s.T, st));
+        CN_CUDA(up(s.segs, w->strand_segments, s.S, st));
+        CN_CUDA(up(s.joints, w->strand_joints, s.J, st));
+        CN_CUDA(up(s.dists, w->strand_distances, s.SD, st));
+    }
+    if (flags & CN_SYNC_RIGID_BODIES) {
+        CN_CUDA(up(s.bodyPos, w->body_positions_inv_mass, s.B, st));
+        CN_CUDA(up(s.bodyRot, w->body_orientations, s.B, st));
+        CN_CUDA(up(s.bodyLin, w->body_linear_velocities, s.B, st));
+        CN_CUDA(up(s.bodyAng, w->body_angular_velocities, s.B, st));
+        CN_CUDA(up(s.bodyScale, w->body_scales, s.B, st));
+        CN_CUDA(up(s.bodyKinPos, w->body_kinematic_target_positions, s.B, st));
+        CN_CUDA(up(s.bodyKinRot, w->body_kinematic_target_orientations, s.B, st));
+        CN_CUDA(up(s.bodyKinFlags, w->body_kinematic_target_flags, s.B, st));
+    }
+    if (flags & CN_SYNC_COLLIDERS) {
+        CN_CUDA(up(s.colGeo, w->collider_geometry, s.C, st));
+        CN_CUDA(up(s.colBp, w->collider_broadphase, s.C, st));
+        CN_CUDA(up(s.colMat, w->collider_materials, s.C, st));
+    }
+    CN_CUDA(cudaStreamSynchronize(st));
     return CN_OK;
 }
 

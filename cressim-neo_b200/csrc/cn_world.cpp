@@ -186,6 +186,9 @@ struct cn_world {
     std::vector<cn_collider_geometry> colGeo;
     std::vector<cn_collider_broadphase> colBp;
     float cellSize = 1.0e-4f;
+    // The packed SoA is rebuilt only after an authoring change, so edits a caller makes through
+    // the SoA's arrays (state, per-constraint parameters) survive later cn_world_get_soa calls.
+    bool packed = false;
 };
 
 namespace {
@@ -903,6 +906,7 @@ cn_status addSoftBody(cn_world *w, SoftBody &&sb, const cn_soft_body_grid_desc *
 CN_API cn_status cn_world_add_soft_body_grid(cn_world *w, const cn_soft_body_grid_desc *d, uint32_t *out)
 {
     if (!w || !d) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_soft_body_grid: null argument");
+    w->packed = false;
     SoftBody sb;
     sb.desc = *d;
     sb.source = SoftSource::RegularGrid;
@@ -915,6 +919,7 @@ CN_API cn_status cn_world_add_soft_body_tet_mesh(cn_world *w, const cn_soft_body
 {
     if (!w || !d || (vertex_count && !positions) || (tet_count && !tet_indices))
         return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_soft_body_tet_mesh: null argument");
+    w->packed = false;
     SoftBody sb;
     sb.desc = *d;
     sb.source = SoftSource::TetMesh;
@@ -928,6 +933,7 @@ CN_API cn_status cn_world_add_soft_body_tetgen(cn_world *w, const cn_soft_body_g
                                                const char *ele_file, uint32_t *out)
 {
     if (!w || !d) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_soft_body_tetgen: null argument");
+    w->packed = false;
     SoftBody sb;
     sb.desc = *d;
     sb.source = SoftSource::TetMesh;
@@ -941,6 +947,7 @@ CN_API cn_status cn_world_add_soft_body_meshfree(cn_world *w, const cn_soft_body
 {
     if (!w || !d || (particle_count && !positions))
         return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_soft_body_meshfree: null argument");
+    w->packed = false;
     SoftBody sb;
     sb.desc = *d;
     sb.source = SoftSource::Meshfree;
@@ -953,6 +960,7 @@ CN_API cn_status cn_world_add_soft_body_meshfree(cn_world *w, const cn_soft_body
 CN_API cn_status cn_world_add_fluid_grid(cn_world *w, const cn_fluid_grid_desc *d, uint32_t *out)
 {
     if (!w || !d) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_fluid_grid: null argument");
+    w->packed = false;
     if (!(d->target_particle_spacing > 0.0f)) return cn::setError(CN_ERR_INVALID_ARGUMENT, "fluid: spacing must be > 0");
     Fluid f;
     f.desc = *d;
@@ -965,6 +973,7 @@ CN_API cn_status cn_world_add_fluid_grid(cn_world *w, const cn_fluid_grid_desc *
 CN_API cn_status cn_world_add_cloth_grid(cn_world *w, const cn_cloth_grid_desc *d, uint32_t *out)
 {
     if (!w || !d) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_cloth_grid: null argument");
+    w->packed = false;
     Cloth c;
     c.desc = *d;
     if (d->static_particle_indices && d->static_particle_count)
@@ -980,6 +989,7 @@ CN_API cn_status cn_world_add_strand(cn_world *w, const cn_strand_desc *d, uint3
 {
     if (!w || !d || !d->rest_positions)
         return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_strand: null argument");
+    w->packed = false;
     Strand st;
     st.desc = *d;
     for (uint32_t i = 0; i < d->rest_position_count; ++i)
@@ -998,6 +1008,7 @@ CN_API cn_status cn_world_add_strand(cn_world *w, const cn_strand_desc *d, uint3
 CN_API cn_status cn_world_add_rigid_body(cn_world *w, const cn_rigid_body_desc *d, uint32_t *out)
 {
     if (!w || !d) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_rigid_body: null argument");
+    w->packed = false;
     if (d->body_type > CN_BODY_DYNAMIC) return cn::setError(CN_ERR_INVALID_ARGUMENT, "rigid body: unknown body type");
     if (out) *out = uint32_t(w->bodies.size());
     w->bodies.push_back(*d);
@@ -1007,6 +1018,7 @@ CN_API cn_status cn_world_add_rigid_body(cn_world *w, const cn_rigid_body_desc *
 CN_API cn_status cn_world_add_collider(cn_world *w, const cn_collider_desc *d, uint32_t *out)
 {
     if (!w || !d) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_collider: null argument");
+    w->packed = false;
     if (d->body >= w->bodies.size()) return cn::setError(CN_ERR_INVALID_ARGUMENT, "collider: body index out of range");
     if (d->shape_type > CN_COLLIDER_CAPSULE) return cn::setError(CN_ERR_INVALID_ARGUMENT, "collider: unknown shape");
     if (out) *out = uint32_t(w->colliders.size());
@@ -1017,8 +1029,11 @@ CN_API cn_status cn_world_add_collider(cn_world *w, const cn_collider_desc *d, u
 CN_API cn_status cn_world_get_soa(cn_world *w, cn_world_soa *o)
 {
     if (!w || !o) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_get_soa: null argument");
-    const cn_status st = pack(*w);
-    if (st != CN_OK) return cn::setError(st, "cn_world_get_soa: invalid world");
+    if (!w->packed) {
+        const cn_status st = pack(*w);
+        if (st != CN_OK) return cn::setError(st, "cn_world_get_soa: invalid world");
+        w->packed = true;
+    }
     std::memset(o, 0, sizeof(*o));
     o->particle_count = uint32_t(w->radii.size());
     o->positions_inv_mass = ptr(w->x);

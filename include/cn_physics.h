@@ -408,6 +408,30 @@ typedef struct cn_scene_view {
     uint32_t reserved;
 } cn_scene_view;
 
+/* DLPack export of one scene-view buffer (the reference's shared_buffer_to_dlpack,
+ * python/bindings.cpp:3303): a non-owning DLManagedTensor over the solver's device memory, valid
+ * until binding_generation changes.  The struct layout is DLPack's (dlpack.h, version 0.8);
+ * the consumer calls `deleter` when done.  Buffers: "positions_inv_mass", "previous_positions",
+ * "velocities" (float32 N x 4), "radii" (float32 N), "kinds" (uint32 N), "strand_segment_states"
+ * (float32 S x 4). */
+typedef struct cn_dl_tensor {
+    void *data;
+    int32_t device_type;            /* kDLCUDA = 2 */
+    int32_t device_id;
+    int32_t ndim;
+    uint8_t dtype_code;             /* kDLInt 0, kDLUInt 1, kDLFloat 2 */
+    uint8_t dtype_bits;
+    uint16_t dtype_lanes;
+    int64_t *shape;
+    int64_t *strides;               /* NULL: compact row-major */
+    uint64_t byte_offset;
+} cn_dl_tensor;
+typedef struct cn_dl_managed_tensor {
+    cn_dl_tensor dl_tensor;
+    void *manager_ctx;
+    void (*deleter)(struct cn_dl_managed_tensor *self);
+} cn_dl_managed_tensor;
+
 /* PhysicsSolver(GpuDevice&, const PhysicsSolverDesc&) + initialize().  device: CUDA ordinal. */
 CN_API cn_status cn_solver_create(const cn_solver_desc *desc, int device, cn_solver **out_solver);
 CN_API void cn_solver_destroy(cn_solver *solver);
@@ -428,6 +452,19 @@ CN_API cn_status cn_solver_set_kinematic_target(cn_solver *solver, uint32_t body
                                                 const float position[3], const float orientation[4]);
 /* PhysicsSolver::gpuSceneView / softPositionsInvMassSharedBuffer: the native device buffers. */
 CN_API cn_status cn_solver_scene_view(cn_solver *solver, cn_scene_view *out_view);
+CN_API cn_status cn_solver_export_dlpack(cn_solver *solver, const char *buffer, cn_dl_managed_tensor **out_tensor);
+/* Incremental upload (the revision-counter path of uploadWorldState,
+ * physics_scene_gpu_state.cpp:2348): the world's element counts must equal the synced ones;
+ * the flagged categories are copied into the existing buffers, so device pointers and
+ * binding_generation stay as they are. */
+typedef enum cn_sync_flags {
+    CN_SYNC_PARTICLE_STATE = 1,     /* positions / inverse masses, velocities */
+    CN_SYNC_PARTICLE_ATTRIBUTES = 2,/* radii, metadata, material indices, contact / fluid materials */
+    CN_SYNC_CONSTRAINTS = 4,        /* edge, bend, dihedral, tet and strand records */
+    CN_SYNC_RIGID_BODIES = 8,       /* body poses, velocities, scales, kinematic targets */
+    CN_SYNC_COLLIDERS = 16          /* collider geometry, broadphase records, materials */
+} cn_sync_flags;
+CN_API cn_status cn_solver_update_world(cn_solver *solver, const cn_world_soa *world, uint32_t flags);
 /* Blocking copy of device particle state to host (readbackPredictedParticleStateBlocking).
  * Any pointer may be NULL. */
 CN_API cn_status cn_solver_read_particles(cn_solver *solver, float *positions_inv_mass,
