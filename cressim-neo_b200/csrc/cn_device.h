@@ -170,7 +170,7 @@ struct Scene {
     uint32_t *nbr = nullptr;          // [N][maxNbr] sorted slots
     uint32_t *nbrCount = nullptr;     // per sorted slot
     uint32_t supCap = 0;              // superset list slots per particle (0: superset lists off)
-    float supMargin = 0.2f;           // superset radius = h * (1 + supMargin)
+    float supMargin = 0.25f;          // superset radius = h * (1 + supMargin)
     uint32_t *sup = nullptr;          // [N][supCap] candidates within the superset radius, traversal order
     uint32_t *supCount = nullptr;     // per sorted slot (> supCap: overflowed)
     uint32_t *fluidMaxDelta = nullptr; // [64] float bits of max |accumulated delta| per iteration

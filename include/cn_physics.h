@@ -511,7 +511,7 @@ typedef enum cn_debug_buffer {
     CN_DEBUG_FLUID_CONSTRAINTS = 5,/* float4[N]: surface normal xyz, density constraint w */
     CN_DEBUG_FLUID_DELTA = 6,      /* float4[N]: last packed delta + interaction weight */
     CN_DEBUG_RIGID_CONTACTS = 7,   /* 64 B records of the last iteration's particle-rigid contacts */
-    CN_DEBUG_FLUID_SUPERSET_COUNTS = 8 /* uint[N]: candidates within h * 1.2 recorded at the substep's first
+    CN_DEBUG_FLUID_SUPERSET_COUNTS = 8 /* uint[N]: candidates within h * 1.25 recorded at the substep's first
                                         * iteration (no reference counterpart; zeros when the lists are off) */
 } cn_debug_buffer;
 /* Copies at most capacity_bytes; *out_bytes receives the full size of the buffer. */
