@@ -96,104 +96,113 @@ __device__ void computeBodyAabb(uint32_t shape, f3 pos, float4 q, float4 p, floa
     mxv = pos + e;
 }
 
+__device__ __forceinline__ void rigidPredictBody(const Scene &s, float dt, float gx, float gy, float gz, uint32_t b)
+{
+    const float4 p = s.bodyPos[b];
+    const float4 q = qNormalize(s.bodyRot[b]);
+    const float4 lin = s.bodyLin[b], ang = s.bodyAng[b];
+    const bool kin = (s.bodyKinFlags[b] & 1u) != 0u;
+    const float4 kq = qNormalize(s.bodyKinRot[b]);
+    s.prevBodyPos[b] = p;
+    s.prevBodyRot[b] = q;
+    const uint32_t type = s.bodyType[b];
+    if (type == CN_BODY_STATIC) {
+        s.predBodyPos[b] = p;
+        s.predBodyRot[b] = q;
+        s.predBodyLin[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+        s.predBodyAng[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else if (type == CN_BODY_KINEMATIC) {
+        const f3 pp = kin ? xyz(s.bodyKinPos[b]) : xyz(p);
+        const float4 pq = kin ? kq : q;
+        const f3 l = (pp - xyz(p)) / mx(dt, kEps);
+        const f3 a = angularVelocityFromQuaternionDelta(q, pq, mx(dt, kEps));
+        s.predBodyPos[b] = mk4(pp, p.w);
+        s.predBodyRot[b] = pq;
+        s.predBodyLin[b] = mk4(l, lin.w);
+        s.predBodyAng[b] = mk4(a, ang.w);
+    } else {
+        const f3 l = xyz(lin) + f3{gx, gy, gz} * dt;
+        s.predBodyPos[b] = mk4(xyz(p) + l * dt, p.w);
+        s.predBodyRot[b] = q;
+        s.predBodyLin[b] = mk4(l, lin.w);
+        s.predBodyAng[b] = ang;
+    }
+}
+
+__device__ __forceinline__ void colliderAabb(const Scene &s, uint32_t c)
+{
+    const cn_collider_broadphase bp = s.colBp[c];
+    const uint32_t ob = bp.owner_body;
+    if (ob >= s.B || bp.enabled_flag == 0u) {
+        s.colAabbMin[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+        s.colAabbMax[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const float4 sc = s.bodyScale[ob];
+    const cn_collider_geometry cg = s.colGeo[c];
+    const float4 params = make_float4(cg.shape_params[0], cg.shape_params[1], cg.shape_params[2],
+                                      cg.shape_params[3]);
+    const f3 lp = f3{cg.local_position[0], cg.local_position[1], cg.local_position[2]} * xyz(sc);
+    const float4 lq = qNormalize(make_float4(cg.local_orientation[0], cg.local_orientation[1],
+                                             cg.local_orientation[2], cg.local_orientation[3]));
+    const float4 bq = qNormalize(s.predBodyRot[ob]);
+    const float4 pbq = qNormalize(s.prevBodyRot[ob]);
+    const f3 cp = xyz(s.predBodyPos[ob]) + qRotate(bq, lp);
+    const float4 cq = qNormalize(qMul(bq, lq));
+    const f3 pcp = xyz(s.prevBodyPos[ob]) + qRotate(pbq, lp);
+    const float4 pcq = qNormalize(qMul(pbq, lq));
+    f3 a0, a1, b0, b1;
+    computeBodyAabb(bp.shape_type, cp, cq, params, sc, a0, a1);
+    computeBodyAabb(bp.shape_type, pcp, pcq, params, sc, b0, b1);
+    const f3 lo = min3(a0, b0) - f3{kBroadPhaseMargin, kBroadPhaseMargin, kBroadPhaseMargin};
+    const f3 hi = max3(a1, b1) + f3{kBroadPhaseMargin, kBroadPhaseMargin, kBroadPhaseMargin};
+    s.colAabbMin[c] = mk4(lo, 0.f);
+    s.colAabbMax[c] = mk4(hi, 0.f);
+}
+
+__device__ __forceinline__ void colliderFrame(const Scene &s, uint32_t c)
+{
+    const cn_collider_broadphase bp = s.colBp[c];
+    float4 *fr = s.colFrame + size_t(c) * 4;
+    const uint32_t b = bp.owner_body;
+    if (bp.enabled_flag == 0u || b >= s.B) {
+        fr[0] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0u));
+        return;
+    }
+    const f3 bpos = xyz(s.predBodyPos[b]);
+    const float4 bq = qNormalize(s.predBodyRot[b]);
+    const float4 sc = s.bodyScale[b];
+    const cn_collider_geometry cg = s.colGeo[c];
+    const f3 cwp = bpos + qRotate(bq, f3{cg.local_position[0], cg.local_position[1], cg.local_position[2]});
+    const float4 cwq = qNormalize(qMul(bq, qNormalize(make_float4(cg.local_orientation[0], cg.local_orientation[1],
+                                                                  cg.local_orientation[2], cg.local_orientation[3]))));
+    const float4 sp = make_float4(cg.shape_params[0], cg.shape_params[1], cg.shape_params[2], cg.shape_params[3]);
+    float4 e0 = make_float4(0.f, 0.f, 0.f, 0.f), e1 = e0;
+    if (bp.shape_type == CN_COLLIDER_SPHERE) {
+        e0.x = sphereRadius(sp, sc);
+    } else if (bp.shape_type == CN_COLLIDER_BOX) {
+        e0 = mk4(boxHalfExtents(sp, sc), 0.f);
+    } else {
+        f3 a, b2;
+        float cr = 0.0f;
+        capsuleSegment(cwp, cwq, sp, sc, a, b2, cr);
+        e0 = mk4(a, cr);
+        e1 = mk4(b2, 0.f);
+    }
+    fr[0] = mk4(cwp, __uint_as_float(1u | (bp.shape_type << 8)));
+    fr[1] = cwq;
+    fr[2] = e0;
+    fr[3] = e1;
+}
+
 __global__ void __launch_bounds__(kThreads) k_rigidPredict(Scene s, float dt, float gx, float gy, float gz)
 {
-    forEachInBlock(s.wB, s.B, [&](uint32_t b) {
-        const float4 p = s.bodyPos[b];
-        const float4 q = qNormalize(s.bodyRot[b]);
-        const float4 lin = s.bodyLin[b], ang = s.bodyAng[b];
-        const bool kin = (s.bodyKinFlags[b] & 1u) != 0u;
-        const float4 kq = qNormalize(s.bodyKinRot[b]);
-        s.prevBodyPos[b] = p;
-        s.prevBodyRot[b] = q;
-        const uint32_t type = s.bodyType[b];
-        if (type == CN_BODY_STATIC) {
-            s.predBodyPos[b] = p;
-            s.predBodyRot[b] = q;
-            s.predBodyLin[b] = make_float4(0.f, 0.f, 0.f, 0.f);
-            s.predBodyAng[b] = make_float4(0.f, 0.f, 0.f, 0.f);
-        } else if (type == CN_BODY_KINEMATIC) {
-            const f3 pp = kin ? xyz(s.bodyKinPos[b]) : xyz(p);
-            const float4 pq = kin ? kq : q;
-            const f3 l = (pp - xyz(p)) / mx(dt, kEps);
-            const f3 a = angularVelocityFromQuaternionDelta(q, pq, mx(dt, kEps));
-            s.predBodyPos[b] = mk4(pp, p.w);
-            s.predBodyRot[b] = pq;
-            s.predBodyLin[b] = mk4(l, lin.w);
-            s.predBodyAng[b] = mk4(a, ang.w);
-        } else {
-            const f3 l = xyz(lin) + f3{gx, gy, gz} * dt;
-            s.predBodyPos[b] = mk4(xyz(p) + l * dt, p.w);
-            s.predBodyRot[b] = q;
-            s.predBodyLin[b] = mk4(l, lin.w);
-            s.predBodyAng[b] = ang;
-        }
-    });
+    forEachInBlock(s.wB, s.B, [&](uint32_t b) { rigidPredictBody(s, dt, gx, gy, gz, b); });
     __syncthreads();
-    forEachInBlock(s.wC, s.C, [&](uint32_t c) {
-        const cn_collider_broadphase bp = s.colBp[c];
-        const uint32_t ob = bp.owner_body;
-        if (ob >= s.B || bp.enabled_flag == 0u) {
-            s.colAabbMin[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-            s.colAabbMax[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-            return;
-        }
-        const float4 sc = s.bodyScale[ob];
-        const cn_collider_geometry cg = s.colGeo[c];
-        const float4 params = make_float4(cg.shape_params[0], cg.shape_params[1], cg.shape_params[2],
-                                          cg.shape_params[3]);
-        const f3 lp = f3{cg.local_position[0], cg.local_position[1], cg.local_position[2]} * xyz(sc);
-        const float4 lq = qNormalize(make_float4(cg.local_orientation[0], cg.local_orientation[1],
-                                                 cg.local_orientation[2], cg.local_orientation[3]));
-        const float4 bq = qNormalize(s.predBodyRot[ob]);
-        const float4 pbq = qNormalize(s.prevBodyRot[ob]);
-        const f3 cp = xyz(s.predBodyPos[ob]) + qRotate(bq, lp);
-        const float4 cq = qNormalize(qMul(bq, lq));
-        const f3 pcp = xyz(s.prevBodyPos[ob]) + qRotate(pbq, lp);
-        const float4 pcq = qNormalize(qMul(pbq, lq));
-        f3 a0, a1, b0, b1;
-        computeBodyAabb(bp.shape_type, cp, cq, params, sc, a0, a1);
-        computeBodyAabb(bp.shape_type, pcp, pcq, params, sc, b0, b1);
-        const f3 lo = min3(a0, b0) - f3{kBroadPhaseMargin, kBroadPhaseMargin, kBroadPhaseMargin};
-        const f3 hi = max3(a1, b1) + f3{kBroadPhaseMargin, kBroadPhaseMargin, kBroadPhaseMargin};
-        s.colAabbMin[c] = mk4(lo, 0.f);
-        s.colAabbMax[c] = mk4(hi, 0.f);
-    });
+    forEachInBlock(s.wC, s.C, [&](uint32_t c) { colliderAabb(s, c); });
     // Collider frames for the fluid boundary queries, with the arithmetic of
     // physics_fluid_boundary_common.hlsli:11-40 (unscaled local offset), done once per collider.
-    forEachInBlock(s.wC, s.C, [&](uint32_t c) {
-        const cn_collider_broadphase bp = s.colBp[c];
-        float4 *fr = s.colFrame + size_t(c) * 4;
-        const uint32_t b = bp.owner_body;
-        if (bp.enabled_flag == 0u || b >= s.B) {
-            fr[0] = make_float4(0.f, 0.f, 0.f, __uint_as_float(0u));
-            return;
-        }
-        const f3 bpos = xyz(s.predBodyPos[b]);
-        const float4 bq = qNormalize(s.predBodyRot[b]);
-        const float4 sc = s.bodyScale[b];
-        const cn_collider_geometry cg = s.colGeo[c];
-        const f3 cwp = bpos + qRotate(bq, f3{cg.local_position[0], cg.local_position[1], cg.local_position[2]});
-        const float4 cwq = qNormalize(qMul(bq, qNormalize(make_float4(cg.local_orientation[0], cg.local_orientation[1],
-                                                                      cg.local_orientation[2], cg.local_orientation[3]))));
-        const float4 sp = make_float4(cg.shape_params[0], cg.shape_params[1], cg.shape_params[2], cg.shape_params[3]);
-        float4 e0 = make_float4(0.f, 0.f, 0.f, 0.f), e1 = e0;
-        if (bp.shape_type == CN_COLLIDER_SPHERE) {
-            e0.x = sphereRadius(sp, sc);
-        } else if (bp.shape_type == CN_COLLIDER_BOX) {
-            e0 = mk4(boxHalfExtents(sp, sc), 0.f);
-        } else {
-            f3 a, b2;
-            float cr = 0.0f;
-            capsuleSegment(cwp, cwq, sp, sc, a, b2, cr);
-            e0 = mk4(a, cr);
-            e1 = mk4(b2, 0.f);
-        }
-        fr[0] = mk4(cwp, __uint_as_float(1u | (bp.shape_type << 8)));
-        fr[1] = cwq;
-        fr[2] = e0;
-        fr[3] = e1;
-    });
+    forEachInBlock(s.wC, s.C, [&](uint32_t c) { colliderFrame(s, c); });
 }
 
 __global__ void k_applyBodyTargets(Scene s, const BodyTarget *list, const uint32_t *count)
@@ -210,14 +219,17 @@ __global__ void k_applyBodyTargets(Scene s, const BodyTarget *list, const uint32
 }
 
 // physics_rigid_update_velocities (copyPredictedRigidBodiesToPersistentState)
+__device__ __forceinline__ void copyPredictedBody(const Scene &s, uint32_t b)
+{
+    s.bodyPos[b] = s.predBodyPos[b];
+    s.bodyRot[b] = s.predBodyRot[b];
+    s.bodyLin[b] = s.predBodyLin[b];
+    s.bodyAng[b] = s.predBodyAng[b];
+}
+
 __global__ void k_copyPredictedRigid(Scene s)
 {
-    forEachInBlock(s.wB, s.B, [&](uint32_t b) {
-        s.bodyPos[b] = s.predBodyPos[b];
-        s.bodyRot[b] = s.predBodyRot[b];
-        s.bodyLin[b] = s.predBodyLin[b];
-        s.bodyAng[b] = s.predBodyAng[b];
-    });
+    forEachInBlock(s.wB, s.B, [&](uint32_t b) { copyPredictedBody(s, b); });
 }
 
 // ------------------------------------------------------------------------------------------
@@ -225,35 +237,40 @@ __global__ void k_copyPredictedRigid(Scene s)
 // physics_soft_predict.cs.hlsl:12-47, physics_particle_build_broad_phase_entries.cs.hlsl:9-35,
 // physics_particle_build_broad_phase_keys.cs.hlsl:8-23
 // ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void predictParticle(const Scene &s, float dt, float gx, float gy, float gz, bool writeKeys, uint32_t i)
+{
+    const float4 pim = s.x[i];
+    const float4 v0 = s.v[i];            // loaded with x (not after the mass test):
+    const uint32_t kind = s.kinds[i];    // one round trip fewer
+    const f3 pos = xyz(pim);
+    s.xprev[i] = mk4(pos, 0.0f);
+    f3 pp = pos;
+    if (pim.w <= kEps) {
+        s.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+        f3 vel = xyz(v0);
+        float gs = 1.0f;
+        if (kind == CN_PARTICLE_FLUID) gs = s.fluidMaterials[s.fluidMatIdx[i]].gravity_scale;
+        vel = vel + f3{gx, gy, gz} * (dt * gs);
+        pp = pos + vel * dt;
+        s.v[i] = mk4(vel, 0.0f);
+        s.x[i] = mk4(pp, pim.w);
+    }
+    if (!writeKeys) return;
+    const float safe = mx(s.cellSize, 1.0e-4f);
+    const float inv = 1.0f / safe;
+    const int cx = int(floorf(pp.x * inv));
+    const int cy = int(floorf(pp.y * inv));
+    const int cz = int(floorf(pp.z * inv));
+    const uint32_t key = cellKey(cx, cy, cz);
+    s.entries[i] = make_int4(cx, cy, cz, int(key));
+    s.keysA[i] = key;
+}
+
 __global__ void __launch_bounds__(kThreads) k_predictKeys(Scene s, float dt, float gx, float gy, float gz,
                                                           bool writeKeys)
 {
-    forEachElem(s.wP, s.N, [&](uint32_t i) {
-        const float4 pim = s.x[i];
-        const f3 pos = xyz(pim);
-        s.xprev[i] = mk4(pos, 0.0f);
-        f3 pp = pos;
-        if (pim.w <= kEps) {
-            s.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        } else {
-            f3 vel = xyz(s.v[i]);
-            float gs = 1.0f;
-            if (s.kinds[i] == CN_PARTICLE_FLUID) gs = s.fluidMaterials[s.fluidMatIdx[i]].gravity_scale;
-            vel = vel + f3{gx, gy, gz} * (dt * gs);
-            pp = pos + vel * dt;
-            s.v[i] = mk4(vel, 0.0f);
-            s.x[i] = mk4(pp, pim.w);
-        }
-        if (!writeKeys) return;
-        const float safe = mx(s.cellSize, 1.0e-4f);
-        const float inv = 1.0f / safe;
-        const int cx = int(floorf(pp.x * inv));
-        const int cy = int(floorf(pp.y * inv));
-        const int cz = int(floorf(pp.z * inv));
-        const uint32_t key = cellKey(cx, cy, cz);
-        s.entries[i] = make_int4(cx, cy, cz, int(key));
-        s.keysA[i] = key;
-    });
+    forEachElem(s.wP, s.N, [&](uint32_t i) { predictParticle(s, dt, gx, gy, gz, writeKeys, i); });
 }
 
 // ------------------------------------------------------------------------------------------
@@ -465,6 +482,46 @@ __global__ void __launch_bounds__(kThreads) k_runNeighbors(Scene s)
 // Particle-rigid candidate pairs (solid particles vs static/kinematic bodies, dedup 16)
 // physics_particle_count_particle_rigid_candidates.cs.hlsl:113-151, emit, finalize.
 // ------------------------------------------------------------------------------------------
+// kMode 0 counts the particle's candidate bodies, 1 emits its pairs from `write` (its offset
+// after the count pass and the scan); both return the count.
+template <uint32_t kMode>
+__device__ __forceinline__ uint32_t rigidCandidatesAt(const Scene &s, uint32_t i, uint32_t write)
+{
+    const f3 p = xyz(s.x[i]);
+    const float r = s.radii[i];
+    const f3 qmin = p - f3{r, r, r}, qmax = p + f3{r, r, r};
+    const uint4 m = s.meta[i];
+    const uint32_t kind = s.kinds[i];
+    const bool proxyOwner = s.ownerTypes[i] == CN_OWNER_RIGID_BODY;
+    const uint32_t owner = s.ownerIdx[i];
+    uint32_t seen[kRigidDedup];
+    uint32_t seenCount = 0, count = 0;
+    const uint2 cq = s.pColRange ? s.pColRange[i] : make_uint2(0u, s.colQueryCount);
+    for (uint32_t k = cq.x; k < cq.y; ++k) {
+        const uint32_t c = s.colQueryOrder[k];
+        if (!aabbOverlaps(qmin, qmax, xyz(s.colAabbMin[c]), xyz(s.colAabbMax[c]))) continue;
+        const cn_collider_broadphase bp = s.colBp[c];
+        const uint32_t b = bp.owner_body;
+        if (proxyOwner && b == owner) continue;
+        const uint32_t bt = s.bodyType[b];
+        if (!(bp.enabled_flag != 0u && bp.environment_index == m.x && (m.w & bp.collision_layer) != 0u &&
+              (bp.collision_mask & m.z) != 0u && (kind == CN_PARTICLE_SOLID || bt == CN_BODY_DYNAMIC) &&
+              s.bodyColRanges[b].y > 0u))
+            continue;
+        bool fresh = true;
+        for (uint32_t q = 0; q < seenCount; ++q)
+            if (seen[q] == b) { fresh = false; break; }
+        if (!fresh) continue;
+        if (seenCount < kRigidDedup) seen[seenCount++] = b;
+        if (kMode != 0u) {
+            if (write >= s.rigidPairCapacity) return count;
+            s.rigidPairs[write++] = make_uint2(i, b);
+        }
+        ++count;
+    }
+    return count;
+}
+
 template <bool kEmit>
 __global__ void __launch_bounds__(kThreads) k_rigidCandidates(Scene s, const uint32_t *total)
 {
@@ -473,42 +530,11 @@ __global__ void __launch_bounds__(kThreads) k_rigidCandidates(Scene s, const uin
         s.meta_->rigidPairCount = min(*total, s.rigidPairCapacity);
     }
     forEachElem(s.wP, s.N, [&](uint32_t i) {
-        if (kEmit && s.candCount[i] == 0u) return;
-        const f3 p = xyz(s.x[i]);
-        const float r = s.radii[i];
-        const f3 qmin = p - f3{r, r, r}, qmax = p + f3{r, r, r};
-        const uint4 m = s.meta[i];
-        const uint32_t kind = s.kinds[i];
-        const bool proxyOwner = s.ownerTypes[i] == CN_OWNER_RIGID_BODY;
-        const uint32_t owner = s.ownerIdx[i];
-        uint32_t seen[kRigidDedup];
-        uint32_t seenCount = 0, count = 0;
-        uint32_t write = kEmit ? s.candOffset[i] : 0u;
-        const uint2 cq = s.pColRange ? s.pColRange[i] : make_uint2(0u, s.colQueryCount);
-        for (uint32_t k = cq.x; k < cq.y; ++k) {
-            const uint32_t c = s.colQueryOrder[k];
-            if (!aabbOverlaps(qmin, qmax, xyz(s.colAabbMin[c]), xyz(s.colAabbMax[c]))) continue;
-            const cn_collider_broadphase bp = s.colBp[c];
-            const uint32_t b = bp.owner_body;
-            if (proxyOwner && b == owner) continue;
-            const uint32_t bt = s.bodyType[b];
-            if (!(bp.enabled_flag != 0u && bp.environment_index == m.x && (m.w & bp.collision_layer) != 0u &&
-                  (bp.collision_mask & m.z) != 0u && (kind == CN_PARTICLE_SOLID || bt == CN_BODY_DYNAMIC) &&
-                  s.bodyColRanges[b].y > 0u))
-                continue;
-            bool fresh = true;
-            for (uint32_t q = 0; q < seenCount; ++q)
-                if (seen[q] == b) { fresh = false; break; }
-            if (!fresh) continue;
-            if (seenCount < kRigidDedup) seen[seenCount++] = b;
-            if (kEmit) {
-                if (write >= s.rigidPairCapacity) return;
-                s.rigidPairs[write++] = make_uint2(i, b);
-            } else {
-                ++count;
-            }
+        if (!kEmit) {
+            s.candCount[i] = rigidCandidatesAt<0u>(s, i, 0u);
+        } else if (s.candCount[i] != 0u) {
+            rigidCandidatesAt<1u>(s, i, s.candOffset[i]);
         }
-        if (!kEmit) s.candCount[i] = count;
     });
 }
 
@@ -1015,102 +1041,134 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
 // ascending constraint order (the reference's incidence order).
 // ------------------------------------------------------------------------------------------
 // physics_soft_solve_edge_constraints.cs.hlsl:10-74
-__global__ void __launch_bounds__(kThreads) k_solveEdges(Scene s, float dt, float relax)
+__device__ __forceinline__ void solveEdge(const Scene &s, float dt, float relax, uint32_t e)
 {
-    forEachElem(s.wE, s.E, [&](uint32_t e) {
-        const cn_soft_edge ed = s.edges[e];
-        float4 cA = make_float4(0.f, 0.f, 0.f, 0.f), cB = cA;
-        if (ed.enabled != 0u) {
-            const float4 a = s.x[ed.particle_a], b = s.x[ed.particle_b];
-            const float wA = a.w, wB = b.w, wSum = wA + wB;
-            const f3 delta = xyz(b) - xyz(a);
-            const float l2 = dot(delta, delta);
-            if (wSum > kEps && l2 > kEps) {
-                const float len = sqrtf(l2);
-                const f3 gA = -delta / len;
-                const f3 gB = -gA;
-                const float alpha = mx(ed.compliance, 0.0f) / mx(dt * dt, kEps);
-                const float Cv = len - ed.rest_length;
-                const float lambda = s.edgeLambda[e];
-                const float den = wSum + alpha;
-                if (den > kEps) {
-                    const float dl = -(Cv + alpha * lambda) / den;
-                    s.edgeLambda[e] = lambda + dl;
-                    cA = mk4(wA * dl * gA * relax, 0.0f);
-                    cB = mk4(wB * dl * gB * relax, 0.0f);
-                }
+    const cn_soft_edge ed = s.edges[e];
+    const float lambda = s.edgeLambda[e]; // with the record: one round trip fewer
+    float4 cA = make_float4(0.f, 0.f, 0.f, 0.f), cB = cA;
+    if (ed.enabled != 0u) {
+        const float4 a = s.x[ed.particle_a], b = s.x[ed.particle_b];
+        const float wA = a.w, wB = b.w, wSum = wA + wB;
+        const f3 delta = xyz(b) - xyz(a);
+        const float l2 = dot(delta, delta);
+        if (wSum > kEps && l2 > kEps) {
+            const float len = sqrtf(l2);
+            const f3 gA = -delta / len;
+            const f3 gB = -gA;
+            const float alpha = mx(ed.compliance, 0.0f) / mx(dt * dt, kEps);
+            const float Cv = len - ed.rest_length;
+            const float den = wSum + alpha;
+            if (den > kEps) {
+                const float dl = -(Cv + alpha * lambda) / den;
+                s.edgeLambda[e] = lambda + dl;
+                cA = mk4(wA * dl * gA * relax, 0.0f);
+                cB = mk4(wB * dl * gB * relax, 0.0f);
             }
         }
-        s.edgeCorr[2 * e] = cA;
-        s.edgeCorr[2 * e + 1] = cB;
-    });
+    }
+    s.edgeCorr[2 * e] = cA;
+    s.edgeCorr[2 * e + 1] = cB;
+}
+
+__global__ void __launch_bounds__(kThreads) k_solveEdges(Scene s, float dt, float relax)
+{
+    forEachElem(s.wE, s.E, [&](uint32_t e) { solveEdge(s, dt, relax, e); });
+}
+
+// Gather of per-constraint correction records in incidence (constraint) order.  The range is
+// loaded together with the position, not after the mass test, and the records are fetched
+// kGatherBatch at a time (all incidence loads, then all record loads) before they are summed in
+// list order: the sum is the one-at-a-time sum, with three memory round trips per batch fewer.
+constexpr uint32_t kGatherBatch = 8u;
+
+template <uint32_t kRecords>
+__device__ __forceinline__ void applyGatherAt(const Scene &s, const uint2 *ranges, const uint2 *inc,
+                                              const float4 *corr, uint32_t i)
+{
+    const float4 p = s.x[i];
+    const uint2 r = ranges[i];
+    if (p.w <= kEps) return;
+    f3 total{0.f, 0.f, 0.f};
+    for (uint32_t k = 0; k < r.y; k += kGatherBatch) {
+        uint32_t slot[kGatherBatch];
+#pragma unroll
+        for (uint32_t j = 0; j < kGatherBatch; ++j) {
+            slot[j] = 0u;
+            if (k + j < r.y) {
+                const uint2 ref = inc[r.x + k + j];
+                slot[j] = kRecords == 2u ? 2u * ref.x + (ref.y == 0u ? 0u : 1u)
+                                         : 4u * ref.x + (ref.y > 3u ? 3u : ref.y);
+            }
+        }
+        float4 c[kGatherBatch];
+#pragma unroll
+        for (uint32_t j = 0; j < kGatherBatch; ++j)
+            if (k + j < r.y) c[j] = corr[slot[j]];
+#pragma unroll
+        for (uint32_t j = 0; j < kGatherBatch; ++j)
+            if (k + j < r.y) total += xyz(c[j]);
+    }
+    s.x[i] = mk4(xyz(p) + total, p.w);
 }
 
 // physics_soft_apply_edge_corrections.cs.hlsl:9-35 (also the strand distance apply:
 // physics_strand_apply_distance_corrections.cs.hlsl:9-38)
+__device__ __forceinline__ void applyPairAt(const Scene &s, const uint2 *ranges, const uint2 *inc, const float4 *corr, uint32_t i)
+{
+    applyGatherAt<2u>(s, ranges, inc, corr, i);
+}
+
 __global__ void __launch_bounds__(kThreads) k_applyPair(Scene s, const uint2 *ranges, const uint2 *inc,
                                                         const float4 *corr)
 {
-    forEachElem(s.wP, s.N, [&](uint32_t i) {
-        const float4 p = s.x[i];
-        if (p.w <= kEps) return;
-        const uint2 r = ranges[i];
-        f3 total{0.f, 0.f, 0.f};
-        for (uint32_t k = 0; k < r.y; ++k) {
-            const uint2 ref = inc[r.x + k];
-            total += xyz(corr[2 * ref.x + (ref.y == 0u ? 0u : 1u)]);
-        }
-        s.x[i] = mk4(xyz(p) + total, p.w);
-    });
+    forEachElem(s.wP, s.N, [&](uint32_t i) { applyPairAt(s, ranges, inc, corr, i); });
 }
 
 // physics_soft_apply_tet_corrections.cs.hlsl:9-50, physics_soft_apply_bend_corrections.cs.hlsl:9-51
+__device__ __forceinline__ void applyQuadAt(const Scene &s, const uint2 *ranges, const uint2 *inc, const float4 *corr, uint32_t i)
+{
+    applyGatherAt<4u>(s, ranges, inc, corr, i);
+}
+
 __global__ void __launch_bounds__(kThreads) k_applyQuad(Scene s, const uint2 *ranges, const uint2 *inc,
                                                         const float4 *corr)
 {
-    forEachElem(s.wP, s.N, [&](uint32_t i) {
-        const float4 p = s.x[i];
-        if (p.w <= kEps) return;
-        const uint2 r = ranges[i];
-        f3 total{0.f, 0.f, 0.f};
-        for (uint32_t k = 0; k < r.y; ++k) {
-            const uint2 ref = inc[r.x + k];
-            total += xyz(corr[4 * ref.x + (ref.y > 3u ? 3u : ref.y)]);
-        }
-        s.x[i] = mk4(xyz(p) + total, p.w);
-    });
+    forEachElem(s.wP, s.N, [&](uint32_t i) { applyQuadAt(s, ranges, inc, corr, i); });
 }
 
 // physics_soft_solve_tet_constraints.cs.hlsl:15-87
+__device__ __forceinline__ void solveTet(const Scene &s, float dt, float relax, uint32_t t)
+{
+    const cn_soft_tet tet = s.tets[t];
+    const float lambda = s.tetLambda[t]; // with the record: one round trip fewer
+    const float4 q0 = s.x[tet.particle_indices[0]], q1 = s.x[tet.particle_indices[1]];
+    const float4 q2 = s.x[tet.particle_indices[2]], q3 = s.x[tet.particle_indices[3]];
+    const float w0 = q0.w, w1 = q1.w, w2 = q2.w, w3 = q3.w;
+    if ((w0 + w1 + w2 + w3) <= kEps) return; // keeps the previous correction record
+    const f3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2), p3 = xyz(q3);
+    const float sv = dot(cross(p1 - p0, p2 - p0), p3 - p0) / 6.0f;
+    const float vs = (sv >= 0.0f) ? 1.0f : -1.0f;
+    const float Cv = fabsf(sv) - mx(tet.rest_volume, 0.0f);
+    const f3 g0 = cross(p3 - p1, p2 - p1) * (vs / 6.0f);
+    const f3 g1 = cross(p2 - p0, p3 - p0) * (vs / 6.0f);
+    const f3 g2 = cross(p3 - p0, p1 - p0) * (vs / 6.0f);
+    const f3 g3 = cross(p1 - p0, p2 - p0) * (vs / 6.0f);
+    const float sg = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
+    const float alpha = mx(tet.compliance, 0.0f) / mx(dt * dt, kEps);
+    const float den = sg + alpha;
+    if (den <= kEps) return;
+    const float dl = -(Cv + alpha * lambda) / den;
+    s.tetLambda[t] = lambda + dl;
+    float4 *out = s.tetCorr + 4 * size_t(t);
+    out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
+    out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
+    out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
+    out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
+}
+
 __global__ void __launch_bounds__(kThreads) k_solveTets(Scene s, float dt, float relax)
 {
-    forEachElem(s.wT, s.T, [&](uint32_t t) {
-        const cn_soft_tet tet = s.tets[t];
-        const float4 q0 = s.x[tet.particle_indices[0]], q1 = s.x[tet.particle_indices[1]];
-        const float4 q2 = s.x[tet.particle_indices[2]], q3 = s.x[tet.particle_indices[3]];
-        const float w0 = q0.w, w1 = q1.w, w2 = q2.w, w3 = q3.w;
-        if ((w0 + w1 + w2 + w3) <= kEps) return; // keeps the previous correction record
-        const f3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2), p3 = xyz(q3);
-        const float sv = dot(cross(p1 - p0, p2 - p0), p3 - p0) / 6.0f;
-        const float vs = (sv >= 0.0f) ? 1.0f : -1.0f;
-        const float Cv = fabsf(sv) - mx(tet.rest_volume, 0.0f);
-        const f3 g0 = cross(p3 - p1, p2 - p1) * (vs / 6.0f);
-        const f3 g1 = cross(p2 - p0, p3 - p0) * (vs / 6.0f);
-        const f3 g2 = cross(p3 - p0, p1 - p0) * (vs / 6.0f);
-        const f3 g3 = cross(p1 - p0, p2 - p0) * (vs / 6.0f);
-        const float sg = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
-        const float alpha = mx(tet.compliance, 0.0f) / mx(dt * dt, kEps);
-        const float lambda = s.tetLambda[t];
-        const float den = sg + alpha;
-        if (den <= kEps) return;
-        const float dl = -(Cv + alpha * lambda) / den;
-        s.tetLambda[t] = lambda + dl;
-        float4 *out = s.tetCorr + 4 * size_t(t);
-        out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
-        out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
-        out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
-        out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
-    });
+    forEachElem(s.wT, s.T, [&](uint32_t t) { solveTet(s, dt, relax, t); });
 }
 
 // physics_soft_solve_bend_constraints.cs.hlsl:20-86
@@ -1466,13 +1524,36 @@ __global__ void __launch_bounds__(kThreads) k_particleContactSolve(Scene s, Conf
 }
 
 // Particle-rigid contact for candidate pair `pi`: physics_particle_rigid_generate_contacts.cs.hlsl:29-210
-__device__ RigidContact generateRigidContact(const Scene &s, uint32_t i, uint32_t b)
+// Particle-side inputs of a particle's rigid contacts, fetched once before its pair loop (in one
+// memory round trip with the first pair).
+struct ContactParticle {
+    f3 pos, prev;
+    float radius;
+    uint4 meta;
+    float4 material;
+    bool proxy;
+};
+
+__device__ __forceinline__ ContactParticle loadContactParticle(const Scene &s, uint32_t i, float4 x)
+{
+    ContactParticle p;
+    p.pos = xyz(x);
+    p.prev = xyz(s.xprev[i]);
+    p.radius = s.radii[i];
+    p.meta = s.meta[i];
+    p.material = s.contactMaterials[s.matIdx[i]];
+    p.proxy = s.ownerTypes[i] == CN_OWNER_RIGID_BODY;
+    return p;
+}
+
+__device__ __forceinline__ RigidContact generateRigidContact(const Scene &s, uint32_t i, uint32_t b,
+                                                             const ContactParticle &pt)
 {
     RigidContact out{};
-    if (s.ownerTypes[i] == CN_OWNER_RIGID_BODY) return out;
-    const f3 sp = xyz(s.x[i]);
-    const float sr = s.radii[i];
-    const uint4 m = s.meta[i];
+    if (pt.proxy) return out;
+    const f3 sp = pt.pos;
+    const float sr = pt.radius;
+    const uint4 m = pt.meta;
     const f3 bpos = xyz(s.predBodyPos[b]);
     const float4 bq = qNormalize(s.predBodyRot[b]);
     const float4 bsc = s.bodyScale[b];
@@ -1484,9 +1565,9 @@ __device__ RigidContact generateRigidContact(const Scene &s, uint32_t i, uint32_
         if (k >= cr.y) break;
         const uint32_t c = s.bodyColIdx[cr.x + k];
         const cn_collider_broadphase bp = s.colBp[c];
+        const cn_collider_geometry cg = s.colGeo[c]; // before the filter: same round trip as bp
         if (bp.enabled_flag == 0u || bp.environment_index != m.x) continue;
         if ((m.w & bp.collision_layer) == 0u || (bp.collision_mask & m.z) == 0u) continue;
-        const cn_collider_geometry cg = s.colGeo[c];
         const f3 clp{cg.local_position[0], cg.local_position[1], cg.local_position[2]};
         const float4 clq = qNormalize(make_float4(cg.local_orientation[0], cg.local_orientation[1],
                                                   cg.local_orientation[2], cg.local_orientation[3]));
@@ -1554,11 +1635,12 @@ __device__ RigidContact generateRigidContact(const Scene &s, uint32_t i, uint32_
 
 // physics_particle_rigid_solve_contacts.cs.hlsl:27-141 for one contact (static/kinematic body:
 // only the particle moves).
-__device__ f3 solveRigidContact(const Scene &s, const Config &cfg, const RigidContact &c, float4 sp)
+__device__ __forceinline__ f3 solveRigidContact(const Scene &s, const Config &cfg, const RigidContact &c, float4 sp,
+                                                const ContactParticle &pt)
 {
-    const uint32_t i = c.particle, b = c.body;
+    const uint32_t b = c.body;
     const float iS = sp.w;
-    const f3 prevS = xyz(s.xprev[i]);
+    const f3 prevS = pt.prev;
     const float4 prevB = s.prevBodyPos[b], predB = s.predBodyPos[b];
     const float4 prevQ = qNormalize(s.prevBodyRot[b]), predQ = qNormalize(s.predBodyRot[b]);
     const float iR = s.bodyType[b] == CN_BODY_DYNAMIC ? predB.w : 0.0f;
@@ -1567,7 +1649,7 @@ __device__ f3 solveRigidContact(const Scene &s, const Config &cfg, const RigidCo
     if (pen <= 0.0f) return f3{0.f, 0.f, 0.f};
     const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
     f3 inI = xyz(s.bodyInvInertia[b]);
-    const f3 mat = combineContactMaterial(s.contactMaterials[s.matIdx[i]], s.colMat[c.collider]);
+    const f3 mat = combineContactMaterial(pt.material, s.colMat[c.collider]);
     if (iR <= kEps) inI = f3{0.f, 0.f, 0.f};
     const f3 prevCP = xyz(prevB) + qRotate(prevQ, xyz(c.rigidLocalPoint));
     const f3 cp = xyz(predB) + qRotate(predQ, xyz(c.rigidLocalPoint));
@@ -1597,41 +1679,45 @@ __device__ f3 solveRigidContact(const Scene &s, const Config &cfg, const RigidCo
 // Generate + solve every candidate pair of particle i (pairs are particle-major), then either
 // accumulate into posCorr (explicit contacts present) or apply directly
 // (physics_particle_apply_position_corrections.cs.hlsl:8-30).
-__global__ void __launch_bounds__(kThreads) k_rigidContacts(Scene s, Config cfg, bool applyDirect)
+__device__ __forceinline__ void rigidContactsAt(const Scene &s, const Config &cfg, bool applyDirect, uint32_t i)
 {
-    forEachElem(s.wP, s.N, [&](uint32_t i) {
-        const uint32_t cnt = s.candCount[i];
-        const float4 sp = s.x[i];
-        f3 corr{0.f, 0.f, 0.f};
-        bool any = false;
-        if (cnt) {
-            const uint32_t off = s.candOffset[i];
-            const uint32_t lim = s.meta_->rigidPairCount;
-            for (uint32_t k = 0; k < cnt; ++k) {
-                const uint32_t pi = off + k;
-                if (pi >= lim) break;
-                const uint2 pr = s.rigidPairs[pi];
-                const RigidContact c = generateRigidContact(s, pr.x, pr.y);
-                s.rigidContacts[pi] = c;
-                if (!c.active) continue;
-                const f3 d = solveRigidContact(s, cfg, c, sp);
-                // float atomic order of the reference == pair order here
-                if (sp.w > kEps) {
-                    corr = corr + d;
-                    any = true;
-                }
+    const uint32_t cnt = s.candCount[i];
+    const uint32_t off = s.candOffset[i]; // with the count: one round trip fewer
+    const float4 sp = s.x[i];
+    f3 corr{0.f, 0.f, 0.f};
+    bool any = false;
+    if (cnt) {
+        const uint32_t lim = s.meta_->rigidPairCount;
+        const ContactParticle pt = loadContactParticle(s, i, sp);
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t pi = off + k;
+            if (pi >= lim) break;
+            const uint2 pr = s.rigidPairs[pi]; // pr.x == i: pairs are emitted particle-major
+            const RigidContact c = generateRigidContact(s, i, pr.y, pt);
+            s.rigidContacts[pi] = c;
+            if (!c.active) continue;
+            const f3 d = solveRigidContact(s, cfg, c, sp, pt);
+            // float atomic order of the reference == pair order here
+            if (sp.w > kEps) {
+                corr = corr + d;
+                any = true;
             }
         }
-        if (applyDirect) {
-            // applyParticlePositionCorrections with an accumulator that only this pass wrote
-            if (sp.w <= kEps) return;
-            s.x[i] = mk4(xyz(sp) + corr, sp.w);
-        } else if (any) {
-            float4 pc = s.posCorr[i];
-            pc = mk4(xyz(pc) + corr, pc.w);
-            s.posCorr[i] = pc;
-        }
-    });
+    }
+    if (applyDirect) {
+        // applyParticlePositionCorrections with an accumulator that only this pass wrote
+        if (sp.w <= kEps) return;
+        s.x[i] = mk4(xyz(sp) + corr, sp.w);
+    } else if (any) {
+        float4 pc = s.posCorr[i];
+        pc = mk4(xyz(pc) + corr, pc.w);
+        s.posCorr[i] = pc;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_rigidContacts(Scene s, Config cfg, bool applyDirect)
+{
+    forEachElem(s.wP, s.N, [&](uint32_t i) { rigidContactsAt(s, cfg, applyDirect, i); });
 }
 
 // physics_particle_apply_position_corrections.cs.hlsl:8-30
@@ -1651,24 +1737,29 @@ __global__ void __launch_bounds__(kThreads) k_applyPositionCorrections(Scene s)
 // ------------------------------------------------------------------------------------------
 // physics_particle_update_velocities.cs.hlsl:13-44 (the fluid accumulated delta lives at the
 // particle's sorted slot)
+__device__ __forceinline__ void updateVelocityAt(const Scene &s, float dt, const float4 *Dfinal, uint32_t i)
+{
+    const float4 p = s.x[i];
+    const float4 prev = s.xprev[i];      // loaded with x (not after the mass test):
+    const uint32_t mi = s.matIdx[i];     // one round trip fewer
+    if (p.w <= kEps || dt <= kEps) {
+        s.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const f3 pp = xyz(prev);
+    f3 pos = xyz(p);
+    if (Dfinal && s.kinds[i] == CN_PARTICLE_FLUID) {
+        pos += xyz(Dfinal[s.rank[i]]);
+        s.x[i] = mk4(pos, p.w);
+    }
+    const float damping = mx(s.contactMaterials[mi].z, 0.0f);
+    const float ds = mx(1.0f - damping * dt, 0.0f);
+    s.v[i] = mk4(((pos - pp) / dt) * ds, 0.0f);
+}
+
 __global__ void __launch_bounds__(kThreads) k_updateVelocities(Scene s, float dt, const float4 *Dfinal)
 {
-    forEachElem(s.wP, s.N, [&](uint32_t i) {
-        const float4 p = s.x[i];
-        if (p.w <= kEps || dt <= kEps) {
-            s.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            return;
-        }
-        const f3 pp = xyz(s.xprev[i]);
-        f3 pos = xyz(p);
-        if (Dfinal && s.kinds[i] == CN_PARTICLE_FLUID) {
-            pos += xyz(Dfinal[s.rank[i]]);
-            s.x[i] = mk4(pos, p.w);
-        }
-        const float damping = mx(s.contactMaterials[s.matIdx[i]].z, 0.0f);
-        const float ds = mx(1.0f - damping * dt, 0.0f);
-        s.v[i] = mk4(((pos - pp) / dt) * ds, 0.0f);
-    });
+    forEachElem(s.wP, s.N, [&](uint32_t i) { updateVelocityAt(s, dt, Dfinal, i); });
 }
 
 // physics_fluid_project_boundary_velocities.cs.hlsl:24-117
@@ -1724,51 +1815,55 @@ __global__ void __launch_bounds__(kThreads) k_fluidBoundaryVelocities(Scene s, f
 // physics_particle_rigid_solve_contact_velocities.cs.hlsl + apply_contact_velocities.cs.hlsl for
 // all `iterations` at once: with static/kinematic bodies each particle's velocity only depends
 // on its own contacts, and the per-particle sum runs in contact order.
+__device__ __forceinline__ void rigidContactVelocitiesAt(const Scene &s, uint32_t iterations, const Config &cfg, uint32_t i)
+{
+    const uint32_t cnt = s.candCount[i];
+    const uint32_t off = s.candOffset[i]; // with the count: one round trip fewer
+    if (cnt == 0u) return;
+    const float iS = s.x[i].w;
+    const float4 v0 = s.v[i];
+    if (iS <= kEps) return; // corrections are only applied to particles with mass
+    const uint32_t lim = s.meta_->rigidPairCount;
+    const float rpt = cfg.restitutionPenetrationThreshold;
+    f3 vel = xyz(v0);
+    const float vw = v0.w;
+    for (uint32_t it = 0; it < iterations; ++it) {
+        f3 corr{0.f, 0.f, 0.f};
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t pi = off + k;
+            if (pi >= lim) break;
+            const RigidContact c = s.rigidContacts[pi];
+            if (!c.active) continue;
+            const uint32_t b = c.body;
+            const float4 rp = s.predBodyPos[b];
+            const float iR = s.bodyType[b] == CN_BODY_DYNAMIC ? rp.w : 0.0f;
+            const float4 rq = qNormalize(s.predBodyRot[b]);
+            const f3 rl = xyz(s.predBodyLin[b]), ra = xyz(s.predBodyAng[b]);
+            const f3 inI = xyz(s.bodyInvInertia[b]);
+            const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
+            const f3 cp = xyz(rp) + qRotate(rq, xyz(c.rigidLocalPoint));
+            const f3 rR = cp - xyz(rp);
+            const f3 rcv = rl + cross(ra, rR);
+            const f3 rel = vel - rcv;
+            const float nv = dot(rel, n);
+            if (nv >= 0.0f) continue;
+            const float nd = iS + contactEffectiveMass(iR, inI, rq, rR, n);
+            if (nd <= kEps) continue;
+            const f3 mat = combineContactMaterial(s.contactMaterials[s.matIdx[i]], s.colMat[c.collider]);
+            const bool er = (-nv > cfg.restitutionVelocityThreshold) && (c.normalPenetration.w <= rpt);
+            const float rest = er ? saturate(mat.y) : 0.0f;
+            const float dnv = er ? (-rest * nv) : 0.0f;
+            const float imp = mx(0.0f, (dnv - nv) / nd);
+            corr = corr + (n * imp) * iS;
+        }
+        vel = vel + corr;
+    }
+    s.v[i] = mk4(vel, vw);
+}
+
 __global__ void __launch_bounds__(kThreads) k_rigidContactVelocities(Scene s, uint32_t iterations, Config cfg)
 {
-    forEachElem(s.wP, s.N, [&](uint32_t i) {
-        const uint32_t cnt = s.candCount[i];
-        if (cnt == 0u) return;
-        const float iS = s.x[i].w;
-        if (iS <= kEps) return; // corrections are only applied to particles with mass
-        const uint32_t off = s.candOffset[i];
-        const uint32_t lim = s.meta_->rigidPairCount;
-        const float rpt = cfg.restitutionPenetrationThreshold;
-        f3 vel = xyz(s.v[i]);
-        const float vw = s.v[i].w;
-        for (uint32_t it = 0; it < iterations; ++it) {
-            f3 corr{0.f, 0.f, 0.f};
-            for (uint32_t k = 0; k < cnt; ++k) {
-                const uint32_t pi = off + k;
-                if (pi >= lim) break;
-                const RigidContact c = s.rigidContacts[pi];
-                if (!c.active) continue;
-                const uint32_t b = c.body;
-                const float4 rp = s.predBodyPos[b];
-                const float iR = s.bodyType[b] == CN_BODY_DYNAMIC ? rp.w : 0.0f;
-                const float4 rq = qNormalize(s.predBodyRot[b]);
-                const f3 rl = xyz(s.predBodyLin[b]), ra = xyz(s.predBodyAng[b]);
-                const f3 inI = xyz(s.bodyInvInertia[b]);
-                const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
-                const f3 cp = xyz(rp) + qRotate(rq, xyz(c.rigidLocalPoint));
-                const f3 rR = cp - xyz(rp);
-                const f3 rcv = rl + cross(ra, rR);
-                const f3 rel = vel - rcv;
-                const float nv = dot(rel, n);
-                if (nv >= 0.0f) continue;
-                const float nd = iS + contactEffectiveMass(iR, inI, rq, rR, n);
-                if (nd <= kEps) continue;
-                const f3 mat = combineContactMaterial(s.contactMaterials[s.matIdx[i]], s.colMat[c.collider]);
-                const bool er = (-nv > cfg.restitutionVelocityThreshold) && (c.normalPenetration.w <= rpt);
-                const float rest = er ? saturate(mat.y) : 0.0f;
-                const float dnv = er ? (-rest * nv) : 0.0f;
-                const float imp = mx(0.0f, (dnv - nv) / nd);
-                corr = corr + (n * imp) * iS;
-            }
-            vel = vel + corr;
-        }
-        s.v[i] = mk4(vel, vw);
-    });
+    forEachElem(s.wP, s.N, [&](uint32_t i) { rigidContactVelocitiesAt(s, iterations, cfg, i); });
 }
 
 // physics_particle_solve_contact_velocities.cs.hlsl (non-proxy) with float atomics.

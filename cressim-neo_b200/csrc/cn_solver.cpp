@@ -1002,14 +1002,21 @@ CN_API cn_status cn_solver_debug_read(cn_solver *sv, cn_debug_buffer which, void
     }
     case CN_DEBUG_RIGID_CONTACTS: {
         if (!s.rigidContacts) { buf.clear(); break; }
-        cn::DeviceMeta m{};
-        CN_CUDA(cudaMemcpy(&m, s.meta_, sizeof(m), cudaMemcpyDeviceToHost));
-        std::vector<uint8_t> c;
-        CN_CUDA(fetch(s.rigidContacts, sizeof(cn::RigidContact) * m.rigidPairCount, c));
+        std::vector<uint8_t> c, cnt, off;
+        CN_CUDA(fetch(s.rigidContacts, sizeof(cn::RigidContact) * s.rigidPairCapacity, c));
+        CN_CUDA(fetch(s.candCount, sizeof(uint32_t) * N, cnt));
+        CN_CUDA(fetch(s.candOffset, sizeof(uint32_t) * N, off));
         const cn::RigidContact *cc = reinterpret_cast<const cn::RigidContact *>(c.data());
-        for (uint32_t k = 0; k < m.rigidPairCount; ++k)
-            if (cc[k].active) {
-                const uint8_t *b = reinterpret_cast<const uint8_t *>(&cc[k]);
+        const uint32_t *pc = reinterpret_cast<const uint32_t *>(cnt.data());
+        const uint32_t *po = reinterpret_cast<const uint32_t *>(off.data());
+        // particle-major pair order; the pairs of a particle sit at its offset in either layout
+        // (scanned offsets or fixed slots)
+        for (uint32_t p = 0; p < N; ++p)
+            for (uint32_t k = 0; k < pc[p]; ++k) {
+                const uint32_t pi = po[p] + k;
+                if (pi >= s.rigidPairCapacity) break; // dropped by a full pair buffer
+                if (!cc[pi].active) continue;
+                const uint8_t *b = reinterpret_cast<const uint8_t *>(&cc[pi]);
                 buf.insert(buf.end(), b, b + sizeof(cn::RigidContact));
             }
         break;
