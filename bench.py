@@ -477,12 +477,31 @@ def run_other_configs(stream, sh, cpu: bool = True) -> dict:
     ms = timed(sv, dt, 10, tool)
     meta = sv.validate_gpu_meta()
     n = soa.particle_count
+    # surface render passes (skinning, normals, bounds) of the frame, from the event probes
+    sv.set_timing(True)
+    surf_ms = 0.0
+    for k in range(3):
+        sv.set_kinematic_target(tool, scenes.tool_path(dt * (k + 20)))
+        sv.step_many(dt, 1, sh)
+        surf_ms += sv.kernel_times().get("surface_render", (0.0, 0))[0] / 3
+    sv.set_timing(False)
+    sr = soa.surface_render.contents
+    V, T, I = sr.vertex_count, sr.triangle_count, sr.vertex_triangle_index_count
+    surf_particles = sum(int(sr.surface_particle_ranges[2 * k + 1]) for k in range(sr.surface_count))
+    chunks = sum((int(sr.surface_particle_ranges[2 * k + 1]) + 63) // 64 for k in range(sr.surface_count))
+    # binding 32 + 4 gathered positions + output per vertex; 3 gathered positions + indices + output
+    # per triangle; range + incident index and face normal + output per vertex; positions + chunk
+    # and surface AABBs for the bounds
+    surf_bytes = V * 112 + T * 80 + V * 32 + I * 20 + surf_particles * 16 + chunks * 64 + sr.surface_count * 32
     out["mixed_surgical"] = {
         "workload": f"mixed: {c['tets']} tets, {c['dihedrals']} dihedrals, {c['segments']} "
                     f"strand segments, {n} particles in all (tissue, cloth, strands, 64^3 fluid), kinematic capsule, "
                     f"{desc.substeps} substeps x {desc.default_iterations} iterations, dt 1/60",
         "value": round(n * desc.substeps / (ms / 1e3), 1), "unit": "particle-substeps/s",
-        "ms_per_frame": round(ms, 3), "meta_status": meta["status"]}
+        "ms_per_frame": round(ms, 3), "meta_status": meta["status"],
+        "surface_render": {"render_vertices": V, "render_triangles": T, "surfaces": sr.surface_count,
+                           "ms_per_frame": round(surf_ms, 4), "algorithmic_bytes": surf_bytes,
+                           "achieved_gbs": round(surf_bytes / max(surf_ms, 1e-6) / 1e6, 1)}}
     sv.close()
     return out
 

@@ -276,6 +276,58 @@ class World:
         _check(self._lib.cn_world_add_collider(self._h, C.byref(d), C.byref(out)))
         return out.value
 
+    def add_surface_mesh(self, owner: str, index: int, positions, indices, normals=None,
+                         match_epsilon: float = 1.0e-3) -> int:
+        """Binds a render mesh to soft body / cloth `index` (owner "soft_body" or "cloth"): (V, 3)
+        positions in the owner's object frame, (F, 3) triangle indices, optional (V, 3) fallback
+        normals.  Returns the mesh's first render vertex in the packed render arrays."""
+        pos = np.ascontiguousarray(np.asarray(positions, dtype=np.float32).reshape(-1, 3))
+        idx = np.ascontiguousarray(np.asarray(indices, dtype=np.uint32).reshape(-1))
+        nrm = None if normals is None else np.ascontiguousarray(np.asarray(normals, dtype=np.float32).reshape(-1, 3))
+        d = _abi.SurfaceMeshDesc()
+        self._lib.cn_surface_mesh_desc_defaults(C.byref(d))
+        d.owner_kind = {"soft_body": 0, "cloth": 1}[owner]
+        d.owner_index = index
+        d.vertex_count = pos.shape[0]
+        d.positions = _f32(pos)
+        d.normals = _f32(nrm) if nrm is not None else None
+        d.index_count = idx.size
+        d.indices = _u32(idx) if idx.size else None
+        d.match_epsilon = match_epsilon
+        out = C.c_uint32()
+        _check(self._lib.cn_world_add_surface_mesh(self._h, C.byref(d), C.byref(out)))
+        return out.value
+
+    def set_surface_render(self, bindings, fallback_normals, triangle_ranges, triangle_indices, triangles,
+                           surface_ranges) -> None:
+        """PhysicsWorld::setSurfaceDeformableRenderData with caller-built arrays: bindings (V, 8)
+        (4 particle indices as uint32 bits, 4 weights), fallback normals (V, 4), per-vertex
+        (start, count) ranges (V, 2) into triangle_indices, triangles (T, 3) particle indices,
+        surface particle ranges (S, 2).  None restores the meshes added with add_surface_mesh."""
+        if bindings is None:
+            _check(self._lib.cn_world_set_surface_render(self._h, None))
+            return
+        b = np.ascontiguousarray(np.asarray(bindings).view(np.uint32).reshape(-1, 8))
+        fn = np.ascontiguousarray(np.asarray(fallback_normals, dtype=np.float32).reshape(-1, 4))
+        rg = np.zeros((b.shape[0], 4), np.uint32)
+        rg[:, :2] = np.asarray(triangle_ranges, dtype=np.uint32).reshape(-1, 2)
+        ti = np.ascontiguousarray(np.asarray(triangle_indices, dtype=np.uint32).reshape(-1))
+        tr = np.zeros((np.asarray(triangles).reshape(-1, 3).shape[0], 4), np.uint32)
+        tr[:, :3] = np.asarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        sr = np.ascontiguousarray(np.asarray(surface_ranges, dtype=np.uint32).reshape(-1, 2))
+        d = _abi.SurfaceRenderData()
+        d.vertex_count = b.shape[0]
+        d.vertex_bindings = C.cast(b.ctypes.data, C.POINTER(_abi.SurfaceVertexBinding))
+        d.fallback_normals = _f32(fn)
+        d.vertex_triangle_ranges = C.cast(rg.ctypes.data, C.POINTER(_abi.SurfaceTriangleRange))
+        d.vertex_triangle_index_count = ti.size
+        d.vertex_triangle_indices = _u32(ti) if ti.size else None
+        d.triangle_count = tr.shape[0]
+        d.triangle_particle_indices = _u32(tr) if tr.size else None
+        d.surface_count = sr.shape[0]
+        d.surface_particle_ranges = _u32(sr) if sr.size else None
+        _check(self._lib.cn_world_set_surface_render(self._h, C.byref(d)))
+
     def soa(self) -> _abi.WorldSoA:
         s = _abi.WorldSoA()
         _check(self._lib.cn_world_get_soa(self._h, C.byref(s)))
@@ -382,6 +434,21 @@ class Solver:
         _check(self._lib.cn_solver_kernel_times(self._h, arr, n.value, C.byref(n)))
         return {arr[i].name.decode(): (arr[i].milliseconds, arr[i].launches) for i in range(n.value)}
 
+    def read_surface_render(self):
+        """(render positions V x 4, render normals V x 4, surface world AABBs S x 8) after the last frame."""
+        v = _abi.SurfaceRenderView()
+        _check(self._lib.cn_solver_surface_render_view(self._h, C.byref(v)))
+        pos = np.zeros((v.vertex_count, 4), np.float32)
+        nrm = np.zeros((v.vertex_count, 4), np.float32)
+        box = np.zeros((v.surface_count, 8), np.float32)
+        _check(self._lib.cn_solver_read_surface_render(self._h, pos.ctypes.data, nrm.ctypes.data, box.ctypes.data))
+        return pos, nrm, box
+
+    def surface_render_view(self) -> dict:
+        v = _abi.SurfaceRenderView()
+        _check(self._lib.cn_solver_surface_render_view(self._h, C.byref(v)))
+        return {name: getattr(v, name) for name, _ in _abi.SurfaceRenderView._fields_}
+
     def graph_stats(self) -> tuple:
         k, t = C.c_uint32(), C.c_uint32()
         _check(self._lib.cn_solver_graph_stats(self._h, C.byref(k), C.byref(t)))
@@ -403,7 +470,8 @@ class Solver:
         new_capsule.argtypes = [C.c_void_p, C.c_char_p, C.c_void_p]
         return torch.utils.dlpack.from_dlpack(new_capsule(ptr, b"dltensor", None))
 
-    SYNC = {"particle_state": 1, "particle_attributes": 2, "constraints": 4, "rigid_bodies": 8, "colliders": 16}
+    SYNC = {"particle_state": 1, "particle_attributes": 2, "constraints": 4, "rigid_bodies": 8, "colliders": 16,
+            "surface_render": 32}
 
     def update_world(self, world: "World | _abi.WorldSoA", *categories: str) -> None:
         """Uploads the named categories (SYNC keys; all when none is named) into the existing

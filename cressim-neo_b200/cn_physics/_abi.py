@@ -55,6 +55,35 @@ class FluidMaterial(C.Structure):
         "vorticity_confinement", "gravity_scale", "cfl_radius")]
 
 
+class SurfaceVertexBinding(C.Structure):
+    _fields_ = [("particle_indices", u32 * 4), ("weights", f32 * 4)]
+
+
+class SurfaceTriangleRange(C.Structure):
+    _fields_ = [("start", u32), ("count", u32), ("reserved0", u32), ("reserved1", u32)]
+
+
+class SurfaceRenderData(C.Structure):
+    _fields_ = [
+        ("vertex_count", u32), ("vertex_bindings", C.POINTER(SurfaceVertexBinding)), ("fallback_normals", P_f32),
+        ("vertex_triangle_ranges", C.POINTER(SurfaceTriangleRange)), ("vertex_triangle_index_count", u32),
+        ("vertex_triangle_indices", P_u32), ("triangle_count", u32), ("triangle_particle_indices", P_u32),
+        ("surface_count", u32), ("surface_particle_ranges", P_u32)]
+
+
+class SurfaceMeshDesc(C.Structure):
+    _fields_ = [("owner_kind", u32), ("owner_index", u32), ("vertex_count", u32), ("positions", P_f32),
+                ("normals", P_f32), ("index_count", u32), ("indices", P_u32), ("match_epsilon", f32),
+                ("reserved", u32 * 3)]
+
+
+class SurfaceRenderView(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("render_positions", "render_normals", "triangle_normals", "chunk_aabbs",
+                                           "world_aabbs")] + [
+        (n, u32) for n in ("vertex_count", "triangle_count", "chunk_count", "surface_count")] + [
+        ("binding_generation", C.c_uint64)]
+
+
 class WorldSoA(C.Structure):
     _fields_ = [
         ("particle_count", u32), ("positions_inv_mass", P_f32), ("velocities", P_f32), ("radii", P_f32),
@@ -79,7 +108,7 @@ class WorldSoA(C.Structure):
         ("body_kinematic_target_flags", P_u32), ("body_collider_ranges", P_u32),
         ("body_collider_indices", P_u32), ("body_collider_index_count", u32),
         ("collider_count", u32), ("collider_geometry", C.c_void_p), ("collider_broadphase", C.c_void_p),
-        ("collider_materials", P_f32),
+        ("collider_materials", P_f32), ("surface_render", C.POINTER(SurfaceRenderData)),
     ]
 
 
@@ -241,6 +270,11 @@ SIGNATURES = [
     ("cn_solver_set_gravity", C.c_int, [C.c_void_p, f32, f32, f32]),
     ("cn_solver_set_kinematic_target", C.c_int, [C.c_void_p, u32, P_f32, P_f32]),
     ("cn_solver_scene_view", C.c_int, [C.c_void_p, C.POINTER(SceneView)]),
+    ("cn_solver_surface_render_view", C.c_int, [C.c_void_p, C.POINTER(SurfaceRenderView)]),
+    ("cn_solver_read_surface_render", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("cn_surface_mesh_desc_defaults", None, [C.POINTER(SurfaceMeshDesc)]),
+    ("cn_world_add_surface_mesh", C.c_int, [C.c_void_p, C.POINTER(SurfaceMeshDesc), C.POINTER(u32)]),
+    ("cn_world_set_surface_render", C.c_int, [C.c_void_p, C.POINTER(SurfaceRenderData)]),
     ("cn_solver_read_particles", C.c_int, [C.c_void_p, P_f32, P_f32, P_f32, u32]),
     ("cn_solver_write_particles", C.c_int, [C.c_void_p, P_f32, P_f32, u32]),
     ("cn_solver_read_strand_orientations", C.c_int, [C.c_void_p, P_f32, u32]),

@@ -9,7 +9,8 @@ shapes and value ranges of the configurations it stands for.
 * ``dam_break``   -- plain PBF dam break: 128x64x128 fluid lattice (1,048,576 particles) at spacing
                      0.05 (h = 0.1, radius 0.03) in a 12.8 x 6.4 x 25.6 box of static walls,
                      viscosity 0.01, vorticity off, jitter +-1e-4.
-* ``mixed_surgical`` -- tissue lattice + cloth + strands + fluid block + a kinematic capsule tool.
+* ``mixed_surgical`` -- tissue lattice + cloth + strands + fluid block + a kinematic capsule tool,
+                        render meshes on the tissue and the cloth.
 """
 from __future__ import annotations
 
@@ -26,6 +27,52 @@ def _jitter(world: World, amplitude: float, seed: int) -> None:
     movable = x[:, 3] > 0.0
     j = rng.uniform(-amplitude, amplitude, size=(x.shape[0], 3)).astype(np.float32)
     x[movable, :3] += j[movable]
+
+
+def grid_surface_mesh(size, spacing):
+    """Boundary render mesh of a regular-grid soft body in its object frame: the lattice points of
+    buildRegularGridSource (soft_body_authoring.cpp:81-176) on the six faces, two triangles per
+    face cell wound so that cross(p2 - p0, p1 - p0) (the reference's face normal) points outward.
+    Returns (positions (V, 3), triangles (F, 3), normals (V, 3))."""
+    f = np.float32
+    ext = [max(f(e), f(1e-4)) for e in size]
+    sp = max(f(spacing), f(1e-4))
+    res = [max(2, int(math.ceil(f(e) / sp)) + 1) for e in ext]
+    rx, ry, rz = res
+    coords = [((np.arange(n, dtype=f) / f(n - 1)) - f(0.5)) * e for n, e in zip(res, ext)]
+    index = {}
+    pos, nrm = [], []
+
+    def vid(i, j, k, n):
+        key = (i, j, k)
+        if key not in index:
+            index[key] = len(pos)
+            pos.append((coords[0][i], coords[1][j], coords[2][k]))
+            nrm.append(n)
+        return index[key]
+
+    tris = []
+    # each face: (fixed axis, fixed value index, outward sign)
+    for axis in range(3):
+        for side, sign in ((0, -1.0), (res[axis] - 1, 1.0)):
+            a, b = [d for d in range(3) if d != axis]
+            n = [0.0, 0.0, 0.0]
+            n[axis] = sign
+            for u in range(res[a] - 1):
+                for v in range(res[b] - 1):
+                    corner = []
+                    for du, dv in ((0, 0), (1, 0), (1, 1), (0, 1)):
+                        ijk = [0, 0, 0]
+                        ijk[axis], ijk[a], ijk[b] = side, u + du, v + dv
+                        corner.append(vid(*ijk, tuple(n)))
+                    q0, q1, q2, q3 = corner
+                    # cross(p2 - p0, p1 - p0) along +axis for (q0, q3, q2) when a < b
+                    outward_ccw = (sign > 0) == ((axis == 1))
+                    if outward_ccw:
+                        tris += [(q0, q1, q2), (q0, q2, q3)]
+                    else:
+                        tris += [(q0, q2, q1), (q0, q3, q2)]
+    return np.array(pos, np.float32), np.array(tris, np.uint32), np.array(nrm, np.float32)
 
 
 def ground(world: World, top_y: float = 0.0, half=(50.0, 0.5, 50.0), friction=0.5) -> int:
@@ -90,9 +137,26 @@ def tool_path(t: float, seed: int = 0, center=(0.0, 0.6, 0.0), amplitude=0.3):
     return tuple(p)
 
 
+def cloth_grid_mesh(resolution, size):
+    """Render mesh of a cloth grid in its own frame: one vertex per particle (the identity
+    mapping of world.cpp:3300-3313) and the grid's triangles (v00, v10, v11), (v00, v11, v01)."""
+    nx, ny = max(resolution[0], 2), max(resolution[1], 2)
+    f = np.float32
+    gx = (np.arange(nx, dtype=f) / f(nx - 1) - f(0.5)) * f(size[0])
+    gz = (np.arange(ny, dtype=f) / f(ny - 1) - f(0.5)) * f(size[1])
+    xx, zz = np.meshgrid(gx, gz, indexing="xy")
+    pos = np.stack([xx.ravel(), np.zeros(nx * ny, f), zz.ravel()], 1)
+    j, i = np.meshgrid(np.arange(ny - 1), np.arange(nx - 1), indexing="ij")
+    v00 = (j * nx + i).ravel()
+    v10, v01, v11 = v00 + 1, v00 + nx, v00 + nx + 1
+    tri = np.concatenate([np.stack([v00, v10, v11], 1), np.stack([v00, v11, v01], 1)]).astype(np.uint32)
+    return pos, tri
+
+
 def mixed_surgical(tissue=(60, 30, 60), cloth=(256, 256), strands=(64, 129), fluid=(64, 64, 64),
-                   seed: int = 0):
-    """Tissue lattice + cloth sheet + strands + fluid block + kinematic capsule (r = 0.01).
+                   seed: int = 0, surfaces: bool = True):
+    """Tissue lattice + cloth sheet + strands + fluid block + kinematic capsule (r = 0.01), with
+    render meshes on the tissue (its boundary faces) and the cloth when `surfaces`.
     Returns (world, desc, frame_dt, tool_body)."""
     w = World()
     sp = 0.02
@@ -118,6 +182,11 @@ def mixed_surgical(tissue=(60, 30, 60), cloth=(256, 256), strands=(64, 129), flu
     ground(w)
     tool = w.add_rigid_body("kinematic", position=tool_path(0.0, seed))
     w.add_collider(tool, "capsule", (0.01, 0.1), friction=0.2)
+    if surfaces:
+        pos, tri, nrm = grid_surface_mesh(tsize, sp)
+        w.add_surface_mesh("soft_body", 0, pos, tri, nrm)
+        cpos, ctri = cloth_grid_mesh(cres, csize)
+        w.add_surface_mesh("cloth", 0, cpos, ctri)
     w.soa()
     _jitter(w, 1.0e-4, seed)
     desc = solver_desc(substeps=8, enable_blocking_readback=0)

@@ -128,6 +128,18 @@ struct Scene {
     const uint32_t *colQueryOrder = nullptr; // moving colliders first, then static
     uint32_t colQueryCount = 0, activeMovingCount = 0;
 
+    // ---- surface render passes (physics/soft/render/*), once per frame ----
+    uint32_t surfV = 0, surfT = 0, surfS = 0, surfChunks = 0;
+    const uint4 *surfBind = nullptr;        // 2 per vertex: particle indices, then weights (bits)
+    const float4 *surfFallback = nullptr;   // per vertex
+    const uint4 *surfRanges = nullptr;      // per vertex (start, count, 0, 0) into surfIdx
+    const uint32_t *surfIdx = nullptr;      // incident triangles
+    const uint4 *surfTri = nullptr;         // per triangle (a, b, c, 0)
+    const uint4 *surfChunk = nullptr;       // per 64-particle chunk (surface, start, count, 0)
+    const uint2 *surfChunkRange = nullptr;  // per surface (first chunk, chunk count)
+    float4 *surfPos = nullptr, *surfNrm = nullptr, *surfTriN = nullptr;
+    float4 *surfChunkAabb = nullptr, *surfWorldAabb = nullptr; // (min, max) pairs
+
     // ---- broadphase ----
     int4 *entries = nullptr;          // (cellX, cellY, cellZ, key) per particle
     uint32_t *keysA = nullptr, *keysB = nullptr, *valsA = nullptr, *valsB = nullptr;
@@ -231,6 +243,8 @@ void launchFluidBoundaryVelocities(const Scene &s, float dt, const Config &c, cu
 void launchRigidContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st);
 void launchParticleContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st);
 void launchCopyPredictedRigid(const Scene &s, cudaStream_t st);
+// Skinning, triangle and vertex normals, chunk and surface AABBs from the current positions.
+void launchSurfaceRender(const Scene &s, cudaStream_t st);
 // debug export of the compacted cell-range table (reference layout)
 void launchExportCellRanges(const Scene &s, uint4 *out, uint32_t capacity, uint32_t *scanTmp,
                             size_t scanTmpBytes, cudaStream_t st);

@@ -1930,6 +1930,133 @@ __global__ void k_runCompact(Scene s, const uint32_t *flags, const uint32_t *off
     out[r] = make_uint4(s.keysA[slot], slot, s.cellEnd[slot] & 0x7fffffffu, 0u);
 }
 
+// ------------------------------------------------------------------------------------------
+// Surface render passes: render-vertex skinning, triangle and vertex normals, chunk and surface
+// world AABBs.  They read only the positions the frame ends with, so they run once per frame
+// (the reference dispatches them after every substep; earlier substeps' outputs are overwritten
+// before anyone can read them).
+// ------------------------------------------------------------------------------------------
+// physics_surface_skin_render_vertices.cs.hlsl:14-36 and
+// physics_surface_update_triangle_normals.cs.hlsl:8-24 (one thread covers a vertex and a triangle)
+__global__ void __launch_bounds__(kThreads) k_surfaceSkinTriangles(Scene s)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < s.surfV) {
+        const uint4 pi = s.surfBind[2 * size_t(i)];
+        const uint4 wb = s.surfBind[2 * size_t(i) + 1];
+        const float4 q0 = s.x[pi.x], q1 = s.x[pi.y], q2 = s.x[pi.z], q3 = s.x[pi.w];
+        f3 acc{0.f, 0.f, 0.f};
+        acc += __uint_as_float(wb.x) * xyz(q0);
+        acc += __uint_as_float(wb.y) * xyz(q1);
+        acc += __uint_as_float(wb.z) * xyz(q2);
+        acc += __uint_as_float(wb.w) * xyz(q3);
+        s.surfPos[i] = mk4(acc, 1.0f);
+    }
+    if (i < s.surfT) {
+        const uint4 t = s.surfTri[i];
+        const f3 p0 = xyz(s.x[t.x]), p1 = xyz(s.x[t.y]), p2 = xyz(s.x[t.z]);
+        s.surfTriN[i] = mk4(cross(p2 - p0, p1 - p0), 0.0f);
+    }
+}
+
+// physics_surface_update_render_normals.cs.hlsl:18-48: incident face normals summed in range
+// order (fetched kGatherBatch at a time), normalised with 1 / sqrt (the shader's rsqrt is the
+// hardware approximation; this is its correctly rounded value), fallback when degenerate.
+__global__ void __launch_bounds__(kThreads) k_surfaceVertexNormals(Scene s)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.surfV) return;
+    const uint4 r = s.surfRanges[i];
+    f3 acc{0.f, 0.f, 0.f};
+    for (uint32_t k = 0; k < r.y; k += kGatherBatch) {
+        uint32_t tri[kGatherBatch];
+#pragma unroll
+        for (uint32_t j = 0; j < kGatherBatch; ++j) tri[j] = (k + j < r.y) ? s.surfIdx[r.x + k + j] : 0u;
+        float4 n[kGatherBatch];
+#pragma unroll
+        for (uint32_t j = 0; j < kGatherBatch; ++j)
+            if (k + j < r.y) n[j] = s.surfTriN[tri[j]];
+#pragma unroll
+        for (uint32_t j = 0; j < kGatherBatch; ++j)
+            if (k + j < r.y) acc += xyz(n[j]);
+    }
+    f3 nrm = acc;
+    const float lenSq = dot(nrm, nrm);
+    if (lenSq <= 1.0e-12f) nrm = xyz(s.surfFallback[i]);
+    else nrm = nrm * (1.0f / sqrtf(lenSq));
+    s.surfNrm[i] = mk4(nrm, 0.0f);
+}
+
+__device__ __forceinline__ void warpMinMax(f3 &mn, f3 &mx3)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn.x = fminf(mn.x, __shfl_xor_sync(0xffffffffu, mn.x, o));
+        mn.y = fminf(mn.y, __shfl_xor_sync(0xffffffffu, mn.y, o));
+        mn.z = fminf(mn.z, __shfl_xor_sync(0xffffffffu, mn.z, o));
+        mx3.x = fmaxf(mx3.x, __shfl_xor_sync(0xffffffffu, mx3.x, o));
+        mx3.y = fmaxf(mx3.y, __shfl_xor_sync(0xffffffffu, mx3.y, o));
+        mx3.z = fmaxf(mx3.z, __shfl_xor_sync(0xffffffffu, mx3.z, o));
+    }
+}
+
+constexpr float kBoundsInit = 3.402823e+38f;
+
+// physics_surface_update_bounds.cs.hlsl:12-65: one warp per 64-particle chunk (min / max are
+// exact, so the reduction order does not matter)
+__global__ void __launch_bounds__(kThreads) k_surfaceChunkBounds(Scene s)
+{
+    const uint32_t c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (c >= s.surfChunks) return; // the whole warp leaves together
+    const uint4 ch = s.surfChunk[c];
+    if (ch.z == 0u) {
+        if (lane == 0u) {
+            s.surfChunkAabb[2 * size_t(c)] = make_float4(0.f, 0.f, 0.f, 0.f);
+            s.surfChunkAabb[2 * size_t(c) + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        return;
+    }
+    f3 mn{kBoundsInit, kBoundsInit, kBoundsInit}, mxv{-kBoundsInit, -kBoundsInit, -kBoundsInit};
+    for (uint32_t k = lane; k < ch.z; k += 32u) {
+        const f3 p = xyz(s.x[ch.y + k]);
+        mn = f3{fminf(mn.x, p.x), fminf(mn.y, p.y), fminf(mn.z, p.z)};
+        mxv = f3{fmaxf(mxv.x, p.x), fmaxf(mxv.y, p.y), fmaxf(mxv.z, p.z)};
+    }
+    warpMinMax(mn, mxv);
+    if (lane == 0u) {
+        s.surfChunkAabb[2 * size_t(c)] = mk4(mn, 0.0f);
+        s.surfChunkAabb[2 * size_t(c) + 1] = mk4(mxv, 0.0f);
+    }
+}
+
+// physics_surface_finalize_bounds.cs.hlsl:12-66: one warp per surface over its chunks
+__global__ void __launch_bounds__(kThreads) k_surfaceWorldBounds(Scene s)
+{
+    const uint32_t sf = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (sf >= s.surfS) return;
+    const uint2 r = s.surfChunkRange[sf];
+    if (r.y == 0u) {
+        if (lane == 0u) {
+            s.surfWorldAabb[2 * size_t(sf)] = make_float4(0.f, 0.f, 0.f, 0.f);
+            s.surfWorldAabb[2 * size_t(sf) + 1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        return;
+    }
+    f3 mn{kBoundsInit, kBoundsInit, kBoundsInit}, mxv{-kBoundsInit, -kBoundsInit, -kBoundsInit};
+    for (uint32_t k = lane; k < r.y; k += 32u) {
+        const f3 a = xyz(s.surfChunkAabb[2 * size_t(r.x + k)]), b = xyz(s.surfChunkAabb[2 * size_t(r.x + k) + 1]);
+        mn = f3{fminf(mn.x, a.x), fminf(mn.y, a.y), fminf(mn.z, a.z)};
+        mxv = f3{fmaxf(mxv.x, b.x), fmaxf(mxv.y, b.y), fmaxf(mxv.z, b.z)};
+    }
+    warpMinMax(mn, mxv);
+    if (lane == 0u) {
+        s.surfWorldAabb[2 * size_t(sf)] = mk4(mn, 0.0f);
+        s.surfWorldAabb[2 * size_t(sf) + 1] = mk4(mxv, 0.0f);
+    }
+}
+
 } // namespace
 
 // ------------------------------------------------------------------------------ launchers
@@ -2123,6 +2250,17 @@ void launchParticleContactVelocities(const Scene &s, uint32_t iterations, const 
     for (uint32_t it = 0; it < iterations; ++it) {
         k_particleContactVelocities<<<blocksFor(s.particlePairCapacity), kThreads, 0, st>>>(s, c);
         k_applyContactVelocities<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+    }
+}
+
+void launchSurfaceRender(const Scene &s, cudaStream_t st)
+{
+    const uint32_t vt = s.surfV > s.surfT ? s.surfV : s.surfT;
+    if (vt) k_surfaceSkinTriangles<<<blocksFor(vt), kThreads, 0, st>>>(s);
+    if (s.surfV) k_surfaceVertexNormals<<<blocksFor(s.surfV), kThreads, 0, st>>>(s);
+    if (s.surfS) {
+        if (s.surfChunks) k_surfaceChunkBounds<<<blocksFor(size_t(s.surfChunks) * 32u), kThreads, 0, st>>>(s);
+        k_surfaceWorldBounds<<<blocksFor(size_t(s.surfS) * 32u), kThreads, 0, st>>>(s);
     }
 }
 

@@ -62,7 +62,7 @@ struct cn_solver {
     struct Probe { const char *name; cudaEvent_t begin, end; };
     std::vector<Probe> probes;
     uint32_t graphKernelNodes = 0, graphNodes = 0;
-    uint32_t contactMaterialCapacity = 0, fluidMaterialCapacity = 0;
+    uint32_t contactMaterialCapacity = 0, fluidMaterialCapacity = 0, surfIdxCapacity = 0;
 };
 
 namespace {
@@ -185,6 +185,27 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
     s.colAabbMin = a.take<float4>(C); s.colAabbMax = a.take<float4>(C);
     s.colFrame = a.take<float4>(size_t(C) * 4);
     s.colQueryOrder = a.take<uint32_t>(C);
+    {
+        const cn_surface_render_data *sr = w.surface_render;
+        s.surfV = sr ? sr->vertex_count : 0u;
+        s.surfT = sr ? sr->triangle_count : 0u;
+        s.surfS = sr ? sr->surface_count : 0u;
+        s.surfChunks = 0;
+        for (uint32_t k = 0; k < s.surfS; ++k) s.surfChunks += (sr->surface_particle_ranges[2 * k + 1] + 63u) / 64u;
+        const uint32_t idxCount = sr ? sr->vertex_triangle_index_count : 0u;
+        s.surfBind = a.take<uint4>(size_t(s.surfV) * 2);
+        s.surfFallback = a.take<float4>(s.surfV);
+        s.surfRanges = a.take<uint4>(s.surfV);
+        s.surfIdx = a.take<uint32_t>(idxCount);
+        s.surfTri = a.take<uint4>(s.surfT);
+        s.surfChunk = a.take<uint4>(s.surfChunks);
+        s.surfChunkRange = a.take<uint2>(s.surfS);
+        s.surfPos = a.take<float4>(s.surfV);
+        s.surfNrm = a.take<float4>(s.surfV);
+        s.surfTriN = a.take<float4>(s.surfT);
+        s.surfChunkAabb = a.take<float4>(size_t(s.surfChunks) * 2);
+        s.surfWorldAabb = a.take<float4>(size_t(s.surfS) * 2);
+    }
     if (sv->hasBroadphase) {
         s.entries = a.take<int4>(N);
         s.keysA = a.take<uint32_t>(N); s.keysB = a.take<uint32_t>(N);
@@ -253,6 +274,64 @@ template <class T> cudaError_t up(const T *dst, const void *src, size_t count, c
     return cudaMemcpyAsync(const_cast<T *>(dst), src, count * sizeof(T), cudaMemcpyHostToDevice, st);
 }
 
+// Index checks of the surface render arrays (the kernels trust them), and the 64-particle bounds
+// chunks of each surface (physics_scene_gpu_state.cpp:3482-3500).
+std::string checkSurfaceRender(const cn_world_soa &w)
+{
+    const cn_surface_render_data *sr = w.surface_render;
+    if (!sr) return {};
+    const uint32_t N = w.particle_count;
+    auto need = [](uint32_t n, const void *p) { return n == 0u || p != nullptr; };
+    if (!need(sr->vertex_count, sr->vertex_bindings) || !need(sr->vertex_count, sr->fallback_normals) ||
+        !need(sr->vertex_count, sr->vertex_triangle_ranges) ||
+        !need(sr->vertex_triangle_index_count, sr->vertex_triangle_indices) ||
+        !need(sr->triangle_count, sr->triangle_particle_indices) || !need(sr->surface_count, sr->surface_particle_ranges))
+        return "surface render: missing array";
+    for (uint32_t v = 0; v < sr->vertex_count; ++v) {
+        for (uint32_t p : sr->vertex_bindings[v].particle_indices)
+            if (p >= N) return "surface render: vertex binding particle index out of range";
+        const cn_surface_triangle_range &r = sr->vertex_triangle_ranges[v];
+        if (uint64_t(r.start) + r.count > sr->vertex_triangle_index_count)
+            return "surface render: vertex triangle range out of range";
+    }
+    for (uint32_t k = 0; k < sr->vertex_triangle_index_count; ++k)
+        if (sr->vertex_triangle_indices[k] >= sr->triangle_count) return "surface render: triangle index out of range";
+    for (uint32_t t = 0; t < sr->triangle_count; ++t)
+        for (uint32_t k = 0; k < 3; ++k)
+            if (sr->triangle_particle_indices[4 * size_t(t) + k] >= N)
+                return "surface render: triangle particle index out of range";
+    for (uint32_t k = 0; k < sr->surface_count; ++k)
+        if (uint64_t(sr->surface_particle_ranges[2 * k]) + sr->surface_particle_ranges[2 * k + 1] > N)
+            return "surface render: surface particle range out of range";
+    return {};
+}
+
+cn_status uploadSurfaceRender(cn_solver *sv, const cn_world_soa &w, cudaStream_t st)
+{
+    const cn_surface_render_data *sr = w.surface_render;
+    const cn::Scene &s = sv->s;
+    if (!sr) return CN_OK;
+    CN_CUDA(up(s.surfBind, reinterpret_cast<const uint4 *>(sr->vertex_bindings), size_t(s.surfV) * 2, st));
+    CN_CUDA(up(s.surfFallback, reinterpret_cast<const float4 *>(sr->fallback_normals), s.surfV, st));
+    CN_CUDA(up(s.surfRanges, reinterpret_cast<const uint4 *>(sr->vertex_triangle_ranges), s.surfV, st));
+    CN_CUDA(up(s.surfIdx, sr->vertex_triangle_indices, sr->vertex_triangle_index_count, st));
+    CN_CUDA(up(s.surfTri, reinterpret_cast<const uint4 *>(sr->triangle_particle_indices), s.surfT, st));
+    std::vector<uint4> chunks;
+    std::vector<uint2> ranges(s.surfS);
+    for (uint32_t k = 0; k < s.surfS; ++k) {
+        const uint32_t off = sr->surface_particle_ranges[2 * k], cnt = sr->surface_particle_ranges[2 * k + 1];
+        ranges[k] = make_uint2(uint32_t(chunks.size()), 0u);
+        for (uint32_t o = 0; o < cnt; o += 64u) {
+            chunks.push_back(make_uint4(k, off + o, std::min(64u, cnt - o), 0u));
+            ++ranges[k].y;
+        }
+    }
+    CN_CUDA(up(s.surfChunk, chunks.data(), chunks.size(), st));
+    CN_CUDA(up(s.surfChunkRange, ranges.data(), ranges.size(), st));
+    CN_CUDA(cudaStreamSynchronize(st)); // the host tables above go out of scope
+    return CN_OK;
+}
+
 void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
 {
     const cn::Scene &s = sv->s;
@@ -313,6 +392,8 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             probe(sv, "contact_velocities", st, [&] { cn::launchRigidContactVelocities(s, sv->contactIt, c, st); });
         cn::launchCopyPredictedRigid(s, st);
     }
+    // physics_solver.cpp:1310-1337 (after the last substep: see launchSurfaceRender)
+    if (s.surfV || s.surfT || s.surfS) probe(sv, "surface_render", st, [&] { cn::launchSurfaceRender(s, st); });
 }
 
 cn_status runFrames(cn_solver *sv, float frameDt, uint32_t frames, cudaStream_t st)
@@ -479,6 +560,11 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
                 return setError(CN_ERR_UNSUPPORTED, "fluid material index above 32767");
     }
 
+    {
+        const std::string err = checkSurfaceRender(*w);
+        if (!err.empty()) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_sync_world: " + err);
+    }
+
     // Collider query order: moving (kinematic) colliders, then static, ascending index.
     std::vector<uint32_t> order;
     const uint32_t moving = cn::colliderQueryOrder(*w, order);
@@ -591,6 +677,10 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     CN_CUDA(up(s.colBp, w->collider_broadphase, s.C, st));
     CN_CUDA(up(s.colMat, w->collider_materials, s.C, st));
     CN_CUDA(up(s.colQueryOrder, order.data(), order.size(), st));
+    {
+        const cn_status r = uploadSurfaceRender(sv, *w, st);
+        if (r != CN_OK) return r;
+    }
     CN_CUDA(cudaStreamSynchronize(st));
 
     sv->cfg = cn::configFromDesc(d);
@@ -598,6 +688,7 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     sv->hostV = w->velocities;
     sv->contactMaterialCapacity = w->contact_material_count;
     sv->fluidMaterialCapacity = w->fluid_material_count;
+    sv->surfIdxCapacity = w->surface_render ? w->surface_render->vertex_triangle_index_count : 0u;
     sv->cellRangeCapacity = cn::nextPow2(std::max<uint32_t>(N * 2u, 1u));
     sv->synced = true;
     ++sv->bindingGeneration;
@@ -697,6 +788,38 @@ CN_API cn_status cn_solver_scene_view(cn_solver *sv, cn_scene_view *v)
     return CN_OK;
 }
 
+CN_API cn_status cn_solver_surface_render_view(cn_solver *sv, cn_surface_render_view *v)
+{
+    if (!sv || !v) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_surface_render_view: null argument");
+    std::memset(v, 0, sizeof(*v));
+    const cn::Scene &s = sv->s;
+    v->render_positions = s.surfPos;
+    v->render_normals = s.surfNrm;
+    v->triangle_normals = s.surfTriN;
+    v->chunk_aabbs = s.surfChunkAabb;
+    v->world_aabbs = s.surfWorldAabb;
+    v->vertex_count = s.surfV;
+    v->triangle_count = s.surfT;
+    v->chunk_count = s.surfChunks;
+    v->surface_count = s.surfS;
+    v->binding_generation = sv->bindingGeneration;
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_read_surface_render(cn_solver *sv, float *positions, float *normals, float *world_aabbs)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_read_surface_render: null solver");
+    if (!sv->synced) return setError(CN_ERR_NOT_INITIALIZED, "cn_solver_read_surface_render: no world synced");
+    CN_CUDA(cudaSetDevice(sv->device));
+    CN_CUDA(cudaDeviceSynchronize());
+    const cn::Scene &s = sv->s;
+    if (positions && s.surfV) CN_CUDA(cudaMemcpy(positions, s.surfPos, sizeof(float4) * s.surfV, cudaMemcpyDeviceToHost));
+    if (normals && s.surfV) CN_CUDA(cudaMemcpy(normals, s.surfNrm, sizeof(float4) * s.surfV, cudaMemcpyDeviceToHost));
+    if (world_aabbs && s.surfS)
+        CN_CUDA(cudaMemcpy(world_aabbs, s.surfWorldAabb, sizeof(float4) * 2 * s.surfS, cudaMemcpyDeviceToHost));
+    return CN_OK;
+}
+
 namespace {
 struct DlHolder {
     cn_dl_managed_tensor t{};
@@ -723,6 +846,9 @@ CN_API cn_status cn_solver_export_dlpack(cn_solver *sv, const char *buffer, cn_d
     else if (name == "radii") { data = const_cast<float *>(s.radii); cols = 1; }
     else if (name == "kinds") { data = const_cast<uint32_t *>(s.kinds); cols = 1; code = 1; }
     else if (name == "strand_segment_states") { data = s.segOrient; rows = s.S; }
+    else if (name == "render_positions") { data = s.surfPos; rows = s.surfV; }
+    else if (name == "render_normals") { data = s.surfNrm; rows = s.surfV; }
+    else if (name == "surface_world_aabbs") { data = s.surfWorldAabb; rows = s.surfS; cols = 8; }
     else return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_export_dlpack: unknown buffer '" + name + "'");
     auto *h = new DlHolder();
     h->shape[0] = rows;
@@ -753,6 +879,16 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
         w->tet_count != s.T || w->strand_segment_count != s.S || w->strand_joint_count != s.J ||
         w->strand_distance_count != s.SD || w->rigid_body_count != s.B || w->collider_count != s.C)
         return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: element counts changed; use cn_solver_sync_world");
+    if (flags & CN_SYNC_SURFACE_RENDER) {
+        const cn_surface_render_data *sr = w->surface_render;
+        uint32_t chunks = 0;
+        for (uint32_t k = 0; sr && k < sr->surface_count; ++k) chunks += (sr->surface_particle_ranges[2 * k + 1] + 63u) / 64u;
+        if ((sr ? sr->vertex_count : 0u) != s.surfV || (sr ? sr->triangle_count : 0u) != s.surfT ||
+            (sr ? sr->surface_count : 0u) != s.surfS || chunks != s.surfChunks)
+            return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: surface render counts changed; use cn_solver_sync_world");
+        const std::string err = checkSurfaceRender(*w);
+        if (!err.empty()) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: " + err);
+    }
     CN_CUDA(cudaSetDevice(sv->device));
     CN_CUDA(cudaDeviceSynchronize()); // frames in flight read these buffers
     cudaStream_t st = sv->ownStream;
@@ -796,6 +932,14 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
         CN_CUDA(up(s.colGeo, w->collider_geometry, s.C, st));
         CN_CUDA(up(s.colBp, w->collider_broadphase, s.C, st));
         CN_CUDA(up(s.colMat, w->collider_materials, s.C, st));
+    }
+    if (flags & CN_SYNC_SURFACE_RENDER) {
+        // the index-array length may differ at equal vertex counts: it must fit the synced one
+        const cn_surface_render_data *sr = w->surface_render;
+        if (sr && sr->vertex_triangle_index_count > sv->surfIdxCapacity)
+            return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: more incident-triangle indices than synced");
+        const cn_status r = uploadSurfaceRender(sv, *w, st);
+        if (r != CN_OK) return r;
     }
     CN_CUDA(cudaStreamSynchronize(st));
     return CN_OK;

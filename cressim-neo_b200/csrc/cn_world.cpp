@@ -7,6 +7,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <fstream>
 #include <set>
@@ -135,6 +136,7 @@ struct SoftBody {
     uint32_t neighbourCount = 0;      // meshfree k-nearest graph
     std::vector<uint32_t> staticIdx;
     std::vector<v3> rest;
+    std::vector<v3> local;            // rest positions in the object (source) frame
     std::vector<std::array<uint32_t, 4>> tets;
     std::vector<std::array<uint32_t, 2>> edges;
     std::vector<std::vector<uint32_t>> adjacency;
@@ -147,6 +149,7 @@ struct Cloth {
     cn_cloth_grid_desc desc;
     std::vector<uint32_t> staticIdx;
     std::vector<v3> rest;
+    std::vector<v3> local;            // rest positions in the cloth's own frame
     std::vector<std::array<uint32_t, 2>> structural;
     std::vector<float> structuralRest;
     struct Hinge { uint32_t e0, e1, o0, o1; float angle; };
@@ -185,6 +188,22 @@ struct cn_world {
     std::vector<cn_strand_distance> dists;
     std::vector<cn_collider_geometry> colGeo;
     std::vector<cn_collider_broadphase> colBp;
+    // surface render data: meshes bound by cn_world_add_surface_mesh (owner-relative particle
+    // indices), or a caller's copy from cn_world_set_surface_render; packed arrays below
+    struct SurfaceMesh {
+        uint32_t ownerKind = 0, ownerIndex = 0;
+        std::vector<cn_surface_vertex_binding> bindings;
+        std::vector<float> fallback;                   // float4 per vertex
+        std::vector<std::array<uint32_t, 3>> triangles; // particle indices (owner-relative)
+        std::vector<std::array<uint32_t, 3>> triVerts;  // render vertices of each kept triangle
+    };
+    std::vector<SurfaceMesh> surfaceMeshes;
+    bool customSurface = false;
+    std::vector<cn_surface_vertex_binding> sBind;
+    std::vector<float> sFallback;
+    std::vector<cn_surface_triangle_range> sRanges;
+    std::vector<uint32_t> sIdx, sTri, sSurf;
+    cn_surface_render_data sData{};
     float cellSize = 1.0e-4f;
     // The packed SoA is rebuilt only after an authoring change, so edits a caller makes through
     // the SoA's arrays (state, per-constraint parameters) survive later cn_world_get_soa calls.
@@ -281,6 +300,7 @@ std::string buildSoftBody(SoftBody &sb)
     if (!meshfree && (idx.size() % 4u) != 0u) return "Soft body tetrahedron index buffer size must be divisible by 4.";
     sb.rest.clear();
     for (const v3 &p : src) sb.rest.push_back(applyTransform(d.rest_transform, p));
+    sb.local = src;
     const uint32_t n = uint32_t(sb.rest.size());
     sb.adjacency.assign(n, {});
     sb.tets.clear();
@@ -432,11 +452,13 @@ cn_status buildCloth(Cloth &c)
     const cn_cloth_grid_desc &d = c.desc;
     const uint32_t nx = std::max<uint32_t>(d.resolution[0], 2u), ny = std::max<uint32_t>(d.resolution[1], 2u);
     c.rest.clear();
+    c.local.clear();
     for (uint32_t j = 0; j < ny; ++j)
-        for (uint32_t i = 0; i < nx; ++i)
-            c.rest.push_back(applyTransform(d.rest_transform,
-                                            v3{(float(i) / float(nx - 1) - 0.5f) * d.size[0], 0.0f,
-                                               (float(j) / float(ny - 1) - 0.5f) * d.size[1]}));
+        for (uint32_t i = 0; i < nx; ++i) {
+            const v3 lp{(float(i) / float(nx - 1) - 0.5f) * d.size[0], 0.0f, (float(j) / float(ny - 1) - 0.5f) * d.size[1]};
+            c.local.push_back(lp);
+            c.rest.push_back(applyTransform(d.rest_transform, lp));
+        }
     struct Inc { uint32_t a, b; std::vector<uint32_t> opp; };
     std::map<uint64_t, Inc> edges;
     auto addTri = [&](uint32_t a, uint32_t b, uint32_t cc) {
@@ -586,6 +608,218 @@ void pushParticle(cn_world &w, v3 p, float invMass, float radius, uint32_t kind,
     w.ownerIdx.push_back(owner);
 }
 
+// ---------------------------------------------------------------------------- surface meshes
+// Render-vertex bindings as the engine's World builds them (world.cpp:180-395, 3255-3554).
+
+// quantizePoint (world.cpp:180-188): nearest integer lattice point at spacing epsilon
+std::array<int64_t, 3> quantizePoint(v3 p, float eps)
+{
+    const double inv = 1.0 / double(std::max(eps, 1.0e-8f));
+    return {std::llround(double(p.x) * inv), std::llround(double(p.y) * inv), std::llround(double(p.z) * inv)};
+}
+
+struct QuantKeyHash {
+    size_t operator()(const std::array<int64_t, 3> &k) const
+    {
+        uint64_t h = 1469598103934665603ull;
+        for (int64_t v : k) h = (h ^ uint64_t(v)) * 1099511628211ull;
+        return size_t(h);
+    }
+};
+
+// makeExactSurfaceDeformableVertexBinding (world.cpp:268-276)
+cn_surface_vertex_binding exactBinding(uint32_t particle)
+{
+    cn_surface_vertex_binding b{};
+    for (int k = 0; k < 4; ++k) b.particle_indices[k] = particle;
+    b.weights[0] = 1.0f;
+    return b;
+}
+
+// makeNearestParticleSkinBinding (world.cpp:278-366): the 4 nearest rest particles (strictly
+// closer ones first, ties keep the earlier particle), weights 1 / (distance + 1e-6) normalised
+cn_surface_vertex_binding nearestBinding(v3 vtx, const std::vector<v3> &rest)
+{
+    struct Cand { float d2; uint32_t idx; bool valid; };
+    std::array<Cand, 4> nearest{};
+    for (auto &c : nearest) c = Cand{std::numeric_limits<float>::max(), 0u, false};
+    for (uint32_t p = 0; p < rest.size(); ++p) {
+        const v3 dlt = rest[p] - vtx;
+        const float d2 = dot(dlt, dlt);
+        for (size_t slot = 0; slot < nearest.size(); ++slot) {
+            if (nearest[slot].valid && d2 >= nearest[slot].d2) continue;
+            for (size_t m = nearest.size() - 1; m > slot; --m) nearest[m] = nearest[m - 1];
+            nearest[slot] = Cand{d2, p, true};
+            break;
+        }
+    }
+    cn_surface_vertex_binding b = exactBinding(nearest[0].valid ? nearest[0].idx : 0u);
+    if (!nearest[0].valid) return b;
+    float raw[4] = {0.f, 0.f, 0.f, 0.f}, sum = 0.0f;
+    for (size_t slot = 0; slot < 4; ++slot) {
+        if (!nearest[slot].valid) continue;
+        const float dist = std::sqrt(std::max(nearest[slot].d2, 0.0f));
+        raw[slot] = 1.0f / (dist + 1.0e-6f);
+        sum += raw[slot];
+        b.particle_indices[slot] = nearest[slot].idx;
+    }
+    if (sum <= 0.0f) return b;
+    for (int k = 0; k < 4; ++k) b.weights[k] = raw[k] / sum;
+    return b;
+}
+
+// dominantParticleIndex (world.cpp:367-388): the first particle of largest weight
+uint32_t dominantParticle(const cn_surface_vertex_binding &b)
+{
+    uint32_t idx = b.particle_indices[0];
+    float wt = b.weights[0];
+    for (int k = 1; k < 4; ++k)
+        if (b.weights[k] > wt) {
+            idx = b.particle_indices[k];
+            wt = b.weights[k];
+        }
+    return idx;
+}
+
+// transformNormal (world.cpp:213-228) with the identity transform
+void fallbackNormal(const float *n, float *out)
+{
+    v3 v = n ? v3{n[0], n[1], n[2]} : v3{0.f, 0.f, 0.f};
+    const float l2 = dot(v, v);
+    if (l2 <= 1.0e-12f) v = v3{0.f, 1.f, 0.f};
+    else v = v * (1.0f / std::sqrt(l2));
+    out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = 0.0f;
+}
+
+std::string bindSurfaceMesh(const cn_world &w, const cn_surface_mesh_desc &d, cn_world::SurfaceMesh &m)
+{
+    const bool cloth = d.owner_kind == CN_SURFACE_OWNER_CLOTH;
+    if (d.owner_kind > CN_SURFACE_OWNER_CLOTH) return "surface mesh: unknown owner kind";
+    if (cloth ? d.owner_index >= w.cloths.size() : d.owner_index >= w.softBodies.size())
+        return "surface mesh: owner index out of range";
+    if (d.vertex_count == 0 || !d.positions) return "surface mesh: missing visual mesh";
+    if (d.index_count && !d.indices) return "surface mesh: missing index buffer";
+    const std::vector<v3> &rest = cloth ? w.cloths[d.owner_index].local : w.softBodies[d.owner_index].local;
+    if (rest.empty()) return "surface mesh: owner has no rest positions";
+    const float eps = d.match_epsilon > 0.0f ? d.match_epsilon : 1.0e-3f;
+    const float eps2 = eps * eps;
+    const uint32_t V = d.vertex_count;
+    auto vtx = [&](uint32_t i) { return v3{d.positions[3 * i], d.positions[3 * i + 1], d.positions[3 * i + 2]}; };
+    m.ownerKind = d.owner_kind;
+    m.ownerIndex = d.owner_index;
+    m.bindings.clear();
+    m.fallback.assign(size_t(V) * 4, 0.0f);
+    for (uint32_t i = 0; i < V; ++i) fallbackNormal(d.normals ? d.normals + 3 * i : nullptr, &m.fallback[4 * size_t(i)]);
+    std::vector<uint32_t> mapping(V, 0u);
+    if (cloth) {
+        // identity when every vertex sits on the particle of its index, else one unique match each
+        bool identity = rest.size() == V;
+        for (uint32_t i = 0; identity && i < V; ++i) {
+            const v3 dl = vtx(i) - rest[i];
+            identity = dot(dl, dl) <= eps2;
+            mapping[i] = i;
+        }
+        if (!identity)
+            for (uint32_t i = 0; i < V; ++i) {
+                uint32_t match = 0, matches = 0;
+                for (uint32_t p = 0; p < rest.size(); ++p) {
+                    const v3 dl = vtx(i) - rest[p];
+                    if (dot(dl, dl) <= eps2) {
+                        match = p;
+                        ++matches;
+                    }
+                }
+                if (matches != 1u)
+                    return "Cloth render binding build failed: mapping is missing, ambiguous, mismatched, or "
+                           "collapses a triangle.";
+                mapping[i] = match;
+            }
+        for (uint32_t t = 0; t + 2u < d.index_count; t += 3u) {
+            const uint32_t a = d.indices[t], b = d.indices[t + 1], c = d.indices[t + 2];
+            if (a >= V || b >= V || c >= V || mapping[a] == mapping[b] || mapping[b] == mapping[c] ||
+                mapping[c] == mapping[a])
+                return "Cloth render binding build failed: mapping is missing, ambiguous, mismatched, or "
+                       "collapses a triangle.";
+        }
+        for (uint32_t i = 0; i < V; ++i) m.bindings.push_back(exactBinding(mapping[i]));
+    } else if (w.softBodies[d.owner_index].source == SoftSource::Meshfree) {
+        for (uint32_t i = 0; i < V; ++i) m.bindings.push_back(nearestBinding(vtx(i), rest));
+    } else {
+        std::unordered_map<std::array<int64_t, 3>, uint32_t, QuantKeyHash> byKey;
+        byKey.reserve(rest.size());
+        for (uint32_t p = 0; p < rest.size(); ++p) byKey.try_emplace(quantizePoint(rest[p], eps), p);
+        for (uint32_t i = 0; i < V; ++i) {
+            const v3 q = vtx(i);
+            const auto it = byKey.find(quantizePoint(q, eps));
+            bool found = it != byKey.end();
+            uint32_t best = found ? it->second : 0u;
+            if (!found) { // findMatchingRestVertexLocal's scan: closest within epsilon, later ties win
+                float bestD2 = eps2;
+                for (uint32_t p = 0; p < rest.size(); ++p) {
+                    const v3 dl = rest[p] - q;
+                    const float d2 = dot(dl, dl);
+                    if (d2 > bestD2) continue;
+                    bestD2 = d2;
+                    best = p;
+                    found = true;
+                }
+            }
+            if (!found)
+                return "Soft-body render binding build failed: visual mesh vertices must match tet rest vertices "
+                       "exactly.";
+            m.bindings.push_back(exactBinding(best));
+        }
+    }
+    m.triangles.clear();
+    m.triVerts.clear();
+    for (uint32_t t = 0; t + 2u < d.index_count; t += 3u) {
+        const uint32_t a = d.indices[t], b = d.indices[t + 1], c = d.indices[t + 2];
+        if (a >= V || b >= V || c >= V) continue;
+        if (cloth)
+            m.triangles.push_back({mapping[a], mapping[b], mapping[c]});
+        else
+            m.triangles.push_back({dominantParticle(m.bindings[a]), dominantParticle(m.bindings[b]),
+                                   dominantParticle(m.bindings[c])});
+        m.triVerts.push_back({a, b, c});
+    }
+    return {};
+}
+
+// Packs the surface render arrays once the particle offsets of the owners are known.
+void packSurfaces(cn_world &w, const std::vector<uint32_t> &softOff, const std::vector<uint32_t> &clothOff)
+{
+    if (w.customSurface) return;
+    w.sBind.clear(); w.sFallback.clear(); w.sRanges.clear(); w.sIdx.clear(); w.sTri.clear(); w.sSurf.clear();
+    for (uint32_t si = 0; si < w.softBodies.size(); ++si) {
+        w.sSurf.push_back(softOff[si]);
+        w.sSurf.push_back(uint32_t(w.softBodies[si].rest.size()));
+    }
+    for (uint32_t ci = 0; ci < w.cloths.size(); ++ci) {
+        w.sSurf.push_back(clothOff[ci]);
+        w.sSurf.push_back(uint32_t(w.cloths[ci].rest.size()));
+    }
+    for (const cn_world::SurfaceMesh &m : w.surfaceMeshes) {
+        const uint32_t off = m.ownerKind == CN_SURFACE_OWNER_CLOTH ? clothOff[m.ownerIndex] : softOff[m.ownerIndex];
+        const uint32_t vBase = uint32_t(w.sBind.size()), tBase = uint32_t(w.sTri.size() / 4);
+        for (cn_surface_vertex_binding b : m.bindings) {
+            for (uint32_t &p : b.particle_indices) p += off;
+            w.sBind.push_back(b);
+        }
+        w.sFallback.insert(w.sFallback.end(), m.fallback.begin(), m.fallback.end());
+        std::vector<std::vector<uint32_t>> incident(m.bindings.size());
+        for (uint32_t t = 0; t < m.triangles.size(); ++t) {
+            for (uint32_t k = 0; k < 3; ++k) w.sTri.push_back(m.triangles[t][k] + off);
+            w.sTri.push_back(0u);
+            for (uint32_t k = 0; k < 3; ++k) incident[m.triVerts[t][k]].push_back(tBase + t);
+        }
+        for (uint32_t v = 0; v < incident.size(); ++v) {
+            w.sRanges.push_back(cn_surface_triangle_range{uint32_t(w.sIdx.size()), uint32_t(incident[v].size()), 0u, 0u});
+            w.sIdx.insert(w.sIdx.end(), incident[v].begin(), incident[v].end());
+        }
+        (void)vBase;
+    }
+}
+
 cn_status pack(cn_world &w)
 {
     w.x.clear(); w.v.clear(); w.radii.clear(); w.kinds.clear(); w.meta.clear(); w.matIdx.clear();
@@ -597,11 +831,13 @@ cn_status pack(cn_world &w)
     const uint32_t strandBase = clothBase + uint32_t(w.cloths.size());
     const uint32_t fluidBase = strandBase + uint32_t(w.strands.size());
 
+    std::vector<uint32_t> softOff, clothOff;
     for (uint32_t si = 0; si < w.softBodies.size(); ++si) {
         SoftBody &sb = w.softBodies[si];
         const cn_soft_body_grid_desc &d = sb.desc;
         const uint32_t mat = findOrAppendContact(w.contactMaterials, normalizeContact(d.material));
         const uint32_t off = uint32_t(w.radii.size());
+        softOff.push_back(off);
         const float inv = d.particle_mass > 0.0f ? 1.0f / d.particle_mass : 0.0f;
         std::unordered_set<uint32_t> fixed(sb.staticIdx.begin(), sb.staticIdx.end());
         const uint32_t layer = d.collision_layer == 0u ? 1u : d.collision_layer;
@@ -637,6 +873,7 @@ cn_status pack(cn_world &w)
         const cn_cloth_grid_desc &d = c.desc;
         const uint32_t mat = findOrAppendContact(w.contactMaterials, normalizeContact(d.material));
         const uint32_t off = uint32_t(w.radii.size());
+        clothOff.push_back(off);
         const float inv = d.particle_mass > 0.0f ? 1.0f / d.particle_mass : 0.0f;
         std::unordered_set<uint32_t> fixed(c.staticIdx.begin(), c.staticIdx.end());
         const uint32_t layer = d.collision_layer == 0u ? 1u : d.collision_layer;
@@ -794,6 +1031,7 @@ cn_status pack(cn_world &w)
         w.bodyColRanges[2 * b + 1] = uint32_t(bodyCols[b].size());
         w.bodyColIdx.insert(w.bodyColIdx.end(), bodyCols[b].begin(), bodyCols[b].end());
     }
+    packSurfaces(w, softOff, clothOff);
     return CN_OK;
 }
 
@@ -1079,6 +1317,65 @@ CN_API cn_status cn_world_get_soa(cn_world *w, cn_world_soa *o)
     o->collider_geometry = ptr(w->colGeo);
     o->collider_broadphase = ptr(w->colBp);
     o->collider_materials = ptr(w->colMat);
+    cn_surface_render_data &sd = w->sData;
+    sd = cn_surface_render_data{};
+    sd.vertex_count = uint32_t(w->sBind.size());
+    sd.vertex_bindings = ptr(w->sBind);
+    sd.fallback_normals = ptr(w->sFallback);
+    sd.vertex_triangle_ranges = ptr(w->sRanges);
+    sd.vertex_triangle_index_count = uint32_t(w->sIdx.size());
+    sd.vertex_triangle_indices = ptr(w->sIdx);
+    sd.triangle_count = uint32_t(w->sTri.size() / 4);
+    sd.triangle_particle_indices = ptr(w->sTri);
+    sd.surface_count = uint32_t(w->sSurf.size() / 2);
+    sd.surface_particle_ranges = ptr(w->sSurf);
+    o->surface_render = (sd.vertex_count || sd.surface_count) ? &sd : nullptr;
+    return CN_OK;
+}
+
+CN_API void cn_surface_mesh_desc_defaults(cn_surface_mesh_desc *d)
+{
+    if (!d) return;
+    std::memset(d, 0, sizeof(*d));
+    d->match_epsilon = 1.0e-3f; // kSoftBodyVertexMatchEpsilon (world.cpp:17)
+}
+
+CN_API cn_status cn_world_add_surface_mesh(cn_world *w, const cn_surface_mesh_desc *d, uint32_t *out_first_vertex)
+{
+    if (!w || !d) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_add_surface_mesh: null argument");
+    cn_world::SurfaceMesh m;
+    const std::string err = bindSurfaceMesh(*w, *d, m);
+    if (!err.empty()) return cn::setError(CN_ERR_INVALID_ARGUMENT, err);
+    uint32_t first = 0;
+    for (const auto &e : w->surfaceMeshes) first += uint32_t(e.bindings.size());
+    if (out_first_vertex) *out_first_vertex = first;
+    w->surfaceMeshes.push_back(std::move(m));
+    w->customSurface = false;
+    w->packed = false;
+    return CN_OK;
+}
+
+CN_API cn_status cn_world_set_surface_render(cn_world *w, const cn_surface_render_data *d)
+{
+    if (!w) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_set_surface_render: null world");
+    w->packed = false;
+    if (!d) {
+        w->customSurface = false;
+        return CN_OK;
+    }
+    auto need = [](uint32_t n, const void *p) { return n == 0u || p != nullptr; };
+    if (!need(d->vertex_count, d->vertex_bindings) || !need(d->vertex_count, d->fallback_normals) ||
+        !need(d->vertex_count, d->vertex_triangle_ranges) ||
+        !need(d->vertex_triangle_index_count, d->vertex_triangle_indices) ||
+        !need(d->triangle_count, d->triangle_particle_indices) || !need(d->surface_count, d->surface_particle_ranges))
+        return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_set_surface_render: missing array");
+    w->customSurface = true;
+    w->sBind.assign(d->vertex_bindings, d->vertex_bindings + d->vertex_count);
+    w->sFallback.assign(d->fallback_normals, d->fallback_normals + size_t(d->vertex_count) * 4);
+    w->sRanges.assign(d->vertex_triangle_ranges, d->vertex_triangle_ranges + d->vertex_count);
+    w->sIdx.assign(d->vertex_triangle_indices, d->vertex_triangle_indices + d->vertex_triangle_index_count);
+    w->sTri.assign(d->triangle_particle_indices, d->triangle_particle_indices + size_t(d->triangle_count) * 4);
+    w->sSurf.assign(d->surface_particle_ranges, d->surface_particle_ranges + size_t(d->surface_count) * 2);
     return CN_OK;
 }
 

@@ -250,7 +250,37 @@ typedef struct cn_world_soa {
     const cn_collider_geometry *collider_geometry;
     const cn_collider_broadphase *collider_broadphase;
     const float *collider_materials;        /* float4[C] (friction, restitution, 0, staticFriction) */
+
+    /* surface render passes (skinning, normals, bounds); NULL: none */
+    const struct cn_surface_render_data *surface_render;
 } cn_world_soa;
+
+/* ------------------------------------------------------------------------ */
+/* Surface render data: what PhysicsWorld::setSurfaceDeformableRenderData   */
+/* holds (physics_world.cpp:3368; SurfaceDeformableRenderDataHost,           */
+/* physics_types.h:1350-1392).  Every frame the solver skins the render      */
+/* vertices, computes triangle and vertex normals and the per-surface world  */
+/* AABBs from the particle positions (shaders in physics/soft/render/).     */
+/* ------------------------------------------------------------------------ */
+typedef struct cn_surface_vertex_binding {   /* SurfaceRenderVertexBinding (32 B) */
+    uint32_t particle_indices[4];
+    float weights[4];
+} cn_surface_vertex_binding;
+typedef struct cn_surface_triangle_range {   /* SurfaceRenderVertexTriangleRange (16 B) */
+    uint32_t start, count, reserved0, reserved1;
+} cn_surface_triangle_range;
+typedef struct cn_surface_render_data {
+    uint32_t vertex_count;
+    const cn_surface_vertex_binding *vertex_bindings;          /* [vertex_count] */
+    const float *fallback_normals;                             /* float4[vertex_count] */
+    const cn_surface_triangle_range *vertex_triangle_ranges;   /* [vertex_count] */
+    uint32_t vertex_triangle_index_count;
+    const uint32_t *vertex_triangle_indices;                   /* incident triangles, in range order */
+    uint32_t triangle_count;
+    const uint32_t *triangle_particle_indices;                 /* uint4[triangle_count] (a, b, c, 0) */
+    uint32_t surface_count;
+    const uint32_t *surface_particle_ranges;                   /* uint2[surface_count] (offset, count) */
+} cn_surface_render_data;
 
 /* ------------------------------------------------------------------------ */
 /* Host authoring (PhysicsWorld mirror): regular-grid soft bodies, fluid      */
@@ -363,6 +393,33 @@ CN_API cn_status cn_world_add_cloth_grid(cn_world *w, const cn_cloth_grid_desc *
 CN_API cn_status cn_world_add_strand(cn_world *w, const cn_strand_desc *d, uint32_t *out_index);
 CN_API cn_status cn_world_add_rigid_body(cn_world *w, const cn_rigid_body_desc *d, uint32_t *out_body);
 CN_API cn_status cn_world_add_collider(cn_world *w, const cn_collider_desc *d, uint32_t *out_collider);
+/* A render mesh bound to a soft body or cloth, as the engine's World builds the surface render
+ * data (world.cpp:3255-3554): every soft body and cloth gets a surface particle range (packed
+ * [soft bodies][cloths]); the mesh's vertices are bound to the owner's particles -- one matching
+ * rest particle within match_epsilon (makeExactSurfaceDeformableVertexBinding; cloth vertices must
+ * match exactly one particle), or, for a meshfree soft body, the 4 nearest rest particles with
+ * inverse-distance weights (makeNearestParticleSkinBinding) -- and each triangle to the dominant
+ * particles of its vertices, with per-vertex incident-triangle lists in triangle order.  Mesh
+ * positions are in the frame of the owner's authored rest positions (the reference's rest-local
+ * frame); normals are the fallback normals (normalised; (0, 1, 0) when degenerate). */
+enum { CN_SURFACE_OWNER_SOFT_BODY = 0, CN_SURFACE_OWNER_CLOTH = 1 };
+typedef struct cn_surface_mesh_desc {
+    uint32_t owner_kind;          /* CN_SURFACE_OWNER_* */
+    uint32_t owner_index;         /* soft body / cloth index in authoring order */
+    uint32_t vertex_count;
+    const float *positions;       /* float3[vertex_count] */
+    const float *normals;         /* float3[vertex_count] or NULL */
+    uint32_t index_count;         /* 3 per triangle */
+    const uint32_t *indices;
+    float match_epsilon;          /* kSoftBodyVertexMatchEpsilon = 1e-3 */
+    uint32_t reserved[3];
+} cn_surface_mesh_desc;
+CN_API void cn_surface_mesh_desc_defaults(cn_surface_mesh_desc *d);
+/* out_first_vertex: index of the mesh's first render vertex in the packed render arrays. */
+CN_API cn_status cn_world_add_surface_mesh(cn_world *w, const cn_surface_mesh_desc *d, uint32_t *out_first_vertex);
+/* PhysicsWorld::setSurfaceDeformableRenderData: replaces the world's surface render data (and
+ * the meshes added above) with a copy of `data`; NULL restores the built data. */
+CN_API cn_status cn_world_set_surface_render(cn_world *w, const cn_surface_render_data *data);
 /* Packs the SoA (PhysicsWorld::ensureDerivedStateUpToDate).  Pointers stay valid until the
  * next mutating call on the world; positions and velocities may be edited in place. */
 CN_API cn_status cn_world_get_soa(cn_world *w, cn_world_soa *out);
@@ -413,7 +470,8 @@ typedef struct cn_scene_view {
  * until binding_generation changes.  The struct layout is DLPack's (dlpack.h, version 0.8);
  * the consumer calls `deleter` when done.  Buffers: "positions_inv_mass", "previous_positions",
  * "velocities" (float32 N x 4), "radii" (float32 N), "kinds" (uint32 N), "strand_segment_states"
- * (float32 S x 4). */
+ * (float32 S x 4), "render_positions", "render_normals" (float32 V x 4), "surface_world_aabbs"
+ * (float32 surfaces x 8: min xyzw, max xyzw). */
 typedef struct cn_dl_tensor {
     void *data;
     int32_t device_type;            /* kDLCUDA = 2 */
@@ -452,6 +510,23 @@ CN_API cn_status cn_solver_set_kinematic_target(cn_solver *solver, uint32_t body
                                                 const float position[3], const float orientation[4]);
 /* PhysicsSolver::gpuSceneView / softPositionsInvMassSharedBuffer: the native device buffers. */
 CN_API cn_status cn_solver_scene_view(cn_solver *solver, cn_scene_view *out_view);
+/* Surface render outputs (renderPositionsBuffer, renderNormalsBuffer, worldAabbsBuffer of
+ * PhysicsGpuSoftSceneView, physics_gpu_scene_view.h:206-217), written at the end of every frame:
+ * render positions float4 (xyz, 1), vertex normals float4 (xyz, 0), unnormalised triangle normals
+ * float4, and AABBs as (min float4, max float4) pairs per 64-particle chunk and per surface. */
+typedef struct cn_surface_render_view {
+    void *render_positions;
+    void *render_normals;
+    void *triangle_normals;
+    void *chunk_aabbs;
+    void *world_aabbs;
+    uint32_t vertex_count, triangle_count, chunk_count, surface_count;
+    uint64_t binding_generation;
+} cn_surface_render_view;
+CN_API cn_status cn_solver_surface_render_view(cn_solver *solver, cn_surface_render_view *out_view);
+/* Blocking host copies of the surface outputs (any pointer may be NULL): float4[vertex_count]
+ * positions and normals, float4[2 * surface_count] world AABBs. */
+CN_API cn_status cn_solver_read_surface_render(cn_solver *solver, float *positions, float *normals, float *world_aabbs);
 CN_API cn_status cn_solver_export_dlpack(cn_solver *solver, const char *buffer, cn_dl_managed_tensor **out_tensor);
 /* Incremental upload (the revision-counter path of uploadWorldState,
  * physics_scene_gpu_state.cpp:2348): the world's element counts must equal the synced ones;
@@ -462,7 +537,8 @@ typedef enum cn_sync_flags {
     CN_SYNC_PARTICLE_ATTRIBUTES = 2,/* radii, metadata, material indices, contact / fluid materials */
     CN_SYNC_CONSTRAINTS = 4,        /* edge, bend, dihedral, tet and strand records */
     CN_SYNC_RIGID_BODIES = 8,       /* body poses, velocities, scales, kinematic targets */
-    CN_SYNC_COLLIDERS = 16          /* collider geometry, broadphase records, materials */
+    CN_SYNC_COLLIDERS = 16,         /* collider geometry, broadphase records, materials */
+    CN_SYNC_SURFACE_RENDER = 32     /* surface render bindings, normals, triangles (same counts) */
 } cn_sync_flags;
 CN_API cn_status cn_solver_update_world(cn_solver *solver, const cn_world_soa *world, uint32_t flags);
 /* Blocking copy of device particle state to host (readbackPredictedParticleStateBlocking).

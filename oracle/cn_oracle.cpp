@@ -339,6 +339,15 @@ struct cno_solver {
     std::vector<f4> distCorr;      // 2 per distance
     uint32_t truncations = 0;
     bool postUpdateNeighbors = true; // physics_solver.cpp:1262-1268
+    // surface render data (SurfaceDeformableRenderDataHost) and outputs
+    std::vector<cn_surface_vertex_binding> surfBind;
+    std::vector<f4> surfFallback;
+    std::vector<cn_surface_triangle_range> surfRanges;
+    std::vector<uint32_t> surfIdx;
+    std::vector<uint32_t> surfTri;            // uint4 per triangle
+    std::vector<uint32_t> surfChunks;         // uint4 per chunk (surface, start, count, 0)
+    std::vector<uint32_t> surfChunkRanges;    // uint2 per surface (start, count)
+    std::vector<f4> surfPos, surfNrm, surfTriN, surfChunkAabb, surfWorldAabb;
 
     // settings shorthands (physics_solver_config.hlsli:27-62)
     float slop() const { return desc.contact.slop; }
@@ -468,6 +477,106 @@ void setupWorld(cno_solver &s, const cn_world_soa &w)
     s.predBodyLin = s.bodyLin; s.predBodyAng = s.bodyAng;
     s.colAabbMin.assign(s.C, f3{0, 0, 0});
     s.colAabbMax.assign(s.C, f3{0, 0, 0});
+    if (const cn_surface_render_data *sr = w.surface_render) {
+        const uint32_t V = sr->vertex_count, T = sr->triangle_count, S = sr->surface_count;
+        s.surfBind.assign(sr->vertex_bindings, sr->vertex_bindings + V);
+        s.surfFallback.resize(V);
+        for (uint32_t v = 0; v < V; ++v)
+            s.surfFallback[v] = f4{sr->fallback_normals[4 * v], sr->fallback_normals[4 * v + 1],
+                                   sr->fallback_normals[4 * v + 2], sr->fallback_normals[4 * v + 3]};
+        s.surfRanges.assign(sr->vertex_triangle_ranges, sr->vertex_triangle_ranges + V);
+        s.surfIdx.assign(sr->vertex_triangle_indices, sr->vertex_triangle_indices + sr->vertex_triangle_index_count);
+        s.surfTri.assign(sr->triangle_particle_indices, sr->triangle_particle_indices + size_t(T) * 4);
+        // 64-particle bounds chunks per surface (physics_scene_gpu_state.cpp:3482-3500)
+        for (uint32_t k = 0; k < S; ++k) {
+            const uint32_t off = sr->surface_particle_ranges[2 * k], cnt = sr->surface_particle_ranges[2 * k + 1];
+            s.surfChunkRanges.push_back(uint32_t(s.surfChunks.size() / 4));
+            uint32_t n = 0;
+            for (uint32_t o = 0; o < cnt; o += 64u, ++n)
+                s.surfChunks.insert(s.surfChunks.end(), {k, off + o, std::min(64u, cnt - o), 0u});
+            s.surfChunkRanges.push_back(n);
+        }
+        s.surfPos.assign(V, f4{0, 0, 0, 0});
+        s.surfNrm.assign(V, f4{0, 0, 0, 0});
+        s.surfTriN.assign(T, f4{0, 0, 0, 0});
+        s.surfChunkAabb.assign(s.surfChunks.size() / 4 * 2, f4{0, 0, 0, 0});
+        s.surfWorldAabb.assign(size_t(S) * 2, f4{0, 0, 0, 0});
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Surface render passes (PhysicsSolver::step, physics_solver.cpp:1310-1337).
+// ---------------------------------------------------------------------------
+// physics_surface_skin_render_vertices.cs.hlsl:14-36
+void skinSurfaceVertices(cno_solver &s)
+{
+    for (size_t v = 0; v < s.surfBind.size(); ++v) {
+        const cn_surface_vertex_binding &b = s.surfBind[v];
+        f3 acc{0.f, 0.f, 0.f};
+        for (int k = 0; k < 4; ++k) acc += b.weights[k] * xyz(s.x[b.particle_indices[k]]);
+        s.surfPos[v] = mk4(acc, 1.0f);
+    }
+}
+
+// physics_surface_update_triangle_normals.cs.hlsl:8-24
+void updateSurfaceTriangleNormals(cno_solver &s)
+{
+    for (size_t t = 0; t < s.surfTriN.size(); ++t) {
+        const f3 p0 = xyz(s.x[s.surfTri[4 * t]]), p1 = xyz(s.x[s.surfTri[4 * t + 1]]), p2 = xyz(s.x[s.surfTri[4 * t + 2]]);
+        s.surfTriN[t] = mk4(cross(p2 - p0, p1 - p0), 0.0f);
+    }
+}
+
+// physics_surface_update_render_normals.cs.hlsl:18-48; rsqrt taken as the correctly rounded
+// 1 / sqrt (the shader's is a hardware approximation)
+void updateSurfaceVertexNormals(cno_solver &s)
+{
+    for (size_t v = 0; v < s.surfRanges.size(); ++v) {
+        const cn_surface_triangle_range &r = s.surfRanges[v];
+        f3 acc{0.f, 0.f, 0.f};
+        for (uint32_t k = 0; k < r.count; ++k) acc += xyz(s.surfTriN[s.surfIdx[r.start + k]]);
+        f3 n = acc;
+        const float lenSq = dot(n, n);
+        if (lenSq <= 1.0e-12f) n = xyz(s.surfFallback[v]);
+        else n = n * (1.0f / std::sqrt(lenSq));
+        s.surfNrm[v] = mk4(n, 0.0f);
+    }
+}
+
+// physics_surface_update_bounds.cs.hlsl:12-65 and physics_surface_finalize_bounds.cs.hlsl:12-66
+void updateSurfaceBounds(cno_solver &s)
+{
+    const float big = 3.402823e+38f;
+    const size_t chunks = s.surfChunks.size() / 4;
+    for (size_t c = 0; c < chunks; ++c) {
+        const uint32_t start = s.surfChunks[4 * c + 1], count = s.surfChunks[4 * c + 2];
+        if (count == 0u) {
+            s.surfChunkAabb[2 * c] = s.surfChunkAabb[2 * c + 1] = f4{0, 0, 0, 0};
+            continue;
+        }
+        f3 lo{big, big, big}, hi{-big, -big, -big};
+        for (uint32_t k = 0; k < count; ++k) {
+            lo = min3(lo, xyz(s.x[start + k]));
+            hi = max3(hi, xyz(s.x[start + k]));
+        }
+        s.surfChunkAabb[2 * c] = mk4(lo, 0.0f);
+        s.surfChunkAabb[2 * c + 1] = mk4(hi, 0.0f);
+    }
+    const size_t S = s.surfChunkRanges.size() / 2;
+    for (size_t k = 0; k < S; ++k) {
+        const uint32_t start = s.surfChunkRanges[2 * k], count = s.surfChunkRanges[2 * k + 1];
+        if (count == 0u) {
+            s.surfWorldAabb[2 * k] = s.surfWorldAabb[2 * k + 1] = f4{0, 0, 0, 0};
+            continue;
+        }
+        f3 lo{big, big, big}, hi{-big, -big, -big};
+        for (uint32_t c = 0; c < count; ++c) {
+            lo = min3(lo, xyz(s.surfChunkAabb[2 * (start + c)]));
+            hi = max3(hi, xyz(s.surfChunkAabb[2 * (start + c) + 1]));
+        }
+        s.surfWorldAabb[2 * k] = mk4(lo, 0.0f);
+        s.surfWorldAabb[2 * k + 1] = mk4(hi, 0.0f);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1917,6 +2026,10 @@ void stepFrame(cno_solver &s, float frameDt)
         }
         if (hasSoftSoftContact && contactIt > 0) particleContactVelocities(s, contactIt);
         if (hasSoftRigidContact && contactIt > 0) particleRigidContactVelocities(s, contactIt);
+        skinSurfaceVertices(s);
+        updateSurfaceTriangleNormals(s);
+        updateSurfaceVertexNormals(s);
+        updateSurfaceBounds(s);
         // copyPredictedRigidBodiesToPersistentState
         for (uint32_t b = 0; b < s.B; ++b) {
             s.bodyPos[b] = s.predBodyPos[b];
@@ -1983,6 +2096,17 @@ CN_API int cno_read_particles(cno_solver *s, float *x, float *v, float *xprev)
     if (x) std::memcpy(x, s->x.data(), s->x.size() * sizeof(f4));
     if (v) std::memcpy(v, s->v.data(), s->v.size() * sizeof(f4));
     if (xprev) std::memcpy(xprev, s->xprev.data(), s->xprev.size() * sizeof(f4));
+    return CN_OK;
+}
+
+CN_API int cno_read_surface_render(cno_solver *s, float *positions, float *normals, float *world_aabbs,
+                                   float *triangle_normals)
+{
+    if (!s) return CN_ERR_INVALID_ARGUMENT;
+    if (positions) std::memcpy(positions, s->surfPos.data(), s->surfPos.size() * sizeof(f4));
+    if (normals) std::memcpy(normals, s->surfNrm.data(), s->surfNrm.size() * sizeof(f4));
+    if (world_aabbs) std::memcpy(world_aabbs, s->surfWorldAabb.data(), s->surfWorldAabb.size() * sizeof(f4));
+    if (triangle_normals) std::memcpy(triangle_normals, s->surfTriN.data(), s->surfTriN.size() * sizeof(f4));
     return CN_OK;
 }
 

@@ -45,6 +45,7 @@ def load() -> C.CDLL:
         lib.cno_meta.restype = C.c_uint32
         lib.cno_meta.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
         lib.cno_fluid_material.argtypes = [C.c_float] * 7 + [C.c_void_p]
+        lib.cno_read_surface_render.argtypes = [C.c_void_p] * 5
         _lib = lib
     return _lib
 
@@ -63,6 +64,9 @@ class Oracle:
             raise RuntimeError("oracle: create failed")
         self.n = soa.particle_count
         self.segments = soa.strand_segment_count
+        sr = soa.surface_render
+        self.surface = (sr.contents.vertex_count, sr.contents.triangle_count, sr.contents.surface_count) if sr \
+            else (0, 0, 0)
 
     def close(self):
         if self._h:
@@ -98,6 +102,16 @@ class Oracle:
         if self.segments:
             self._lib.cno_read_strand_orientations(self._h, q.ctypes.data)
         return q
+
+    def read_surface_render(self):
+        """(render positions V x 4, render normals V x 4, world AABBs S x 8, triangle normals T x 4)."""
+        V, T, S = self.surface
+        pos = np.zeros((V, 4), np.float32)
+        nrm = np.zeros((V, 4), np.float32)
+        box = np.zeros((S, 8), np.float32)
+        tri = np.zeros((T, 4), np.float32)
+        self._lib.cno_read_surface_render(self._h, pos.ctypes.data, nrm.ctypes.data, box.ctypes.data, tri.ctypes.data)
+        return pos, nrm, box, tri
 
     def debug_read(self, name: str) -> np.ndarray:
         which = DEBUG[name]
