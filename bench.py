@@ -302,10 +302,12 @@ def run_ours(args):
         "clocks": clk,
         "meta_status": meta["status"],
     }
-    # the batched / served and differentiable forms are single-GPU workloads of their own: they
-    # run once, in single-GPU runs, rather than on every rank of a scaling run
-    if world == 1 and args.serve_scenes > 0:
-        line["served"] = run_served(args, stream, sh)
+    # the batched / served form shards its scene pool across the ranks; the differentiable form
+    # and the other configurations are single-GPU workloads of their own
+    if args.serve_scenes > 0:
+        served = run_served(args, stream, sh, rank, world)
+        if rank == 0:
+            line["served"] = served
     if world == 1 and not args.no_diff:
         line["differentiation"] = run_diff(stream)
     if world == 1 and not args.no_configs:
@@ -320,18 +322,26 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
-def run_served(args, stream, sh) -> dict:
+def run_served(args, stream, sh, rank: int = 0, world: int = 1) -> dict:
     """The batched and served forms on a pool of soft-tissue scenes (2K-60K tets, log-uniform),
     against the plain per-scene drop-in (one cn_solver per scene) on the same pool.
 
     plain: one frame of every scene, scene after scene, each through its own solver;
     batched: one tick stepping every scene together (saturated);
     served: Poisson arrivals of 1-8-frame requests with drifting tool poses, replayed in real
-    time through the server (admission by a device-memory budget, continuous batching)."""
+    time through the server (admission by a device-memory budget, continuous batching).
+
+    With several ranks the pool is sharded at scene granularity (scene k on rank k mod N, its
+    requests with it; no collective on the data path): each rank runs its shard, times are the
+    slowest rank's and counts add up (the pool is fixed: strong scaling).  Returns the whole-job
+    figures on rank 0, None elsewhere."""
     import torch
+    import torch.distributed as dist
     from cn_physics import Batch, Server, Solver, batch_desc, serving
 
-    pool = serving.tissue_pool(args.serve_scenes, seed=0)
+    count = args.serve_scenes
+    mine = list(range(rank, count, world))
+    pool = serving.tissue_pool(count, seed=0, indices=mine)
     P = sum(sc.particles for sc in pool)
     T = sum(sc.tets for sc in pool)
     E = sum(sc.world.counts()["edges"] for sc in pool)
@@ -348,11 +358,13 @@ def run_served(args, stream, sh) -> dict:
         solvers.append(sv)
     serving.plain_round(pool, solvers, dt, sh)  # graph capture + warm-up
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
     ev[0].record(stream)
     serving.plain_round(pool, solvers, dt, sh)
     ev[1].record(stream)
     torch.cuda.synchronize()
-    plain_ms = ev[0].elapsed_time(ev[1])
+    plain_ms = max_over_ranks(ev[0].elapsed_time(ev[1]), world)
     for sv in solvers:
         sv.close()
     del solvers
@@ -368,11 +380,13 @@ def run_served(args, stream, sh) -> dict:
     torch.cuda.synchronize()
     ticks = []
     for _ in range(5):
+        if world > 1:
+            dist.barrier()
         ev[0].record(stream)
         b.step(ids, dt, sh)
         ev[1].record(stream)
         torch.cuda.synchronize()
-        ticks.append(ev[0].elapsed_time(ev[1]))
+        ticks.append(max_over_ranks(ev[0].elapsed_time(ev[1]), world))
     tick_ms = float(np.median(ticks))
     b.close()
 
@@ -382,20 +396,38 @@ def run_served(args, stream, sh) -> dict:
     srv = Server(b, dt)
     sids = [srv.register(sc.world.soa()) for sc in pool]
     prefetched = sum(1 for k in sids if srv.admit(k))  # warm start: resident before the clock starts
-    reqs = serving.poisson_requests(pool, steps_per_second=args.serve_rate, duration_s=args.serve_seconds, seed=1)
+    poses = [serving.tool_start(d) for d in serving.pool_dims(count, seed=0)]
+    reqs = serving.poisson_requests(poses, steps_per_second=args.serve_rate, duration_s=args.serve_seconds, seed=1)
+    _, reqs = serving.shard(reqs, count, rank, world)
+    if world > 1:
+        dist.barrier()
     out = serving.serve(srv, pool, sids, reqs, sh)
-    st = out["stats"]
     bstats = b.stats()
     srv.close()
     b.close()
+    part = {"out": out, "P": P, "T": T, "E": E, "prefetched": prefetched, "budget_bytes": bstats["budget_bytes"],
+            "budget_used_bytes": bstats["budget_used_bytes"], "tune": tune}
+    parts = [part]
+    if world > 1:
+        parts = [None] * world
+        dist.all_gather_object(parts, part)
+    if rank != 0:
+        return None
+    merged = serving.merge_served([q["out"] for q in parts])
+    P = sum(q["P"] for q in parts)
+    T = sum(q["T"] for q in parts)
+    E = sum(q["E"] for q in parts)
+    prefetched = sum(q["prefetched"] for q in parts)
     plain_rate = P * sub / (plain_ms / 1e3)
     batched_rate = P * sub / (tick_ms / 1e3)
-    served_rate = st["particle_substeps"] / out["elapsed_s"]
+    served_rate = merged["particle_substeps"] / merged["elapsed_s"]
+    tick_p = [q["out"]["stats"] for q in parts]
     return {
-        "workload": f"tissue_pool_{len(pool)}: XPBD tissue blocks, tets log-uniform 2K-60K, per-tet compliance "
+        "workload": f"tissue_pool_{count}: XPBD tissue blocks, tets log-uniform 2K-60K, per-tet compliance "
                     f"log-normal (sigma 0.5), kinematic capsule tool, dt 1/60, {sub} substep x "
                     f"{desc.default_iterations} iterations",
-        "scenes": len(pool), "particles": P, "tets": T, "edges": E, "unit": "particle-substeps/s",
+        "scenes": count, "particles": P, "tets": T, "edges": E, "unit": "particle-substeps/s",
+        "ranks": world, "sharding": "scene k on rank k mod N, no data-path collective" if world > 1 else None,
         "plain": {"value": round(plain_rate, 1), "round_ms": round(plain_ms, 3),
                   "method": "one cn_solver per scene, one frame of every scene in turn (CUDA-graph replays)"},
         "batched": {"value": round(batched_rate, 1), "tick_ms_p50": round(tick_ms, 3),
@@ -404,14 +436,17 @@ def run_served(args, stream, sh) -> dict:
                     "autotune_candidates": tune["candidates"]},
         "batched_over_plain": round(batched_rate / plain_rate, 2),
         "served": {"offered_frames_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds,
-                   "requests": out["requests"], "frames": st["scene_steps"], "value": round(served_rate, 1),
-                   "frames_per_s": round(st["scene_steps"] / out["elapsed_s"], 1),
-                   "elapsed_s": round(out["elapsed_s"], 3),
-                   "request_latency_ms": {"p50": round(out["latency_ms_p50"], 3), "p99": round(out["latency_ms_p99"], 3)},
-                   "step_latency_ms": {"p50": round(st["tick_ms_p50"], 3), "p99": round(st["tick_ms_p99"], 3)},
-                   "ticks": st["ticks"], "prefetched_scenes": prefetched,
-                   "admissions_during_run": st["admissions"] - prefetched, "evictions": st["evictions"],
-                   "budget_bytes": bstats["budget_bytes"], "budget_used_bytes": bstats["budget_used_bytes"]},
+                   "requests": merged["requests"], "frames": merged["frames"], "value": round(served_rate, 1),
+                   "frames_per_s": round(merged["frames"] / merged["elapsed_s"], 1),
+                   "elapsed_s": round(merged["elapsed_s"], 3),
+                   "request_latency_ms": {"p50": round(merged["latency_ms_p50"], 3),
+                                          "p99": round(merged["latency_ms_p99"], 3)},
+                   "step_latency_ms": {"p50": round(max(x["tick_ms_p50"] for x in tick_p), 3),
+                                       "p99": round(max(x["tick_ms_p99"] for x in tick_p), 3)},
+                   "ticks": merged["ticks"], "prefetched_scenes": prefetched,
+                   "admissions_during_run": merged["admissions"] - prefetched, "evictions": merged["evictions"],
+                   "budget_bytes": sum(q["budget_bytes"] for q in parts),
+                   "budget_used_bytes": sum(q["budget_used_bytes"] for q in parts)},
     }
 
 

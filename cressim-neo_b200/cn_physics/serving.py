@@ -35,6 +35,13 @@ class TissueScene:
     tool_pose: np.ndarray = field(default_factory=lambda: np.zeros(3, np.float32))
 
 
+def tool_start(cells) -> np.ndarray:
+    """Initial tool pose of a pool scene: resting just above the lattice top."""
+    cy = max(int(cells[1]), 1)
+    top = (cy - 0.25) * SPACING + 0.002
+    return np.array([0.0, top + TOOL_RADIUS + 0.004, 0.0], np.float32)
+
+
 def tissue_scene(cells=(10, 6, 10), seed: int = 0, compliance_sigma: float = 0.5) -> TissueScene:
     cx, cy, cz = (max(int(c), 1) for c in cells)
     rng = np.random.default_rng(seed)
@@ -46,8 +53,7 @@ def tissue_scene(cells=(10, 6, 10), seed: int = 0, compliance_sigma: float = 0.5
     w.add_soft_body_grid(size, SPACING, position=(0.0, size[1] * 0.5 + 0.002, 0.0), radius=0.4 * SPACING,
                          edge_compliance=1e-5, volume_compliance=1e-6, static_particles=pinned, friction=0.3)
     scenes.ground(w)
-    top = size[1] + 0.002
-    tool_pos = np.array([0.0, top + TOOL_RADIUS + 0.004, 0.0], np.float32)
+    tool_pos = tool_start((cx, cy, cz))
     tool = w.add_rigid_body("kinematic", position=tuple(float(v) for v in tool_pos))
     w.add_collider(tool, "capsule", (TOOL_RADIUS, TOOL_HALF_HEIGHT), local_orientation=(0.0, 0.0, 0.7071068, 0.7071068),
                    friction=0.2)
@@ -61,19 +67,49 @@ def tissue_scene(cells=(10, 6, 10), seed: int = 0, compliance_sigma: float = 0.5
     return TissueScene(w, tool, (cx, cy, cz), c["tets"], c["particles"], tool_pos)
 
 
-def tissue_pool(count: int = 512, seed: int = 0, tet_range=(2000, 60000)) -> list:
-    """`count` scenes with tet counts log-uniform in `tet_range`, built from seeded lattice dims."""
+def pool_dims(count: int = 512, seed: int = 0, tet_range=(2000, 60000)) -> list:
+    """Seeded lattice dims of the pool's scenes (tet counts log-uniform in `tet_range`)."""
     rng = np.random.default_rng(seed)
     out = []
-    for k in range(count):
+    for _ in range(count):
         target = math.exp(rng.uniform(math.log(tet_range[0]), math.log(tet_range[1])))
         cells = target / 5.0
         a = rng.uniform(0.7, 1.4, size=3)
         a = a / np.cbrt(np.prod(a))
         side = np.cbrt(cells)
-        dims = tuple(max(2, int(round(side * r))) for r in a)
-        out.append(tissue_scene(dims, seed=seed * 100003 + k))
+        out.append(tuple(max(2, int(round(side * r))) for r in a))
     return out
+
+
+def tissue_pool(count: int = 512, seed: int = 0, tet_range=(2000, 60000), indices=None) -> list:
+    """`count` scenes with tet counts log-uniform in `tet_range`, built from seeded lattice dims;
+    with `indices`, only those scenes of the pool (a rank's shard), each as the whole pool has it."""
+    dims = pool_dims(count, seed, tet_range)
+    ks = range(count) if indices is None else indices
+    return [tissue_scene(dims[k], seed=seed * 100003 + k) for k in ks]
+
+
+def shard(requests: list, count: int, rank: int, world: int):
+    """Scene-granular partition of a pool of `count` scenes: scene k is served by rank k mod world.
+    Returns the rank's global scene indices and its requests, re-indexed into its shard (arrival
+    times unchanged)."""
+    mine = list(range(rank, count, world))
+    local = {g: i for i, g in enumerate(mine)}
+    return mine, [Request(r.arrival, local[r.scene], r.steps, r.targets) for r in requests if r.scene in local]
+
+
+def merge_served(parts: list) -> dict:
+    """Whole-job figures of a sharded run from every rank's serve() result: frames and
+    particle-substeps add up, the wall time is the slowest rank's, latency percentiles are taken
+    over every request."""
+    lat = np.concatenate([np.asarray(p["latencies_ms"], np.float64) for p in parts]) if parts else np.zeros(0)
+    st = [p["stats"] for p in parts]
+    return {"elapsed_s": max(p["elapsed_s"] for p in parts), "requests": sum(p["requests"] for p in parts),
+            "frames": sum(x["scene_steps"] for x in st), "particle_substeps": sum(x["particle_substeps"] for x in st),
+            "ticks": sum(x["ticks"] for x in st), "admissions": sum(x["admissions"] for x in st),
+            "evictions": sum(x["evictions"] for x in st),
+            "latency_ms_p50": float(np.percentile(lat, 50)) if lat.size else None,
+            "latency_ms_p99": float(np.percentile(lat, 99)) if lat.size else None}
 
 
 @dataclass
@@ -86,11 +122,12 @@ class Request:
 
 def poisson_requests(pool: list, steps_per_second: float = 20000.0, duration_s: float = 1.0, seed: int = 0,
                      drift: float = 0.001) -> list:
-    """Poisson arrivals carrying `steps_per_second` frames per second in total (1-8 frames each)."""
+    """Poisson arrivals carrying `steps_per_second` frames per second in total (1-8 frames each).
+    `pool`: the scenes, or their initial tool poses."""
     rng = np.random.default_rng(seed)
     rate = steps_per_second / 4.5
     t, out = 0.0, []
-    poses = [sc.tool_pose.copy() for sc in pool]
+    poses = [np.array(sc.tool_pose if hasattr(sc, "tool_pose") else sc, np.float32) for sc in pool]
     quat = np.array([0.0, 0.0, 0.7071068, 0.7071068], np.float32)
     while True:
         t += rng.exponential(1.0 / rate)
@@ -125,7 +162,7 @@ def serve(server: Server, pool: list, pool_ids: list, requests: list, stream: in
     done = server.poll()
     lat = np.array([d["done_s"] - d["submit_s"] for d in done]) * 1e3
     st = server.stats()
-    return {"elapsed_s": elapsed, "requests": len(done), "stats": st,
+    return {"elapsed_s": elapsed, "requests": len(done), "stats": st, "latencies_ms": lat.tolist(),
             "latency_ms_p50": float(np.percentile(lat, 50)) if lat.size else None,
             "latency_ms_p99": float(np.percentile(lat, 99)) if lat.size else None}
 
