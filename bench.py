@@ -254,9 +254,8 @@ def run_ours(args):
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        assert lib.cn_solver_write_particles(solver._h, xp, vp, n) == 0
-        solver.step_many(dt, 1, sh)
-        assert lib.cn_solver_read_particles(solver._h, xp, vp, None, n) == 0
+        # upload x, v -> frame -> read x, v back, in order on the stream, one wait per frame
+        assert lib.cn_solver_step_io(solver._h, C.c_float(dt), xp, vp, xp, vp, C.c_void_p(sh)) == 0
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e_value = whole_job_rate(n, substeps, e2e_steps, world, e2e_s)

@@ -969,6 +969,24 @@ CN_API cn_status cn_solver_write_particles(cn_solver *sv, const float *x, const 
     return CN_OK;
 }
 
+CN_API cn_status cn_solver_step_io(cn_solver *sv, float frame_dt, const float *x_in, const float *v_in, float *x_out,
+                                   float *v_out, void *stream)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_step_io: null solver");
+    if (!sv->synced) return setError(CN_ERR_NOT_INITIALIZED, "cn_solver_step_io: no world synced");
+    CN_CUDA(cudaSetDevice(sv->device));
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : sv->ownStream;
+    const size_t bytes = sizeof(float4) * sv->s.N;
+    if (x_in) CN_CUDA(cudaMemcpyAsync(sv->s.x, x_in, bytes, cudaMemcpyHostToDevice, st));
+    if (v_in) CN_CUDA(cudaMemcpyAsync(sv->s.v, v_in, bytes, cudaMemcpyHostToDevice, st));
+    const cn_status r = runFrames(sv, frame_dt, 1, st);
+    if (r != CN_OK) return r;
+    if (x_out) CN_CUDA(cudaMemcpyAsync(x_out, sv->s.x, bytes, cudaMemcpyDeviceToHost, st));
+    if (v_out) CN_CUDA(cudaMemcpyAsync(v_out, sv->s.v, bytes, cudaMemcpyDeviceToHost, st));
+    CN_CUDA(cudaStreamSynchronize(st));
+    return CN_OK;
+}
+
 CN_API cn_status cn_solver_read_strand_orientations(cn_solver *sv, float *q, uint32_t count)
 {
     if (!sv || !q) return setError(CN_ERR_INVALID_ARGUMENT, "read_strand_orientations: null argument");

@@ -551,6 +551,14 @@ CN_API cn_status cn_solver_write_particles(cn_solver *solver, const float *posit
                                            const float *velocities, uint32_t count);
 CN_API cn_status cn_solver_read_strand_orientations(cn_solver *solver, float *orientations,
                                                     uint32_t count);
+/* One frame with host state in and out (uploadParticles, physics_scene_gpu_state.cpp:3163, then
+ * PhysicsSolver::step with its blocking readback, :4082-4155): float4[N] positions / velocities
+ * are copied to the device (NULL: keep the device state), the frame runs, and the resulting
+ * state is copied back (NULL: skip), all in order on `stream` (NULL: the solver's own) with one
+ * wait at the end.  Host buffers should be pinned for full copy bandwidth. */
+CN_API cn_status cn_solver_step_io(cn_solver *solver, float frame_dt, const float *positions_in,
+                                   const float *velocities_in, float *positions_out, float *velocities_out,
+                                   void *stream);
 
 /* Debug switches (no reference counterpart; all off by default):
  *  CN_DEBUG_KEEP_FLUID_DELTA   keep the last iteration's packed fluid delta for cn_solver_debug_read;

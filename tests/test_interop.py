@@ -50,3 +50,31 @@ def test_incremental_update_equals_a_fresh_sync():
     xa, va, _ = a.read_particles()
     xb, vb, _ = b.read_particles()
     assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+
+
+def test_step_io_equals_write_step_read():
+    """cn_solver_step_io (upload, frame, blocking readback on one stream) gives the bits of the
+    three separate calls."""
+    import ctypes as C
+    import torch
+    w, desc, dt = scenes.xpbd_cube(n=8, spacing=0.1, pin_bottom=False, lift=0.02)
+    soa = w.soa()
+    a, b = Solver(desc), Solver(desc)
+    a.sync_world(soa)
+    b.sync_world(soa)
+    x0, v0, _ = a.read_particles()
+    x0 = x0.copy()
+    x0[:, 1] += 0.01
+    n = x0.shape[0]
+    xh = torch.from_numpy(x0.copy()).pin_memory()
+    vh = torch.from_numpy(v0.copy()).pin_memory()
+    f = lambda t: C.cast(t.data_ptr(), C.POINTER(C.c_float))
+    for _ in range(3):
+        assert a._lib.cn_solver_step_io(a._h, C.c_float(dt), f(xh), f(vh), f(xh), f(vh), None) == 0
+    b.write_particles(x0, v0)
+    for _ in range(3):
+        xb, vb, _ = b.read_particles()
+        b.write_particles(xb, vb)
+        b.step(dt)
+    xb, vb, _ = b.read_particles()
+    assert np.array_equal(xh.numpy(), xb) and np.array_equal(vh.numpy(), vb)
