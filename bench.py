@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--e2e-steps", type=int, default=20)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="frames of the e2e run (0: the timed frames again)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--dims", type=str, default="128,64,128", help="fluid lattice (profiling runs use smaller ones)")
     ap.add_argument("--serve-scenes", type=int, default=512, help="tissue scenes of the served/batched pool (0: skip)")
@@ -238,17 +238,18 @@ def run_ours(args):
     solver.set_timing(False)
     probe_frame_ms = sum(t for t, _ in ktimes.values())
 
-    # e2e through the C ABI: pinned host state uploaded and read back every frame
+    # e2e through the C ABI: the timed frames again, from the same state, with the pinned host
+    # state uploaded and read back every frame
     xh = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
     vh = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
-    x, v, _ = solver.read_particles()
-    xh.numpy()[:] = x
-    vh.numpy()[:] = v
+    solver.write_particles(x0, v0)
+    xh.numpy()[:] = x0
+    vh.numpy()[:] = v0
     lib = solver._lib
     import ctypes as C
     xp = C.cast(xh.data_ptr(), C.POINTER(C.c_float))
     vp = C.cast(vh.data_ptr(), C.POINTER(C.c_float))
-    e2e_steps = max(1, min(args.e2e_steps, args.steps))
+    e2e_steps = args.steps if args.e2e_steps <= 0 else max(1, min(args.e2e_steps, args.steps))
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
