@@ -247,13 +247,18 @@ class World:
         return out.value
 
     def add_rigid_body(self, body_type="static", position=(0, 0, 0), orientation=(0, 0, 0, 1),
-                       scale=(1, 1, 1)) -> int:
+                       scale=(1, 1, 1), *, mass=None, inverse_inertia=None) -> int:
+        """RigidBodyState: mass and local inverse inertia matter for dynamic bodies."""
         d = _abi.RigidBodyDesc()
         self._lib.cn_rigid_body_desc_defaults(C.byref(d))
         d.body_type = {"static": 0, "kinematic": 1, "dynamic": 2}[body_type]
         d.position = (C.c_float * 3)(*position)
         d.orientation = (C.c_float * 4)(*orientation)
         d.scale = (C.c_float * 3)(*scale)
+        if mass is not None:
+            d.mass = mass
+        if inverse_inertia is not None:
+            d.inverse_inertia_local = (C.c_float * 3)(*inverse_inertia)
         out = C.c_uint32()
         _check(self._lib.cn_world_add_rigid_body(self._h, C.byref(d), C.byref(out)))
         return out.value
@@ -398,6 +403,7 @@ class Solver:
         _check(self._lib.cn_solver_sync_world(self._h, C.byref(soa)))
         self._n = soa.particle_count
         self._segments = soa.strand_segment_count
+        self._bodies = soa.rigid_body_count
 
     def step(self, dt: float, stream: int = 0) -> None:
         _check(self._lib.cn_solver_step(self._h, dt, C.c_void_p(stream) if stream else None))
@@ -433,6 +439,13 @@ class Solver:
         arr = (_abi.KernelTime * max(n.value, 1))()
         _check(self._lib.cn_solver_kernel_times(self._h, arr, n.value, C.byref(n)))
         return {arr[i].name.decode(): (arr[i].milliseconds, arr[i].launches) for i in range(n.value)}
+
+    def read_rigid_bodies(self, count: Optional[int] = None):
+        """(positions with inverse mass, orientations, linear, angular velocities), each (B, 4)."""
+        n = self._bodies if count is None else count
+        out = [np.zeros((n, 4), np.float32) for _ in range(4)]
+        _check(self._lib.cn_solver_read_rigid_bodies(self._h, *(a.ctypes.data for a in out), n))
+        return tuple(out)
 
     def read_surface_render(self):
         """(render positions V x 4, render normals V x 4, surface world AABBs S x 8) after the last frame."""

@@ -271,6 +271,7 @@ SIGNATURES = [
     ("cn_solver_set_kinematic_target", C.c_int, [C.c_void_p, u32, P_f32, P_f32]),
     ("cn_solver_scene_view", C.c_int, [C.c_void_p, C.POINTER(SceneView)]),
     ("cn_solver_surface_render_view", C.c_int, [C.c_void_p, C.POINTER(SurfaceRenderView)]),
+    ("cn_solver_read_rigid_bodies", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, u32]),
     ("cn_solver_step_io", C.c_int, [C.c_void_p, f32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cn_solver_read_surface_render", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("cn_surface_mesh_desc_defaults", None, [C.POINTER(SurfaceMeshDesc)]),

@@ -122,6 +122,9 @@ struct Scene {
     float4 *prevBodyPos = nullptr, *prevBodyRot = nullptr;
     float4 *predBodyPos = nullptr, *predBodyRot = nullptr, *predBodyLin = nullptr, *predBodyAng = nullptr;
     float4 *colAabbMin = nullptr, *colAabbMax = nullptr;
+    // dynamic bodies: corrections summed (float atomics) over a pass, applied per body after it
+    uint32_t hasDynamic = 0;
+    float4 *bodyTransCorr = nullptr, *bodyRotCorr = nullptr, *bodyLinVelCorr = nullptr, *bodyAngVelCorr = nullptr;
     // Per collider, the world frame the fluid boundary queries use this substep (4 float4:
     // centre + shape/enabled word, orientation, shape extents, capsule end).
     float4 *colFrame = nullptr;
@@ -207,6 +210,8 @@ struct Config {
     float fluidSolveCoefficient, fluidRelaxation, fluidBoundaryDensityScale, fluidBoundaryDeltaScale;
     float fluidMaxUnderDensityRatio;
     float gravity[3];
+    // per-iteration caps on a dynamic body's summed corrections (physics_solver_config.hlsli:31-34)
+    float maxTranslationCorrection, maxRotationCorrection, maxLinearVelocityCorrection, maxAngularVelocityCorrection;
 };
 
 // A kinematic target staged for a batch tick: pos.xyz, pos.w = the body index (bits); rot = xyzw.
@@ -243,6 +248,12 @@ void launchFluidBoundaryVelocities(const Scene &s, float dt, const Config &c, cu
 void launchRigidContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st);
 void launchParticleContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st);
 void launchCopyPredictedRigid(const Scene &s, cudaStream_t st);
+// Dynamic bodies: summed position corrections applied (physics_rigid_apply_corrections), velocities
+// from the pose change (physics_rigid_update_velocities), and the particle-rigid velocity
+// iterations with the bodies' velocity corrections applied after each.
+void launchApplyRigidCorrections(const Scene &s, const Config &c, cudaStream_t st);
+void launchUpdateRigidVelocities(const Scene &s, float dt, cudaStream_t st);
+void launchRigidContactVelocitiesDynamic(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st);
 // Skinning, triangle and vertex normals, chunk and surface AABBs from the current positions.
 void launchSurfaceRender(const Scene &s, cudaStream_t st);
 // debug export of the compacted cell-range table (reference layout)

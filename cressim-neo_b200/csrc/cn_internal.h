@@ -92,6 +92,10 @@ inline Config configFromDesc(const cn_solver_desc &d)
     c.fluidBoundaryDeltaScale = d.fluid.boundary_delta_scale;
     c.fluidMaxUnderDensityRatio = d.fluid.max_under_density_ratio;
     c.gravity[0] = d.gravity[0]; c.gravity[1] = d.gravity[1]; c.gravity[2] = d.gravity[2];
+    c.maxTranslationCorrection = d.rigid.max_translation_correction_per_iteration;
+    c.maxRotationCorrection = d.rigid.max_rotation_correction_per_iteration;
+    c.maxLinearVelocityCorrection = d.rigid.max_linear_velocity_correction_per_iteration;
+    c.maxAngularVelocityCorrection = d.rigid.max_angular_velocity_correction_per_iteration;
     return c;
 }
 

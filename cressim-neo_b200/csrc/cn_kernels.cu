@@ -123,7 +123,7 @@ __device__ __forceinline__ void rigidPredictBody(const Scene &s, float dt, float
     } else {
         const f3 l = xyz(lin) + f3{gx, gy, gz} * dt;
         s.predBodyPos[b] = mk4(xyz(p) + l * dt, p.w);
-        s.predBodyRot[b] = q;
+        s.predBodyRot[b] = integrateOrientation(q, xyz(ang), dt);
         s.predBodyLin[b] = mk4(l, lin.w);
         s.predBodyAng[b] = ang;
     }
@@ -1633,20 +1633,27 @@ __device__ __forceinline__ RigidContact generateRigidContact(const Scene &s, uin
     return out;
 }
 
-// physics_particle_rigid_solve_contacts.cs.hlsl:27-141 for one contact (static/kinematic body:
-// only the particle moves).
-__device__ __forceinline__ f3 solveRigidContact(const Scene &s, const Config &cfg, const RigidContact &c, float4 sp,
-                                                const ContactParticle &pt)
+// physics_particle_rigid_solve_contacts.cs.hlsl:27-141 for one contact: the particle's correction
+// and, for a dynamic body, the body's translation / rotation corrections.
+struct ContactCorrection {
+    f3 soft, rigidT, rigidR;
+    bool rigid;
+};
+
+__device__ __forceinline__ ContactCorrection solveRigidContact(const Scene &s, const Config &cfg,
+                                                               const RigidContact &c, float4 sp,
+                                                               const ContactParticle &pt)
 {
+    ContactCorrection out{f3{0.f, 0.f, 0.f}, f3{0.f, 0.f, 0.f}, f3{0.f, 0.f, 0.f}, false};
     const uint32_t b = c.body;
     const float iS = sp.w;
     const f3 prevS = pt.prev;
     const float4 prevB = s.prevBodyPos[b], predB = s.predBodyPos[b];
     const float4 prevQ = qNormalize(s.prevBodyRot[b]), predQ = qNormalize(s.predBodyRot[b]);
     const float iR = s.bodyType[b] == CN_BODY_DYNAMIC ? predB.w : 0.0f;
-    if (iS <= kEps && iR <= kEps) return f3{0.f, 0.f, 0.f};
+    if (iS <= kEps && iR <= kEps) return out;
     const float pen = mn(mx(c.normalPenetration.w - cfg.slop, 0.0f), cfg.softMaxCorrection);
-    if (pen <= 0.0f) return f3{0.f, 0.f, 0.f};
+    if (pen <= 0.0f) return out;
     const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
     f3 inI = xyz(s.bodyInvInertia[b]);
     const f3 mat = combineContactMaterial(pt.material, s.colMat[c.collider]);
@@ -1656,9 +1663,11 @@ __device__ __forceinline__ f3 solveRigidContact(const Scene &s, const Config &cf
     const f3 rR = cp - xyz(predB);
     const float nmR = contactEffectiveMass(iR, inI, predQ, rR, n);
     const float denom = iS + nmR;
-    if (denom <= kEps) return f3{0.f, 0.f, 0.f};
+    if (denom <= kEps) return out;
     const float lambda = (pen / denom) * cfg.softContactRelaxation;
     f3 corr = n * (iS * lambda);
+    f3 rt = -n * (iR * lambda);
+    f3 rr = -mulWorldInvInertia(inI, predQ, cross(rR, n)) * lambda;
     const f3 relDisp = (cp - prevCP) - (xyz(sp) - prevS);
     const f3 fd = positionFrictionDelta(projectOntoTangent(relDisp, n), pen, mat.x, mat.z,
                                         cfg.positionFrictionMinDistance);
@@ -1670,10 +1679,24 @@ __device__ __forceinline__ f3 solveRigidContact(const Scene &s, const Config &cf
         if (tden > kEps) {
             const float tl = fdist / tden;
             corr += t * (tl * iS * cfg.softContactRelaxation);
+            rt -= t * (tl * iR * cfg.softContactRelaxation);
+            rr -= mulWorldInvInertia(inI, predQ, cross(rR, t)) * (tl * cfg.softContactRelaxation);
         }
     }
-    if (iS > kEps) return corr;
-    return f3{0.f, 0.f, 0.f};
+    if (iS > kEps) out.soft = corr;
+    if (iR > kEps) {
+        out.rigidT = rt;
+        out.rigidR = rr;
+        out.rigid = true;
+    }
+    return out;
+}
+
+__device__ __forceinline__ void atomicAdd3(float4 *p, f3 v)
+{
+    atomicAdd(&p->x, v.x);
+    atomicAdd(&p->y, v.y);
+    atomicAdd(&p->z, v.z);
 }
 
 // Generate + solve every candidate pair of particle i (pairs are particle-major), then either
@@ -1696,11 +1719,15 @@ __device__ __forceinline__ void rigidContactsAt(const Scene &s, const Config &cf
             const RigidContact c = generateRigidContact(s, i, pr.y, pt);
             s.rigidContacts[pi] = c;
             if (!c.active) continue;
-            const f3 d = solveRigidContact(s, cfg, c, sp, pt);
-            // float atomic order of the reference == pair order here
+            const ContactCorrection d = solveRigidContact(s, cfg, c, sp, pt);
+            // the particle's float-atomic order of the reference == pair order here
             if (sp.w > kEps) {
-                corr = corr + d;
+                corr = corr + d.soft;
                 any = true;
+            }
+            if (d.rigid) { // many particles push one body: float atomics, as the reference
+                atomicAdd3(&s.bodyTransCorr[pr.y], d.rigidT);
+                atomicAdd3(&s.bodyRotCorr[pr.y], d.rigidR);
             }
         }
     }
@@ -1864,6 +1891,127 @@ __device__ __forceinline__ void rigidContactVelocitiesAt(const Scene &s, uint32_
 __global__ void __launch_bounds__(kThreads) k_rigidContactVelocities(Scene s, uint32_t iterations, Config cfg)
 {
     forEachElem(s.wP, s.N, [&](uint32_t i) { rigidContactVelocitiesAt(s, iterations, cfg, i); });
+}
+
+// ------------------------------------------------------------------------------------------
+// Dynamic bodies
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ f3 clampLength(f3 v, float maxLen)
+{
+    const float l = length(v);
+    if (l > maxLen && l > kEps) v = v * (maxLen / l);
+    return v;
+}
+
+// physics_rigid_apply_corrections.cs.hlsl:13-54 (clears the sums for the next pass)
+__global__ void k_applyRigidCorrections(Scene s, Config cfg)
+{
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.B) return;
+    float4 p = s.predBodyPos[b];
+    float4 q = qNormalize(s.predBodyRot[b]);
+    f3 tc = xyz(s.bodyTransCorr[b]);
+    f3 rc = xyz(s.bodyRotCorr[b]);
+    if (s.bodyType[b] == CN_BODY_DYNAMIC && p.w != 0.0f) {
+        tc = clampLength(tc, cfg.maxTranslationCorrection);
+        rc = clampLength(rc, cfg.maxRotationCorrection);
+        p = mk4(xyz(p) + tc, p.w);
+        q = qNormalize(qMul(qFromRotationVector(rc), q));
+    }
+    s.predBodyPos[b] = p;
+    s.predBodyRot[b] = q;
+    s.bodyTransCorr[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+    s.bodyRotCorr[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// physics_rigid_update_velocities.cs.hlsl:14-51
+__global__ void k_updateRigidVelocities(Scene s, float dt)
+{
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.B) return;
+    const float4 prevP = s.prevBodyPos[b];
+    const float4 prevQ = qNormalize(s.prevBodyRot[b]);
+    const float4 p = s.predBodyPos[b];
+    float4 q = qNormalize(s.predBodyRot[b]);
+    if (s.bodyType[b] == CN_BODY_STATIC) {
+        s.predBodyRot[b] = qNormalize(q);
+        s.predBodyLin[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+        s.predBodyAng[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const f3 l = (xyz(p) - xyz(prevP)) / mx(dt, kEps);
+    const f3 a = angularVelocityFromQuaternionDelta(prevQ, q, mx(dt, kEps));
+    s.predBodyRot[b] = q;
+    s.predBodyLin[b] = mk4(l, 0.0f);
+    s.predBodyAng[b] = mk4(a, 0.0f);
+}
+
+// One iteration of physics_particle_rigid_solve_contact_velocities.cs.hlsl:30-123 with dynamic
+// bodies: a particle's impulses from its contacts (pair order, its velocity of this iteration)
+// are applied to it directly (physics_particle_apply_contact_velocities); the bodies' shares are
+// summed with float atomics and applied by k_applyRigidContactVelocities.
+__global__ void __launch_bounds__(kThreads) k_rigidContactVelocityStep(Scene s, Config cfg)
+{
+    forEachElem(s.wP, s.N, [&](uint32_t i) {
+        const uint32_t cnt = s.candCount[i];
+        const uint32_t off = s.candOffset[i];
+        if (cnt == 0u) return;
+        const float iS = s.x[i].w;
+        const float4 v0 = s.v[i];
+        const uint32_t lim = s.meta_->rigidPairCount;
+        const f3 vel = xyz(v0);
+        f3 corr{0.f, 0.f, 0.f};
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t pi = off + k;
+            if (pi >= lim) break;
+            const RigidContact c = s.rigidContacts[pi];
+            if (!c.active) continue;
+            const uint32_t b = c.body;
+            const float4 rp = s.predBodyPos[b];
+            const float iR = s.bodyType[b] == CN_BODY_DYNAMIC ? rp.w : 0.0f;
+            if (iS <= kEps && iR <= kEps) continue;
+            const float4 rq = qNormalize(s.predBodyRot[b]);
+            const f3 rl = xyz(s.predBodyLin[b]), ra = xyz(s.predBodyAng[b]);
+            const f3 inI = xyz(s.bodyInvInertia[b]);
+            const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
+            const f3 cp = xyz(rp) + qRotate(rq, xyz(c.rigidLocalPoint));
+            const f3 rR = cp - xyz(rp);
+            const f3 rel = vel - (rl + cross(ra, rR));
+            const float nv = dot(rel, n);
+            if (nv >= 0.0f) continue;
+            const float nd = iS + contactEffectiveMass(iR, inI, rq, rR, n);
+            if (nd <= kEps) continue;
+            const f3 mat = combineContactMaterial(s.contactMaterials[s.matIdx[i]], s.colMat[c.collider]);
+            const bool er = (-nv > cfg.restitutionVelocityThreshold) && (c.normalPenetration.w <= cfg.restitutionPenetrationThreshold);
+            const float rest = er ? saturate(mat.y) : 0.0f;
+            const float dnv = er ? (-rest * nv) : 0.0f;
+            const f3 ti = n * mx(0.0f, (dnv - nv) / nd);
+            if (iS > kEps) corr = corr + ti * iS;
+            if (iR > kEps) {
+                atomicAdd3(&s.bodyLinVelCorr[b], -ti * iR);
+                atomicAdd3(&s.bodyAngVelCorr[b], mulWorldInvInertia(inI, rq, cross(rR, -ti)));
+            }
+        }
+        if (iS > kEps) s.v[i] = mk4(vel + corr, v0.w);
+    });
+}
+
+// physics_rigid_apply_contact_velocities.cs.hlsl:14-58
+__global__ void k_applyRigidContactVelocities(Scene s, Config cfg)
+{
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= s.B) return;
+    float4 lin = s.predBodyLin[b], ang = s.predBodyAng[b];
+    if (s.bodyType[b] == CN_BODY_DYNAMIC) {
+        const f3 lc = clampLength(xyz(s.bodyLinVelCorr[b]), cfg.maxLinearVelocityCorrection);
+        const f3 ac = clampLength(xyz(s.bodyAngVelCorr[b]), cfg.maxAngularVelocityCorrection);
+        lin = mk4(xyz(lin) + lc, lin.w);
+        ang = mk4(xyz(ang) + ac, ang.w);
+    }
+    s.predBodyLin[b] = lin;
+    s.predBodyAng[b] = ang;
+    s.bodyLinVelCorr[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+    s.bodyAngVelCorr[b] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // physics_particle_solve_contact_velocities.cs.hlsl (non-proxy) with float atomics.
@@ -2243,6 +2391,26 @@ void launchRigidContactVelocities(const Scene &s, uint32_t iterations, const Con
 {
     if (s.N == 0 || iterations == 0) return;
     k_rigidContactVelocities<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, iterations, c);
+}
+
+void launchApplyRigidCorrections(const Scene &s, const Config &c, cudaStream_t st)
+{
+    if (s.B == 0) return;
+    k_applyRigidCorrections<<<blocksFor(s.B), kThreads, 0, st>>>(s, c);
+}
+
+void launchUpdateRigidVelocities(const Scene &s, float dt, cudaStream_t st)
+{
+    if (s.B == 0) return;
+    k_updateRigidVelocities<<<blocksFor(s.B), kThreads, 0, st>>>(s, dt);
+}
+
+void launchRigidContactVelocitiesDynamic(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st)
+{
+    for (uint32_t it = 0; it < iterations; ++it) {
+        if (s.N) k_rigidContactVelocityStep<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, c);
+        if (s.B) k_applyRigidContactVelocities<<<blocksFor(s.B), kThreads, 0, st>>>(s, c);
+    }
 }
 
 void launchParticleContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st)

@@ -106,6 +106,21 @@ __device__ __forceinline__ f3 angularVelocityFromQuaternionDelta(float4 prev, fl
     return im * (angle / (l * dt));
 }
 
+// physics_math.hlsli:55-73: rotation-vector quaternion and orientation integration
+__device__ __forceinline__ float4 qFromRotationVector(f3 rv)
+{
+    const float a2 = dot(rv, rv);
+    if (a2 <= kEps) return qNormalize(mk4(rv * 0.5f, 1.0f));
+    const float angle = sqrtf(a2);
+    const float half = 0.5f * angle;
+    const float sc = sinf(half) / angle;
+    return qNormalize(mk4(rv * sc, cosf(half)));
+}
+__device__ __forceinline__ float4 integrateOrientation(float4 q, f3 w, float dt)
+{
+    return qNormalize(qMul(qFromRotationVector(w * dt), q));
+}
+
 // physics_shape_common.hlsli:24-42
 __host__ __device__ __forceinline__ float sphereRadius(float4 p, float4 s)
 {

@@ -48,7 +48,7 @@ struct cn_solver {
     size_t scanScratchBytes = 0;
     float *hostX = nullptr, *hostV = nullptr;
     bool synced = false;
-    bool hasFluid = false, ppPossible = false, rigidPossible = false, hasBroadphase = false;
+    bool hasFluid = false, ppPossible = false, rigidPossible = false, hasBroadphase = false, hasDynamic = false;
     uint32_t substeps = 1, fluidIt = 1, softIt = 1, contactIt = 1, maxIt = 1;
     bool postUpdateNeighbors = false, writeFluidDebug = false, forceBroadphase = false;
     cudaGraph_t graph = nullptr;
@@ -183,6 +183,11 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
     s.predBodyPos = a.take<float4>(B); s.predBodyRot = a.take<float4>(B);
     s.predBodyLin = a.take<float4>(B); s.predBodyAng = a.take<float4>(B);
     s.colAabbMin = a.take<float4>(C); s.colAabbMax = a.take<float4>(C);
+    s.hasDynamic = sv->hasDynamic ? 1u : 0u;
+    if (sv->hasDynamic) {
+        s.bodyTransCorr = a.take<float4>(B); s.bodyRotCorr = a.take<float4>(B);
+        s.bodyLinVelCorr = a.take<float4>(B); s.bodyAngVelCorr = a.take<float4>(B);
+    }
     s.colFrame = a.take<float4>(size_t(C) * 4);
     s.colQueryOrder = a.take<uint32_t>(C);
     {
@@ -359,6 +364,12 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
         if (s.S) cudaMemsetAsync(s.segLambda, 0, sizeof(float4) * s.S, st);
         if (s.J) cudaMemsetAsync(s.jointLambda, 0, sizeof(float4) * s.J, st);
         if (s.fluidMaxDelta) cudaMemsetAsync(s.fluidMaxDelta, 0, sizeof(uint32_t) * 64, st);
+        if (s.hasDynamic) { // clearRigidCorrections (physics_rigid_clear_corrections.cs.hlsl)
+            cudaMemsetAsync(s.bodyTransCorr, 0, sizeof(float4) * s.B, st);
+            cudaMemsetAsync(s.bodyRotCorr, 0, sizeof(float4) * s.B, st);
+            cudaMemsetAsync(s.bodyLinVelCorr, 0, sizeof(float4) * s.B, st);
+            cudaMemsetAsync(s.bodyAngVelCorr, 0, sizeof(float4) * s.B, st);
+        }
         if (sv->ppPossible) {
             cudaMemsetAsync(s.posCorr, 0, sizeof(float4) * N, st);
             cudaMemsetAsync(s.velCorr, 0, sizeof(float4) * N, st);
@@ -381,15 +392,26 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             }
             if (runSoft) probe(sv, "soft_constraints", st, [&] { cn::launchSoftIteration(s, dt, c, st); });
             if (runPP || runRigid) probe(sv, "contacts", st, [&] { cn::launchContacts(s, c, runPP, runRigid, st); });
+            // applyRigidCorrections (physics_solver.cpp:1170-1177); with only static and kinematic
+            // bodies the summed corrections are zero and the pass is left out
+            if (runRigid && s.hasDynamic) cn::launchApplyRigidCorrections(s, c, st);
         }
+        // updateRigidVelocities (physics_solver.cpp:1241-1246): for static and kinematic bodies it
+        // restates what the rigid predict wrote, so it runs for scenes with dynamic bodies
+        if (s.hasDynamic) cn::launchUpdateRigidVelocities(s, dt, st);
         const float4 *fluidDelta = sv->hasFluid ? ((sv->fluidIt & 1u) ? s.Db : s.Da) : nullptr;
         probe(sv, "update_velocities", st, [&] { cn::launchUpdateVelocities(s, dt, fluidDelta, st); });
         if (sv->hasFluid) probe(sv, "fluid_boundary_velocities", st, [&] { cn::launchFluidBoundaryVelocities(s, dt, c, st); });
         if (sv->hasFluid && sv->postUpdateNeighbors) cn::launchFluidNeighborsOnly(s, st);
         if (sv->ppPossible && sv->contactIt)
             probe(sv, "contact_velocities", st, [&] { cn::launchParticleContactVelocities(s, sv->contactIt, c, st); });
-        if (sv->rigidPossible && sv->contactIt)
-            probe(sv, "contact_velocities", st, [&] { cn::launchRigidContactVelocities(s, sv->contactIt, c, st); });
+        if (sv->rigidPossible && sv->contactIt) {
+            if (s.hasDynamic)
+                probe(sv, "contact_velocities", st,
+                      [&] { cn::launchRigidContactVelocitiesDynamic(s, sv->contactIt, c, st); });
+            else
+                probe(sv, "contact_velocities", st, [&] { cn::launchRigidContactVelocities(s, sv->contactIt, c, st); });
+        }
         cn::launchCopyPredictedRigid(s, st);
     }
     // physics_solver.cpp:1310-1337 (after the last substep: see launchSurfaceRender)
@@ -527,13 +549,16 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
                 solidGroups.push_back(g);
         }
     }
+    bool anyDynamic = false;
     for (uint32_t b = 0; b < w->rigid_body_count; ++b)
-        if (w->body_types[b] == CN_BODY_DYNAMIC)
-            return setError(CN_ERR_UNSUPPORTED, "dynamic rigid bodies are outside the particle substep; use static or kinematic bodies");
+        if (w->body_types[b] == CN_BODY_DYNAMIC) anyDynamic = true;
+    if (anyDynamic && anyFluid)
+        return setError(CN_ERR_UNSUPPORTED, "fluid particles against dynamic rigid bodies are not implemented");
     for (uint32_t m = 0; m < w->fluid_material_count; ++m)
         if (w->fluid_materials[m].vorticity_confinement > 1.0e-6f)
             return setError(CN_ERR_UNSUPPORTED, "vorticity confinement is not implemented");
     sv->hasFluid = anyFluid;
+    sv->hasDynamic = anyDynamic;
     const bool contactWork = sv->contactIt > 0;
     sv->ppPossible = contactWork && N > 1 && anySolid && (anyFluid || anySelf || solidGroups.size() > 1);
     sv->rigidPossible = contactWork && N > 0 && w->collider_count > 0 && anySolid;
@@ -966,6 +991,22 @@ CN_API cn_status cn_solver_write_particles(cn_solver *sv, const float *x, const 
     if (x) CN_CUDA(cudaMemcpyAsync(sv->s.x, x, sizeof(float4) * count, cudaMemcpyHostToDevice, sv->ownStream));
     if (v) CN_CUDA(cudaMemcpyAsync(sv->s.v, v, sizeof(float4) * count, cudaMemcpyHostToDevice, sv->ownStream));
     CN_CUDA(cudaStreamSynchronize(sv->ownStream));
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_read_rigid_bodies(cn_solver *sv, float *pos, float *rot, float *lin, float *ang,
+                                             uint32_t count)
+{
+    if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_read_rigid_bodies: null solver");
+    if (count > sv->s.B) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_read_rigid_bodies: count > bodies");
+    CN_CUDA(cudaSetDevice(sv->device));
+    CN_CUDA(cudaDeviceSynchronize());
+    const size_t bytes = sizeof(float4) * count;
+    if (!count) return CN_OK;
+    if (pos) CN_CUDA(cudaMemcpy(pos, sv->s.bodyPos, bytes, cudaMemcpyDeviceToHost));
+    if (rot) CN_CUDA(cudaMemcpy(rot, sv->s.bodyRot, bytes, cudaMemcpyDeviceToHost));
+    if (lin) CN_CUDA(cudaMemcpy(lin, sv->s.bodyLin, bytes, cudaMemcpyDeviceToHost));
+    if (ang) CN_CUDA(cudaMemcpy(ang, sv->s.bodyAng, bytes, cudaMemcpyDeviceToHost));
     return CN_OK;
 }
 

@@ -551,6 +551,11 @@ CN_API cn_status cn_solver_write_particles(cn_solver *solver, const float *posit
                                            const float *velocities, uint32_t count);
 CN_API cn_status cn_solver_read_strand_orientations(cn_solver *solver, float *orientations,
                                                     uint32_t count);
+/* Blocking copy of the rigid bodies' state after the last frame (readbackPredictedRigidStateBlocking,
+ * physics_scene_gpu_state.h:423): float4[count] positions (w = inverse mass), orientations (xyzw),
+ * linear and angular velocities.  Any pointer may be NULL. */
+CN_API cn_status cn_solver_read_rigid_bodies(cn_solver *solver, float *positions_inv_mass, float *orientations,
+                                             float *linear_velocities, float *angular_velocities, uint32_t count);
 /* One frame with host state in and out (uploadParticles, physics_scene_gpu_state.cpp:3163, then
  * PhysicsSolver::step with its blocking readback, :4082-4155): float4[N] positions / velocities
  * are copied to the device (NULL: keep the device state), the frame runs, and the resulting

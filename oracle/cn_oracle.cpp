@@ -123,6 +123,24 @@ inline f3 AngularVelocityFromQuaternionDelta(f4 prev, f4 cur, float dt)
     return im * (angle / (l * dt));
 }
 
+// physics_math.hlsli:55-73
+inline f4 QuaternionFromRotationVector(f3 rv)
+{
+    const float a2 = dot(rv, rv);
+    if (a2 <= kEps) return QNormalize(mk4(rv * 0.5f, 1.0f));
+    const float angle = std::sqrt(a2);
+    const float half = 0.5f * angle;
+    const float sc = std::sin(half) / angle;
+    return QNormalize(mk4(rv * sc, std::cos(half)));
+}
+inline f4 IntegrateOrientation(f4 q, f3 w, float dt) { return QNormalize(QMul(QuaternionFromRotationVector(w * dt), q)); }
+inline f3 ClampLength(f3 v, float maxLen)
+{
+    const float l = length(v);
+    if (l > maxLen && l > kEps) v = v * (maxLen / l);
+    return v;
+}
+
 // physics_shape_common.hlsli:24-42
 inline float SphereRadius(f4 p, f4 s)
 {
@@ -313,6 +331,9 @@ struct cno_solver {
     std::vector<f4> colMat;
     std::vector<f4> prevBodyPos, prevBodyRot, predBodyPos, predBodyRot, predBodyLin, predBodyAng;
     std::vector<f3> colAabbMin, colAabbMax;
+    // dynamic bodies: summed position / velocity corrections of a pass
+    bool hasDynamic = false;
+    std::vector<f3> bodyTransCorr, bodyRotCorr, bodyLinVelCorr, bodyAngVelCorr;
     std::vector<uint32_t> colliderQueryOrder; // moving colliders first, then static
     uint32_t activeMovingCount = 0;
     // transient state
@@ -477,6 +498,9 @@ void setupWorld(cno_solver &s, const cn_world_soa &w)
     s.predBodyLin = s.bodyLin; s.predBodyAng = s.bodyAng;
     s.colAabbMin.assign(s.C, f3{0, 0, 0});
     s.colAabbMax.assign(s.C, f3{0, 0, 0});
+    for (uint32_t b = 0; b < s.B; ++b) s.hasDynamic = s.hasDynamic || s.bodyType[b] == CN_BODY_DYNAMIC;
+    s.bodyTransCorr.assign(s.B, f3{0, 0, 0}); s.bodyRotCorr.assign(s.B, f3{0, 0, 0});
+    s.bodyLinVelCorr.assign(s.B, f3{0, 0, 0}); s.bodyAngVelCorr.assign(s.B, f3{0, 0, 0});
     if (const cn_surface_render_data *sr = w.surface_render) {
         const uint32_t V = sr->vertex_count, T = sr->triangle_count, S = sr->surface_count;
         s.surfBind.assign(sr->vertex_bindings, sr->vertex_bindings + V);
@@ -608,10 +632,9 @@ void predictRigid(cno_solver &s, float dt)
             s.predBodyLin[b] = mk4(l, lin.w); s.predBodyAng[b] = mk4(a, ang.w);
             continue;
         }
-        // Dynamic bodies are integrated but receive no particle feedback in this restatement.
         f3 l = xyz(lin) + g * dt;
         s.predBodyPos[b] = mk4(xyz(p) + l * dt, p.w);
-        s.predBodyRot[b] = q;
+        s.predBodyRot[b] = IntegrateOrientation(q, xyz(ang), dt);
         s.predBodyLin[b] = mk4(l, lin.w);
         s.predBodyAng[b] = ang;
     }
@@ -1739,6 +1762,8 @@ void particleRigidContacts(cno_solver &s)
         if (denom <= kEps) continue;
         const float lambda = (pen / denom) * relax;
         f3 corr = n * (iS * lambda);
+        f3 rt = -n * (iR * lambda);
+        f3 rr = -MulWorldInvInertia(inI, predQ, cross(rR, n)) * lambda;
         const f3 relDisp = (cp - prevCP) - (xyz(sp) - prevS);
         const f3 tdisp = ProjectOntoTangent(relDisp, n);
         f3 fd{0, 0, 0};
@@ -1756,9 +1781,72 @@ void particleRigidContacts(cno_solver &s)
             if (tden > kEps) {
                 const float tl = fdist / tden;
                 corr += t * (tl * iS * relax);
+                rt -= t * (tl * iR * relax);
+                rr -= MulWorldInvInertia(inI, predQ, cross(rR, t)) * (tl * relax);
             }
         }
         if (iS > kEps) s.posCorr[i] = mk4(xyz(s.posCorr[i]) + corr, s.posCorr[i].w);
+        if (iR > kEps) { // float atomics in the reference; summed here in pair order
+            s.bodyTransCorr[b] += rt;
+            s.bodyRotCorr[b] += rr;
+        }
+    }
+}
+
+// physics_rigid_apply_corrections.cs.hlsl:13-54
+void applyRigidCorrections(cno_solver &s)
+{
+    for (uint32_t b = 0; b < s.B; ++b) {
+        f4 p = s.predBodyPos[b];
+        f4 q = QNormalize(s.predBodyRot[b]);
+        f3 tc = s.bodyTransCorr[b], rc = s.bodyRotCorr[b];
+        if (s.bodyType[b] == CN_BODY_DYNAMIC && p.w != 0.0f) {
+            tc = ClampLength(tc, s.desc.rigid.max_translation_correction_per_iteration);
+            rc = ClampLength(rc, s.desc.rigid.max_rotation_correction_per_iteration);
+            p = mk4(xyz(p) + tc, p.w);
+            q = QNormalize(QMul(QuaternionFromRotationVector(rc), q));
+        }
+        s.predBodyPos[b] = p;
+        s.predBodyRot[b] = q;
+        s.bodyTransCorr[b] = f3{0, 0, 0};
+        s.bodyRotCorr[b] = f3{0, 0, 0};
+    }
+}
+
+// physics_rigid_update_velocities.cs.hlsl:14-51
+void updateRigidVelocities(cno_solver &s, float dt)
+{
+    for (uint32_t b = 0; b < s.B; ++b) {
+        const f4 prevP = s.prevBodyPos[b];
+        const f4 prevQ = QNormalize(s.prevBodyRot[b]);
+        const f4 p = s.predBodyPos[b];
+        const f4 q = QNormalize(s.predBodyRot[b]);
+        if (s.bodyType[b] == CN_BODY_STATIC) {
+            s.predBodyRot[b] = QNormalize(q);
+            s.predBodyLin[b] = f4{0, 0, 0, 0};
+            s.predBodyAng[b] = f4{0, 0, 0, 0};
+            continue;
+        }
+        const f3 l = (xyz(p) - xyz(prevP)) / std::max(dt, kEps);
+        const f3 a = AngularVelocityFromQuaternionDelta(prevQ, q, std::max(dt, kEps));
+        s.predBodyRot[b] = q;
+        s.predBodyLin[b] = mk4(l, 0.0f);
+        s.predBodyAng[b] = mk4(a, 0.0f);
+    }
+}
+
+// physics_rigid_apply_contact_velocities.cs.hlsl:14-58
+void applyRigidContactVelocities(cno_solver &s)
+{
+    for (uint32_t b = 0; b < s.B; ++b) {
+        if (s.bodyType[b] == CN_BODY_DYNAMIC) {
+            const f3 lc = ClampLength(s.bodyLinVelCorr[b], s.desc.rigid.max_linear_velocity_correction_per_iteration);
+            const f3 ac = ClampLength(s.bodyAngVelCorr[b], s.desc.rigid.max_angular_velocity_correction_per_iteration);
+            s.predBodyLin[b] = mk4(xyz(s.predBodyLin[b]) + lc, s.predBodyLin[b].w);
+            s.predBodyAng[b] = mk4(xyz(s.predBodyAng[b]) + ac, s.predBodyAng[b].w);
+        }
+        s.bodyLinVelCorr[b] = f3{0, 0, 0};
+        s.bodyAngVelCorr[b] = f3{0, 0, 0};
     }
 }
 
@@ -1887,6 +1975,10 @@ void particleRigidContactVelocities(cno_solver &s, uint32_t iterations)
             const float imp = std::max(0.0f, (dnv - nv) / nd);
             const f3 ti = n * imp;
             if (iS > kEps) s.velCorr[i] = mk4(xyz(s.velCorr[i]) + ti * iS, s.velCorr[i].w);
+            if (iR > kEps) { // float atomics in the reference; summed here in contact order
+                s.bodyLinVelCorr[b] += -ti * iR;
+                s.bodyAngVelCorr[b] += MulWorldInvInertia(inI, rq, cross(rR, -ti));
+            }
         }
         for (uint32_t i = 0; i < s.N; ++i) {
             f4 vel = s.v[i];
@@ -1896,6 +1988,7 @@ void particleRigidContactVelocities(cno_solver &s, uint32_t iterations)
             s.v[i] = vel;
             s.velCorr[i] = f4{0, 0, 0, 0};
         }
+        if (s.hasDynamic) applyRigidContactVelocities(s);
     }
 }
 
@@ -1986,6 +2079,11 @@ void stepFrame(cno_solver &s, float frameDt)
         std::fill(s.distLambda.begin(), s.distLambda.end(), 0.0f);
         std::fill(s.segLambda.begin(), s.segLambda.end(), f4{0, 0, 0, 0});
         std::fill(s.jointLambda.begin(), s.jointLambda.end(), f4{0, 0, 0, 0});
+        // clearRigidCorrections (physics_rigid_clear_corrections.cs.hlsl)
+        std::fill(s.bodyTransCorr.begin(), s.bodyTransCorr.end(), f3{0, 0, 0});
+        std::fill(s.bodyRotCorr.begin(), s.bodyRotCorr.end(), f3{0, 0, 0});
+        std::fill(s.bodyLinVelCorr.begin(), s.bodyLinVelCorr.end(), f3{0, 0, 0});
+        std::fill(s.bodyAngVelCorr.begin(), s.bodyAngVelCorr.end(), f3{0, 0, 0});
 
         for (uint32_t it = 0; it < maxIt; ++it) {
             const bool runSoft = hasSoftInternal && it < softIt;
@@ -2016,7 +2114,12 @@ void stepFrame(cno_solver &s, float frameDt)
             if (runContacts) particleParticleContacts(s);
             if (runRigid) particleRigidContacts(s);
             if (runContacts || runRigid) applyPositionCorrections(s);
+            // applyRigidCorrections (physics_solver.cpp:1170-1177); zero sums without dynamic bodies
+            if (runRigid && s.hasDynamic) applyRigidCorrections(s);
         }
+        // updateRigidVelocities (physics_solver.cpp:1241-1246); restates the predict without
+        // dynamic bodies
+        if (s.hasDynamic) updateRigidVelocities(s, dt);
         updateVelocities(s, dt);
         if (hasFluidWork) projectFluidBoundaryVelocities(s, dt);
         if (hasFluidWork && s.postUpdateNeighbors) {
@@ -2096,6 +2199,17 @@ CN_API int cno_read_particles(cno_solver *s, float *x, float *v, float *xprev)
     if (x) std::memcpy(x, s->x.data(), s->x.size() * sizeof(f4));
     if (v) std::memcpy(v, s->v.data(), s->v.size() * sizeof(f4));
     if (xprev) std::memcpy(xprev, s->xprev.data(), s->xprev.size() * sizeof(f4));
+    return CN_OK;
+}
+
+CN_API int cno_read_rigid_bodies(cno_solver *s, float *pos, float *rot, float *lin, float *ang)
+{
+    if (!s) return CN_ERR_INVALID_ARGUMENT;
+    const size_t bytes = size_t(s->B) * sizeof(f4);
+    if (pos) std::memcpy(pos, s->bodyPos.data(), bytes);
+    if (rot) std::memcpy(rot, s->bodyRot.data(), bytes);
+    if (lin) std::memcpy(lin, s->bodyLin.data(), bytes);
+    if (ang) std::memcpy(ang, s->bodyAng.data(), bytes);
     return CN_OK;
 }
 

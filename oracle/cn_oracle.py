@@ -46,6 +46,7 @@ def load() -> C.CDLL:
         lib.cno_meta.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
         lib.cno_fluid_material.argtypes = [C.c_float] * 7 + [C.c_void_p]
         lib.cno_read_surface_render.argtypes = [C.c_void_p] * 5
+        lib.cno_read_rigid_bodies.argtypes = [C.c_void_p] * 5
         _lib = lib
     return _lib
 
@@ -64,6 +65,7 @@ class Oracle:
             raise RuntimeError("oracle: create failed")
         self.n = soa.particle_count
         self.segments = soa.strand_segment_count
+        self.bodies = soa.rigid_body_count
         sr = soa.surface_render
         self.surface = (sr.contents.vertex_count, sr.contents.triangle_count, sr.contents.surface_count) if sr \
             else (0, 0, 0)
@@ -102,6 +104,12 @@ class Oracle:
         if self.segments:
             self._lib.cno_read_strand_orientations(self._h, q.ctypes.data)
         return q
+
+    def read_rigid_bodies(self):
+        """(positions with inverse mass, orientations, linear, angular velocities), each (B, 4)."""
+        out = [np.zeros((self.bodies, 4), np.float32) for _ in range(4)]
+        self._lib.cno_read_rigid_bodies(self._h, *(a.ctypes.data for a in out))
+        return tuple(out)
 
     def read_surface_render(self):
         """(render positions V x 4, render normals V x 4, world AABBs S x 8, triangle normals T x 4)."""
