@@ -19,7 +19,7 @@ INCLUDE = HERE.parent / "include"
 LIB = HERE / "libcn_physics.so"
 OBJ_DIR = HERE / "_build"
 
-CUDA_SOURCES = ["cn_kernels.cu", "cn_sort.cu", "cn_noalloc.cu", "cn_diff.cu"]
+CUDA_SOURCES = ["cn_kernels.cu", "cn_sort.cu", "cn_noalloc.cu", "cn_diff.cu", "cn_rigid.cu"]
 HOST_SOURCES = ["cn_solver.cpp", "cn_world.cpp", "cn_batch.cpp", "cn_server.cpp"]
 HEADERS = ["cn_device.h", "cn_math.cuh", "cn_internal.h"]
 

@@ -171,8 +171,9 @@ class Meta(C.Structure):
         "particle_rigid_candidate_overflow", "particle_particle_candidate_count",
         "required_particle_particle_candidate_count", "particle_particle_candidate_overflow",
         "fluid_boundary_candidate_overflow", "active_particle_rigid_contact_count",
-        "active_particle_contact_count", "fluid_neighbor_truncations", "device_wait_timeouts")] + [
-        ("reserved", u32 * 5)]
+        "active_particle_contact_count", "fluid_neighbor_truncations", "device_wait_timeouts",
+        "rigid_rigid_candidate_count", "required_rigid_rigid_candidate_count", "rigid_rigid_candidate_overflow")] + [
+        ("reserved", u32 * 2)]
 
 
 class SceneView(C.Structure):

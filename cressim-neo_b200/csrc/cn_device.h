@@ -42,8 +42,29 @@ struct DeviceMeta {
     uint32_t boundaryMaskOverflow;
     uint32_t neighborTruncations;
     uint32_t waitTimeouts;
-    uint32_t reserved[7];
+    uint32_t rigidRigidPairCount;     // min(required, capacity) collider pairs of the rigid broadphase
+    uint32_t requiredRigidRigidPairs;
+    uint32_t rigidGroupCount;         // body pairs with active contacts (velocity-solve groups)
+    uint32_t rigidContactSlots;       // kRigidPairContacts x rigidRigidPairCount
+    uint32_t reserved[3];
 };
+
+// Rigid-rigid contact point of a collider pair (GpuRigidContact, physics_rigid_types.hlsli):
+// kRigidPairContacts slots per pair (box-box manifolds fill up to 4, other shapes one), 80 B.
+constexpr uint32_t kRigidPairContacts = 4u; // kRigidContactsPerPair
+struct RigidPairContact {
+    uint32_t bodyA, bodyB, active, reserved;
+    float4 normalPenetration;   // normal A -> B, penetration
+    float4 localPointA, localPointB;
+    float4 material;            // friction, restitution, static friction
+};
+// Velocity-solve slot of a contact in its body-pair group
+// (GpuRigidBodyPairContactAggregateSlot): normal (w kinetic friction), local points (A.w static
+// friction), solver state (accumulated normal impulse, restitution target, tangent accumulation).
+struct RigidSlot {
+    float4 normal, localA, localB, state;
+};
+constexpr uint32_t kRigidGroupContacts = 16u; // kRigidBodyPairAggregateContacts
 
 constexpr uint32_t kMaxBoundaryColliders = 64u;  // bits of the per-particle boundary mask
 constexpr uint32_t kRigidDedup = 16u;            // kParticleRigidDedupCacheSize
@@ -122,6 +143,21 @@ struct Scene {
     float4 *prevBodyPos = nullptr, *prevBodyRot = nullptr;
     float4 *predBodyPos = nullptr, *predBodyRot = nullptr, *predBodyLin = nullptr, *predBodyAng = nullptr;
     float4 *colAabbMin = nullptr, *colAabbMax = nullptr;
+    // rigid-rigid contacts (scenes with dynamic bodies): LBVH over the query-order colliders, the
+    // moving colliders' candidate pairs, one contact per pair, body-pair groups for the velocities
+    uint32_t rrCapacity = 0;
+    uint32_t *rrCount = nullptr, *rrOffset = nullptr;     // per moving collider
+    uint2 *rrPairs = nullptr;                              // (collider A, collider B), canonical
+    RigidPairContact *rrContacts = nullptr;
+    RigidSlot *rrSlots = nullptr;                          // per sorted contact
+    uint32_t *rrKeyA = nullptr, *rrValA = nullptr, *rrKeyB = nullptr, *rrValB = nullptr;
+    uint32_t *rrHead = nullptr, *rrGroupOf = nullptr;      // per sorted contact
+    uint2 *rrGroups = nullptr;                             // (first sorted contact, contacts)
+    uint32_t *bvhKeyA = nullptr, *bvhValA = nullptr, *bvhKeyB = nullptr, *bvhValB = nullptr;
+    uint2 *bvhChildren = nullptr;                          // per internal node
+    uint32_t *bvhParent = nullptr, *bvhVisits = nullptr;   // per node / internal node
+    float4 *bvhMin = nullptr, *bvhMax = nullptr;           // per node
+    float4 *bvhBounds = nullptr;                           // scene centre bounds (2)
     // dynamic bodies: corrections summed (float atomics) over a pass, applied per body after it
     uint32_t hasDynamic = 0;
     float4 *bodyTransCorr = nullptr, *bodyRotCorr = nullptr, *bodyLinVelCorr = nullptr, *bodyAngVelCorr = nullptr;
@@ -212,6 +248,9 @@ struct Config {
     float gravity[3];
     // per-iteration caps on a dynamic body's summed corrections (physics_solver_config.hlsli:31-34)
     float maxTranslationCorrection, maxRotationCorrection, maxLinearVelocityCorrection, maxAngularVelocityCorrection;
+    // rigid-rigid contacts (physics_solver_config.hlsli:23-30)
+    float rigidRestitutionThreshold, baumgarte, depenetrationRelaxation, maxDepenetration, velocityPenetrationStiffness;
+    float manifoldMergeDistance; // manifold_merge_slop_multiplier x slop
 };
 
 // A kinematic target staged for a batch tick: pos.xyz, pos.w = the body index (bits); rot = xyzw.
@@ -254,6 +293,24 @@ void launchCopyPredictedRigid(const Scene &s, cudaStream_t st);
 void launchApplyRigidCorrections(const Scene &s, const Config &c, cudaStream_t st);
 void launchUpdateRigidVelocities(const Scene &s, float dt, cudaStream_t st);
 void launchRigidContactVelocitiesDynamic(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st);
+
+// ---------------------------------------------------------------- rigid-rigid contacts (cn_rigid.cu)
+// Scratch of the rigid broadphase and grouping (sort + scan), in bytes, for C colliders and
+// `pairs` candidate pairs.
+size_t rigidScratchBytes(uint32_t colliders, uint32_t pairs);
+// LBVH over the colliders' world AABBs, the moving colliders' candidate pairs, and one contact
+// per pair (physics_rigid_bvh_*, physics_rigid_count/emit_pairs, physics_rigid_generate_contacts).
+void launchRigidBroadphaseAndContacts(const Scene &s, const Config &c, void *scratch, cudaStream_t st);
+// Body-pair groups of the active contacts and their velocity slots
+// (physics_rigid_init_contact_velocities).
+void launchRigidVelocityInit(const Scene &s, const Config &c, void *scratch, cudaStream_t st);
+// Position-level depenetration of every contact (physics_rigid_depenetrate_contacts).
+void launchRigidDepenetration(const Scene &s, const Config &c, cudaStream_t st);
+// `iterations` rounds of the group velocity solve, the body corrections applied after each
+// (physics_rigid_solve_contact_velocities + apply_contact_velocities); rounds past
+// `contactIterations` only apply.
+void launchRigidContactVelocitySolve(const Scene &s, const Config &c, uint32_t iterations, uint32_t contactIterations,
+                                     cudaStream_t st);
 // Skinning, triangle and vertex normals, chunk and surface AABBs from the current positions.
 void launchSurfaceRender(const Scene &s, cudaStream_t st);
 // debug export of the compacted cell-range table (reference layout)

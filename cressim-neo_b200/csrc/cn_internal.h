@@ -96,6 +96,12 @@ inline Config configFromDesc(const cn_solver_desc &d)
     c.maxRotationCorrection = d.rigid.max_rotation_correction_per_iteration;
     c.maxLinearVelocityCorrection = d.rigid.max_linear_velocity_correction_per_iteration;
     c.maxAngularVelocityCorrection = d.rigid.max_angular_velocity_correction_per_iteration;
+    c.rigidRestitutionThreshold = d.contact.rigid_restitution_velocity_threshold;
+    c.baumgarte = d.rigid.depenetration_baumgarte;
+    c.depenetrationRelaxation = d.rigid.depenetration_relaxation;
+    c.maxDepenetration = d.rigid.depenetration_max_correction_per_iteration;
+    c.velocityPenetrationStiffness = d.rigid.velocity_penetration_stiffness;
+    c.manifoldMergeDistance = d.contact.manifold_merge_slop_multiplier * d.contact.slop;
     return c;
 }
 

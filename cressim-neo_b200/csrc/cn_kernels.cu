@@ -72,29 +72,9 @@ template <class F> __device__ __forceinline__ void forEachInBlock(const WorkList
 }
 
 // ------------------------------------------------------------------------------------------
-// Rigid predict (static / kinematic; dynamic bodies are integrated without particle feedback)
+// Rigid predict (static, kinematic and dynamic branches)
 // physics_rigid_predict.cs.hlsl:20-81, collider world AABBs physics_rigid_update_world_aabbs.cs.hlsl
 // ------------------------------------------------------------------------------------------
-__device__ void computeBodyAabb(uint32_t shape, f3 pos, float4 q, float4 p, float4 sc, f3 &mnv, f3 &mxv)
-{
-    f3 e{0.f, 0.f, 0.f};
-    if (shape == CN_COLLIDER_SPHERE) {
-        const float r = sphereRadius(p, sc);
-        e = f3{r, r, r};
-    } else if (shape == CN_COLLIDER_BOX) {
-        const f3 h = boxHalfExtents(p, sc);
-        e = fabs3(qRotate(q, f3{1.f, 0.f, 0.f})) * h.x + fabs3(qRotate(q, f3{0.f, 1.f, 0.f})) * h.y +
-            fabs3(qRotate(q, f3{0.f, 0.f, 1.f})) * h.z;
-    } else {
-        f3 a, b;
-        float r = 0.0f;
-        capsuleSegment(pos, q, p, sc, a, b, r);
-        const f3 axis = fabs3(qRotate(q, f3{0.f, 1.f, 0.f}));
-        e = axis * (0.5f * length(b - a)) + f3{r, r, r};
-    }
-    mnv = pos - e;
-    mxv = pos + e;
-}
 
 __device__ __forceinline__ void rigidPredictBody(const Scene &s, float dt, float gx, float gy, float gz, uint32_t b)
 {

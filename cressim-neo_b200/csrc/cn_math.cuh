@@ -146,6 +146,38 @@ __host__ __device__ __forceinline__ f3 closestFaceNormalLocal(f3 lp, f3 h)
     if (d.y <= d.z) return f3{0.f, lp.y >= 0.0f ? 1.0f : -1.0f, 0.f};
     return f3{0.f, 0.f, lp.z >= 0.0f ? 1.0f : -1.0f};
 }
+// physics_shape_common.hlsli:45-98: box axes, ComputeBodyAabb, closest point and support point
+__host__ __device__ __forceinline__ void computeBodyAabb(uint32_t shape, f3 pos, float4 q, float4 p, float4 sc, f3 &mnv, f3 &mxv)
+{
+    f3 e{0.f, 0.f, 0.f};
+    if (shape == CN_COLLIDER_SPHERE) {
+        const float r = sphereRadius(p, sc);
+        e = f3{r, r, r};
+    } else if (shape == CN_COLLIDER_BOX) {
+        const f3 h = boxHalfExtents(p, sc);
+        e = fabs3(qRotate(q, f3{1.f, 0.f, 0.f})) * h.x + fabs3(qRotate(q, f3{0.f, 1.f, 0.f})) * h.y +
+            fabs3(qRotate(q, f3{0.f, 0.f, 1.f})) * h.z;
+    } else {
+        f3 a, b;
+        float r = 0.0f;
+        capsuleSegment(pos, q, p, sc, a, b, r);
+        const f3 axis = fabs3(qRotate(q, f3{0.f, 1.f, 0.f}));
+        e = axis * (0.5f * length(b - a)) + f3{r, r, r};
+    }
+    mnv = pos - e;
+    mxv = pos + e;
+}
+
+__host__ __device__ __forceinline__ f3 closestPointOnBox(f3 q, f3 c, float4 o, f3 h)
+{
+    const f3 lp = qInvRotate(o, q - c);
+    return c + qRotate(o, clamp3(lp, -h, h));
+}
+__host__ __device__ __forceinline__ f3 boxSupportPoint(f3 c, float4 o, f3 h, f3 dir)
+{
+    const f3 ld = qInvRotate(o, dir);
+    return c + qRotate(o, f3{ld.x >= 0.0f ? h.x : -h.x, ld.y >= 0.0f ? h.y : -h.y, ld.z >= 0.0f ? h.z : -h.z});
+}
 // physics_shape_common.hlsli:75-80
 __host__ __device__ __forceinline__ bool aabbOverlaps(f3 minA, f3 maxA, f3 minB, f3 maxB)
 {

@@ -49,7 +49,9 @@ struct cn_solver {
     float *hostX = nullptr, *hostV = nullptr;
     bool synced = false;
     bool hasFluid = false, ppPossible = false, rigidPossible = false, hasBroadphase = false, hasDynamic = false;
-    uint32_t substeps = 1, fluidIt = 1, softIt = 1, contactIt = 1, maxIt = 1;
+    uint32_t substeps = 1, fluidIt = 1, softIt = 1, contactIt = 1, maxIt = 1, jointIt = 1, rrIt = 1;
+    bool rigidRigid = false;       // dynamic bodies among >= 2 colliders: rigid-rigid contacts
+    void *rigidScratch = nullptr;
     bool postUpdateNeighbors = false, writeFluidDebug = false, forceBroadphase = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
@@ -187,6 +189,27 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
     if (sv->hasDynamic) {
         s.bodyTransCorr = a.take<float4>(B); s.bodyRotCorr = a.take<float4>(B);
         s.bodyLinVelCorr = a.take<float4>(B); s.bodyAngVelCorr = a.take<float4>(B);
+    }
+    s.rrCapacity = 0;
+    if (sv->rigidRigid) {
+        const uint32_t P = std::max<uint32_t>(64u, 16u * C);
+        s.rrCapacity = P;
+        s.rrCount = a.take<uint32_t>(C); s.rrOffset = a.take<uint32_t>(C);
+        const uint32_t K = P * cn::kRigidPairContacts;
+        s.rrPairs = a.take<uint2>(P);
+        s.rrContacts = a.take<cn::RigidPairContact>(K);
+        s.rrSlots = a.take<cn::RigidSlot>(K);
+        s.rrKeyA = a.take<uint32_t>(K); s.rrValA = a.take<uint32_t>(K);
+        s.rrKeyB = a.take<uint32_t>(K); s.rrValB = a.take<uint32_t>(K);
+        s.rrHead = a.take<uint32_t>(K); s.rrGroupOf = a.take<uint32_t>(K);
+        s.rrGroups = a.take<uint2>(K);
+        s.bvhKeyA = a.take<uint32_t>(C); s.bvhValA = a.take<uint32_t>(C);
+        s.bvhKeyB = a.take<uint32_t>(C); s.bvhValB = a.take<uint32_t>(C);
+        s.bvhChildren = a.take<uint2>(C);
+        s.bvhParent = a.take<uint32_t>(2 * C); s.bvhVisits = a.take<uint32_t>(C);
+        s.bvhMin = a.take<float4>(2 * C); s.bvhMax = a.take<float4>(2 * C);
+        s.bvhBounds = a.take<float4>(2);
+        sv->rigidScratch = a.take<uint8_t>(cn::rigidScratchBytes(C, K));
     }
     s.colFrame = a.take<float4>(size_t(C) * 4);
     s.colQueryOrder = a.take<uint32_t>(C);
@@ -345,6 +368,8 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
     const uint32_t N = s.N;
     for (uint32_t sub = 0; sub < sv->substeps; ++sub) {
         probe(sv, "rigid_predict", st, [&] { cn::launchRigidPredict(s, dt, c.gravity[0], c.gravity[1], c.gravity[2], st); });
+        if (sv->rigidRigid)
+            probe(sv, "rigid_broadphase_contacts", st, [&] { cn::launchRigidBroadphaseAndContacts(s, c, sv->rigidScratch, st); });
         probe(sv, "predict_keys", st, [&] { cn::launchPredictAndKeys(s, dt, c, st); });
         if (sv->hasBroadphase && (sv->hasFluid || sv->ppPossible || sv->forceBroadphase)) {
             probe(sv, "radix_sort", st, [&] {
@@ -356,6 +381,8 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             probe(sv, "particle_candidates", st, [&] { cn::launchParticleCandidates(s, sv->scanScratch, sv->scanScratchBytes, st); });
         if (sv->rigidPossible)
             probe(sv, "rigid_candidates", st, [&] { cn::launchRigidCandidates(s, sv->scanScratch, sv->scanScratchBytes, st); });
+        // initRigidContactVelocities (physics_solver.cpp:736-743)
+        if (sv->rigidRigid) cn::launchRigidVelocityInit(s, c, sv->rigidScratch, st);
         // clearSoftConstraintState (physics_clear_soft_constraint_state.cs.hlsl:14-54)
         if (s.E) cudaMemsetAsync(s.edgeLambda, 0, sizeof(float) * s.E, st);
         if (s.Bn + s.D) cudaMemsetAsync(s.bendLambda, 0, sizeof(float) * (s.Bn + s.D), st);
@@ -380,7 +407,8 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             const bool runSoft = hasSoftInternal && it < sv->softIt;
             const bool runPP = sv->ppPossible && it < sv->contactIt;
             const bool runRigid = sv->rigidPossible && it < sv->contactIt;
-            if (!runFluid && !runSoft && !runPP && !runRigid) break; // remaining iterations are empty
+            const bool runRigidRigid = sv->rigidRigid && it < sv->rrIt;
+            if (!runFluid && !runSoft && !runPP && !runRigid && !runRigidRigid) break; // remaining iterations are empty
             if (runFluid) {
                 if (it == 0 || cn::fluidGatherEachIteration(s))
                     probe(sv, "fluid_gather", st, [&] { cn::launchFluidGather(s, it, st); });
@@ -392,9 +420,11 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             }
             if (runSoft) probe(sv, "soft_constraints", st, [&] { cn::launchSoftIteration(s, dt, c, st); });
             if (runPP || runRigid) probe(sv, "contacts", st, [&] { cn::launchContacts(s, c, runPP, runRigid, st); });
+            // finalRigidContactDepenetration (physics_solver.cpp:1111-1117)
+            if (runRigidRigid) probe(sv, "rigid_depenetration", st, [&] { cn::launchRigidDepenetration(s, c, st); });
             // applyRigidCorrections (physics_solver.cpp:1170-1177); with only static and kinematic
             // bodies the summed corrections are zero and the pass is left out
-            if (runRigid && s.hasDynamic) cn::launchApplyRigidCorrections(s, c, st);
+            if ((runRigid || runRigidRigid) && s.hasDynamic) cn::launchApplyRigidCorrections(s, c, st);
         }
         // updateRigidVelocities (physics_solver.cpp:1241-1246): for static and kinematic bodies it
         // restates what the rigid predict wrote, so it runs for scenes with dynamic bodies
@@ -412,6 +442,11 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             else
                 probe(sv, "contact_velocities", st, [&] { cn::launchRigidContactVelocities(s, sv->contactIt, c, st); });
         }
+        // solveRigidContactVelocities (physics_solver.cpp:1345-1354)
+        if (sv->rigidRigid)
+            probe(sv, "rigid_contact_velocities", st, [&] {
+                cn::launchRigidContactVelocitySolve(s, c, std::max(sv->rrIt, sv->jointIt), sv->rrIt, st);
+            });
         cn::launchCopyPredictedRigid(s, st);
     }
     // physics_solver.cpp:1310-1337 (after the last substep: see launchSurfaceRender)
@@ -535,6 +570,8 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     sv->contactIt = cn::resolveIter(d.soft_contact_iterations, defIt);
     const uint32_t jointIt = cn::resolveIter(d.rigid_joint_iterations, defIt);
     const uint32_t rrIt = cn::resolveIter(d.rigid_rigid_contact_iterations, defIt);
+    sv->jointIt = jointIt;
+    sv->rrIt = rrIt;
     sv->maxIt = std::max(std::max(std::max(sv->fluidIt, sv->softIt), sv->contactIt), std::max(jointIt, rrIt));
     bool anyFluid = false, anySolid = false, anySelf = false;
     std::vector<uint32_t> solidGroups;
@@ -590,9 +627,12 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
         if (!err.empty()) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_sync_world: " + err);
     }
 
-    // Collider query order: moving (kinematic) colliders, then static, ascending index.
+    // Collider query order: moving (kinematic, dynamic) colliders, then static, ascending index.
     std::vector<uint32_t> order;
     const uint32_t moving = cn::colliderQueryOrder(*w, order);
+    sv->rigidRigid = anyDynamic && rrIt > 0 && order.size() >= 2 && moving > 0;
+    if (sv->rigidRigid && uint64_t(w->rigid_body_count) * w->rigid_body_count >= 0xffffffffull)
+        return setError(CN_ERR_UNSUPPORTED, "more than 65535 rigid bodies in a scene with dynamic bodies");
     if (anyFluid && order.size() > cn::kMaxBoundaryColliders)
         return setError(CN_ERR_UNSUPPORTED, "more than 64 colliders in a scene with fluid");
 
@@ -761,9 +801,12 @@ CN_API cn_status cn_solver_validate_meta(cn_solver *sv, cn_meta *out)
     out->active_particle_contact_count = m.activeParticleContacts;
     out->fluid_neighbor_truncations = m.neighborTruncations;
     out->device_wait_timeouts = m.waitTimeouts;
+    out->rigid_rigid_candidate_count = m.rigidRigidPairCount;
+    out->required_rigid_rigid_candidate_count = m.requiredRigidRigidPairs;
+    out->rigid_rigid_candidate_overflow = m.requiredRigidRigidPairs > sv->s.rrCapacity ? 1u : 0u;
     if (m.waitTimeouts) return setError(CN_ERR_DEVICE_TIMEOUT, "a bounded device wait gave up (sort look-back)");
     if (out->particle_rigid_candidate_overflow || out->particle_particle_candidate_overflow ||
-        out->fluid_boundary_candidate_overflow)
+        out->fluid_boundary_candidate_overflow || out->rigid_rigid_candidate_overflow)
         return setError(CN_ERR_CAPACITY, "candidate buffer overflow");
     return CN_OK;
 }

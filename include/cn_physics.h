@@ -444,7 +444,10 @@ typedef struct cn_meta {
     uint32_t active_particle_contact_count;
     uint32_t fluid_neighbor_truncations;         /* particles whose neighbour list hit max_fluid_neighborhood */
     uint32_t device_wait_timeouts;               /* bounded spins that gave up (sort look-back) */
-    uint32_t reserved[5];
+    uint32_t rigid_rigid_candidate_count;        /* collider pairs of the rigid broadphase (GpuBroadPhaseMeta) */
+    uint32_t required_rigid_rigid_candidate_count;
+    uint32_t rigid_rigid_candidate_overflow;
+    uint32_t reserved[2];
 } cn_meta;
 
 /* Non-owning device pointers (reference: PhysicsGpuSceneView,

@@ -334,6 +334,18 @@ struct cno_solver {
     // dynamic bodies: summed position / velocity corrections of a pass
     bool hasDynamic = false;
     std::vector<f3> bodyTransCorr, bodyRotCorr, bodyLinVelCorr, bodyAngVelCorr;
+    // rigid-rigid contacts: candidate collider pairs, one contact each, body-pair groups
+    struct RigidPairContact {
+        uint32_t bodyA = 0, bodyB = 0;
+        bool active = false;
+        f4 normalPenetration{0, 0, 0, 0}, localA{0, 0, 0, 0}, localB{0, 0, 0, 0}, material{0, 0, 0, 0};
+    };
+    struct RigidSlot { f4 normal, localA, localB, state; };
+    std::vector<std::pair<uint32_t, uint32_t>> rrPairs;
+    std::vector<RigidPairContact> rrContacts;
+    std::vector<std::vector<RigidSlot>> rrGroups;
+    std::vector<std::pair<uint32_t, uint32_t>> rrGroupBodies;
+    uint32_t requiredRigidRigidPairs = 0;
     std::vector<uint32_t> colliderQueryOrder; // moving colliders first, then static
     uint32_t activeMovingCount = 0;
     // transient state
@@ -1835,6 +1847,766 @@ void updateRigidVelocities(cno_solver &s, float dt)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Rigid-rigid contacts (scenes with dynamic bodies).
+// ---------------------------------------------------------------------------
+// ComputePositionFrictionDelta (physics_rigid_solver_shared.hlsli:50-68)
+inline f3 PositionFrictionDelta(f3 td, float pen, float kin, float stat, float minDist)
+{
+    const float d = length(td);
+    if (d <= minDist || pen <= kEps) return f3{0, 0, 0};
+    const float sl = saturate(stat) * pen;
+    if (d <= sl) return td;
+    return td * std::min(saturate(kin) * pen / d, 1.0f);
+}
+inline f3 ClosestPointOnBox(f3 q, f3 c, f4 o, f3 h) { return c + QRotate(o, clamp3(QInvRotate(o, q - c), f3{-h.x, -h.y, -h.z}, h)); }
+inline f3 BoxSupportPoint(f3 c, f4 o, f3 h, f3 dir)
+{
+    const f3 ld = QInvRotate(o, dir);
+    return c + QRotate(o, f3{ld.x >= 0.0f ? h.x : -h.x, ld.y >= 0.0f ? h.y : -h.y, ld.z >= 0.0f ? h.z : -h.z});
+}
+inline float Comp(f3 v, uint32_t i) { return i == 0u ? v.x : (i == 1u ? v.y : v.z); }
+inline float PenetrationFromPoints(f3 a, f3 b, f3 n) { return std::max(0.0f, -dot(b - a, n)); }
+
+// physics_rigid_contact_primitives.hlsli:17-47
+bool SphereSphere(f3 cA, float rA, f3 cB, float rB, f3 &n, f3 &pA, f3 &pB, float &pen)
+{
+    n = pA = pB = f3{0, 0, 0};
+    pen = 0.0f;
+    const f3 d = cB - cA;
+    const float d2 = dot(d, d);
+    const float r = rA + rB;
+    if (d2 > r * r) return false;
+    const float dist = std::sqrt(std::max(d2, 0.0f));
+    n = dist > kEps ? d / dist : f3{0, 1, 0};
+    pA = cA + n * rA;
+    pB = cB - n * rB;
+    pen = PenetrationFromPoints(pA, pB, n);
+    return pen > 0.0f;
+}
+// :50-99
+bool SphereBox(f3 sc, float sr, f3 bc, f4 bq, f3 h, f3 &n, f3 &pA, f3 &pB, float &pen)
+{
+    n = pA = pB = f3{0, 0, 0};
+    pen = 0.0f;
+    const f3 ls = QInvRotate(bq, sc - bc);
+    const f3 cl = clamp3(ls, f3{-h.x, -h.y, -h.z}, h);
+    const bool inside = ls.x >= -h.x && ls.y >= -h.y && ls.z >= -h.z && ls.x <= h.x && ls.y <= h.y && ls.z <= h.z;
+    if (!inside) {
+        const f3 bp = bc + QRotate(bq, cl);
+        const f3 d = bp - sc;
+        const float d2 = dot(d, d);
+        if (d2 > sr * sr) return false;
+        const float dist = std::sqrt(std::max(d2, 0.0f));
+        n = dist > kEps ? d / dist : f3{0, 1, 0};
+        pA = sc + n * sr;
+        pB = bp;
+        pen = PenetrationFromPoints(pA, pB, n);
+        return pen > 0.0f;
+    }
+    const f3 lfn = ClosestFaceNormalLocal(ls, h);
+    const float depth = std::min(h.x - std::fabs(ls.x), std::min(h.y - std::fabs(ls.y), h.z - std::fabs(ls.z)));
+    n = -QRotate(bq, lfn);
+    pB = bc + QRotate(bq, ls + lfn * depth);
+    pA = sc + n * sr;
+    pen = depth + sr;
+    return pen > 0.0f;
+}
+// :101-119
+bool SphereCapsule(f3 sc, float sr, f3 a, f3 b, float cr, f3 &n, f3 &pA, f3 &pB, float &pen)
+{
+    const f3 seg = b - a;
+    const float l2 = dot(seg, seg);
+    float t = 0.0f;
+    if (l2 > kEps) t = saturate(dot(sc - a, seg) / l2);
+    return SphereSphere(sc, sr, a + seg * t, cr, n, pA, pB, pen);
+}
+// :272-331
+void ClosestSegmentSegment(f3 a0, f3 a1, f3 b0, f3 b1, f3 &oa, f3 &ob)
+{
+    oa = a0;
+    ob = b0;
+    const f3 d1 = a1 - a0, d2 = b1 - b0, r = a0 - b0;
+    const float a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+    float sv = 0.0f, t = 0.0f;
+    if (a <= kEps && e <= kEps) return;
+    if (a <= kEps) {
+        t = saturate(f / e);
+    } else {
+        const float c = dot(d1, r);
+        if (e <= kEps) {
+            sv = saturate(-c / a);
+        } else {
+            const float b = dot(d1, d2);
+            const float den = a * e - b * b;
+            if (den != 0.0f) sv = saturate((b * f - c * e) / den);
+            const float tn = b * sv + f;
+            if (tn < 0.0f) { t = 0.0f; sv = saturate(-c / a); }
+            else if (tn > e) { t = 1.0f; sv = saturate((b - c) / a); }
+            else t = tn / e;
+        }
+    }
+    oa = a0 + d1 * sv;
+    ob = b0 + d2 * t;
+}
+// :121-270 (separating-axis test, the deepest axis' contact points)
+bool BoxBox(f3 cA, f4 qA, f3 hA, f3 cB, f4 qB, f3 hB, f3 &n, f3 &pA, f3 &pB, float &pen)
+{
+    n = pA = pB = f3{0, 0, 0};
+    pen = 0.0f;
+    const f3 axA[3] = {QRotate(qA, f3{1, 0, 0}), QRotate(qA, f3{0, 1, 0}), QRotate(qA, f3{0, 0, 1})};
+    const f3 axB[3] = {QRotate(qB, f3{1, 0, 0}), QRotate(qB, f3{0, 1, 0}), QRotate(qB, f3{0, 0, 1})};
+    const f3 cd = cB - cA;
+    auto proj = [](f3 axis, const f3 *ax, f3 h) {
+        return h.x * std::fabs(dot(axis, ax[0])) + h.y * std::fabs(dot(axis, ax[1])) + h.z * std::fabs(dot(axis, ax[2]));
+    };
+    float minPen = 3.402823466e+38f;
+    f3 best{0, 1, 0};
+    uint32_t bType = 0, bA = 0, bB = 0;
+    auto test = [&](f3 axis, uint32_t type, uint32_t ia, uint32_t ib) {
+        const float l2 = dot(axis, axis);
+        if (l2 <= kEps) return true;
+        const f3 nn = axis * (1.0f / std::sqrt(l2));
+        const float dist = std::fabs(dot(cd, nn));
+        const float ov = proj(nn, axA, hA) + proj(nn, axB, hB) - dist;
+        if (ov < 0.0f) return false;
+        if (ov < minPen) {
+            minPen = ov;
+            best = dot(cd, nn) >= 0.0f ? nn : -nn;
+            bType = type; bA = ia; bB = ib;
+        }
+        return true;
+    };
+    for (uint32_t i = 0; i < 3; ++i) if (!test(axA[i], 0, i, 0)) return false;
+    for (uint32_t i = 0; i < 3; ++i) if (!test(axB[i], 1, i, 0)) return false;
+    for (uint32_t a = 0; a < 3; ++a)
+        for (uint32_t b = 0; b < 3; ++b)
+            if (!test(cross(axA[a], axB[b]), 2, a, b)) return false;
+    n = best;
+    auto edge = [](uint32_t axis, f3 c, const f3 *ax, f3 h, f3 dir, f3 &e0, f3 &e1) {
+        const uint32_t oa = (axis + 1) % 3, ob = (axis + 2) % 3;
+        const float sa = dot(ax[oa], dir) >= 0.0f ? 1.0f : -1.0f;
+        const float sb = dot(ax[ob], dir) >= 0.0f ? 1.0f : -1.0f;
+        const f3 ec = c + ax[oa] * (Comp(h, oa) * sa) + ax[ob] * (Comp(h, ob) * sb);
+        const f3 eh = ax[axis] * Comp(h, axis);
+        e0 = ec - eh;
+        e1 = ec + eh;
+    };
+    if (bType == 2) {
+        f3 ea0, ea1, eb0, eb1;
+        edge(bA, cA, axA, hA, n, ea0, ea1);
+        edge(bB, cB, axB, hB, -n, eb0, eb1);
+        ClosestSegmentSegment(ea0, ea1, eb0, eb1, pA, pB);
+    } else if (bType == 1) {
+        pB = BoxSupportPoint(cB, qB, hB, -n);
+        pA = ClosestPointOnBox(pB, cA, qA, hA);
+    } else {
+        pA = BoxSupportPoint(cA, qA, hA, n);
+        pB = ClosestPointOnBox(pA, cB, qB, hB);
+    }
+    pen = minPen;
+    return pen > 0.0f;
+}
+// :333-448
+void ClosestSegmentBox(f3 sa, f3 sb, f3 bc, f4 bq, f3 h, f3 &outSeg, f3 &outBox, bool &inter)
+{
+    outSeg = sa;
+    outBox = ClosestPointOnBox(sa, bc, bq, h);
+    const f3 la = QInvRotate(bq, sa - bc), lb = QInvRotate(bq, sb - bc);
+    const f3 d = lb - la;
+    // SegmentIntersectsAabbLocal
+    inter = true;
+    float tMin = 0.0f, tMax = 1.0f;
+    for (uint32_t ax = 0; ax < 3 && inter; ++ax) {
+        const float o = Comp(la, ax), dl = Comp(d, ax), lo = -Comp(h, ax), hi = Comp(h, ax);
+        if (std::fabs(dl) <= kEps) {
+            if (o < lo || o > hi) inter = false;
+            continue;
+        }
+        const float inv = 1.0f / dl;
+        float t0 = (lo - o) * inv, t1 = (hi - o) * inv;
+        if (t0 > t1) std::swap(t0, t1);
+        tMin = std::max(tMin, t0);
+        tMax = std::min(tMax, t1);
+        if (tMin > tMax) inter = false;
+    }
+    if (inter) {
+        outSeg = bc + QRotate(bq, la + d * tMin);
+        outBox = outSeg;
+        return;
+    }
+    float bestD2 = 3.402823466e+38f;
+    const f3 nh{-h.x, -h.y, -h.z};
+    f3 bestSeg = la, bestBox = clamp3(la, nh, h);
+    auto cand = [&](float t) {
+        if (t < 0.0f || t > 1.0f) return;
+        const f3 sp = lerp3(la, lb, t);
+        const f3 bp = clamp3(sp, nh, h);
+        const float d2 = dot(sp - bp, sp - bp);
+        if (d2 < bestD2) { bestD2 = d2; bestSeg = sp; bestBox = bp; }
+    };
+    cand(0.0f);
+    cand(1.0f);
+    for (uint32_t ax = 0; ax < 3; ++ax) {
+        const float dl = Comp(d, ax);
+        if (std::fabs(dl) > kEps) {
+            cand((-Comp(h, ax) - Comp(la, ax)) / dl);
+            cand((Comp(h, ax) - Comp(la, ax)) / dl);
+        }
+    }
+    outSeg = bc + QRotate(bq, bestSeg);
+    outBox = bc + QRotate(bq, bestBox);
+}
+// :467-518
+bool BoxCapsule(f3 bc, f4 bq, f3 h, f3 ca, f3 cb, float cr, f3 &n, f3 &pA, f3 &pB, float &pen)
+{
+    n = pA = pB = f3{0, 0, 0};
+    pen = 0.0f;
+    f3 segP, boxP;
+    bool inter = false;
+    ClosestSegmentBox(ca, cb, bc, bq, h, segP, boxP, inter);
+    if (!inter) {
+        const f3 d = segP - boxP;
+        const float d2 = dot(d, d);
+        if (d2 > cr * cr) return false;
+        const float dist = std::sqrt(std::max(d2, 0.0f));
+        n = dist > kEps ? d / dist : f3{0, 1, 0};
+        pA = boxP;
+        pB = segP - n * cr;
+        pen = PenetrationFromPoints(pA, pB, n);
+        return pen > 0.0f;
+    }
+    const f3 ls = QInvRotate(bq, segP - bc);
+    const f3 lfn = ClosestFaceNormalLocal(ls, h);
+    n = QRotate(bq, lfn);
+    const float depth = std::min(h.x - std::fabs(ls.x), std::min(h.y - std::fabs(ls.y), h.z - std::fabs(ls.z)));
+    pA = bc + QRotate(bq, ls + lfn * depth);
+    pB = segP - n * cr;
+    pen = PenetrationFromPoints(pA, pB, n);
+    return pen > 0.0f;
+}
+// GenerateRigidContact (:520-641)
+bool RigidContactPoints(uint32_t tA, f3 cA, f4 qA, f4 prA, f4 sA, uint32_t tB, f3 cB, f4 qB, f4 prB, f4 sB,
+                        f3 &n, f3 &pA, f3 &pB, float &pen)
+{
+    n = pA = pB = f3{0, 0, 0};
+    pen = 0.0f;
+    const uint32_t S = CN_COLLIDER_SPHERE, X = CN_COLLIDER_BOX, K = CN_COLLIDER_CAPSULE;
+    if (tA == S && tB == S) return SphereSphere(cA, SphereRadius(prA, sA), cB, SphereRadius(prB, sB), n, pA, pB, pen);
+    if (tA == S && tB == X) return SphereBox(cA, SphereRadius(prA, sA), cB, qB, BoxHalfExtents(prB, sB), n, pA, pB, pen);
+    if (tA == X && tB == S) {
+        f3 ns, ps, pb;
+        const bool hit = SphereBox(cB, SphereRadius(prB, sB), cA, qA, BoxHalfExtents(prA, sA), ns, ps, pb, pen);
+        n = -ns; pA = pb; pB = ps;
+        pen = PenetrationFromPoints(pA, pB, n);
+        return hit && pen > 0.0f;
+    }
+    if (tA == S && tB == K) {
+        f3 b0, b1; float rB = 0.0f;
+        CapsuleSegment(cB, qB, prB, sB, b0, b1, rB);
+        return SphereCapsule(cA, SphereRadius(prA, sA), b0, b1, rB, n, pA, pB, pen);
+    }
+    if (tA == K && tB == S) {
+        f3 a0, a1; float rA = 0.0f;
+        CapsuleSegment(cA, qA, prA, sA, a0, a1, rA);
+        f3 ns, ps, pc;
+        const bool hit = SphereCapsule(cB, SphereRadius(prB, sB), a0, a1, rA, ns, ps, pc, pen);
+        n = -ns; pA = pc; pB = ps;
+        pen = PenetrationFromPoints(pA, pB, n);
+        return hit && pen > 0.0f;
+    }
+    if (tA == X && tB == X) return BoxBox(cA, qA, BoxHalfExtents(prA, sA), cB, qB, BoxHalfExtents(prB, sB), n, pA, pB, pen);
+    if (tA == K && tB == K) {
+        f3 a0, a1, b0, b1, ca, cb; float rA = 0.0f, rB = 0.0f;
+        CapsuleSegment(cA, qA, prA, sA, a0, a1, rA);
+        CapsuleSegment(cB, qB, prB, sB, b0, b1, rB);
+        ClosestSegmentSegment(a0, a1, b0, b1, ca, cb);
+        return SphereSphere(ca, rA, cb, rB, n, pA, pB, pen);
+    }
+    if (tA == X && tB == K) {
+        f3 b0, b1; float rB = 0.0f;
+        CapsuleSegment(cB, qB, prB, sB, b0, b1, rB);
+        return BoxCapsule(cA, qA, BoxHalfExtents(prA, sA), b0, b1, rB, n, pA, pB, pen);
+    }
+    if (tA == K && tB == X) {
+        f3 a0, a1; float rA = 0.0f;
+        CapsuleSegment(cA, qA, prA, sA, a0, a1, rA);
+        f3 nb, pbx, pcap;
+        const bool hit = BoxCapsule(cB, qB, BoxHalfExtents(prB, sB), a0, a1, rA, nb, pbx, pcap, pen);
+        n = -nb; pA = pcap; pB = pbx;
+        pen = PenetrationFromPoints(pA, pB, n);
+        return hit && pen > 0.0f;
+    }
+    return false;
+}
+
+// physics_rigid_box_box_manifold.hlsli: face-preferring separating axis, incident face clipped
+// against the reference face (or the edge pair, or corner recovery), reduced to <= 4 points.
+struct BoxCand { f3 a, b; float pen; };
+bool BoxBoxSat(f3 cA, const f3 *axA, f3 hA, f3 cB, const f3 *axB, f3 hB, f3 &nOut, float &penOut, uint32_t &type,
+               uint32_t &ia, uint32_t &ib)
+{
+    nOut = f3{0, 0, 0}; penOut = 0.0f; type = 0; ia = ib = 0;
+    const f3 cd = cB - cA;
+    auto proj = [](f3 axis, const f3 *ax, f3 h) {
+        return h.x * std::fabs(dot(axis, ax[0])) + h.y * std::fabs(dot(axis, ax[1])) + h.z * std::fabs(dot(axis, ax[2]));
+    };
+    float bestFace = 3.402823466e+38f, bestEdge = 3.402823466e+38f;
+    f3 faceAxis{0, 1, 0}, edgeAxis{0, 1, 0};
+    uint32_t faceType = 0, faceA = 0, edgeA = 0, edgeB = 0;
+    bool hasEdge = false;
+    for (uint32_t side = 0; side < 2; ++side)
+        for (uint32_t i = 0; i < 3; ++i) {
+            f3 n = side == 0 ? axA[i] : axB[i];
+            const float ov = proj(n, axA, hA) + proj(n, axB, hB) - std::fabs(dot(cd, n));
+            if (ov < 0.0f) return false;
+            if (dot(cd, n) < 0.0f) n = -n;
+            if (ov < bestFace - 5.0e-4f) { bestFace = ov; faceAxis = n; faceType = side; faceA = i; }
+        }
+    for (uint32_t a = 0; a < 3; ++a)
+        for (uint32_t b = 0; b < 3; ++b) {
+            const f3 axis = cross(axA[a], axB[b]);
+            const float l2 = dot(axis, axis);
+            if (l2 <= kEps) continue;
+            hasEdge = true;
+            f3 n = axis * (1.0f / std::sqrt(l2));
+            const float ov = proj(n, axA, hA) + proj(n, axB, hB) - std::fabs(dot(cd, n));
+            if (ov < 0.0f) return false;
+            if (dot(cd, n) < 0.0f) n = -n;
+            if (ov < bestEdge) { bestEdge = ov; edgeAxis = n; edgeA = a; edgeB = b; }
+        }
+    if (hasEdge && bestEdge < bestFace * 0.95f - 1.0e-3f) {
+        nOut = edgeAxis; penOut = bestEdge; type = 2; ia = edgeA; ib = edgeB;
+    } else {
+        nOut = faceAxis; penOut = bestFace; type = faceType; ia = faceA; ib = 0;
+    }
+    return penOut > 0.0f;
+}
+void InsertBoxCand(f3 pa, f3 pb, float pen, float merge2, std::vector<BoxCand> &cand)
+{
+    if (pen <= kEps) return;
+    const f3 mid = (pa + pb) * 0.5f;
+    for (auto &c : cand) {
+        const f3 d = (c.a + c.b) * 0.5f - mid;
+        if (dot(d, d) <= merge2) {
+            if (pen > c.pen) c = BoxCand{pa, pb, pen};
+            return;
+        }
+    }
+    if (cand.size() < 16) { cand.push_back(BoxCand{pa, pb, pen}); return; }
+    size_t r = 0;
+    for (size_t i = 1; i < cand.size(); ++i) if (cand[i].pen < cand[r].pen) r = i;
+    if (pen > cand[r].pen) cand[r] = BoxCand{pa, pb, pen};
+}
+uint32_t ClipPlane(const f3 *in, uint32_t inCount, f3 origin, f3 normal, float offset, bool keepLess, f3 *out)
+{
+    if (inCount == 0) return 0;
+    uint32_t oc = 0;
+    f3 prev = in[inCount - 1];
+    float prevC = dot(prev - origin, normal);
+    bool prevIn = keepLess ? prevC <= offset : prevC >= offset;
+    for (uint32_t i = 0; i < inCount && i < 8; ++i) {
+        const f3 cur = in[i];
+        const float curC = dot(cur - origin, normal);
+        const bool curIn = keepLess ? curC <= offset : curC >= offset;
+        if (curIn != prevIn) {
+            const float den = curC - prevC;
+            const float t = std::fabs(den) > kEps ? (offset - prevC) / den : 0.0f;
+            if (oc < 8) out[oc++] = lerp3(prev, cur, saturate(t));
+        }
+        if (curIn && oc < 8) out[oc++] = cur;
+        prev = cur; prevC = curC; prevIn = curIn;
+    }
+    return oc;
+}
+bool InsideBox(f3 p, f3 c, f4 q, f3 h)
+{
+    const f3 l = QInvRotate(q, p - c);
+    return l.x >= -h.x && l.y >= -h.y && l.z >= -h.z && l.x <= h.x && l.y <= h.y && l.z <= h.z;
+}
+f3 ProjectInsideAlong(f3 p, f3 c, f4 q, f3 h, f3 dir)
+{
+    if (!InsideBox(p, c, q, h)) return ClosestPointOnBox(p, c, q, h);
+    const f3 lp = QInvRotate(q, p - c);
+    const f3 ld = QInvRotate(q, SafeNormalize(dir, f3{0, 1, 0}));
+    float bestT = 3.402823466e+38f;
+    for (uint32_t ax = 0; ax < 3; ++ax) {
+        const float d = Comp(ld, ax);
+        if (std::fabs(d) <= kEps) continue;
+        const float face = d > 0.0f ? Comp(h, ax) : -Comp(h, ax);
+        const float t = (face - Comp(lp, ax)) / d;
+        if (t >= 0.0f && t < bestT) bestT = t;
+    }
+    f3 ls = lp;
+    if (bestT < 3.402823466e+37f) ls = lp + ld * bestT;
+    else ls = lp + ClosestFaceNormalLocal(lp, h) * std::min(h.x - std::fabs(lp.x), std::min(h.y - std::fabs(lp.y), h.z - std::fabs(lp.z)));
+    return c + QRotate(q, ls);
+}
+uint32_t BoxBoxManifold(f3 cA, f4 qA, f3 hA, f3 cB, f4 qB, f3 hB, f3 nIn, float merge2, float slop, f3 &n,
+                        f3 *ptsA, f3 *ptsB, float *pens)
+{
+    std::vector<BoxCand> cand;
+    const f3 axA[3] = {QRotate(qA, f3{1, 0, 0}), QRotate(qA, f3{0, 1, 0}), QRotate(qA, f3{0, 0, 1})};
+    const f3 axB[3] = {QRotate(qB, f3{1, 0, 0}), QRotate(qB, f3{0, 1, 0}), QRotate(qB, f3{0, 0, 1})};
+    n = SafeNormalize(nIn, f3{0, 1, 0});
+    f3 satN; float satPen = 0.0f; uint32_t type = 0, ia = 0, ib = 0;
+    const bool sat = BoxBoxSat(cA, axA, hA, cB, axB, hB, satN, satPen, type, ia, ib);
+    if (sat) n = SafeNormalize(satN, n);
+    auto edge = [](uint32_t axis, f3 c, const f3 *ax, f3 h, f3 dir, f3 &e0, f3 &e1) {
+        const uint32_t oa = (axis + 1) % 3, ob = (axis + 2) % 3;
+        const float sa = dot(ax[oa], dir) >= 0.0f ? 1.0f : -1.0f;
+        const float sb = dot(ax[ob], dir) >= 0.0f ? 1.0f : -1.0f;
+        const f3 ec = c + ax[oa] * (Comp(h, oa) * sa) + ax[ob] * (Comp(h, ob) * sb);
+        const f3 eh = ax[axis] * Comp(h, axis);
+        e0 = ec - eh; e1 = ec + eh;
+    };
+    if (sat && type == 2) {
+        f3 ea0, ea1, eb0, eb1, pa, pb;
+        edge(ia, cA, axA, hA, n, ea0, ea1);
+        edge(ib, cB, axB, hB, -n, eb0, eb1);
+        ClosestSegmentSegment(ea0, ea1, eb0, eb1, pa, pb);
+        InsertBoxCand(pa, pb, std::max(satPen, PenetrationFromPoints(pa, pb, n)), merge2, cand);
+    }
+    if (sat && type < 2) {
+        const bool refA = type == 0;
+        const f3 *rax = refA ? axA : axB;
+        const f3 rc = refA ? cA : cB, rh = refA ? hA : hB;
+        const float sign = dot(rax[ia], refA ? n : -n) >= 0.0f ? 1.0f : -1.0f;
+        const uint32_t tu = (ia + 1) % 3, tv = (ia + 2) % 3;
+        const f3 refN = rax[ia] * sign;
+        const f3 refC = rc + refN * Comp(rh, ia);
+        const f3 refU = rax[tu], refV = rax[tv];
+        const float halfU = Comp(rh, tu), halfV = Comp(rh, tv);
+        const f3 *iax = refA ? axB : axA;
+        const f3 ic = refA ? cB : cA, ih = refA ? hB : hA;
+        uint32_t ii = 0;
+        float best = std::fabs(dot(iax[0], refN));
+        for (uint32_t i = 1; i < 3; ++i) {
+            const float al = std::fabs(dot(iax[i], refN));
+            if (al > best) { best = al; ii = i; }
+        }
+        const float isign = dot(iax[ii], refN) >= 0.0f ? -1.0f : 1.0f;
+        const uint32_t iu = (ii + 1) % 3, iv = (ii + 2) % 3;
+        const f3 iN = iax[ii] * isign;
+        const f3 iC = ic + iN * Comp(ih, ii);
+        const f3 du = iax[iu] * Comp(ih, iu), dv = iax[iv] * Comp(ih, iv);
+        f3 pA8[8] = {iC + du + dv, iC - du + dv, iC - du - dv, iC + du - dv}, pB8[8];
+        uint32_t pc = 4;
+        pc = ClipPlane(pA8, pc, refC, refU, halfU, true, pB8);
+        pc = ClipPlane(pB8, pc, refC, refU, -halfU, false, pA8);
+        pc = ClipPlane(pA8, pc, refC, refV, halfV, true, pB8);
+        pc = ClipPlane(pB8, pc, refC, refV, -halfV, false, pA8);
+        for (uint32_t i = 0; i < pc && i < 8; ++i) {
+            const f3 ip = pA8[i];
+            const float sep = dot(ip - refC, refN);
+            if (sep > slop) continue;
+            const f3 rp = ip - refN * sep;
+            const float pen = std::max(0.0f, -sep);
+            if (refA) InsertBoxCand(rp, ip, pen, merge2, cand);
+            else InsertBoxCand(ip, rp, pen, merge2, cand);
+        }
+    }
+    if (cand.empty()) {
+        for (uint32_t k = 0; k < 8; ++k) {
+            auto corner = [k](f3 c, f4 q, f3 h) {
+                return c + QRotate(q, f3{(k & 1u) ? h.x : -h.x, (k & 2u) ? h.y : -h.y, (k & 4u) ? h.z : -h.z});
+            };
+            const f3 ca = corner(cA, qA, hA);
+            f3 pbA = ClosestPointOnBox(ca, cB, qB, hB);
+            if (InsideBox(ca, cB, qB, hB)) pbA = ProjectInsideAlong(ca, cB, qB, hB, -n);
+            InsertBoxCand(ca, pbA, PenetrationFromPoints(ca, pbA, n), merge2, cand);
+            const f3 cb = corner(cB, qB, hB);
+            f3 paB = ClosestPointOnBox(cb, cA, qA, hA);
+            if (InsideBox(cb, cA, qA, hA)) paB = ProjectInsideAlong(cb, cA, qA, hA, n);
+            InsertBoxCand(paB, cb, PenetrationFromPoints(paB, cb, n), merge2, cand);
+        }
+    }
+    if (cand.empty()) return 0;
+    const f3 tx = SafeNormalize(cross(std::fabs(n.y) < 0.9f ? f3{0, 1, 0} : f3{1, 0, 0}, n), f3{1, 0, 0});
+    const f3 ty = cross(n, tx);
+    const size_t count = cand.size();
+    std::vector<float> mu(count), mv(count);
+    std::vector<bool> sel(count, false);
+    for (size_t i = 0; i < count; ++i) {
+        const f3 mid = (cand[i].a + cand[i].b) * 0.5f;
+        mu[i] = dot(mid, tx);
+        mv[i] = dot(mid, ty);
+    }
+    const uint32_t target = uint32_t(std::min<size_t>(count, 4));
+    size_t deepest = 0;
+    for (size_t i = 1; i < count; ++i) if (cand[i].pen > cand[deepest].pen) deepest = i;
+    sel[deepest] = true;
+    uint32_t out = 0;
+    ptsA[out] = cand[deepest].a; ptsB[out] = cand[deepest].b; pens[out++] = cand[deepest].pen;
+    while (out < target) {
+        size_t bi = 0; float bs = -1.0f; bool found = false;
+        for (size_t i = 0; i < count; ++i) {
+            if (sel[i]) continue;
+            float md = 3.402823466e+38f;
+            for (size_t j = 0; j < count; ++j) {
+                if (!sel[j]) continue;
+                const float du2 = mu[i] - mu[j], dv2 = mv[i] - mv[j];
+                md = std::min(md, du2 * du2 + dv2 * dv2);
+            }
+            const float score = md + cand[i].pen * 1.0e-4f;
+            if (score > bs) { bs = score; bi = i; found = true; }
+        }
+        if (!found) break;
+        sel[bi] = true;
+        ptsA[out] = cand[bi].a; ptsB[out] = cand[bi].b; pens[out++] = cand[bi].pen;
+    }
+    return out;
+}
+
+// physics_rigid_count_pairs / emit_pairs + generate_contacts: every moving collider against the
+// others (a moving partner once, at the higher collider index; a static one always), canonical
+// (lower shape type first), then one contact per pair.
+void rigidPairsAndContacts(cno_solver &s)
+{
+    s.rrPairs.clear();
+    s.rrContacts.clear();
+    const uint32_t C = s.C;
+    const uint32_t cap = std::max<uint32_t>(64u, 16u * C);
+    uint32_t required = 0;
+    const std::vector<uint32_t> &order = s.colliderQueryOrder;
+    for (uint32_t k = 0; k < s.activeMovingCount && order.size() >= 2; ++k) {
+        const uint32_t cA = order[k];
+        const cn_collider_broadphase &a = s.colBp[cA];
+        for (uint32_t cB : order) {
+            if (cB == cA) continue;
+            const cn_collider_broadphase &b = s.colBp[cB];
+            if (b.owner_body == a.owner_body) continue;
+            if (s.bodyType[b.owner_body] != CN_BODY_STATIC && cB < cA) continue;
+            if (a.environment_index != b.environment_index) continue;
+            if ((a.collision_mask & b.collision_layer) == 0u || (b.collision_mask & a.collision_layer) == 0u) continue;
+            if (!AabbOverlaps(s.colAabbMin[cA], s.colAabbMax[cA], s.colAabbMin[cB], s.colAabbMax[cB])) continue;
+            if (required < cap) s.rrPairs.push_back(a.shape_type > b.shape_type ? std::make_pair(cB, cA) : std::make_pair(cA, cB));
+            ++required;
+        }
+    }
+    s.requiredRigidRigidPairs = required;
+    s.rrContacts.assign(s.rrPairs.size() * 4, cno_solver::RigidPairContact{});
+    const float merge = s.desc.contact.manifold_merge_slop_multiplier * s.slop();
+    for (size_t p = 0; p < s.rrPairs.size(); ++p) {
+        const auto &pr = s.rrPairs[p];
+        cno_solver::RigidPairContact *slot = &s.rrContacts[4 * p];
+        const cn_collider_broadphase &bpA = s.colBp[pr.first], &bpB = s.colBp[pr.second];
+        const uint32_t bA = bpA.owner_body, bB = bpB.owner_body;
+        if (bA >= s.B || bB >= s.B || bA == bB) continue;
+        if (s.bodyType[bA] != CN_BODY_DYNAMIC && s.bodyType[bB] != CN_BODY_DYNAMIC) continue;
+        const f4 posA = s.predBodyPos[bA], posB = s.predBodyPos[bB];
+        const f4 qA = QNormalize(s.predBodyRot[bA]), qB = QNormalize(s.predBodyRot[bB]);
+        const cn_collider_geometry &gA = s.colGeo[pr.first], &gB = s.colGeo[pr.second];
+        const f4 prmA{gA.shape_params[0], gA.shape_params[1], gA.shape_params[2], gA.shape_params[3]};
+        const f4 prmB{gB.shape_params[0], gB.shape_params[1], gB.shape_params[2], gB.shape_params[3]};
+        const f4 scA = s.bodyScale[bA], scB = s.bodyScale[bB];
+        const f3 mat = CombineContactMaterial(s.colMat[pr.first], s.colMat[pr.second]);
+        const f3 cpA = xyz(posA) + QRotate(qA, f3{gA.local_position[0], gA.local_position[1], gA.local_position[2]} * xyz(scA));
+        const f3 cpB = xyz(posB) + QRotate(qB, f3{gB.local_position[0], gB.local_position[1], gB.local_position[2]} * xyz(scB));
+        const f4 cqA = QNormalize(QMul(qA, QNormalize(f4{gA.local_orientation[0], gA.local_orientation[1], gA.local_orientation[2], gA.local_orientation[3]})));
+        const f4 cqB = QNormalize(QMul(qB, QNormalize(f4{gB.local_orientation[0], gB.local_orientation[1], gB.local_orientation[2], gB.local_orientation[3]})));
+        f3 a0, a1, b0, b1;
+        ComputeBodyAabb(bpA.shape_type, cpA, cqA, prmA, scA, a0, a1);
+        ComputeBodyAabb(bpB.shape_type, cpB, cqB, prmB, scB, b0, b1);
+        if (!AabbOverlaps(a0, a1, b0, b1)) continue;
+        auto write = [&](uint32_t k, f3 n, float pen, f3 pa, f3 pb) {
+            cno_solver::RigidPairContact c;
+            c.bodyA = bA; c.bodyB = bB; c.active = true;
+            c.normalPenetration = mk4(n, pen);
+            c.material = mk4(mat, 0.0f);
+            c.localA = mk4(QInvRotate(qA, pa - xyz(posA)), 1.0f);
+            c.localB = mk4(QInvRotate(qB, pb - xyz(posB)), 1.0f);
+            slot[k] = c;
+        };
+        if (bpA.shape_type == CN_COLLIDER_BOX && bpB.shape_type == CN_COLLIDER_BOX) {
+            const f3 hA = BoxHalfExtents(prmA, scA), hB = BoxHalfExtents(prmB, scB);
+            const f3 axA[3] = {QRotate(cqA, f3{1, 0, 0}), QRotate(cqA, f3{0, 1, 0}), QRotate(cqA, f3{0, 0, 1})};
+            const f3 axB[3] = {QRotate(cqB, f3{1, 0, 0}), QRotate(cqB, f3{0, 1, 0}), QRotate(cqB, f3{0, 0, 1})};
+            f3 satN; float satPen = 0.0f; uint32_t t0, t1, t2;
+            if (!BoxBoxSat(cpA, axA, hA, cpB, axB, hB, satN, satPen, t0, t1, t2)) continue;
+            f3 pa[4], pb[4], n; float pens[4];
+            const uint32_t m = BoxBoxManifold(cpA, cqA, hA, cpB, cqB, hB, SafeNormalize(satN, f3{0, 1, 0}), merge * merge,
+                                              s.slop(), n, pa, pb, pens);
+            if (m > 0) {
+                for (uint32_t k = 0; k < m; ++k) write(k, n, pens[k], pa[k], pb[k]);
+                continue;
+            }
+        }
+        f3 n, pa, pb;
+        float pen = 0.0f;
+        if (!RigidContactPoints(bpA.shape_type, cpA, cqA, prmA, scA, bpB.shape_type, cpB, cqB, prmB, scB, n, pa, pb, pen) ||
+            pen <= 0.0f) continue;
+        write(0, SafeNormalize(n, f3{0, 1, 0}), pen, pa, pb);
+    }
+}
+
+// physics_rigid_init_contact_velocities.cs.hlsl: canonical contacts grouped by body pair (pair
+// order within a group, at most 16), each with its restitution target.
+void rigidVelocityInit(cno_solver &s)
+{
+    s.rrGroups.clear();
+    s.rrGroupBodies.clear();
+    std::vector<std::pair<uint64_t, uint32_t>> keyed;
+    for (uint32_t p = 0; p < s.rrContacts.size(); ++p) {
+        const auto &c = s.rrContacts[p];
+        if (!c.active) continue;
+        keyed.push_back({uint64_t(std::min(c.bodyA, c.bodyB)) * s.B + std::max(c.bodyA, c.bodyB), p});
+    }
+    std::stable_sort(keyed.begin(), keyed.end(), [](const auto &x, const auto &y) { return x.first < y.first; });
+    const float thr = s.desc.contact.rigid_restitution_velocity_threshold;
+    for (size_t j = 0; j < keyed.size(); ++j) {
+        if (j == 0 || keyed[j].first != keyed[j - 1].first) {
+            s.rrGroups.emplace_back();
+            const auto &c = s.rrContacts[keyed[j].second];
+            s.rrGroupBodies.push_back({std::min(c.bodyA, c.bodyB), std::max(c.bodyA, c.bodyB)});
+        }
+        if (s.rrGroups.back().size() >= 16u) continue;
+        auto c = s.rrContacts[keyed[j].second];
+        if (c.bodyA > c.bodyB) {
+            std::swap(c.bodyA, c.bodyB);
+            c.normalPenetration = mk4(-xyz(c.normalPenetration), c.normalPenetration.w);
+            std::swap(c.localA, c.localB);
+        }
+        cno_solver::RigidSlot sl;
+        const f3 nrm = SafeNormalize(xyz(c.normalPenetration), f3{0, 1, 0});
+        sl.normal = mk4(nrm, saturate(c.material.x));
+        sl.localA = mk4(xyz(c.localA), saturate(c.material.z));
+        sl.localB = c.localB;
+        sl.state = f4{0, 0, 0, 0};
+        const f4 pA = s.predBodyPos[c.bodyA], pB = s.predBodyPos[c.bodyB];
+        const f4 oA = QNormalize(s.predBodyRot[c.bodyA]), oB = QNormalize(s.predBodyRot[c.bodyB]);
+        const f3 rA = (xyz(pA) + QRotate(oA, xyz(c.localA))) - xyz(pA);
+        const f3 rB = (xyz(pB) + QRotate(oB, xyz(c.localB))) - xyz(pB);
+        const f3 vA = xyz(s.predBodyLin[c.bodyA]) + cross(xyz(s.predBodyAng[c.bodyA]), rA);
+        const f3 vB = xyz(s.predBodyLin[c.bodyB]) + cross(xyz(s.predBodyAng[c.bodyB]), rB);
+        const float nv = dot(vB - vA, nrm);
+        if (nv < -thr) sl.state.y = -saturate(c.material.y) * nv;
+        s.rrGroups.back().push_back(sl);
+    }
+}
+
+// physics_rigid_depenetrate_contacts.cs.hlsl:22-137 (summed in pair order)
+void rigidDepenetration(cno_solver &s)
+{
+    const float slop = s.slop(), baum = s.desc.rigid.depenetration_baumgarte;
+    const float maxC = s.desc.rigid.depenetration_max_correction_per_iteration;
+    const float relax = s.desc.rigid.depenetration_relaxation;
+    const float minFric = s.desc.contact.position_friction_min_distance;
+    for (const auto &c : s.rrContacts) {
+        if (!c.active) continue;
+        const uint32_t bA = c.bodyA, bB = c.bodyB;
+        const f4 pA0 = s.predBodyPos[bA], pB0 = s.predBodyPos[bB];
+        const bool dA = s.bodyType[bA] == CN_BODY_DYNAMIC, dB = s.bodyType[bB] == CN_BODY_DYNAMIC;
+        const float iA = dA ? pA0.w : 0.0f, iB = dB ? pB0.w : 0.0f;
+        if (iA == 0.0f && iB == 0.0f) continue;
+        const f4 qA = QNormalize(s.predBodyRot[bA]), qB = QNormalize(s.predBodyRot[bB]);
+        const f4 pqA = QNormalize(s.prevBodyRot[bA]), pqB = QNormalize(s.prevBodyRot[bB]);
+        f3 inA = xyz(s.bodyInvInertia[bA]), inB = xyz(s.bodyInvInertia[bB]);
+        if (iA == 0.0f) inA = f3{0, 0, 0};
+        if (iB == 0.0f) inB = f3{0, 0, 0};
+        const f3 ptA = xyz(pA0) + QRotate(qA, xyz(c.localA)), ptB = xyz(pB0) + QRotate(qB, xyz(c.localB));
+        const f3 ppA = xyz(s.prevBodyPos[bA]) + QRotate(pqA, xyz(c.localA));
+        const f3 ppB = xyz(s.prevBodyPos[bB]) + QRotate(pqB, xyz(c.localB));
+        const f3 n = SafeNormalize(xyz(c.normalPenetration), f3{0, 1, 0});
+        const float raw = std::max(-dot(ptB - ptA, n) - slop, 0.0f);
+        const float pen = std::min(raw * baum, maxC);
+        if (pen <= 0.0f) continue;
+        const f3 rA = ptA - xyz(pA0), rB = ptB - xyz(pB0);
+        const float den = ContactEffectiveMass(iA, inA, qA, rA, n) + ContactEffectiveMass(iB, inB, qB, rB, n);
+        if (den <= kEps) continue;
+        const float lambda = (pen / den) * relax;
+        f3 tA = -n * (iA * lambda);
+        f3 rotA = -MulWorldInvInertia(inA, qA, cross(rA, n)) * lambda;
+        f3 tB = n * (iB * lambda);
+        f3 rotB = MulWorldInvInertia(inB, qB, cross(rB, n)) * lambda;
+        const f3 rel = (ptB - ppB) - (ptA - ppA);
+        const f3 fd = PositionFrictionDelta(ProjectOntoTangent(rel, n), pen, saturate(c.material.x), saturate(c.material.z), minFric);
+        const float fdist = length(fd);
+        if (fdist > 0.0f) {
+            const f3 t = fd / fdist;
+            const float tden = ContactEffectiveMass(iA, inA, qA, rA, t) + ContactEffectiveMass(iB, inB, qB, rB, t);
+            if (tden > kEps) {
+                const float tl = (fdist / tden) * relax;
+                tA += t * (iA * tl);
+                rotA += MulWorldInvInertia(inA, qA, cross(rA, t)) * tl;
+                tB -= t * (iB * tl);
+                rotB -= MulWorldInvInertia(inB, qB, cross(rB, t)) * tl;
+            }
+        }
+        if (dA && iA != 0.0f) { s.bodyTransCorr[bA] += tA; s.bodyRotCorr[bA] += rotA; }
+        if (dB && iB != 0.0f) { s.bodyTransCorr[bB] += tB; s.bodyRotCorr[bB] += rotB; }
+    }
+}
+
+// physics_rigid_solve_contact_velocities.cs.hlsl (one group at a time, the velocity change of
+// each group summed into the bodies' corrections)
+void rigidSolveVelocities(cno_solver &s)
+{
+    const float slop = s.slop(), stiff = s.desc.rigid.velocity_penetration_stiffness;
+    for (size_t g = 0; g < s.rrGroups.size(); ++g) {
+        auto &slots = s.rrGroups[g];
+        const uint32_t bA = s.rrGroupBodies[g].first, bB = s.rrGroupBodies[g].second;
+        const f4 pA = s.predBodyPos[bA], pB = s.predBodyPos[bB];
+        const float iA = s.bodyType[bA] == CN_BODY_DYNAMIC ? pA.w : 0.0f;
+        const float iB = s.bodyType[bB] == CN_BODY_DYNAMIC ? pB.w : 0.0f;
+        if (iA == 0.0f && iB == 0.0f) continue;
+        const f4 oA = QNormalize(s.predBodyRot[bA]), oB = QNormalize(s.predBodyRot[bB]);
+        f3 inA = xyz(s.bodyInvInertia[bA]), inB = xyz(s.bodyInvInertia[bB]);
+        if (iA == 0.0f) inA = f3{0, 0, 0};
+        if (iB == 0.0f) inB = f3{0, 0, 0};
+        const f3 lA0 = xyz(s.predBodyLin[bA]), lB0 = xyz(s.predBodyLin[bB]);
+        const f3 aA0 = xyz(s.predBodyAng[bA]), aB0 = xyz(s.predBodyAng[bB]);
+        f3 lA = lA0, lB = lB0, aA = aA0, aB = aB0;
+        for (uint32_t pass = 0; pass < 2; ++pass) {
+            for (auto &sl : slots) {
+                const bool hasRest = sl.state.y > 0.0f;
+                if ((pass == 0 && hasRest) || (pass == 1 && !hasRest)) continue;
+                const f3 n = SafeNormalize(xyz(sl.normal), f3{0, 1, 0});
+                const f3 ptA = xyz(pA) + QRotate(oA, xyz(sl.localA)), ptB = xyz(pB) + QRotate(oB, xyz(sl.localB));
+                const f3 rA = ptA - xyz(pA), rB = ptB - xyz(pB);
+                const float nv = dot((lB + cross(aB, rB)) - (lA + cross(aA, rA)), n);
+                const float pen = std::max(PenetrationFromPoints(ptA, ptB, n) - slop, 0.0f);
+                const float nd = ContactEffectiveMass(iA, inA, oA, rA, n) + ContactEffectiveMass(iB, inB, oB, rB, n);
+                if (nd <= kEps) continue;
+                float vi = (sl.state.y - nv) / nd;
+                if (vi < -sl.state.x) vi = -sl.state.x;
+                const float pi = pen > 0.0f ? (stiff * pen) / nd : 0.0f;
+                const float applied = vi + pi;
+                sl.state.x = sl.state.x + applied;
+                if (std::fabs(applied) > kEps) {
+                    const f3 imp = n * applied;
+                    if (iA > kEps) { lA += -imp * iA; aA += MulWorldInvInertia(inA, oA, cross(rA, -imp)); }
+                    if (iB > kEps) { lB += imp * iB; aB += MulWorldInvInertia(inB, oB, cross(rB, imp)); }
+                }
+                const float kf = saturate(sl.normal.w), sf = saturate(sl.localA.w);
+                const f3 tv = ProjectOntoTangent((lB + cross(aB, rB)) - (lA + cross(aA, rA)), n);
+                const float ts = length(tv);
+                if (ts > 1.0e-5f) {
+                    const f3 t = tv / ts;
+                    const float td = ContactEffectiveMass(iA, inA, oA, rA, t) + ContactEffectiveMass(iB, inB, oB, rB, t);
+                    if (td > kEps) {
+                        const float raw = -dot(tv, t) / td;
+                        const float old = sl.state.z;
+                        const float maxS = sf * sl.state.x, maxD = kf * sl.state.x;
+                        const float un = old + raw;
+                        float acc = un;
+                        if (std::fabs(un) > maxS) acc = std::min(std::max(un, -maxD), maxD);
+                        const float at = acc - old;
+                        sl.state.z = acc;
+                        if (std::fabs(at) > kEps) {
+                            const f3 ti = t * at;
+                            if (iA > kEps) { lA += -ti * iA; aA += MulWorldInvInertia(inA, oA, cross(rA, -ti)); }
+                            if (iB > kEps) { lB += ti * iB; aB += MulWorldInvInertia(inB, oB, cross(rB, ti)); }
+                        }
+                    }
+                }
+            }
+        }
+        if (iA > kEps) { s.bodyLinVelCorr[bA] += lA - lA0; s.bodyAngVelCorr[bA] += aA - aA0; }
+        if (iB > kEps) { s.bodyLinVelCorr[bB] += lB - lB0; s.bodyAngVelCorr[bB] += aB - aB0; }
+    }
+}
+
 // physics_rigid_apply_contact_velocities.cs.hlsl:14-58
 void applyRigidContactVelocities(cno_solver &s)
 {
@@ -2060,6 +2832,8 @@ void stepFrame(cno_solver &s, float frameDt)
         const bool hasBroadphase = hasSoftSoftContact || hasFluidWork || hasRigidCand;
 
         predictRigid(s, dt);
+        const bool rigidRigid = s.hasDynamic && rrIt > 0 && s.colliderQueryOrder.size() >= 2 && s.activeMovingCount > 0;
+        if (rigidRigid) rigidPairsAndContacts(s);
         predictSoft(s, dt);
         if (hasBroadphase) broadphase(s);
         s.particlePairs.clear();
@@ -2070,6 +2844,7 @@ void stepFrame(cno_solver &s, float frameDt)
             if (hasRigidCand) buildParticleRigidCandidates(s);
             if (hasFluidWork && s.C > 0) buildFluidBoundaryCandidates(s);
         }
+        if (rigidRigid) rigidVelocityInit(s);
         // clearSoftConstraintState (physics_clear_soft_constraint_state.cs.hlsl:14-54)
         std::fill(s.posCorr.begin(), s.posCorr.end(), f4{0, 0, 0, 0});
         std::fill(s.velCorr.begin(), s.velCorr.end(), f4{0, 0, 0, 0});
@@ -2114,8 +2889,10 @@ void stepFrame(cno_solver &s, float frameDt)
             if (runContacts) particleParticleContacts(s);
             if (runRigid) particleRigidContacts(s);
             if (runContacts || runRigid) applyPositionCorrections(s);
+            const bool runRigidRigid = rigidRigid && it < rrIt;
+            if (runRigidRigid) rigidDepenetration(s);
             // applyRigidCorrections (physics_solver.cpp:1170-1177); zero sums without dynamic bodies
-            if (runRigid && s.hasDynamic) applyRigidCorrections(s);
+            if ((runRigid || runRigidRigid) && s.hasDynamic) applyRigidCorrections(s);
         }
         // updateRigidVelocities (physics_solver.cpp:1241-1246); restates the predict without
         // dynamic bodies
@@ -2133,6 +2910,12 @@ void stepFrame(cno_solver &s, float frameDt)
         updateSurfaceTriangleNormals(s);
         updateSurfaceVertexNormals(s);
         updateSurfaceBounds(s);
+        // solveRigidContactVelocities (physics_solver.cpp:1345-1354)
+        if (rigidRigid)
+            for (uint32_t it = 0; it < std::max(rrIt, jointIt); ++it) {
+                if (it < rrIt) rigidSolveVelocities(s);
+                applyRigidContactVelocities(s);
+            }
         // copyPredictedRigidBodiesToPersistentState
         for (uint32_t b = 0; b < s.B; ++b) {
             s.bodyPos[b] = s.predBodyPos[b];
@@ -2261,12 +3044,14 @@ CN_API uint32_t cno_meta(cno_solver *s, uint32_t *out, uint32_t n)
 {
     // (required rigid pairs, rigid pair count, required particle pairs, particle pair count,
     //  active rigid contacts, active particle contacts, neighbour-list truncations)
-    const uint32_t vals[7] = {s->requiredRigidPairs, uint32_t(s->rigidPairs.size()),
+    //  required rigid-rigid collider pairs, rigid-rigid pairs kept)
+    const uint32_t vals[9] = {s->requiredRigidPairs, uint32_t(s->rigidPairs.size()),
                               s->requiredParticlePairs, uint32_t(s->particlePairs.size()),
                               uint32_t(s->activeRigidContacts.size()),
-                              uint32_t(s->activeParticleContacts.size()), s->truncations};
-    for (uint32_t i = 0; i < n && i < 7; ++i) out[i] = vals[i];
-    return 7;
+                              uint32_t(s->activeParticleContacts.size()), s->truncations,
+                              s->requiredRigidRigidPairs, uint32_t(s->rrPairs.size())};
+    for (uint32_t i = 0; i < n && i < 9; ++i) out[i] = vals[i];
+    return 9;
 }
 
 // Host derivations restated for cross-checking the product's authoring code:
