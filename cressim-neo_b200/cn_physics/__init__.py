@@ -281,6 +281,23 @@ class World:
         _check(self._lib.cn_world_add_collider(self._h, C.byref(d), C.byref(out)))
         return out.value
 
+    def set_rigid_proxy_particles(self, body: int, local_positions, radius: float, *, friction=0.5,
+                                  restitution=0.0, damping=0.0, static_friction=-1.0, environment=0, layer=1,
+                                  mask=0xFFFFFFFF) -> None:
+        """Proxy collision particles of `body` at (K, 3) body-frame points (before the body scale):
+        carried with the body, they collide with particles and with other bodies' colliders."""
+        pos = np.ascontiguousarray(np.asarray(local_positions, dtype=np.float32).reshape(-1, 3))
+        d = _abi.RigidProxyDesc()
+        self._lib.cn_rigid_proxy_desc_defaults(C.byref(d))
+        d.body = body
+        d.local_positions = pos.ctypes.data_as(_abi.P_f32)
+        d.count = pos.shape[0]
+        d.radius = radius
+        d.material = _abi.ContactMaterialDesc(friction, restitution, damping, static_friction)
+        d.environment_index, d.collision_layer, d.collision_mask = environment, layer, mask
+        _check(self._lib.cn_world_set_rigid_proxy_particles(self._h, C.byref(d)))
+        self._soa = None
+
     def add_surface_mesh(self, owner: str, index: int, positions, indices, normals=None,
                          match_epsilon: float = 1.0e-3) -> int:
         """Binds a render mesh to soft body / cloth `index` (owner "soft_body" or "cloth"): (V, 3)

@@ -109,6 +109,7 @@ class WorldSoA(C.Structure):
         ("body_collider_indices", P_u32), ("body_collider_index_count", u32),
         ("collider_count", u32), ("collider_geometry", C.c_void_p), ("collider_broadphase", C.c_void_p),
         ("collider_materials", P_f32), ("surface_render", C.POINTER(SurfaceRenderData)),
+        ("rigid_proxy_local_positions", P_f32), ("body_proxy_contact_materials", P_f32),
     ]
 
 
@@ -165,6 +166,12 @@ class ColliderDesc(C.Structure):
                 ("collision_layer", u32), ("collision_mask", u32)]
 
 
+class RigidProxyDesc(C.Structure):
+    _fields_ = [("body", u32), ("local_positions", P_f32), ("count", u32), ("radius", f32),
+                ("material", ContactMaterialDesc), ("environment_index", u32), ("collision_layer", u32),
+                ("collision_mask", u32)]
+
+
 class Meta(C.Structure):
     _fields_ = [(n, u32) for n in (
         "particle_rigid_candidate_count", "required_particle_rigid_candidate_count",
@@ -172,8 +179,9 @@ class Meta(C.Structure):
         "required_particle_particle_candidate_count", "particle_particle_candidate_overflow",
         "fluid_boundary_candidate_overflow", "active_particle_rigid_contact_count",
         "active_particle_contact_count", "fluid_neighbor_truncations", "device_wait_timeouts",
-        "rigid_rigid_candidate_count", "required_rigid_rigid_candidate_count", "rigid_rigid_candidate_overflow")] + [
-        ("reserved", u32 * 2)]
+        "rigid_rigid_candidate_count", "required_rigid_rigid_candidate_count", "rigid_rigid_candidate_overflow",
+        "proxy_rigid_contact_count", "required_proxy_rigid_contact_count", "proxy_rigid_contact_overflow")] + [
+        ("reserved", u32 * 1)]
 
 
 class SceneView(C.Structure):
@@ -247,6 +255,7 @@ SIGNATURES = [
     ("cn_strand_desc_defaults", None, [C.POINTER(StrandDesc)]),
     ("cn_rigid_body_desc_defaults", None, [C.POINTER(RigidBodyDesc)]),
     ("cn_collider_desc_defaults", None, [C.POINTER(ColliderDesc)]),
+    ("cn_rigid_proxy_desc_defaults", None, [C.POINTER(RigidProxyDesc)]),
     ("cn_world_create", C.c_int, [C.POINTER(C.c_void_p)]),
     ("cn_world_destroy", None, [C.c_void_p]),
     ("cn_world_add_soft_body_grid", C.c_int, [C.c_void_p, C.POINTER(SoftBodyGridDesc), P_u32]),
@@ -261,6 +270,7 @@ SIGNATURES = [
     ("cn_world_add_strand", C.c_int, [C.c_void_p, C.POINTER(StrandDesc), P_u32]),
     ("cn_world_add_rigid_body", C.c_int, [C.c_void_p, C.POINTER(RigidBodyDesc), P_u32]),
     ("cn_world_add_collider", C.c_int, [C.c_void_p, C.POINTER(ColliderDesc), P_u32]),
+    ("cn_world_set_rigid_proxy_particles", C.c_int, [C.c_void_p, C.POINTER(RigidProxyDesc)]),
     ("cn_world_get_soa", C.c_int, [C.c_void_p, C.POINTER(WorldSoA)]),
     ("cn_solver_create", C.c_int, [C.POINTER(SolverDesc), C.c_int, C.POINTER(C.c_void_p)]),
     ("cn_solver_destroy", None, [C.c_void_p]),

@@ -459,6 +459,8 @@ CN_API cn_status cn_batch_add_scene(cn_batch *b, const cn_world_soa *w, uint32_t
     for (uint32_t i = 0; i < N; ++i) {
         if (w->kinds[i] == CN_PARTICLE_FLUID)
             return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: fluid particles are not batched");
+        if (w->owner_types[i] == CN_OWNER_RIGID_BODY)
+            return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: rigid proxy particles are not batched");
         const uint32_t ph = w->metadata[4 * i + 1];
         if (ph & CN_PHASE_SELF_COLLIDE)
             return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: self-colliding bodies are not batched");

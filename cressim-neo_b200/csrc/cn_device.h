@@ -45,8 +45,10 @@ struct DeviceMeta {
     uint32_t rigidRigidPairCount;     // min(required, capacity) collider pairs of the rigid broadphase
     uint32_t requiredRigidRigidPairs;
     uint32_t rigidGroupCount;         // body pairs with active contacts (velocity-solve groups)
-    uint32_t rigidContactSlots;       // kRigidPairContacts x rigidRigidPairCount
-    uint32_t reserved[3];
+    uint32_t rigidContactSlots;       // kRigidPairContacts x rigidRigidPairCount + proxy contact slots
+    uint32_t proxyContactSlots;       // min(required, capacity) proxy particle -> body contact slots
+    uint32_t requiredProxyContacts;   // proxy candidates (GpuProxyRigidContactMeta.requiredContactCount)
+    uint32_t reserved[1];
 };
 
 // Rigid-rigid contact point of a collider pair (GpuRigidContact, physics_rigid_types.hlsli):
@@ -158,6 +160,14 @@ struct Scene {
     uint32_t *bvhParent = nullptr, *bvhVisits = nullptr;   // per node / internal node
     float4 *bvhMin = nullptr, *bvhMax = nullptr;           // per node
     float4 *bvhBounds = nullptr;                           // scene centre bounds (2)
+    // Contact slots: kRigidPairContacts per collider pair, then one per proxy candidate
+    // (physics_rigid_generate_proxy_contacts.cs.hlsl appends after the pair contacts)
+    uint32_t proxyCapacity = 0, rrSlotCapacity = 0;
+    // rigid proxy particles: the first nProxy particles, owned by rigid bodies
+    // (physics_particle_sync_rigid_proxy_particles.cs.hlsl)
+    uint32_t nProxy = 0;
+    const float4 *proxyLocal = nullptr;    // per proxy: scaled body-frame position
+    const float4 *bodyProxyMat = nullptr;  // per body: its proxies' contact material
     // dynamic bodies: corrections summed (float atomics) over a pass, applied per body after it
     uint32_t hasDynamic = 0;
     float4 *bodyTransCorr = nullptr, *bodyRotCorr = nullptr, *bodyLinVelCorr = nullptr, *bodyAngVelCorr = nullptr;
@@ -293,6 +303,9 @@ void launchCopyPredictedRigid(const Scene &s, cudaStream_t st);
 void launchApplyRigidCorrections(const Scene &s, const Config &c, cudaStream_t st);
 void launchUpdateRigidVelocities(const Scene &s, float dt, cudaStream_t st);
 void launchRigidContactVelocitiesDynamic(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st);
+// Rigid proxy particles placed at their bodies' predicted poses
+// (physics_particle_sync_rigid_proxy_particles.cs.hlsl; the predict does it for the first time).
+void launchSyncRigidProxies(const Scene &s, cudaStream_t st);
 
 // ---------------------------------------------------------------- rigid-rigid contacts (cn_rigid.cu)
 // Scratch of the rigid broadphase and grouping (sort + scan), in bytes, for C colliders and
@@ -301,6 +314,9 @@ size_t rigidScratchBytes(uint32_t colliders, uint32_t pairs);
 // LBVH over the colliders' world AABBs, the moving colliders' candidate pairs, and one contact
 // per pair (physics_rigid_bvh_*, physics_rigid_count/emit_pairs, physics_rigid_generate_contacts).
 void launchRigidBroadphaseAndContacts(const Scene &s, const Config &c, void *scratch, cudaStream_t st);
+// One contact slot per proxy candidate after the pair contacts: a proxy particle as a sphere of
+// its body against the candidate body's colliders (physics_rigid_generate_proxy_contacts).
+void launchProxyRigidContacts(const Scene &s, cudaStream_t st);
 // Body-pair groups of the active contacts and their velocity slots
 // (physics_rigid_init_contact_velocities).
 void launchRigidVelocityInit(const Scene &s, const Config &c, void *scratch, cudaStream_t st);

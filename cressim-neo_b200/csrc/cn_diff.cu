@@ -770,7 +770,8 @@ CN_API cn_status cn_diff_set_scene(cn_diff *g, const cn_world_soa *w)
         return setError(CN_ERR_UNSUPPORTED, "cn_diff_set_scene: the differentiable rollout covers edges and tets "
                                             "without colliders");
     for (uint32_t i = 0; i < w->particle_count; ++i)
-        if (w->kinds[i] == CN_PARTICLE_FLUID) return setError(CN_ERR_UNSUPPORTED, "cn_diff_set_scene: fluid particles");
+        if (w->kinds[i] == CN_PARTICLE_FLUID || (w->owner_types && w->owner_types[i] == CN_OWNER_RIGID_BODY))
+            return setError(CN_ERR_UNSUPPORTED, "cn_diff_set_scene: fluid or rigid proxy particles");
     cudaSetDevice(g->device);
     cudaDeviceSynchronize();
     g->f32.release();

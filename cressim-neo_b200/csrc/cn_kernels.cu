@@ -217,6 +217,14 @@ __global__ void k_copyPredictedRigid(Scene s)
 // physics_soft_predict.cs.hlsl:12-47, physics_particle_build_broad_phase_entries.cs.hlsl:9-35,
 // physics_particle_build_broad_phase_keys.cs.hlsl:8-23
 // ------------------------------------------------------------------------------------------
+// physics_particle_sync_rigid_proxy_particles.cs.hlsl: a proxy particle at its body's predicted pose
+__device__ __forceinline__ f3 proxyWorldPosition(const Scene &s, uint32_t i)
+{
+    const uint32_t b = s.ownerIdx[i];
+    const float4 q = qNormalize(s.predBodyRot[b]);
+    return xyz(s.predBodyPos[b]) + qRotate(q, xyz(s.proxyLocal[i]));
+}
+
 __device__ __forceinline__ void predictParticle(const Scene &s, float dt, float gx, float gy, float gz, bool writeKeys, uint32_t i)
 {
     const float4 pim = s.x[i];
@@ -234,6 +242,10 @@ __device__ __forceinline__ void predictParticle(const Scene &s, float dt, float 
         vel = vel + f3{gx, gy, gz} * (dt * gs);
         pp = pos + vel * dt;
         s.v[i] = mk4(vel, 0.0f);
+        s.x[i] = mk4(pp, pim.w);
+    }
+    if (i < s.nProxy) { // the proxy sync that follows the predict (physics_solver.cpp:587-592)
+        pp = proxyWorldPosition(s, i);
         s.x[i] = mk4(pp, pim.w);
     }
     if (!writeKeys) return;
@@ -1423,6 +1435,13 @@ __global__ void __launch_bounds__(kThreads) k_solveDistances(Scene s, float dt, 
     s.distCorr[2 * c + 1] = cB;
 }
 
+__device__ __forceinline__ void atomicAdd3(float4 *p, f3 v)
+{
+    atomicAdd(&p->x, v.x);
+    atomicAdd(&p->y, v.y);
+    atomicAdd(&p->z, v.z);
+}
+
 // ------------------------------------------------------------------------------------------
 // Contacts
 // ------------------------------------------------------------------------------------------
@@ -1457,8 +1476,34 @@ __global__ void __launch_bounds__(kThreads) k_particleContactGenerate(Scene s)
     s.particleContacts[pi] = out;
 }
 
-// physics_particle_solve_explicit_contacts.cs.hlsl (non-proxy branch); float atomics as in the
-// reference.
+// The rigid side of a proxy particle in a particle-particle contact: its body (inverse mass only
+// for a dynamic body), the contact point at the body's predicted pose and its lever arm.
+struct ProxySide {
+    uint32_t body;
+    float4 q;
+    f3 r, invI;
+};
+
+__device__ __forceinline__ void loadProxySide(const Scene &s, uint32_t p, ProxySide &ps, float &invMass, f3 &cur)
+{
+    const uint32_t b = s.ownerIdx[p];
+    const float4 bp = s.predBodyPos[b];
+    ps.body = b;
+    ps.q = qNormalize(s.predBodyRot[b]);
+    invMass = s.bodyType[b] == CN_BODY_DYNAMIC ? bp.w : 0.0f;
+    ps.invI = invMass > kEps ? xyz(s.bodyInvInertia[b]) : f3{0.f, 0.f, 0.f};
+    cur = xyz(bp) + qRotate(ps.q, xyz(s.proxyLocal[p]));
+    ps.r = cur - xyz(bp);
+}
+
+__device__ __forceinline__ f3 proxyPreviousPoint(const Scene &s, uint32_t p, uint32_t b)
+{
+    return xyz(s.prevBodyPos[b]) + qRotate(qNormalize(s.prevBodyRot[b]), xyz(s.proxyLocal[p]));
+}
+
+// physics_particle_solve_explicit_contacts.cs.hlsl; float atomics as in the reference.  A rigid
+// proxy's share goes to its body's translation / rotation sums (effective mass with the lever
+// arm); every other particle's to its position correction.
 __global__ void __launch_bounds__(kThreads) k_particleContactSolve(Scene s, Config cfg)
 {
     const uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1467,39 +1512,72 @@ __global__ void __launch_bounds__(kThreads) k_particleContactSolve(Scene s, Conf
     if (c.active == 0u) return;
     atomicAdd(&s.meta_->activeParticleContacts, 1u);
     const float4 A = s.x[c.a], Bp = s.x[c.b];
-    const float iA = A.w, iB = Bp.w;
+    float iA = A.w, iB = Bp.w;
+    f3 curA = xyz(A), curB = xyz(Bp);
+    const bool proxyA = c.a < s.nProxy, proxyB = c.b < s.nProxy;
+    ProxySide psA{}, psB{};
+    if (proxyA) loadProxySide(s, c.a, psA, iA, curA);
+    if (proxyB) loadProxySide(s, c.b, psB, iB, curB);
     if (iA <= kEps && iB <= kEps) return;
     const float pen = mn(mx(c.normalPenetration.w - cfg.slop, 0.0f), cfg.softMaxCorrection);
     if (pen <= 0.0f) return;
     const f3 mat = xyz(c.material);
     const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
-    const f3 relDisp = (xyz(Bp) - xyz(s.xprev[c.b])) - (xyz(A) - xyz(s.xprev[c.a]));
-    const float denom = iA + iB;
+    const f3 prevA = proxyA ? proxyPreviousPoint(s, c.a, psA.body) : xyz(s.xprev[c.a]);
+    const f3 prevB = proxyB ? proxyPreviousPoint(s, c.b, psB.body) : xyz(s.xprev[c.b]);
+    const f3 relDisp = (curB - prevB) - (curA - prevA);
+    const float nmA = proxyA ? contactEffectiveMass(iA, psA.invI, psA.q, psA.r, n) : iA;
+    const float nmB = proxyB ? contactEffectiveMass(iB, psB.invI, psB.q, psB.r, n) : iB;
+    const float denom = nmA + nmB;
     if (denom <= kEps) return;
     const float lambda = (pen / denom) * cfg.softContactRelaxation;
-    f3 cA = -n * (iA * lambda);
-    f3 cB = n * (iB * lambda);
+    f3 cA{0.f, 0.f, 0.f}, cB{0.f, 0.f, 0.f}, tA{0.f, 0.f, 0.f}, tB{0.f, 0.f, 0.f}, rA{0.f, 0.f, 0.f},
+        rB{0.f, 0.f, 0.f};
+    if (proxyA) {
+        tA = -n * (iA * lambda);
+        rA = -mulWorldInvInertia(psA.invI, psA.q, cross(psA.r, n)) * lambda;
+    } else {
+        cA = -n * (iA * lambda);
+    }
+    if (proxyB) {
+        tB = n * (iB * lambda);
+        rB = mulWorldInvInertia(psB.invI, psB.q, cross(psB.r, n)) * lambda;
+    } else {
+        cB = n * (iB * lambda);
+    }
     const f3 fd = positionFrictionDelta(projectOntoTangent(relDisp, n), pen, mat.x, mat.z,
                                         cfg.positionFrictionMinDistance);
     const float fdist = length(fd);
     if (fdist > 0.0f) {
         const f3 t = fd / fdist;
-        const float tden = iA + iB;
+        const float tmA = proxyA ? contactEffectiveMass(iA, psA.invI, psA.q, psA.r, t) : iA;
+        const float tmB = proxyB ? contactEffectiveMass(iB, psB.invI, psB.q, psB.r, t) : iB;
+        const float tden = tmA + tmB;
         if (tden > kEps) {
             const float tl = (fdist / tden) * cfg.softContactRelaxation;
-            cA += t * (iA * tl);
-            cB -= t * (iB * tl);
+            if (proxyA) {
+                tA += t * (iA * tl);
+                rA += mulWorldInvInertia(psA.invI, psA.q, cross(psA.r, t)) * tl;
+            } else {
+                cA += t * (iA * tl);
+            }
+            if (proxyB) {
+                tB -= t * (iB * tl);
+                rB -= mulWorldInvInertia(psB.invI, psB.q, cross(psB.r, t)) * tl;
+            } else {
+                cB -= t * (iB * tl);
+            }
         }
     }
-    if (iA > kEps) {
-        atomicAdd(&s.posCorr[c.a].x, cA.x);
-        atomicAdd(&s.posCorr[c.a].y, cA.y);
-        atomicAdd(&s.posCorr[c.a].z, cA.z);
+    if (!proxyA && iA > kEps) atomicAdd3(&s.posCorr[c.a], cA);
+    if (!proxyB && iB > kEps) atomicAdd3(&s.posCorr[c.b], cB);
+    if (proxyA && iA > kEps) {
+        atomicAdd3(&s.bodyTransCorr[psA.body], tA);
+        atomicAdd3(&s.bodyRotCorr[psA.body], rA);
     }
-    if (iB > kEps) {
-        atomicAdd(&s.posCorr[c.b].x, cB.x);
-        atomicAdd(&s.posCorr[c.b].y, cB.y);
-        atomicAdd(&s.posCorr[c.b].z, cB.z);
+    if (proxyB && iB > kEps) {
+        atomicAdd3(&s.bodyTransCorr[psB.body], tB);
+        atomicAdd3(&s.bodyRotCorr[psB.body], rB);
     }
 }
 
@@ -1670,13 +1748,6 @@ __device__ __forceinline__ ContactCorrection solveRigidContact(const Scene &s, c
         out.rigid = true;
     }
     return out;
-}
-
-__device__ __forceinline__ void atomicAdd3(float4 *p, f3 v)
-{
-    atomicAdd(&p->x, v.x);
-    atomicAdd(&p->y, v.y);
-    atomicAdd(&p->z, v.z);
 }
 
 // Generate + solve every candidate pair of particle i (pairs are particle-major), then either
@@ -1994,20 +2065,38 @@ __global__ void k_applyRigidContactVelocities(Scene s, Config cfg)
     s.bodyAngVelCorr[b] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
-// physics_particle_solve_contact_velocities.cs.hlsl (non-proxy) with float atomics.
+// physics_particle_solve_contact_velocities.cs.hlsl with float atomics: a rigid proxy moves with
+// its body's velocity at the proxy's lever arm, and its impulse share goes to the body's
+// velocity sums.
 __global__ void __launch_bounds__(kThreads) k_particleContactVelocities(Scene s, Config cfg)
 {
     const uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x;
     if (pi >= s.meta_->particlePairCount) return;
     const ParticleContact c = s.particleContacts[pi];
     if (c.active == 0u) return;
-    const float iA = s.x[c.a].w, iB = s.x[c.b].w;
+    float iA = s.x[c.a].w, iB = s.x[c.b].w;
+    f3 vA = xyz(s.v[c.a]), vB = xyz(s.v[c.b]);
+    const bool proxyA = c.a < s.nProxy, proxyB = c.b < s.nProxy;
+    ProxySide psA{}, psB{};
+    if (proxyA) {
+        f3 cur;
+        loadProxySide(s, c.a, psA, iA, cur);
+        psA.r = qRotate(psA.q, xyz(s.proxyLocal[c.a]));
+        vA = xyz(s.predBodyLin[psA.body]) + cross(xyz(s.predBodyAng[psA.body]), psA.r);
+    }
+    if (proxyB) {
+        f3 cur;
+        loadProxySide(s, c.b, psB, iB, cur);
+        psB.r = qRotate(psB.q, xyz(s.proxyLocal[c.b]));
+        vB = xyz(s.predBodyLin[psB.body]) + cross(xyz(s.predBodyAng[psB.body]), psB.r);
+    }
     if (iA <= kEps && iB <= kEps) return;
-    const f3 vA = xyz(s.v[c.a]), vB = xyz(s.v[c.b]);
     const f3 n = safeNormalize(xyz(c.normalPenetration), f3{0.f, 1.f, 0.f});
     const float nv = dot(vB - vA, n);
     if (nv >= 0.0f) return;
-    const float denom = iA + iB;
+    const float nmA = proxyA ? contactEffectiveMass(iA, psA.invI, psA.q, psA.r, n) : iA;
+    const float nmB = proxyB ? contactEffectiveMass(iB, psB.invI, psB.q, psB.r, n) : iB;
+    const float denom = nmA + nmB;
     if (denom <= kEps) return;
     const f3 mat = xyz(c.material);
     const bool er = (-nv > cfg.restitutionVelocityThreshold) && (c.normalPenetration.w <= cfg.restitutionPenetrationThreshold);
@@ -2015,17 +2104,15 @@ __global__ void __launch_bounds__(kThreads) k_particleContactVelocities(Scene s,
     const float dnv = er ? (-rest * nv) : 0.0f;
     const float imp = mx(0.0f, (dnv - nv) / denom);
     const f3 ti = n * imp;
-    if (iA > kEps) {
-        const f3 d = -ti * iA;
-        atomicAdd(&s.velCorr[c.a].x, d.x);
-        atomicAdd(&s.velCorr[c.a].y, d.y);
-        atomicAdd(&s.velCorr[c.a].z, d.z);
+    if (!proxyA && iA > kEps) atomicAdd3(&s.velCorr[c.a], -ti * iA);
+    if (!proxyB && iB > kEps) atomicAdd3(&s.velCorr[c.b], ti * iB);
+    if (proxyA && iA > kEps) {
+        atomicAdd3(&s.bodyLinVelCorr[psA.body], -ti * iA);
+        atomicAdd3(&s.bodyAngVelCorr[psA.body], mulWorldInvInertia(psA.invI, psA.q, cross(psA.r, -ti)));
     }
-    if (iB > kEps) {
-        const f3 d = ti * iB;
-        atomicAdd(&s.velCorr[c.b].x, d.x);
-        atomicAdd(&s.velCorr[c.b].y, d.y);
-        atomicAdd(&s.velCorr[c.b].z, d.z);
+    if (proxyB && iB > kEps) {
+        atomicAdd3(&s.bodyLinVelCorr[psB.body], ti * iB);
+        atomicAdd3(&s.bodyAngVelCorr[psB.body], mulWorldInvInertia(psB.invI, psB.q, cross(psB.r, ti)));
     }
 }
 
@@ -2398,7 +2485,22 @@ void launchParticleContactVelocities(const Scene &s, uint32_t iterations, const 
     for (uint32_t it = 0; it < iterations; ++it) {
         k_particleContactVelocities<<<blocksFor(s.particlePairCapacity), kThreads, 0, st>>>(s, c);
         k_applyContactVelocities<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+        // the bodies' sums (only proxies of dynamic bodies add to them)
+        if (s.hasDynamic && s.nProxy) k_applyRigidContactVelocities<<<blocksFor(s.B), kThreads, 0, st>>>(s, c);
     }
+}
+
+// physics_particle_sync_rigid_proxy_particles.cs.hlsl after the bodies' corrections
+__global__ void __launch_bounds__(kThreads) k_syncRigidProxies(Scene s)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= s.nProxy) return;
+    s.x[i] = mk4(proxyWorldPosition(s, i), s.x[i].w);
+}
+
+void launchSyncRigidProxies(const Scene &s, cudaStream_t st)
+{
+    if (s.nProxy) k_syncRigidProxies<<<blocksFor(s.nProxy), kThreads, 0, st>>>(s);
 }
 
 void launchSurfaceRender(const Scene &s, cudaStream_t st)

@@ -889,6 +889,85 @@ __global__ void k_rigidNarrowPhase(Scene s, Config cfg)
     write(0u, safeNormalize(n, f3{0.f, 1.f, 0.f}), pen, pa, pb);
 }
 
+// physics_rigid_generate_proxy_contacts.cs.hlsl: proxy candidate k (a proxy particle of body A
+// and a candidate body B) fills contact slot pairSlots + k with the deepest contact between the
+// proxy sphere and B's enabled colliders (collider frames without the body scale, as
+// ComposeColliderWorldPosition), or leaves it inactive.  Proxy particles lead the particle order
+// and candidates are emitted particle by particle, so the proxies' candidates open the list; a
+// slot per candidate keeps the contact order deterministic (the reference appends hits with an
+// atomic counter).
+__global__ void k_proxyRigidContacts(Scene s)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t last = s.nProxy - 1u;
+    const uint32_t proxyCands = min(s.meta_->rigidPairCount, s.candOffset[last] + s.candCount[last]);
+    const uint32_t used = min(proxyCands, s.proxyCapacity);
+    const uint32_t base = kRigidPairContacts * s.meta_->rigidRigidPairCount;
+    if (k == 0) {
+        s.meta_->requiredProxyContacts = proxyCands;
+        s.meta_->proxyContactSlots = used;
+        s.meta_->rigidContactSlots = base + used;
+    }
+    if (k >= used) return;
+    RigidPairContact out{};
+    const uint2 pr = s.rigidPairs[k];
+    const uint32_t p = pr.x, bB = pr.y;
+    const uint32_t bA = s.ownerIdx[p];
+    const float4 posA = s.predBodyPos[bA], posB = s.predBodyPos[bB];
+    if (p >= s.nProxy || bA == bB || (posA.w <= kEps && posB.w <= kEps)) {
+        s.rrContacts[base + k] = out;
+        return;
+    }
+    const f3 sc = xyz(s.x[p]);
+    const float sr = s.radii[p];
+    const float4 qA = qNormalize(s.predBodyRot[bA]), qB = qNormalize(s.predBodyRot[bB]);
+    const float4 scB = s.bodyScale[bB];
+    const float4 proxyMat = s.bodyProxyMat[bA];
+    const uint2 cr = s.bodyColRanges[bB];
+    float best = 0.0f;
+    f3 bestN{0.f, 1.f, 0.f}, bestA{0.f, 0.f, 0.f}, bestB{0.f, 0.f, 0.f}, bestMat{0.f, 0.f, 0.f};
+    for (uint32_t i = 0; i < kColliderIterationCap; ++i) {
+        if (i >= cr.y) break;
+        const uint32_t c = s.bodyColIdx[cr.x + i];
+        const cn_collider_broadphase bp = s.colBp[c];
+        if (bp.enabled_flag == 0u) continue;
+        const cn_collider_geometry g = s.colGeo[c];
+        const f3 cwp = xyz(posB) + qRotate(qB, f3{g.local_position[0], g.local_position[1], g.local_position[2]});
+        const float4 cwq = qNormalize(qMul(qB, qNormalize(make_float4(g.local_orientation[0], g.local_orientation[1],
+                                                                     g.local_orientation[2], g.local_orientation[3]))));
+        const float4 prm = colliderParams(g);
+        f3 n, pa, pb;
+        float pen = 0.0f;
+        bool hit;
+        if (bp.shape_type == CN_COLLIDER_SPHERE) {
+            hit = sphereSphere(sc, sr, cwp, sphereRadius(prm, scB), n, pa, pb, pen);
+        } else if (bp.shape_type == CN_COLLIDER_BOX) {
+            hit = sphereBox(sc, sr, cwp, cwq, boxHalfExtents(prm, scB), n, pa, pb, pen);
+        } else {
+            f3 ca, cb;
+            float capR = 0.0f;
+            capsuleSegment(cwp, cwq, prm, scB, ca, cb, capR);
+            hit = sphereCapsule(sc, sr, ca, cb, capR, n, pa, pb, pen);
+        }
+        if (!hit || pen <= best) continue;
+        best = pen;
+        bestN = safeNormalize(n, f3{0.f, 1.f, 0.f});
+        bestA = pa;
+        bestB = pb;
+        bestMat = combineContactMaterial(proxyMat, s.colMat[c]);
+    }
+    if (best > 0.0f) {
+        out.bodyA = bA;
+        out.bodyB = bB;
+        out.active = 1u;
+        out.normalPenetration = mk4(bestN, best);
+        out.localPointA = mk4(qInvRotate(qA, bestA - xyz(posA)), 0.0f);
+        out.localPointB = mk4(qInvRotate(qB, bestB - xyz(posB)), 0.0f);
+        out.material = mk4(bestMat, 0.0f);
+    }
+    s.rrContacts[base + k] = out;
+}
+
 // ------------------------------------------------------------------------- velocity groups
 // Sort key of a contact: its canonical body pair (inactive contacts last).
 __global__ void k_rigidGroupKeys(Scene s)
@@ -903,7 +982,7 @@ __global__ void k_rigidGroupKeys(Scene s)
 __global__ void k_rigidGroupHeads(Scene s)
 {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= s.rrCapacity * kRigidPairContacts) return;
+    if (j >= s.rrSlotCapacity) return;
     const uint32_t n = s.meta_->rigidContactSlots;
     const uint32_t key = j < n ? s.rrKeyA[j] : 0xffffffffu;
     s.rrHead[j] = (j < n && key != 0xffffffffu && (j == 0u || s.rrKeyA[j - 1] != key)) ? 1u : 0u;
@@ -1141,8 +1220,8 @@ size_t rigidScratchBytes(uint32_t colliders, uint32_t pairs)
 void launchRigidBroadphaseAndContacts(const Scene &s, const Config &c, void *scratch, cudaStream_t st)
 {
     const uint32_t n = s.colQueryCount;
-    if (n == 0 || s.activeMovingCount == 0) {
-        cudaMemsetAsync(&s.meta_->rigidRigidPairCount, 0, 4 * sizeof(uint32_t), st);
+    if (n < 2 || s.activeMovingCount == 0 || s.rrCapacity == 0) { // no collider pairs: proxy contacts alone
+        cudaMemsetAsync(&s.meta_->rigidRigidPairCount, 0, 6 * sizeof(uint32_t), st);
         return;
     }
     uint32_t *total = static_cast<uint32_t *>(scratch);
@@ -1161,12 +1240,18 @@ void launchRigidBroadphaseAndContacts(const Scene &s, const Config &c, void *scr
     k_rigidNarrowPhase<<<blocksOf(s.rrCapacity), kRigidThreads, 0, st>>>(s, c);
 }
 
+void launchProxyRigidContacts(const Scene &s, cudaStream_t st)
+{
+    if (s.proxyCapacity == 0 || s.nProxy == 0) return;
+    k_proxyRigidContacts<<<blocksOf(s.proxyCapacity), kRigidThreads, 0, st>>>(s);
+}
+
 void launchRigidVelocityInit(const Scene &s, const Config &c, void *scratch, cudaStream_t st)
 {
-    if (s.rrCapacity == 0) return;
+    if (s.rrSlotCapacity == 0) return;
     uint32_t *total = static_cast<uint32_t *>(scratch);
     void *work = static_cast<uint8_t *>(scratch) + 256;
-    const uint32_t slots = s.rrCapacity * kRigidPairContacts;
+    const uint32_t slots = s.rrSlotCapacity;
     k_rigidGroupKeys<<<blocksOf(slots), kRigidThreads, 0, st>>>(s);
     radixSortPairs(s.rrKeyA, s.rrValA, s.rrKeyB, s.rrValB, slots, work, &s.meta_->waitTimeouts, st,
                    &s.meta_->rigidContactSlots);
@@ -1177,8 +1262,8 @@ void launchRigidVelocityInit(const Scene &s, const Config &c, void *scratch, cud
 
 void launchRigidDepenetration(const Scene &s, const Config &c, cudaStream_t st)
 {
-    if (s.rrCapacity == 0) return;
-    k_rigidDepenetrate<<<blocksOf(s.rrCapacity * kRigidPairContacts), kRigidThreads, 0, st>>>(s, c);
+    if (s.rrSlotCapacity == 0) return;
+    k_rigidDepenetrate<<<blocksOf(s.rrSlotCapacity), kRigidThreads, 0, st>>>(s, c);
 }
 
 void launchRigidContactVelocitySolve(const Scene &s, const Config &c, uint32_t iterations, uint32_t contactIterations,
@@ -1186,8 +1271,8 @@ void launchRigidContactVelocitySolve(const Scene &s, const Config &c, uint32_t i
 {
     if (s.B == 0) return;
     for (uint32_t it = 0; it < iterations; ++it) {
-        if (it < contactIterations && s.rrCapacity)
-            k_rigidSolveVelocities<<<blocksOf(s.rrCapacity * kRigidPairContacts), kRigidThreads, 0, st>>>(s, c);
+        if (it < contactIterations && s.rrSlotCapacity)
+            k_rigidSolveVelocities<<<blocksOf(s.rrSlotCapacity), kRigidThreads, 0, st>>>(s, c);
         k_rigidApplyVelocityCorrections<<<blocksOf(s.B), kRigidThreads, 0, st>>>(s, c);
     }
 }

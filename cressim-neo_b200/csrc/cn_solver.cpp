@@ -49,6 +49,8 @@ struct cn_solver {
     float *hostX = nullptr, *hostV = nullptr;
     bool synced = false;
     bool hasFluid = false, ppPossible = false, rigidPossible = false, hasBroadphase = false, hasDynamic = false;
+    uint32_t nProxy = 0;          // rigid proxy particles (the leading particles)
+    bool proxyContacts = false;   // proxy particle -> collider contacts in the rigid contact solve
     uint32_t substeps = 1, fluidIt = 1, softIt = 1, contactIt = 1, maxIt = 1, jointIt = 1, rrIt = 1;
     bool rigidRigid = false;       // dynamic bodies among >= 2 colliders: rigid-rigid contacts
     void *rigidScratch = nullptr;
@@ -185,17 +187,24 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
     s.predBodyPos = a.take<float4>(B); s.predBodyRot = a.take<float4>(B);
     s.predBodyLin = a.take<float4>(B); s.predBodyAng = a.take<float4>(B);
     s.colAabbMin = a.take<float4>(C); s.colAabbMax = a.take<float4>(C);
+    s.nProxy = sv->nProxy;
+    s.proxyLocal = a.take<float4>(sv->nProxy);
+    s.bodyProxyMat = a.take<float4>(sv->nProxy ? B : 0u);
     s.hasDynamic = sv->hasDynamic ? 1u : 0u;
     if (sv->hasDynamic) {
         s.bodyTransCorr = a.take<float4>(B); s.bodyRotCorr = a.take<float4>(B);
         s.bodyLinVelCorr = a.take<float4>(B); s.bodyAngVelCorr = a.take<float4>(B);
     }
     s.rrCapacity = 0;
+    s.proxyCapacity = 0;
+    s.rrSlotCapacity = 0;
     if (sv->rigidRigid) {
         const uint32_t P = std::max<uint32_t>(64u, 16u * C);
         s.rrCapacity = P;
+        s.proxyCapacity = sv->proxyContacts ? std::max<uint32_t>(64u, 4u * sv->nProxy) : 0u;
         s.rrCount = a.take<uint32_t>(C); s.rrOffset = a.take<uint32_t>(C);
-        const uint32_t K = P * cn::kRigidPairContacts;
+        const uint32_t K = P * cn::kRigidPairContacts + s.proxyCapacity;
+        s.rrSlotCapacity = K;
         s.rrPairs = a.take<uint2>(P);
         s.rrContacts = a.take<cn::RigidPairContact>(K);
         s.rrSlots = a.take<cn::RigidSlot>(K);
@@ -276,7 +285,7 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
         s.nbr = a.take<uint32_t>(std::max<size_t>(size_t(N) * s.maxNbr, 1));
         s.nbrCount = a.take<uint32_t>(N);
     }
-    if (sv->rigidPossible) {
+    if (sv->rigidPossible || sv->proxyContacts) {
         s.candCount = a.take<uint32_t>(N);
         s.candOffset = a.take<uint32_t>(N);
         s.rigidPairCapacity = std::max<uint32_t>(N * 8u, 64u);
@@ -379,8 +388,10 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
         }
         if (sv->ppPossible)
             probe(sv, "particle_candidates", st, [&] { cn::launchParticleCandidates(s, sv->scanScratch, sv->scanScratchBytes, st); });
-        if (sv->rigidPossible)
+        if (sv->rigidPossible || sv->proxyContacts)
             probe(sv, "rigid_candidates", st, [&] { cn::launchRigidCandidates(s, sv->scanScratch, sv->scanScratchBytes, st); });
+        // generateProxyRigidContacts (physics_solver.cpp:722-727)
+        if (sv->proxyContacts) cn::launchProxyRigidContacts(s, st);
         // initRigidContactVelocities (physics_solver.cpp:736-743)
         if (sv->rigidRigid) cn::launchRigidVelocityInit(s, c, sv->rigidScratch, st);
         // clearSoftConstraintState (physics_clear_soft_constraint_state.cs.hlsl:14-54)
@@ -424,7 +435,10 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             if (runRigidRigid) probe(sv, "rigid_depenetration", st, [&] { cn::launchRigidDepenetration(s, c, st); });
             // applyRigidCorrections (physics_solver.cpp:1170-1177); with only static and kinematic
             // bodies the summed corrections are zero and the pass is left out
-            if ((runRigid || runRigidRigid) && s.hasDynamic) cn::launchApplyRigidCorrections(s, c, st);
+            if ((runRigid || runRigidRigid) && s.hasDynamic) {
+                cn::launchApplyRigidCorrections(s, c, st);
+                cn::launchSyncRigidProxies(s, st); // syncRigidProxyParticles (physics_solver.cpp:1178-1186)
+            }
         }
         // updateRigidVelocities (physics_solver.cpp:1241-1246): for static and kinematic bodies it
         // restates what the rigid predict wrote, so it runs for scenes with dynamic bodies
@@ -628,9 +642,28 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     }
 
     // Collider query order: moving (kinematic, dynamic) colliders, then static, ascending index.
+    // Rigid proxy particles: PhysicsWorld packs them before every other particle
+    // (physics_world.cpp:4931-5023), which the passes rely on.
+    uint32_t nProxy = 0;
+    while (nProxy < N && w->owner_types[nProxy] == CN_OWNER_RIGID_BODY) ++nProxy;
+    for (uint32_t i = nProxy; i < N; ++i)
+        if (w->owner_types[i] == CN_OWNER_RIGID_BODY)
+            return setError(CN_ERR_UNSUPPORTED, "rigid proxy particles must lead the particle order");
+    if (nProxy) {
+        if (!w->rigid_proxy_local_positions || !w->body_proxy_contact_materials)
+            return setError(CN_ERR_INVALID_ARGUMENT, "rigid proxy particles without local positions or materials");
+        for (uint32_t i = 0; i < nProxy; ++i)
+            if (w->owner_indices[i] >= w->rigid_body_count)
+                return setError(CN_ERR_INVALID_ARGUMENT, "rigid proxy particle of a body out of range");
+    }
+    sv->nProxy = nProxy;
+
     std::vector<uint32_t> order;
     const uint32_t moving = cn::colliderQueryOrder(*w, order);
-    sv->rigidRigid = anyDynamic && rrIt > 0 && order.size() >= 2 && moving > 0;
+    // useInitialRigidContactSolve (physics_solver.cpp:512-514) for scenes where a body can move:
+    // collider pairs of the rigid broadphase, or proxy particles against colliders
+    sv->rigidRigid = anyDynamic && rrIt > 0 && ((order.size() >= 2 && moving > 0) || (nProxy > 0 && w->collider_count > 0));
+    sv->proxyContacts = sv->rigidRigid && nProxy > 0 && w->collider_count > 0;
     if (sv->rigidRigid && uint64_t(w->rigid_body_count) * w->rigid_body_count >= 0xffffffffull)
         return setError(CN_ERR_UNSUPPORTED, "more than 65535 rigid bodies in a scene with dynamic bodies");
     if (anyFluid && order.size() > cn::kMaxBoundaryColliders)
@@ -742,6 +775,10 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     CN_CUDA(up(s.colBp, w->collider_broadphase, s.C, st));
     CN_CUDA(up(s.colMat, w->collider_materials, s.C, st));
     CN_CUDA(up(s.colQueryOrder, order.data(), order.size(), st));
+    if (nProxy) {
+        CN_CUDA(up(s.proxyLocal, w->rigid_proxy_local_positions, nProxy, st));
+        CN_CUDA(up(s.bodyProxyMat, w->body_proxy_contact_materials, s.B, st));
+    }
     {
         const cn_status r = uploadSurfaceRender(sv, *w, st);
         if (r != CN_OK) return r;
@@ -804,9 +841,13 @@ CN_API cn_status cn_solver_validate_meta(cn_solver *sv, cn_meta *out)
     out->rigid_rigid_candidate_count = m.rigidRigidPairCount;
     out->required_rigid_rigid_candidate_count = m.requiredRigidRigidPairs;
     out->rigid_rigid_candidate_overflow = m.requiredRigidRigidPairs > sv->s.rrCapacity ? 1u : 0u;
+    out->proxy_rigid_contact_count = m.proxyContactSlots;
+    out->required_proxy_rigid_contact_count = m.requiredProxyContacts;
+    out->proxy_rigid_contact_overflow = m.requiredProxyContacts > sv->s.proxyCapacity ? 1u : 0u;
     if (m.waitTimeouts) return setError(CN_ERR_DEVICE_TIMEOUT, "a bounded device wait gave up (sort look-back)");
     if (out->particle_rigid_candidate_overflow || out->particle_particle_candidate_overflow ||
-        out->fluid_boundary_candidate_overflow || out->rigid_rigid_candidate_overflow)
+        out->fluid_boundary_candidate_overflow || out->rigid_rigid_candidate_overflow ||
+        out->proxy_rigid_contact_overflow)
         return setError(CN_ERR_CAPACITY, "candidate buffer overflow");
     return CN_OK;
 }
@@ -975,6 +1016,11 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
             return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: more materials than synced; use cn_solver_sync_world");
         CN_CUDA(up(s.contactMaterials, w->contact_materials, w->contact_material_count, st));
         CN_CUDA(up(s.fluidMaterials, w->fluid_materials, w->fluid_material_count, st));
+        if (s.nProxy) {
+            if (!w->rigid_proxy_local_positions)
+                return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: rigid proxy local positions missing");
+            CN_CUDA(up(s.proxyLocal, w->rigid_proxy_local_positions, s.nProxy, st));
+        }
     }
     if (flags & CN_SYNC_CONSTRAINTS) {
         // records only: incidence tables depend on the particle indices, which must not change
@@ -995,6 +1041,11 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
         CN_CUDA(up(s.bodyKinPos, w->body_kinematic_target_positions, s.B, st));
         CN_CUDA(up(s.bodyKinRot, w->body_kinematic_target_orientations, s.B, st));
         CN_CUDA(up(s.bodyKinFlags, w->body_kinematic_target_flags, s.B, st));
+        if (s.nProxy) {
+            if (!w->body_proxy_contact_materials)
+                return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: proxy contact materials missing");
+            CN_CUDA(up(s.bodyProxyMat, w->body_proxy_contact_materials, s.B, st));
+        }
     }
     if (flags & CN_SYNC_COLLIDERS) {
         CN_CUDA(up(s.colGeo, w->collider_geometry, s.C, st));

@@ -156,6 +156,10 @@ struct Cloth {
     std::vector<Hinge> hinges;
     std::vector<std::vector<uint32_t>> adjacency;
 };
+struct RigidProxies {
+    cn_rigid_proxy_desc desc;
+    std::vector<v3> local;            // body frame, before the body scale
+};
 struct Strand {
     cn_strand_desc desc;
     std::vector<uint32_t> staticIdx;
@@ -174,9 +178,10 @@ struct cn_world {
     std::vector<Fluid> fluids;
     std::vector<cn_rigid_body_desc> bodies;
     std::vector<cn_collider_desc> colliders;
+    std::vector<RigidProxies> proxies;  // at most one set per body
     // packed SoA storage
     std::vector<float> x, v, radii, contactMaterials, bodyPos, bodyRot, bodyLin, bodyAng, bodyScale,
-        bodyInvI, bodyKinPos, bodyKinRot, colMat, segOrient;
+        bodyInvI, bodyKinPos, bodyKinRot, colMat, segOrient, proxyLocal, bodyProxyMat;
     std::vector<uint32_t> kinds, meta, matIdx, fluidMatIdx, ownerTypes, ownerIdx, adjOff, adjCnt, adjIdx,
         bodyTypes, bodyKinFlags, bodyColRanges, bodyColIdx;
     std::vector<cn_fluid_material> fluidMaterials;
@@ -830,6 +835,36 @@ cn_status pack(cn_world &w)
     const uint32_t clothBase = uint32_t(w.softBodies.size());
     const uint32_t strandBase = clothBase + uint32_t(w.cloths.size());
     const uint32_t fluidBase = strandBase + uint32_t(w.strands.size());
+    const uint32_t proxyBase = fluidBase + uint32_t(w.fluids.size());
+
+    // Rigid proxy particles first, bodies in index order (physics_world.cpp:4931-5023): inverse
+    // mass 0, a phase group of their own per body (no self collision), the scaled local position
+    // kept for the per-substep sync; the body's packed proxy material (zero without proxies).
+    w.proxyLocal.clear();
+    w.bodyProxyMat.assign(w.bodies.size() * 4, 0.0f);
+    for (uint32_t b = 0; b < w.bodies.size(); ++b) {
+        const RigidProxies *rp = nullptr;
+        for (const RigidProxies &r : w.proxies)
+            if (r.desc.body == b) rp = &r;
+        if (!rp || rp->local.empty() || rp->desc.radius <= 0.0f) continue;
+        const cn_rigid_body_desc &bd = w.bodies[b];
+        const cn_contact_material_desc m = normalizeContact(rp->desc.material);
+        const uint32_t mat = findOrAppendContact(w.contactMaterials, m);
+        const float packed[4] = {m.friction, m.restitution, m.damping, m.static_friction};
+        std::memcpy(&w.bodyProxyMat[4 * b], packed, sizeof(packed));
+        const quat q{bd.orientation[0], bd.orientation[1], bd.orientation[2], bd.orientation[3]};
+        const v3 pos{bd.position[0], bd.position[1], bd.position[2]};
+        const uint32_t layer = rp->desc.collision_layer == 0u ? 1u : rp->desc.collision_layer;
+        for (const v3 &l : rp->local) {
+            const v3 scaled{l.x * bd.scale[0], l.y * bd.scale[1], l.z * bd.scale[2]};
+            pushParticle(w, rotate(q, scaled) + pos, 0.0f, rp->desc.radius, CN_PARTICLE_SOLID, rp->desc.environment_index,
+                         packPhase(proxyBase + b, false), layer, rp->desc.collision_mask, mat, 0xffffffffu,
+                         CN_OWNER_RIGID_BODY, b);
+            adjacency.emplace_back();
+            w.proxyLocal.insert(w.proxyLocal.end(), {scaled.x, scaled.y, scaled.z, 0.0f});
+        }
+    }
+    const bool anyProxy = !w.proxyLocal.empty();
 
     std::vector<uint32_t> softOff, clothOff;
     for (uint32_t si = 0; si < w.softBodies.size(); ++si) {
@@ -962,6 +997,8 @@ cn_status pack(cn_world &w)
             adjacency.emplace_back();
         }
     }
+    if (anyProxy) w.proxyLocal.resize(w.radii.size() * 4, 0.0f); // zero for every other particle
+    else w.bodyProxyMat.clear();
     // adjacency CSR
     w.adjOff.assign(adjacency.size(), 0);
     w.adjCnt.assign(adjacency.size(), 0);
@@ -1264,6 +1301,36 @@ CN_API cn_status cn_world_add_collider(cn_world *w, const cn_collider_desc *d, u
     return CN_OK;
 }
 
+CN_API void cn_rigid_proxy_desc_defaults(cn_rigid_proxy_desc *d)
+{
+    if (!d) return;
+    std::memset(d, 0, sizeof(*d));
+    d->material.static_friction = -1.0f;
+    d->collision_layer = 1u;
+    d->collision_mask = 0xffffffffu;
+}
+
+CN_API cn_status cn_world_set_rigid_proxy_particles(cn_world *w, const cn_rigid_proxy_desc *d)
+{
+    if (!w || !d) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_set_rigid_proxy_particles: null argument");
+    if (d->body >= w->bodies.size()) return cn::setError(CN_ERR_INVALID_ARGUMENT, "rigid proxies: body index out of range");
+    if (d->count && !d->local_positions) return cn::setError(CN_ERR_INVALID_ARGUMENT, "rigid proxies: null positions");
+    w->packed = false;
+    RigidProxies rp;
+    rp.desc = *d;
+    rp.desc.local_positions = nullptr;
+    rp.desc.radius = std::max(d->radius, 0.0f);
+    for (uint32_t i = 0; i < d->count; ++i)
+        rp.local.push_back(v3{d->local_positions[3 * i], d->local_positions[3 * i + 1], d->local_positions[3 * i + 2]});
+    for (RigidProxies &r : w->proxies)
+        if (r.desc.body == d->body) {
+            r = std::move(rp);
+            return CN_OK;
+        }
+    w->proxies.push_back(std::move(rp));
+    return CN_OK;
+}
+
 CN_API cn_status cn_world_get_soa(cn_world *w, cn_world_soa *o)
 {
     if (!w || !o) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_get_soa: null argument");
@@ -1330,6 +1397,8 @@ CN_API cn_status cn_world_get_soa(cn_world *w, cn_world_soa *o)
     sd.surface_count = uint32_t(w->sSurf.size() / 2);
     sd.surface_particle_ranges = ptr(w->sSurf);
     o->surface_render = (sd.vertex_count || sd.surface_count) ? &sd : nullptr;
+    o->rigid_proxy_local_positions = w->proxyLocal.empty() ? nullptr : w->proxyLocal.data();
+    o->body_proxy_contact_materials = w->bodyProxyMat.empty() ? nullptr : w->bodyProxyMat.data();
     return CN_OK;
 }
 

@@ -253,6 +253,12 @@ typedef struct cn_world_soa {
 
     /* surface render passes (skinning, normals, bounds); NULL: none */
     const struct cn_surface_render_data *surface_render;
+
+    /* rigid proxy particles (PhysicsWorld packs them first: particles owned by a rigid body,
+     * owner type CN_OWNER_RIGID_BODY, must form the prefix [0, proxies) of the particle order).
+     * NULL when the world has none. */
+    const float *rigid_proxy_local_positions;  /* float4[N]: scaled body-frame position (others 0) */
+    const float *body_proxy_contact_materials; /* float4[B]: the proxies' packed contact material */
 } cn_world_soa;
 
 /* ------------------------------------------------------------------------ */
@@ -366,8 +372,23 @@ CN_API void cn_soft_body_grid_desc_defaults(cn_soft_body_grid_desc *d);
 CN_API void cn_fluid_grid_desc_defaults(cn_fluid_grid_desc *d);
 CN_API void cn_cloth_grid_desc_defaults(cn_cloth_grid_desc *d);
 CN_API void cn_strand_desc_defaults(cn_strand_desc *d);
+/* Proxy collision particles of a rigid body (RigidBodyState proxy fields,
+ * physics_types.h:401-417): spheres of one radius at body-frame points, carried with the body
+ * every substep (physics_particle_sync_rigid_proxy_particles.cs.hlsl).  They collide with
+ * particles (explicit contacts, whose share goes to the body) and with other bodies' colliders
+ * (rigid contacts, physics_rigid_generate_proxy_contacts.cs.hlsl). */
+typedef struct cn_rigid_proxy_desc {
+    uint32_t body;
+    const float *local_positions; uint32_t count;  /* float3[count], body frame before scaling */
+    float radius;                                   /* <= 0: no proxies (the reference skips the body) */
+    cn_contact_material_desc material;
+    uint32_t environment_index;
+    uint32_t collision_layer, collision_mask;       /* 1, 0xffffffff */
+} cn_rigid_proxy_desc;
+
 CN_API void cn_rigid_body_desc_defaults(cn_rigid_body_desc *d);
 CN_API void cn_collider_desc_defaults(cn_collider_desc *d);
+CN_API void cn_rigid_proxy_desc_defaults(cn_rigid_proxy_desc *d);
 
 CN_API cn_status cn_world_create(cn_world **out_world);
 CN_API void cn_world_destroy(cn_world *world);
@@ -393,6 +414,9 @@ CN_API cn_status cn_world_add_cloth_grid(cn_world *w, const cn_cloth_grid_desc *
 CN_API cn_status cn_world_add_strand(cn_world *w, const cn_strand_desc *d, uint32_t *out_index);
 CN_API cn_status cn_world_add_rigid_body(cn_world *w, const cn_rigid_body_desc *d, uint32_t *out_body);
 CN_API cn_status cn_world_add_collider(cn_world *w, const cn_collider_desc *d, uint32_t *out_collider);
+/* Sets (replaces) the proxy particles of body d->body; packed before every soft body, cloth,
+ * strand and fluid particle, bodies in index order (physics_world.cpp:4931-5023). */
+CN_API cn_status cn_world_set_rigid_proxy_particles(cn_world *w, const cn_rigid_proxy_desc *d);
 /* A render mesh bound to a soft body or cloth, as the engine's World builds the surface render
  * data (world.cpp:3255-3554): every soft body and cloth gets a surface particle range (packed
  * [soft bodies][cloths]); the mesh's vertices are bound to the owner's particles -- one matching
@@ -447,7 +471,10 @@ typedef struct cn_meta {
     uint32_t rigid_rigid_candidate_count;        /* collider pairs of the rigid broadphase (GpuBroadPhaseMeta) */
     uint32_t required_rigid_rigid_candidate_count;
     uint32_t rigid_rigid_candidate_overflow;
-    uint32_t reserved[2];
+    uint32_t proxy_rigid_contact_count;          /* proxy particle -> collider contacts (GpuProxyRigidContactMeta) */
+    uint32_t required_proxy_rigid_contact_count;
+    uint32_t proxy_rigid_contact_overflow;
+    uint32_t reserved[1];
 } cn_meta;
 
 /* Non-owning device pointers (reference: PhysicsGpuSceneView,

@@ -346,6 +346,10 @@ struct cno_solver {
     std::vector<std::vector<RigidSlot>> rrGroups;
     std::vector<std::pair<uint32_t, uint32_t>> rrGroupBodies;
     uint32_t requiredRigidRigidPairs = 0;
+    // rigid proxy particles: the leading nProxy particles, carried with their bodies
+    uint32_t nProxy = 0;
+    std::vector<f4> proxyLocal, bodyProxyMat;
+    uint32_t proxyContactSlots = 0, requiredProxyContacts = 0;
     std::vector<uint32_t> colliderQueryOrder; // moving colliders first, then static
     uint32_t activeMovingCount = 0;
     // transient state
@@ -403,6 +407,12 @@ void setupWorld(cno_solver &s, const cn_world_soa &w)
     copyArr(s.fluidMatIdx, w.fluid_material_indices, N);
     copyArr(s.ownerTypes, w.owner_types, N);
     copyArr(s.ownerIdx, w.owner_indices, N);
+    s.nProxy = 0;
+    while (s.nProxy < N && s.ownerTypes[s.nProxy] == CN_OWNER_RIGID_BODY) ++s.nProxy;
+    if (s.nProxy) {
+        copyArr(s.proxyLocal, w.rigid_proxy_local_positions, s.nProxy);
+        copyArr(s.bodyProxyMat, w.body_proxy_contact_materials, w.rigid_body_count);
+    }
     copyArr(s.adjOff, w.adjacency_offsets, N);
     copyArr(s.adjCnt, w.adjacency_counts, N);
     copyArr(s.adjIdx, w.adjacency_indices, w.adjacency_index_count);
@@ -706,6 +716,17 @@ void predictSoft(cno_solver &s, float dt)
         const f3 pp = xyz(pim) + vel * dt;
         s.v[i] = mk4(vel, 0.0f);
         s.x[i] = mk4(pp, pim.w);
+    }
+}
+
+// physics_particle_sync_rigid_proxy_particles.cs.hlsl:13-39: a proxy particle at its body's
+// predicted pose (the inverse mass kept)
+void syncRigidProxies(cno_solver &s)
+{
+    for (uint32_t i = 0; i < s.nProxy; ++i) {
+        const uint32_t b = s.ownerIdx[i];
+        const f4 q = QNormalize(s.predBodyRot[b]);
+        s.x[i] = mk4(xyz(s.predBodyPos[b]) + QRotate(q, xyz(s.proxyLocal[i])), s.x[i].w);
     }
 }
 
@@ -1615,20 +1636,54 @@ void particleParticleContacts(cno_solver &s)
     const float relax = s.desc.contact.soft_relaxation;
     const float maxCorr = s.desc.contact.soft_max_correction_per_iteration;
     const float minFric = s.desc.contact.position_friction_min_distance;
-    for (const ParticleContact &c : s.activeParticleContacts) { // float atomics in contact order
+    // physics_particle_solve_explicit_contacts.cs.hlsl:27-238 (float atomics in contact order);
+    // a rigid proxy's share goes to its body
+    for (const ParticleContact &c : s.activeParticleContacts) {
         const f4 A = s.x[c.a], Bp = s.x[c.b];
-        const float iA = A.w, iB = Bp.w;
+        const bool proxyA = c.a < s.nProxy, proxyB = c.b < s.nProxy;
+        float iA = A.w, iB = Bp.w;
+        f3 curA = xyz(A), curB = xyz(Bp), prevA = xyz(s.xprev[c.a]), prevB = xyz(s.xprev[c.b]);
+        f3 rA{0, 0, 0}, rB{0, 0, 0}, inA{0, 0, 0}, inB{0, 0, 0};
+        f4 qA{0, 0, 0, 1}, qB{0, 0, 0, 1};
+        uint32_t bA = 0, bB = 0;
+        auto proxySide = [&](uint32_t p, uint32_t &b, float &im, f3 &inv, f4 &q, f3 &cur, f3 &prev, f3 &r) {
+            b = s.ownerIdx[p];
+            const f4 bp = s.predBodyPos[b];
+            q = QNormalize(s.predBodyRot[b]);
+            const f4 pq = QNormalize(s.prevBodyRot[b]);
+            im = s.bodyType[b] == CN_BODY_DYNAMIC ? bp.w : 0.0f;
+            inv = im > kEps ? xyz(s.bodyInvInertia[b]) : f3{0, 0, 0};
+            const f3 l = xyz(s.proxyLocal[p]);
+            cur = xyz(bp) + QRotate(q, l);
+            prev = xyz(s.prevBodyPos[b]) + QRotate(pq, l);
+            r = cur - xyz(bp);
+        };
+        if (proxyA) proxySide(c.a, bA, iA, inA, qA, curA, prevA, rA);
+        if (proxyB) proxySide(c.b, bB, iB, inB, qB, curB, prevB, rB);
         if (iA <= kEps && iB <= kEps) continue;
         const float pen = std::min(std::max(c.normalPenetration.w - s.slop(), 0.0f), maxCorr);
         if (pen <= 0.0f) continue;
         const f3 mat = xyz(c.material);
         const f3 n = SafeNormalize(xyz(c.normalPenetration), f3{0, 1, 0});
-        const f3 relDisp = (xyz(Bp) - xyz(s.xprev[c.b])) - (xyz(A) - xyz(s.xprev[c.a]));
-        const float denom = iA + iB;
+        const f3 relDisp = (curB - prevB) - (curA - prevA);
+        const float nmA = proxyA ? ContactEffectiveMass(iA, inA, qA, rA, n) : iA;
+        const float nmB = proxyB ? ContactEffectiveMass(iB, inB, qB, rB, n) : iB;
+        const float denom = nmA + nmB;
         if (denom <= kEps) continue;
         const float lambda = (pen / denom) * relax;
-        f3 cA = -n * (iA * lambda);
-        f3 cB = n * (iB * lambda);
+        f3 cA{0, 0, 0}, cB{0, 0, 0}, tA{0, 0, 0}, tB{0, 0, 0}, wA{0, 0, 0}, wB{0, 0, 0};
+        if (proxyA) {
+            tA = -n * (iA * lambda);
+            wA = -MulWorldInvInertia(inA, qA, cross(rA, n)) * lambda;
+        } else {
+            cA = -n * (iA * lambda);
+        }
+        if (proxyB) {
+            tB = n * (iB * lambda);
+            wB = MulWorldInvInertia(inB, qB, cross(rB, n)) * lambda;
+        } else {
+            cB = n * (iB * lambda);
+        }
         const f3 tdisp = ProjectOntoTangent(relDisp, n);
         // ComputePositionFrictionDelta (physics_rigid_solver_shared.hlsli:50-68)
         f3 fd{0, 0, 0};
@@ -1641,15 +1696,35 @@ void particleParticleContacts(cno_solver &s)
         const float fdist = length(fd);
         if (fdist > 0.0f) {
             const f3 t = fd / fdist;
-            const float tden = iA + iB;
+            const float tmA = proxyA ? ContactEffectiveMass(iA, inA, qA, rA, t) : iA;
+            const float tmB = proxyB ? ContactEffectiveMass(iB, inB, qB, rB, t) : iB;
+            const float tden = tmA + tmB;
             if (tden > kEps) {
                 const float tl = (fdist / tden) * relax;
-                cA += t * (iA * tl);
-                cB -= t * (iB * tl);
+                if (proxyA) {
+                    tA += t * (iA * tl);
+                    wA += MulWorldInvInertia(inA, qA, cross(rA, t)) * tl;
+                } else {
+                    cA += t * (iA * tl);
+                }
+                if (proxyB) {
+                    tB -= t * (iB * tl);
+                    wB -= MulWorldInvInertia(inB, qB, cross(rB, t)) * tl;
+                } else {
+                    cB -= t * (iB * tl);
+                }
             }
         }
-        if (iA > kEps) s.posCorr[c.a] = mk4(xyz(s.posCorr[c.a]) + cA, s.posCorr[c.a].w);
-        if (iB > kEps) s.posCorr[c.b] = mk4(xyz(s.posCorr[c.b]) + cB, s.posCorr[c.b].w);
+        if (!proxyA && iA > kEps) s.posCorr[c.a] = mk4(xyz(s.posCorr[c.a]) + cA, s.posCorr[c.a].w);
+        if (!proxyB && iB > kEps) s.posCorr[c.b] = mk4(xyz(s.posCorr[c.b]) + cB, s.posCorr[c.b].w);
+        if (proxyA && iA > kEps) {
+            s.bodyTransCorr[bA] = s.bodyTransCorr[bA] + tA;
+            s.bodyRotCorr[bA] = s.bodyRotCorr[bA] + wA;
+        }
+        if (proxyB && iB > kEps) {
+            s.bodyTransCorr[bB] = s.bodyTransCorr[bB] + tB;
+            s.bodyRotCorr[bB] = s.bodyRotCorr[bB] + wB;
+        }
     }
 }
 
@@ -2440,6 +2515,75 @@ void rigidPairsAndContacts(cno_solver &s)
     }
 }
 
+// physics_rigid_generate_proxy_contacts.cs.hlsl:30-183: every candidate of a proxy particle
+// (proxies lead the particle order, so their candidates open the list) gets a contact after the
+// pair contacts -- the deepest between the proxy sphere of body A and the candidate body B's
+// enabled colliders, framed without the body scale (ComposeColliderWorldPosition) -- or an
+// inactive one; at most max(64, 4 x proxies) of them.
+void proxyRigidContacts(cno_solver &s)
+{
+    uint32_t proxyCands = 0;
+    while (proxyCands < s.rigidPairs.size() && s.rigidPairs[proxyCands].first < s.nProxy) ++proxyCands;
+    const uint32_t cap = std::max<uint32_t>(64u, 4u * s.nProxy);
+    const uint32_t used = std::min(proxyCands, cap);
+    s.requiredProxyContacts = proxyCands;
+    s.proxyContactSlots = used;
+    for (uint32_t k = 0; k < used; ++k) {
+        cno_solver::RigidPairContact out;
+        const uint32_t p = s.rigidPairs[k].first, bB = s.rigidPairs[k].second;
+        const uint32_t bA = s.ownerIdx[p];
+        const f4 posA = s.predBodyPos[bA], posB = s.predBodyPos[bB];
+        if (bA == bB || (posA.w <= kEps && posB.w <= kEps)) {
+            s.rrContacts.push_back(out);
+            continue;
+        }
+        const f3 sc = xyz(s.x[p]);
+        const float sr = s.radii[p];
+        const f4 qA = QNormalize(s.predBodyRot[bA]), qB = QNormalize(s.predBodyRot[bB]);
+        const f4 scB = s.bodyScale[bB];
+        float best = 0.0f;
+        f3 bestN{0, 1, 0}, bestA{0, 0, 0}, bestB{0, 0, 0}, bestMat{0, 0, 0};
+        const uint32_t off = s.bodyColRanges[2 * bB], cnt = s.bodyColRanges[2 * bB + 1];
+        for (uint32_t i = 0; i < kColliderCap && i < cnt; ++i) {
+            const uint32_t c = s.bodyColIdx[off + i];
+            const cn_collider_broadphase &bp = s.colBp[c];
+            if (bp.enabled_flag == 0u) continue;
+            const cn_collider_geometry &g = s.colGeo[c];
+            const f3 cwp = xyz(posB) + QRotate(qB, f3{g.local_position[0], g.local_position[1], g.local_position[2]});
+            const f4 cwq = QNormalize(QMul(qB, QNormalize(f4{g.local_orientation[0], g.local_orientation[1],
+                                                             g.local_orientation[2], g.local_orientation[3]})));
+            const f4 prm{g.shape_params[0], g.shape_params[1], g.shape_params[2], g.shape_params[3]};
+            f3 n, pa, pb;
+            float pen = 0.0f;
+            bool hit;
+            if (bp.shape_type == CN_COLLIDER_SPHERE) {
+                hit = SphereSphere(sc, sr, cwp, SphereRadius(prm, scB), n, pa, pb, pen);
+            } else if (bp.shape_type == CN_COLLIDER_BOX) {
+                hit = SphereBox(sc, sr, cwp, cwq, BoxHalfExtents(prm, scB), n, pa, pb, pen);
+            } else {
+                f3 ca, cb;
+                float capR = 0.0f;
+                CapsuleSegment(cwp, cwq, prm, scB, ca, cb, capR);
+                hit = SphereCapsule(sc, sr, ca, cb, capR, n, pa, pb, pen);
+            }
+            if (!hit || pen <= best) continue;
+            best = pen;
+            bestN = SafeNormalize(n, f3{0, 1, 0});
+            bestA = pa;
+            bestB = pb;
+            bestMat = CombineContactMaterial(s.bodyProxyMat[bA], s.colMat[c]);
+        }
+        if (best > 0.0f) {
+            out.bodyA = bA; out.bodyB = bB; out.active = true;
+            out.normalPenetration = mk4(bestN, best);
+            out.localA = mk4(QInvRotate(qA, bestA - xyz(posA)), 0.0f);
+            out.localB = mk4(QInvRotate(qB, bestB - xyz(posB)), 0.0f);
+            out.material = mk4(bestMat, 0.0f);
+        }
+        s.rrContacts.push_back(out);
+    }
+}
+
 // physics_rigid_init_contact_velocities.cs.hlsl: canonical contacts grouped by body pair (pair
 // order within a group, at most 16), each with its restitution target.
 void rigidVelocityInit(cno_solver &s)
@@ -2773,14 +2917,32 @@ void particleContactVelocities(cno_solver &s, uint32_t iterations)
     const float rpt = s.desc.contact.restitution_penetration_slop_multiplier * s.slop();
     for (uint32_t it = 0; it < iterations; ++it) {
         for (const ParticleContact &c : s.activeParticleContacts) {
-            const float iA = s.x[c.a].w, iB = s.x[c.b].w;
-            const f3 vA = xyz(s.v[c.a]), vB = xyz(s.v[c.b]);
+            float iA = s.x[c.a].w, iB = s.x[c.b].w;
+            f3 vA = xyz(s.v[c.a]), vB = xyz(s.v[c.b]);
+            const bool proxyA = c.a < s.nProxy, proxyB = c.b < s.nProxy;
+            f3 rA{0, 0, 0}, rB{0, 0, 0}, inA{0, 0, 0}, inB{0, 0, 0};
+            f4 qA{0, 0, 0, 1}, qB{0, 0, 0, 1};
+            uint32_t bA = 0, bB = 0;
+            // a proxy moves with its body (ComputeContactPointVelocity at the proxy's lever arm)
+            auto proxySide = [&](uint32_t p, uint32_t &b, float &im, f3 &inv, f4 &q, f3 &vel, f3 &r) {
+                b = s.ownerIdx[p];
+                const f4 bp = s.predBodyPos[b];
+                q = QNormalize(s.predBodyRot[b]);
+                im = s.bodyType[b] == CN_BODY_DYNAMIC ? bp.w : 0.0f;
+                inv = im > kEps ? xyz(s.bodyInvInertia[b]) : f3{0, 0, 0};
+                r = QRotate(q, xyz(s.proxyLocal[p]));
+                vel = xyz(s.predBodyLin[b]) + cross(xyz(s.predBodyAng[b]), r);
+            };
+            if (proxyA) proxySide(c.a, bA, iA, inA, qA, vA, rA);
+            if (proxyB) proxySide(c.b, bB, iB, inB, qB, vB, rB);
             if (iA <= kEps && iB <= kEps) continue;
             const f3 n = SafeNormalize(xyz(c.normalPenetration), f3{0, 1, 0});
             const f3 rel = vB - vA;
             const float nv = dot(rel, n);
             if (nv >= 0.0f) continue;
-            const float denom = iA + iB;
+            const float nmA = proxyA ? ContactEffectiveMass(iA, inA, qA, rA, n) : iA;
+            const float nmB = proxyB ? ContactEffectiveMass(iB, inB, qB, rB, n) : iB;
+            const float denom = nmA + nmB;
             if (denom <= kEps) continue;
             const f3 mat = xyz(c.material);
             const bool er = (-nv > rvt) && (c.normalPenetration.w <= rpt);
@@ -2788,8 +2950,16 @@ void particleContactVelocities(cno_solver &s, uint32_t iterations)
             const float dnv = er ? (-rest * nv) : 0.0f;
             const float imp = std::max(0.0f, (dnv - nv) / denom);
             const f3 ti = n * imp;
-            if (iA > kEps) s.velCorr[c.a] = mk4(xyz(s.velCorr[c.a]) + (-ti * iA), s.velCorr[c.a].w);
-            if (iB > kEps) s.velCorr[c.b] = mk4(xyz(s.velCorr[c.b]) + ti * iB, s.velCorr[c.b].w);
+            if (!proxyA && iA > kEps) s.velCorr[c.a] = mk4(xyz(s.velCorr[c.a]) + (-ti * iA), s.velCorr[c.a].w);
+            if (!proxyB && iB > kEps) s.velCorr[c.b] = mk4(xyz(s.velCorr[c.b]) + ti * iB, s.velCorr[c.b].w);
+            if (proxyA && iA > kEps) {
+                s.bodyLinVelCorr[bA] = s.bodyLinVelCorr[bA] + (-ti * iA);
+                s.bodyAngVelCorr[bA] = s.bodyAngVelCorr[bA] + MulWorldInvInertia(inA, qA, cross(rA, -ti));
+            }
+            if (proxyB && iB > kEps) {
+                s.bodyLinVelCorr[bB] = s.bodyLinVelCorr[bB] + ti * iB;
+                s.bodyAngVelCorr[bB] = s.bodyAngVelCorr[bB] + MulWorldInvInertia(inB, qB, cross(rB, ti));
+            }
         }
         for (uint32_t i = 0; i < s.N; ++i) {
             f4 vel = s.v[i];
@@ -2799,6 +2969,9 @@ void particleContactVelocities(cno_solver &s, uint32_t iterations)
             s.v[i] = vel;
             s.velCorr[i] = f4{0, 0, 0, 0};
         }
+        // the bodies' sums after every iteration (solveParticleContactVelocities,
+        // physics_pass_dispatcher.cpp:3255-3270); only proxies of dynamic bodies add to them
+        if (s.hasDynamic && s.nProxy) applyRigidContactVelocities(s);
     }
 }
 
@@ -2832,9 +3005,12 @@ void stepFrame(cno_solver &s, float frameDt)
         const bool hasBroadphase = hasSoftSoftContact || hasFluidWork || hasRigidCand;
 
         predictRigid(s, dt);
-        const bool rigidRigid = s.hasDynamic && rrIt > 0 && s.colliderQueryOrder.size() >= 2 && s.activeMovingCount > 0;
+        // useInitialRigidContactSolve (physics_solver.cpp:512-514) where a body can move
+        const bool rigidRigid = s.hasDynamic && rrIt > 0 &&
+                                ((s.colliderQueryOrder.size() >= 2 && s.activeMovingCount > 0) || (s.nProxy > 0 && s.C > 0));
         if (rigidRigid) rigidPairsAndContacts(s);
         predictSoft(s, dt);
+        syncRigidProxies(s);
         if (hasBroadphase) broadphase(s);
         s.particlePairs.clear();
         s.rigidPairs.clear();
@@ -2844,6 +3020,7 @@ void stepFrame(cno_solver &s, float frameDt)
             if (hasRigidCand) buildParticleRigidCandidates(s);
             if (hasFluidWork && s.C > 0) buildFluidBoundaryCandidates(s);
         }
+        if (rigidRigid && s.nProxy > 0 && hasRigidCand) proxyRigidContacts(s);
         if (rigidRigid) rigidVelocityInit(s);
         // clearSoftConstraintState (physics_clear_soft_constraint_state.cs.hlsl:14-54)
         std::fill(s.posCorr.begin(), s.posCorr.end(), f4{0, 0, 0, 0});
@@ -2892,7 +3069,10 @@ void stepFrame(cno_solver &s, float frameDt)
             const bool runRigidRigid = rigidRigid && it < rrIt;
             if (runRigidRigid) rigidDepenetration(s);
             // applyRigidCorrections (physics_solver.cpp:1170-1177); zero sums without dynamic bodies
-            if ((runRigid || runRigidRigid) && s.hasDynamic) applyRigidCorrections(s);
+            if ((runRigid || runRigidRigid) && s.hasDynamic) {
+                applyRigidCorrections(s);
+                syncRigidProxies(s);   // physics_solver.cpp:1178-1186
+            }
         }
         // updateRigidVelocities (physics_solver.cpp:1241-1246); restates the predict without
         // dynamic bodies
@@ -3045,13 +3225,15 @@ CN_API uint32_t cno_meta(cno_solver *s, uint32_t *out, uint32_t n)
     // (required rigid pairs, rigid pair count, required particle pairs, particle pair count,
     //  active rigid contacts, active particle contacts, neighbour-list truncations)
     //  required rigid-rigid collider pairs, rigid-rigid pairs kept)
-    const uint32_t vals[9] = {s->requiredRigidPairs, uint32_t(s->rigidPairs.size()),
-                              s->requiredParticlePairs, uint32_t(s->particlePairs.size()),
-                              uint32_t(s->activeRigidContacts.size()),
-                              uint32_t(s->activeParticleContacts.size()), s->truncations,
-                              s->requiredRigidRigidPairs, uint32_t(s->rrPairs.size())};
-    for (uint32_t i = 0; i < n && i < 9; ++i) out[i] = vals[i];
-    return 9;
+    //  required proxy contact slots, proxy contact slots kept)
+    const uint32_t vals[11] = {s->requiredRigidPairs, uint32_t(s->rigidPairs.size()),
+                               s->requiredParticlePairs, uint32_t(s->particlePairs.size()),
+                               uint32_t(s->activeRigidContacts.size()),
+                               uint32_t(s->activeParticleContacts.size()), s->truncations,
+                               s->requiredRigidRigidPairs, uint32_t(s->rrPairs.size()),
+                               s->requiredProxyContacts, s->proxyContactSlots};
+    for (uint32_t i = 0; i < n && i < 11; ++i) out[i] = vals[i];
+    return 11;
 }
 
 // Host derivations restated for cross-checking the product's authoring code:

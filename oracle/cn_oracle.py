@@ -130,11 +130,11 @@ class Oracle:
         return buf
 
     def meta(self) -> dict:
-        out = (C.c_uint32 * 9)()
-        self._lib.cno_meta(self._h, out, 9)
+        out = (C.c_uint32 * 11)()
+        self._lib.cno_meta(self._h, out, 11)
         keys = ["required_rigid_pairs", "rigid_pairs", "required_particle_pairs", "particle_pairs",
                 "active_rigid_contacts", "active_particle_contacts", "neighbor_truncations",
-                "required_rigid_rigid_pairs", "rigid_rigid_pairs"]
+                "required_rigid_rigid_pairs", "rigid_rigid_pairs", "required_proxy_contacts", "proxy_contacts"]
         return dict(zip(keys, list(out)))
 
 
