@@ -443,8 +443,10 @@ class Solver:
         q = (C.c_float * 4)(*orientation)
         _check(self._lib.cn_solver_set_kinematic_target(self._h, body, p, q))
 
-    def set_debug(self, keep_fluid_delta=False, post_update_neighbors=False, force_broadphase=False) -> None:
-        flags = (1 if keep_fluid_delta else 0) | (2 if post_update_neighbors else 0) | (4 if force_broadphase else 0)
+    def set_debug(self, keep_fluid_delta=False, post_update_neighbors=False, force_broadphase=False,
+                  walk_cells=False) -> None:
+        flags = ((1 if keep_fluid_delta else 0) | (2 if post_update_neighbors else 0) | (4 if force_broadphase else 0)
+                 | (8 if walk_cells else 0))
         _check(self._lib.cn_solver_set_debug(self._h, flags))
 
     def set_timing(self, enable: bool = True) -> None:

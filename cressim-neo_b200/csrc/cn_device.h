@@ -220,6 +220,7 @@ struct Scene {
     float4 *Xs = nullptr;             // x at the sorted slot (w = invMass)
     float4 *P = nullptr;              // x + accumulated delta, w = tag word (fluid bit, material, group)
     float4 *Pb = nullptr;             // second position buffer (odd iterations) when x is fixed over them
+    float4 *P0 = nullptr;             // positions at the superset build when contacts also move fluid x
     float4 *Da = nullptr, *Db = nullptr; // accumulated delta ping-pong
     float4 *Cs = nullptr;             // surface normal xyz, density constraint w
     float4 *Dx = nullptr;             // packed delta + interaction weight (last iteration)
@@ -285,7 +286,8 @@ void launchFluidIteration(const Scene &s, uint32_t iter, float dt, const Config 
 void launchFluidGather(const Scene &s, uint32_t iter, cudaStream_t st);
 // False when the positions are double-buffered: the gather then runs at the first iteration only.
 bool fluidGatherEachIteration(const Scene &s);
-void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter, cudaStream_t st);
+// walkCells: every iteration walks the 27 cells (no superset lists).
+void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter, bool walkCells, cudaStream_t st);
 void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
                                 cudaStream_t st);
 void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st);

@@ -608,10 +608,13 @@ __global__ void __launch_bounds__(kThreads) k_particleCandidates(Scene s, const 
 // Fluid solve (cell order).
 // ------------------------------------------------------------------------------------------
 // Position of this fluid iteration: x + accumulated delta (iteration > 0), in sorted slots.
-// With `P2` (double-buffered positions, see k_fluidDeltaApplyClamp) the first iteration writes
-// both buffers, so the tags of slots the iterations never rewrite are valid in each.
+// With `P2` the first iteration writes a second copy: the other buffer of double-buffered
+// positions (see k_fluidDeltaApplyClamp), so the tags of slots the iterations never rewrite are
+// valid in each, or the superset build positions P0.  With `P0` (later iterations of a scene whose
+// contacts also move fluid x) a particle's move is measured from P0, otherwise it is its
+// accumulated delta.
 __global__ void __launch_bounds__(kThreads) k_fluidGather(Scene s, float4 *Xs, const float4 *Dcur,
-                                                          uint32_t iter, float4 *P2)
+                                                          uint32_t iter, float4 *P2, const float4 *P0)
 {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     float largest = 0.0f;
@@ -620,12 +623,16 @@ __global__ void __launch_bounds__(kThreads) k_fluidGather(Scene s, float4 *Xs, c
         const f3 d = iter > 0 ? xyz(Dcur[slot]) : f3{0.f, 0.f, 0.f};
         const uint32_t info = s.sInfo[slot];
         const uint32_t tag = (info & 0x7fffffffu) | ((info & kFluidBit) && xp.w > kEps ? kFluidBit : 0u);
+        const f3 p = xyz(xp) + d;
         Xs[slot] = xp;
-        s.P[slot] = mk4(xyz(xp) + d, __uint_as_float(tag));
-        if (P2) P2[slot] = mk4(xyz(xp) + d, __uint_as_float(tag));
-        if (info & kFluidBit) largest = sqrtf(dot(d, d));
+        s.P[slot] = mk4(p, __uint_as_float(tag));
+        if (P2) P2[slot] = mk4(p, __uint_as_float(tag));
+        if (info & kFluidBit) {
+            const f3 moved = P0 ? p - xyz(P0[slot]) : d;
+            largest = sqrtf(dot(moved, moved));
+        }
     }
-    // largest accumulated delta of this iteration: validity of the superset lists
+    // largest move of this iteration: validity of the superset lists
     if (s.fluidMaxDelta && iter > 0 && iter < kMaxTrackedIterations) {
         for (int o = 16; o > 0; o >>= 1) largest = fmaxf(largest, __shfl_xor_sync(0xffffffffu, largest, o));
         if ((threadIdx.x & 31) == 0 && largest > 0.0f)
@@ -2351,20 +2358,21 @@ void launchFluidGather(const Scene &s, uint32_t iter, cudaStream_t st)
 {
     if (s.N == 0) return;
     const float4 *Dcur = (iter & 1u) ? s.Db : s.Da;
-    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), s.Xs, Dcur, iter,
-                                                       (s.Pb && iter == 0) ? s.Pb : nullptr);
+    float4 *second = iter == 0 ? (s.Pb ? s.Pb : s.P0) : nullptr;
+    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), s.Xs, Dcur, iter, second,
+                                                       iter > 0 ? s.P0 : nullptr);
 }
 
 bool fluidGatherEachIteration(const Scene &s) { return s.Pb == nullptr; }
 
 bool fluidListsInterleaved() { return kInterleavedLists; }
 
-void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter, cudaStream_t st)
+void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter, bool walkCells, cudaStream_t st)
 {
     if (s.N == 0) return;
     const Scene sp = withPositions(s, iter);
     float4 *Dk = (iter & 1u) ? s.Db : s.Da;
-    if (s.sup == nullptr)
+    if (s.sup == nullptr || walkCells)
         k_fluidNeighborsDensity<0u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter, Dk);
     else if (iter == 0)
         k_fluidNeighborsDensity<1u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter, Dk);
@@ -2387,7 +2395,7 @@ void launchFluidIteration(const Scene &s, uint32_t iter, float dt, const Config 
                           cudaStream_t st)
 {
     if (iter == 0 || fluidGatherEachIteration(s)) launchFluidGather(s, iter, st);
-    launchFluidNeighborsDensity(s, c, iter, st);
+    launchFluidNeighborsDensity(s, c, iter, false, st);
     launchFluidDeltaApplyClamp(s, iter, dt, c, writeDebug, st);
 }
 
@@ -2395,7 +2403,7 @@ void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)
 {
     if (s.N == 0) return;
     // Positions after the velocity update; the accumulated delta was folded into x.
-    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, s.Da, 0u, nullptr);
+    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, s.Da, 0u, nullptr, nullptr);
     Config dummy{};
     k_fluidNeighborsDensity<0u><<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u, nullptr);
 }

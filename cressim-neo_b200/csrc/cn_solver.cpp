@@ -54,7 +54,7 @@ struct cn_solver {
     uint32_t substeps = 1, fluidIt = 1, softIt = 1, contactIt = 1, maxIt = 1, jointIt = 1, rrIt = 1;
     bool rigidRigid = false;       // dynamic bodies among >= 2 colliders: rigid-rigid contacts
     void *rigidScratch = nullptr;
-    bool postUpdateNeighbors = false, writeFluidDebug = false, forceBroadphase = false;
+    bool postUpdateNeighbors = false, writeFluidDebug = false, forceBroadphase = false, walkCells = false;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graphExec = nullptr;
     float graphDt = -1.0f;
@@ -275,12 +275,14 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
         s.runComp = a.take<uint32_t>(N); s.runPos = a.take<uint32_t>(N);
         s.cvals = a.take<uint32_t>(N); s.cCell = a.take<int4>(N); s.cRun = a.take<uint32_t>(N);
         s.fluidMaxDelta = a.take<uint32_t>(64);
-        if (!sv->ppPossible) { // fluid x is fixed during the iterations: superset lists are exact
-            s.supCap = 160u;
-            s.sup = a.take<uint32_t>(size_t(N) * s.supCap);
-            s.supCount = a.take<uint32_t>(N);
-            s.Pb = a.take<float4>(N);
-        }
+        // Superset lists (k_fluidNeighborsDensity modes 1 and 2).  Without particle-particle
+        // contacts fluid x is fixed over the iterations and the positions are double-buffered;
+        // with them the gather records each iteration's largest move from the build positions P0.
+        s.supCap = 160u;
+        s.sup = a.take<uint32_t>(size_t(N) * s.supCap);
+        s.supCount = a.take<uint32_t>(N);
+        if (!sv->ppPossible) s.Pb = a.take<float4>(N);
+        else s.P0 = a.take<float4>(N);
         s.maxNbr = sv->desc.max_fluid_neighborhood;
         s.nbr = a.take<uint32_t>(std::max<size_t>(size_t(N) * s.maxNbr, 1));
         s.nbrCount = a.take<uint32_t>(N);
@@ -424,8 +426,8 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
                 if (it == 0 || cn::fluidGatherEachIteration(s))
                     probe(sv, "fluid_gather", st, [&] { cn::launchFluidGather(s, it, st); });
                 // the first iteration of a substep also records the superset lists when they are on
-                probe(sv, (it == 0 && s.sup) ? "fluid_neighbors_superset" : "fluid_neighbors_density", st,
-                      [&] { cn::launchFluidNeighborsDensity(s, c, it, st); });
+                probe(sv, (it == 0 && s.sup && !sv->walkCells) ? "fluid_neighbors_superset" : "fluid_neighbors_density", st,
+                      [&] { cn::launchFluidNeighborsDensity(s, c, it, sv->walkCells, st); });
                 probe(sv, "fluid_delta_apply_clamp", st,
                       [&] { cn::launchFluidDeltaApplyClamp(s, it, dt, c, sv->writeFluidDebug, st); });
             }
@@ -1138,6 +1140,7 @@ CN_API cn_status cn_solver_set_debug(cn_solver *sv, uint32_t flags)
     sv->writeFluidDebug = (flags & 1u) != 0u;
     sv->postUpdateNeighbors = (flags & 2u) != 0u;
     sv->forceBroadphase = (flags & 4u) != 0u;
+    sv->walkCells = (flags & 8u) != 0u;
     releaseGraph(sv);
     return CN_OK;
 }

@@ -601,8 +601,11 @@ CN_API cn_status cn_solver_step_io(cn_solver *solver, float frame_dt, const floa
  *      reference does (physics_solver.cpp:1262-1268); the lists feed only vorticity confinement and
  *      render anisotropy, so the default schedule skips the rebuild;
  *  CN_DEBUG_FORCE_BROADPHASE   run the cell-key sort even when no consumer in the scene needs it
- *      (the reference always runs it once any contact family is enabled). */
-enum { CN_DEBUG_KEEP_FLUID_DELTA = 1, CN_DEBUG_POST_UPDATE_NEIGHBORS = 2, CN_DEBUG_FORCE_BROADPHASE = 4 };
+ *      (the reference always runs it once any contact family is enabled);
+ *  CN_DEBUG_WALK_CELLS         build every fluid iteration's neighbour lists by walking the 27 cells,
+ *      as the reference does, instead of filtering the substep's superset lists (same lists). */
+enum { CN_DEBUG_KEEP_FLUID_DELTA = 1, CN_DEBUG_POST_UPDATE_NEIGHBORS = 2, CN_DEBUG_FORCE_BROADPHASE = 4,
+       CN_DEBUG_WALK_CELLS = 8 };
 CN_API cn_status cn_solver_set_debug(cn_solver *solver, uint32_t flags);
 
 /* Per-kernel-group device times of the last replayed frame (no reference counterpart: the

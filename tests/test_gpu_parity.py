@@ -201,3 +201,45 @@ def test_dam_break_density_drift_20_steps():
     cg = gpu.debug_read("fluid_constraints").view(np.float32).reshape(-1, 4)[:, 3].astype(np.float64)
     co = ora.debug_read("fluid_constraints").view(np.float32).reshape(-1, 4)[:, 3].astype(np.float64)
     assert abs(cg.mean() - co.mean()) <= 1e-3 * max(abs(co.mean()), 1e-12) + 1e-12
+
+
+def fluid_with_distant_tissue():
+    """Fluid block plus a pinned soft body out of its reach: particle-particle contacts are on (the
+    contacts may move fluid x, so the superset lists are validated by each particle's move since
+    their build) but none forms, so the run is free of float atomics."""
+    w, desc, dt = small_fluid((12, 10, 12))
+    pinned = [x * 3 * 4 + z for x in range(4) for z in range(4)]
+    w.add_soft_body_grid((0.3, 0.2, 0.3), 0.1, position=(5.0, 0.2, 5.0), radius=0.03, edge_compliance=1e-5,
+                         volume_compliance=1e-6, static_particles=pinned)
+    return w, desc, dt
+
+
+def test_superset_lists_with_contacts_equal_the_cell_walk():
+    w, desc, dt = fluid_with_distant_tissue()
+    desc.fluid_iterations = 4
+    soa = w.soa()
+    runs = []
+    for walk in (False, True):
+        gpu = Solver(desc)
+        gpu.set_debug(keep_fluid_delta=True, walk_cells=walk)
+        gpu.sync_world(soa)
+        gpu.set_timing(True)
+        for _ in range(3):
+            gpu.step(dt)
+        runs.append((gpu.debug_read("fluid_neighbor_counts").view(np.uint32).copy(),
+                     gpu.debug_read("fluid_neighbors").view(np.uint32).reshape(-1, 128).copy(),
+                     gpu.read_particles(), set(gpu.kernel_times())))
+    (c0, l0, s0, k0), (c1, l1, s1, k1) = runs
+    assert "fluid_neighbors_superset" in k0 and "fluid_neighbors_superset" not in k1
+    assert np.array_equal(c0, c1)
+    for p in range(len(c0)):
+        assert np.array_equal(l0[p, :c0[p]], l1[p, :c0[p]]), p
+    for a, b in zip(s0, s1):
+        assert np.array_equal(a, b)
+    ora = cn_oracle.Oracle(desc, soa)
+    ora.set_post_update_neighbors(False)
+    for _ in range(3):
+        ora.step(dt)
+    assert np.array_equal(c0, ora.debug_read("fluid_neighbor_counts").view(np.uint32))
+    for a, b in zip(s0, ora.read_particles()):
+        np.testing.assert_allclose(a, b, rtol=RTOL, atol=ATOL_V)
