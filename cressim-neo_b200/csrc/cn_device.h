@@ -87,6 +87,7 @@ struct Scene {
     WorkList wP, wE, wT, wB, wC;      // particles, edges, tets, rigid bodies, colliders
     const uint2 *pColRange = nullptr; // per particle: its scene's range of colQueryOrder
     uint32_t N = 0;
+    uint32_t solidEnd = 0;            // 1 + the largest index of a non-fluid particle
     // ---- particles (reference order) ----
     float4 *x = nullptr, *xprev = nullptr, *v = nullptr;
     const float *radii = nullptr;

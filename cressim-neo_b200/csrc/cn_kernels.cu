@@ -553,11 +553,17 @@ __global__ void __launch_bounds__(kThreads) k_particleCandidates(Scene s, const 
     }
     if (i >= s.N) return;
     if (kEmit && s.ppCount[i] == 0u) return;
+    const uint32_t kind = s.kinds[i];
+    // Pairs go from the lower index up and fluid-fluid pairs are excluded: a fluid particle past
+    // every solid (the world packs fluids last) has no candidate to walk for.
+    if (!kEmit && kind == CN_PARTICLE_FLUID && i >= s.solidEnd) {
+        s.ppCount[i] = 0u;
+        return;
+    }
     const int4 e = s.entries[i];
     const f3 pos = xyz(s.x[i]);
     const float r = s.radii[i];
     const uint4 m = s.meta[i];
-    const uint32_t kind = s.kinds[i];
     uint32_t count = 0;
     uint32_t write = kEmit ? s.ppOffset[i] : 0u;
     for (int dz = -1; dz <= 1; ++dz)
@@ -763,6 +769,7 @@ __global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighbors
     const float h = mx(fm.smoothing_radius, 1.0e-4f);
     const float h2 = sqrtThreshold(h);
     const float kW = spikyK(h);
+    const float invH = 1.0f / h;
     const float st = mx(fm.surface_tension, 0.0f);
     const f3 sp = xyz(self);
     // Lists are interleaved (entry k of slot i at k * N + i): a warp's k-th entries share lines.
@@ -800,8 +807,8 @@ __global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighbors
                 out[count++ * lstr] = cc[j];
                 if (density) {
                     const float dist = sqrtf(d2);
-                    rho += spikyWk(dist, h, kW);
-                    if (st > kEps) normal += spikyGradK(delta, dist, h, kW);
+                    rho += spikyWk(dist, h, invH, kW);
+                    if (st > kEps) normal += spikyGradK(delta, dist, h, invH, kW);
                 }
             }
         }
@@ -854,8 +861,8 @@ __global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighbors
                         out[count++ * lstr] = c;
                         if (density) {
                             const float dist = sqrtf(d2);
-                            rho += spikyWk(dist, h, kW);
-                            if (st > kEps) normal += spikyGradK(delta, dist, h, kW);
+                            rho += spikyWk(dist, h, invH, kW);
+                            if (st > kEps) normal += spikyGradK(delta, dist, h, invH, kW);
                         }
                     }
                 }
@@ -872,7 +879,7 @@ __global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighbors
         if (!fluidGhostDelta(s, s.colQueryOrder[kk], sp, h, ghost)) continue;
         const float dist = length(ghost);
         if (dist >= h) continue;
-        rho += spikyWk(dist, h, kW) * cfg.fluidBoundaryDensityScale;
+        rho += spikyWk(dist, h, invH, kW) * cfg.fluidBoundaryDensityScale;
     }
     const float rho0 = mx(fm.rest_density, 1.0f);
     const float C = mx(rho - rho0, -rho0 * mx(cfg.fluidMaxUnderDensityRatio, 0.0f)) * fm.density_constraint_scale;
@@ -918,6 +925,7 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
         const float sC = snc.w;
         const float h = mx(fm.smoothing_radius, 1.0e-4f);
         const float kW = spikyK(h);
+        const float invH = 1.0f / h;
         const float cohesion = dt * mx(fm.cohesion, 0.0f);
         const float visc = dt * mx(fm.viscosity, 0.0f);
         const float st = mx(fm.surface_tension, 0.0f);
@@ -953,13 +961,13 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
             const f3 delta = sp - xyz(np);
             const float dist = length(delta);
             if (dist >= h || dist <= kEps) continue;
-            const f3 nij = delta / dist;
+            const f3 nij = delta * (1.0f / dist);
             // spikyDW / spikyW of physics_fluid_common.hlsli:17-41 sharing 1 - dist / h
-            const float om = 1.0f - dist / h;
-            const float dw = -2.0f * kW * om / h;
+            const float om = 1.0f - dist * invH;
+            const float dw = -2.0f * kW * om * invH;
             f3 pd = -0.5f * (sC + ncw) * dw * nij;
             if (infoMaterial(tag) == myMat) {
-                if (cohesion > kEps) pd -= nij * (cohesion * cohesionW(dist, h, fm.cohesion1, fm.cohesion2));
+                if (cohesion > kEps) pd -= nij * (cohesion * cohesionW(dist, h, invH, fm.cohesion1, fm.cohesion2));
                 if (needRel) {
                     const f3 nd = iter > 0 ? xyz(nd4) : f3{0.f, 0.f, 0.f};
                     const f3 rel = sdl - nd;
@@ -986,8 +994,8 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
             if (!fluidGhostDelta(s, s.colQueryOrder[k], sp, h, ghost)) continue;
             const float dist = length(ghost);
             if (dist <= kEps || dist >= h) continue;
-            const f3 nij = ghost / dist;
-            const float dw = spikyDWk(dist, h, kW);
+            const f3 nij = ghost * (1.0f / dist);
+            const float dw = spikyDWk(dist, h, invH, kW);
             bd += -mx(sC, 0.0f) * dw * nij;
         }
         bd = bd * cfg.fluidBoundaryDeltaScale;

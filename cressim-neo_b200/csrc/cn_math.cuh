@@ -217,58 +217,38 @@ __host__ __device__ __forceinline__ f3 positionFrictionDelta(f3 tdisp, float pen
     return tdisp * mn(saturate(kinetic) * pen / td, 1.0f);
 }
 
-// physics_fluid_common.hlsli:17-66
-__host__ __device__ __forceinline__ float spikyW(float d, float h)
-{
-    if (d >= h) return 0.0f;
-    const float om = 1.0f - d / h;
-    const float h3 = h * h * h;
-    const float k = 15.0f / (3.14159265359f * h3);
-    return k * om * om;
-}
-__host__ __device__ __forceinline__ float spikyDW(float d, float h)
-{
-    if (d <= kEps || d >= h) return 0.0f;
-    const float om = 1.0f - d / h;
-    const float h3 = h * h * h;
-    const float k = 15.0f / (3.14159265359f * h3);
-    return -2.0f * k * om / h;
-}
-__host__ __device__ __forceinline__ f3 spikyGrad(f3 delta, float d, float h)
-{
-    if (d <= kEps || d >= h) return f3{0.f, 0.f, 0.f};
-    const float dw = spikyDW(d, h);
-    return dw * (delta / d);
-}
-// The same kernels with the normalisation 15 / (pi h^3) passed in: a per-material constant whose
-// value does not depend on the neighbour, so computing it once per particle changes no bits.
+// physics_fluid_common.hlsli:17-66.  The shaders divide by the smoothing radius and by the pair
+// distance; SPIR-V's OpFDiv is specified to 2.5 ulp, not correctly rounded, and these kernels
+// (and the oracle) take each such quotient as the product with the correctly rounded reciprocal
+// -- one reciprocal per particle (1 / h) or per pair (1 / d) -- at most 1.5 ulp from the exact
+// quotient.  The normalisation 15 / (pi h^3) is passed in, computed once per particle.
 __host__ __device__ __forceinline__ float spikyK(float h)
 {
     const float h3 = h * h * h;
     return 15.0f / (3.14159265359f * h3);
 }
-__host__ __device__ __forceinline__ float spikyWk(float d, float h, float k)
+__host__ __device__ __forceinline__ float spikyWk(float d, float h, float invH, float k)
 {
     if (d >= h) return 0.0f;
-    const float om = 1.0f - d / h;
+    const float om = 1.0f - d * invH;
     return k * om * om;
 }
-__host__ __device__ __forceinline__ float spikyDWk(float d, float h, float k)
+__host__ __device__ __forceinline__ float spikyDWk(float d, float h, float invH, float k)
 {
     if (d <= kEps || d >= h) return 0.0f;
-    const float om = 1.0f - d / h;
-    return -2.0f * k * om / h;
+    const float om = 1.0f - d * invH;
+    return -2.0f * k * om * invH;
 }
-__host__ __device__ __forceinline__ f3 spikyGradK(f3 delta, float d, float h, float k)
+__host__ __device__ __forceinline__ f3 spikyGradK(f3 delta, float d, float h, float invH, float k)
 {
     if (d <= kEps || d >= h) return f3{0.f, 0.f, 0.f};
-    const float dw = spikyDWk(d, h, k);
-    return dw * (delta / d);
+    const float dw = spikyDWk(d, h, invH, k);
+    return dw * (delta * (1.0f / d));
 }
-__host__ __device__ __forceinline__ float cohesionW(float d, float h, float c1, float c2)
+__host__ __device__ __forceinline__ float cohesionW(float d, float h, float invH, float c1, float c2)
 {
     if (d <= kEps || d >= h) return 0.0f;
-    const float q = d / h;
+    const float q = d * invH;
     return c1 * q * q * q + c2 * q * q - 1.0f;
 }
 

@@ -716,6 +716,12 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     layout(sv, a, *w, edgeI, bendI, tetI, segI, jointI);
     cn::Scene &s = sv->s;
     s.cellSize = w->particle_grid_cell_size;
+    s.solidEnd = 0;
+    for (uint32_t i = N; i > 0; --i)
+        if (w->kinds[i - 1] != CN_PARTICLE_FLUID) {
+            s.solidEnd = i;
+            break;
+        }
     s.colQueryCount = uint32_t(order.size());
     s.activeMovingCount = moving;
     cudaStream_t st = sv->ownStream;

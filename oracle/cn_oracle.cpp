@@ -216,11 +216,13 @@ inline f3 CombineContactMaterial(f4 a, f4 b)
 }
 inline f3 ProjectOntoTangent(f3 v, f3 n) { return v - n * dot(v, n); }
 
-// physics_fluid_common.hlsli:17-41
+// physics_fluid_common.hlsli:17-41.  A quotient by the smoothing radius or by a pair distance is
+// taken as the product with the correctly rounded reciprocal (SPIR-V's OpFDiv, which the shaders
+// compile to, is specified to 2.5 ulp rather than correctly rounded); the kernels do the same.
 inline float SpikyW(float d, float h)
 {
     if (d >= h) return 0.0f;
-    const float om = 1.0f - d / h;
+    const float om = 1.0f - d * (1.0f / h);
     const float h3 = h * h * h;
     const float k = 15.0f / (3.14159265359f * h3);
     return k * om * om;
@@ -228,21 +230,22 @@ inline float SpikyW(float d, float h)
 inline float SpikyDW(float d, float h)
 {
     if (d <= kEps || d >= h) return 0.0f;
-    const float om = 1.0f - d / h;
+    const float invH = 1.0f / h;
+    const float om = 1.0f - d * invH;
     const float h3 = h * h * h;
     const float k = 15.0f / (3.14159265359f * h3);
-    return -2.0f * k * om / h;
+    return -2.0f * k * om * invH;
 }
 inline f3 SpikyGrad(f3 delta, float d, float h)
 {
     if (d <= kEps || d >= h) return f3{0, 0, 0};
     const float dw = SpikyDW(d, h);
-    return dw * (delta / d);
+    return dw * (delta * (1.0f / d));
 }
 inline float CohesionW(float d, float h, float c1, float c2)
 {
     if (d <= kEps || d >= h) return 0.0f;
-    const float q = d / h;
+    const float q = d * (1.0f / h);
     return c1 * q * q * q + c2 * q * q - 1.0f;
 }
 
@@ -1132,7 +1135,7 @@ void fluidDeltaPositions(cno_solver &s, uint32_t iter, float dt)
             const float dist = length(delta);
             if (dist >= h || dist <= kEps) continue;
             const f4 nnc = s.fluidNormalC[c];
-            const f3 nij = delta / dist;
+            const f3 nij = delta * (1.0f / dist);
             const float dw = SpikyDW(dist, h);
             f3 pd = -0.5f * (sC + nnc.w) * dw * nij;
             if (s.fluidMatIdx[i] == s.fluidMatIdx[c]) {
@@ -1157,7 +1160,7 @@ void fluidDeltaPositions(cno_solver &s, uint32_t iter, float dt)
             if (!FluidGhostDelta(s, c, sp, h, ghost)) continue;
             const float dist = length(ghost);
             if (dist <= kEps || dist >= h) continue;
-            const f3 nij = ghost / dist;
+            const f3 nij = ghost * (1.0f / dist);
             const float dw = SpikyDW(dist, h);
             bd += -std::max(sC, 0.0f) * dw * nij;
         }
