@@ -88,6 +88,7 @@ struct Scene {
     const uint2 *pColRange = nullptr; // per particle: its scene's range of colQueryOrder
     uint32_t N = 0;
     uint32_t solidEnd = 0;            // 1 + the largest index of a non-fluid particle
+    uint32_t fluidExtras = 0;         // a fluid material has cohesion or surface tension
     // ---- particles (reference order) ----
     float4 *x = nullptr, *xprev = nullptr, *v = nullptr;
     const float *radii = nullptr;

@@ -13,6 +13,7 @@
 //    order, so their sums are deterministic (the reference uses float atomics).
 // Arithmetic follows the reference's expression order; the library is built with
 // --fmad=false so float32 results match a CPU evaluation of the same order.
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -445,12 +446,8 @@ __device__ __forceinline__ bool findRunCompute(const Scene &s, uint32_t key, uin
 // Per run j: the 27 neighbour runs in the reference's traversal order (dz, dy, dx), looked up
 // once per substep.  Entry k = (compute start | checkCoordinates << 31, end); empty when the
 // target cell has no run or its (uniform) run holds another cell that hashes to the same key.
-__global__ void __launch_bounds__(kThreads) k_runNeighbors(Scene s)
+__device__ __forceinline__ void runNeighborAt(const Scene &s, uint32_t j, uint32_t k)
 {
-    // one thread per (run j, neighbour k): the 27 hash probes of a run proceed in parallel
-    const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    const uint32_t j = uint32_t(t / 27u), k = uint32_t(t % 27u);
-    if (j >= __ldg(s.runTotal)) return;
     const uint32_t r = s.runVal[j];
     const int4 e = s.sCell[s.runHashStart[r] & 0x7fffffffu];
     const int dz = int(k / 9u) - 1, dy = int((k / 3u) % 3u) - 1, dx = int(k % 3u) - 1;
@@ -468,6 +465,16 @@ __global__ void __launch_bounds__(kThreads) k_runNeighbors(Scene s)
         }
     }
     s.runNbr[size_t(j) * 27u + k] = rg;
+}
+
+__global__ void __launch_bounds__(kThreads) k_runNeighbors(Scene s)
+{
+    // one thread per (run j, neighbour k), striding over the runs that exist (a device count):
+    // the 27 hash probes of a run proceed in parallel
+    const uint64_t items = uint64_t(__ldg(s.runTotal)) * 27u;
+    for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < items;
+         t += uint64_t(gridDim.x) * blockDim.x)
+        runNeighborAt(s, uint32_t(t / 27u), uint32_t(t % 27u));
 }
 
 // ------------------------------------------------------------------------------------------
@@ -743,11 +750,15 @@ __device__ __forceinline__ bool neighborAllowed(const Scene &s, uint32_t tag, ui
 //         neighbour of this iteration is in the superset, and filtering it in order yields exactly
 //         the list the cell walk would build.  Otherwise (or if this particle's superset
 //         overflowed) the particle walks the cells.
-// One instantiation per mode, so the cell walk's register needs do not set the filter's occupancy.
+// One instantiation per mode, so the cell walk's register needs do not set the filter's occupancy;
+// the filter is held to 64 registers (4 blocks of 256 per SM: 14 % faster than 65 registers and
+// 3 blocks, measured; 48 registers and 5 blocks spill).
 // With `Dk` (the accumulated delta this iteration starts from) the density constraint is also
 // stored in Dk.w, so the delta kernel reads a neighbour's delta and constraint in one load.
-template <uint32_t mode>
-__global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighborsDensity(Scene s, Config cfg, bool density,
+// kExtras false: no fluid material has surface tension, so the colour-field normal is not summed
+// (fewer live registers: the filter then runs at 5 blocks of 256 per SM, 10 % faster, measured).
+template <uint32_t mode, bool kExtras>
+__global__ void __launch_bounds__(kThreads, (mode == 1u || !kExtras) ? 5 : 4) k_fluidNeighborsDensity(Scene s, Config cfg, bool density,
                                                                                     uint32_t iter, float4 *Dk)
 {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -770,7 +781,7 @@ __global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighbors
     const float h2 = sqrtThreshold(h);
     const float kW = spikyK(h);
     const float invH = 1.0f / h;
-    const float st = mx(fm.surface_tension, 0.0f);
+    const float st = kExtras ? mx(fm.surface_tension, 0.0f) : 0.0f;
     const f3 sp = xyz(self);
     // Lists are interleaved (entry k of slot i at k * N + i): a warp's k-th entries share lines.
     uint32_t *out = kInterleavedLists ? s.nbr + slot : s.nbr + size_t(slot) * maxN;
@@ -808,7 +819,7 @@ __global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighbors
                 if (density) {
                     const float dist = sqrtf(d2);
                     rho += spikyWk(dist, h, invH, kW);
-                    if (st > kEps) normal += spikyGradK(delta, dist, h, invH, kW);
+                    if (kExtras && st > kEps) normal += spikyGradK(delta, dist, h, invH, kW);
                 }
             }
         }
@@ -862,7 +873,7 @@ __global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighbors
                         if (density) {
                             const float dist = sqrtf(d2);
                             rho += spikyWk(dist, h, invH, kW);
-                            if (st > kEps) normal += spikyGradK(delta, dist, h, invH, kW);
+                            if (kExtras && st > kEps) normal += spikyGradK(delta, dist, h, invH, kW);
                         }
                     }
                 }
@@ -883,7 +894,7 @@ __global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighbors
     }
     const float rho0 = mx(fm.rest_density, 1.0f);
     const float C = mx(rho - rho0, -rho0 * mx(cfg.fluidMaxUnderDensityRatio, 0.0f)) * fm.density_constraint_scale;
-    if (st > kEps) {
+    if (kExtras && st > kEps) {
         normal = normal * st;
         s.Cs[slot] = mk4(normal, C);
     } else {
@@ -901,7 +912,11 @@ __global__ void __launch_bounds__(kThreads, mode == 1u ? 5 : 1) k_fluidNeighbors
 // writes the next iteration's position x + accumulated delta -- what k_fluidGather would compute
 // -- into the other position buffer, and records the largest accumulated delta for the superset
 // test of the next iteration, so the gather runs once per substep.
-__global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Config cfg, const float4 *Xs,
+//
+// kExtras false: no fluid material of the scene has cohesion or surface tension, so those terms
+// are zero for every pair and the kernel is built without them (fewer live registers).
+template <bool kExtras>
+__global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidDeltaApplyClamp(Scene s, Config cfg, const float4 *Xs,
                                                                    const float4 *Dcur, float4 *Dnext,
                                                                    uint32_t iter, float dt, bool writeDx,
                                                                    float4 *Pnext)
@@ -926,16 +941,17 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
         const float h = mx(fm.smoothing_radius, 1.0e-4f);
         const float kW = spikyK(h);
         const float invH = 1.0f / h;
-        const float cohesion = dt * mx(fm.cohesion, 0.0f);
+        const float cohesion = kExtras ? dt * mx(fm.cohesion, 0.0f) : 0.0f;
         const float visc = dt * mx(fm.viscosity, 0.0f);
-        const float st = mx(fm.surface_tension, 0.0f);
+        const float st = kExtras ? mx(fm.surface_tension, 0.0f) : 0.0f;
         const float cfl = mx(fm.cfl_radius, 0.0f);
         const bool needRel = visc > kEps || cfl > kEps;
         const f3 sn = st > kEps ? xyz(snc) : f3{0.f, 0.f, 0.f};
         f3 dp{0.f, 0.f, 0.f};
         const uint32_t cnt = s.nbrCount[slot];
+        // 32-bit list offsets (N x max neighbours < 2^32 is checked at sync)
         const uint32_t *lst = kInterleavedLists ? s.nbr + slot : s.nbr + size_t(slot) * s.maxNbr;
-        const size_t lstr = kInterleavedLists ? size_t(s.N) : 1u;
+        const uint32_t lstr = kInterleavedLists ? s.N : 1u;
         // Software-pipelined over the list: the next neighbour's slot, position word, constraint
         // and accumulated delta are in flight while the current pair term is computed.
         // A neighbour's accumulated delta (xyz, used from the second iteration on) and density
@@ -967,7 +983,8 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
             const float dw = -2.0f * kW * om * invH;
             f3 pd = -0.5f * (sC + ncw) * dw * nij;
             if (infoMaterial(tag) == myMat) {
-                if (cohesion > kEps) pd -= nij * (cohesion * cohesionW(dist, h, invH, fm.cohesion1, fm.cohesion2));
+                if (kExtras && cohesion > kEps)
+                    pd -= nij * (cohesion * cohesionW(dist, h, invH, fm.cohesion1, fm.cohesion2));
                 if (needRel) {
                     const f3 nd = iter > 0 ? xyz(nd4) : f3{0.f, 0.f, 0.f};
                     const f3 rel = sdl - nd;
@@ -980,7 +997,7 @@ __global__ void __launch_bounds__(kThreads) k_fluidDeltaApplyClamp(Scene s, Conf
                         if (proj < -cfl) pd -= nij * (proj + cfl) * 0.5f;
                     }
                 }
-                if (st > kEps) pd -= dt * (sn - xyz(ld4(&s.Cs[c])));
+                if (kExtras && st > kEps) pd -= dt * (sn - xyz(ld4(&s.Cs[c])));
             }
             dp += pd;
             weight += 1.0f;
@@ -2331,7 +2348,9 @@ void launchCellSetup(const Scene &s, uint32_t *scanTmp, void *sortScratch, cudaS
         exclusiveScan(s.runLenSorted, s.runCompStart, s.N, scanTmp, scanTmp + 1, st);
         k_runPlace<<<blocksFor(s.N), kThreads, 0, st>>>(s);
         k_computeOrderSetup<<<blocksFor(s.N), kThreads, 0, st>>>(s);
-        k_runNeighbors<<<blocksFor(size_t(s.N) * 27u), kThreads, 0, st>>>(s);
+        // the runs number at most N (about N / 8 in a settled fluid): a fixed grid strides over them
+        const unsigned grid = unsigned(std::min<size_t>(blocksFor(size_t(s.N) * 27u), 148u * 16u));
+        k_runNeighbors<<<grid, kThreads, 0, st>>>(s);
     }
 }
 
@@ -2380,12 +2399,16 @@ void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter,
     if (s.N == 0) return;
     const Scene sp = withPositions(s, iter);
     float4 *Dk = (iter & 1u) ? s.Db : s.Da;
-    if (s.sup == nullptr || walkCells)
-        k_fluidNeighborsDensity<0u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter, Dk);
-    else if (iter == 0)
-        k_fluidNeighborsDensity<1u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter, Dk);
-    else
-        k_fluidNeighborsDensity<2u><<<blocksFor(s.N), kThreads, 0, st>>>(sp, c, true, iter, Dk);
+    const unsigned g = blocksFor(s.N);
+    if (s.sup == nullptr || walkCells) {
+        if (s.fluidExtras) k_fluidNeighborsDensity<0u, true><<<g, kThreads, 0, st>>>(sp, c, true, iter, Dk);
+        else k_fluidNeighborsDensity<0u, false><<<g, kThreads, 0, st>>>(sp, c, true, iter, Dk);
+    } else if (iter == 0) { // the superset build: the lean build measured slower, so one variant
+        k_fluidNeighborsDensity<1u, true><<<g, kThreads, 0, st>>>(sp, c, true, iter, Dk);
+    } else {
+        if (s.fluidExtras) k_fluidNeighborsDensity<2u, true><<<g, kThreads, 0, st>>>(sp, c, true, iter, Dk);
+        else k_fluidNeighborsDensity<2u, false><<<g, kThreads, 0, st>>>(sp, c, true, iter, Dk);
+    }
 }
 
 void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
@@ -2395,8 +2418,12 @@ void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const C
     const float4 *Dcur = (iter & 1u) ? s.Db : s.Da;
     float4 *Dnext = (iter & 1u) ? s.Da : s.Db;
     float4 *Pnext = s.Pb ? ((iter & 1u) ? s.P : s.Pb) : nullptr;
-    k_fluidDeltaApplyClamp<<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), c, s.Xs, Dcur, Dnext, iter,
-                                                                dt, writeDebug, Pnext);
+    if (s.fluidExtras)
+        k_fluidDeltaApplyClamp<true><<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), c, s.Xs, Dcur, Dnext,
+                                                                      iter, dt, writeDebug, Pnext);
+    else
+        k_fluidDeltaApplyClamp<false><<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), c, s.Xs, Dcur, Dnext,
+                                                                       iter, dt, writeDebug, Pnext);
 }
 
 void launchFluidIteration(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
@@ -2413,7 +2440,7 @@ void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)
     // Positions after the velocity update; the accumulated delta was folded into x.
     k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, s.Da, 0u, nullptr, nullptr);
     Config dummy{};
-    k_fluidNeighborsDensity<0u><<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u, nullptr);
+    k_fluidNeighborsDensity<0u, false><<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u, nullptr);
 }
 
 void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st)

@@ -612,6 +612,8 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
             return setError(CN_ERR_UNSUPPORTED, "vorticity confinement is not implemented");
     sv->hasFluid = anyFluid;
     sv->hasDynamic = anyDynamic;
+    if (anyFluid && (uint64_t(N) * std::max<uint32_t>(d.max_fluid_neighborhood, 160u) >= (uint64_t(1) << 32)))
+        return setError(CN_ERR_UNSUPPORTED, "fluid scene too large for 32-bit neighbour list offsets");
     const bool contactWork = sv->contactIt > 0;
     sv->ppPossible = contactWork && N > 1 && anySolid && (anyFluid || anySelf || solidGroups.size() > 1);
     sv->rigidPossible = contactWork && N > 0 && w->collider_count > 0 && anySolid;
@@ -716,6 +718,9 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     layout(sv, a, *w, edgeI, bendI, tetI, segI, jointI);
     cn::Scene &s = sv->s;
     s.cellSize = w->particle_grid_cell_size;
+    s.fluidExtras = 0;
+    for (uint32_t m = 0; m < w->fluid_material_count; ++m)
+        if (w->fluid_materials[m].cohesion > 0.0f || w->fluid_materials[m].surface_tension > 1.0e-6f) s.fluidExtras = 1;
     s.solidEnd = 0;
     for (uint32_t i = N; i > 0; --i)
         if (w->kinds[i - 1] != CN_PARTICLE_FLUID) {
