@@ -451,10 +451,12 @@ def run_served(args, stream, sh, rank: int = 0, world: int = 1) -> dict:
 
 
 def run_other_configs(stream, sh, cpu: bool = True) -> dict:
-    """The plain XPBD cube (16^3 vertices, 16,875 tets, 10 substeps x 20 iterations, ground) and the
-    mixed surgical scene (60x30x60 tissue, 256^2 cloth, 64 strands of 129, 64^3 fluid, kinematic
-    capsule on a seeded path, 8 substeps), each timed over frames replayed from its CUDA graph;
-    the cube also beside the oracle on the host cores (the reference's CPU-runnable case)."""
+    """The plain XPBD cube (16^3 vertices, 16,875 tets, 10 substeps x 20 iterations, ground), a pile
+    of 4,096 dynamic rigid bodies in 4 layers with 4 proxy-particle bodies (rigid broadphase and
+    contacts), and
+    the mixed surgical scene (60x30x60 tissue, 256^2 cloth, 64 strands of 129, 64^3 fluid,
+    kinematic capsule on a seeded path, 8 substeps), each timed over frames replayed from its CUDA
+    graph; the cube also beside the oracle on the host cores (the reference's CPU-runnable case)."""
     import torch
     from cn_physics import Solver, scenes
     out = {}
@@ -503,6 +505,28 @@ def run_other_configs(stream, sh, cpu: bool = True) -> dict:
         cube["cpu_baseline"] = {"value": round(n * d2.substeps * frames / el, 1), "unit": "particle-substeps/s",
                                 "cores": threads, "kind": "port", "sample": f"{frames} frames of the same cube"}
     out["xpbd_cube"] = cube
+
+    # dynamic rigid bodies: 4,096 spheres / capsules / boxes dropped in 4 layers of 32 x 32 plus 4
+    # bodies of 27 proxy particles; timed once the pile has formed (frames 60-119)
+    w, desc, dt, bodies = scenes.rigid_pile()
+    soa = w.soa()
+    sv = Solver(desc)
+    sv.sync_world(soa)
+    sv.step_many(dt, 57, sh)
+    ms = timed(sv, dt, 60)
+    meta = sv.validate_gpu_meta()
+    c = w.counts()
+    pos = sv.read_rigid_bodies()[0]
+    out["rigid_pile"] = {
+        "workload": f"rigid pile: {len(bodies) - 4} dynamic spheres / capsules / boxes in 4 layers + 4 bodies of "
+                    f"27 proxy particles, {c['colliders']} colliders, ground box, {desc.substeps} substeps x "
+                    f"{desc.default_iterations} iterations, dt 1/60",
+        "value": round(c["bodies"] * desc.substeps / (ms / 1e3), 1), "unit": "body-substeps/s",
+        "ms_per_frame": round(ms, 3), "kernels_per_frame": sv.graph_stats()[0],
+        "rigid_rigid_pairs": meta["rigid_rigid_candidate_count"],
+        "proxy_contacts": meta["proxy_rigid_contact_count"], "meta_status": meta["status"],
+        "lowest_body_y": round(float(pos[1:, 1].min()), 4)}
+    sv.close()
 
     w, desc, dt, tool = scenes.mixed_surgical()
     soa = w.soa()

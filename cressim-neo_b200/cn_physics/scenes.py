@@ -191,3 +191,41 @@ def mixed_surgical(tissue=(60, 30, 60), cloth=(256, 256), strands=(64, 129), flu
     _jitter(w, 1.0e-4, seed)
     desc = solver_desc(substeps=8, enable_blocking_readback=0)
     return w, desc, 1.0 / 60.0, tool
+
+
+def rigid_pile(layers: int = 4, per_side: int = 32, seed: int = 0, proxy_tools: int = 4):
+    """Dynamic bodies dropped onto the ground in `layers` layers of per_side^2 (spheres, capsules and
+    boxes in turn, seeded jitter), plus `proxy_tools` dynamic bodies made of 27 proxy particles each:
+    the rigid broadphase (LBVH), the box-box manifold, depenetration and the body-pair velocity
+    solve, and proxy contacts.  Returns (world, desc, frame_dt, bodies)."""
+    rng = np.random.default_rng(seed)
+    w = World()
+    ground(w)
+    bodies = []
+    pitch = 0.12
+    half = (per_side - 1) * pitch * 0.5
+    k = 0
+    for ly in range(layers):
+        for ix in range(per_side):
+            for iz in range(per_side):
+                p = (ix * pitch - half + float(rng.uniform(-0.01, 0.01)), 0.06 + ly * pitch,
+                     iz * pitch - half + float(rng.uniform(-0.01, 0.01)))
+                b = w.add_rigid_body("dynamic", position=p, mass=0.2, inverse_inertia=(400.0,) * 3)
+                if k % 3 == 0:
+                    w.add_collider(b, "sphere", (0.04,), friction=0.5)
+                elif k % 3 == 1:
+                    w.add_collider(b, "capsule", (0.03, 0.03), friction=0.5)
+                else:
+                    w.add_collider(b, "box", (0.04, 0.04, 0.04), friction=0.5)
+                bodies.append(b)
+                k += 1
+    g = (np.arange(3) - 1.0) * 0.04
+    lattice = np.array([(x, y, z) for x in g for y in g for z in g], np.float32)
+    for t in range(proxy_tools):
+        p = (-half + (t + 0.5) * 2 * half / max(proxy_tools, 1), 0.3 + layers * pitch, 0.0)
+        b = w.add_rigid_body("dynamic", position=p, mass=0.5, inverse_inertia=(800.0,) * 3)
+        w.set_rigid_proxy_particles(b, lattice, 0.02, friction=0.5)
+        bodies.append(b)
+    w.soa()
+    desc = solver_desc(substeps=4, default_iterations=10, enable_blocking_readback=0)
+    return w, desc, 1.0 / 60.0, bodies

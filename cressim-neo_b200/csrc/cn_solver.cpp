@@ -199,9 +199,11 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
     s.proxyCapacity = 0;
     s.rrSlotCapacity = 0;
     if (sv->rigidRigid) {
-        const uint32_t P = std::max<uint32_t>(64u, 16u * C);
+        // estimateRigidCandidatePairCapacityFromColliderCount (rigid_body_common.cpp:35-47): 32
+        // pairs per collider; proxy contact slots: 8 per proxy, the particle-rigid candidate rate
+        const uint32_t P = std::max<uint32_t>(64u, 32u * C);
         s.rrCapacity = P;
-        s.proxyCapacity = sv->proxyContacts ? std::max<uint32_t>(64u, 4u * sv->nProxy) : 0u;
+        s.proxyCapacity = sv->proxyContacts ? std::max<uint32_t>(64u, 8u * sv->nProxy) : 0u;
         s.rrCount = a.take<uint32_t>(C); s.rrOffset = a.take<uint32_t>(C);
         const uint32_t K = P * cn::kRigidPairContacts + s.proxyCapacity;
         s.rrSlotCapacity = K;

@@ -2444,7 +2444,7 @@ void rigidPairsAndContacts(cno_solver &s)
     s.rrPairs.clear();
     s.rrContacts.clear();
     const uint32_t C = s.C;
-    const uint32_t cap = std::max<uint32_t>(64u, 16u * C);
+    const uint32_t cap = std::max<uint32_t>(64u, 32u * C); // rigid_body_common.cpp:35-47
     uint32_t required = 0;
     const std::vector<uint32_t> &order = s.colliderQueryOrder;
     for (uint32_t k = 0; k < s.activeMovingCount && order.size() >= 2; ++k) {
@@ -2522,12 +2522,12 @@ void rigidPairsAndContacts(cno_solver &s)
 // (proxies lead the particle order, so their candidates open the list) gets a contact after the
 // pair contacts -- the deepest between the proxy sphere of body A and the candidate body B's
 // enabled colliders, framed without the body scale (ComposeColliderWorldPosition) -- or an
-// inactive one; at most max(64, 4 x proxies) of them.
+// inactive one; at most max(64, 8 x proxies) of them.
 void proxyRigidContacts(cno_solver &s)
 {
     uint32_t proxyCands = 0;
     while (proxyCands < s.rigidPairs.size() && s.rigidPairs[proxyCands].first < s.nProxy) ++proxyCands;
-    const uint32_t cap = std::max<uint32_t>(64u, 4u * s.nProxy);
+    const uint32_t cap = std::max<uint32_t>(64u, 8u * s.nProxy);
     const uint32_t used = std::min(proxyCands, cap);
     s.requiredProxyContacts = proxyCands;
     s.proxyContactSlots = used;

@@ -196,3 +196,20 @@ def test_proxy_particles_are_not_batched():
     bt = Batch(batch_desc(solver_desc(**DESC)))
     with pytest.raises(CNError):
         bt.add_scene(w.soa())
+
+
+@pytest.mark.gpu
+def test_small_rigid_pile_with_proxy_bodies_matches_the_oracle():
+    """Spheres, capsules and boxes in two layers with proxy-particle bodies dropped on them: the
+    same candidate pairs frame by frame while the pile forms, states within tolerance."""
+    w, desc, dt, bodies = scenes.rigid_pile(layers=2, per_side=4)
+    gpu, ora = pair(w, desc)
+    for k in range(12):
+        gpu.step(dt)
+        ora.step(dt)
+        m, om = gpu.validate_gpu_meta(), ora.meta()
+        assert m["status"] == "OK"
+        assert m["required_rigid_rigid_candidate_count"] == om["required_rigid_rigid_pairs"], k
+        assert m["required_proxy_rigid_contact_count"] == om["required_proxy_contacts"], k
+    pg, po = gpu.read_rigid_bodies()[0], ora.read_rigid_bodies()[0]
+    assert np.abs(pg[:, :3] - po[:, :3]).max() < 1e-3   # the drift bar: contact order and float atomics
