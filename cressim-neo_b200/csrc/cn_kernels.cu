@@ -481,8 +481,46 @@ __global__ void __launch_bounds__(kThreads) k_runNeighbors(Scene s)
 // Particle-rigid candidate pairs (solid particles vs static/kinematic bodies, dedup 16)
 // physics_particle_count_particle_rigid_candidates.cs.hlsl:113-151, emit, finalize.
 // ------------------------------------------------------------------------------------------
+// Query-order positions of the colliders whose AABB overlaps [qmin, qmax], ascending, from this
+// substep's LBVH over the query-order colliders (built for scenes with dynamic bodies); false when
+// more than kCandidateHits overlap or the walk outgrows its stack -- the caller then scans.
+constexpr uint32_t kCandidateHits = 32u, kCandidateStack = 64u;
+__device__ __forceinline__ bool bvhOverlaps(const Scene &s, f3 qmin, f3 qmax, uint32_t *hits, uint32_t &nh)
+{
+    const uint32_t n = s.colQueryCount;
+    uint32_t stack[kCandidateStack];
+    uint32_t sp = 0;
+    nh = 0;
+    stack[sp++] = 0u;
+    while (sp > 0u) {
+        const uint32_t node = stack[--sp];
+        if (!aabbOverlaps(qmin, qmax, xyz(s.bvhMin[node]), xyz(s.bvhMax[node]))) continue;
+        if (node >= n - 1u) {
+            if (nh == kCandidateHits) return false;
+            hits[nh++] = s.bvhValA[node - (n - 1u)];
+            continue;
+        }
+        if (sp + 2u > kCandidateStack) return false;
+        const uint2 ch = s.bvhChildren[node];
+        stack[sp++] = ch.y;
+        stack[sp++] = ch.x;
+    }
+    for (uint32_t a = 1; a < nh; ++a) { // insertion sort: a handful of hits
+        const uint32_t v = hits[a];
+        uint32_t b = a;
+        while (b > 0u && hits[b - 1] > v) {
+            hits[b] = hits[b - 1];
+            --b;
+        }
+        hits[b] = v;
+    }
+    return true;
+}
+
 // kMode 0 counts the particle's candidate bodies, 1 emits its pairs from `write` (its offset
-// after the count pass and the scan); both return the count.
+// after the count pass and the scan); both return the count.  Colliders are taken in query order
+// (moving, then static): by a linear scan, or -- with many colliders and an LBVH this substep --
+// from the tree's overlaps sorted back into query order, the same sequence.
 template <uint32_t kMode>
 __device__ __forceinline__ uint32_t rigidCandidatesAt(const Scene &s, uint32_t i, uint32_t write)
 {
@@ -495,28 +533,43 @@ __device__ __forceinline__ uint32_t rigidCandidatesAt(const Scene &s, uint32_t i
     const uint32_t owner = s.ownerIdx[i];
     uint32_t seen[kRigidDedup];
     uint32_t seenCount = 0, count = 0;
-    const uint2 cq = s.pColRange ? s.pColRange[i] : make_uint2(0u, s.colQueryCount);
-    for (uint32_t k = cq.x; k < cq.y; ++k) {
+    // one overlapping collider (query position k): filter, dedup by body, count / emit; false
+    // when the emission buffer is full
+    auto consider = [&](uint32_t k) -> bool {
         const uint32_t c = s.colQueryOrder[k];
-        if (!aabbOverlaps(qmin, qmax, xyz(s.colAabbMin[c]), xyz(s.colAabbMax[c]))) continue;
         const cn_collider_broadphase bp = s.colBp[c];
         const uint32_t b = bp.owner_body;
-        if (proxyOwner && b == owner) continue;
+        if (proxyOwner && b == owner) return true;
         const uint32_t bt = s.bodyType[b];
         if (!(bp.enabled_flag != 0u && bp.environment_index == m.x && (m.w & bp.collision_layer) != 0u &&
               (bp.collision_mask & m.z) != 0u && (kind == CN_PARTICLE_SOLID || bt == CN_BODY_DYNAMIC) &&
               s.bodyColRanges[b].y > 0u))
-            continue;
+            return true;
         bool fresh = true;
         for (uint32_t q = 0; q < seenCount; ++q)
             if (seen[q] == b) { fresh = false; break; }
-        if (!fresh) continue;
+        if (!fresh) return true;
         if (seenCount < kRigidDedup) seen[seenCount++] = b;
         if (kMode != 0u) {
-            if (write >= s.rigidPairCapacity) return count;
+            if (write >= s.rigidPairCapacity) return false;
             s.rigidPairs[write++] = make_uint2(i, b);
         }
         ++count;
+        return true;
+    };
+    if (s.rrCapacity != 0u && s.activeMovingCount != 0u && s.colQueryCount > kCandidateHits && !s.pColRange) {
+        uint32_t hits[kCandidateHits], nh;
+        if (bvhOverlaps(s, qmin, qmax, hits, nh)) {
+            for (uint32_t j = 0; j < nh; ++j)
+                if (!consider(hits[j])) break;
+            return count;
+        }
+    }
+    const uint2 cq = s.pColRange ? s.pColRange[i] : make_uint2(0u, s.colQueryCount);
+    for (uint32_t k = cq.x; k < cq.y; ++k) {
+        const uint32_t c = s.colQueryOrder[k];
+        if (!aabbOverlaps(qmin, qmax, xyz(s.colAabbMin[c]), xyz(s.colAabbMax[c]))) continue;
+        if (!consider(k)) break;
     }
     return count;
 }

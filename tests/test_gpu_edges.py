@@ -143,3 +143,26 @@ def test_full_rigid_candidate_buffer_is_reported_and_matches():
     x_g, _, _ = gpu.read_particles()
     x_o, _, _ = ora.read_particles()
     np.testing.assert_allclose(x_g, x_o, rtol=1e-5, atol=1e-6)
+
+
+def test_rigid_candidates_from_the_lbvh_keep_the_scan_order():
+    """With more than 32 colliders and a dynamic body (so the substep builds the LBVH) the
+    particle-rigid candidates come from the tree, sorted back into query order: the candidate
+    counts and the contact records (candidate order) equal the oracle's linear scan."""
+    w = World()
+    w.add_soft_body_grid((0.4, 0.2, 0.4), 0.05, position=(0.0, 0.3, 0.0), radius=0.03,
+                         edge_compliance=1e-5, volume_compliance=1e-6, friction=0.3)
+    rng = np.random.default_rng(3)
+    for k in range(48):   # static spheres around and inside the block
+        b = w.add_rigid_body("static", position=tuple(rng.uniform((-0.3, 0.1, -0.3), (0.3, 0.5, 0.3))))
+        w.add_collider(b, "sphere", (float(rng.uniform(0.02, 0.06)),))
+    far = w.add_rigid_body("dynamic", position=(5.0, 1.0, 5.0), mass=1.0, inverse_inertia=(10.0,) * 3)
+    w.add_collider(far, "box", (0.1, 0.1, 0.1))
+    w.add_collider(far, "sphere", (0.05,), local_position=(0.0, 0.2, 0.0))
+    gpu, ora, _ = pair(w, solver_desc(substeps=1, default_iterations=4))
+    step_both(gpu, ora, 1.0 / 60.0, 1)
+    m, om = gpu.validate_gpu_meta(), ora.meta()
+    assert m["required_particle_rigid_candidate_count"] == om["required_rigid_pairs"] > 0
+    g, o = gpu.debug_read("rigid_contacts"), ora.debug_read("rigid_contacts")
+    assert g.size == o.size > 0 and np.array_equal(g.view(np.uint8), o.view(np.uint8))
+    same_state(gpu, ora)
