@@ -161,6 +161,7 @@ struct Scene {
     uint2 *bvhChildren = nullptr;                          // per internal node
     uint32_t *bvhParent = nullptr, *bvhVisits = nullptr;   // per node / internal node
     float4 *bvhMin = nullptr, *bvhMax = nullptr;           // per node
+    float4 *bvhWide = nullptr;                             // per internal node: both child boxes (4)
     float4 *bvhBounds = nullptr;                           // scene centre bounds (2)
     // Contact slots: kRigidPairContacts per collider pair, then one per proxy candidate
     // (physics_rigid_generate_proxy_contacts.cs.hlsl appends after the pair contacts)
@@ -271,6 +272,43 @@ struct BodyTarget {
     float4 pos;
     float4 rot;
 };
+
+#ifdef __CUDACC__
+// Walks the LBVH over the query-order colliders (colQueryCount >= 2) and calls leaf(j) for every
+// sorted leaf j whose box overlaps [qmin, qmax]; leaf returns false to stop the walk.  Each visit
+// reads one internal node's record of both child boxes, so only overlapping subtrees are entered.
+// Returns false when a push found the kStack-entry stack full (that subtree was skipped).
+template <uint32_t kStack, class V, class F>
+__device__ __forceinline__ bool bvhQuery(const Scene &s, V qmin, V qmax, F &&leaf)
+{
+    const uint32_t inner = s.colQueryCount - 1u;
+    auto hit = [&](const float4 &lo, const float4 &hi) {
+        return qmin.x <= hi.x && qmax.x >= lo.x && qmin.y <= hi.y && qmax.y >= lo.y && qmin.z <= hi.z &&
+               qmax.z >= lo.z;
+    };
+    uint32_t stack[kStack];
+    uint32_t sp = 0;
+    bool complete = true;
+    stack[sp++] = 0u;
+    while (sp > 0u) {
+        const float4 *w = s.bvhWide + size_t(stack[--sp]) * 4u;
+        const float4 l0 = w[0], l1 = w[1], r0 = w[2], r1 = w[3];
+        const uint32_t lc = __float_as_uint(l0.w), rc = __float_as_uint(r0.w);
+        const bool lo = hit(l0, l1), ro = hit(r0, r1);
+        if (lo && lc >= inner && !leaf(lc - inner)) return complete;
+        if (ro && rc >= inner && !leaf(rc - inner)) return complete;
+        if (ro && rc < inner) {
+            if (sp < kStack) stack[sp++] = rc;
+            else complete = false;
+        }
+        if (lo && lc < inner) {
+            if (sp < kStack) stack[sp++] = lc;
+            else complete = false;
+        }
+    }
+    return complete;
+}
+#endif
 
 // ------------------------------------------------------------------ launchers (cn_kernels.cu)
 // Writes `*count` staged kinematic targets (what cn_solver_set_kinematic_target writes for one).

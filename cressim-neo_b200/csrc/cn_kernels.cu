@@ -487,24 +487,14 @@ __global__ void __launch_bounds__(kThreads) k_runNeighbors(Scene s)
 constexpr uint32_t kCandidateHits = 32u, kCandidateStack = 64u;
 __device__ __forceinline__ bool bvhOverlaps(const Scene &s, f3 qmin, f3 qmax, uint32_t *hits, uint32_t &nh)
 {
-    const uint32_t n = s.colQueryCount;
-    uint32_t stack[kCandidateStack];
-    uint32_t sp = 0;
     nh = 0;
-    stack[sp++] = 0u;
-    while (sp > 0u) {
-        const uint32_t node = stack[--sp];
-        if (!aabbOverlaps(qmin, qmax, xyz(s.bvhMin[node]), xyz(s.bvhMax[node]))) continue;
-        if (node >= n - 1u) {
-            if (nh == kCandidateHits) return false;
-            hits[nh++] = s.bvhValA[node - (n - 1u)];
-            continue;
-        }
-        if (sp + 2u > kCandidateStack) return false;
-        const uint2 ch = s.bvhChildren[node];
-        stack[sp++] = ch.y;
-        stack[sp++] = ch.x;
-    }
+    bool room = true;
+    const bool complete = bvhQuery<kCandidateStack>(s, qmin, qmax, [&](uint32_t leaf) -> bool {
+        if (nh == kCandidateHits) return room = false;
+        hits[nh++] = s.bvhValA[leaf];
+        return true;
+    });
+    if (!complete || !room) return false;
     for (uint32_t a = 1; a < nh; ++a) { // insertion sort: a handful of hits
         const uint32_t v = hits[a];
         uint32_t b = a;

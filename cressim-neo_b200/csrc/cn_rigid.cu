@@ -31,9 +31,10 @@ __device__ __forceinline__ bool broadPhaseCollide(const cn_collider_broadphase &
 
 // ------------------------------------------------------------------------------------- LBVH
 // Scene bounds of the AABB centres (physics_rigid_reduce_extent_*): one block.
-__global__ void k_bvhBounds(Scene s)
+constexpr int kBoundsThreads = 1024; // one block: every collider's centre in a few strides
+__global__ void __launch_bounds__(kBoundsThreads) k_bvhBounds(Scene s)
 {
-    __shared__ float lo[3][kRigidThreads], hi[3][kRigidThreads];
+    __shared__ float lo[3][kBoundsThreads], hi[3][kBoundsThreads];
     f3 mn{3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f}, mxv{-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
     for (uint32_t k = threadIdx.x; k < s.colQueryCount; k += blockDim.x) {
         const uint32_t c = s.colQueryOrder[k];
@@ -146,6 +147,11 @@ __global__ void k_bvhRefit(Scene s)
         const float4 b0 = __ldcg(&s.bvhMin[ch.y]), b1 = __ldcg(&s.bvhMax[ch.y]);
         s.bvhMin[p] = mk4(min3(xyz(a0), xyz(b0)), 0.f);
         s.bvhMax[p] = mk4(max3(xyz(a1), xyz(b1)), 0.f);
+        float4 *w = s.bvhWide + size_t(p) * 4u; // the walk's record: child boxes and indices
+        w[0] = mk4(xyz(a0), __uint_as_float(ch.x));
+        w[1] = mk4(xyz(a1), 0.f);
+        w[2] = mk4(xyz(b0), __uint_as_float(ch.y));
+        w[3] = mk4(xyz(b1), 0.f);
         node = p;
     }
 }
@@ -168,33 +174,24 @@ __global__ void k_rigidPairs(Scene s, const uint32_t *total)
     const f3 qmin = xyz(s.colAabbMin[cA]), qmax = xyz(s.colAabbMax[cA]);
     uint32_t count = 0, write = kEmit ? s.rrOffset[k] : 0u;
     if (n >= 2u) {
-        uint32_t stack[kBvhStack];
-        uint32_t sp = 0;
-        stack[sp++] = 0u;
-        while (sp > 0u) {
-            const uint32_t node = stack[--sp];
-            if (!aabbOverlaps(qmin, qmax, xyz(s.bvhMin[node]), xyz(s.bvhMax[node]))) continue;
-            if (node >= n - 1u) {
-                const uint32_t cB = s.colQueryOrder[s.bvhValA[node - (n - 1u)]];
-                if (cB == cA) continue;
-                const cn_collider_broadphase b = s.colBp[cB];
-                if (b.owner_body == a.owner_body) continue;
-                const bool bMoving = s.bodyType[b.owner_body] != CN_BODY_STATIC;
-                if (bMoving && cB < cA) continue;
-                if (!broadPhaseCollide(a, b)) continue;
-                if (kEmit) {
-                    if (write >= s.rrCapacity) return;
-                    // CanonicalizeRigidPair (physics_rigid_types.hlsli:282-305): lower shape type first
-                    s.rrPairs[write++] = a.shape_type > b.shape_type ? make_uint2(cB, cA) : make_uint2(cA, cB);
-                } else {
-                    ++count;
-                }
-                continue;
+        // a full stack skips the subtree, as the reference's 128-entry traversal stack does
+        bvhQuery<kBvhStack>(s, qmin, qmax, [&](uint32_t leaf) -> bool {
+            const uint32_t cB = s.colQueryOrder[s.bvhValA[leaf]];
+            if (cB == cA) return true;
+            const cn_collider_broadphase b = s.colBp[cB];
+            if (b.owner_body == a.owner_body) return true;
+            const bool bMoving = s.bodyType[b.owner_body] != CN_BODY_STATIC;
+            if (bMoving && cB < cA) return true;
+            if (!broadPhaseCollide(a, b)) return true;
+            if (kEmit) {
+                if (write >= s.rrCapacity) return false;
+                // CanonicalizeRigidPair (physics_rigid_types.hlsli:282-305): lower shape type first
+                s.rrPairs[write++] = a.shape_type > b.shape_type ? make_uint2(cB, cA) : make_uint2(cA, cB);
+            } else {
+                ++count;
             }
-            const uint2 ch = s.bvhChildren[node];
-            if (sp < kBvhStack) stack[sp++] = ch.y;
-            if (sp < kBvhStack) stack[sp++] = ch.x;
-        }
+            return true;
+        });
     }
     if (!kEmit) s.rrCount[k] = count;
 }
@@ -1227,16 +1224,18 @@ void launchRigidBroadphaseAndContacts(const Scene &s, const Config &c, void *scr
     uint32_t *total = static_cast<uint32_t *>(scratch);
     void *work = static_cast<uint8_t *>(scratch) + 256;
     if (n >= 2) {
-        k_bvhBounds<<<1, kRigidThreads, 0, st>>>(s);
+        k_bvhBounds<<<1, kBoundsThreads, 0, st>>>(s);
         k_bvhMorton<<<blocksOf(n), kRigidThreads, 0, st>>>(s);
         radixSortPairs(s.bvhKeyA, s.bvhValA, s.bvhKeyB, s.bvhValB, n, work, &s.meta_->waitTimeouts, st);
         k_bvhBuild<<<blocksOf(n - 1), kRigidThreads, 0, st>>>(s);
         cudaMemsetAsync(s.bvhVisits, 0, sizeof(uint32_t) * (n - 1), st);
         k_bvhRefit<<<blocksOf(n), kRigidThreads, 0, st>>>(s);
     }
-    k_rigidPairs<false><<<blocksOf(s.activeMovingCount), kRigidThreads, 0, st>>>(s, nullptr);
+    // one warp per block: the walks are latency-bound chains, so they go to as many SMs as possible
+    const unsigned pairBlocks = unsigned((s.activeMovingCount + 31u) / 32u);
+    k_rigidPairs<false><<<pairBlocks, 32, 0, st>>>(s, nullptr);
     exclusiveScan(s.rrCount, s.rrOffset, s.activeMovingCount, total, work, st);
-    k_rigidPairs<true><<<blocksOf(s.activeMovingCount), kRigidThreads, 0, st>>>(s, total);
+    k_rigidPairs<true><<<pairBlocks, 32, 0, st>>>(s, total);
     k_rigidNarrowPhase<<<blocksOf(s.rrCapacity), kRigidThreads, 0, st>>>(s, c);
 }
 

@@ -219,6 +219,7 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
         s.bvhChildren = a.take<uint2>(C);
         s.bvhParent = a.take<uint32_t>(2 * C); s.bvhVisits = a.take<uint32_t>(C);
         s.bvhMin = a.take<float4>(2 * C); s.bvhMax = a.take<float4>(2 * C);
+        s.bvhWide = a.take<float4>(4 * C);
         s.bvhBounds = a.take<float4>(2);
         sv->rigidScratch = a.take<uint8_t>(cn::rigidScratchBytes(C, K));
     }
