@@ -152,6 +152,7 @@ struct Scene {
     uint32_t rrCapacity = 0;
     uint32_t *rrCount = nullptr, *rrOffset = nullptr;     // per moving collider
     uint2 *rrPairs = nullptr;                              // (collider A, collider B), canonical
+    uint2 *rrStage = nullptr;                              // per moving collider: its first pairs
     RigidPairContact *rrContacts = nullptr;
     RigidSlot *rrSlots = nullptr;                          // per sorted contact
     uint32_t *rrKeyA = nullptr, *rrValA = nullptr, *rrKeyB = nullptr, *rrValB = nullptr;

@@ -157,43 +157,67 @@ __global__ void k_bvhRefit(Scene s)
 }
 
 // physics_rigid_count_pairs / emit_pairs.cs.hlsl: moving collider k of the query order walks
-// the tree; a moving partner counts once (higher collider index), a static one always.
-template <bool kEmit>
-__global__ void k_rigidPairs(Scene s, const uint32_t *total)
+// the tree; a moving partner counts once (higher collider index), a static one always.  The count
+// pass also stages the first kPairStage canonical pairs of its walk (rrStage, kPairStage per
+// moving collider), so the emit pass copies them to their scanned offsets and walks again only
+// for a collider with more partners: one walk per collider, the same pairs in the same order.
+constexpr uint32_t kPairStage = 32u;
+
+template <class F>
+__device__ __forceinline__ void walkPairs(const Scene &s, uint32_t cA, F &&emit)
+{
+    const cn_collider_broadphase a = s.colBp[cA];
+    const f3 qmin = xyz(s.colAabbMin[cA]), qmax = xyz(s.colAabbMax[cA]);
+    // a full stack skips the subtree, as the reference's 128-entry traversal stack does
+    bvhQuery<kBvhStack>(s, qmin, qmax, [&](uint32_t leaf) -> bool {
+        const uint32_t cB = s.colQueryOrder[s.bvhValA[leaf]];
+        if (cB == cA) return true;
+        const cn_collider_broadphase b = s.colBp[cB];
+        if (b.owner_body == a.owner_body) return true;
+        const bool bMoving = s.bodyType[b.owner_body] != CN_BODY_STATIC;
+        if (bMoving && cB < cA) return true;
+        if (!broadPhaseCollide(a, b)) return true;
+        // CanonicalizeRigidPair (physics_rigid_types.hlsli:282-305): lower shape type first
+        return emit(a.shape_type > b.shape_type ? make_uint2(cB, cA) : make_uint2(cA, cB));
+    });
+}
+
+__global__ void k_rigidPairsCount(Scene s)
 {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (kEmit && k == 0) {
+    if (k >= s.activeMovingCount) return;
+    uint32_t count = 0;
+    uint2 *stage = s.rrStage + size_t(k) * kPairStage;
+    if (s.colQueryCount >= 2u)
+        walkPairs(s, s.colQueryOrder[k], [&](uint2 pr) -> bool {
+            if (count < kPairStage) stage[count] = pr;
+            ++count;
+            return true;
+        });
+    s.rrCount[k] = count;
+}
+
+__global__ void k_rigidPairsEmit(Scene s, const uint32_t *total)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k == 0) {
         s.meta_->requiredRigidRigidPairs = *total;
         s.meta_->rigidRigidPairCount = min(*total, s.rrCapacity);
         s.meta_->rigidContactSlots = kRigidPairContacts * min(*total, s.rrCapacity);
     }
     if (k >= s.activeMovingCount) return;
-    const uint32_t n = s.colQueryCount;
-    const uint32_t cA = s.colQueryOrder[k];
-    const cn_collider_broadphase a = s.colBp[cA];
-    const f3 qmin = xyz(s.colAabbMin[cA]), qmax = xyz(s.colAabbMax[cA]);
-    uint32_t count = 0, write = kEmit ? s.rrOffset[k] : 0u;
-    if (n >= 2u) {
-        // a full stack skips the subtree, as the reference's 128-entry traversal stack does
-        bvhQuery<kBvhStack>(s, qmin, qmax, [&](uint32_t leaf) -> bool {
-            const uint32_t cB = s.colQueryOrder[s.bvhValA[leaf]];
-            if (cB == cA) return true;
-            const cn_collider_broadphase b = s.colBp[cB];
-            if (b.owner_body == a.owner_body) return true;
-            const bool bMoving = s.bodyType[b.owner_body] != CN_BODY_STATIC;
-            if (bMoving && cB < cA) return true;
-            if (!broadPhaseCollide(a, b)) return true;
-            if (kEmit) {
-                if (write >= s.rrCapacity) return false;
-                // CanonicalizeRigidPair (physics_rigid_types.hlsli:282-305): lower shape type first
-                s.rrPairs[write++] = a.shape_type > b.shape_type ? make_uint2(cB, cA) : make_uint2(cA, cB);
-            } else {
-                ++count;
-            }
-            return true;
-        });
+    const uint32_t count = s.rrCount[k];
+    uint32_t write = s.rrOffset[k];
+    if (count <= kPairStage) {
+        const uint2 *stage = s.rrStage + size_t(k) * kPairStage;
+        for (uint32_t j = 0; j < count && write < s.rrCapacity; ++j) s.rrPairs[write++] = stage[j];
+        return;
     }
-    if (!kEmit) s.rrCount[k] = count;
+    walkPairs(s, s.colQueryOrder[k], [&](uint2 pr) -> bool {
+        if (write >= s.rrCapacity) return false;
+        s.rrPairs[write++] = pr;
+        return true;
+    });
 }
 
 // ------------------------------------------------------------------------------ narrow phase
@@ -1233,9 +1257,9 @@ void launchRigidBroadphaseAndContacts(const Scene &s, const Config &c, void *scr
     }
     // one warp per block: the walks are latency-bound chains, so they go to as many SMs as possible
     const unsigned pairBlocks = unsigned((s.activeMovingCount + 31u) / 32u);
-    k_rigidPairs<false><<<pairBlocks, 32, 0, st>>>(s, nullptr);
+    k_rigidPairsCount<<<pairBlocks, 32, 0, st>>>(s);
     exclusiveScan(s.rrCount, s.rrOffset, s.activeMovingCount, total, work, st);
-    k_rigidPairs<true><<<pairBlocks, 32, 0, st>>>(s, total);
+    k_rigidPairsEmit<<<pairBlocks, 32, 0, st>>>(s, total);
     k_rigidNarrowPhase<<<blocksOf(s.rrCapacity), kRigidThreads, 0, st>>>(s, c);
 }
 
