@@ -121,6 +121,8 @@ struct Scene {
     const uint2 *tetRanges = nullptr, *tetInc = nullptr;
     const uint2 *segRanges = nullptr, *segInc = nullptr;
     const uint2 *segJointRanges = nullptr, *segJointInc = nullptr;
+    // per family: the particles [x, y) with records (a single world's apply window)
+    uint2 edgeWin{0u, 0u}, bendWin{0u, 0u}, tetWin{0u, 0u}, segWin{0u, 0u};
     // lambdas and per-constraint correction records
     float *edgeLambda = nullptr, *bendLambda = nullptr, *tetLambda = nullptr, *distLambda = nullptr;
     float4 *segLambda = nullptr, *jointLambda = nullptr;

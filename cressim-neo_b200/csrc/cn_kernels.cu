@@ -1195,10 +1195,17 @@ __device__ __forceinline__ void applyPairAt(const Scene &s, const uint2 *ranges,
     applyGatherAt<2u>(s, ranges, inc, corr, i);
 }
 
+// A single world applies over `win`, the particles [lo, hi) that the family touches (bodies are
+// contiguous in the particle order; the others have no records and keep x); a batch over its tiles.
 __global__ void __launch_bounds__(kThreads) k_applyPair(Scene s, const uint2 *ranges, const uint2 *inc,
-                                                        const float4 *corr)
+                                                        const float4 *corr, uint2 win)
 {
-    forEachElem(s.wP, s.N, [&](uint32_t i) { applyPairAt(s, ranges, inc, corr, i); });
+    if (s.wP.tiles) {
+        forEachElem(s.wP, s.N, [&](uint32_t i) { applyPairAt(s, ranges, inc, corr, i); });
+        return;
+    }
+    const uint32_t i = win.x + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < win.y) applyPairAt(s, ranges, inc, corr, i);
 }
 
 // physics_soft_apply_tet_corrections.cs.hlsl:9-50, physics_soft_apply_bend_corrections.cs.hlsl:9-51
@@ -1208,9 +1215,14 @@ __device__ __forceinline__ void applyQuadAt(const Scene &s, const uint2 *ranges,
 }
 
 __global__ void __launch_bounds__(kThreads) k_applyQuad(Scene s, const uint2 *ranges, const uint2 *inc,
-                                                        const float4 *corr)
+                                                        const float4 *corr, uint2 win)
 {
-    forEachElem(s.wP, s.N, [&](uint32_t i) { applyQuadAt(s, ranges, inc, corr, i); });
+    if (s.wP.tiles) {
+        forEachElem(s.wP, s.N, [&](uint32_t i) { applyQuadAt(s, ranges, inc, corr, i); });
+        return;
+    }
+    const uint32_t i = win.x + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < win.y) applyQuadAt(s, ranges, inc, corr, i);
 }
 
 // physics_soft_solve_tet_constraints.cs.hlsl:15-87
@@ -2497,12 +2509,18 @@ void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)
     k_fluidNeighborsDensity<0u, false><<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u, nullptr);
 }
 
+// Grid of an apply pass: the batch's work list, else the family's particle window.
+inline unsigned applyGrid(const Scene &s, uint2 win)
+{
+    return s.wP.tiles ? gridFor(s.wP, s.N) : blocksFor(win.y > win.x ? win.y - win.x : 0u);
+}
+
 void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st)
 {
     const float relax = c.softInternalRelaxation;
     if (s.E) {
         k_solveEdges<<<gridFor(s.wE, s.E), kThreads, 0, st>>>(s, dt, relax);
-        k_applyPair<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, s.edgeRanges, s.edgeInc, s.edgeCorr);
+        k_applyPair<<<applyGrid(s, s.edgeWin), kThreads, 0, st>>>(s, s.edgeRanges, s.edgeInc, s.edgeCorr, s.edgeWin);
     }
     if (s.S) {
         k_solveSegments<<<blocksFor(s.S), kThreads, 0, st>>>(s, dt, relax);
@@ -2511,7 +2529,7 @@ void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t
     if (s.Bn || s.D) {
         if (s.Bn) k_solveBends<<<blocksFor(s.Bn), kThreads, 0, st>>>(s, dt, relax);
         if (s.D) k_solveDihedrals<<<blocksFor(s.D), kThreads, 0, st>>>(s, dt, relax);
-        k_applyQuad<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.bendRanges, s.bendInc, s.bendCorr);
+        k_applyQuad<<<applyGrid(s, s.bendWin), kThreads, 0, st>>>(s, s.bendRanges, s.bendInc, s.bendCorr, s.bendWin);
     }
     if (s.J) {
         k_solveJoints<<<blocksFor(s.J), kThreads, 0, st>>>(s, dt, relax);
@@ -2519,11 +2537,11 @@ void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t
     }
     if (s.SD) {
         k_solveDistances<<<blocksFor(s.SD), kThreads, 0, st>>>(s, dt, relax);
-        k_applyPair<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.segRanges, s.segInc, s.distCorr);
+        k_applyPair<<<applyGrid(s, s.segWin), kThreads, 0, st>>>(s, s.segRanges, s.segInc, s.distCorr, s.segWin);
     }
     if (s.T) {
         k_solveTets<<<gridFor(s.wT, s.T), kThreads, 0, st>>>(s, dt, relax);
-        k_applyQuad<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, s.tetRanges, s.tetInc, s.tetCorr);
+        k_applyQuad<<<applyGrid(s, s.tetWin), kThreads, 0, st>>>(s, s.tetRanges, s.tetInc, s.tetCorr, s.tetWin);
     }
 }
 
