@@ -30,6 +30,8 @@ constexpr bool kInterleavedLists = true;
 constexpr bool kInterleavedLists = false;
 #endif
 inline unsigned blocksFor(size_t n) { return n == 0 ? 1u : unsigned((n + kThreads - 1) / kThreads); }
+// Grid of a kernel that strides over a device-counted list of capacity n: 16 blocks per SM at most.
+inline unsigned pairGrid(size_t n) { return std::min<unsigned>(blocksFor(n), 148u * 16u); }
 // Per-slot fluid word: bit 31 = fluid particle, bits 16..30 = fluid material, bits 0..15 = filter
 // group (a dense id of the particle's (environment, layer, mask) triple).  P.w carries the same
 // word with bit 31 meaning "fluid and invMass > kEps" (the neighbour candidate filter).
@@ -1543,12 +1545,8 @@ __device__ __forceinline__ void atomicAdd3(float4 *p, f3 v)
 // Contacts
 // ------------------------------------------------------------------------------------------
 // physics_particle_generate_explicit_contacts.cs.hlsl (no suturing state, no rigid proxies)
-__global__ void __launch_bounds__(kThreads) k_particleContactGenerate(Scene s)
+__device__ __forceinline__ void particleContactGenerateAt(const Scene &s, uint32_t pi)
 {
-    const uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t count = s.meta_->particlePairCount;
-    if (pi == 0) s.meta_->activeParticleContacts = 0u;
-    if (pi >= count) return;
     ParticleContact out{};
     const uint2 pr = s.particlePairs[pi];
     const uint32_t a = pr.x, b = pr.y;
@@ -1571,6 +1569,15 @@ __global__ void __launch_bounds__(kThreads) k_particleContactGenerate(Scene s)
         }
     }
     s.particleContacts[pi] = out;
+}
+
+__global__ void __launch_bounds__(kThreads) k_particleContactGenerate(Scene s)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) s.meta_->activeParticleContacts = 0u;
+    // a fixed grid strides over the pairs that exist (a device count), not the capacity
+    const uint32_t count = s.meta_->particlePairCount;
+    for (uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x; pi < count; pi += gridDim.x * blockDim.x)
+        particleContactGenerateAt(s, pi);
 }
 
 // The rigid side of a proxy particle in a particle-particle contact: its body (inverse mass only
@@ -1601,10 +1608,8 @@ __device__ __forceinline__ f3 proxyPreviousPoint(const Scene &s, uint32_t p, uin
 // physics_particle_solve_explicit_contacts.cs.hlsl; float atomics as in the reference.  A rigid
 // proxy's share goes to its body's translation / rotation sums (effective mass with the lever
 // arm); every other particle's to its position correction.
-__global__ void __launch_bounds__(kThreads) k_particleContactSolve(Scene s, Config cfg)
+__device__ __forceinline__ void particleContactSolveAt(const Scene &s, const Config &cfg, uint32_t pi)
 {
-    const uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pi >= s.meta_->particlePairCount) return;
     const ParticleContact c = s.particleContacts[pi];
     if (c.active == 0u) return;
     atomicAdd(&s.meta_->activeParticleContacts, 1u);
@@ -1676,6 +1681,14 @@ __global__ void __launch_bounds__(kThreads) k_particleContactSolve(Scene s, Conf
         atomicAdd3(&s.bodyTransCorr[psB.body], tB);
         atomicAdd3(&s.bodyRotCorr[psB.body], rB);
     }
+}
+
+__global__ void __launch_bounds__(kThreads) k_particleContactSolve(Scene s, Config cfg)
+{
+    // a fixed grid strides over the pairs that exist (a device count), not the capacity
+    const uint32_t count = s.meta_->particlePairCount;
+    for (uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x; pi < count; pi += gridDim.x * blockDim.x)
+        particleContactSolveAt(s, cfg, pi);
 }
 
 // Particle-rigid contact for candidate pair `pi`: physics_particle_rigid_generate_contacts.cs.hlsl:29-210
@@ -2165,10 +2178,8 @@ __global__ void k_applyRigidContactVelocities(Scene s, Config cfg)
 // physics_particle_solve_contact_velocities.cs.hlsl with float atomics: a rigid proxy moves with
 // its body's velocity at the proxy's lever arm, and its impulse share goes to the body's
 // velocity sums.
-__global__ void __launch_bounds__(kThreads) k_particleContactVelocities(Scene s, Config cfg)
+__device__ __forceinline__ void particleContactVelocitiesAt(const Scene &s, const Config &cfg, uint32_t pi)
 {
-    const uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (pi >= s.meta_->particlePairCount) return;
     const ParticleContact c = s.particleContacts[pi];
     if (c.active == 0u) return;
     float iA = s.x[c.a].w, iB = s.x[c.b].w;
@@ -2211,6 +2222,14 @@ __global__ void __launch_bounds__(kThreads) k_particleContactVelocities(Scene s,
         atomicAdd3(&s.bodyLinVelCorr[psB.body], ti * iB);
         atomicAdd3(&s.bodyAngVelCorr[psB.body], mulWorldInvInertia(psB.invI, psB.q, cross(psB.r, ti)));
     }
+}
+
+__global__ void __launch_bounds__(kThreads) k_particleContactVelocities(Scene s, Config cfg)
+{
+    // a fixed grid strides over the pairs that exist (a device count), not the capacity
+    const uint32_t count = s.meta_->particlePairCount;
+    for (uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x; pi < count; pi += gridDim.x * blockDim.x)
+        particleContactVelocitiesAt(s, cfg, pi);
 }
 
 // physics_particle_apply_contact_velocities.cs.hlsl
@@ -2550,8 +2569,8 @@ void launchContacts(const Scene &s, const Config &c, bool particleContacts, bool
 {
     if (particleContacts) {
         const uint32_t cap = s.particlePairCapacity;
-        k_particleContactGenerate<<<blocksFor(cap), kThreads, 0, st>>>(s);
-        k_particleContactSolve<<<blocksFor(cap), kThreads, 0, st>>>(s, c);
+        k_particleContactGenerate<<<pairGrid(cap), kThreads, 0, st>>>(s);
+        k_particleContactSolve<<<pairGrid(cap), kThreads, 0, st>>>(s, c);
     }
     if (rigidContacts) k_rigidContacts<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, c, !particleContacts);
     if (particleContacts) k_applyPositionCorrections<<<blocksFor(s.N), kThreads, 0, st>>>(s);
@@ -2598,7 +2617,7 @@ void launchRigidContactVelocitiesDynamic(const Scene &s, uint32_t iterations, co
 void launchParticleContactVelocities(const Scene &s, uint32_t iterations, const Config &c, cudaStream_t st)
 {
     for (uint32_t it = 0; it < iterations; ++it) {
-        k_particleContactVelocities<<<blocksFor(s.particlePairCapacity), kThreads, 0, st>>>(s, c);
+        k_particleContactVelocities<<<pairGrid(s.particlePairCapacity), kThreads, 0, st>>>(s, c);
         k_applyContactVelocities<<<blocksFor(s.N), kThreads, 0, st>>>(s);
         // the bodies' sums (only proxies of dynamic bodies add to them)
         if (s.hasDynamic && s.nProxy) k_applyRigidContactVelocities<<<blocksFor(s.B), kThreads, 0, st>>>(s, c);
