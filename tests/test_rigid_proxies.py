@@ -213,3 +213,52 @@ def test_small_rigid_pile_with_proxy_bodies_matches_the_oracle():
         assert m["required_proxy_rigid_contact_count"] == om["required_proxy_contacts"], k
     pg, po = gpu.read_rigid_bodies()[0], ora.read_rigid_bodies()[0]
     assert np.abs(pg[:, :3] - po[:, :3]).max() < 1e-3   # the drift bar: contact order and float atomics
+
+
+@pytest.mark.gpu
+def test_kinematic_proxy_tool_stirs_fluid_like_the_oracle():
+    """Proxy particles of a kinematic tool moving through a fluid block: explicit fluid-proxy
+    contacts (the proxy side immovable), the fluid solve with its superset lists validated by each
+    particle's move, GPU against the oracle."""
+    w = World()
+    w.add_fluid_grid((0.3, 0.2, 0.3), 0.02, position=(0.0, 0.11, 0.0), radius=0.012)
+    scenes.ground(w)
+    tool = w.add_rigid_body("kinematic", position=(0.0, 0.12, 0.0))
+    rod = [(0.0, 0.025 * k - 0.05, 0.0) for k in range(5)]
+    w.set_rigid_proxy_particles(tool, rod, 0.02, friction=0.2)
+    desc = solver_desc(substeps=2, default_iterations=4, fluid_iterations=4)
+    gpu, ora = pair(w, desc)
+    touched = 0
+    for k in range(6):
+        target = (0.01 * (k + 1), 0.12, 0.0)
+        gpu.set_kinematic_target(tool, target)
+        ora.set_kinematic_target(tool, target)
+        gpu.step(1.0 / 120.0)
+        ora.step(1.0 / 120.0)
+        n = gpu.validate_gpu_meta()["active_particle_contact_count"]
+        assert n == ora.meta()["active_particle_contacts"], k   # contacts of the last iteration
+        touched = max(touched, n)
+    xg, vg, _ = gpu.read_particles()
+    xo, vo, _ = ora.read_particles()
+    np.testing.assert_allclose(xg[:5], xo[:5], rtol=1e-6, atol=1e-6)       # the proxies: the tool's pose
+    np.testing.assert_allclose(xg, xo, rtol=1e-4, atol=1e-5)               # float atomics in the contacts
+    assert touched > 0
+
+
+@pytest.mark.gpu
+def test_incremental_update_moves_proxy_points():
+    """cn_solver_update_world with the particle attributes uploads new proxy local positions:
+    the proxies take them at the next substep's sync, as after a full sync."""
+    w, b = proxy_drop(y0=0.5)
+    soa = w.soa()
+    gpu = Solver(solver_desc(**DESC))
+    gpu.sync_world(soa)
+    gpu.step(1.0 / 60.0)
+    local = np.ctypeslib.as_array(soa.rigid_proxy_local_positions, (soa.particle_count, 4))
+    local[:27, :3] *= 1.5
+    gpu.update_world(soa, "particle_attributes")
+    gpu.step(1.0 / 60.0)
+    x = gpu.read_particles()[0]
+    p, q = gpu.read_rigid_bodies()[:2]
+    want = np.array([qrot(q[b], local[k, :3]) + p[b, :3] for k in range(27)])
+    np.testing.assert_allclose(x[:27, :3], want, atol=2e-5)
