@@ -188,6 +188,22 @@ __global__ void __launch_bounds__(kThreads) k_rigidPredict(Scene s, float dt, fl
     forEachInBlock(s.wC, s.C, [&](uint32_t c) { colliderFrame(s, c); });
 }
 
+// The same in two grid-wide launches (bodies, then colliders), for a single world with many bodies:
+// one block would walk them all in turn.
+__global__ void __launch_bounds__(kThreads) k_rigidPredictBodies(Scene s, float dt, float gx, float gy, float gz)
+{
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < s.B) rigidPredictBody(s, dt, gx, gy, gz, b);
+}
+
+__global__ void __launch_bounds__(kThreads) k_colliderBoundsFrames(Scene s)
+{
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= s.C) return;
+    colliderAabb(s, c);
+    colliderFrame(s, c);
+}
+
 __global__ void k_applyBodyTargets(Scene s, const BodyTarget *list, const uint32_t *count)
 {
     const uint32_t n = *count;
@@ -2394,6 +2410,11 @@ __global__ void __launch_bounds__(kThreads) k_surfaceWorldBounds(Scene s)
 void launchRigidPredict(const Scene &s, float dt, float gx, float gy, float gz, cudaStream_t st)
 {
     if (s.B == 0 && s.C == 0) return;
+    if (!s.wB.tiles && s.B + s.C > 4u * kThreads) {
+        if (s.B) k_rigidPredictBodies<<<blocksFor(s.B), kThreads, 0, st>>>(s, dt, gx, gy, gz);
+        if (s.C) k_colliderBoundsFrames<<<blocksFor(s.C), kThreads, 0, st>>>(s);
+        return;
+    }
     k_rigidPredict<<<1, kThreads, 0, st>>>(s, dt, gx, gy, gz);
 }
 
