@@ -161,7 +161,7 @@ __global__ void k_bvhRefit(Scene s)
 // pass also stages the first kPairStage canonical pairs of its walk (rrStage, kPairStage per
 // moving collider), so the emit pass copies them to their scanned offsets and walks again only
 // for a collider with more partners: one walk per collider, the same pairs in the same order.
-constexpr uint32_t kPairStage = 32u;
+constexpr uint32_t kPairStage = 64u;
 
 template <class F>
 __device__ __forceinline__ void walkPairs(const Scene &s, uint32_t cA, F &&emit)

@@ -205,7 +205,7 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
         s.rrCapacity = P;
         s.proxyCapacity = sv->proxyContacts ? std::max<uint32_t>(64u, 8u * sv->nProxy) : 0u;
         s.rrCount = a.take<uint32_t>(C); s.rrOffset = a.take<uint32_t>(C);
-        s.rrStage = a.take<uint2>(size_t(C) * 32u); // kPairStage per collider
+        s.rrStage = a.take<uint2>(size_t(C) * 64u); // kPairStage per collider
         const uint32_t K = P * cn::kRigidPairContacts + s.proxyCapacity;
         s.rrSlotCapacity = K;
         s.rrPairs = a.take<uint2>(P);
