@@ -250,6 +250,7 @@ struct Scene {
     uint32_t rigidPairCapacity = 0;
     RigidContact *rigidContacts = nullptr;
     uint2 *particlePairs = nullptr;   // (a, b)
+    uint2 *ppStage = nullptr;         // per particle: its first pairs, staged by the count pass
     uint32_t particlePairCapacity = 0;
     ParticleContact *particleContacts = nullptr;
     DeviceMeta *meta_ = nullptr;

@@ -611,6 +611,8 @@ __device__ __forceinline__ bool isAdjacent(const Scene &s, uint32_t p, uint32_t 
     return false;
 }
 
+constexpr uint32_t kPairStageP = 8u; // staged particle-particle pairs per particle
+
 template <bool kEmit>
 __global__ void __launch_bounds__(kThreads) k_particleCandidates(Scene s, const uint32_t *total)
 {
@@ -621,6 +623,14 @@ __global__ void __launch_bounds__(kThreads) k_particleCandidates(Scene s, const 
     }
     if (i >= s.N) return;
     if (kEmit && s.ppCount[i] == 0u) return;
+    // The count pass stages a particle's first kPairStageP pairs; the emit pass copies them to
+    // their scanned offsets and walks again only for a particle with more.
+    uint2 *stage = s.ppStage + size_t(i) * kPairStageP;
+    if (kEmit && s.ppCount[i] <= kPairStageP) {
+        uint32_t write = s.ppOffset[i];
+        for (uint32_t k = 0; k < s.ppCount[i] && write < s.particlePairCapacity; ++k) s.particlePairs[write++] = stage[k];
+        return;
+    }
     const uint32_t kind = s.kinds[i];
     // Pairs go from the lower index up and fluid-fluid pairs are excluded: a fluid particle past
     // every solid (the world packs fluids last) has no candidate to walk for.
@@ -671,6 +681,7 @@ __global__ void __launch_bounds__(kThreads) k_particleCandidates(Scene s, const 
                         if (write >= s.particlePairCapacity) return;
                         s.particlePairs[write++] = make_uint2(i, c);
                     } else {
+                        if (count < kPairStageP) stage[count] = make_uint2(i, c);
                         ++count;
                     }
                 }

@@ -300,6 +300,7 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
     }
     if (sv->ppPossible) {
         s.ppCount = a.take<uint32_t>(N);
+        s.ppStage = a.take<uint2>(size_t(N) * 8u); // kPairStageP per particle
         s.ppOffset = a.take<uint32_t>(N);
         s.particlePairCapacity = std::max<uint32_t>(N * 8u, 64u);
         s.particlePairs = a.take<uint2>(s.particlePairCapacity);
