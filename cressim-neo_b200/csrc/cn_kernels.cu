@@ -878,7 +878,7 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidNeighborsDen
             uint32_t cc[4];
             float4 qq[4];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) cc[j] = (k + j < n) ? sup[(k + j) * lstr] : slot;
+            for (int j = 0; j < 4; ++j) cc[j] = (k + j < n) ? __ldcs(&sup[(k + j) * lstr]) : slot;
 #pragma unroll
             for (int j = 0; j < 4; ++j) qq[j] = ld4(&s.P[cc[j]]);
 #pragma unroll
@@ -1039,8 +1039,8 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidDeltaApplyCl
         // A neighbour's accumulated delta (xyz, used from the second iteration on) and density
         // constraint (w, stored there by the density kernel) come in one load.
         const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
-        uint32_t cN = cnt > 0 ? lst[0] : 0u;
-        uint32_t cNN = cnt > 1 ? lst[lstr] : 0u;
+        uint32_t cN = cnt > 0 ? __ldcs(&lst[0]) : 0u; // list words are read once: streaming loads
+        uint32_t cNN = cnt > 1 ? __ldcs(&lst[lstr]) : 0u;
         float4 npN = cnt > 0 ? ld4(&s.P[cN]) : zero4;
         float4 dN = cnt > 0 ? ld4(&Dcur[cN]) : zero4;
         for (uint32_t k = 0; k < cnt; ++k) {
@@ -1050,7 +1050,7 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidDeltaApplyCl
             const float4 nd4 = dN;
             if (k + 1 < cnt) {
                 cN = cNN;
-                if (k + 2 < cnt) cNN = lst[(k + 2) * lstr];
+                if (k + 2 < cnt) cNN = __ldcs(&lst[(k + 2) * lstr]);
                 npN = ld4(&s.P[cN]);
                 dN = ld4(&Dcur[cN]);
             }
