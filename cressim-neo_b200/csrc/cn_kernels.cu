@@ -937,12 +937,12 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidNeighborsDen
                         if (d2 >= rec2) return;
                         if (c == slot || !neighborAllowed(s, __float_as_uint(q.w), myGroup, selfCompat, m, c)) return;
                         if (buildSup) {
-                            if (supN < s.supCap) sup[supN * lstr] = c;
+                            if (supN < s.supCap) __stcs(&sup[supN * lstr], c); // written once, read later
                             ++supN;
                         }
                         if (d2 >= h2) return;
                         if (count >= maxN) { truncated = 1; return; }
-                        out[count++ * lstr] = c;
+                        __stcs(&out[count++ * lstr], c);
                         if (density) {
                             const float dist = sqrtf(d2);
                             rho += spikyWk(dist, h, invH, kW);
