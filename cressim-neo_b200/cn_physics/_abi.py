@@ -295,7 +295,7 @@ SIGNATURES = [
     ("cn_solver_set_timing", C.c_int, [C.c_void_p, u32]),
     ("cn_solver_kernel_times", C.c_int, [C.c_void_p, C.c_void_p, u32, P_u32]),
     ("cn_solver_graph_stats", C.c_int, [C.c_void_p, P_u32, P_u32]),
-    ("cn_sort_cell_keys_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, u32, C.c_void_p]),
+    ("cn_sort_cell_keys_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, u32, C.c_void_p, C.c_void_p]),
     ("cn_solver_debug_read", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     ("cn_batch_desc_defaults", None, [C.POINTER(BatchDesc)]),
     ("cn_batch_create", C.c_int, [C.POINTER(BatchDesc), C.c_int, C.POINTER(C.c_void_p)]),

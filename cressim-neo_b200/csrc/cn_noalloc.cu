@@ -33,7 +33,9 @@ uint32_t *g_scratchPtr[kMaxDevices] = {};
 
 // Device address of the scratch array on the current device.  In host code the array's name is
 // only a host-side stand-in, so the address must come from cudaGetSymbolAddress, once per device
-// with that device current.
+// with that device current.  The address is cached for the life of the process: after
+// cudaDeviceReset (which unloads the module and may place the array elsewhere) the cached address
+// is stale, so this entry point must not be called on a device that has been reset.
 cn_status scratchForCurrentDevice(uint32_t **out)
 {
     int device = 0;
@@ -60,14 +62,25 @@ cn_status scratchForCurrentDevice(uint32_t **out)
 extern "C" {
 
 CN_API cn_status cn_sort_cell_keys_noalloc(const uint32_t *keys, uint32_t *sorted_keys, uint32_t *sorted_indices,
-                                           uint32_t count, void *stream)
+                                           uint32_t count, uint32_t *out_timeouts, void *stream)
 {
     if (count > kNoAllocMaxKeys)
         return cn::setError(CN_ERR_CAPACITY, "cn_sort_cell_keys_noalloc: " + std::to_string(count) +
                                                  " keys exceed the allocation-free limit of 1048576");
-    if (count == 0) return CN_OK;
+    if (count == 0) {
+        if (out_timeouts)
+            return cudaMemsetAsync(out_timeouts, 0, sizeof(uint32_t), static_cast<cudaStream_t>(stream)) == cudaSuccess
+                       ? CN_OK
+                       : cn::setError(CN_ERR_CUDA, "cn_sort_cell_keys_noalloc: cudaMemsetAsync failed");
+        return CN_OK;
+    }
     if (!keys || !sorted_keys || !sorted_indices)
         return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_sort_cell_keys_noalloc: null device pointer");
+    // The sort works in place on (sorted_keys, sorted_indices) after copying the keys there, so an
+    // output that is the input would sort `keys` in place, and the two outputs must be distinct.
+    if (sorted_keys == keys || sorted_indices == keys || sorted_indices == sorted_keys)
+        return cn::setError(CN_ERR_INVALID_ARGUMENT,
+                            "cn_sort_cell_keys_noalloc: keys, sorted_keys and sorted_indices must not alias");
     if (cn::radixSortScratchBytes(count) > kMetaWords * sizeof(uint32_t))
         return cn::setError(CN_ERR_CAPACITY, "cn_sort_cell_keys_noalloc: sort metadata exceeds its reserved region");
     uint32_t *scratch = nullptr;
@@ -80,10 +93,17 @@ CN_API cn_status cn_sort_cell_keys_noalloc(const uint32_t *keys, uint32_t *sorte
     uint32_t *timeouts = valsB + kNoAllocMaxKeys;
     // The sort runs in place on (sorted_keys, sorted_indices) with the scratch arrays as the
     // ping-pong pair; it zeroes its histogram and look-back words itself.
-    cudaError_t e = cudaMemcpyAsync(sorted_keys, keys, size_t(count) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+    // The timeout word counts look-back waits that gave up during this call; it starts at zero.
+    cudaError_t e = cudaMemsetAsync(timeouts, 0, sizeof(uint32_t), s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(sorted_keys, keys, size_t(count) * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
     if (e != cudaSuccess)
         return cn::setError(CN_ERR_CUDA, std::string("cn_sort_cell_keys_noalloc: ") + cudaGetErrorString(e));
     cn::radixSortPairs(sorted_keys, sorted_indices, keysB, valsB, count, meta, timeouts, s);
+    // A nonzero count means a tile stopped waiting for an earlier tile's digit counts, so its
+    // offsets (and the output permutation) are wrong; the caller reads it once `stream` is done.
+    if (out_timeouts)
+        cudaMemcpyAsync(out_timeouts, timeouts, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
     e = cudaGetLastError();
     if (e != cudaSuccess)
         return cn::setError(CN_ERR_CUDA, std::string("cn_sort_cell_keys_noalloc: ") + cudaGetErrorString(e));

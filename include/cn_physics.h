@@ -789,9 +789,15 @@ CN_API cn_status cn_diff_memory(cn_diff *diff, uint64_t *bytes);
  * file-scope device array that every GPU loading the library keeps until exit; the first call on
  * a device looks its address up (cudaGetSymbolAddress), so make that first call before any stream
  * capture.  All calls share the array: calls that overlap on the GPU (different streams or
- * threads without ordering) race.  `keys` is not modified; `stream` may be NULL. */
+ * threads without ordering) race.  The cached address does not survive cudaDeviceReset: do not
+ * call this on a device that has been reset.  `keys`, `sorted_keys` and `sorted_indices` each
+ * hold `count` 32-bit words and must not alias one another (CN_ERR_INVALID_ARGUMENT); `keys` is
+ * not modified.  `out_timeouts` (a device pointer, may be NULL) receives the number of look-back
+ * waits that gave up; a nonzero value means the output permutation is invalid.  Outputs are
+ * ready once `stream` (may be NULL) has completed the work this call enqueued. */
 CN_API cn_status cn_sort_cell_keys_noalloc(const uint32_t *keys, uint32_t *sorted_keys,
-                                           uint32_t *sorted_indices, uint32_t count, void *stream);
+                                           uint32_t *sorted_indices, uint32_t count,
+                                           uint32_t *out_timeouts, void *stream);
 
 #ifdef __cplusplus
 }
