@@ -12,11 +12,12 @@
 // -ffp-contract=off so no multiply-add is fused.
 //
 // Parity status: the reference's GPU path (Vulkan/D3D12 through Diligent + DXC)
-// cannot be built or run here, and its tests pin no numeric output of the
-// substep, so this restatement is pinned only by the known answers the
-// reference's tests hold for scene authoring (regular-grid counts) and by the
-// golden fixtures generated from it under tests/golden/ ("parity unpinned" for
-// substep numerics).
+// cannot be built or run here, but its compute shaders can: oracle/ref_build.py
+// compiles them for the host and oracle/ref_driver.py runs them in the solver's
+// pass order.  Built with -DCN_ORACLE_QUOTIENTS (the shaders' own quotients in the
+// fluid kernels) this restatement reproduces those runs bit for bit on every
+// golden scene (tests/golden/ref_*.npz, tests/test_reference_pinned.py); the
+// default build differs only by the reciprocal products documented below.
 //
 // Deliberate restatement choices (documented where they occur):
 //  * rigid-BVH traversal order is replaced by "moving colliders, then static
@@ -219,10 +220,17 @@ inline f3 ProjectOntoTangent(f3 v, f3 n) { return v - n * dot(v, n); }
 // physics_fluid_common.hlsli:17-41.  A quotient by the smoothing radius or by a pair distance is
 // taken as the product with the correctly rounded reciprocal (SPIR-V's OpFDiv, which the shaders
 // compile to, is specified to 2.5 ulp rather than correctly rounded); the kernels do the same.
+// Built with CN_ORACLE_QUOTIENTS the oracle keeps the shaders' quotients instead: that build is
+// compared bit for bit with the reference's own kernels executed on the host (oracle/_ref).
+#ifdef CN_ORACLE_QUOTIENTS
+#define CN_DIV(a, b) ((a) / (b))
+#else
+#define CN_DIV(a, b) ((a) * (1.0f / (b)))
+#endif
 inline float SpikyW(float d, float h)
 {
     if (d >= h) return 0.0f;
-    const float om = 1.0f - d * (1.0f / h);
+    const float om = 1.0f - CN_DIV(d, h);
     const float h3 = h * h * h;
     const float k = 15.0f / (3.14159265359f * h3);
     return k * om * om;
@@ -230,22 +238,29 @@ inline float SpikyW(float d, float h)
 inline float SpikyDW(float d, float h)
 {
     if (d <= kEps || d >= h) return 0.0f;
-    const float invH = 1.0f / h;
-    const float om = 1.0f - d * invH;
+    const float om = 1.0f - CN_DIV(d, h);
     const float h3 = h * h * h;
     const float k = 15.0f / (3.14159265359f * h3);
-    return -2.0f * k * om * invH;
+    return CN_DIV(-2.0f * k * om, h);
+}
+inline f3 divv(f3 v, float d)
+{
+#ifdef CN_ORACLE_QUOTIENTS
+    return v / d;
+#else
+    return v * (1.0f / d);
+#endif
 }
 inline f3 SpikyGrad(f3 delta, float d, float h)
 {
     if (d <= kEps || d >= h) return f3{0, 0, 0};
     const float dw = SpikyDW(d, h);
-    return dw * (delta * (1.0f / d));
+    return dw * divv(delta, d);
 }
 inline float CohesionW(float d, float h, float c1, float c2)
 {
     if (d <= kEps || d >= h) return 0.0f;
-    const float q = d * (1.0f / h);
+    const float q = CN_DIV(d, h);
     return c1 * q * q * q + c2 * q * q - 1.0f;
 }
 
@@ -1135,7 +1150,7 @@ void fluidDeltaPositions(cno_solver &s, uint32_t iter, float dt)
             const float dist = length(delta);
             if (dist >= h || dist <= kEps) continue;
             const f4 nnc = s.fluidNormalC[c];
-            const f3 nij = delta * (1.0f / dist);
+            const f3 nij = divv(delta, dist);
             const float dw = SpikyDW(dist, h);
             f3 pd = -0.5f * (sC + nnc.w) * dw * nij;
             if (s.fluidMatIdx[i] == s.fluidMatIdx[c]) {
@@ -1160,7 +1175,7 @@ void fluidDeltaPositions(cno_solver &s, uint32_t iter, float dt)
             if (!FluidGhostDelta(s, c, sp, h, ghost)) continue;
             const float dist = length(ghost);
             if (dist <= kEps || dist >= h) continue;
-            const f3 nij = ghost * (1.0f / dist);
+            const f3 nij = divv(ghost, dist);
             const float dw = SpikyDW(dist, h);
             bd += -std::max(sC, 0.0f) * dw * nij;
         }

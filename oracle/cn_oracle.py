@@ -13,24 +13,27 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "libcn_oracle.so"
+# The same restatement with the shaders' own quotients in the fluid kernels (no reciprocal
+# products); compared bit for bit with the reference's kernels executed on the host.
+LIB_QUOTIENTS = HERE / "libcn_oracle_quot.so"
 
 DEBUG = {"cell_entries": 0, "sorted_keys": 1, "cell_ranges": 2, "fluid_neighbor_counts": 3,
          "fluid_neighbors": 4, "fluid_constraints": 5, "fluid_delta": 6, "rigid_contacts": 7}
 
-_lib = None
+_libs: dict = {}
 
 
 def build() -> Path:
-    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    subprocess.run(["make", "-s", "-C", str(HERE), "all", "quotients"], check=True)
     return LIB
 
 
-def load() -> C.CDLL:
-    global _lib
-    if _lib is None:
-        if not LIB.exists():
+def load(quotients: bool = False) -> C.CDLL:
+    path = LIB_QUOTIENTS if quotients else LIB
+    if path not in _libs:
+        if not path.exists():
             build()
-        lib = C.CDLL(str(LIB))
+        lib = C.CDLL(str(path))
         lib.cno_create.restype = C.c_void_p
         lib.cno_create.argtypes = [C.c_void_p, C.c_void_p]
         lib.cno_destroy.argtypes = [C.c_void_p]
@@ -47,8 +50,8 @@ def load() -> C.CDLL:
         lib.cno_fluid_material.argtypes = [C.c_float] * 7 + [C.c_void_p]
         lib.cno_read_surface_render.argtypes = [C.c_void_p] * 5
         lib.cno_read_rigid_bodies.argtypes = [C.c_void_p] * 5
-        _lib = lib
-    return _lib
+        _libs[path] = lib
+    return _libs[path]
 
 
 def set_threads(n: int) -> int:
@@ -58,8 +61,8 @@ def set_threads(n: int) -> int:
 class Oracle:
     """CPU restatement of PhysicsSolver::step over the same SoA the GPU solver receives."""
 
-    def __init__(self, desc, soa):
-        self._lib = load()
+    def __init__(self, desc, soa, quotients: bool = False):
+        self._lib = load(quotients)
         self._h = self._lib.cno_create(C.byref(desc), C.byref(soa))
         if not self._h:
             raise RuntimeError("oracle: create failed")

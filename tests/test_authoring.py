@@ -130,8 +130,10 @@ def test_tetgen_round_trip_matches_tet_mesh(tmp_path):
 
 
 def test_tetgen_reference_fixtures(tmp_path):
-    # The reference's own fixture files, read as text where the reference tree is present.
-    fx = Path("/root/reference/tests/physics/fixtures")
+    # The reference's own fixture files, read as text where the reference tree is present (its
+    # root is the one oracle/ref_build.py uses: CN_REFERENCE_ROOT or the default checkout).
+    import ref_build
+    fx = ref_build.DEFAULT_REFERENCE / "tests" / "physics" / "fixtures"
     if not (fx / "soft_body_simple.node").exists():
         pytest.skip("reference fixtures not present")
     ref = World()
