@@ -3,7 +3,8 @@
 CPU: the oracle still reproduces every file bit for bit (it may not drift).
 GPU: the sm_100a path, through the C ABI, reproduces every file bit for bit -- positions,
 velocities, previous positions, the sorted (cellKey, index) pairs, neighbour counts and the
-SHA-256 of the neighbour lists of the last substep.
+SHA-256 of the neighbour lists of the last substep -- except the scenes whose constraints go
+through acos (make_golden.TRANSCENDENTAL), held to 1e-5.
 """
 import sys
 from pathlib import Path
@@ -45,4 +46,30 @@ def _gpu_stepper(desc, soa):
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", NAMES)
 def test_gpu_reproduces_golden(name):
-    _compare(name, make_golden.run(_gpu_stepper, name))
+    got = make_golden.run(_gpu_stepper, name)
+    if name in make_golden.TRANSCENDENTAL:
+        make_golden.assert_state_close(name, got, np.load(GOLDEN / f"{name}.npz"))
+        return
+    _compare(name, got)
+
+
+def _gpu_default_stepper(desc, soa):
+    from cn_physics import Solver
+    s = Solver(desc)          # the shipped schedule: no debug flags
+    s.sync_world(soa)
+    return s
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", NAMES)
+def test_gpu_default_schedule_reproduces_golden_state(name):
+    """Without the post-update neighbour rebuild (which only feeds vorticity confinement and
+    render anisotropy) the state and the sorted key pairs are the golden file's, bit for bit."""
+    got = make_golden.run(_gpu_default_stepper, name)
+    ref = np.load(GOLDEN / f"{name}.npz")
+    if name in make_golden.TRANSCENDENTAL:
+        make_golden.assert_state_close(name, got, ref)
+        return
+    for key in ("x", "v", "x_prev", "sorted_keys"):
+        if key in ref.files:
+            assert np.array_equal(np.asarray(got[key]).view(np.uint8), ref[key].view(np.uint8)), (name, key)
