@@ -9,10 +9,11 @@ with the particle state uploaded from pinned host memory and read back every fra
 reference's enableBlockingReadback behaviour).  Under torchrun each rank steps its own replica
 of the scene (the single-scene substep does not shard), so `scaling` is "weak".
 
---impl reference times the reference's CPU implementation of the same path.  The reference's
-own solver is Vulkan/D3D12 HLSL behind Diligent Engine and cannot run here, so its CPU
-restatement (the oracle under oracle/) is timed on the host cores, with every thread it can use,
-on a bounded lattice sample of the same scene.
+--impl reference times the reference's CPU implementation of the same path on the same full
+workload.  The reference's own solver is Vulkan/D3D12 HLSL behind Diligent Engine and cannot run
+here, so its CPU restatement (the oracle under oracle/, pinned to the reference's own shaders) is
+timed on the host cores with every thread it can use; the scene comes from oracle/cn_scenes.py,
+so that arm loads no product library.
 """
 from __future__ import annotations
 
@@ -187,6 +188,7 @@ def run_ours(args):
     soa = w.soa()
     n = soa.particle_count
     solver = Solver(desc, device=local)
+    free0 = torch.cuda.mem_get_info(local)[0]
     solver.sync_world(soa)
     # A dedicated stream: the C ABI reads a NULL stream as "the solver's own stream", and torch's
     # default stream has handle 0, so stepping on it would leave the events below unordered.
@@ -195,6 +197,7 @@ def run_ours(args):
     assert sh != 0
     solver.step_many(dt, max(args.warmup, 0), sh)
     torch.cuda.synchronize()
+    resident_gb = (free0 - torch.cuda.mem_get_info(local)[0]) / 1e9   # the solver's device state
     x0, v0, _ = solver.read_particles()  # the timed frames are replayed below for the kernel split
     uuid = None
     try:
@@ -289,7 +292,7 @@ def run_ours(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD if dims == (128, 64, 128) else f"pbf_dam_break_{dims[0]}x{dims[1]}x{dims[2]}",
                    "particles": n, "substeps": substeps, "fluid_iterations": desc.fluid_iterations,
-                   "frame_dt": dt, "parallelism": f"replicas{world}", "l2": "working set > L2 (~0.9 GB resident)",
+                   "frame_dt": dt, "parallelism": f"replicas{world}", "l2": f"working set > L2 ({resident_gb:.2f} GB resident on the device)",
                    "mean_neighbors": round(counts, 2), "mean_superset": round(sup_counts, 2)},
         "e2e": {"value": round(e2e_value, 1), "unit": "particle-substeps/s", "h2d_bytes_per_step": 32 * n,
                 "d2h_bytes_per_step": 32 * n, "steps": e2e_steps},
@@ -697,17 +700,21 @@ def cpu_baseline(budget_s: float = 15.0, dims=(64, 32, 64), max_frames: int = 8)
                       f"{frames} frames x {desc.substeps} substeps, {el:.1f} s"}
 
 
-def run_reference(args, dims=(48, 24, 48)):
+def run_reference(args):
+    """The reference's CPU implementation of the path on this workload: the oracle (the C++
+    restatement of the reference's substep, pinned bit for bit to the reference's own shaders run
+    on the host) on the full 128 x 64 x 128 dam break, every host thread.  The scene is built by
+    oracle/cn_scenes.py, so this arm loads no product library."""
     rank, local, world = dist_env()
     if rank != 0:
         return
     sys.path.insert(0, str(ROOT / "oracle"))
     import cn_oracle
-    from cn_physics import scenes
+    import cn_scenes
 
     threads = cn_oracle.set_threads(os.cpu_count() or 1)
-    w, desc, dt = scenes.dam_break(nx=dims[0], ny=dims[1], nz=dims[2])
-    soa = w.soa()
+    scene = cn_scenes.DamBreak()
+    soa, desc, dt = scene.soa(), scene.desc, scene.frame_dt
     ora = cn_oracle.Oracle(desc, soa)
     for _ in range(max(args.warmup, 0)):
         ora.step(dt)
@@ -715,14 +722,17 @@ def run_reference(args, dims=(48, 24, 48)):
     for _ in range(args.steps):
         ora.step(dt)
     el = time.perf_counter() - t0
-    value = soa.particle_count * desc.substeps * args.steps / el
-    sample = (f"{dims[0]}x{dims[1]}x{dims[2]} lattice ({soa.particle_count} particles) of the dam break; "
-              "CPU restatement of the reference's HLSL passes (its Vulkan path cannot run here)")
+    n = soa.particle_count
+    value = n * desc.substeps * args.steps / el
+    sample = (f"the full workload: {n} particles, {args.steps} frames x {desc.substeps} substeps after "
+              f"{args.warmup} warm-up frames, {el:.1f} s; the oracle (C++ restatement of the reference's "
+              "HLSL passes, bit-identical to them with the shaders' quotients) on the host cores, as the "
+              "reference's own Vulkan path cannot run here")
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": "particle-substeps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(el * 1e3 / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "particles": soa.particle_count, "substeps": desc.substeps,
-                       "fluid_iterations": desc.fluid_iterations, "frame_dt": dt},
+            "config": {"workload": WORKLOAD, "particles": n, "substeps": desc.substeps,
+                       "fluid_iterations": desc.fluid_iterations, "frame_dt": dt, "parallelism": "host threads"},
             "cpu_baseline": {"value": round(value, 1), "unit": "particle-substeps/s", "cores": threads,
                              "kind": "port", "sample": sample},
             "e2e": {"value": round(value, 1), "unit": "particle-substeps/s", "h2d_bytes_per_step": 0,
