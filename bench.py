@@ -700,7 +700,7 @@ def cpu_baseline(budget_s: float = 15.0, dims=(64, 32, 64), max_frames: int = 8)
                       f"{frames} frames x {desc.substeps} substeps, {el:.1f} s"}
 
 
-def run_reference(args):
+def run_reference(args, dims=(128, 64, 128)):
     """The reference's CPU implementation of the path on this workload: the oracle (the C++
     restatement of the reference's substep, pinned bit for bit to the reference's own shaders run
     on the host) on the full 128 x 64 x 128 dam break, every host thread.  The scene is built by
@@ -713,7 +713,7 @@ def run_reference(args):
     import cn_scenes
 
     threads = cn_oracle.set_threads(os.cpu_count() or 1)
-    scene = cn_scenes.DamBreak()
+    scene = cn_scenes.DamBreak(*dims)
     soa, desc, dt = scene.soa(), scene.desc, scene.frame_dt
     ora = cn_oracle.Oracle(desc, soa)
     for _ in range(max(args.warmup, 0)):
@@ -731,7 +731,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": "particle-substeps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(el * 1e3 / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "particles": n, "substeps": desc.substeps,
+            "config": {"workload": WORKLOAD if tuple(dims) == (128, 64, 128) else
+                       f"pbf_dam_break_{dims[0]}x{dims[1]}x{dims[2]}", "particles": n, "substeps": desc.substeps,
                        "fluid_iterations": desc.fluid_iterations, "frame_dt": dt, "parallelism": "host threads"},
             "cpu_baseline": {"value": round(value, 1), "unit": "particle-substeps/s", "cores": threads,
                              "kind": "port", "sample": sample},
