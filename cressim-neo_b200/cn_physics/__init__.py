@@ -365,6 +365,29 @@ class World:
         s = self._soa or self.soa()
         return _view(s.velocities, s.particle_count, np.float32, 4)
 
+    def layout_mapping(self) -> dict:
+        """ParticleLayoutMapping (include/engine/particle_layout_mapping.h): per-particle arrays and
+        per-owner (ids, environment, particle offset, particle count), as numpy copies."""
+        m = _abi.ParticleLayoutMapping()
+        _check(self._lib.cn_world_particle_layout_mapping(self._h, C.byref(m)))
+        n = m.particle_count
+        out = {"particle_count": n, "soft_body_count": m.soft_body_count, "cloth_count": m.cloth_count,
+               "fluid_count": m.fluid_count, "strand_count": m.strand_count,
+               "layout_revision": m.layout_revision}
+        for name in ("environment_indices", "particle_kinds", "owner_types", "owner_indices", "strand_ids",
+                     "strand_orders", "strand_roles", "owning_soft_body_indices", "particle_material_indices",
+                     "fluid_material_indices", "phases", "collision_layers", "collision_masks",
+                     "adjacency_offsets", "adjacency_counts"):
+            out[name] = _view(getattr(m, name), n, np.uint32).copy()
+        for owner in ("soft_bodies", "cloths", "fluids", "strands"):
+            r = getattr(m, owner)
+            ids = np.ctypeslib.as_array(r.ids, (r.count,)).copy() if r.count else np.zeros(0, np.uint64)
+            out[owner] = {"ids": ids,
+                          "environment_indices": _view(r.environment_indices, r.count, np.uint32).copy(),
+                          "particle_offsets": _view(r.particle_offsets, r.count, np.uint32).copy(),
+                          "particle_counts": _view(r.particle_counts, r.count, np.uint32).copy()}
+        return out
+
     def counts(self) -> dict:
         s = self._soa or self.soa()
         return {"particles": s.particle_count, "edges": s.edge_count, "bends": s.bend_count,

@@ -113,6 +113,22 @@ class WorldSoA(C.Structure):
     ]
 
 
+class OwnerRanges(C.Structure):
+    _fields_ = [("count", u32), ("ids", C.POINTER(C.c_uint64)), ("environment_indices", P_u32),
+                ("particle_offsets", P_u32), ("particle_counts", P_u32)]
+
+
+class ParticleLayoutMapping(C.Structure):
+    _fields_ = [("particle_count", u32), ("soft_body_count", u32), ("cloth_count", u32), ("fluid_count", u32),
+                ("strand_count", u32), ("layout_revision", C.c_uint64)] + \
+               [(n, P_u32) for n in ("environment_indices", "particle_kinds", "owner_types", "owner_indices",
+                                     "strand_ids", "strand_orders", "strand_roles", "owning_soft_body_indices",
+                                     "particle_material_indices", "fluid_material_indices", "phases",
+                                     "collision_layers", "collision_masks", "adjacency_offsets",
+                                     "adjacency_counts")] + \
+               [(n, OwnerRanges) for n in ("soft_bodies", "cloths", "fluids", "strands")]
+
+
 class Transform(C.Structure):
     _fields_ = [("position", f32 * 3), ("rotation", f32 * 4), ("scale", f32 * 3)]
 
@@ -295,6 +311,7 @@ SIGNATURES = [
     ("cn_solver_set_timing", C.c_int, [C.c_void_p, u32]),
     ("cn_solver_kernel_times", C.c_int, [C.c_void_p, C.c_void_p, u32, P_u32]),
     ("cn_solver_graph_stats", C.c_int, [C.c_void_p, P_u32, P_u32]),
+    ("cn_world_particle_layout_mapping", C.c_int, [C.c_void_p, C.POINTER(ParticleLayoutMapping)]),
     ("cn_sort_cell_keys_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, u32, C.c_void_p, C.c_void_p]),
     ("cn_solver_debug_read", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),
     ("cn_batch_desc_defaults", None, [C.POINTER(BatchDesc)]),

@@ -104,14 +104,14 @@ def xpbd_cube(n: int = 16, spacing: float = 1.0 / 16.0, seed: int = 0, radius: f
 
 
 def dam_break(nx: int = 128, ny: int = 64, nz: int = 128, spacing: float = 0.05, seed: int = 0,
-              box=(12.8, 6.4, 25.6)):
+              box=(12.8, 6.4, 25.6), vorticity: float = 0.0):
     """Returns (world, desc, frame_dt)."""
     w = World()
     r = 0.6 * spacing  # h = max((2/0.6) r, 2r) = 2 * spacing
     size = (nx * spacing, ny * spacing, nz * spacing)
     offset = r - 0.5 * spacing
     center = (size[0] * 0.5 + offset, size[1] * 0.5 + offset, size[2] * 0.5 + offset)
-    w.add_fluid_grid(size, spacing, position=center, radius=r, viscosity=0.01, vorticity=0.0)
+    w.add_fluid_grid(size, spacing, position=center, radius=r, viscosity=0.01, vorticity=vorticity)
     body = w.add_rigid_body("static")
     bx, by, bz = box
     t = 0.5

@@ -234,6 +234,13 @@ struct Scene {
     uint4 *sMeta = nullptr;           // metadata at the sorted slot
     uint32_t *sInfo = nullptr;        // kind (bit 31 = fluid) | fluid material index
     unsigned long long *sBoundary = nullptr; // boundary-collider candidate mask (query order)
+    // Scenes with more colliders than the mask has bits keep per-slot candidate lists instead
+    // (physics_particle_count/emit_fluid_boundary_candidates.cs.hlsl): bCount / bOffset per
+    // compute slot, bList the colliders' query positions in ascending order (bList == nullptr:
+    // the mask is used).
+    uint32_t *bCount = nullptr, *bOffset = nullptr, *bList = nullptr;
+    uint32_t bListCap = 0;
+    uint32_t colBvh = 0;              // the collider LBVH is built every substep (boundary queries)
     uint32_t maxNbr = 128;
     uint32_t *nbr = nullptr;          // [N][maxNbr] sorted slots
     uint32_t *nbrCount = nullptr;     // per sorted slot
@@ -242,6 +249,7 @@ struct Scene {
     uint32_t *sup = nullptr;          // [N][supCap] candidates within the superset radius, traversal order
     uint32_t *supCount = nullptr;     // per sorted slot (> supCap: overflowed)
     uint32_t *fluidMaxDelta = nullptr; // [64] float bits of max |accumulated delta| per iteration
+    float4 *fluidVort = nullptr;      // curl xyz + magnitude per sorted slot (vorticity confinement)
 
     // ---- contact candidates ----
     uint32_t *candCount = nullptr, *candOffset = nullptr; // per particle
@@ -319,6 +327,8 @@ __device__ __forceinline__ bool bvhQuery(const Scene &s, V qmin, V qmax, F &&lea
 void launchApplyBodyTargets(const Scene &s, const BodyTarget *list, const uint32_t *count, uint32_t capacity,
                             cudaStream_t st);
 void launchRigidPredict(const Scene &s, float dt, float gx, float gy, float gz, cudaStream_t st);
+// The LBVH over the query-order colliders' world AABBs (cn_rigid.cu), after the rigid predict.
+void launchColliderBvh(const Scene &s, void *scratch, cudaStream_t st);
 void launchPredictAndKeys(const Scene &s, float dt, const Config &c, cudaStream_t st);
 void launchCellSetup(const Scene &s, uint32_t *scanTmp, void *sortScratch, cudaStream_t st);
 // Neighbour and superset lists: entry k of compute slot i at k * N + i (true) or i * cap + k.
@@ -335,6 +345,8 @@ void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter,
 void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const Config &c, bool writeDebug,
                                 cudaStream_t st);
 void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st);
+// Vorticity confinement (after launchFluidNeighborsOnly's post-update lists): curl, then force.
+void launchFluidVorticity(const Scene &s, float dt, cudaStream_t st);
 void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st);
 void launchContacts(const Scene &s, const Config &c, bool particleContacts, bool rigidContacts,
                     cudaStream_t st);

@@ -317,6 +317,14 @@ __device__ __forceinline__ uint32_t fluidBoundaryMaskFor(const Scene &s, uint32_
     return overflow;
 }
 
+// The same query for scenes with more colliders than the mask holds: counts (kEmit false) or
+// writes (kEmit true, at most `room` entries) the candidates' query positions in ascending order.
+// With the collider LBVH built this substep, the overlapping leaves come from the tree (sorted
+// back into query order; more than kCandidateHits of them fall back to the scan); the filters
+// are those of the mask query.
+template <bool kEmit>
+__device__ uint32_t fluidBoundaryListFor(const Scene &s, uint32_t p, f3 pos, uint32_t *out, uint32_t room);
+
 __global__ void __launch_bounds__(kThreads) k_cellSetup(Scene s)
 {
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -444,10 +452,27 @@ __global__ void __launch_bounds__(kThreads) k_computeOrderSetup(Scene s)
     s.sMeta[cslot] = s.meta[p];
     s.sInfo[cslot] = fluid ? (kFluidBit | ((s.fluidMatIdx[p] & 0x7fffu) << 16) | (s.fluidGroup[p] & 0xffffu)) : 0u;
     unsigned long long mask = 0ull;
-    if (fluid && s.colQueryCount > 0) {
+    if (s.bList) {
+        s.bCount[cslot] = fluid && s.colQueryCount > 0 ? fluidBoundaryListFor<false>(s, p, xyz(s.x[p]), nullptr, 0u) : 0u;
+    } else if (fluid && s.colQueryCount > 0) {
         if (fluidBoundaryMaskFor(s, p, xyz(s.x[p]), mask)) atomicAdd(&s.meta_->boundaryMaskOverflow, 1u);
     }
     s.sBoundary[cslot] = mask;
+}
+
+// Per compute slot: its boundary candidates at its offset (after the count above and a scan).
+__global__ void __launch_bounds__(kThreads) k_fluidBoundaryEmit(Scene s)
+{
+    const uint32_t cslot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cslot >= s.N) return;
+    const uint32_t n = s.bCount[cslot];
+    if (n == 0u) return;
+    const uint32_t off = s.bOffset[cslot];
+    const uint32_t room = off < s.bListCap ? s.bListCap - off : 0u;
+    if (room < n) atomicAdd(&s.meta_->boundaryMaskOverflow, 1u);
+    if (room == 0u) return;
+    const uint32_t p = s.cvals[cslot];
+    fluidBoundaryListFor<true>(s, p, xyz(s.x[p]), s.bList + off, room < n ? room : n);
 }
 
 // The run of cell key `key` in compute slots (FindCellRange semantics).
@@ -523,6 +548,37 @@ __device__ __forceinline__ bool bvhOverlaps(const Scene &s, f3 qmin, f3 qmax, ui
         hits[b] = v;
     }
     return true;
+}
+
+template <bool kEmit>
+__device__ uint32_t fluidBoundaryListFor(const Scene &s, uint32_t p, f3 pos, uint32_t *out, uint32_t room)
+{
+    const float pr = mx(s.radii[p], 0.0f);
+    const cn_fluid_material &fm = s.fluidMaterials[s.fluidMatIdx[p]];
+    const float support = mx(fm.smoothing_radius, pr);
+    const float reuse = mx(mx(fm.cfl_radius, pr), support);
+    const float qr = support + reuse;
+    const f3 qmin = pos - f3{qr, qr, qr}, qmax = pos + f3{qr, qr, qr};
+    const uint4 m = s.meta[p];
+    uint32_t count = 0;
+    auto consider = [&](uint32_t k) {
+        const uint32_t c = s.colQueryOrder[k];
+        if (!aabbOverlaps(qmin, qmax, xyz(s.colAabbMin[c]), xyz(s.colAabbMax[c]))) return;
+        const cn_collider_broadphase bp = s.colBp[c];
+        const uint32_t bt = s.bodyType[bp.owner_body];
+        if (bp.enabled_flag != 0u && bp.environment_index == m.x && bt != CN_BODY_DYNAMIC &&
+            (m.w & bp.collision_layer) != 0u && (bp.collision_mask & m.z) != 0u) {
+            if (kEmit && count < room) out[count] = k;
+            ++count;
+        }
+    };
+    uint32_t hits[kCandidateHits], nh = 0;
+    if (s.colBvh && s.colQueryCount >= 2u && bvhOverlaps(s, qmin, qmax, hits, nh)) {
+        for (uint32_t i = 0; i < nh; ++i) consider(hits[i]);
+    } else {
+        for (uint32_t k = 0; k < s.colQueryCount; ++k) consider(k);
+    }
+    return count;
 }
 
 // kMode 0 counts the particle's candidate bodies, 1 emits its pairs from `write` (its offset
@@ -785,6 +841,29 @@ __device__ __forceinline__ bool fluidGhostDelta(const Scene &s, uint32_t c, f3 p
     return true;
 }
 
+// Calls f(k) for every boundary candidate of compute slot `slot` (collider query positions k,
+// ascending): from the mask, or from the slot's candidate list.
+template <class F> __device__ __forceinline__ void forEachBoundary(const Scene &s, uint32_t slot, F &&f)
+{
+    if (!s.bList) {
+        unsigned long long bm = s.sBoundary[slot];
+        while (bm) {
+            const uint32_t k = __ffsll(bm) - 1;
+            bm &= bm - 1ull;
+            f(k);
+        }
+    } else {
+        const uint32_t off = s.bOffset[slot];
+        const uint32_t n = s.bCount[slot];
+        const uint32_t end = off + n < s.bListCap ? off + n : s.bListCap;
+        for (uint32_t e = off; e < end; ++e) f(__ldg(&s.bList[e]));
+    }
+}
+__device__ __forceinline__ bool hasBoundary(const Scene &s, uint32_t slot)
+{
+    return s.bList ? s.bCount[slot] != 0u : s.sBoundary[slot] != 0ull;
+}
+
 // Smallest float t with sqrtf(t) >= h: `length(d) >= h` (the reference's neighbour test) is exactly
 // `dot(d, d) >= t` because the IEEE square root is correctly rounded and monotonic, so the square
 // root is only taken for accepted neighbours.
@@ -964,16 +1043,13 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidNeighborsDen
     s.nbrCount[slot] = count;
     if (truncated) atomicAdd(&s.meta_->neighborTruncations, 1u);
     if (!density) return;
-    unsigned long long bm = s.sBoundary[slot];
-    while (bm) {
-        const uint32_t kk = __ffsll(bm) - 1;
-        bm &= bm - 1ull;
+    forEachBoundary(s, slot, [&](uint32_t kk) {
         f3 ghost;
-        if (!fluidGhostDelta(s, s.colQueryOrder[kk], sp, h, ghost)) continue;
+        if (!fluidGhostDelta(s, s.colQueryOrder[kk], sp, h, ghost)) return;
         const float dist = length(ghost);
-        if (dist >= h) continue;
+        if (dist >= h) return;
         rho += spikyWk(dist, h, invH, kW) * cfg.fluidBoundaryDensityScale;
-    }
+    });
     const float rho0 = mx(fm.rest_density, 1.0f);
     const float C = mx(rho - rho0, -rho0 * mx(cfg.fluidMaxUnderDensityRatio, 0.0f)) * fm.density_constraint_scale;
     if (kExtras && st > kEps) {
@@ -1085,18 +1161,15 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidDeltaApplyCl
             weight += 1.0f;
         }
         f3 bd{0.f, 0.f, 0.f};
-        unsigned long long bm = s.sBoundary[slot];
-        while (bm) {
-            const uint32_t k = __ffsll(bm) - 1;
-            bm &= bm - 1ull;
+        forEachBoundary(s, slot, [&](uint32_t k) {
             f3 ghost;
-            if (!fluidGhostDelta(s, s.colQueryOrder[k], sp, h, ghost)) continue;
+            if (!fluidGhostDelta(s, s.colQueryOrder[k], sp, h, ghost)) return;
             const float dist = length(ghost);
-            if (dist <= kEps || dist >= h) continue;
+            if (dist <= kEps || dist >= h) return;
             const f3 nij = ghost * (1.0f / dist);
             const float dw = spikyDWk(dist, h, invH, kW);
             bd += -mx(sC, 0.0f) * dw * nij;
-        }
+        });
         bd = bd * cfg.fluidBoundaryDeltaScale;
         packed = dp * cfg.fluidSolveCoefficient + bd;
     }
@@ -1108,23 +1181,19 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidDeltaApplyCl
     // clamp (physics_fluid_clamp_boundary.cs.hlsl:36-79)
     const f3 base = xyz(Xs[slot]);
     f3 cur = base + acc;
-    unsigned long long bm0 = s.sBoundary[slot];
-    if (bm0) {
+    if (hasBoundary(s, slot)) {
         const uint32_t p = s.cvals[slot];
         const float pr = mx(s.radii[p], 0.0f);
         for (uint32_t sweep = 0; sweep < 2u; ++sweep) {
             bool changed = false;
-            unsigned long long bm = bm0;
-            while (bm) {
-                const uint32_t k = __ffsll(bm) - 1;
-                bm &= bm - 1ull;
+            forEachBoundary(s, slot, [&](uint32_t k) {
                 float sd = 0.0f;
                 f3 n{0.f, 1.f, 0.f};
-                if (!fluidBoundaryContactInfo(s, s.colQueryOrder[k], cur, sd, n)) continue;
-                if (sd >= pr) continue;
+                if (!fluidBoundaryContactInfo(s, s.colQueryOrder[k], cur, sd, n)) return;
+                if (sd >= pr) return;
                 cur += n * (pr - sd);
                 changed = true;
-            }
+            });
             if (!changed) break;
         }
     }
@@ -1140,6 +1209,76 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidDeltaApplyCl
             if (int(threadIdx.x & 31u) == __ffs(mask) - 1 && big > 0u) atomicMax(&s.fluidMaxDelta[next], big);
         }
     }
+}
+
+// Vorticity confinement over the lists of the post-update rebuild, in compute order (positions in
+// s.P after the velocity update, velocities in particle order).
+// physics_fluid_compute_vorticity.cs.hlsl:13-76: curl of the velocity field from same-material
+// neighbours, with its magnitude in w.
+__global__ void __launch_bounds__(kThreads) k_fluidVorticity(Scene s)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= s.N) return;
+    const uint32_t info = s.sInfo[slot];
+    float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 self = s.P[slot];
+    const cn_fluid_material &fm = s.fluidMaterials[infoMaterial(info)];
+    if ((info & kFluidBit) && mx(fm.vorticity_confinement, 0.0f) > kEps && (__float_as_uint(self.w) & kFluidBit)) {
+        const f3 sp = xyz(self), sv = xyz(s.v[s.cvals[slot]]);
+        const float h = mx(fm.smoothing_radius, 1.0e-4f);
+        const float kW = spikyK(h), invH = 1.0f / h;
+        const uint32_t mat = infoMaterial(info);
+        f3 curl{0.f, 0.f, 0.f};
+        const uint32_t cnt = s.nbrCount[slot];
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t c = s.nbr[size_t(k) * s.N + slot];
+            const float4 q = s.P[c];
+            if (infoMaterial(__float_as_uint(q.w)) != mat) continue;
+            const f3 delta = sp - xyz(q);
+            const float dist = length(delta);
+            if (dist <= kEps || dist >= h) continue;
+            curl += cross(xyz(s.v[s.cvals[c]]) - sv, spikyGradK(delta, dist, h, invH, kW));
+        }
+        out = mk4(curl, length(curl));
+    }
+    s.fluidVort[slot] = out;
+}
+
+// physics_fluid_apply_vorticity_confinement.cs.hlsl:13-92: the confinement force along the
+// gradient of the curl magnitude, added to the particle's velocity (w cleared).
+__global__ void __launch_bounds__(kThreads) k_fluidVorticityApply(Scene s, float dt)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= s.N) return;
+    const uint32_t info = s.sInfo[slot];
+    if ((info & kFluidBit) == 0u) return;
+    const cn_fluid_material &fm = s.fluidMaterials[infoMaterial(info)];
+    const float conf = mx(fm.vorticity_confinement, 0.0f);
+    if (conf <= kEps) return;
+    const float4 self = s.P[slot];
+    if ((__float_as_uint(self.w) & kFluidBit) == 0u) return;
+    const float4 sc = s.fluidVort[slot];
+    if (sc.w <= kEps) return;
+    const f3 sp = xyz(self);
+    const float h = mx(fm.smoothing_radius, 1.0e-4f);
+    const float kW = spikyK(h), invH = 1.0f / h;
+    const uint32_t mat = infoMaterial(info);
+    f3 grad{0.f, 0.f, 0.f};
+    const uint32_t cnt = s.nbrCount[slot];
+    for (uint32_t k = 0; k < cnt; ++k) {
+        const uint32_t c = s.nbr[size_t(k) * s.N + slot];
+        const float4 q = s.P[c];
+        if (infoMaterial(__float_as_uint(q.w)) != mat) continue;
+        const f3 delta = sp - xyz(q);
+        const float dist = length(delta);
+        if (dist <= kEps || dist >= h) continue;
+        grad += s.fluidVort[c].w * spikyGradK(delta, dist, h, invH, kW);
+    }
+    const float gl = length(grad);
+    if (gl <= kEps) return;
+    const f3 force = conf * cross(grad / gl, xyz(sc));
+    const uint32_t p = s.cvals[slot];
+    s.v[p] = mk4(xyz(s.v[p]) + dt * force, 0.0f);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1982,8 +2121,8 @@ __global__ void __launch_bounds__(kThreads) k_fluidBoundaryVelocities(Scene s, f
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.N || s.kinds[i] != CN_PARTICLE_FLUID) return;
-    unsigned long long bm = s.sBoundary[s.rank[i]];
-    if (!bm) return;
+    const uint32_t slot = s.rank[i];
+    if (!hasBoundary(s, slot)) return;
     const f3 pos = xyz(s.x[i]);
     const float pr = mx(s.radii[i], 0.0f);
     const f3 vel = xyz(s.v[i]);
@@ -1992,22 +2131,20 @@ __global__ void __launch_bounds__(kThreads) k_fluidBoundaryVelocities(Scene s, f
     float bestD = 3.402823466e+38f;
     f3 bestN{0.f, 1.f, 0.f}, bestMat{0.f, 0.f, 0.f};
     bool found = false;
-    while (bm) {
-        const uint32_t k = __ffsll(bm) - 1;
-        bm &= bm - 1ull;
+    forEachBoundary(s, slot, [&](uint32_t k) {
         const uint32_t c = s.colQueryOrder[k];
         float sd = 0.0f;
         f3 n{0.f, 1.f, 0.f};
-        if (!fluidBoundaryContactInfo(s, c, pos, sd, n)) continue;
+        if (!fluidBoundaryContactInfo(s, c, pos, sd, n)) return;
         const float cd = pr + 2.0f * cfg.slop;
-        if (sd > cd) continue;
+        if (sd > cd) return;
         if (sd < bestD) {
             bestD = sd;
             bestN = n;
             bestMat = combineContactMaterial(pm, s.colMat[c]);
             found = true;
         }
-    }
+    });
     if (!found) return;
     const float pen = mx(pr - bestD, 0.0f);
     const float cd = mx(pr + 2.0f * cfg.slop, 1.0e-5f);
@@ -2464,6 +2601,10 @@ void launchCellSetup(const Scene &s, uint32_t *scanTmp, void *sortScratch, cudaS
         exclusiveScan(s.runLenSorted, s.runCompStart, s.N, scanTmp, scanTmp + 1, st);
         k_runPlace<<<blocksFor(s.N), kThreads, 0, st>>>(s);
         k_computeOrderSetup<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+        if (s.bList) { // per-slot fluid boundary candidate lists (more colliders than the mask holds)
+            exclusiveScan(s.bCount, s.bOffset, s.N, scanTmp, scanTmp + 1, st);
+            k_fluidBoundaryEmit<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+        }
         // the runs number at most N (about N / 8 in a settled fluid): a fixed grid strides over them
         const unsigned grid = unsigned(std::min<size_t>(blocksFor(size_t(s.N) * 27u), 148u * 16u));
         k_runNeighbors<<<grid, kThreads, 0, st>>>(s);
@@ -2549,6 +2690,13 @@ void launchFluidIteration(const Scene &s, uint32_t iter, float dt, const Config 
     if (iter == 0 || fluidGatherEachIteration(s)) launchFluidGather(s, iter, st);
     launchFluidNeighborsDensity(s, c, iter, false, st);
     launchFluidDeltaApplyClamp(s, iter, dt, c, writeDebug, st);
+}
+
+void launchFluidVorticity(const Scene &s, float dt, cudaStream_t st)
+{
+    if (s.N == 0 || !s.fluidVort) return;
+    k_fluidVorticity<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+    k_fluidVorticityApply<<<blocksFor(s.N), kThreads, 0, st>>>(s, dt);
 }
 
 void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)

@@ -1238,6 +1238,19 @@ size_t rigidScratchBytes(uint32_t colliders, uint32_t pairs)
     return (sortBytes > scan ? sortBytes : scan) + 256;
 }
 
+void launchColliderBvh(const Scene &s, void *scratch, cudaStream_t st)
+{
+    const uint32_t n = s.colQueryCount;
+    if (n < 2) return;
+    void *work = static_cast<uint8_t *>(scratch) + 256;
+    k_bvhBounds<<<1, kBoundsThreads, 0, st>>>(s);
+    k_bvhMorton<<<blocksOf(n), kRigidThreads, 0, st>>>(s);
+    radixSortPairs(s.bvhKeyA, s.bvhValA, s.bvhKeyB, s.bvhValB, n, work, &s.meta_->waitTimeouts, st);
+    k_bvhBuild<<<blocksOf(n - 1), kRigidThreads, 0, st>>>(s);
+    cudaMemsetAsync(s.bvhVisits, 0, sizeof(uint32_t) * (n - 1), st);
+    k_bvhRefit<<<blocksOf(n), kRigidThreads, 0, st>>>(s);
+}
+
 void launchRigidBroadphaseAndContacts(const Scene &s, const Config &c, void *scratch, cudaStream_t st)
 {
     const uint32_t n = s.colQueryCount;
@@ -1247,14 +1260,7 @@ void launchRigidBroadphaseAndContacts(const Scene &s, const Config &c, void *scr
     }
     uint32_t *total = static_cast<uint32_t *>(scratch);
     void *work = static_cast<uint8_t *>(scratch) + 256;
-    if (n >= 2) {
-        k_bvhBounds<<<1, kBoundsThreads, 0, st>>>(s);
-        k_bvhMorton<<<blocksOf(n), kRigidThreads, 0, st>>>(s);
-        radixSortPairs(s.bvhKeyA, s.bvhValA, s.bvhKeyB, s.bvhValB, n, work, &s.meta_->waitTimeouts, st);
-        k_bvhBuild<<<blocksOf(n - 1), kRigidThreads, 0, st>>>(s);
-        cudaMemsetAsync(s.bvhVisits, 0, sizeof(uint32_t) * (n - 1), st);
-        k_bvhRefit<<<blocksOf(n), kRigidThreads, 0, st>>>(s);
-    }
+    if (!s.colBvh) launchColliderBvh(s, scratch, st); // else built after the rigid predict already
     // one warp per block: the walks are latency-bound chains, so they go to as many SMs as possible
     const unsigned pairBlocks = unsigned((s.activeMovingCount + 31u) / 32u);
     k_rigidPairsCount<<<pairBlocks, 32, 0, st>>>(s);

@@ -49,6 +49,7 @@ struct cn_solver {
     float *hostX = nullptr, *hostV = nullptr;
     bool synced = false;
     bool hasFluid = false, ppPossible = false, rigidPossible = false, hasBroadphase = false, hasDynamic = false;
+    bool fluidBoundaryLists = false, vorticity = false, fluidXMoves = false;
     uint32_t nProxy = 0;          // rigid proxy particles (the leading particles)
     bool proxyContacts = false;   // proxy particle -> collider contacts in the rigid contact solve
     uint32_t substeps = 1, fluidIt = 1, softIt = 1, contactIt = 1, maxIt = 1, jointIt = 1, rrIt = 1;
@@ -215,6 +216,11 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
         s.rrKeyB = a.take<uint32_t>(K); s.rrValB = a.take<uint32_t>(K);
         s.rrHead = a.take<uint32_t>(K); s.rrGroupOf = a.take<uint32_t>(K);
         s.rrGroups = a.take<uint2>(K);
+        sv->rigidScratch = a.take<uint8_t>(cn::rigidScratchBytes(C, K));
+    } else if (sv->fluidBoundaryLists) {
+        sv->rigidScratch = a.take<uint8_t>(cn::rigidScratchBytes(C, 1u));
+    }
+    if (sv->rigidRigid || sv->fluidBoundaryLists) { // the LBVH over the colliders
         s.bvhKeyA = a.take<uint32_t>(C); s.bvhValA = a.take<uint32_t>(C);
         s.bvhKeyB = a.take<uint32_t>(C); s.bvhValB = a.take<uint32_t>(C);
         s.bvhChildren = a.take<uint2>(C);
@@ -222,8 +228,8 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
         s.bvhMin = a.take<float4>(2 * C); s.bvhMax = a.take<float4>(2 * C);
         s.bvhWide = a.take<float4>(4 * C);
         s.bvhBounds = a.take<float4>(2);
-        sv->rigidScratch = a.take<uint8_t>(cn::rigidScratchBytes(C, K));
     }
+    s.colBvh = sv->fluidBoundaryLists ? 1u : 0u;
     s.colFrame = a.take<float4>(size_t(C) * 4);
     s.colQueryOrder = a.take<uint32_t>(C);
     {
@@ -267,6 +273,12 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
         s.sMeta = a.take<uint4>(N);
         s.sInfo = a.take<uint32_t>(N);
         s.sBoundary = a.take<unsigned long long>(N);
+        if (sv->fluidBoundaryLists) {
+            // physics_scene_gpu_state.cpp:728-729: 32 boundary candidates per particle
+            s.bListCap = std::max<uint32_t>(N * 32u, 64u);
+            s.bCount = a.take<uint32_t>(N); s.bOffset = a.take<uint32_t>(N);
+            s.bList = a.take<uint32_t>(s.bListCap);
+        }
         s.runFlag = a.take<uint32_t>(N);
         s.runIdx = a.take<uint32_t>(N);
         s.runStartOf = a.take<uint32_t>(N);
@@ -285,11 +297,12 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
         s.supCap = 160u;
         s.sup = a.take<uint32_t>(size_t(N) * s.supCap);
         s.supCount = a.take<uint32_t>(N);
-        if (!sv->ppPossible) s.Pb = a.take<float4>(N);
+        if (!sv->fluidXMoves) s.Pb = a.take<float4>(N);
         else s.P0 = a.take<float4>(N);
         s.maxNbr = sv->desc.max_fluid_neighborhood;
         s.nbr = a.take<uint32_t>(std::max<size_t>(size_t(N) * s.maxNbr, 1));
         s.nbrCount = a.take<uint32_t>(N);
+        if (sv->vorticity) s.fluidVort = a.take<float4>(N);
     }
     if (sv->rigidPossible || sv->proxyContacts) {
         s.candCount = a.take<uint32_t>(N);
@@ -384,6 +397,7 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
     const uint32_t N = s.N;
     for (uint32_t sub = 0; sub < sv->substeps; ++sub) {
         probe(sv, "rigid_predict", st, [&] { cn::launchRigidPredict(s, dt, c.gravity[0], c.gravity[1], c.gravity[2], st); });
+        if (s.colBvh) probe(sv, "collider_bvh", st, [&] { cn::launchColliderBvh(s, sv->rigidScratch, st); });
         if (sv->rigidRigid)
             probe(sv, "rigid_broadphase_contacts", st, [&] { cn::launchRigidBroadphaseAndContacts(s, c, sv->rigidScratch, st); });
         probe(sv, "predict_keys", st, [&] { cn::launchPredictAndKeys(s, dt, c, st); });
@@ -453,7 +467,9 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
         const float4 *fluidDelta = sv->hasFluid ? ((sv->fluidIt & 1u) ? s.Db : s.Da) : nullptr;
         probe(sv, "update_velocities", st, [&] { cn::launchUpdateVelocities(s, dt, fluidDelta, st); });
         if (sv->hasFluid) probe(sv, "fluid_boundary_velocities", st, [&] { cn::launchFluidBoundaryVelocities(s, dt, c, st); });
-        if (sv->hasFluid && sv->postUpdateNeighbors) cn::launchFluidNeighborsOnly(s, st);
+        // post-update neighbour rebuild and vorticity confinement (physics_solver.cpp:1262-1285)
+        if (sv->hasFluid && (sv->postUpdateNeighbors || sv->vorticity)) cn::launchFluidNeighborsOnly(s, st);
+        if (sv->vorticity) probe(sv, "fluid_vorticity", st, [&] { cn::launchFluidVorticity(s, dt, st); });
         if (sv->ppPossible && sv->contactIt)
             probe(sv, "contact_velocities", st, [&] { cn::launchParticleContactVelocities(s, sv->contactIt, c, st); });
         if (sv->rigidPossible && sv->contactIt) {
@@ -610,18 +626,21 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     bool anyDynamic = false;
     for (uint32_t b = 0; b < w->rigid_body_count; ++b)
         if (w->body_types[b] == CN_BODY_DYNAMIC) anyDynamic = true;
-    if (anyDynamic && anyFluid)
-        return setError(CN_ERR_UNSUPPORTED, "fluid particles against dynamic rigid bodies are not implemented");
+    sv->vorticity = false;
     for (uint32_t m = 0; m < w->fluid_material_count; ++m)
-        if (w->fluid_materials[m].vorticity_confinement > 1.0e-6f)
-            return setError(CN_ERR_UNSUPPORTED, "vorticity confinement is not implemented");
+        if (w->fluid_materials[m].vorticity_confinement > 1.0e-6f) sv->vorticity = anyFluid;
     sv->hasFluid = anyFluid;
     sv->hasDynamic = anyDynamic;
     if (anyFluid && (uint64_t(N) * std::max<uint32_t>(d.max_fluid_neighborhood, 160u) >= (uint64_t(1) << 32)))
         return setError(CN_ERR_UNSUPPORTED, "fluid scene too large for 32-bit neighbour list offsets");
     const bool contactWork = sv->contactIt > 0;
     sv->ppPossible = contactWork && N > 1 && anySolid && (anyFluid || anySelf || solidGroups.size() > 1);
-    sv->rigidPossible = contactWork && N > 0 && w->collider_count > 0 && anySolid;
+    // particle-rigid contacts: solid particles against every body, fluid particles against dynamic
+    // ones (physics_particle_count_particle_rigid_candidates.cs.hlsl:113-151)
+    sv->rigidPossible = contactWork && N > 0 && w->collider_count > 0 && (anySolid || (anyFluid && anyDynamic));
+    // Fluid x then also moves between the fluid iterations (contacts with dynamic bodies, or with
+    // other particles): the positions are gathered every iteration, not double-buffered.
+    sv->fluidXMoves = sv->ppPossible || (anyFluid && anyDynamic && sv->rigidPossible);
     sv->hasBroadphase = N > 0 && ((contactWork && N > 1) || anyFluid || w->collider_count > 0);
 
     // Fluid filter groups: dense ids of the distinct (environment, layer, mask) triples.
@@ -675,8 +694,8 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     sv->proxyContacts = sv->rigidRigid && nProxy > 0 && w->collider_count > 0;
     if (sv->rigidRigid && uint64_t(w->rigid_body_count) * w->rigid_body_count >= 0xffffffffull)
         return setError(CN_ERR_UNSUPPORTED, "more than 65535 rigid bodies in a scene with dynamic bodies");
-    if (anyFluid && order.size() > cn::kMaxBoundaryColliders)
-        return setError(CN_ERR_UNSUPPORTED, "more than 64 colliders in a scene with fluid");
+    // More colliders than the boundary mask holds: per-particle candidate lists over a collider LBVH
+    sv->fluidBoundaryLists = anyFluid && order.size() > cn::kMaxBoundaryColliders;
 
     // Incidence tables.
     const cn::Incidence edgeI = cn::buildIncidence(N, w->edge_count, 2, [&](uint32_t c, uint32_t k) {

@@ -193,6 +193,11 @@ struct cn_world {
     std::vector<cn_strand_distance> dists;
     std::vector<cn_collider_geometry> colGeo;
     std::vector<cn_collider_broadphase> colBp;
+    // ParticleLayoutMapping views (filled by pack)
+    struct OwnerRanges { std::vector<uint64_t> ids; std::vector<uint32_t> env, off, cnt; };
+    std::vector<uint32_t> lmEnv, lmPhase, lmLayer, lmMask, lmStrandId, lmStrandOrder, lmStrandRole, lmOwningSoft;
+    OwnerRanges lmSoft, lmCloth, lmFluid, lmStrand;
+    uint64_t layoutRevision = 0;
     // surface render data: meshes bound by cn_world_add_surface_mesh (owner-relative particle
     // indices), or a caller's copy from cn_world_set_surface_render; packed arrays below
     struct SurfaceMesh {
@@ -825,6 +830,50 @@ void packSurfaces(cn_world &w, const std::vector<uint32_t> &softOff, const std::
     }
 }
 
+// The ParticleLayoutMapping views of the packed particles (physics_world.cpp:4919-5400 fill the
+// same per-particle arrays: strand ids / orders for strand particles, 0xffffffff elsewhere; the
+// owning soft body for soft-body particles, 0xffffffff elsewhere; no strand roles without
+// suturing) and each owner's contiguous slot range.
+void packLayoutMapping(cn_world &w)
+{
+    const size_t N = w.radii.size();
+    w.lmEnv.resize(N); w.lmPhase.resize(N); w.lmLayer.resize(N); w.lmMask.resize(N);
+    w.lmStrandId.assign(N, 0xffffffffu); w.lmStrandOrder.assign(N, 0xffffffffu);
+    w.lmStrandRole.assign(N, 0u); w.lmOwningSoft.assign(N, 0xffffffffu);
+    cn_world::OwnerRanges *byType[6] = {nullptr, &w.lmSoft, &w.lmFluid, &w.lmStrand, nullptr, &w.lmCloth};
+    const size_t owners[6] = {0, w.softBodies.size(), w.fluids.size(), w.strands.size(), 0, w.cloths.size()};
+    for (int t = 0; t < 6; ++t) {
+        if (!byType[t]) continue;
+        cn_world::OwnerRanges &r = *byType[t];
+        r.ids.resize(owners[t]);
+        r.env.assign(owners[t], 0u);
+        r.off.assign(owners[t], 0u);
+        r.cnt.assign(owners[t], 0u);
+        for (size_t k = 0; k < owners[t]; ++k) r.ids[k] = k;
+    }
+    for (size_t i = 0; i < N; ++i) {
+        w.lmEnv[i] = w.meta[4 * i];
+        w.lmPhase[i] = w.meta[4 * i + 1];
+        w.lmLayer[i] = w.meta[4 * i + 2];
+        w.lmMask[i] = w.meta[4 * i + 3];
+        const uint32_t type = w.ownerTypes[i], owner = w.ownerIdx[i];
+        if (type < 6 && byType[type] && owner < owners[type]) {
+            cn_world::OwnerRanges &r = *byType[type];
+            if (r.cnt[owner] == 0u) {
+                r.off[owner] = uint32_t(i);
+                r.env[owner] = w.meta[4 * i];
+            }
+            if (type == CN_OWNER_STRAND) {
+                w.lmStrandId[i] = owner;
+                w.lmStrandOrder[i] = r.cnt[owner];
+            }
+            ++r.cnt[owner];
+        }
+        if (type == CN_OWNER_SOFT_BODY) w.lmOwningSoft[i] = owner;
+    }
+    ++w.layoutRevision;
+}
+
 cn_status pack(cn_world &w)
 {
     w.x.clear(); w.v.clear(); w.radii.clear(); w.kinds.clear(); w.meta.clear(); w.matIdx.clear();
@@ -1069,6 +1118,7 @@ cn_status pack(cn_world &w)
         w.bodyColIdx.insert(w.bodyColIdx.end(), bodyCols[b].begin(), bodyCols[b].end());
     }
     packSurfaces(w, softOff, clothOff);
+    packLayoutMapping(w);
     return CN_OK;
 }
 
@@ -1328,6 +1378,52 @@ CN_API cn_status cn_world_set_rigid_proxy_particles(cn_world *w, const cn_rigid_
             return CN_OK;
         }
     w->proxies.push_back(std::move(rp));
+    return CN_OK;
+}
+
+CN_API cn_status cn_world_particle_layout_mapping(cn_world *w, cn_particle_layout_mapping *o)
+{
+    if (!w || !o) return cn::setError(CN_ERR_INVALID_ARGUMENT, "cn_world_particle_layout_mapping: null argument");
+    if (!w->packed) {
+        const cn_status st = pack(*w);
+        if (st != CN_OK) return cn::setError(st, "cn_world_particle_layout_mapping: invalid world");
+        w->packed = true;
+    }
+    std::memset(o, 0, sizeof(*o));
+    o->particle_count = uint32_t(w->radii.size());
+    o->soft_body_count = uint32_t(w->softBodies.size());
+    o->cloth_count = uint32_t(w->cloths.size());
+    o->fluid_count = uint32_t(w->fluids.size());
+    o->strand_count = uint32_t(w->strands.size());
+    o->layout_revision = w->layoutRevision;
+    o->environment_indices = ptr(w->lmEnv);
+    o->particle_kinds = ptr(w->kinds);
+    o->owner_types = ptr(w->ownerTypes);
+    o->owner_indices = ptr(w->ownerIdx);
+    o->strand_ids = ptr(w->lmStrandId);
+    o->strand_orders = ptr(w->lmStrandOrder);
+    o->strand_roles = ptr(w->lmStrandRole);
+    o->owning_soft_body_indices = ptr(w->lmOwningSoft);
+    o->particle_material_indices = ptr(w->matIdx);
+    o->fluid_material_indices = ptr(w->fluidMatIdx);
+    o->phases = ptr(w->lmPhase);
+    o->collision_layers = ptr(w->lmLayer);
+    o->collision_masks = ptr(w->lmMask);
+    o->adjacency_offsets = ptr(w->adjOff);
+    o->adjacency_counts = ptr(w->adjCnt);
+    auto ranges = [](cn_world::OwnerRanges &r) {
+        cn_particle_owner_ranges out{};
+        out.count = uint32_t(r.ids.size());
+        out.ids = ptr(r.ids);
+        out.environment_indices = ptr(r.env);
+        out.particle_offsets = ptr(r.off);
+        out.particle_counts = ptr(r.cnt);
+        return out;
+    };
+    o->soft_bodies = ranges(w->lmSoft);
+    o->cloths = ranges(w->lmCloth);
+    o->fluids = ranges(w->lmFluid);
+    o->strands = ranges(w->lmStrand);
     return CN_OK;
 }
 

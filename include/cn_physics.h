@@ -463,7 +463,7 @@ typedef struct cn_meta {
     uint32_t particle_particle_candidate_count;
     uint32_t required_particle_particle_candidate_count;
     uint32_t particle_particle_candidate_overflow;
-    uint32_t fluid_boundary_candidate_overflow;  /* more boundary colliders than the per-particle mask holds */
+    uint32_t fluid_boundary_candidate_overflow;  /* particles whose boundary candidates exceeded their capacity */
     uint32_t active_particle_rigid_contact_count;
     uint32_t active_particle_contact_count;
     uint32_t fluid_neighbor_truncations;         /* particles whose neighbour list hit max_fluid_neighborhood */
@@ -778,6 +778,32 @@ CN_API cn_status cn_diff_backward(cn_diff *diff, const void *grad_x_out, const v
                                   void *grad_tet_compliance, void *grad_x0, void *grad_v0, void *stream);
 /* Device bytes of the state the adjoint keeps (checkpoints, one segment, one substep). */
 CN_API cn_status cn_diff_memory(cn_diff *diff, uint64_t *bytes);
+
+/* ParticleLayoutMapping (include/engine/particle_layout_mapping.h:11-68, filled by
+ * Runtime::tryGetPreparedParticleLayoutMapping, src/engine/runtime.cpp:867-955): the packed
+ * particle slots' owners and filters, and each owner's slot range, for the RL-environment glue
+ * that slices the exported particle buffers.  Per-particle arrays hold particle_count entries,
+ * per-owner arrays the owner count; owner ids are the handles the cn_world_add_* calls returned
+ * (the reference's EntityId of the owning entity).  layout_revision changes whenever a new
+ * packing changes how slots are interpreted.  Pointers stay valid until the next authoring call. */
+typedef struct cn_particle_owner_ranges {
+    uint32_t count;
+    const uint64_t *ids;
+    const uint32_t *environment_indices, *particle_offsets, *particle_counts;
+} cn_particle_owner_ranges;
+
+typedef struct cn_particle_layout_mapping {
+    uint32_t particle_count, soft_body_count, cloth_count, fluid_count, strand_count;
+    uint64_t layout_revision;
+    const uint32_t *environment_indices, *particle_kinds, *owner_types, *owner_indices;
+    const uint32_t *strand_ids, *strand_orders, *strand_roles, *owning_soft_body_indices;
+    const uint32_t *particle_material_indices, *fluid_material_indices;
+    const uint32_t *phases, *collision_layers, *collision_masks;
+    const uint32_t *adjacency_offsets, *adjacency_counts;
+    cn_particle_owner_ranges soft_bodies, cloths, fluids, strands;
+} cn_particle_layout_mapping;
+
+CN_API cn_status cn_world_particle_layout_mapping(cn_world *world, cn_particle_layout_mapping *out);
 
 /* Allocation-free broadphase sort (no counterpart in the reference).
  * For callers that must not allocate device memory while they run -- engines whose device memory

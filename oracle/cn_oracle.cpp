@@ -376,7 +376,7 @@ struct cno_solver {
     std::vector<CellRange> cellRanges;
     uint32_t cellRangeCapacity = 0;
     std::vector<uint32_t> nbrCount, nbrList;
-    std::vector<f4> fluidDelta, fluidNormalC, fluidDx;
+    std::vector<f4> fluidDelta, fluidNormalC, fluidDx, fluidVorticity;
     std::vector<std::vector<uint32_t>> boundaryCand; // collider indices per particle (fluids)
     std::vector<std::pair<uint32_t, uint32_t>> rigidPairs;    // (particle, body)
     std::vector<std::pair<uint32_t, uint32_t>> particlePairs; // (a, b)
@@ -1182,6 +1182,71 @@ void fluidDeltaPositions(cno_solver &s, uint32_t iter, float dt)
         bd = bd * bdelta;
         const f3 packed = dp * coef + bd;
         s.fluidDx[i] = mk4(packed, weight);
+    }
+}
+
+// physics_fluid_compute_vorticity.cs.hlsl:13-76 then physics_fluid_apply_vorticity_confinement.cs.hlsl:13-92,
+// over the lists of the post-update rebuild: the curl of the velocity field from same-material
+// neighbours, then the confinement force along the gradient of its magnitude, added to v.
+bool anyVorticity(const cno_solver &s)
+{
+    for (const cn_fluid_material &m : s.fluidMaterials)
+        if (std::max(m.vorticity_confinement, 0.0f) > kEps) return true;
+    return false;
+}
+void fluidVorticity(cno_solver &s, float dt)
+{
+    const uint32_t maxN = s.desc.max_fluid_neighborhood;
+    s.fluidVorticity.assign(s.N, f4{0, 0, 0, 0});
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        if (s.kinds[i] != CN_PARTICLE_FLUID) continue;
+        const cn_fluid_material &fm = s.fluidMaterials[s.fluidMatIdx[i]];
+        if (std::max(fm.vorticity_confinement, 0.0f) <= kEps) continue;
+        const f4 self = s.x[i];
+        if (self.w <= kEps) continue;
+        const f3 sp = xyz(self), sv = xyz(s.v[i]);
+        const float h = std::max(fm.smoothing_radius, 1.0e-4f);
+        f3 curl{0, 0, 0};
+        const uint32_t *lst = &s.nbrList[size_t(i) * maxN];
+        for (uint32_t k = 0; k < s.nbrCount[i]; ++k) {
+            const uint32_t c = lst[k];
+            if (s.fluidMatIdx[i] != s.fluidMatIdx[c]) continue;
+            const f3 delta = sp - xyz(s.x[c]);
+            const float dist = length(delta);
+            if (dist <= kEps || dist >= h) continue;
+            curl += cross(xyz(s.v[c]) - sv, SpikyGrad(delta, dist, h));
+        }
+        s.fluidVorticity[i] = mk4(curl, length(curl));
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t ii = 0; ii < int64_t(s.N); ++ii) {
+        const uint32_t i = uint32_t(ii);
+        if (s.kinds[i] != CN_PARTICLE_FLUID) continue;
+        const cn_fluid_material &fm = s.fluidMaterials[s.fluidMatIdx[i]];
+        const float conf = std::max(fm.vorticity_confinement, 0.0f);
+        if (conf <= kEps) continue;
+        const f4 self = s.x[i];
+        if (self.w <= kEps) continue;
+        const f4 sc = s.fluidVorticity[i];
+        if (sc.w <= kEps) continue;
+        const f3 sp = xyz(self);
+        const float h = std::max(fm.smoothing_radius, 1.0e-4f);
+        f3 grad{0, 0, 0};
+        const uint32_t *lst = &s.nbrList[size_t(i) * maxN];
+        for (uint32_t k = 0; k < s.nbrCount[i]; ++k) {
+            const uint32_t c = lst[k];
+            if (s.fluidMatIdx[i] != s.fluidMatIdx[c]) continue;
+            const f3 delta = sp - xyz(s.x[c]);
+            const float dist = length(delta);
+            if (dist <= kEps || dist >= h) continue;
+            grad += s.fluidVorticity[c].w * SpikyGrad(delta, dist, h);
+        }
+        const float gl = length(grad);
+        if (gl <= kEps) continue;
+        const f3 force = conf * cross(grad / gl, xyz(sc));
+        s.v[i] = mk4(xyz(s.v[i]) + dt * force, 0.0f);
     }
 }
 
@@ -3097,11 +3162,13 @@ void stepFrame(cno_solver &s, float frameDt)
         if (s.hasDynamic) updateRigidVelocities(s, dt);
         updateVelocities(s, dt);
         if (hasFluidWork) projectFluidBoundaryVelocities(s, dt);
-        if (hasFluidWork && s.postUpdateNeighbors) {
-            // post-update neighbour rebuild (physics_solver.cpp:1262-1268); its lists feed only
-            // vorticity confinement and render anisotropy.
+        const bool vorticity = hasFluidWork && anyVorticity(s);
+        if (hasFluidWork && (s.postUpdateNeighbors || vorticity)) {
+            // post-update neighbour rebuild (physics_solver.cpp:1262-1268); its lists feed
+            // vorticity confinement (physics_solver.cpp:1269-1285) and render anisotropy.
             buildFluidNeighbors(s, maxIt > 0 ? maxIt - 1 : 0);
         }
+        if (vorticity) fluidVorticity(s, dt);
         if (hasSoftSoftContact && contactIt > 0) particleContactVelocities(s, contactIt);
         if (hasSoftRigidContact && contactIt > 0) particleRigidContactVelocities(s, contactIt);
         skinSurfaceVertices(s);

@@ -3,8 +3,8 @@
 (physics_particle_rigid_solve_contacts.cs.hlsl:64-141, ..._solve_contact_velocities.cs.hlsl),
 the bodies' summed corrections applied per iteration (physics_rigid_apply_corrections,
 physics_rigid_apply_contact_velocities) and their velocities from the pose change
-(physics_rigid_update_velocities).  The reference sums a body's corrections with float atomics,
-so GPU and oracle agree within tolerance, not bit for bit."""
+(physics_rigid_update_velocities), also with fluid particles.  The reference sums a body's
+corrections with float atomics, so GPU and oracle agree within tolerance, not bit for bit."""
 import numpy as np
 import pytest
 
@@ -39,13 +39,52 @@ def test_oracle_sphere_comes_to_rest_on_the_tissue():
     assert x[:, 1].max() < 0.26                         # the tissue top is pressed, not pierced
 
 
+def fluid_tank_and_sphere(mass=0.2, radius=0.06):
+    """A small fluid tank (static walls) with a light dynamic sphere dropped into it: fluid
+    particles take particle-rigid contacts against the dynamic body (physics_particle_count_
+    particle_rigid_candidates.cs.hlsl: solid particles against every body, fluid ones against
+    dynamic bodies) and push it back (the body's share, physics_particle_rigid_solve_contacts.cs.hlsl:97-140)."""
+    w, desc, dt = scenes.dam_break(nx=12, ny=6, nz=12, box=(0.6, 0.6, 0.6))
+    inv_i = 1.0 / (0.4 * mass * radius * radius)
+    b = w.add_rigid_body("dynamic", position=(0.3, 0.42, 0.3), mass=mass, inverse_inertia=(inv_i,) * 3)
+    w.add_collider(b, "sphere", (radius,), friction=0.2)
+    w.soa()
+    return w, desc, dt, b
+
+
+def test_oracle_sphere_enters_the_fluid_and_is_held_up():
+    w, desc, dt, b = fluid_tank_and_sphere()
+    o = cn_oracle.Oracle(desc, w.soa())
+    heights = []
+    for _ in range(150):
+        o.step(dt)
+        heights.append(o.read_rigid_bodies()[0][b, 1])
+    x, _, _ = o.read_particles()
+    assert min(heights) < 0.33                          # it went into the fluid layer (top ~0.33)
+    assert 0.3 < heights[-1] < 0.5                      # and floats, held up by the fluid
+    assert np.isfinite(x).all()
+
+
 @pytest.mark.gpu
-def test_fluid_with_dynamic_bodies_is_rejected():
-    w, _ = tissue_and_sphere()
-    w.add_fluid_grid((0.1, 0.1, 0.1), 0.05, position=(1.0, 0.5, 0.0), radius=0.03)
-    sv = Solver(solver_desc())
-    with pytest.raises(CNError):
-        sv.sync_world(w.soa())
+def test_fluid_with_a_dynamic_body_against_the_oracle():
+    w, desc, dt, b = fluid_tank_and_sphere()
+    soa = w.soa()
+    gpu = Solver(desc)
+    gpu.sync_world(soa)
+    ora = cn_oracle.Oracle(desc, soa)
+    for frame in range(45):
+        gpu.step(dt)
+        ora.step(dt)
+        if frame == 34:   # before the first contact: the same sums in the same order
+            for a, c in zip(gpu.read_particles(), ora.read_particles()):
+                np.testing.assert_allclose(a, c, rtol=1e-5, atol=1e-6)
+    # the first contacts: the body's share is summed with float atomics (GPU) or in pair order
+    # (oracle), as the reference's order is the GPU's schedule
+    for a, c in zip(gpu.read_particles(), ora.read_particles()):
+        np.testing.assert_allclose(a, c, rtol=1e-4, atol=1e-4)
+    gb, ob = gpu.read_rigid_bodies(), ora.read_rigid_bodies()
+    np.testing.assert_allclose(gb[0][b, :3], ob[0][b, :3], rtol=1e-4, atol=1e-4)
+    assert gpu.validate_gpu_meta()["status"] == "OK"
 
 
 @pytest.mark.gpu

@@ -166,3 +166,43 @@ def test_rigid_candidates_from_the_lbvh_keep_the_scan_order():
     g, o = gpu.debug_read("rigid_contacts"), ora.debug_read("rigid_contacts")
     assert g.size == o.size > 0 and np.array_equal(g.view(np.uint8), o.view(np.uint8))
     same_state(gpu, ora)
+
+
+def multi_environment_fluid(envs=14, n=(6, 5, 6), seed=0):
+    """`envs` fluid blocks, each in its own environment with its own five static walls (5 x envs
+    colliders: past the 64 bits of the boundary mask, so the per-particle candidate lists over the
+    collider LBVH carry the boundary), side by side along x."""
+    w = World()
+    sp = 0.05
+    body = w.add_rigid_body("static")
+    size = (n[0] * sp, n[1] * sp, n[2] * sp)
+    box = (0.6, 0.5, 0.6)
+    t = 0.1
+    for e in range(envs):
+        ox = e * 1.0
+        w.add_fluid_grid(size, sp, position=(ox + 0.3, size[1] * 0.5 + 0.03, 0.3), radius=0.6 * sp,
+                         environment=e)
+        bx, by, bz = box
+        for half, local in (((bx * 0.5 + 2 * t, t, bz * 0.5 + 2 * t), (ox + bx * 0.5, -t, bz * 0.5)),
+                            ((t, by * 0.5 + 2 * t, bz * 0.5 + 2 * t), (ox - t, by * 0.5, bz * 0.5)),
+                            ((t, by * 0.5 + 2 * t, bz * 0.5 + 2 * t), (ox + bx + t, by * 0.5, bz * 0.5)),
+                            ((bx * 0.5 + 2 * t, by * 0.5 + 2 * t, t), (ox + bx * 0.5, by * 0.5, -t)),
+                            ((bx * 0.5 + 2 * t, by * 0.5 + 2 * t, t), (ox + bx * 0.5, by * 0.5, bz + t))):
+            w.add_collider(body, "box", half, local, environment=e)
+    w.soa()
+    x = w.positions()
+    rng = np.random.default_rng(seed)
+    x[:, :3] += rng.uniform(-1e-4, 1e-4, size=(x.shape[0], 3)).astype(np.float32)
+    return w, solver_desc(substeps=2, fluid_iterations=4, enable_blocking_readback=0), 1.0 / 120.0
+
+
+def test_fluid_against_more_than_64_colliders():
+    w, desc, dt = multi_environment_fluid()
+    assert w.counts()["colliders"] == 70
+    gpu, ora, _ = pair(w, desc)
+    step_both(gpu, ora, dt, 6)
+    for a, b in zip(gpu.read_particles(), ora.read_particles()):
+        assert np.array_equal(a, b)
+    same_lists(gpu, ora)
+    meta = gpu.validate_gpu_meta()
+    assert meta["status"] == "OK" and meta["fluid_boundary_candidate_overflow"] == 0, meta
