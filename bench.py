@@ -312,7 +312,7 @@ def run_ours(args):
         if rank == 0:
             line["served"] = served
     if world == 1 and not args.no_diff:
-        line["differentiation"] = run_diff(stream)
+        line["differentiation"] = run_diff(stream, cpu_sample=not args.no_cpu_baseline)
     if world == 1 and not args.no_configs:
         line["other_configs"] = run_other_configs(stream, sh, cpu=not args.no_cpu_baseline)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -398,7 +398,9 @@ def run_served(args, stream, sh, rank: int = 0, world: int = 1) -> dict:
     b = Batch(bd)
     srv = Server(b, dt)
     sids = [srv.register(sc.world.soa()) for sc in pool]
-    prefetched = sum(1 for k in sids if srv.admit(k))  # warm start: resident before the clock starts
+    # warm start: the even-numbered half of the pool is resident before the clock starts; the
+    # other half is admitted against the budget by the server when its first request arrives
+    prefetched = sum(1 for j, k in enumerate(sids) if mine[j] % 2 == 0 and srv.admit(k))
     poses = [serving.tool_start(d) for d in serving.pool_dims(count, seed=0)]
     reqs = serving.poisson_requests(poses, steps_per_second=args.serve_rate, duration_s=args.serve_seconds, seed=1)
     _, reqs = serving.shard(reqs, count, rank, world)
@@ -410,6 +412,7 @@ def run_served(args, stream, sh, rank: int = 0, world: int = 1) -> dict:
     b.close()
     part = {"out": out, "P": P, "T": T, "E": E, "prefetched": prefetched, "budget_bytes": bstats["budget_bytes"],
             "budget_used_bytes": bstats["budget_used_bytes"], "tune": tune}
+    cpu = served_cpu_baseline(pool, desc, dt) if (rank == 0 and world == 1 and not args.no_cpu_baseline) else None
     parts = [part]
     if world > 1:
         parts = [None] * world
@@ -450,7 +453,36 @@ def run_served(args, stream, sh, rank: int = 0, world: int = 1) -> dict:
                    "admissions_during_run": merged["admissions"] - prefetched, "evictions": merged["evictions"],
                    "budget_bytes": sum(q["budget_bytes"] for q in parts),
                    "budget_used_bytes": sum(q["budget_used_bytes"] for q in parts)},
+        "cpu_baseline": cpu,
     }
+
+
+def _oracle_module():
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import cn_oracle
+    return cn_oracle, cn_oracle.set_threads(os.cpu_count() or 1)
+
+
+def served_cpu_baseline(pool, desc, dt, budget_s: float = 8.0) -> dict:
+    """The oracle stepping the pool's scenes one after another, one frame each (the per-scene CPU
+    stepping a served pool replaces), in pool order until the time budget is spent."""
+    cn_oracle, threads = _oracle_module()
+    lat, particles = [], 0
+    t0 = time.perf_counter()
+    for sc in pool:
+        o = cn_oracle.Oracle(desc, sc.world.soa())
+        o.set_kinematic_target(sc.tool, tuple(float(v) for v in sc.tool_pose))
+        t1 = time.perf_counter()
+        o.step(dt)
+        lat.append((time.perf_counter() - t1) * 1e3)
+        particles += sc.particles
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = sum(lat) / 1e3
+    return {"value": round(particles * desc.substeps / el, 1), "unit": "particle-substeps/s", "cores": threads,
+            "kind": "port", "frame_ms": {"p50": round(float(np.percentile(lat, 50)), 3),
+                                         "p99": round(float(np.percentile(lat, 99)), 3)},
+            "sample": f"one frame of each of the first {len(lat)} pool scenes ({particles} particles), {el:.1f} s"}
 
 
 def run_other_configs(stream, sh, cpu: bool = True) -> dict:
@@ -495,9 +527,7 @@ def run_other_configs(stream, sh, cpu: bool = True) -> dict:
             "us_per_kernel": round(ms * 1e3 / max(kernels, 1), 3)}
     sv.close()
     if cpu:
-        sys.path.insert(0, str(ROOT / "oracle"))
-        import cn_oracle
-        threads = cn_oracle.set_threads(os.cpu_count() or 1)
+        cn_oracle, threads = _oracle_module()
         w2, d2, dt2 = scenes.xpbd_cube()
         o = cn_oracle.Oracle(d2, w2.soa())
         t0, frames = time.perf_counter(), 0
@@ -565,6 +595,21 @@ def run_other_configs(stream, sh, cpu: bool = True) -> dict:
                            "ms_per_frame": round(surf_ms, 4), "algorithmic_bytes": surf_bytes,
                            "achieved_gbs": round(surf_bytes / max(surf_ms, 1e-6) / 1e6, 1)}}
     sv.close()
+    if cpu:
+        # the oracle on the same scene for one frame of 2 substeps at the substep dt of the
+        # 8-substep frame: the work per particle-substep is that of the full frame
+        cn_oracle, threads = _oracle_module()
+        w2, d2, dt2, tool2 = scenes.mixed_surgical()
+        sub = d2.substeps
+        d2.substeps = 2
+        o = cn_oracle.Oracle(d2, w2.soa())
+        o.set_kinematic_target(tool2, scenes.tool_path(dt2))
+        t0 = time.perf_counter()
+        o.step(dt2 * 2 / sub)
+        el = time.perf_counter() - t0
+        out["mixed_surgical"]["cpu_baseline"] = {
+            "value": round(n * 2 / el, 1), "unit": "particle-substeps/s", "cores": threads, "kind": "port",
+            "sample": f"one frame of 2 substeps (substep dt 1/{int(round(sub / dt2))}) of the same scene, {el:.1f} s"}
     return out
 
 
@@ -583,7 +628,7 @@ def _diff_block(dims, spacing=0.1, base=1e-11, seed=0):
     return w
 
 
-def run_diff(stream) -> dict:
+def run_diff(stream, cpu_sample: bool = True) -> dict:
     """Differentiation: a 28x14x28-vertex block (47,385 tets), 32 substeps x 20 iterations,
     surface-vertex MSE against a target rolled out with log-normal (sigma 0.3) per-tet stiffness;
     gradient with respect to per-tet compliance and initial velocities, checkpoint every 8
@@ -663,6 +708,21 @@ def run_diff(stream) -> dict:
     fd = (L(c64 + eps * u) - L(c64 - eps * u)) / (2 * eps)
     an = float((g64 * u).sum())
     r64.close()
+
+    # CPU: the oracle's float32 XPBD substep on the same block, 4 of the 32 substeps; a
+    # central-difference gradient with respect to every compliance costs 2 T rollouts
+    cpu = None
+    if cpu_sample:
+        from cn_physics import solver_desc
+        cn_oracle, threads = _oracle_module()
+        o = cn_oracle.Oracle(solver_desc(substeps=4, default_iterations=20, soft_internal_relaxation=0.2), w.soa())
+        t0 = time.perf_counter()
+        o.step(4.0 / 480.0)
+        sub_s = (time.perf_counter() - t0) / 4
+        cpu = {"value": round(n / sub_s, 1), "unit": "particle-substeps/s", "cores": threads, "kind": "port",
+               "rollout_s": round(sub_s * 32, 3), "fd_gradient_s": round(sub_s * 32 * 2 * t, 1),
+               "sample": "4 substeps x 20 iterations of the same block (float32); rollout = 32 substeps, "
+                         f"fd_gradient = 2 x {t} rollouts"}
     return {"workload": f"XPBD block {dims[0]}x{dims[1]}x{dims[2]} vertices ({t} tets, {n} particles), 32 substeps x "
                         f"20 iterations, checkpoint every 8 substeps, surface MSE vs a log-normal (sigma 0.3) "
                         f"stiffness target; gradients w.r.t. per-tet compliance and initial velocities",
@@ -670,7 +730,8 @@ def run_diff(stream) -> dict:
             "particle_substeps_per_s_forward": round(n * 32 / (fwd_ms / 1e3), 1),
             "adjoint_state_bytes": kept, "full_tape_bytes": tape,
             "fd_check": {"instance": "9x8x8 vertices (1,960 tets), FP64, eps 1e-6, random log-space direction",
-                         "adjoint": an, "central_difference": fd, "relative_error": abs(an - fd) / abs(fd)}}
+                         "adjoint": an, "central_difference": fd, "relative_error": abs(an - fd) / abs(fd)},
+            "cpu_baseline": cpu}
 
 
 def solver_neighbor_mean(solver) -> tuple:
