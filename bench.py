@@ -526,6 +526,19 @@ def run_other_configs(stream, sh, cpu: bool = True) -> dict:
             "ms_per_frame": round(ms, 4), "kernels_per_frame": kernels,
             "us_per_kernel": round(ms * 1e3 / max(kernels, 1), 3)}
     sv.close()
+    # the same cube under the other XPBD schedules (all opt-in): fused iterations (one cluster
+    # kernel per substep) and the graph-coloured Jacobi / Gauss-Seidel schedules
+    cube["schedules"] = {}
+    for label, sched, fused in (("gather_fused", 0, 1), ("colour_jacobi", 1, 0), ("colour_jacobi_fused", 1, 1),
+                                ("gauss_seidel", 2, 0), ("gauss_seidel_fused", 2, 1)):
+        w2, d2, dt2 = scenes.xpbd_cube()
+        d2.soft.xpbd_schedule, d2.soft.fused_iterations = sched, fused
+        s2 = Solver(d2)
+        s2.sync_world(w2.soa())
+        ms2 = timed(s2, dt2, 20)
+        cube["schedules"][label] = {"ms_per_frame": round(ms2, 4), "kernels_per_frame": s2.graph_stats()[0],
+                                    "fused": s2.schedule_info()["fused_iterations"]}
+        s2.close()
     if cpu:
         cn_oracle, threads = _oracle_module()
         w2, d2, dt2 = scenes.xpbd_cube()

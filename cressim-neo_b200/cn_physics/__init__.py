@@ -62,6 +62,30 @@ def solver_desc(**overrides) -> _abi.SolverDesc:
     return d
 
 
+def colour_constraints(elements, element_count: int) -> tuple:
+    """Greedy graph colouring of one constraint family (host only): `elements` (M, k) uint32 are
+    each constraint's particles (segments for strand joints); entries >= element_count are
+    ignored.  Returns (order, starts): the constraints grouped by colour, ascending within a
+    colour, and the colour boundaries (colours + 1 entries)."""
+    e = np.ascontiguousarray(elements, dtype=np.uint32)
+    m = e.shape[0]
+    k = e.shape[1] if e.ndim == 2 else 1
+    order = np.zeros(max(m, 1), np.uint32)
+    cap = max(k * 64, 64)
+    while True:
+        starts = np.zeros(cap + 1, np.uint32)
+        n = C.c_uint32()
+        st = load().cn_colour_constraints(e.ctypes.data_as(_abi.P_u32), m, k, element_count,
+                                          order.ctypes.data_as(_abi.P_u32), starts.ctypes.data_as(_abi.P_u32),
+                                          cap, C.byref(n))
+        if st == 0:
+            return order[:m].copy(), starts[:n.value + 1].copy()
+        if n.value > cap:
+            cap = n.value
+            continue
+        _check(st)
+
+
 def _f32(arr) -> C.POINTER(C.c_float):
     return arr.ctypes.data_as(_abi.P_f32)
 
@@ -508,6 +532,16 @@ class Solver:
         k, t = C.c_uint32(), C.c_uint32()
         _check(self._lib.cn_solver_graph_stats(self._h, C.byref(k), C.byref(t)))
         return k.value, t.value
+
+    def schedule_info(self) -> dict:
+        """The XPBD schedule in use: xpbd_schedule, fused_iterations (1: one cluster kernel per
+        substep), cluster_ctas, threads_per_cta, colours per family (edges, strand segments,
+        bends + dihedrals, strand joints, strand distances, tets)."""
+        v = _abi.ScheduleInfo()
+        _check(self._lib.cn_solver_schedule_info(self._h, C.byref(v)))
+        out = {name: getattr(v, name) for name, _ in _abi.ScheduleInfo._fields_}
+        out["colours"] = dict(zip(("edges", "segments", "bends", "joints", "distances", "tets"), v.colours))
+        return out
 
     def gpu_scene_view(self) -> dict:
         v = _abi.SceneView()

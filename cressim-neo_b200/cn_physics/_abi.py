@@ -28,8 +28,18 @@ class JointSettings(C.Structure):
     _fields_ = [(f"f{i}", f32) for i in range(8)]
 
 
+XPBD_GATHER, XPBD_COLOUR_JACOBI, XPBD_COLOUR_GAUSS_SEIDEL = 0, 1, 2
+FUSED_OFF, FUSED_ON = 0, 1
+
+
 class SoftSettings(C.Structure):
-    _fields_ = [("internal_relaxation", f32), ("reserved", f32 * 7)]
+    _fields_ = [("internal_relaxation", f32), ("xpbd_schedule", u32), ("fused_iterations", u32),
+                ("reserved", f32 * 5)]
+
+
+class ScheduleInfo(C.Structure):
+    _fields_ = [("xpbd_schedule", u32), ("fused_iterations", u32), ("cluster_ctas", u32),
+                ("threads_per_cta", u32), ("colours", u32 * 6)]
 
 
 class FluidSettings(C.Structure):
@@ -311,6 +321,8 @@ SIGNATURES = [
     ("cn_solver_set_timing", C.c_int, [C.c_void_p, u32]),
     ("cn_solver_kernel_times", C.c_int, [C.c_void_p, C.c_void_p, u32, P_u32]),
     ("cn_solver_graph_stats", C.c_int, [C.c_void_p, P_u32, P_u32]),
+    ("cn_solver_schedule_info", C.c_int, [C.c_void_p, C.POINTER(ScheduleInfo)]),
+    ("cn_colour_constraints", C.c_int, [P_u32, u32, u32, u32, P_u32, P_u32, u32, P_u32]),
     ("cn_world_particle_layout_mapping", C.c_int, [C.c_void_p, C.POINTER(ParticleLayoutMapping)]),
     ("cn_sort_cell_keys_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, u32, C.c_void_p, C.c_void_p]),
     ("cn_solver_debug_read", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t, C.POINTER(C.c_size_t)]),

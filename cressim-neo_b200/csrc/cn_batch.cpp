@@ -356,6 +356,8 @@ CN_API cn_status cn_batch_create(const cn_batch_desc *d, int device, cn_batch **
         return setError(CN_ERR_NO_DEVICE, "cn_batch_create: no CUDA device");
     }
     if (device < 0 || device >= count) return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_create: bad device");
+    if (d->solver.soft.xpbd_schedule != CN_XPBD_GATHER)
+        return setError(CN_ERR_UNSUPPORTED, "cn_batch_create: a batch runs the gather XPBD schedule");
     auto *b = new cn_batch();
     b->desc = *d;
     b->device = device;

@@ -82,6 +82,10 @@ struct WorkList {
     uint32_t grid = 0;
 };
 
+// XPBD families in the order a soft iteration solves them (physics_solver.cpp:915-1019).
+constexpr uint32_t kFamilies = 6u;
+enum : uint32_t { kFamEdges = 0u, kFamSegments = 1u, kFamBends = 2u, kFamJoints = 3u, kFamDistances = 4u, kFamTets = 5u };
+
 struct Scene {
     // per-tick work lists of a batch (all null for a single world)
     WorkList wP, wE, wT, wB, wC;      // particles, edges, tets, rigid bodies, colliders
@@ -133,6 +137,12 @@ struct Scene {
     float4 *jointCorr = nullptr;  // 2 per joint (twistRotationA, twistRotationB)
     float4 *distCorr = nullptr;   // 2 per distance
     float4 *posCorr = nullptr, *velCorr = nullptr;
+    // coloured XPBD schedules: per family (kFam*) the constraint indices grouped by colour,
+    // the colour-Jacobi per-particle sum of a family's corrections (zero between families) and
+    // the per-segment sum of the joint family's orientation corrections
+    const uint32_t *colOrder[kFamilies] = {};
+    float4 *softAcc = nullptr;
+    float4 *orientAcc = nullptr;
 
     // ---- rigid bodies / colliders ----
     uint32_t B = 0, C = 0;
@@ -348,6 +358,26 @@ void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st);
 // Vorticity confinement (after launchFluidNeighborsOnly's post-update lists): curl, then force.
 void launchFluidVorticity(const Scene &s, float dt, cudaStream_t st);
 void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st);
+// The XPBD schedule of a solver: CN_XPBD_* and, for the coloured schedules, each family's colour
+// count and colour start offsets into Scene::colOrder (host copies for the per-colour launches,
+// device copies for the fused kernel).
+struct XpbdPlan {
+    uint32_t schedule = 0;
+    uint32_t colours[kFamilies] = {};
+    const uint32_t *hostStarts[kFamilies] = {};
+    const uint32_t *devStarts[kFamilies] = {};
+};
+void launchSoftIteration(const Scene &s, float dt, const Config &c, const XpbdPlan &plan, cudaStream_t st);
+// Fused iterations: one thread-block cluster runs every iteration of a substep (soft families in
+// `plan`'s schedule, then the particle-rigid contacts when `rigid`), phases separated by cluster
+// barriers.  fusedIterationsShape() is {0, 0} when the cluster launch is unavailable.
+struct FusedShape {
+    uint32_t ctas = 0, threads = 0;
+};
+FusedShape fusedIterationsShape();
+void launchFusedIterations(const Scene &s, const Config &c, float dt, const XpbdPlan &plan, uint32_t iterations,
+                           uint32_t softIterations, uint32_t contactIterations, bool rigid, const FusedShape &shape,
+                           cudaStream_t st);
 void launchContacts(const Scene &s, const Config &c, bool particleContacts, bool rigidContacts,
                     cudaStream_t st);
 void launchUpdateVelocities(const Scene &s, float dt, const float4 *fluidDelta, cudaStream_t st);

@@ -2,6 +2,7 @@
 // reporting, the device arena, incidence tables and the solver constants.
 #pragma once
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -72,6 +73,56 @@ template <class F> Incidence buildIncidence(uint32_t n, uint32_t constraints, ui
             const uint32_t p = particlesOf(c, k);
             if (p < n) out.inc[out.ranges[p].x + fill[p]++] = make_uint2(c, k);
         }
+    return out;
+}
+
+// Greedy graph colouring of one constraint family: constraint c, in ascending order, takes the
+// lowest colour no earlier constraint sharing one of its elements has (elementOf(c, k) >= n is
+// no element).  order = the constraints grouped by colour, ascending within a colour;
+// starts[k] .. starts[k + 1] = colour k.  Per-element used-colour bitsets of `words` 64-bit
+// words, widened when a constraint needs a colour past them.
+struct Colouring {
+    std::vector<uint32_t> order, starts;
+    uint32_t colours() const { return starts.empty() ? 0u : uint32_t(starts.size() - 1); }
+};
+template <class F> Colouring colourGreedy(uint32_t n, uint32_t constraints, uint32_t perConstraint, F &&elementOf)
+{
+    Colouring out;
+    if (constraints == 0) return out;
+    uint32_t words = 1;
+    std::vector<uint64_t> used(size_t(n) * words, 0ull);
+    std::vector<uint32_t> colourOf(constraints, 0u);
+    std::vector<uint32_t> el(perConstraint);
+    uint32_t colours = 0;
+    for (uint32_t c = 0; c < constraints; ++c) {
+        uint32_t m = 0;
+        for (uint32_t k = 0; k < perConstraint; ++k) {
+            const uint32_t e = elementOf(c, k);
+            if (e < n) el[m++] = e;
+        }
+        uint32_t colour = words * 64u;
+        for (uint32_t w = 0; w < words && colour == words * 64u; ++w) {
+            uint64_t taken = 0;
+            for (uint32_t k = 0; k < m; ++k) taken |= used[size_t(el[k]) * words + w];
+            if (~taken) colour = w * 64u + uint32_t(__builtin_ctzll(~taken));
+        }
+        if (colour >= words * 64u) { // every colour of the current words is taken: widen
+            std::vector<uint64_t> wider(size_t(n) * (words + 1), 0ull);
+            for (size_t e = 0; e < n; ++e)
+                for (uint32_t w = 0; w < words; ++w) wider[e * (words + 1) + w] = used[e * words + w];
+            used.swap(wider);
+            ++words;
+        }
+        for (uint32_t k = 0; k < m; ++k) used[size_t(el[k]) * words + colour / 64u] |= 1ull << (colour % 64u);
+        colourOf[c] = colour;
+        colours = std::max(colours, colour + 1u);
+    }
+    out.starts.assign(colours + 1u, 0u);
+    for (uint32_t c = 0; c < constraints; ++c) ++out.starts[colourOf[c] + 1u];
+    for (uint32_t k = 0; k < colours; ++k) out.starts[k + 1u] += out.starts[k];
+    out.order.resize(constraints);
+    std::vector<uint32_t> fill(out.starts.begin(), out.starts.end() - 1);
+    for (uint32_t c = 0; c < constraints; ++c) out.order[fill[colourOf[c]]++] = c;
     return out;
 }
 

@@ -15,6 +15,7 @@
 // --fmad=false so float32 results match a CPU evaluation of the same order.
 #include <algorithm>
 #include <cstdint>
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "cn_device.h"
@@ -1429,10 +1430,8 @@ __global__ void __launch_bounds__(kThreads) k_solveTets(Scene s, float dt, float
 }
 
 // physics_soft_solve_bend_constraints.cs.hlsl:20-86
-__global__ void __launch_bounds__(kThreads) k_solveBends(Scene s, float dt, float relax)
+__device__ __forceinline__ void solveBendAt(const Scene &s, float dt, float relax, uint32_t b)
 {
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= s.Bn) return;
     const cn_soft_bend bd = s.bends[b];
     float4 *out = s.bendCorr + 4 * size_t(b);
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1466,11 +1465,15 @@ __global__ void __launch_bounds__(kThreads) k_solveBends(Scene s, float dt, floa
     out[0] = o0; out[1] = o1; out[2] = o2; out[3] = z;
 }
 
-// physics_cloth_solve_dihedral_constraints.cs.hlsl:20-95
-__global__ void __launch_bounds__(kThreads) k_solveDihedrals(Scene s, float dt, float relax)
+__global__ void __launch_bounds__(kThreads) k_solveBends(Scene s, float dt, float relax)
 {
-    const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
-    if (d >= s.D) return;
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < s.Bn) solveBendAt(s, dt, relax, b);
+}
+
+// physics_cloth_solve_dihedral_constraints.cs.hlsl:20-95
+__device__ __forceinline__ void solveDihedralAt(const Scene &s, float dt, float relax, uint32_t d)
+{
     const uint32_t ci = s.Bn + d;
     const cn_cloth_dihedral h = s.dihedrals[d];
     float4 *out = s.bendCorr + 4 * size_t(ci);
@@ -1515,6 +1518,12 @@ __global__ void __launch_bounds__(kThreads) k_solveDihedrals(Scene s, float dt, 
     out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
 }
 
+__global__ void __launch_bounds__(kThreads) k_solveDihedrals(Scene s, float dt, float relax)
+{
+    const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if (d < s.D) solveDihedralAt(s, dt, relax, d);
+}
+
 // 3x3 helpers of physics_strand_solve_{segment,joint}_constraints.cs.hlsl:12-64
 struct m3 { float m[3][3]; };
 __device__ __forceinline__ void addOuter(m3 &acc, float sc, f3 a, f3 b)
@@ -1549,10 +1558,8 @@ __device__ __forceinline__ float strandOrientationInvMass(float wA, float wB, fl
 }
 
 // physics_strand_solve_segment_constraints.cs.hlsl:66-147
-__global__ void __launch_bounds__(kThreads) k_solveSegments(Scene s, float dt, float relax)
+__device__ __forceinline__ void solveSegmentAt(const Scene &s, float dt, float relax, uint32_t g)
 {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= s.S) return;
     const cn_strand_segment sg = s.segs[g];
     const float4 a = s.x[sg.particle_a], b = s.x[sg.particle_b];
     const float wA = a.w, wB = b.w, wSum = wA + wB;
@@ -1592,10 +1599,15 @@ __global__ void __launch_bounds__(kThreads) k_solveSegments(Scene s, float dt, f
     out[0] = o0; out[1] = o1; out[2] = o2;
 }
 
-// physics_strand_apply_segment_corrections.cs.hlsl:11-43
-__global__ void __launch_bounds__(kThreads) k_applySegments(Scene s)
+__global__ void __launch_bounds__(kThreads) k_solveSegments(Scene s, float dt, float relax)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < s.S) solveSegmentAt(s, dt, relax, g);
+}
+
+// physics_strand_apply_segment_corrections.cs.hlsl:11-43
+__device__ __forceinline__ void applySegmentsAt(const Scene &s, uint32_t i)
+{
     if (i < s.N) {
         const float4 p = s.x[i];
         if (p.w > kEps) {
@@ -1611,11 +1623,14 @@ __global__ void __launch_bounds__(kThreads) k_applySegments(Scene s)
     if (i < s.S) s.segOrient[i] = qNormalize(add4(s.segOrient[i], s.segCorr[3 * size_t(i) + 2]));
 }
 
-// physics_strand_solve_joint_constraints.cs.hlsl:66-154
-__global__ void __launch_bounds__(kThreads) k_solveJoints(Scene s, float dt, float relax)
+__global__ void __launch_bounds__(kThreads) k_applySegments(Scene s)
 {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= s.J) return;
+    applySegmentsAt(s, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// physics_strand_solve_joint_constraints.cs.hlsl:66-154
+__device__ __forceinline__ void solveJointAt(const Scene &s, float dt, float relax, uint32_t j)
+{
     const cn_strand_joint jt = s.joints[j];
     const cn_strand_segment sA = s.segs[jt.segment_a], sB = s.segs[jt.segment_b];
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -1657,11 +1672,15 @@ __global__ void __launch_bounds__(kThreads) k_solveJoints(Scene s, float dt, flo
     s.jointCorr[2 * size_t(j) + 1] = tB;
 }
 
-// physics_strand_apply_joint_corrections.cs.hlsl
-__global__ void __launch_bounds__(kThreads) k_applyJoints(Scene s)
+__global__ void __launch_bounds__(kThreads) k_solveJoints(Scene s, float dt, float relax)
 {
-    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= s.S) return;
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < s.J) solveJointAt(s, dt, relax, j);
+}
+
+// physics_strand_apply_joint_corrections.cs.hlsl
+__device__ __forceinline__ void applyJointsAt(const Scene &s, uint32_t g)
+{
     const uint2 r = s.segJointRanges[g];
     float4 total = make_float4(0.f, 0.f, 0.f, 0.f);
     for (uint32_t k = 0; k < r.y; ++k) {
@@ -1671,11 +1690,15 @@ __global__ void __launch_bounds__(kThreads) k_applyJoints(Scene s)
     s.segOrient[g] = qNormalize(add4(s.segOrient[g], total));
 }
 
-// physics_strand_solve_distance_constraints.cs.hlsl:10-59
-__global__ void __launch_bounds__(kThreads) k_solveDistances(Scene s, float dt, float relax)
+__global__ void __launch_bounds__(kThreads) k_applyJoints(Scene s)
 {
-    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= s.SD) return;
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < s.S) applyJointsAt(s, g);
+}
+
+// physics_strand_solve_distance_constraints.cs.hlsl:10-59
+__device__ __forceinline__ void solveDistanceAt(const Scene &s, float dt, float relax, uint32_t c)
+{
     const cn_strand_distance dc = s.dists[c];
     float4 cA = make_float4(0.f, 0.f, 0.f, 0.f), cB = cA;
     const float4 a = s.x[dc.particle_a], b = s.x[dc.particle_b];
@@ -1698,6 +1721,12 @@ __global__ void __launch_bounds__(kThreads) k_solveDistances(Scene s, float dt, 
     }
     s.distCorr[2 * c] = cA;
     s.distCorr[2 * c + 1] = cB;
+}
+
+__global__ void __launch_bounds__(kThreads) k_solveDistances(Scene s, float dt, float relax)
+{
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < s.SD) solveDistanceAt(s, dt, relax, c);
 }
 
 __device__ __forceinline__ void atomicAdd3(float4 *p, f3 v)
@@ -2708,10 +2737,360 @@ void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)
     k_fluidNeighborsDensity<0u, false><<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u, nullptr);
 }
 
+// ------------------------------------------------------------------------------------------
+// Graph-coloured XPBD schedules
+// ------------------------------------------------------------------------------------------
+// A colour's constraints share no particle (no segment, for joints).  Each constraint is solved
+// by the gather schedule's own per-constraint function, which writes its correction records and
+// lambda; the same thread then moves its records into the particles (Gauss-Seidel: applied
+// before the next colour is solved) or into the per-particle sum (colour Jacobi: every
+// correction of the family from the positions at the family's start, summed in colour order).
+__device__ __forceinline__ void moveRecord(const Scene &s, bool gaussSeidel, uint32_t p, float4 r)
+{
+    if (p >= s.N) return;
+    if (gaussSeidel) {
+        const float4 q = s.x[p];
+        if (q.w > kEps) s.x[p] = mk4(xyz(q) + xyz(r), q.w);
+    } else {
+        const float4 a = s.softAcc[p];
+        s.softAcc[p] = mk4(xyz(a) + xyz(r), 0.0f);
+    }
+}
+
+__device__ __forceinline__ void moveOrientation(const Scene &s, bool gaussSeidel, uint32_t g, float4 r)
+{
+    if (g >= s.S) return;
+    if (gaussSeidel) s.segOrient[g] = qNormalize(add4(s.segOrient[g], r));
+    else s.orientAcc[g] = add4(s.orientAcc[g], r);
+}
+
+template <uint32_t kFam>
+__device__ __forceinline__ void colourConstraint(const Scene &s, float dt, float relax, bool gaussSeidel, uint32_t c)
+{
+    if constexpr (kFam == kFamEdges) {
+        solveEdge(s, dt, relax, c);
+        const cn_soft_edge ed = s.edges[c];
+        moveRecord(s, gaussSeidel, ed.particle_a, s.edgeCorr[2 * size_t(c)]);
+        moveRecord(s, gaussSeidel, ed.particle_b, s.edgeCorr[2 * size_t(c) + 1]);
+    } else if constexpr (kFam == kFamSegments) {
+        // a segment's orientation is read by its own constraint alone: applied in place
+        solveSegmentAt(s, dt, relax, c);
+        const cn_strand_segment sg = s.segs[c];
+        moveRecord(s, gaussSeidel, sg.particle_a, s.segCorr[3 * size_t(c)]);
+        moveRecord(s, gaussSeidel, sg.particle_b, s.segCorr[3 * size_t(c) + 1]);
+        s.segOrient[c] = qNormalize(add4(s.segOrient[c], s.segCorr[3 * size_t(c) + 2]));
+    } else if constexpr (kFam == kFamBends) {
+        const float4 *r = s.bendCorr + 4 * size_t(c);
+        if (c < s.Bn) {
+            solveBendAt(s, dt, relax, c);
+            const cn_soft_bend b = s.bends[c];
+            moveRecord(s, gaussSeidel, b.particle0, r[0]);
+            moveRecord(s, gaussSeidel, b.particle1, r[1]);
+            moveRecord(s, gaussSeidel, b.particle2, r[2]);
+        } else {
+            solveDihedralAt(s, dt, relax, c - s.Bn);
+            const cn_cloth_dihedral h = s.dihedrals[c - s.Bn];
+            moveRecord(s, gaussSeidel, h.edge_particle0, r[0]);
+            moveRecord(s, gaussSeidel, h.edge_particle1, r[1]);
+            moveRecord(s, gaussSeidel, h.opposite_particle0, r[2]);
+            moveRecord(s, gaussSeidel, h.opposite_particle1, r[3]);
+        }
+    } else if constexpr (kFam == kFamJoints) {
+        solveJointAt(s, dt, relax, c);
+        const cn_strand_joint jt = s.joints[c];
+        moveOrientation(s, gaussSeidel, jt.segment_a, s.jointCorr[2 * size_t(c)]);
+        moveOrientation(s, gaussSeidel, jt.segment_b, s.jointCorr[2 * size_t(c) + 1]);
+    } else if constexpr (kFam == kFamDistances) {
+        solveDistanceAt(s, dt, relax, c);
+        const cn_strand_distance dc = s.dists[c];
+        moveRecord(s, gaussSeidel, dc.particle_a, s.distCorr[2 * size_t(c)]);
+        moveRecord(s, gaussSeidel, dc.particle_b, s.distCorr[2 * size_t(c) + 1]);
+    } else {
+        solveTet(s, dt, relax, c);
+        const cn_soft_tet t = s.tets[c];
+        const float4 *r = s.tetCorr + 4 * size_t(c);
+        moveRecord(s, gaussSeidel, t.particle_indices[0], r[0]);
+        moveRecord(s, gaussSeidel, t.particle_indices[1], r[1]);
+        moveRecord(s, gaussSeidel, t.particle_indices[2], r[2]);
+        moveRecord(s, gaussSeidel, t.particle_indices[3], r[3]);
+    }
+}
+
+// End of a colour-Jacobi family: x += the family's sum (particles with invMass > kEps), sum
+// cleared; for joints the orientation sum, then the normalisation every segment gets.
+__device__ __forceinline__ void colourJacobiApplyAt(const Scene &s, uint32_t i)
+{
+    const float4 a = s.softAcc[i];
+    s.softAcc[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 p = s.x[i];
+    if (p.w > kEps) s.x[i] = mk4(xyz(p) + xyz(a), p.w);
+}
+
+__device__ __forceinline__ void colourJacobiOrientAt(const Scene &s, uint32_t g)
+{
+    const float4 a = s.orientAcc[g];
+    s.orientAcc[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+    s.segOrient[g] = qNormalize(add4(s.segOrient[g], a));
+}
+
+template <uint32_t kFam, bool kGaussSeidel>
+__global__ void __launch_bounds__(kThreads) k_colourSolve(Scene s, float dt, float relax, uint32_t begin, uint32_t end)
+{
+    const uint32_t k = begin + blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < end) colourConstraint<kFam>(s, dt, relax, kGaussSeidel, s.colOrder[kFam][k]);
+}
+
+__global__ void __launch_bounds__(kThreads) k_colourJacobiApply(Scene s, uint2 win)
+{
+    const uint32_t i = win.x + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < win.y) colourJacobiApplyAt(s, i);
+}
+
+__global__ void __launch_bounds__(kThreads) k_colourJacobiOrient(Scene s)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < s.S) colourJacobiOrientAt(s, g);
+}
+
+__host__ __device__ __forceinline__ uint32_t familySize(const Scene &s, uint32_t fam)
+{
+    return fam == kFamEdges ? s.E
+         : fam == kFamSegments ? s.S
+         : fam == kFamBends ? s.Bn + s.D
+         : fam == kFamJoints ? s.J
+         : fam == kFamDistances ? s.SD
+         : s.T;
+}
+
+// The particles a family's colour-Jacobi sum can touch (strand distances share the strand
+// segments' particles).
+__host__ __device__ __forceinline__ uint2 familyWindow(const Scene &s, uint32_t fam)
+{
+    return fam == kFamEdges ? s.edgeWin
+         : fam == kFamBends ? s.bendWin
+         : fam == kFamTets ? s.tetWin
+         : s.segWin;
+}
+
+template <uint32_t kFam>
+void launchColourFamily(const Scene &s, float dt, float relax, const XpbdPlan &plan, cudaStream_t st)
+{
+    if (familySize(s, kFam) == 0) return;
+    const bool gs = plan.schedule == CN_XPBD_COLOUR_GAUSS_SEIDEL;
+    const uint32_t *starts = plan.hostStarts[kFam];
+    for (uint32_t k = 0; k < plan.colours[kFam]; ++k) {
+        const uint32_t b = starts[k], e = starts[k + 1];
+        if (e <= b) continue;
+        if (gs) k_colourSolve<kFam, true><<<blocksFor(e - b), kThreads, 0, st>>>(s, dt, relax, b, e);
+        else k_colourSolve<kFam, false><<<blocksFor(e - b), kThreads, 0, st>>>(s, dt, relax, b, e);
+    }
+    if (gs) return;
+    if (kFam == kFamJoints) {
+        k_colourJacobiOrient<<<blocksFor(s.S), kThreads, 0, st>>>(s);
+    } else {
+        const uint2 win = familyWindow(s, kFam);
+        if (win.y > win.x) k_colourJacobiApply<<<blocksFor(win.y - win.x), kThreads, 0, st>>>(s, win);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Fused iterations: one thread-block cluster, every iteration of the substep
+// ------------------------------------------------------------------------------------------
+// The phases of the per-phase kernels (family solve, family apply, particle-rigid contacts), each
+// a loop of the cluster's threads over its elements, separated by cluster barriers: the
+// barrier's release / acquire at cluster scope orders every global write of a phase before
+// every read of the next.  Each element is computed by the same device function as in the
+// per-phase kernels, so the results are the same bit for bit.  Every thread passes every barrier
+// (the loops' trip counts are uniform), and nothing waits on anything but the barriers.
+constexpr uint32_t kFusedThreads = 512u;
+constexpr uint32_t kFusedMaxCtas = 16u;
+
+struct FusedPlan {
+    uint32_t iterations, softIterations, contactIterations, rigid;
+    uint32_t colours[kFamilies];
+    const uint32_t *starts[kFamilies];
+};
+
+template <uint32_t kFam, uint32_t kSchedule>
+__device__ __forceinline__ void fusedFamily(const Scene &s, float dt, float relax, const FusedPlan &plan,
+                                            uint32_t tid, uint32_t nth)
+{
+    namespace cg = cooperative_groups;
+    const uint32_t n = familySize(s, kFam);
+    if (n == 0u) return;
+    if constexpr (kSchedule == CN_XPBD_GATHER) {
+        for (uint32_t c = tid; c < n; c += nth) {
+            if constexpr (kFam == kFamEdges) solveEdge(s, dt, relax, c);
+            else if constexpr (kFam == kFamSegments) solveSegmentAt(s, dt, relax, c);
+            else if constexpr (kFam == kFamBends) {
+                if (c < s.Bn) solveBendAt(s, dt, relax, c);
+                else solveDihedralAt(s, dt, relax, c - s.Bn);
+            } else if constexpr (kFam == kFamJoints) solveJointAt(s, dt, relax, c);
+            else if constexpr (kFam == kFamDistances) solveDistanceAt(s, dt, relax, c);
+            else solveTet(s, dt, relax, c);
+        }
+        cg::this_cluster().sync();
+        if constexpr (kFam == kFamEdges) {
+            for (uint32_t i = s.edgeWin.x + tid; i < s.edgeWin.y; i += nth)
+                applyPairAt(s, s.edgeRanges, s.edgeInc, s.edgeCorr, i);
+        } else if constexpr (kFam == kFamSegments) {
+            const uint32_t m = s.N > s.S ? s.N : s.S;
+            for (uint32_t i = tid; i < m; i += nth) applySegmentsAt(s, i);
+        } else if constexpr (kFam == kFamBends) {
+            for (uint32_t i = s.bendWin.x + tid; i < s.bendWin.y; i += nth)
+                applyQuadAt(s, s.bendRanges, s.bendInc, s.bendCorr, i);
+        } else if constexpr (kFam == kFamJoints) {
+            for (uint32_t g = tid; g < s.S; g += nth) applyJointsAt(s, g);
+        } else if constexpr (kFam == kFamDistances) {
+            for (uint32_t i = s.segWin.x + tid; i < s.segWin.y; i += nth)
+                applyPairAt(s, s.segRanges, s.segInc, s.distCorr, i);
+        } else {
+            for (uint32_t i = s.tetWin.x + tid; i < s.tetWin.y; i += nth)
+                applyQuadAt(s, s.tetRanges, s.tetInc, s.tetCorr, i);
+        }
+        cg::this_cluster().sync();
+    } else {
+        constexpr bool gs = kSchedule == CN_XPBD_COLOUR_GAUSS_SEIDEL;
+        const uint32_t *order = s.colOrder[kFam];
+        const uint32_t *starts = plan.starts[kFam];
+        for (uint32_t k = 0; k < plan.colours[kFam]; ++k) {
+            const uint32_t b = starts[k], e = starts[k + 1];
+            for (uint32_t j = b + tid; j < e; j += nth) colourConstraint<kFam>(s, dt, relax, gs, order[j]);
+            cg::this_cluster().sync();
+        }
+        if constexpr (!gs) {
+            if constexpr (kFam == kFamJoints) {
+                for (uint32_t g = tid; g < s.S; g += nth) colourJacobiOrientAt(s, g);
+            } else {
+                const uint2 win = familyWindow(s, kFam);
+                for (uint32_t i = win.x + tid; i < win.y; i += nth) colourJacobiApplyAt(s, i);
+            }
+            cg::this_cluster().sync();
+        }
+    }
+}
+
+template <uint32_t kSchedule>
+__global__ void __launch_bounds__(kFusedThreads, 1) k_fusedIterations(Scene s, Config cfg, float dt, FusedPlan plan)
+{
+    namespace cg = cooperative_groups;
+    const cg::cluster_group cl = cg::this_cluster();
+    const uint32_t tid = cl.block_rank() * blockDim.x + threadIdx.x;
+    const uint32_t nth = cl.num_blocks() * blockDim.x;
+    const float relax = cfg.softInternalRelaxation;
+    for (uint32_t it = 0; it < plan.iterations; ++it) {
+        if (it < plan.softIterations) {
+            fusedFamily<kFamEdges, kSchedule>(s, dt, relax, plan, tid, nth);
+            fusedFamily<kFamSegments, kSchedule>(s, dt, relax, plan, tid, nth);
+            fusedFamily<kFamBends, kSchedule>(s, dt, relax, plan, tid, nth);
+            fusedFamily<kFamJoints, kSchedule>(s, dt, relax, plan, tid, nth);
+            fusedFamily<kFamDistances, kSchedule>(s, dt, relax, plan, tid, nth);
+            fusedFamily<kFamTets, kSchedule>(s, dt, relax, plan, tid, nth);
+        }
+        if (plan.rigid != 0u && it < plan.contactIterations) {
+            for (uint32_t i = tid; i < s.N; i += nth) rigidContactsAt(s, cfg, true, i);
+            cl.sync();
+        }
+    }
+}
+
+template <uint32_t kSchedule> cudaError_t fusedLaunch(const Scene &s, const Config &c, float dt, const FusedPlan &plan,
+                                                     const FusedShape &shape, cudaStream_t st)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(shape.ctas, 1, 1);
+    cfg.blockDim = dim3(shape.threads, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = shape.ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_fusedIterations<kSchedule>, s, c, dt, plan);
+}
+
 // Grid of an apply pass: the batch's work list, else the family's particle window.
 inline unsigned applyGrid(const Scene &s, uint2 win)
 {
     return s.wP.tiles ? gridFor(s.wP, s.N) : blocksFor(win.y > win.x ? win.y - win.x : 0u);
+}
+
+void launchSoftIteration(const Scene &s, float dt, const Config &c, const XpbdPlan &plan, cudaStream_t st)
+{
+    if (plan.schedule == CN_XPBD_GATHER) {
+        launchSoftIteration(s, dt, c, st);
+        return;
+    }
+    const float relax = c.softInternalRelaxation;
+    launchColourFamily<kFamEdges>(s, dt, relax, plan, st);
+    launchColourFamily<kFamSegments>(s, dt, relax, plan, st);
+    launchColourFamily<kFamBends>(s, dt, relax, plan, st);
+    launchColourFamily<kFamJoints>(s, dt, relax, plan, st);
+    launchColourFamily<kFamDistances>(s, dt, relax, plan, st);
+    launchColourFamily<kFamTets>(s, dt, relax, plan, st);
+}
+
+FusedShape fusedIterationsShape()
+{
+    // one CTA per SM, as many SMs as one cluster may span (16 where the device allows the
+    // non-portable size, else the portable 8)
+    FusedShape out;
+    const void *fns[3] = {reinterpret_cast<const void *>(&k_fusedIterations<CN_XPBD_GATHER>),
+                          reinterpret_cast<const void *>(&k_fusedIterations<CN_XPBD_COLOUR_JACOBI>),
+                          reinterpret_cast<const void *>(&k_fusedIterations<CN_XPBD_COLOUR_GAUSS_SEIDEL>)};
+    for (const void *f : fns)
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            cudaGetLastError();
+            return out;
+        }
+    for (uint32_t ctas : {kFusedMaxCtas, 8u}) {
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(ctas, 1, 1);
+        cfg.blockDim = dim3(kFusedThreads, 1, 1);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = ctas;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        bool ok = true;
+        for (const void *f : fns) {
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, f, &cfg) != cudaSuccess || clusters < 1) {
+                cudaGetLastError();
+                ok = false;
+                break;
+            }
+        }
+        if (ok) {
+            out.ctas = ctas;
+            out.threads = kFusedThreads;
+            return out;
+        }
+    }
+    return out;
+}
+
+void launchFusedIterations(const Scene &s, const Config &c, float dt, const XpbdPlan &plan, uint32_t iterations,
+                           uint32_t softIterations, uint32_t contactIterations, bool rigid, const FusedShape &shape,
+                           cudaStream_t st)
+{
+    FusedPlan fp{};
+    fp.iterations = iterations;
+    fp.softIterations = softIterations;
+    fp.contactIterations = contactIterations;
+    fp.rigid = rigid ? 1u : 0u;
+    for (uint32_t f = 0; f < kFamilies; ++f) {
+        fp.colours[f] = plan.schedule == CN_XPBD_GATHER ? 0u : plan.colours[f];
+        fp.starts[f] = plan.devStarts[f];
+    }
+    if (plan.schedule == CN_XPBD_COLOUR_JACOBI) fusedLaunch<CN_XPBD_COLOUR_JACOBI>(s, c, dt, fp, shape, st);
+    else if (plan.schedule == CN_XPBD_COLOUR_GAUSS_SEIDEL) fusedLaunch<CN_XPBD_COLOUR_GAUSS_SEIDEL>(s, c, dt, fp, shape, st);
+    else fusedLaunch<CN_XPBD_GATHER>(s, c, dt, fp, shape, st);
 }
 
 void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st)

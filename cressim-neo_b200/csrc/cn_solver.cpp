@@ -68,6 +68,13 @@ struct cn_solver {
     std::vector<Probe> probes;
     uint32_t graphKernelNodes = 0, graphNodes = 0;
     uint32_t contactMaterialCapacity = 0, fluidMaterialCapacity = 0, surfIdxCapacity = 0;
+    // XPBD schedule: per-family colourings (coloured schedules), the plan the launches read, and
+    // whether each substep's iterations run in one cluster kernel
+    cn::Colouring colouring[cn::kFamilies];
+    cn::XpbdPlan plan{};
+    bool fused = false;
+    cn::FusedShape fusedShape{};
+    bool fusedShapeQueried = false;
 };
 
 namespace {
@@ -172,6 +179,14 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
     s.distCorr = a.take<float4>(size_t(s.SD) * 2);
     s.posCorr = a.take<float4>(N);
     s.velCorr = a.take<float4>(N);
+    for (uint32_t f = 0; f < cn::kFamilies; ++f) {
+        const cn::Colouring &col = sv->colouring[f];
+        s.colOrder[f] = col.colours() ? a.take<uint32_t>(col.order.size()) : nullptr;
+        sv->plan.devStarts[f] = col.colours() ? a.take<uint32_t>(col.starts.size()) : nullptr;
+    }
+    const bool coloured = sv->plan.schedule != CN_XPBD_GATHER;
+    s.softAcc = coloured ? a.take<float4>(N) : nullptr;
+    s.orientAcc = coloured ? a.take<float4>(w.strand_segment_count) : nullptr;
     s.B = w.rigid_body_count;
     s.C = w.collider_count;
     const uint32_t B = std::max<uint32_t>(s.B, 1u), C = std::max<uint32_t>(s.C, 1u);
@@ -434,7 +449,17 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             cudaMemsetAsync(s.velCorr, 0, sizeof(float4) * N, st);
         }
         const bool hasSoftInternal = N > 0 && (s.E || s.Bn || s.D || s.T || s.S || s.J || s.SD);
-        for (uint32_t it = 0; it < sv->maxIt; ++it) {
+        if (sv->fused) {
+            // every iteration of the substep in one cluster kernel (soft families, then the
+            // particle-rigid contacts of the iteration)
+            const uint32_t softIt = hasSoftInternal ? sv->softIt : 0u;
+            const uint32_t contactIt = sv->rigidPossible ? sv->contactIt : 0u;
+            probe(sv, "fused_iterations", st, [&] {
+                cn::launchFusedIterations(s, c, dt, sv->plan, std::max(softIt, contactIt), softIt, contactIt,
+                                          sv->rigidPossible, sv->fusedShape, st);
+            });
+        }
+        for (uint32_t it = 0; it < (sv->fused ? 0u : sv->maxIt); ++it) {
             const bool runFluid = sv->hasFluid && it < sv->fluidIt;
             const bool runSoft = hasSoftInternal && it < sv->softIt;
             const bool runPP = sv->ppPossible && it < sv->contactIt;
@@ -450,7 +475,7 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
                 probe(sv, "fluid_delta_apply_clamp", st,
                       [&] { cn::launchFluidDeltaApplyClamp(s, it, dt, c, sv->writeFluidDebug, st); });
             }
-            if (runSoft) probe(sv, "soft_constraints", st, [&] { cn::launchSoftIteration(s, dt, c, st); });
+            if (runSoft) probe(sv, "soft_constraints", st, [&] { cn::launchSoftIteration(s, dt, c, sv->plan, st); });
             if (runPP || runRigid) probe(sv, "contacts", st, [&] { cn::launchContacts(s, c, runPP, runRigid, st); });
             // finalRigidContactDepenetration (physics_solver.cpp:1111-1117)
             if (runRigidRigid) probe(sv, "rigid_depenetration", st, [&] { cn::launchRigidDepenetration(s, c, st); });
@@ -725,6 +750,59 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
         return k == 0 ? j.segment_a : j.segment_b;
     });
 
+    // XPBD schedule: the coloured schedules colour every family (elements: particles; segments
+    // for the joints, whose corrections move orientations)
+    const uint32_t schedule = d.soft.xpbd_schedule;
+    if (schedule > CN_XPBD_COLOUR_GAUSS_SEIDEL)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_sync_world: unknown soft.xpbd_schedule");
+    if (d.soft.fused_iterations > CN_FUSED_ON)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_sync_world: unknown soft.fused_iterations");
+    sv->plan = cn::XpbdPlan{};
+    sv->plan.schedule = schedule;
+    for (cn::Colouring &col : sv->colouring) col = cn::Colouring{};
+    if (schedule != CN_XPBD_GATHER) {
+        // the gather applies strand distance records through the strand-segment incidence; the
+        // colour schedules apply them to the distance's own particles, the same ones when each
+        // distance constraint spans its segment (as cn_world authors strands)
+        if (w->strand_distance_count &&
+            (w->strand_distance_count != w->strand_segment_count ||
+             !std::equal(w->strand_distances, w->strand_distances + w->strand_distance_count, w->strand_segments,
+                         [](const cn_strand_distance &dc, const cn_strand_segment &sg) {
+                             return dc.particle_a == sg.particle_a && dc.particle_b == sg.particle_b;
+                         })))
+            return setError(CN_ERR_UNSUPPORTED,
+                            "coloured XPBD schedules need each strand distance constraint on its segment's particles");
+        sv->colouring[cn::kFamEdges] = cn::colourGreedy(N, w->edge_count, 2, [&](uint32_t c, uint32_t k) {
+            return k == 0 ? w->edges[c].particle_a : w->edges[c].particle_b;
+        });
+        sv->colouring[cn::kFamSegments] = cn::colourGreedy(N, S, 2, [&](uint32_t c, uint32_t k) {
+            return k == 0 ? w->strand_segments[c].particle_a : w->strand_segments[c].particle_b;
+        });
+        sv->colouring[cn::kFamBends] = cn::colourGreedy(N, nb + w->dihedral_count, 4, [&](uint32_t c, uint32_t k) -> uint32_t {
+            if (c < nb) {
+                if (k == 3) return 0xffffffffu;
+                const cn_soft_bend &b = w->bends[c];
+                return k == 0 ? b.particle0 : (k == 1 ? b.particle1 : b.particle2);
+            }
+            const cn_cloth_dihedral &h = w->dihedrals[c - nb];
+            const uint32_t p[4] = {h.edge_particle0, h.edge_particle1, h.opposite_particle0, h.opposite_particle1};
+            return p[k];
+        });
+        sv->colouring[cn::kFamJoints] = cn::colourGreedy(S, w->strand_joint_count, 2, [&](uint32_t c, uint32_t k) {
+            return k == 0 ? w->strand_joints[c].segment_a : w->strand_joints[c].segment_b;
+        });
+        sv->colouring[cn::kFamDistances] = cn::colourGreedy(N, w->strand_distance_count, 2, [&](uint32_t c, uint32_t k) {
+            return k == 0 ? w->strand_distances[c].particle_a : w->strand_distances[c].particle_b;
+        });
+        sv->colouring[cn::kFamTets] = cn::colourGreedy(N, w->tet_count, 4, [&](uint32_t c, uint32_t k) {
+            return w->tets[c].particle_indices[k];
+        });
+        for (uint32_t f = 0; f < cn::kFamilies; ++f) {
+            sv->plan.colours[f] = sv->colouring[f].colours();
+            sv->plan.hostStarts[f] = sv->colouring[f].starts.empty() ? nullptr : sv->colouring[f].starts.data();
+        }
+    }
+
     cn::Arena a;
     a.reset(nullptr);
     layout(sv, a, *w, edgeI, bendI, tetI, segI, jointI);
@@ -809,6 +887,12 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     CN_CUDA(up(s.segInc, segI.inc.data(), segI.inc.size(), st));
     CN_CUDA(up(s.segJointRanges, jointI.ranges.data(), jointI.ranges.size(), st));
     CN_CUDA(up(s.segJointInc, jointI.inc.data(), jointI.inc.size(), st));
+    for (uint32_t f = 0; f < cn::kFamilies; ++f) {
+        const cn::Colouring &col = sv->colouring[f];
+        if (!col.colours()) continue;
+        CN_CUDA(up(const_cast<uint32_t *>(s.colOrder[f]), col.order.data(), col.order.size(), st));
+        CN_CUDA(up(const_cast<uint32_t *>(sv->plan.devStarts[f]), col.starts.data(), col.starts.size(), st));
+    }
     CN_CUDA(up(s.bodyPos, w->body_positions_inv_mass, s.B, st));
     CN_CUDA(up(s.bodyRot, w->body_orientations, s.B, st));
     CN_CUDA(up(s.bodyLin, w->body_linear_velocities, s.B, st));
@@ -836,6 +920,21 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     CN_CUDA(cudaStreamSynchronize(st));
 
     sv->cfg = cn::configFromDesc(d);
+    // Fused iterations: soft bodies against static and kinematic colliders only, each phase at
+    // most kFusedRounds passes of the cluster's threads over its elements
+    sv->fused = false;
+    if (d.soft.fused_iterations == CN_FUSED_ON && N > 0 && !sv->hasFluid && !sv->ppPossible && !sv->hasDynamic &&
+        !sv->rigidRigid && nProxy == 0 && (s.E || s.Bn || s.D || s.T || s.S || s.J || s.SD)) {
+        if (!sv->fusedShapeQueried) {
+            sv->fusedShape = cn::fusedIterationsShape();
+            sv->fusedShapeQueried = true;
+        }
+        constexpr uint32_t kFusedRounds = 4u;
+        const uint64_t cap = uint64_t(sv->fusedShape.ctas) * sv->fusedShape.threads * kFusedRounds;
+        const uint64_t most = std::max({uint64_t(N), uint64_t(s.E), uint64_t(s.Bn) + s.D, uint64_t(s.T), uint64_t(s.S),
+                                        uint64_t(s.J), uint64_t(s.SD)});
+        sv->fused = cap > 0 && most <= cap;
+    }
     sv->hostX = w->positions_inv_mass;
     sv->hostV = w->velocities;
     sv->contactMaterialCapacity = w->contact_material_count;
@@ -1234,6 +1333,38 @@ CN_API cn_status cn_solver_graph_stats(cn_solver *sv, uint32_t *kernel_nodes, ui
     if (!sv) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_graph_stats: null solver");
     if (kernel_nodes) *kernel_nodes = sv->graphKernelNodes;
     if (nodes) *nodes = sv->graphNodes;
+    return CN_OK;
+}
+
+CN_API cn_status cn_solver_schedule_info(cn_solver *sv, cn_schedule_info *out)
+{
+    if (!sv || !out) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_schedule_info: null argument");
+    if (!sv->synced) return setError(CN_ERR_NOT_INITIALIZED, "cn_solver_schedule_info: no world synced");
+    std::memset(out, 0, sizeof(*out));
+    out->xpbd_schedule = sv->plan.schedule;
+    out->fused_iterations = sv->fused ? 1u : 0u;
+    out->cluster_ctas = sv->fused ? sv->fusedShape.ctas : 0u;
+    out->threads_per_cta = sv->fused ? sv->fusedShape.threads : 0u;
+    for (uint32_t f = 0; f < cn::kFamilies; ++f) out->colours[f] = sv->plan.colours[f];
+    return CN_OK;
+}
+
+CN_API cn_status cn_colour_constraints(const uint32_t *elements, uint32_t constraint_count, uint32_t per_constraint,
+                                       uint32_t element_count, uint32_t *order, uint32_t *colour_starts,
+                                       uint32_t colour_capacity, uint32_t *colours)
+{
+    if (!colours || (constraint_count && (!elements || !order || !colour_starts || per_constraint == 0)))
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_colour_constraints: null argument");
+    const cn::Colouring col = cn::colourGreedy(element_count, constraint_count, per_constraint, [&](uint32_t c, uint32_t k) {
+        return elements[size_t(c) * per_constraint + k];
+    });
+    *colours = col.colours();
+    if (constraint_count) std::copy(col.order.begin(), col.order.end(), order);
+    const size_t keep = std::min<size_t>(col.starts.size(), size_t(colour_capacity) + 1u);
+    if (colour_starts) std::copy(col.starts.begin(), col.starts.begin() + keep, colour_starts);
+    if (col.colours() > colour_capacity)
+        return setError(CN_ERR_CAPACITY, "cn_colour_constraints: more colours than colour_capacity");
+    cn::clearError();
     return CN_OK;
 }
 

@@ -87,9 +87,32 @@ typedef struct cn_joint_settings {
     float min_xpbd_dt;
 } cn_joint_settings;
 
+/* XPBD projection schedule of the soft families (edges, strand segments, bends and dihedrals,
+ * strand joints, strand distances, tets; the family order of physics_solver.cpp:915-1019).
+ *   CN_XPBD_GATHER: the reference's Jacobi solve -- every constraint of a family writes its
+ *     correction records from the positions at the family's start, then each particle gathers
+ *     its records in ascending constraint order.  The default; bit-exact with the reference.
+ *   CN_XPBD_COLOUR_JACOBI: the same Jacobi update without the gather: each family is split by a
+ *     greedy graph colouring (no two constraints of a colour share a particle or, for joints, a
+ *     segment) and each colour adds its corrections straight into a per-particle sum, so the
+ *     sum runs in colour order instead of constraint order (agrees with GATHER to rounding).
+ *   CN_XPBD_COLOUR_GAUSS_SEIDEL: opt-in; each colour's corrections are applied before the next
+ *     colour is solved (not the reference's update: stable at internal_relaxation 1, where the
+ *     Jacobi gather diverges, and closer to the converged state after the same iterations). */
+enum { CN_XPBD_GATHER = 0, CN_XPBD_COLOUR_JACOBI = 1, CN_XPBD_COLOUR_GAUSS_SEIDEL = 2 };
+/* Fused iterations (opt-in): scenes of soft bodies against static or kinematic colliders (no
+ * fluid, no particle-particle contacts, no dynamic bodies) small enough for one thread-block
+ * cluster run all iterations of a substep in one cluster kernel, its phases separated by cluster
+ * barriers (the same arithmetic, in the same order, as the per-phase kernels: bit-identical).
+ * Off by default: on B200 the per-phase kernels over all SMs are faster even for a 4,096-particle
+ * cube, whose dependent record -> position loads one 16-SM cluster cannot hide. */
+enum { CN_FUSED_OFF = 0, CN_FUSED_ON = 1 };
+
 typedef struct cn_soft_settings {
     float internal_relaxation; /* 0.2 */
-    float reserved[7];
+    uint32_t xpbd_schedule;    /* CN_XPBD_GATHER */
+    uint32_t fused_iterations; /* CN_FUSED_OFF */
+    float reserved[5];
 } cn_soft_settings;
 
 typedef struct cn_fluid_settings {
@@ -621,6 +644,28 @@ CN_API cn_status cn_solver_kernel_times(cn_solver *solver, cn_kernel_time *out, 
                                         uint32_t *count);
 /* Nodes of the captured frame graph: kernel launches and all nodes (launch count per frame). */
 CN_API cn_status cn_solver_graph_stats(cn_solver *solver, uint32_t *kernel_nodes, uint32_t *nodes);
+
+/* The XPBD schedule a synced solver runs (soft settings xpbd_schedule / fused_iterations). */
+typedef struct cn_schedule_info {
+    uint32_t xpbd_schedule;     /* CN_XPBD_* */
+    uint32_t fused_iterations;  /* 1: each substep's iterations run in one cluster kernel */
+    uint32_t cluster_ctas;      /* CTAs of that cluster (0 when not fused) */
+    uint32_t threads_per_cta;
+    uint32_t colours[6];        /* colours per family: edges, strand segments, bends + dihedrals,
+                                 * strand joints, strand distances, tets (0 under CN_XPBD_GATHER) */
+} cn_schedule_info;
+CN_API cn_status cn_solver_schedule_info(cn_solver *solver, cn_schedule_info *out);
+
+/* Greedy graph colouring of one constraint family (host only, no device needed).  Constraint c,
+ * taken in ascending order, receives the lowest colour that no earlier constraint sharing one of
+ * its elements has.  elements[c * per_constraint + k] are constraint c's particles (segments for
+ * strand joints); entries >= element_count are ignored.  Writes order[constraint_count] (the
+ * constraints grouped by colour, ascending within a colour) and colour_starts[colours + 1];
+ * *colours receives the colour count.  CN_ERR_CAPACITY when more than colour_capacity colours
+ * are needed (colour_starts then holds colour_capacity + 1 entries at most). */
+CN_API cn_status cn_colour_constraints(const uint32_t *elements, uint32_t constraint_count, uint32_t per_constraint,
+                                       uint32_t element_count, uint32_t *order, uint32_t *colour_starts,
+                                       uint32_t colour_capacity, uint32_t *colours);
 
 /* Intermediate buffers of the last substep, for parity checks.  Each is converted to the
  * reference's layout and indexing (particle order, not cell order). */

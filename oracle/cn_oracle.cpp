@@ -392,6 +392,11 @@ struct cno_solver {
     std::vector<f4> segCorr;       // 3 per segment
     std::vector<f4> jointCorr;     // 5 per joint
     std::vector<f4> distCorr;      // 2 per distance
+    // coloured XPBD schedules (desc.soft.xpbd_schedule != 0): per family (edges, strand
+    // segments, bends + dihedrals, strand joints, strand distances, tets) the constraints grouped
+    // by colour, the colour boundaries, and the colour-Jacobi sums
+    std::vector<uint32_t> colOrder[6], colStarts[6];
+    std::vector<f4> softAcc, orientAcc;
     uint32_t truncations = 0;
     bool postUpdateNeighbors = true; // physics_solver.cpp:1262-1268
     // surface render data (SurfaceDeformableRenderDataHost) and outputs
@@ -1289,36 +1294,37 @@ void fluidApplyAndClamp(cno_solver &s, uint32_t iter)
 
 // ---- XPBD families (Jacobi: solve writes per-constraint records, apply gathers) ----
 // physics_soft_solve_edge_constraints.cs.hlsl:10-74
+void solveEdgeOne(cno_solver &s, float dt, float relax, uint32_t e)
+{
+    const cn_soft_edge &ed = s.edges[e];
+    f4 &cA = s.edgeCorr[2 * e], &cB = s.edgeCorr[2 * e + 1];
+    cA = f4{0, 0, 0, 0}; cB = f4{0, 0, 0, 0};
+    if (ed.enabled == 0u) return;
+    const f4 a = s.x[ed.particle_a], b = s.x[ed.particle_b];
+    const float wA = a.w, wB = b.w, wSum = wA + wB;
+    if (wSum <= kEps) return;
+    const f3 delta = xyz(b) - xyz(a);
+    const float l2 = dot(delta, delta);
+    if (l2 <= kEps) return;
+    const float len = std::sqrt(l2);
+    const f3 gA = -delta / len;
+    const f3 gB = -gA;
+    const float compliance = std::max(ed.compliance, 0.0f);
+    const float alpha = compliance / std::max(dt * dt, kEps);
+    const float Cv = len - ed.rest_length;
+    const float lambda = s.edgeLambda[e];
+    const float den = wSum + alpha;
+    if (den <= kEps) return;
+    const float dl = -(Cv + alpha * lambda) / den;
+    s.edgeLambda[e] = lambda + dl;
+    cA = mk4(wA * dl * gA * relax, 0.0f);
+    cB = mk4(wB * dl * gB * relax, 0.0f);
+}
 void solveEdges(cno_solver &s, float dt)
 {
     const float relax = s.desc.soft.internal_relaxation;
 #pragma omp parallel for schedule(static)
-    for (int64_t ee = 0; ee < int64_t(s.edges.size()); ++ee) {
-        const uint32_t e = uint32_t(ee);
-        const cn_soft_edge &ed = s.edges[e];
-        f4 &cA = s.edgeCorr[2 * e], &cB = s.edgeCorr[2 * e + 1];
-        cA = f4{0, 0, 0, 0}; cB = f4{0, 0, 0, 0};
-        if (ed.enabled == 0u) continue;
-        const f4 a = s.x[ed.particle_a], b = s.x[ed.particle_b];
-        const float wA = a.w, wB = b.w, wSum = wA + wB;
-        if (wSum <= kEps) continue;
-        const f3 delta = xyz(b) - xyz(a);
-        const float l2 = dot(delta, delta);
-        if (l2 <= kEps) continue;
-        const float len = std::sqrt(l2);
-        const f3 gA = -delta / len;
-        const f3 gB = -gA;
-        const float compliance = std::max(ed.compliance, 0.0f);
-        const float alpha = compliance / std::max(dt * dt, kEps);
-        const float Cv = len - ed.rest_length;
-        const float lambda = s.edgeLambda[e];
-        const float den = wSum + alpha;
-        if (den <= kEps) continue;
-        const float dl = -(Cv + alpha * lambda) / den;
-        s.edgeLambda[e] = lambda + dl;
-        cA = mk4(wA * dl * gA * relax, 0.0f);
-        cB = mk4(wB * dl * gB * relax, 0.0f);
-    }
+    for (int64_t ee = 0; ee < int64_t(s.edges.size()); ++ee) solveEdgeOne(s, dt, relax, uint32_t(ee));
 }
 // physics_soft_apply_edge_corrections.cs.hlsl:9-35 (and the strand distance apply, which
 // indexes its correction records through the strand-segment incidence table,
@@ -1360,124 +1366,127 @@ void applyQuadCorrections(cno_solver &s, const std::vector<Range> &ranges,
     }
 }
 // physics_soft_solve_tet_constraints.cs.hlsl:15-87
+void solveTetOne(cno_solver &s, float dt, float relax, uint32_t t)
+{
+    const cn_soft_tet &tet = s.tets[t];
+    const f4 q0 = s.x[tet.particle_indices[0]], q1 = s.x[tet.particle_indices[1]];
+    const f4 q2 = s.x[tet.particle_indices[2]], q3 = s.x[tet.particle_indices[3]];
+    const float w0 = q0.w, w1 = q1.w, w2 = q2.w, w3 = q3.w;
+    if ((w0 + w1 + w2 + w3) <= kEps) return; // keeps the previous correction record
+    const f3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2), p3 = xyz(q3);
+    const float sv = dot(cross(p1 - p0, p2 - p0), p3 - p0) / 6.0f;
+    const float vs = (sv >= 0.0f) ? 1.0f : -1.0f;
+    const float vol = std::fabs(sv);
+    const float rv = std::max(tet.rest_volume, 0.0f);
+    const float Cv = vol - rv;
+    const f3 g0 = cross(p3 - p1, p2 - p1) * (vs / 6.0f);
+    const f3 g1 = cross(p2 - p0, p3 - p0) * (vs / 6.0f);
+    const f3 g2 = cross(p3 - p0, p1 - p0) * (vs / 6.0f);
+    const f3 g3 = cross(p1 - p0, p2 - p0) * (vs / 6.0f);
+    const float sg = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
+    const float compliance = std::max(tet.compliance, 0.0f);
+    const float alpha = compliance / std::max(dt * dt, kEps);
+    const float lambda = s.tetLambda[t];
+    const float den = sg + alpha;
+    if (den <= kEps) return;
+    const float dl = -(Cv + alpha * lambda) / den;
+    s.tetLambda[t] = lambda + dl;
+    s.tetCorr[4 * t + 0] = mk4(w0 * dl * g0 * relax, 0.0f);
+    s.tetCorr[4 * t + 1] = mk4(w1 * dl * g1 * relax, 0.0f);
+    s.tetCorr[4 * t + 2] = mk4(w2 * dl * g2 * relax, 0.0f);
+    s.tetCorr[4 * t + 3] = mk4(w3 * dl * g3 * relax, 0.0f);
+}
 void solveTets(cno_solver &s, float dt)
 {
     const float relax = s.desc.soft.internal_relaxation;
 #pragma omp parallel for schedule(static)
-    for (int64_t tt = 0; tt < int64_t(s.tets.size()); ++tt) {
-        const uint32_t t = uint32_t(tt);
-        const cn_soft_tet &tet = s.tets[t];
-        const f4 q0 = s.x[tet.particle_indices[0]], q1 = s.x[tet.particle_indices[1]];
-        const f4 q2 = s.x[tet.particle_indices[2]], q3 = s.x[tet.particle_indices[3]];
-        const float w0 = q0.w, w1 = q1.w, w2 = q2.w, w3 = q3.w;
-        if ((w0 + w1 + w2 + w3) <= kEps) continue; // keeps the previous correction record
-        const f3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2), p3 = xyz(q3);
-        const float sv = dot(cross(p1 - p0, p2 - p0), p3 - p0) / 6.0f;
-        const float vs = (sv >= 0.0f) ? 1.0f : -1.0f;
-        const float vol = std::fabs(sv);
-        const float rv = std::max(tet.rest_volume, 0.0f);
-        const float Cv = vol - rv;
-        const f3 g0 = cross(p3 - p1, p2 - p1) * (vs / 6.0f);
-        const f3 g1 = cross(p2 - p0, p3 - p0) * (vs / 6.0f);
-        const f3 g2 = cross(p3 - p0, p1 - p0) * (vs / 6.0f);
-        const f3 g3 = cross(p1 - p0, p2 - p0) * (vs / 6.0f);
-        const float sg = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
-        const float compliance = std::max(tet.compliance, 0.0f);
-        const float alpha = compliance / std::max(dt * dt, kEps);
-        const float lambda = s.tetLambda[t];
-        const float den = sg + alpha;
-        if (den <= kEps) continue;
-        const float dl = -(Cv + alpha * lambda) / den;
-        s.tetLambda[t] = lambda + dl;
-        s.tetCorr[4 * t + 0] = mk4(w0 * dl * g0 * relax, 0.0f);
-        s.tetCorr[4 * t + 1] = mk4(w1 * dl * g1 * relax, 0.0f);
-        s.tetCorr[4 * t + 2] = mk4(w2 * dl * g2 * relax, 0.0f);
-        s.tetCorr[4 * t + 3] = mk4(w3 * dl * g3 * relax, 0.0f);
-    }
+    for (int64_t tt = 0; tt < int64_t(s.tets.size()); ++tt) solveTetOne(s, dt, relax, uint32_t(tt));
 }
 // physics_soft_solve_bend_constraints.cs.hlsl:20-86
+void solveBendOne(cno_solver &s, float dt, float relax, uint32_t b)
+{
+    const cn_soft_bend &bd = s.bends[b];
+    f4 *out = &s.bendCorr[4 * b];
+    out[0] = out[1] = out[2] = out[3] = f4{0, 0, 0, 0};
+    const f4 q0 = s.x[bd.particle0], q1 = s.x[bd.particle1], q2 = s.x[bd.particle2];
+    const float w0 = q0.w, w1 = q1.w, w2 = q2.w;
+    if (w0 + w1 + w2 <= kEps) return;
+    const f3 e0 = xyz(q0) - xyz(q1), e1 = xyz(q2) - xyz(q1);
+    const float l0s = dot(e0, e0), l1s = dot(e1, e1);
+    if (l0s <= kEps || l1s <= kEps) return;
+    const float l0 = std::sqrt(l0s), l1 = std::sqrt(l1s);
+    const f3 d0 = e0 / l0, d1 = e1 / l1;
+    const float ct = std::min(std::max(dot(d0, d1), -1.0f + 1.0e-4f), 1.0f - 1.0e-4f);
+    const float st2 = std::max(1.0f - ct * ct, 1.0e-8f);
+    const float st = std::sqrt(st2);
+    const float theta = std::acos(ct);
+    const f3 g0 = -(d1 - ct * d0) / std::max(l0 * st, kEps);
+    const f3 g2 = -(d0 - ct * d1) / std::max(l1 * st, kEps);
+    const f3 g1 = -(g0 + g2);
+    const float den = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2);
+    const float alpha = std::max(bd.compliance, 0.0f) / std::max(dt * dt, kEps);
+    if (den + alpha <= kEps) return;
+    const float Cv = theta - bd.rest_angle;
+    const float lambda = s.bendLambda[b];
+    const float dl = -(Cv + alpha * lambda) / (den + alpha);
+    s.bendLambda[b] = lambda + dl;
+    out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
+    out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
+    out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
+}
 void solveBends(cno_solver &s, float dt)
 {
     const float relax = s.desc.soft.internal_relaxation;
 #pragma omp parallel for schedule(static)
-    for (int64_t bb = 0; bb < int64_t(s.bends.size()); ++bb) {
-        const uint32_t b = uint32_t(bb);
-        const cn_soft_bend &bd = s.bends[b];
-        f4 *out = &s.bendCorr[4 * b];
-        out[0] = out[1] = out[2] = out[3] = f4{0, 0, 0, 0};
-        const f4 q0 = s.x[bd.particle0], q1 = s.x[bd.particle1], q2 = s.x[bd.particle2];
-        const float w0 = q0.w, w1 = q1.w, w2 = q2.w;
-        if (w0 + w1 + w2 <= kEps) continue;
-        const f3 e0 = xyz(q0) - xyz(q1), e1 = xyz(q2) - xyz(q1);
-        const float l0s = dot(e0, e0), l1s = dot(e1, e1);
-        if (l0s <= kEps || l1s <= kEps) continue;
-        const float l0 = std::sqrt(l0s), l1 = std::sqrt(l1s);
-        const f3 d0 = e0 / l0, d1 = e1 / l1;
-        const float ct = std::min(std::max(dot(d0, d1), -1.0f + 1.0e-4f), 1.0f - 1.0e-4f);
-        const float st2 = std::max(1.0f - ct * ct, 1.0e-8f);
-        const float st = std::sqrt(st2);
-        const float theta = std::acos(ct);
-        const f3 g0 = -(d1 - ct * d0) / std::max(l0 * st, kEps);
-        const f3 g2 = -(d0 - ct * d1) / std::max(l1 * st, kEps);
-        const f3 g1 = -(g0 + g2);
-        const float den = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2);
-        const float alpha = std::max(bd.compliance, 0.0f) / std::max(dt * dt, kEps);
-        if (den + alpha <= kEps) continue;
-        const float Cv = theta - bd.rest_angle;
-        const float lambda = s.bendLambda[b];
-        const float dl = -(Cv + alpha * lambda) / (den + alpha);
-        s.bendLambda[b] = lambda + dl;
-        out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
-        out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
-        out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
-    }
+    for (int64_t bb = 0; bb < int64_t(s.bends.size()); ++bb) solveBendOne(s, dt, relax, uint32_t(bb));
 }
 // physics_cloth_solve_dihedral_constraints.cs.hlsl:20-95
+void solveDihedralOne(cno_solver &s, float dt, float relax, uint32_t d)
+{
+    const uint32_t off = uint32_t(s.bends.size());
+    const uint32_t ci = off + d;
+    const cn_cloth_dihedral &h = s.dihedrals[d];
+    f4 *out = &s.bendCorr[4 * ci];
+    out[0] = out[1] = out[2] = out[3] = f4{0, 0, 0, 0};
+    const f4 e0m = s.x[h.edge_particle0], e1m = s.x[h.edge_particle1];
+    const f4 o0m = s.x[h.opposite_particle0], o1m = s.x[h.opposite_particle1];
+    const f3 p0 = xyz(o0m), p1 = xyz(o1m), p2 = xyz(e0m), p3 = xyz(e1m);
+    const f3 edge = p3 - p2;
+    const float el2 = dot(edge, edge);
+    const f3 rn0 = cross(p2 - p0, p3 - p0);
+    const f3 rn1 = cross(p3 - p1, p2 - p1);
+    const float n0s = dot(rn0, rn0), n1s = dot(rn1, rn1);
+    if (el2 <= kEps || n0s <= kEps || n1s <= kEps) return;
+    const float el = std::sqrt(el2);
+    const float iel = 1.0f / el;
+    const f3 sn0 = rn0 / n0s, sn1 = rn1 / n1s;
+    const f3 dO0 = el * sn0, dO1 = el * sn1;
+    const f3 dE0 = dot(p0 - p3, edge) * iel * sn0 + dot(p1 - p3, edge) * iel * sn1;
+    const f3 dE1 = dot(p2 - p0, edge) * iel * sn0 + dot(p2 - p1, edge) * iel * sn1;
+    const f3 g0 = -dE0, g1 = -dE1, g2 = -dO0, g3 = -dO1;
+    const f3 n0 = rn0 / std::sqrt(n0s), n1 = rn1 / std::sqrt(n1s);
+    const float theta = std::atan2(dot(edge * iel, cross(n0, n1)),
+                                   std::min(std::max(dot(n0, n1), -1.0f), 1.0f));
+    const float twoPi = 6.283185307179586f;
+    float Cv = theta - h.rest_angle;
+    Cv = Cv - twoPi * std::floor((Cv + 3.141592653589793f) / twoPi);
+    const float w0 = e0m.w, w1 = e1m.w, w2 = o0m.w, w3 = o1m.w;
+    const float den = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
+    const float alpha = std::max(h.compliance, 0.0f) / std::max(dt * dt, kEps);
+    if (den + alpha <= kEps) return;
+    const float lambda = s.bendLambda[ci];
+    const float dl = -(Cv + alpha * lambda) / (den + alpha);
+    s.bendLambda[ci] = lambda + dl;
+    out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
+    out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
+    out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
+    out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
+}
 void solveDihedrals(cno_solver &s, float dt)
 {
     const float relax = s.desc.soft.internal_relaxation;
-    const uint32_t off = uint32_t(s.bends.size());
 #pragma omp parallel for schedule(static)
-    for (int64_t dd = 0; dd < int64_t(s.dihedrals.size()); ++dd) {
-        const uint32_t d = uint32_t(dd);
-        const uint32_t ci = off + d;
-        const cn_cloth_dihedral &h = s.dihedrals[d];
-        f4 *out = &s.bendCorr[4 * ci];
-        out[0] = out[1] = out[2] = out[3] = f4{0, 0, 0, 0};
-        const f4 e0m = s.x[h.edge_particle0], e1m = s.x[h.edge_particle1];
-        const f4 o0m = s.x[h.opposite_particle0], o1m = s.x[h.opposite_particle1];
-        const f3 p0 = xyz(o0m), p1 = xyz(o1m), p2 = xyz(e0m), p3 = xyz(e1m);
-        const f3 edge = p3 - p2;
-        const float el2 = dot(edge, edge);
-        const f3 rn0 = cross(p2 - p0, p3 - p0);
-        const f3 rn1 = cross(p3 - p1, p2 - p1);
-        const float n0s = dot(rn0, rn0), n1s = dot(rn1, rn1);
-        if (el2 <= kEps || n0s <= kEps || n1s <= kEps) continue;
-        const float el = std::sqrt(el2);
-        const float iel = 1.0f / el;
-        const f3 sn0 = rn0 / n0s, sn1 = rn1 / n1s;
-        const f3 dO0 = el * sn0, dO1 = el * sn1;
-        const f3 dE0 = dot(p0 - p3, edge) * iel * sn0 + dot(p1 - p3, edge) * iel * sn1;
-        const f3 dE1 = dot(p2 - p0, edge) * iel * sn0 + dot(p2 - p1, edge) * iel * sn1;
-        const f3 g0 = -dE0, g1 = -dE1, g2 = -dO0, g3 = -dO1;
-        const f3 n0 = rn0 / std::sqrt(n0s), n1 = rn1 / std::sqrt(n1s);
-        const float theta = std::atan2(dot(edge * iel, cross(n0, n1)),
-                                       std::min(std::max(dot(n0, n1), -1.0f), 1.0f));
-        const float twoPi = 6.283185307179586f;
-        float Cv = theta - h.rest_angle;
-        Cv = Cv - twoPi * std::floor((Cv + 3.141592653589793f) / twoPi);
-        const float w0 = e0m.w, w1 = e1m.w, w2 = o0m.w, w3 = o1m.w;
-        const float den = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
-        const float alpha = std::max(h.compliance, 0.0f) / std::max(dt * dt, kEps);
-        if (den + alpha <= kEps) continue;
-        const float lambda = s.bendLambda[ci];
-        const float dl = -(Cv + alpha * lambda) / (den + alpha);
-        s.bendLambda[ci] = lambda + dl;
-        out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
-        out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
-        out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
-        out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
-    }
+    for (int64_t dd = 0; dd < int64_t(s.dihedrals.size()); ++dd) solveDihedralOne(s, dt, relax, uint32_t(dd));
 }
 
 // 3x3 helpers of physics_strand_solve_{segment,joint}_constraints.cs.hlsl:12-64
@@ -1519,49 +1528,50 @@ inline float StrandOrientationInvMass(float wA, float wB, float rl)
     return 12.0f * avg / std::max(rl * rl, kEps);
 }
 // physics_strand_solve_segment_constraints.cs.hlsl:66-147
+void solveSegmentOne(cno_solver &s, float dt, float relax, uint32_t g)
+{
+    const cn_strand_segment &sg = s.segs[g];
+    const f4 a = s.x[sg.particle_a], b = s.x[sg.particle_b];
+    const float wA = a.w, wB = b.w, wSum = wA + wB;
+    f4 *out = &s.segCorr[3 * g];
+    out[0] = out[1] = out[2] = f4{0, 0, 0, 0};
+    if (wSum <= kEps) return;
+    const f3 delta = xyz(b) - xyz(a);
+    if (dot(delta, delta) <= kEps) return;
+    const f4 q = QNormalize(s.segOrient[g]);
+    const f3 axis = QRotate(q, f3{1, 0, 0});
+    const float irl = 1.0f / std::max(sg.rest_length, kEps);
+    const float oim = StrandOrientationInvMass(wA, wB, sg.rest_length);
+    const f3 Cv = delta * irl - axis;
+    const float alpha = std::max(sg.stretch_shear_compliance, 0.0f) / std::max(dt * dt, kEps);
+    const f3 lambda = xyz(s.segLambda[g]);
+    const f3 qv = xyz(q);
+    const float qw = q.w;
+    const f3 gQw = 2.0f * f3{qw, qv.z, -qv.y};
+    const f3 gQx = 2.0f * f3{0.0f, qv.y, qv.z};
+    const f3 gQy = 2.0f * f3{-qv.y, 0.0f, -qw};
+    const f3 gQz = 2.0f * f3{-qv.z, qw, 0.0f};
+    const float dg = wSum * irl * irl + alpha;
+    m3 sys{{{dg, 0, 0}, {0, dg, 0}, {0, 0, dg}}};
+    addScaled(sys, oim, outer(gQx, gQx));
+    addScaled(sys, oim, outer(gQy, gQy));
+    addScaled(sys, oim, outer(gQz, gQz));
+    addScaled(sys, oim, outer(gQw, gQw));
+    const f3 rhs = -(Cv + alpha * lambda);
+    const f3 dl = mul3(inverse3(sys), rhs);
+    if (dot(dl, dl) > 0.0f) {
+        s.segLambda[g] = mk4(lambda + dl, 0.0f);
+        out[0] = mk4(-wA * irl * dl * relax, 0.0f);
+        out[1] = mk4(wB * irl * dl * relax, 0.0f);
+        const f4 qg{-dot(gQx, dl), -dot(gQy, dl), -dot(gQz, dl), -dot(gQw, dl)};
+        out[2] = qg * (oim * relax);
+    }
+}
 void solveSegments(cno_solver &s, float dt)
 {
     const float relax = s.desc.soft.internal_relaxation;
 #pragma omp parallel for schedule(static)
-    for (int64_t gg = 0; gg < int64_t(s.segs.size()); ++gg) {
-        const uint32_t g = uint32_t(gg);
-        const cn_strand_segment &sg = s.segs[g];
-        const f4 a = s.x[sg.particle_a], b = s.x[sg.particle_b];
-        const float wA = a.w, wB = b.w, wSum = wA + wB;
-        f4 *out = &s.segCorr[3 * g];
-        out[0] = out[1] = out[2] = f4{0, 0, 0, 0};
-        if (wSum <= kEps) continue;
-        const f3 delta = xyz(b) - xyz(a);
-        if (dot(delta, delta) <= kEps) continue;
-        const f4 q = QNormalize(s.segOrient[g]);
-        const f3 axis = QRotate(q, f3{1, 0, 0});
-        const float irl = 1.0f / std::max(sg.rest_length, kEps);
-        const float oim = StrandOrientationInvMass(wA, wB, sg.rest_length);
-        const f3 Cv = delta * irl - axis;
-        const float alpha = std::max(sg.stretch_shear_compliance, 0.0f) / std::max(dt * dt, kEps);
-        const f3 lambda = xyz(s.segLambda[g]);
-        const f3 qv = xyz(q);
-        const float qw = q.w;
-        const f3 gQw = 2.0f * f3{qw, qv.z, -qv.y};
-        const f3 gQx = 2.0f * f3{0.0f, qv.y, qv.z};
-        const f3 gQy = 2.0f * f3{-qv.y, 0.0f, -qw};
-        const f3 gQz = 2.0f * f3{-qv.z, qw, 0.0f};
-        const float dg = wSum * irl * irl + alpha;
-        m3 sys{{{dg, 0, 0}, {0, dg, 0}, {0, 0, dg}}};
-        addScaled(sys, oim, outer(gQx, gQx));
-        addScaled(sys, oim, outer(gQy, gQy));
-        addScaled(sys, oim, outer(gQz, gQz));
-        addScaled(sys, oim, outer(gQw, gQw));
-        const f3 rhs = -(Cv + alpha * lambda);
-        const f3 dl = mul3(inverse3(sys), rhs);
-        if (dot(dl, dl) > 0.0f) {
-            s.segLambda[g] = mk4(lambda + dl, 0.0f);
-            out[0] = mk4(-wA * irl * dl * relax, 0.0f);
-            out[1] = mk4(wB * irl * dl * relax, 0.0f);
-            const f4 qg{-dot(gQx, dl), -dot(gQy, dl), -dot(gQz, dl), -dot(gQw, dl)};
-            out[2] = qg * (oim * relax);
-        }
-    }
+    for (int64_t gg = 0; gg < int64_t(s.segs.size()); ++gg) solveSegmentOne(s, dt, relax, uint32_t(gg));
 }
 // physics_strand_apply_segment_corrections.cs.hlsl:11-43
 void applySegments(cno_solver &s)
@@ -1586,52 +1596,53 @@ void applySegments(cno_solver &s)
     }
 }
 // physics_strand_solve_joint_constraints.cs.hlsl:66-154
+void solveJointOne(cno_solver &s, float dt, float relax, uint32_t j)
+{
+    const cn_strand_joint &jt = s.joints[j];
+    const cn_strand_segment &sA = s.segs[jt.segment_a], &sB = s.segs[jt.segment_b];
+    f4 *out = &s.jointCorr[5 * j];
+    for (int k = 0; k < 5; ++k) out[k] = f4{0, 0, 0, 0};
+    const f4 oA = QNormalize(s.segOrient[jt.segment_a]);
+    const f4 oB = QNormalize(s.segOrient[jt.segment_b]);
+    const float wA0 = s.x[sA.particle_a].w, wA1 = s.x[sA.particle_b].w;
+    const float wB0 = s.x[sB.particle_a].w, wB1 = s.x[sB.particle_b].w;
+    const float imA = StrandOrientationInvMass(wA0, wA1, sA.rest_length);
+    const float imB = StrandOrientationInvMass(wB0, wB1, sB.rest_length);
+    const f4 rel = QNormalize(QMul(QConj(oA), oB));
+    f4 rr = QNormalize(f4{jt.rest_relative_orientation[0], jt.rest_relative_orientation[1],
+                          jt.rest_relative_orientation[2], jt.rest_relative_orientation[3]});
+    if (dot4(rel, rr) < 0.0f) rr = f4{-rr.x, -rr.y, -rr.z, -rr.w};
+    const f3 Cv = xyz(rel) - xyz(rr);
+    const f4 lambda = s.jointLambda[j];
+    const float ba = std::max(jt.bend_compliance, 0.0f) / std::max(dt * dt, kEps);
+    const float ta = std::max(jt.twist_compliance, 0.0f) / std::max(dt * dt, kEps);
+    const f3 av{ta, ba, ba};
+    m3 sys{{{av.x, 0, 0}, {0, av.y, 0}, {0, 0, av.z}}};
+    const f3 va = xyz(oA), vb = xyz(oB);
+    const float wa = oA.w, wb = oB.w;
+    const f3 gAX{-wb, vb.z, -vb.y}, gAY{-vb.z, -wb, vb.x}, gAZ{vb.y, -vb.x, -wb}, gAW = vb;
+    const f3 gBX{wa, -va.z, va.y}, gBY{va.z, wa, -va.x}, gBZ{-va.y, va.x, wa}, gBW = -va;
+    addScaled(sys, imA, outer(gAX, gAX));
+    addScaled(sys, imA, outer(gAY, gAY));
+    addScaled(sys, imA, outer(gAZ, gAZ));
+    addScaled(sys, imA, outer(gAW, gAW));
+    addScaled(sys, imB, outer(gBX, gBX));
+    addScaled(sys, imB, outer(gBY, gBY));
+    addScaled(sys, imB, outer(gBZ, gBZ));
+    addScaled(sys, imB, outer(gBW, gBW));
+    const f3 rhs = -(Cv + av * xyz(lambda));
+    const f3 dl = mul3(inverse3(sys), rhs);
+    if (dot(dl, dl) > 0.0f) {
+        s.jointLambda[j] = mk4(xyz(lambda) + dl, 0.0f);
+        out[3] = f4{dot(gAX, dl), dot(gAY, dl), dot(gAZ, dl), dot(gAW, dl)} * (imA * relax);
+        out[4] = f4{dot(gBX, dl), dot(gBY, dl), dot(gBZ, dl), dot(gBW, dl)} * (imB * relax);
+    }
+}
 void solveJoints(cno_solver &s, float dt)
 {
     const float relax = s.desc.soft.internal_relaxation;
 #pragma omp parallel for schedule(static)
-    for (int64_t jj = 0; jj < int64_t(s.joints.size()); ++jj) {
-        const uint32_t j = uint32_t(jj);
-        const cn_strand_joint &jt = s.joints[j];
-        const cn_strand_segment &sA = s.segs[jt.segment_a], &sB = s.segs[jt.segment_b];
-        f4 *out = &s.jointCorr[5 * j];
-        for (int k = 0; k < 5; ++k) out[k] = f4{0, 0, 0, 0};
-        const f4 oA = QNormalize(s.segOrient[jt.segment_a]);
-        const f4 oB = QNormalize(s.segOrient[jt.segment_b]);
-        const float wA0 = s.x[sA.particle_a].w, wA1 = s.x[sA.particle_b].w;
-        const float wB0 = s.x[sB.particle_a].w, wB1 = s.x[sB.particle_b].w;
-        const float imA = StrandOrientationInvMass(wA0, wA1, sA.rest_length);
-        const float imB = StrandOrientationInvMass(wB0, wB1, sB.rest_length);
-        const f4 rel = QNormalize(QMul(QConj(oA), oB));
-        f4 rr = QNormalize(f4{jt.rest_relative_orientation[0], jt.rest_relative_orientation[1],
-                              jt.rest_relative_orientation[2], jt.rest_relative_orientation[3]});
-        if (dot4(rel, rr) < 0.0f) rr = f4{-rr.x, -rr.y, -rr.z, -rr.w};
-        const f3 Cv = xyz(rel) - xyz(rr);
-        const f4 lambda = s.jointLambda[j];
-        const float ba = std::max(jt.bend_compliance, 0.0f) / std::max(dt * dt, kEps);
-        const float ta = std::max(jt.twist_compliance, 0.0f) / std::max(dt * dt, kEps);
-        const f3 av{ta, ba, ba};
-        m3 sys{{{av.x, 0, 0}, {0, av.y, 0}, {0, 0, av.z}}};
-        const f3 va = xyz(oA), vb = xyz(oB);
-        const float wa = oA.w, wb = oB.w;
-        const f3 gAX{-wb, vb.z, -vb.y}, gAY{-vb.z, -wb, vb.x}, gAZ{vb.y, -vb.x, -wb}, gAW = vb;
-        const f3 gBX{wa, -va.z, va.y}, gBY{va.z, wa, -va.x}, gBZ{-va.y, va.x, wa}, gBW = -va;
-        addScaled(sys, imA, outer(gAX, gAX));
-        addScaled(sys, imA, outer(gAY, gAY));
-        addScaled(sys, imA, outer(gAZ, gAZ));
-        addScaled(sys, imA, outer(gAW, gAW));
-        addScaled(sys, imB, outer(gBX, gBX));
-        addScaled(sys, imB, outer(gBY, gBY));
-        addScaled(sys, imB, outer(gBZ, gBZ));
-        addScaled(sys, imB, outer(gBW, gBW));
-        const f3 rhs = -(Cv + av * xyz(lambda));
-        const f3 dl = mul3(inverse3(sys), rhs);
-        if (dot(dl, dl) > 0.0f) {
-            s.jointLambda[j] = mk4(xyz(lambda) + dl, 0.0f);
-            out[3] = f4{dot(gAX, dl), dot(gAY, dl), dot(gAZ, dl), dot(gAW, dl)} * (imA * relax);
-            out[4] = f4{dot(gBX, dl), dot(gBY, dl), dot(gBZ, dl), dot(gBW, dl)} * (imB * relax);
-        }
-    }
+    for (int64_t jj = 0; jj < int64_t(s.joints.size()); ++jj) solveJointOne(s, dt, relax, uint32_t(jj));
 }
 // physics_strand_apply_joint_corrections.cs.hlsl
 void applyJoints(cno_solver &s)
@@ -1649,32 +1660,217 @@ void applyJoints(cno_solver &s)
     }
 }
 // physics_strand_solve_distance_constraints.cs.hlsl:10-59
+void solveDistanceOne(cno_solver &s, float dt, float relax, uint32_t c)
+{
+    const cn_strand_distance &dc = s.dists[c];
+    f4 &cA = s.distCorr[2 * c], &cB = s.distCorr[2 * c + 1];
+    cA = cB = f4{0, 0, 0, 0};
+    const f4 a = s.x[dc.particle_a], b = s.x[dc.particle_b];
+    const float wA = a.w, wB = b.w, wSum = wA + wB;
+    if (wSum <= kEps) return;
+    const f3 delta = xyz(b) - xyz(a);
+    const float l2 = dot(delta, delta);
+    if (l2 <= kEps) return;
+    const float len = std::sqrt(l2);
+    const f3 grad = delta / len;
+    const float alpha = std::max(dc.distance_compliance, 0.0f) / std::max(dt * dt, kEps);
+    const float lambda = s.distLambda[c];
+    const float Cv = len - dc.rest_length;
+    const float den = wSum + alpha;
+    if (den > kEps) {
+        const float dl = -(Cv + alpha * lambda) / den;
+        s.distLambda[c] = lambda + dl;
+        cA = mk4(wA * dl * -grad * relax, 0.0f);
+        cB = mk4(wB * dl * grad * relax, 0.0f);
+    }
+}
 void solveDistances(cno_solver &s, float dt)
 {
     const float relax = s.desc.soft.internal_relaxation;
 #pragma omp parallel for schedule(static)
-    for (int64_t cc = 0; cc < int64_t(s.dists.size()); ++cc) {
-        const uint32_t c = uint32_t(cc);
-        const cn_strand_distance &dc = s.dists[c];
-        f4 &cA = s.distCorr[2 * c], &cB = s.distCorr[2 * c + 1];
-        cA = cB = f4{0, 0, 0, 0};
-        const f4 a = s.x[dc.particle_a], b = s.x[dc.particle_b];
-        const float wA = a.w, wB = b.w, wSum = wA + wB;
-        if (wSum <= kEps) continue;
-        const f3 delta = xyz(b) - xyz(a);
-        const float l2 = dot(delta, delta);
-        if (l2 <= kEps) continue;
-        const float len = std::sqrt(l2);
-        const f3 grad = delta / len;
-        const float alpha = std::max(dc.distance_compliance, 0.0f) / std::max(dt * dt, kEps);
-        const float lambda = s.distLambda[c];
-        const float Cv = len - dc.rest_length;
-        const float den = wSum + alpha;
-        if (den > kEps) {
-            const float dl = -(Cv + alpha * lambda) / den;
-            s.distLambda[c] = lambda + dl;
-            cA = mk4(wA * dl * -grad * relax, 0.0f);
-            cB = mk4(wB * dl * grad * relax, 0.0f);
+    for (int64_t cc = 0; cc < int64_t(s.dists.size()); ++cc) solveDistanceOne(s, dt, relax, uint32_t(cc));
+}
+
+// ---- coloured XPBD schedules (this build's opt-in; no reference counterpart) ----
+// Greedy colouring: constraint c, in ascending order, takes the lowest colour that no earlier
+// constraint sharing one of its elements holds.  Restated here with per-element colour lists.
+template <class F>
+void colourFamily(uint32_t n, uint32_t count, uint32_t per, F elementOf, std::vector<uint32_t> &order,
+                  std::vector<uint32_t> &starts)
+{
+    order.clear();
+    starts.clear();
+    if (count == 0) return;
+    std::vector<std::vector<uint32_t>> held(n);
+    std::vector<uint32_t> colourOf(count);
+    uint32_t colours = 0;
+    for (uint32_t c = 0; c < count; ++c) {
+        std::vector<uint32_t> taken;
+        for (uint32_t k = 0; k < per; ++k) {
+            const uint32_t e = elementOf(c, k);
+            if (e < n) taken.insert(taken.end(), held[e].begin(), held[e].end());
+        }
+        std::sort(taken.begin(), taken.end());
+        uint32_t colour = 0;
+        for (uint32_t t : taken) {
+            if (t == colour) ++colour;
+            else if (t > colour) break;
+        }
+        for (uint32_t k = 0; k < per; ++k) {
+            const uint32_t e = elementOf(c, k);
+            if (e < n) held[e].push_back(colour);
+        }
+        colourOf[c] = colour;
+        colours = std::max(colours, colour + 1);
+    }
+    starts.assign(colours + 1, 0);
+    for (uint32_t c = 0; c < count; ++c) ++starts[colourOf[c] + 1];
+    for (uint32_t k = 0; k < colours; ++k) starts[k + 1] += starts[k];
+    order.resize(count);
+    std::vector<uint32_t> fill(starts.begin(), starts.end() - 1);
+    for (uint32_t c = 0; c < count; ++c) order[fill[colourOf[c]]++] = c;
+}
+
+void buildColourings(cno_solver &s)
+{
+    const uint32_t N = s.N, S = uint32_t(s.segs.size()), nb = uint32_t(s.bends.size());
+    colourFamily(N, uint32_t(s.edges.size()), 2, [&](uint32_t c, uint32_t k) {
+        return k == 0 ? s.edges[c].particle_a : s.edges[c].particle_b; }, s.colOrder[0], s.colStarts[0]);
+    colourFamily(N, S, 2, [&](uint32_t c, uint32_t k) {
+        return k == 0 ? s.segs[c].particle_a : s.segs[c].particle_b; }, s.colOrder[1], s.colStarts[1]);
+    colourFamily(N, nb + uint32_t(s.dihedrals.size()), 4, [&](uint32_t c, uint32_t k) -> uint32_t {
+        if (c < nb) {
+            const cn_soft_bend &b = s.bends[c];
+            return k == 0 ? b.particle0 : k == 1 ? b.particle1 : k == 2 ? b.particle2 : 0xffffffffu;
+        }
+        const cn_cloth_dihedral &h = s.dihedrals[c - nb];
+        return k == 0 ? h.edge_particle0 : k == 1 ? h.edge_particle1 : k == 2 ? h.opposite_particle0
+                                                                             : h.opposite_particle1;
+    }, s.colOrder[2], s.colStarts[2]);
+    colourFamily(S, uint32_t(s.joints.size()), 2, [&](uint32_t c, uint32_t k) {
+        return k == 0 ? s.joints[c].segment_a : s.joints[c].segment_b; }, s.colOrder[3], s.colStarts[3]);
+    colourFamily(N, uint32_t(s.dists.size()), 2, [&](uint32_t c, uint32_t k) {
+        return k == 0 ? s.dists[c].particle_a : s.dists[c].particle_b; }, s.colOrder[4], s.colStarts[4]);
+    colourFamily(N, uint32_t(s.tets.size()), 4, [&](uint32_t c, uint32_t k) {
+        return s.tets[c].particle_indices[k]; }, s.colOrder[5], s.colStarts[5]);
+    s.softAcc.assign(N, f4{0, 0, 0, 0});
+    s.orientAcc.assign(S, f4{0, 0, 0, 0});
+}
+
+// A constraint's records into its particles (Gauss-Seidel: x += r where invMass > kEps) or into
+// the family's per-particle sum (colour Jacobi).
+inline void moveRecord(cno_solver &s, bool gs, uint32_t p, const f4 &r)
+{
+    if (p >= s.N) return;
+    if (gs) {
+        const f4 q = s.x[p];
+        if (q.w > kEps) s.x[p] = mk4(xyz(q) + xyz(r), q.w);
+    } else {
+        s.softAcc[p] = mk4(xyz(s.softAcc[p]) + xyz(r), 0.0f);
+    }
+}
+inline void moveOrientation(cno_solver &s, bool gs, uint32_t g, const f4 &r)
+{
+    if (g >= s.segs.size()) return;
+    if (gs) s.segOrient[g] = QNormalize(s.segOrient[g] + r);
+    else s.orientAcc[g] = s.orientAcc[g] + r;
+}
+
+void colourOne(cno_solver &s, uint32_t fam, float dt, float relax, bool gs, uint32_t c)
+{
+    const uint32_t nb = uint32_t(s.bends.size());
+    switch (fam) {
+    case 0: {
+        solveEdgeOne(s, dt, relax, c);
+        moveRecord(s, gs, s.edges[c].particle_a, s.edgeCorr[2 * c]);
+        moveRecord(s, gs, s.edges[c].particle_b, s.edgeCorr[2 * c + 1]);
+        break;
+    }
+    case 1: { // the segment's own orientation is read by it alone: applied in place
+        solveSegmentOne(s, dt, relax, c);
+        moveRecord(s, gs, s.segs[c].particle_a, s.segCorr[3 * c]);
+        moveRecord(s, gs, s.segs[c].particle_b, s.segCorr[3 * c + 1]);
+        s.segOrient[c] = QNormalize(s.segOrient[c] + s.segCorr[3 * c + 2]);
+        break;
+    }
+    case 2: {
+        const f4 *r = &s.bendCorr[4 * size_t(c)];
+        if (c < nb) {
+            solveBendOne(s, dt, relax, c);
+            moveRecord(s, gs, s.bends[c].particle0, r[0]);
+            moveRecord(s, gs, s.bends[c].particle1, r[1]);
+            moveRecord(s, gs, s.bends[c].particle2, r[2]);
+        } else {
+            solveDihedralOne(s, dt, relax, c - nb);
+            const cn_cloth_dihedral &h = s.dihedrals[c - nb];
+            moveRecord(s, gs, h.edge_particle0, r[0]);
+            moveRecord(s, gs, h.edge_particle1, r[1]);
+            moveRecord(s, gs, h.opposite_particle0, r[2]);
+            moveRecord(s, gs, h.opposite_particle1, r[3]);
+        }
+        break;
+    }
+    case 3: {
+        solveJointOne(s, dt, relax, c);
+        moveOrientation(s, gs, s.joints[c].segment_a, s.jointCorr[5 * c + 3]);
+        moveOrientation(s, gs, s.joints[c].segment_b, s.jointCorr[5 * c + 4]);
+        break;
+    }
+    case 4: {
+        solveDistanceOne(s, dt, relax, c);
+        moveRecord(s, gs, s.dists[c].particle_a, s.distCorr[2 * c]);
+        moveRecord(s, gs, s.dists[c].particle_b, s.distCorr[2 * c + 1]);
+        break;
+    }
+    default: {
+        solveTetOne(s, dt, relax, c);
+        for (uint32_t k = 0; k < 4; ++k) moveRecord(s, gs, s.tets[c].particle_indices[k], s.tetCorr[4 * c + k]);
+        break;
+    }
+    }
+}
+
+// Particles [lo, hi) with records in a family's incidence (strand distances: the segments').
+std::pair<uint32_t, uint32_t> familyWindow(const cno_solver &s, uint32_t fam)
+{
+    const std::vector<Range> &r = fam == 0 ? s.edgeRanges : fam == 2 ? s.bendRanges : fam == 5 ? s.tetRanges : s.segRanges;
+    uint32_t lo = uint32_t(r.size()), hi = 0;
+    for (uint32_t i = 0; i < r.size(); ++i)
+        if (r[i].count) {
+            lo = std::min(lo, i);
+            hi = i + 1;
+        }
+    return lo < hi ? std::make_pair(lo, hi) : std::make_pair(0u, 0u);
+}
+
+// One soft iteration under a coloured schedule: each family in the gather order, colour by colour.
+void colouredSoftIteration(cno_solver &s, float dt)
+{
+    const float relax = s.desc.soft.internal_relaxation;
+    const bool gs = s.desc.soft.xpbd_schedule == CN_XPBD_COLOUR_GAUSS_SEIDEL;
+    for (uint32_t fam = 0; fam < 6; ++fam) {
+        const std::vector<uint32_t> &order = s.colOrder[fam], &starts = s.colStarts[fam];
+        if (order.empty()) continue;
+        for (size_t k = 0; k + 1 < starts.size(); ++k) {
+#pragma omp parallel for schedule(static)
+            for (int64_t j = int64_t(starts[k]); j < int64_t(starts[k + 1]); ++j)
+                colourOne(s, fam, dt, relax, gs, order[size_t(j)]);
+        }
+        if (gs) continue;
+        if (fam == 3) {
+            for (size_t g = 0; g < s.segs.size(); ++g) {
+                const f4 a = s.orientAcc[g];
+                s.orientAcc[g] = f4{0, 0, 0, 0};
+                s.segOrient[g] = QNormalize(s.segOrient[g] + a);
+            }
+            continue;
+        }
+        const auto win = familyWindow(s, fam);
+        for (uint32_t i = win.first; i < win.second; ++i) {
+            const f4 a = s.softAcc[i];
+            s.softAcc[i] = f4{0, 0, 0, 0};
+            const f4 p = s.x[i];
+            if (p.w > kEps) s.x[i] = mk4(xyz(p) + xyz(a), p.w);
         }
     }
 }
@@ -3131,7 +3327,9 @@ void stepFrame(cno_solver &s, float frameDt)
                 fluidDeltaPositions(s, it, dt);
                 fluidApplyAndClamp(s, it);
             }
-            if (runSoft) {
+            if (runSoft && s.desc.soft.xpbd_schedule != CN_XPBD_GATHER) {
+                colouredSoftIteration(s, dt);
+            } else if (runSoft) {
                 solveEdges(s, dt);
                 applyPairCorrections(s, s.edgeRanges, s.edgeInc, s.edgeCorr);
                 solveSegments(s, dt);
@@ -3216,6 +3414,7 @@ CN_API cno_solver *cno_create(const cn_solver_desc *desc, const cn_world_soa *wo
     cno_solver *s = new cno_solver();
     s->desc = *desc;
     setupWorld(*s, *world);
+    if (desc->soft.xpbd_schedule != CN_XPBD_GATHER) buildColourings(*s);
     return s;
 }
 

@@ -37,14 +37,14 @@ def test_struct_sizes_match_header():
     src = r'''
 #include <stdio.h>
 #include "cn_physics.h"
-int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n",
+int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n",
  sizeof(cn_solver_desc),
  sizeof(cn_world_soa), sizeof(cn_soft_body_grid_desc), sizeof(cn_fluid_grid_desc), sizeof(cn_cloth_grid_desc),
  sizeof(cn_strand_desc), sizeof(cn_rigid_body_desc), sizeof(cn_collider_desc), sizeof(cn_meta), sizeof(cn_scene_view),
  sizeof(cn_batch_desc), sizeof(cn_batch_stats), sizeof(cn_batch_tuning), sizeof(cn_server_desc),
  sizeof(cn_request_done), sizeof(cn_server_stats), sizeof(cn_diff_desc), sizeof(cn_surface_vertex_binding),
  sizeof(cn_surface_triangle_range), sizeof(cn_surface_render_data), sizeof(cn_surface_mesh_desc),
- sizeof(cn_surface_render_view), sizeof(cn_rigid_proxy_desc)); return 0;}
+ sizeof(cn_surface_render_view), sizeof(cn_rigid_proxy_desc), sizeof(cn_schedule_info), sizeof(cn_soft_settings)); return 0;}
 '''
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "s.c")
@@ -58,7 +58,8 @@ int main(){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %
                                   _abi.Meta, _abi.SceneView, _abi.BatchDesc, _abi.BatchStats, _abi.BatchTuning,
                                   _abi.ServerDesc, _abi.RequestDone, _abi.ServerStats, _abi.DiffDesc,
                                   _abi.SurfaceVertexBinding, _abi.SurfaceTriangleRange, _abi.SurfaceRenderData,
-                                  _abi.SurfaceMeshDesc, _abi.SurfaceRenderView, _abi.RigidProxyDesc)]
+                                  _abi.SurfaceMeshDesc, _abi.SurfaceRenderView, _abi.RigidProxyDesc,
+                                  _abi.ScheduleInfo, _abi.SoftSettings)]
     assert got == want
 
 
