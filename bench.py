@@ -395,6 +395,7 @@ def run_served(args, stream, sh, rank: int = 0, world: int = 1) -> dict:
 
     # served: a fresh batch (same schedule) behind the server, Poisson load in real time
     bd.tile_elements, bd.blocks_per_sm = tune["tile_elements"], tune["blocks_per_sm"]
+    bd.fused_cluster_ctas = tune["cluster_ctas"]
     b = Batch(bd)
     srv = Server(b, dt)
     sids = [srv.register(sc.world.soa()) for sc in pool]
@@ -438,7 +439,8 @@ def run_served(args, stream, sh, rank: int = 0, world: int = 1) -> dict:
                   "method": "one cn_solver per scene, one frame of every scene in turn (CUDA-graph replays)"},
         "batched": {"value": round(batched_rate, 1), "tick_ms_p50": round(tick_ms, 3),
                     "tick_ms_max": round(max(ticks), 3), "schedule": {"tile_elements": tune["tile_elements"],
-                                                                      "blocks_per_sm": tune["blocks_per_sm"]},
+                                                                      "blocks_per_sm": tune["blocks_per_sm"],
+                                                                      "fused_cluster_ctas": tune["cluster_ctas"]},
                     "autotune_candidates": tune["candidates"]},
         "batched_over_plain": round(batched_rate / plain_rate, 2),
         "served": {"offered_frames_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds,

@@ -672,13 +672,20 @@ class Batch:
     def set_schedule(self, tile_elements: int, blocks_per_sm: int) -> None:
         _check(self._lib.cn_batch_set_schedule(self._h, tile_elements, blocks_per_sm))
 
+    def set_fused(self, cluster_ctas: int) -> None:
+        """0: per-phase iteration kernels; 1, 2, 4 or 8: the persistent fused iterations, one
+        cluster of that many CTAs per scene at a time."""
+        _check(self._lib.cn_batch_set_fused(self._h, cluster_ctas))
+
     def autotune(self, scenes: Sequence[int], dt: float) -> dict:
         ids = np.ascontiguousarray(np.asarray(scenes, dtype=np.uint32))
         t = _abi.BatchTuning()
         _check(self._lib.cn_batch_autotune(self._h, _u32(ids), ids.size, dt, C.byref(t)))
         return {"tile_elements": t.tile_elements, "blocks_per_sm": t.blocks_per_sm, "tick_ms": t.tick_ms,
+                "cluster_ctas": t.cluster_ctas,
                 "candidates": [(t.candidates[k].tile_elements, t.candidates[k].blocks_per_sm,
-                                round(t.candidates[k].tick_ms, 4)) for k in range(t.candidate_count)]}
+                                round(t.candidates[k].tick_ms, 4), t.candidates[k].cluster_ctas)
+                               for k in range(t.candidate_count)]}
 
 
 class Server:

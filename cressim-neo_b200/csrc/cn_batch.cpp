@@ -151,6 +151,12 @@ struct cn_batch {
     uint32_t substeps = 1, softIt = 1, contactIt = 1, maxIt = 1;
     uint32_t tileElems = 256, blocksPerSm = 8, smCount = 148, grid = 0;
     uint64_t ticks = 0;
+    // persistent fused iterations: CTAs per scene cluster (0: per-phase kernels), clusters of the
+    // grid, and the tick's scene list (per stepped scene its particle, edge and tet ranges;
+    // counter 6 = scenes, counter 7 = the next scene to take, both staged with the work lists)
+    uint32_t clusterCtas = 0, clusters = 0;
+    uint2 *dScenes = nullptr;
+    uint2 *hScenes[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -197,6 +203,14 @@ cn_status allocWorkLists(cn_batch *b)
         if (b->hStage[k]) cudaFreeHost(b->hStage[k]);
     b->dTiles = nullptr; b->dCounts = nullptr; b->dTargets = nullptr;
     b->hStage[0] = b->hStage[1] = nullptr;
+    if (b->dScenes) cudaFree(b->dScenes);
+    for (int k = 0; k < 2; ++k)
+        if (b->hScenes[k]) cudaFreeHost(b->hScenes[k]);
+    b->dScenes = nullptr;
+    b->hScenes[0] = b->hScenes[1] = nullptr;
+    const size_t sceneListBytes = size_t(3) * std::max<uint32_t>(b->desc.max_scenes, 1u) * sizeof(uint2);
+    CN_CUDA(cudaMalloc(&b->dScenes, sceneListBytes));
+    for (int k = 0; k < 2; ++k) CN_CUDA(cudaMallocHost(&b->hScenes[k], sceneListBytes));
     CN_CUDA(cudaMalloc(&b->dTiles, size_t(b->tileTotal) * sizeof(uint2)));
     CN_CUDA(cudaMalloc(&b->dCounts, 8 * sizeof(uint32_t)));
     CN_CUDA(cudaMalloc(&b->dTargets, size_t(b->targetCap) * sizeof(cn::BodyTarget)));
@@ -279,7 +293,19 @@ void enqueueTick(cn_batch *b, float frameDt, cudaStream_t st)
         if (b->contactIt) cn::launchRigidCandidates(s, b->scanScratch, b->scanScratchBytes, st);
         if (s.E) cudaMemsetAsync(s.edgeLambda, 0, sizeof(float) * s.E, st);
         if (s.T) cudaMemsetAsync(s.tetLambda, 0, sizeof(float) * s.T, st);
-        for (uint32_t it = 0; it < b->maxIt; ++it) {
+        if (b->clusterCtas) {
+            // every iteration of the substep in one persistent kernel, one scene per cluster
+            cn::BatchFusedPlan plan{};
+            plan.iterations = b->maxIt;
+            plan.softIterations = b->softIt;
+            plan.contactIterations = b->contactIt;
+            plan.scenes = b->dScenes;
+            plan.sceneCount = b->dCounts + 6;
+            plan.next = b->dCounts + 7;
+            if (sub > 0) cudaMemsetAsync(b->dCounts + 7, 0, sizeof(uint32_t), st);
+            cn::launchBatchFusedIterations(s, c, dt, plan, b->clusterCtas, b->clusters, st);
+        }
+        for (uint32_t it = 0; it < (b->clusterCtas ? 0u : b->maxIt); ++it) {
             const bool runSoft = (s.E || s.T) && it < b->softIt;
             const bool runRigid = it < b->contactIt;
             if (!runSoft && !runRigid) break;
@@ -406,6 +432,13 @@ CN_API cn_status cn_batch_create(const cn_batch_desc *d, int device, cn_batch **
         cn_batch_destroy(b);
         return st;
     }
+    if (d->fused_cluster_ctas) {
+        const cn_status fs = cn_batch_set_fused(b, d->fused_cluster_ctas);
+        if (fs != CN_OK) {
+            cn_batch_destroy(b);
+            return fs;
+        }
+    }
     b->cfg = cn::configFromDesc(d->solver);
     const cn_solver_desc &sd = d->solver;
     b->substeps = std::max<uint32_t>(sd.substeps, 1u);
@@ -437,8 +470,10 @@ CN_API void cn_batch_destroy(cn_batch *b)
     if (b->dTiles) cudaFree(b->dTiles);
     if (b->dCounts) cudaFree(b->dCounts);
     if (b->dTargets) cudaFree(b->dTargets);
+    if (b->dScenes) cudaFree(b->dScenes);
     for (int k = 0; k < 2; ++k) {
         if (b->hStage[k]) cudaFreeHost(b->hStage[k]);
+        if (b->hScenes[k]) cudaFreeHost(b->hScenes[k]);
         if (b->stageDone[k]) cudaEventDestroy(b->stageDone[k]);
     }
     if (b->ownStream) cudaStreamDestroy(b->ownStream);
@@ -655,11 +690,17 @@ CN_API cn_status cn_batch_step(cn_batch *b, const uint32_t *scene_ids, uint32_t 
     cn::BodyTarget *targets = reinterpret_cast<cn::BodyTarget *>(counts + 8);
     std::memset(counts, 0, 8 * sizeof(uint32_t));
     const uint32_t te = b->tileElems;
+    if (count > std::max<uint32_t>(b->desc.max_scenes, 1u))
+        return setError(CN_ERR_CAPACITY, "cn_batch_step: more scenes than max_scenes");
+    uint2 *sceneList = b->hScenes[k];
     for (uint32_t n = 0; n < count; ++n) {
         const uint32_t id = scene_ids[n];
         if (id >= b->scenes.size() || !b->scenes[id].live)
             return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_step: scene " + std::to_string(id) + " is not resident");
         const BatchScene &sc = b->scenes[id];
+        sceneList[3 * n] = make_uint2(sc.p.start, sc.p.start + sc.p.count);
+        sceneList[3 * n + 1] = make_uint2(sc.e.start, sc.e.start + sc.e.count);
+        sceneList[3 * n + 2] = make_uint2(sc.t.start, sc.t.start + sc.t.count);
         const Range fam[5] = {sc.p, sc.e, sc.t, sc.b, sc.c};
         for (int f = 0; f < 5; ++f) {
             const uint32_t step = f >= 3 ? std::max<uint32_t>(fam[f].count, 1u) : te;
@@ -673,6 +714,7 @@ CN_API cn_status cn_batch_step(cn_batch *b, const uint32_t *scene_ids, uint32_t 
     const uint32_t nt = uint32_t(std::min<size_t>(b->pendingTargets.size(), b->targetCap));
     std::copy(b->pendingTargets.begin(), b->pendingTargets.begin() + nt, targets);
     counts[5] = nt;
+    counts[6] = count; // scenes of the fused iterations; counts[7] (the next one to take) stays 0
     b->pendingTargets.erase(b->pendingTargets.begin(), b->pendingTargets.begin() + nt);
     const cn_status gs = ensureGraph(b, frame_dt);
     if (gs != CN_OK) return gs;
@@ -682,6 +724,8 @@ CN_API cn_status cn_batch_step(cn_batch *b, const uint32_t *scene_ids, uint32_t 
                                     cudaMemcpyHostToDevice, st));
     CN_CUDA(cudaMemcpyAsync(b->dCounts, counts, 8 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     if (nt) CN_CUDA(cudaMemcpyAsync(b->dTargets, targets, size_t(nt) * sizeof(cn::BodyTarget), cudaMemcpyHostToDevice, st));
+    if (count && b->clusterCtas)
+        CN_CUDA(cudaMemcpyAsync(b->dScenes, sceneList, size_t(3) * count * sizeof(uint2), cudaMemcpyHostToDevice, st));
     CN_CUDA(cudaEventRecord(b->stageDone[k], st));
     CN_CUDA(cudaGraphLaunch(b->graphExec, st));
     CN_CUDA(cudaGetLastError());
@@ -743,6 +787,26 @@ CN_API cn_status cn_batch_get_stats(cn_batch *b, cn_batch_stats *out)
     out->ticks = b->ticks;
     out->tile_elements = b->tileElems;
     out->grid_blocks = b->grid;
+    out->fused_cluster_ctas = b->clusterCtas;
+    return CN_OK;
+}
+
+CN_API cn_status cn_batch_set_fused(cn_batch *b, uint32_t cluster_ctas)
+{
+    if (!b) return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_set_fused: null batch");
+    if (cluster_ctas != 0u && cluster_ctas != 1u && cluster_ctas != 2u && cluster_ctas != 4u && cluster_ctas != 8u)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_set_fused: cluster_ctas is 0, 1, 2, 4 or 8");
+    CN_CUDA(cudaSetDevice(b->device));
+    CN_CUDA(cudaDeviceSynchronize());
+    uint32_t clusters = 0;
+    if (cluster_ctas) {
+        clusters = cn::batchFusedClusters(cluster_ctas);
+        if (clusters == 0u) return setError(CN_ERR_UNSUPPORTED, "cn_batch_set_fused: clusters of this size cannot be formed");
+        clusters = std::min<uint32_t>(clusters, std::max<uint32_t>(b->desc.max_scenes, 1u));
+    }
+    b->clusterCtas = cluster_ctas;
+    b->clusters = clusters;
+    releaseGraph(b);
     return CN_OK;
 }
 
@@ -791,47 +855,62 @@ CN_API cn_status cn_batch_autotune(cn_batch *b, const uint32_t *scene_ids, uint3
     b->pendingTargets.clear();
     const uint32_t tiles[] = {128, 256, 512, 1024};
     const uint32_t blocks[] = {4, 8, 16, 32};
+    const uint32_t clusterSizes[] = {1, 2, 4, 8};
     float best = 1e30f;
-    uint32_t bestTile = b->tileElems, bestBlocks = b->blocksPerSm;
+    uint32_t bestTile = b->tileElems, bestBlocks = b->blocksPerSm, bestCtas = 0;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     std::memset(out, 0, sizeof(*out));
     uint32_t n = 0;
+    const uint32_t capacity = uint32_t(sizeof(out->candidates) / sizeof(out->candidates[0]));
+    // warm-up (capture + first replay), then three timed ticks; the state is restored after
+    auto trial = [&](uint32_t te, uint32_t bps, uint32_t ctas) -> cn_status {
+        cn_status st = cn_batch_step(b, scene_ids, count, frame_dt, b->ownStream);
+        if (st != CN_OK) return st;
+        cudaEventRecord(e0, b->ownStream);
+        for (int r = 0; r < 3; ++r) cn_batch_step(b, scene_ids, count, frame_dt, b->ownStream);
+        cudaEventRecord(e1, b->ownStream);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= 3.0f;
+        if (n < capacity) out->candidates[n++] = cn_batch_candidate{te, bps, ms, ctas};
+        if (ms < best) {
+            best = ms;
+            bestTile = te;
+            bestBlocks = bps;
+            bestCtas = ctas;
+        }
+        const cudaError_t e = save(false);
+        return e == cudaSuccess ? CN_OK : setError(CN_ERR_CUDA, std::string("cn_batch_autotune: ") + cudaGetErrorString(e));
+    };
+    cn_status st = cn_batch_set_fused(b, 0);
     for (uint32_t te : tiles)
         for (uint32_t bps : blocks) {
-            cn_status st = cn_batch_set_schedule(b, te, bps);
-            if (st != CN_OK) break;
-            // warm-up (capture + first replay), then the timed ticks
-            st = cn_batch_step(b, scene_ids, count, frame_dt, b->ownStream);
-            if (st != CN_OK) break;
-            cudaEventRecord(e0, b->ownStream);
-            for (int r = 0; r < 3; ++r) cn_batch_step(b, scene_ids, count, frame_dt, b->ownStream);
-            cudaEventRecord(e1, b->ownStream);
-            cudaEventSynchronize(e1);
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            ms /= 3.0f;
-            if (n < 16) {
-                out->candidates[n].tile_elements = te;
-                out->candidates[n].blocks_per_sm = bps;
-                out->candidates[n].tick_ms = ms;
-                ++n;
-            }
-            if (ms < best) {
-                best = ms;
-                bestTile = te;
-                bestBlocks = bps;
-            }
-            CN_CUDA(save(false));
+            if (st == CN_OK) st = cn_batch_set_schedule(b, te, bps);
+            if (st == CN_OK) st = trial(te, bps, 0);
         }
+    // the persistent fused iterations, with the other phases at the best tile schedule so far
+    const uint32_t tileForFused = bestTile, blocksForFused = bestBlocks;
+    if (st == CN_OK) st = cn_batch_set_schedule(b, tileForFused, blocksForFused);
+    for (uint32_t ctas : clusterSizes) {
+        if (st != CN_OK) break;
+        if (cn_batch_set_fused(b, ctas) != CN_OK) {
+            cn::clearError(); // clusters of this size cannot be formed: not a candidate
+            continue;
+        }
+        st = trial(tileForFused, blocksForFused, ctas);
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     out->candidate_count = n;
     out->tile_elements = bestTile;
     out->blocks_per_sm = bestBlocks;
+    out->cluster_ctas = bestCtas;
     out->tick_ms = best;
-    const cn_status st = cn_batch_set_schedule(b, bestTile, bestBlocks);
+    if (st == CN_OK) st = cn_batch_set_schedule(b, bestTile, bestBlocks);
+    if (st == CN_OK) st = cn_batch_set_fused(b, bestCtas);
     CN_CUDA(save(false));
     b->pendingTargets = staged;
     b->ticks = 0;

@@ -375,6 +375,19 @@ struct FusedShape {
     uint32_t ctas = 0, threads = 0;
 };
 FusedShape fusedIterationsShape();
+// A batch tick's iterations as one persistent kernel (cn_batch): `clusters` clusters of `ctas`
+// CTAs, each taking stepped scenes from `next` (zero at the tick's start) until `sceneCount`;
+// scenes[3 j .. 3 j + 2] = scene j's particle, edge and tet ranges [x, y).
+struct BatchFusedPlan {
+    uint32_t iterations, softIterations, contactIterations;
+    const uint2 *scenes;
+    const uint32_t *sceneCount;
+    uint32_t *next;
+};
+// Clusters of `ctas` CTAs that fit on the device at once (0: unavailable).
+uint32_t batchFusedClusters(uint32_t ctas);
+void launchBatchFusedIterations(const Scene &s, const Config &c, float dt, const BatchFusedPlan &plan, uint32_t ctas,
+                                uint32_t clusters, cudaStream_t st);
 void launchFusedIterations(const Scene &s, const Config &c, float dt, const XpbdPlan &plan, uint32_t iterations,
                            uint32_t softIterations, uint32_t contactIterations, bool rigid, const FusedShape &shape,
                            cudaStream_t st);

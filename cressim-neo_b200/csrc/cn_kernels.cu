@@ -2994,6 +2994,56 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_fusedIterations(Scene s, C
     }
 }
 
+// A batch tick's iterations as one persistent kernel: each thread-block cluster takes the next
+// stepped scene from a device counter and runs every iteration of the substep on it (edge and
+// tet families in the gather schedule, then the particle-rigid contacts), its phases separated
+// by cluster barriers, so one scene's records and positions stay on chip across the iterations
+// instead of the whole pool streaming through HBM once per phase.  Per element the same device
+// functions as the per-phase batch kernels: bit-identical results.  The scene index is taken by
+// one thread and handed to the cluster through its shared memory between two barriers, so the
+// loop's trip count is uniform over the cluster.
+constexpr uint32_t kBatchFusedThreads = 256u;
+
+__global__ void __launch_bounds__(kBatchFusedThreads, 2) k_batchFusedIterations(Scene s, Config cfg, float dt,
+                                                                           BatchFusedPlan plan)
+{
+    namespace cg = cooperative_groups;
+    const cg::cluster_group cl = cg::this_cluster();
+    __shared__ uint32_t taken;
+    const uint32_t tid = cl.block_rank() * blockDim.x + threadIdx.x;
+    const uint32_t nth = cl.num_blocks() * blockDim.x;
+    const uint32_t count = *plan.sceneCount;
+    const float relax = cfg.softInternalRelaxation;
+    for (;;) {
+        if (cl.block_rank() == 0u && threadIdx.x == 0u) taken = atomicAdd(plan.next, 1u);
+        cl.sync();
+        const uint32_t j = *cl.map_shared_rank(&taken, 0);
+        cl.sync(); // every thread has its copy before the leader takes the next one
+        if (j >= count) break;
+        const uint2 pr = plan.scenes[3u * j], er = plan.scenes[3u * j + 1u], tr = plan.scenes[3u * j + 2u];
+        for (uint32_t it = 0; it < plan.iterations; ++it) {
+            if ((s.E || s.T) && it < plan.softIterations) {
+                if (s.E) {
+                    for (uint32_t e = er.x + tid; e < er.y; e += nth) solveEdge(s, dt, relax, e);
+                    cl.sync();
+                    for (uint32_t i = pr.x + tid; i < pr.y; i += nth) applyPairAt(s, s.edgeRanges, s.edgeInc, s.edgeCorr, i);
+                    cl.sync();
+                }
+                if (s.T) {
+                    for (uint32_t t = tr.x + tid; t < tr.y; t += nth) solveTet(s, dt, relax, t);
+                    cl.sync();
+                    for (uint32_t i = pr.x + tid; i < pr.y; i += nth) applyQuadAt(s, s.tetRanges, s.tetInc, s.tetCorr, i);
+                    cl.sync();
+                }
+            }
+            if (it < plan.contactIterations) {
+                for (uint32_t i = pr.x + tid; i < pr.y; i += nth) rigidContactsAt(s, cfg, true, i);
+                cl.sync();
+            }
+        }
+    }
+}
+
 template <uint32_t kSchedule> cudaError_t fusedLaunch(const Scene &s, const Config &c, float dt, const FusedPlan &plan,
                                                      const FusedShape &shape, cudaStream_t st)
 {
@@ -3091,6 +3141,50 @@ void launchFusedIterations(const Scene &s, const Config &c, float dt, const Xpbd
     if (plan.schedule == CN_XPBD_COLOUR_JACOBI) fusedLaunch<CN_XPBD_COLOUR_JACOBI>(s, c, dt, fp, shape, st);
     else if (plan.schedule == CN_XPBD_COLOUR_GAUSS_SEIDEL) fusedLaunch<CN_XPBD_COLOUR_GAUSS_SEIDEL>(s, c, dt, fp, shape, st);
     else fusedLaunch<CN_XPBD_GATHER>(s, c, dt, fp, shape, st);
+}
+
+uint32_t batchFusedClusters(uint32_t ctas)
+{
+    if (ctas == 0u || ctas > 8u) return 0u;
+    if (cudaFuncSetAttribute(reinterpret_cast<const void *>(&k_batchFusedIterations),
+                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        cudaGetLastError();
+        return 0u;
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(ctas, 1, 1);
+    cfg.blockDim = dim3(kBatchFusedThreads, 1, 1);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, reinterpret_cast<const void *>(&k_batchFusedIterations), &cfg) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 0u;
+    }
+    return clusters > 0 ? uint32_t(clusters) : 0u;
+}
+
+void launchBatchFusedIterations(const Scene &s, const Config &c, float dt, const BatchFusedPlan &plan, uint32_t ctas,
+                                uint32_t clusters, cudaStream_t st)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(ctas * clusters, 1, 1);
+    cfg.blockDim = dim3(kBatchFusedThreads, 1, 1);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = ctas;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_batchFusedIterations, s, c, dt, plan);
 }
 
 void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st)

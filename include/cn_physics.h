@@ -704,22 +704,29 @@ typedef struct cn_batch_desc {
     uint32_t tile_elements;         /* elements per work tile (autotuned by cn_batch_autotune) */
     uint32_t blocks_per_sm;         /* grid of the tile kernels = SMs x this */
     uint32_t rigid_pairs_per_particle;
-    uint32_t reserved[3];
+    uint32_t fused_cluster_ctas;    /* 0: the iterations as per-phase kernels over the tick's work
+                                     * lists; n: as one persistent kernel, each cluster of n CTAs
+                                     * taking one scene at a time (bit-identical; autotuned) */
+    uint32_t reserved[2];
 } cn_batch_desc;
 
 typedef struct cn_batch_stats {
     uint32_t resident_scenes;
     uint32_t particles_used, particle_capacity, edges_used, edge_capacity, tets_used, tet_capacity;
-    uint32_t tile_elements, grid_blocks, reserved0;
+    uint32_t tile_elements, grid_blocks, fused_cluster_ctas;
     uint64_t budget_bytes, budget_used_bytes, pool_bytes, ticks;
 } cn_batch_stats;
 
-typedef struct cn_batch_candidate { uint32_t tile_elements, blocks_per_sm; float tick_ms; uint32_t reserved; } cn_batch_candidate;
+/* cluster_ctas: 0 for the per-phase iteration kernels, else the CTAs per scene of the persistent
+ * fused iterations (cn_batch_desc.fused_cluster_ctas). */
+typedef struct cn_batch_candidate { uint32_t tile_elements, blocks_per_sm; float tick_ms; uint32_t cluster_ctas; } cn_batch_candidate;
 typedef struct cn_batch_tuning {
     uint32_t tile_elements, blocks_per_sm;
     float tick_ms;
     uint32_t candidate_count;
-    cn_batch_candidate candidates[16];
+    cn_batch_candidate candidates[24];
+    uint32_t cluster_ctas;
+    uint32_t reserved[3];
 } cn_batch_tuning;
 
 CN_API void cn_batch_desc_defaults(cn_batch_desc *desc);
@@ -742,8 +749,12 @@ CN_API cn_status cn_batch_read_particles(cn_batch *batch, uint32_t scene, float 
 CN_API cn_status cn_batch_export_scene(cn_batch *batch, uint32_t scene, cn_world_soa *world);
 CN_API cn_status cn_batch_get_stats(cn_batch *batch, cn_batch_stats *out);
 CN_API cn_status cn_batch_set_schedule(cn_batch *batch, uint32_t tile_elements, uint32_t blocks_per_sm);
-/* Times a tick of `scenes` for each (tile size, blocks per SM) candidate, keeps the fastest and
- * restores the scenes' state. */
+/* 0: per-phase iteration kernels; 1, 2, 4 or 8: the persistent fused iterations with clusters of
+ * that many CTAs.  CN_ERR_UNSUPPORTED when the device cannot form such clusters. */
+CN_API cn_status cn_batch_set_fused(cn_batch *batch, uint32_t cluster_ctas);
+/* Times a tick of `scenes` for each (tile size, blocks per SM) candidate of the per-phase
+ * kernels, then for the persistent fused iterations with clusters of 1, 2, 4 and 8 CTAs (at the
+ * best tile schedule), keeps the fastest and restores the scenes' state. */
 CN_API cn_status cn_batch_autotune(cn_batch *batch, const uint32_t *scenes, uint32_t count, float frame_dt,
                                    cn_batch_tuning *out);
 

@@ -65,12 +65,18 @@ def test_batch_create_fails_without_device():
 
 
 @pytest.mark.gpu
-def test_batched_scene_equals_its_own_solver_and_is_independent_of_the_mix():
+@pytest.mark.parametrize("cluster_ctas", [0, 1, 2, 4, 8])
+def test_batched_scene_equals_its_own_solver_and_is_independent_of_the_mix(cluster_ctas):
+    """cluster_ctas 0: the per-phase iteration kernels; else the persistent fused iterations with
+    one cluster of that many CTAs per scene (8 substeps per tick: the scene counter is reset
+    between substeps)."""
     pool = small_pool(4)
     frames = 6
     tg = [targets_for(sc, frames, seed=10 + k) for k, sc in enumerate(pool)]
     ref = [own_solver_run(sc, tg[k]) for k, sc in enumerate(pool)]
-    b = Batch(batch_desc(serving.serving_solver_desc(), memory_budget_bytes=1 << 30, particle_capacity=20000))
+    b = Batch(batch_desc(serving.serving_solver_desc(), memory_budget_bytes=1 << 30, particle_capacity=20000,
+                         fused_cluster_ctas=cluster_ctas))
+    assert b.stats()["fused_cluster_ctas"] == cluster_ctas
     ids = [b.add_scene(sc.world.soa()) for sc in pool]
     # scenes 0 and 2 stepped every tick; 1 and 3 only on some ticks (they catch up afterwards)
     done = [0] * len(pool)
@@ -99,6 +105,9 @@ def test_autotune_keeps_state_and_results():
     ids = [b.add_scene(sc.world.soa()) for sc in pool]
     tune = b.autotune(ids, DT)
     assert tune["candidates"] and tune["tick_ms"] > 0
+    fused = [c for c in tune["candidates"] if c[3] > 0]
+    assert len(tune["candidates"]) == 16 + len(fused) and {c[3] for c in fused} <= {1, 2, 4, 8} and fused
+    assert b.stats()["fused_cluster_ctas"] == tune["cluster_ctas"]
     for f in range(3):
         for k in range(len(pool)):
             b.set_kinematic_target(ids[k], pool[k].tool, tg[k][f][:3], tg[k][f][3:])
