@@ -296,6 +296,16 @@ struct BodyTarget {
 };
 
 #ifdef __CUDACC__
+// Programmatic dependent launch: a kernel launched with programmatic stream serialization may
+// start while the previous kernel of its stream finishes; it waits here until that kernel has
+// completed and its writes are visible, then lets the next kernel of the stream launch.  For a
+// kernel launched without the attribute both instructions return at once.
+__device__ __forceinline__ void pdlEnter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Walks the LBVH over the query-order colliders (colQueryCount >= 2) and calls leaf(j) for every
 // sorted leaf j whose box overlaps [qmin, qmax]; leaf returns false to stop the walk.  Each visit
 // reads one internal node's record of both child boxes, so only overlapping subtrees are entered.

@@ -15,6 +15,8 @@
 // --fmad=false so float32 results match a CPU evaluation of the same order.
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
+#include <utility>
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -60,6 +62,33 @@ template <class F> __device__ __forceinline__ void forEachElem(const WorkList &w
     }
 }
 inline unsigned gridFor(const WorkList &w, size_t n) { return w.tiles ? w.grid : blocksFor(n); }
+
+// Launches `k` with programmatic stream serialization (the kernel starts with pdlEnter()), so its
+// launch and CTA dispatch overlap the previous kernel's tail; CN_PDL=0 in the environment turns
+// it off.  Used for the kernels of the solver iterations, which run back to back in thousands.
+bool pdlEnabled()
+{
+    static const bool on = [] {
+        const char *e = std::getenv("CN_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+template <class... P, class... A>
+void launchPdl(void (*k)(P...), unsigned grid, unsigned block, cudaStream_t st, A &&...args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid, 1, 1);
+    cfg.blockDim = dim3(block, 1, 1);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = pdlEnabled() ? 1u : 0u;
+    cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
 // The same for loops that one block runs over a small family (rigid bodies, colliders).
 template <class F> __device__ __forceinline__ void forEachInBlock(const WorkList &w, uint32_t n, F &&f)
 {
@@ -758,6 +787,7 @@ __global__ void __launch_bounds__(kThreads) k_particleCandidates(Scene s, const 
 __global__ void __launch_bounds__(kThreads) k_fluidGather(Scene s, float4 *Xs, const float4 *Dcur,
                                                           uint32_t iter, float4 *P2, const float4 *P0)
 {
+    pdlEnter();
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     float largest = 0.0f;
     if (slot < s.N) {
@@ -914,6 +944,7 @@ template <uint32_t mode, bool kExtras>
 __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidNeighborsDensity(Scene s, Config cfg, bool density,
                                                                                     uint32_t iter, float4 *Dk)
 {
+    pdlEnter();
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= s.N) return;
     const uint32_t info = s.sInfo[slot];
@@ -1080,6 +1111,7 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidDeltaApplyCl
                                                                    uint32_t iter, float dt, bool writeDx,
                                                                    float4 *Pnext)
 {
+    pdlEnter();
     const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= s.N) return;
     const uint32_t info = s.sInfo[slot];
@@ -1318,6 +1350,7 @@ __device__ __forceinline__ void solveEdge(const Scene &s, float dt, float relax,
 
 __global__ void __launch_bounds__(kThreads) k_solveEdges(Scene s, float dt, float relax)
 {
+    pdlEnter();
     forEachElem(s.wE, s.E, [&](uint32_t e) { solveEdge(s, dt, relax, e); });
 }
 
@@ -1369,6 +1402,7 @@ __device__ __forceinline__ void applyPairAt(const Scene &s, const uint2 *ranges,
 __global__ void __launch_bounds__(kThreads) k_applyPair(Scene s, const uint2 *ranges, const uint2 *inc,
                                                         const float4 *corr, uint2 win)
 {
+    pdlEnter();
     if (s.wP.tiles) {
         forEachElem(s.wP, s.N, [&](uint32_t i) { applyPairAt(s, ranges, inc, corr, i); });
         return;
@@ -1386,6 +1420,7 @@ __device__ __forceinline__ void applyQuadAt(const Scene &s, const uint2 *ranges,
 __global__ void __launch_bounds__(kThreads) k_applyQuad(Scene s, const uint2 *ranges, const uint2 *inc,
                                                         const float4 *corr, uint2 win)
 {
+    pdlEnter();
     if (s.wP.tiles) {
         forEachElem(s.wP, s.N, [&](uint32_t i) { applyQuadAt(s, ranges, inc, corr, i); });
         return;
@@ -1426,6 +1461,7 @@ __device__ __forceinline__ void solveTet(const Scene &s, float dt, float relax, 
 
 __global__ void __launch_bounds__(kThreads) k_solveTets(Scene s, float dt, float relax)
 {
+    pdlEnter();
     forEachElem(s.wT, s.T, [&](uint32_t t) { solveTet(s, dt, relax, t); });
 }
 
@@ -1467,6 +1503,7 @@ __device__ __forceinline__ void solveBendAt(const Scene &s, float dt, float rela
 
 __global__ void __launch_bounds__(kThreads) k_solveBends(Scene s, float dt, float relax)
 {
+    pdlEnter();
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b < s.Bn) solveBendAt(s, dt, relax, b);
 }
@@ -1520,6 +1557,7 @@ __device__ __forceinline__ void solveDihedralAt(const Scene &s, float dt, float 
 
 __global__ void __launch_bounds__(kThreads) k_solveDihedrals(Scene s, float dt, float relax)
 {
+    pdlEnter();
     const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
     if (d < s.D) solveDihedralAt(s, dt, relax, d);
 }
@@ -1601,6 +1639,7 @@ __device__ __forceinline__ void solveSegmentAt(const Scene &s, float dt, float r
 
 __global__ void __launch_bounds__(kThreads) k_solveSegments(Scene s, float dt, float relax)
 {
+    pdlEnter();
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g < s.S) solveSegmentAt(s, dt, relax, g);
 }
@@ -1625,6 +1664,7 @@ __device__ __forceinline__ void applySegmentsAt(const Scene &s, uint32_t i)
 
 __global__ void __launch_bounds__(kThreads) k_applySegments(Scene s)
 {
+    pdlEnter();
     applySegmentsAt(s, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
@@ -1674,6 +1714,7 @@ __device__ __forceinline__ void solveJointAt(const Scene &s, float dt, float rel
 
 __global__ void __launch_bounds__(kThreads) k_solveJoints(Scene s, float dt, float relax)
 {
+    pdlEnter();
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j < s.J) solveJointAt(s, dt, relax, j);
 }
@@ -1692,6 +1733,7 @@ __device__ __forceinline__ void applyJointsAt(const Scene &s, uint32_t g)
 
 __global__ void __launch_bounds__(kThreads) k_applyJoints(Scene s)
 {
+    pdlEnter();
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g < s.S) applyJointsAt(s, g);
 }
@@ -1725,6 +1767,7 @@ __device__ __forceinline__ void solveDistanceAt(const Scene &s, float dt, float 
 
 __global__ void __launch_bounds__(kThreads) k_solveDistances(Scene s, float dt, float relax)
 {
+    pdlEnter();
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < s.SD) solveDistanceAt(s, dt, relax, c);
 }
@@ -1768,6 +1811,7 @@ __device__ __forceinline__ void particleContactGenerateAt(const Scene &s, uint32
 
 __global__ void __launch_bounds__(kThreads) k_particleContactGenerate(Scene s)
 {
+    pdlEnter();
     if (blockIdx.x == 0 && threadIdx.x == 0) s.meta_->activeParticleContacts = 0u;
     // a fixed grid strides over the pairs that exist (a device count), not the capacity
     const uint32_t count = s.meta_->particlePairCount;
@@ -1880,6 +1924,7 @@ __device__ __forceinline__ void particleContactSolveAt(const Scene &s, const Con
 
 __global__ void __launch_bounds__(kThreads) k_particleContactSolve(Scene s, Config cfg)
 {
+    pdlEnter();
     // a fixed grid strides over the pairs that exist (a device count), not the capacity
     const uint32_t count = s.meta_->particlePairCount;
     for (uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x; pi < count; pi += gridDim.x * blockDim.x)
@@ -2100,12 +2145,14 @@ __device__ __forceinline__ void rigidContactsAt(const Scene &s, const Config &cf
 
 __global__ void __launch_bounds__(kThreads) k_rigidContacts(Scene s, Config cfg, bool applyDirect)
 {
+    pdlEnter();
     forEachElem(s.wP, s.N, [&](uint32_t i) { rigidContactsAt(s, cfg, applyDirect, i); });
 }
 
 // physics_particle_apply_position_corrections.cs.hlsl:8-30
 __global__ void __launch_bounds__(kThreads) k_applyPositionCorrections(Scene s)
 {
+    pdlEnter();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= s.N) return;
     const f3 c = xyz(s.posCorr[i]);
@@ -2142,6 +2189,7 @@ __device__ __forceinline__ void updateVelocityAt(const Scene &s, float dt, const
 
 __global__ void __launch_bounds__(kThreads) k_updateVelocities(Scene s, float dt, const float4 *Dfinal)
 {
+    pdlEnter();
     forEachElem(s.wP, s.N, [&](uint32_t i) { updateVelocityAt(s, dt, Dfinal, i); });
 }
 
@@ -2672,7 +2720,7 @@ void launchFluidGather(const Scene &s, uint32_t iter, cudaStream_t st)
     if (s.N == 0) return;
     const float4 *Dcur = (iter & 1u) ? s.Db : s.Da;
     float4 *second = iter == 0 ? (s.Pb ? s.Pb : s.P0) : nullptr;
-    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), s.Xs, Dcur, iter, second,
+    launchPdl(k_fluidGather, blocksFor(s.N), kThreads, st, withPositions(s, iter), s.Xs, Dcur, iter, second,
                                                        iter > 0 ? s.P0 : nullptr);
 }
 
@@ -2687,14 +2735,14 @@ void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter,
     float4 *Dk = (iter & 1u) ? s.Db : s.Da;
     const unsigned g = blocksFor(s.N);
     if (s.sup == nullptr || walkCells) {
-        if (s.fluidExtras) k_fluidNeighborsDensity<0u, true><<<g, kThreads, 0, st>>>(sp, c, true, iter, Dk);
-        else k_fluidNeighborsDensity<0u, false><<<g, kThreads, 0, st>>>(sp, c, true, iter, Dk);
+        if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<0u, true>, g, kThreads, st, sp, c, true, iter, Dk);
+        else launchPdl(k_fluidNeighborsDensity<0u, false>, g, kThreads, st, sp, c, true, iter, Dk);
     } else if (iter == 0) {
-        if (s.fluidExtras) k_fluidNeighborsDensity<1u, true><<<g, kThreads, 0, st>>>(sp, c, true, iter, Dk);
-        else k_fluidNeighborsDensity<1u, false><<<g, kThreads, 0, st>>>(sp, c, true, iter, Dk);
+        if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<1u, true>, g, kThreads, st, sp, c, true, iter, Dk);
+        else launchPdl(k_fluidNeighborsDensity<1u, false>, g, kThreads, st, sp, c, true, iter, Dk);
     } else {
-        if (s.fluidExtras) k_fluidNeighborsDensity<2u, true><<<g, kThreads, 0, st>>>(sp, c, true, iter, Dk);
-        else k_fluidNeighborsDensity<2u, false><<<g, kThreads, 0, st>>>(sp, c, true, iter, Dk);
+        if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<2u, true>, g, kThreads, st, sp, c, true, iter, Dk);
+        else launchPdl(k_fluidNeighborsDensity<2u, false>, g, kThreads, st, sp, c, true, iter, Dk);
     }
 }
 
@@ -2706,10 +2754,10 @@ void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const C
     float4 *Dnext = (iter & 1u) ? s.Da : s.Db;
     float4 *Pnext = s.Pb ? ((iter & 1u) ? s.P : s.Pb) : nullptr;
     if (s.fluidExtras)
-        k_fluidDeltaApplyClamp<true><<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), c, s.Xs, Dcur, Dnext,
+        launchPdl(k_fluidDeltaApplyClamp<true>, blocksFor(s.N), kThreads, st, withPositions(s, iter), c, s.Xs, Dcur, Dnext,
                                                                       iter, dt, writeDebug, Pnext);
     else
-        k_fluidDeltaApplyClamp<false><<<blocksFor(s.N), kThreads, 0, st>>>(withPositions(s, iter), c, s.Xs, Dcur, Dnext,
+        launchPdl(k_fluidDeltaApplyClamp<false>, blocksFor(s.N), kThreads, st, withPositions(s, iter), c, s.Xs, Dcur, Dnext,
                                                                        iter, dt, writeDebug, Pnext);
 }
 
@@ -2732,9 +2780,9 @@ void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)
 {
     if (s.N == 0) return;
     // Positions after the velocity update; the accumulated delta was folded into x.
-    k_fluidGather<<<blocksFor(s.N), kThreads, 0, st>>>(s, s.Xs, s.Da, 0u, nullptr, nullptr);
+    launchPdl(k_fluidGather, blocksFor(s.N), kThreads, st, s, s.Xs, s.Da, 0u, nullptr, nullptr);
     Config dummy{};
-    k_fluidNeighborsDensity<0u, false><<<blocksFor(s.N), kThreads, 0, st>>>(s, dummy, false, 0u, nullptr);
+    launchPdl(k_fluidNeighborsDensity<0u, false>, blocksFor(s.N), kThreads, st, s, dummy, false, 0u, nullptr);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -2836,18 +2884,21 @@ __device__ __forceinline__ void colourJacobiOrientAt(const Scene &s, uint32_t g)
 template <uint32_t kFam, bool kGaussSeidel>
 __global__ void __launch_bounds__(kThreads) k_colourSolve(Scene s, float dt, float relax, uint32_t begin, uint32_t end)
 {
+    pdlEnter();
     const uint32_t k = begin + blockIdx.x * blockDim.x + threadIdx.x;
     if (k < end) colourConstraint<kFam>(s, dt, relax, kGaussSeidel, s.colOrder[kFam][k]);
 }
 
 __global__ void __launch_bounds__(kThreads) k_colourJacobiApply(Scene s, uint2 win)
 {
+    pdlEnter();
     const uint32_t i = win.x + blockIdx.x * blockDim.x + threadIdx.x;
     if (i < win.y) colourJacobiApplyAt(s, i);
 }
 
 __global__ void __launch_bounds__(kThreads) k_colourJacobiOrient(Scene s)
 {
+    pdlEnter();
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g < s.S) colourJacobiOrientAt(s, g);
 }
@@ -2881,15 +2932,15 @@ void launchColourFamily(const Scene &s, float dt, float relax, const XpbdPlan &p
     for (uint32_t k = 0; k < plan.colours[kFam]; ++k) {
         const uint32_t b = starts[k], e = starts[k + 1];
         if (e <= b) continue;
-        if (gs) k_colourSolve<kFam, true><<<blocksFor(e - b), kThreads, 0, st>>>(s, dt, relax, b, e);
-        else k_colourSolve<kFam, false><<<blocksFor(e - b), kThreads, 0, st>>>(s, dt, relax, b, e);
+        if (gs) launchPdl(k_colourSolve<kFam, true>, blocksFor(e - b), kThreads, st, s, dt, relax, b, e);
+        else launchPdl(k_colourSolve<kFam, false>, blocksFor(e - b), kThreads, st, s, dt, relax, b, e);
     }
     if (gs) return;
     if (kFam == kFamJoints) {
-        k_colourJacobiOrient<<<blocksFor(s.S), kThreads, 0, st>>>(s);
+        launchPdl(k_colourJacobiOrient, blocksFor(s.S), kThreads, st, s);
     } else {
         const uint2 win = familyWindow(s, kFam);
-        if (win.y > win.x) k_colourJacobiApply<<<blocksFor(win.y - win.x), kThreads, 0, st>>>(s, win);
+        if (win.y > win.x) launchPdl(k_colourJacobiApply, blocksFor(win.y - win.x), kThreads, st, s, win);
     }
 }
 
@@ -3191,29 +3242,29 @@ void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t
 {
     const float relax = c.softInternalRelaxation;
     if (s.E) {
-        k_solveEdges<<<gridFor(s.wE, s.E), kThreads, 0, st>>>(s, dt, relax);
-        k_applyPair<<<applyGrid(s, s.edgeWin), kThreads, 0, st>>>(s, s.edgeRanges, s.edgeInc, s.edgeCorr, s.edgeWin);
+        launchPdl(k_solveEdges, gridFor(s.wE, s.E), kThreads, st, s, dt, relax);
+        launchPdl(k_applyPair, applyGrid(s, s.edgeWin), kThreads, st, s, s.edgeRanges, s.edgeInc, s.edgeCorr, s.edgeWin);
     }
     if (s.S) {
-        k_solveSegments<<<blocksFor(s.S), kThreads, 0, st>>>(s, dt, relax);
-        k_applySegments<<<blocksFor(s.N > s.S ? s.N : s.S), kThreads, 0, st>>>(s);
+        launchPdl(k_solveSegments, blocksFor(s.S), kThreads, st, s, dt, relax);
+        launchPdl(k_applySegments, blocksFor(s.N > s.S ? s.N : s.S), kThreads, st, s);
     }
     if (s.Bn || s.D) {
-        if (s.Bn) k_solveBends<<<blocksFor(s.Bn), kThreads, 0, st>>>(s, dt, relax);
-        if (s.D) k_solveDihedrals<<<blocksFor(s.D), kThreads, 0, st>>>(s, dt, relax);
-        k_applyQuad<<<applyGrid(s, s.bendWin), kThreads, 0, st>>>(s, s.bendRanges, s.bendInc, s.bendCorr, s.bendWin);
+        if (s.Bn) launchPdl(k_solveBends, blocksFor(s.Bn), kThreads, st, s, dt, relax);
+        if (s.D) launchPdl(k_solveDihedrals, blocksFor(s.D), kThreads, st, s, dt, relax);
+        launchPdl(k_applyQuad, applyGrid(s, s.bendWin), kThreads, st, s, s.bendRanges, s.bendInc, s.bendCorr, s.bendWin);
     }
     if (s.J) {
-        k_solveJoints<<<blocksFor(s.J), kThreads, 0, st>>>(s, dt, relax);
-        k_applyJoints<<<blocksFor(s.S), kThreads, 0, st>>>(s);
+        launchPdl(k_solveJoints, blocksFor(s.J), kThreads, st, s, dt, relax);
+        launchPdl(k_applyJoints, blocksFor(s.S), kThreads, st, s);
     }
     if (s.SD) {
-        k_solveDistances<<<blocksFor(s.SD), kThreads, 0, st>>>(s, dt, relax);
-        k_applyPair<<<applyGrid(s, s.segWin), kThreads, 0, st>>>(s, s.segRanges, s.segInc, s.distCorr, s.segWin);
+        launchPdl(k_solveDistances, blocksFor(s.SD), kThreads, st, s, dt, relax);
+        launchPdl(k_applyPair, applyGrid(s, s.segWin), kThreads, st, s, s.segRanges, s.segInc, s.distCorr, s.segWin);
     }
     if (s.T) {
-        k_solveTets<<<gridFor(s.wT, s.T), kThreads, 0, st>>>(s, dt, relax);
-        k_applyQuad<<<applyGrid(s, s.tetWin), kThreads, 0, st>>>(s, s.tetRanges, s.tetInc, s.tetCorr, s.tetWin);
+        launchPdl(k_solveTets, gridFor(s.wT, s.T), kThreads, st, s, dt, relax);
+        launchPdl(k_applyQuad, applyGrid(s, s.tetWin), kThreads, st, s, s.tetRanges, s.tetInc, s.tetCorr, s.tetWin);
     }
 }
 
@@ -3222,17 +3273,17 @@ void launchContacts(const Scene &s, const Config &c, bool particleContacts, bool
 {
     if (particleContacts) {
         const uint32_t cap = s.particlePairCapacity;
-        k_particleContactGenerate<<<pairGrid(cap), kThreads, 0, st>>>(s);
-        k_particleContactSolve<<<pairGrid(cap), kThreads, 0, st>>>(s, c);
+        launchPdl(k_particleContactGenerate, pairGrid(cap), kThreads, st, s);
+        launchPdl(k_particleContactSolve, pairGrid(cap), kThreads, st, s, c);
     }
-    if (rigidContacts) k_rigidContacts<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, c, !particleContacts);
-    if (particleContacts) k_applyPositionCorrections<<<blocksFor(s.N), kThreads, 0, st>>>(s);
+    if (rigidContacts) launchPdl(k_rigidContacts, gridFor(s.wP, s.N), kThreads, st, s, c, !particleContacts);
+    if (particleContacts) launchPdl(k_applyPositionCorrections, blocksFor(s.N), kThreads, st, s);
 }
 
 void launchUpdateVelocities(const Scene &s, float dt, const float4 *fluidDelta, cudaStream_t st)
 {
     if (s.N == 0) return;
-    k_updateVelocities<<<gridFor(s.wP, s.N), kThreads, 0, st>>>(s, dt, fluidDelta);
+    launchPdl(k_updateVelocities, gridFor(s.wP, s.N), kThreads, st, s, dt, fluidDelta);
 }
 
 void launchFluidBoundaryVelocities(const Scene &s, float dt, const Config &c, cudaStream_t st)

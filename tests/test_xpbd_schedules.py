@@ -276,3 +276,35 @@ def test_coloured_schedule_info_and_batch_rejection():
     from cn_physics import Batch, batch_desc
     with pytest.raises(CNError):
         Batch(batch_desc(desc, memory_budget_bytes=1 << 28))
+
+
+_PDL_SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+from cn_physics import Solver, scenes
+w, desc, dt = scenes.xpbd_cube(n=12, spacing=1.0 / 12)
+s = Solver(desc)
+s.sync_world(w.soa())
+for _ in range(3):
+    s.step(dt)
+x, v, _ = s.read_particles()
+np.save(sys.argv[2], np.concatenate([x, v]))
+"""
+
+
+@pytest.mark.gpu
+def test_programmatic_dependent_launch_changes_no_bits(tmp_path):
+    """The iteration kernels are launched with programmatic stream serialization (each waits for
+    its predecessor in pdlEnter); with CN_PDL=0 they launch plainly.  Same bits either way."""
+    import os
+    import subprocess
+    root = Path(__file__).resolve().parent.parent / "cressim-neo_b200"
+    script = tmp_path / "run.py"
+    script.write_text(_PDL_SCRIPT)
+    out = {}
+    for flag in ("1", "0"):
+        env = dict(os.environ, CN_PDL=flag)
+        dst = tmp_path / f"pdl{flag}.npy"
+        subprocess.run([sys.executable, str(script), str(root), str(dst)], env=env, check=True, timeout=600)
+        out[flag] = np.load(dst)
+    _bits(out["1"], out["0"], "pdl on / off")
