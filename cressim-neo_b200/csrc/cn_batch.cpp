@@ -111,8 +111,8 @@ inline float fromBits(uint32_t u)
 
 // Device bytes one element of each family takes in the pool (used for the budget accounting).
 constexpr uint64_t kBytesPerParticle = 3 * 16 + 6 * 4 + 16 + 2 * 8 + 2 * 4 + 8;
-constexpr uint64_t kBytesPerEdge = 32 + 4 + 2 * 16 + 2 * 8;
-constexpr uint64_t kBytesPerTet = 32 + 4 + 4 * 16 + 4 * 8;
+constexpr uint64_t kBytesPerEdge = 32 + 4 + 2 * 16 + 2 * 4;
+constexpr uint64_t kBytesPerTet = 32 + 4 + 4 * 16 + 4 * 4;
 constexpr uint64_t kBytesPerBody = 16 * 16 + 8 + 8;
 constexpr uint64_t kBytesPerCollider = 48 + 32 + 16 + 3 * 16 + 4 * 16 + 4 + 4;
 
@@ -244,8 +244,10 @@ void layoutPool(cn_batch *b, cn::Arena &a)
     s.E = E; s.T = T;
     s.edges = a.take<cn_soft_edge>(E);
     s.tets = a.take<cn_soft_tet>(T);
-    s.edgeRanges = a.take<uint2>(P); s.edgeInc = a.take<uint2>(size_t(E) * 2);
-    s.tetRanges = a.take<uint2>(P); s.tetInc = a.take<uint2>(size_t(T) * 4);
+    s.edgeRanges = a.take<uint2>(P);
+    s.tetRanges = a.take<uint2>(P);
+    s.edgeDst = a.take<uint32_t>(size_t(E) * 2);
+    s.tetDst = a.take<uint32_t>(size_t(T) * 4);
     s.edgeLambda = a.take<float>(E);
     s.tetLambda = a.take<float>(T);
     s.edgeCorr = a.take<float4>(size_t(E) * 2);
@@ -567,11 +569,15 @@ CN_API cn_status cn_batch_add_scene(cn_batch *b, const cn_world_soa *w, uint32_t
     const cn::Incidence tetI = cn::buildIncidence(N, w->tet_count, 4, [&](uint32_t c, uint32_t k) {
         return w->tets[c].particle_indices[k];
     });
-    std::vector<uint2> eRanges(edgeI.ranges), tRanges(tetI.ranges), eInc(edgeI.inc), tInc(tetI.inc);
+    std::vector<uint2> eRanges(edgeI.ranges), tRanges(tetI.ranges);
     for (auto &r : eRanges) r.x += sc.ei.start;
     for (auto &r : tRanges) r.x += sc.ti.start;
-    for (auto &r : eInc) r.x += e0;
-    for (auto &r : tInc) r.x += t0;
+    // gather slots, rebased with the scene's incidence ranges
+    std::vector<uint32_t> eDst(edgeI.dst), tDst(tetI.dst);
+    for (auto &d : eDst)
+        if (d != 0xffffffffu) d += sc.ei.start;
+    for (auto &d : tDst)
+        if (d != 0xffffffffu) d += sc.ti.start;
     std::vector<uint2> colRange(N, make_uint2(c0, c0 + sc.queryCount));
     std::vector<uint32_t> queryOrder(order);
     for (auto &q : queryOrder) q += c0;
@@ -607,8 +613,8 @@ CN_API cn_status cn_batch_add_scene(cn_batch *b, const cn_world_soa *w, uint32_t
     CN_CUDA(upTo(const_cast<uint2 *>(s.pColRange) + p0, colRange.data(), N, st));
     CN_CUDA(upTo(const_cast<cn_soft_edge *>(s.edges) + e0, edges.data(), edges.size(), st));
     CN_CUDA(upTo(const_cast<cn_soft_tet *>(s.tets) + t0, tets.data(), tets.size(), st));
-    CN_CUDA(upTo(const_cast<uint2 *>(s.edgeInc) + sc.ei.start, eInc.data(), eInc.size(), st));
-    CN_CUDA(upTo(const_cast<uint2 *>(s.tetInc) + sc.ti.start, tInc.data(), tInc.size(), st));
+    CN_CUDA(upTo(const_cast<uint32_t *>(s.edgeDst) + size_t(e0) * 2, eDst.data(), eDst.size(), st));
+    CN_CUDA(upTo(const_cast<uint32_t *>(s.tetDst) + size_t(t0) * 4, tDst.data(), tDst.size(), st));
     CN_CUDA(upTo(const_cast<float4 *>(s.contactMaterials) + m0, materials.data(), materials.size(), st));
     const uint32_t nb = w->rigid_body_count, nc = w->collider_count;
     CN_CUDA(upTo(s.bodyPos + b0, reinterpret_cast<const float4 *>(w->body_positions_inv_mass), nb, st));

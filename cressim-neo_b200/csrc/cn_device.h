@@ -118,24 +118,31 @@ struct Scene {
     const cn_strand_joint *joints = nullptr;
     const cn_strand_distance *dists = nullptr;
     float4 *segOrient = nullptr;
-    // incidence: per-particle (start, count) and (constraint, slot) records, ascending
-    // constraint order (physics_scene_gpu_state.cpp:3255-3420)
-    const uint2 *edgeRanges = nullptr, *edgeInc = nullptr;
-    const uint2 *bendRanges = nullptr, *bendInc = nullptr;
-    const uint2 *tetRanges = nullptr, *tetInc = nullptr;
+    // incidence: per-particle (start, count) of its entries in ascending constraint order
+    // (physics_scene_gpu_state.cpp:3255-3420); the (constraint, slot) lists themselves are kept
+    // for the strand segments and joints, whose applies read them
+    const uint2 *edgeRanges = nullptr;
+    const uint2 *bendRanges = nullptr;
+    const uint2 *tetRanges = nullptr;
     const uint2 *segRanges = nullptr, *segInc = nullptr;
     const uint2 *segJointRanges = nullptr, *segJointInc = nullptr;
+    // gather slots: for each constraint entry (edge 2, bend / dihedral 4, tet 4, strand distance 2)
+    // the index in its particle's incidence list, where the solve writes that entry's correction
+    // record (0xffffffff: no particle); the gathers read each particle's records contiguously.
+    // Strand distances use the strand-segment incidence (the reference applies distance c's
+    // records to segment c's particles).
+    const uint32_t *edgeDst = nullptr, *bendDst = nullptr, *tetDst = nullptr, *distDst = nullptr;
     // per family: the particles [x, y) with records (a single world's apply window)
     uint2 edgeWin{0u, 0u}, bendWin{0u, 0u}, tetWin{0u, 0u}, segWin{0u, 0u};
     // lambdas and per-constraint correction records
     float *edgeLambda = nullptr, *bendLambda = nullptr, *tetLambda = nullptr, *distLambda = nullptr;
     float4 *segLambda = nullptr, *jointLambda = nullptr;
-    float4 *edgeCorr = nullptr;   // 2 per edge
-    float4 *bendCorr = nullptr;   // 4 per bend / dihedral
-    float4 *tetCorr = nullptr;    // 4 per tet
+    float4 *edgeCorr = nullptr;   // per edge incidence entry (gather slot)
+    float4 *bendCorr = nullptr;   // per bend / dihedral incidence entry
+    float4 *tetCorr = nullptr;    // per tet incidence entry
     float4 *segCorr = nullptr;    // 3 per segment
     float4 *jointCorr = nullptr;  // 2 per joint (twistRotationA, twistRotationB)
-    float4 *distCorr = nullptr;   // 2 per distance
+    float4 *distCorr = nullptr;   // per strand-segment incidence entry
     float4 *posCorr = nullptr, *velCorr = nullptr;
     // coloured XPBD schedules: per family (kFam*) the constraint indices grouped by colour,
     // the colour-Jacobi per-particle sum of a family's corrections (zero between families) and

@@ -47,9 +47,12 @@ private:
 };
 
 // Per-particle incidence lists in ascending constraint order
-// (physics_scene_gpu_state.cpp:3273-3420): ranges[p] = (start, count), inc = (constraint, slot).
+// (physics_scene_gpu_state.cpp:3273-3420): ranges[p] = (start, count), inc = (constraint, slot);
+// dst[c * perConstraint + k] = the position of (c, k) in inc (0xffffffff when entry k names no
+// particle), the gather slot of that entry's correction record.
 struct Incidence {
     std::vector<uint2> ranges, inc;
+    std::vector<uint32_t> dst;
 };
 template <class F> Incidence buildIncidence(uint32_t n, uint32_t constraints, uint32_t perConstraint, F &&particlesOf)
 {
@@ -67,11 +70,15 @@ template <class F> Incidence buildIncidence(uint32_t n, uint32_t constraints, ui
         run += counts[i];
     }
     out.inc.resize(run);
+    out.dst.assign(size_t(constraints) * perConstraint, 0xffffffffu);
     std::vector<uint32_t> fill(n, 0);
     for (uint32_t c = 0; c < constraints; ++c)
         for (uint32_t k = 0; k < perConstraint; ++k) {
             const uint32_t p = particlesOf(c, k);
-            if (p < n) out.inc[out.ranges[p].x + fill[p]++] = make_uint2(c, k);
+            if (p >= n) continue;
+            const uint32_t at = out.ranges[p].x + fill[p]++;
+            out.inc[at] = make_uint2(c, k);
+            out.dst[size_t(c) * perConstraint + k] = at;
         }
     return out;
 }

@@ -1318,6 +1318,18 @@ __global__ void __launch_bounds__(kThreads) k_fluidVorticityApply(Scene s, float
 // XPBD families: Jacobi solve writes per-constraint records, apply gathers them per particle in
 // ascending constraint order (the reference's incidence order).
 // ------------------------------------------------------------------------------------------
+// A constraint's correction record for one of its particles goes to that particle's gather slot
+// (kNoSlot: the entry names no particle, e.g. slot 3 of a 3-point bend).
+constexpr uint32_t kNoSlot = 0xffffffffu;
+__device__ __forceinline__ void putRecord(float4 *corr, uint32_t slot, float4 v)
+{
+    if (slot != kNoSlot) corr[slot] = v;
+}
+__device__ __forceinline__ float4 recordAt(const float4 *corr, uint32_t slot)
+{
+    return slot != kNoSlot ? corr[slot] : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
 // physics_soft_solve_edge_constraints.cs.hlsl:10-74
 __device__ __forceinline__ void solveEdge(const Scene &s, float dt, float relax, uint32_t e)
 {
@@ -1344,8 +1356,9 @@ __device__ __forceinline__ void solveEdge(const Scene &s, float dt, float relax,
             }
         }
     }
-    s.edgeCorr[2 * e] = cA;
-    s.edgeCorr[2 * e + 1] = cB;
+    const uint2 d = reinterpret_cast<const uint2 *>(s.edgeDst)[e];
+    putRecord(s.edgeCorr, d.x, cA);
+    putRecord(s.edgeCorr, d.y, cB);
 }
 
 __global__ void __launch_bounds__(kThreads) k_solveEdges(Scene s, float dt, float relax)
@@ -1354,35 +1367,23 @@ __global__ void __launch_bounds__(kThreads) k_solveEdges(Scene s, float dt, floa
     forEachElem(s.wE, s.E, [&](uint32_t e) { solveEdge(s, dt, relax, e); });
 }
 
-// Gather of per-constraint correction records in incidence (constraint) order.  The range is
-// loaded together with the position, not after the mass test, and the records are fetched
-// kGatherBatch at a time (all incidence loads, then all record loads) before they are summed in
-// list order: the sum is the one-at-a-time sum, with three memory round trips per batch fewer.
+// Gather of the correction records: each particle's records sit contiguously at its incidence
+// range, in ascending constraint order (the solves write each record to its gather slot), and are
+// fetched kGatherBatch at a time before they are summed in list order -- the one-at-a-time sum,
+// with the range and the records as the only dependent loads.
 constexpr uint32_t kGatherBatch = 8u;
 
-template <uint32_t kRecords>
-__device__ __forceinline__ void applyGatherAt(const Scene &s, const uint2 *ranges, const uint2 *inc,
-                                              const float4 *corr, uint32_t i)
+__device__ __forceinline__ void applyGatherAt(const Scene &s, const uint2 *ranges, const float4 *corr, uint32_t i)
 {
     const float4 p = s.x[i];
     const uint2 r = ranges[i];
     if (p.w <= kEps) return;
     f3 total{0.f, 0.f, 0.f};
     for (uint32_t k = 0; k < r.y; k += kGatherBatch) {
-        uint32_t slot[kGatherBatch];
-#pragma unroll
-        for (uint32_t j = 0; j < kGatherBatch; ++j) {
-            slot[j] = 0u;
-            if (k + j < r.y) {
-                const uint2 ref = inc[r.x + k + j];
-                slot[j] = kRecords == 2u ? 2u * ref.x + (ref.y == 0u ? 0u : 1u)
-                                         : 4u * ref.x + (ref.y > 3u ? 3u : ref.y);
-            }
-        }
         float4 c[kGatherBatch];
 #pragma unroll
         for (uint32_t j = 0; j < kGatherBatch; ++j)
-            if (k + j < r.y) c[j] = corr[slot[j]];
+            if (k + j < r.y) c[j] = corr[r.x + k + j];
 #pragma unroll
         for (uint32_t j = 0; j < kGatherBatch; ++j)
             if (k + j < r.y) total += xyz(c[j]);
@@ -1390,43 +1391,19 @@ __device__ __forceinline__ void applyGatherAt(const Scene &s, const uint2 *range
     s.x[i] = mk4(xyz(p) + total, p.w);
 }
 
-// physics_soft_apply_edge_corrections.cs.hlsl:9-35 (also the strand distance apply:
-// physics_strand_apply_distance_corrections.cs.hlsl:9-38)
-__device__ __forceinline__ void applyPairAt(const Scene &s, const uint2 *ranges, const uint2 *inc, const float4 *corr, uint32_t i)
-{
-    applyGatherAt<2u>(s, ranges, inc, corr, i);
-}
-
+// physics_soft_apply_edge_corrections.cs.hlsl:9-35, physics_soft_apply_tet_corrections.cs.hlsl:9-50,
+// physics_soft_apply_bend_corrections.cs.hlsl:9-51, physics_strand_apply_distance_corrections.cs.hlsl:9-38.
 // A single world applies over `win`, the particles [lo, hi) that the family touches (bodies are
 // contiguous in the particle order; the others have no records and keep x); a batch over its tiles.
-__global__ void __launch_bounds__(kThreads) k_applyPair(Scene s, const uint2 *ranges, const uint2 *inc,
-                                                        const float4 *corr, uint2 win)
+__global__ void __launch_bounds__(kThreads) k_applyGather(Scene s, const uint2 *ranges, const float4 *corr, uint2 win)
 {
     pdlEnter();
     if (s.wP.tiles) {
-        forEachElem(s.wP, s.N, [&](uint32_t i) { applyPairAt(s, ranges, inc, corr, i); });
+        forEachElem(s.wP, s.N, [&](uint32_t i) { applyGatherAt(s, ranges, corr, i); });
         return;
     }
     const uint32_t i = win.x + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < win.y) applyPairAt(s, ranges, inc, corr, i);
-}
-
-// physics_soft_apply_tet_corrections.cs.hlsl:9-50, physics_soft_apply_bend_corrections.cs.hlsl:9-51
-__device__ __forceinline__ void applyQuadAt(const Scene &s, const uint2 *ranges, const uint2 *inc, const float4 *corr, uint32_t i)
-{
-    applyGatherAt<4u>(s, ranges, inc, corr, i);
-}
-
-__global__ void __launch_bounds__(kThreads) k_applyQuad(Scene s, const uint2 *ranges, const uint2 *inc,
-                                                        const float4 *corr, uint2 win)
-{
-    pdlEnter();
-    if (s.wP.tiles) {
-        forEachElem(s.wP, s.N, [&](uint32_t i) { applyQuadAt(s, ranges, inc, corr, i); });
-        return;
-    }
-    const uint32_t i = win.x + blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < win.y) applyQuadAt(s, ranges, inc, corr, i);
+    if (i < win.y) applyGatherAt(s, ranges, corr, i);
 }
 
 // physics_soft_solve_tet_constraints.cs.hlsl:15-87
@@ -1452,11 +1429,11 @@ __device__ __forceinline__ void solveTet(const Scene &s, float dt, float relax, 
     if (den <= kEps) return;
     const float dl = -(Cv + alpha * lambda) / den;
     s.tetLambda[t] = lambda + dl;
-    float4 *out = s.tetCorr + 4 * size_t(t);
-    out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
-    out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
-    out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
-    out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
+    const uint4 d = reinterpret_cast<const uint4 *>(s.tetDst)[t];
+    putRecord(s.tetCorr, d.x, mk4(w0 * dl * g0 * relax, 0.0f));
+    putRecord(s.tetCorr, d.y, mk4(w1 * dl * g1 * relax, 0.0f));
+    putRecord(s.tetCorr, d.z, mk4(w2 * dl * g2 * relax, 0.0f));
+    putRecord(s.tetCorr, d.w, mk4(w3 * dl * g3 * relax, 0.0f));
 }
 
 __global__ void __launch_bounds__(kThreads) k_solveTets(Scene s, float dt, float relax)
@@ -1469,7 +1446,6 @@ __global__ void __launch_bounds__(kThreads) k_solveTets(Scene s, float dt, float
 __device__ __forceinline__ void solveBendAt(const Scene &s, float dt, float relax, uint32_t b)
 {
     const cn_soft_bend bd = s.bends[b];
-    float4 *out = s.bendCorr + 4 * size_t(b);
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     float4 o0 = z, o1 = z, o2 = z;
     const float4 q0 = s.x[bd.particle0], q1 = s.x[bd.particle1], q2 = s.x[bd.particle2];
@@ -1498,7 +1474,11 @@ __device__ __forceinline__ void solveBendAt(const Scene &s, float dt, float rela
             o2 = mk4(w2 * dl * g2 * relax, 0.0f);
         }
     }
-    out[0] = o0; out[1] = o1; out[2] = o2; out[3] = z;
+    const uint4 d = reinterpret_cast<const uint4 *>(s.bendDst)[b];
+    putRecord(s.bendCorr, d.x, o0);
+    putRecord(s.bendCorr, d.y, o1);
+    putRecord(s.bendCorr, d.z, o2);
+    putRecord(s.bendCorr, d.w, z);
 }
 
 __global__ void __launch_bounds__(kThreads) k_solveBends(Scene s, float dt, float relax)
@@ -1513,7 +1493,13 @@ __device__ __forceinline__ void solveDihedralAt(const Scene &s, float dt, float 
 {
     const uint32_t ci = s.Bn + d;
     const cn_cloth_dihedral h = s.dihedrals[d];
-    float4 *out = s.bendCorr + 4 * size_t(ci);
+    const uint4 dst = reinterpret_cast<const uint4 *>(s.bendDst)[ci];
+    auto put4 = [&](float4 a, float4 b, float4 c, float4 e) {
+        putRecord(s.bendCorr, dst.x, a);
+        putRecord(s.bendCorr, dst.y, b);
+        putRecord(s.bendCorr, dst.z, c);
+        putRecord(s.bendCorr, dst.w, e);
+    };
     const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 e0m = s.x[h.edge_particle0], e1m = s.x[h.edge_particle1];
     const float4 o0m = s.x[h.opposite_particle0], o1m = s.x[h.opposite_particle1];
@@ -1524,7 +1510,7 @@ __device__ __forceinline__ void solveDihedralAt(const Scene &s, float dt, float 
     const f3 rn1 = cross(p3 - p1, p2 - p1);
     const float n0s = dot(rn0, rn0), n1s = dot(rn1, rn1);
     if (el2 <= kEps || n0s <= kEps || n1s <= kEps) {
-        out[0] = z; out[1] = z; out[2] = z; out[3] = z;
+        put4(z, z, z, z);
         return;
     }
     const float el = sqrtf(el2);
@@ -1543,16 +1529,14 @@ __device__ __forceinline__ void solveDihedralAt(const Scene &s, float dt, float 
     const float den = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
     const float alpha = mx(h.compliance, 0.0f) / mx(dt * dt, kEps);
     if (den + alpha <= kEps) {
-        out[0] = z; out[1] = z; out[2] = z; out[3] = z;
+        put4(z, z, z, z);
         return;
     }
     const float lambda = s.bendLambda[ci];
     const float dl = -(Cv + alpha * lambda) / (den + alpha);
     s.bendLambda[ci] = lambda + dl;
-    out[0] = mk4(w0 * dl * g0 * relax, 0.0f);
-    out[1] = mk4(w1 * dl * g1 * relax, 0.0f);
-    out[2] = mk4(w2 * dl * g2 * relax, 0.0f);
-    out[3] = mk4(w3 * dl * g3 * relax, 0.0f);
+    put4(mk4(w0 * dl * g0 * relax, 0.0f), mk4(w1 * dl * g1 * relax, 0.0f), mk4(w2 * dl * g2 * relax, 0.0f),
+         mk4(w3 * dl * g3 * relax, 0.0f));
 }
 
 __global__ void __launch_bounds__(kThreads) k_solveDihedrals(Scene s, float dt, float relax)
@@ -1761,8 +1745,9 @@ __device__ __forceinline__ void solveDistanceAt(const Scene &s, float dt, float 
             cB = mk4(wB * dl * grad * relax, 0.0f);
         }
     }
-    s.distCorr[2 * c] = cA;
-    s.distCorr[2 * c + 1] = cB;
+    const uint2 d = reinterpret_cast<const uint2 *>(s.distDst)[c];
+    putRecord(s.distCorr, d.x, cA);
+    putRecord(s.distCorr, d.y, cB);
 }
 
 __global__ void __launch_bounds__(kThreads) k_solveDistances(Scene s, float dt, float relax)
@@ -2818,8 +2803,9 @@ __device__ __forceinline__ void colourConstraint(const Scene &s, float dt, float
     if constexpr (kFam == kFamEdges) {
         solveEdge(s, dt, relax, c);
         const cn_soft_edge ed = s.edges[c];
-        moveRecord(s, gaussSeidel, ed.particle_a, s.edgeCorr[2 * size_t(c)]);
-        moveRecord(s, gaussSeidel, ed.particle_b, s.edgeCorr[2 * size_t(c) + 1]);
+        const uint2 d = reinterpret_cast<const uint2 *>(s.edgeDst)[c];
+        moveRecord(s, gaussSeidel, ed.particle_a, recordAt(s.edgeCorr, d.x));
+        moveRecord(s, gaussSeidel, ed.particle_b, recordAt(s.edgeCorr, d.y));
     } else if constexpr (kFam == kFamSegments) {
         // a segment's orientation is read by its own constraint alone: applied in place
         solveSegmentAt(s, dt, relax, c);
@@ -2828,20 +2814,20 @@ __device__ __forceinline__ void colourConstraint(const Scene &s, float dt, float
         moveRecord(s, gaussSeidel, sg.particle_b, s.segCorr[3 * size_t(c) + 1]);
         s.segOrient[c] = qNormalize(add4(s.segOrient[c], s.segCorr[3 * size_t(c) + 2]));
     } else if constexpr (kFam == kFamBends) {
-        const float4 *r = s.bendCorr + 4 * size_t(c);
+        const uint4 d = reinterpret_cast<const uint4 *>(s.bendDst)[c];
         if (c < s.Bn) {
             solveBendAt(s, dt, relax, c);
             const cn_soft_bend b = s.bends[c];
-            moveRecord(s, gaussSeidel, b.particle0, r[0]);
-            moveRecord(s, gaussSeidel, b.particle1, r[1]);
-            moveRecord(s, gaussSeidel, b.particle2, r[2]);
+            moveRecord(s, gaussSeidel, b.particle0, recordAt(s.bendCorr, d.x));
+            moveRecord(s, gaussSeidel, b.particle1, recordAt(s.bendCorr, d.y));
+            moveRecord(s, gaussSeidel, b.particle2, recordAt(s.bendCorr, d.z));
         } else {
             solveDihedralAt(s, dt, relax, c - s.Bn);
             const cn_cloth_dihedral h = s.dihedrals[c - s.Bn];
-            moveRecord(s, gaussSeidel, h.edge_particle0, r[0]);
-            moveRecord(s, gaussSeidel, h.edge_particle1, r[1]);
-            moveRecord(s, gaussSeidel, h.opposite_particle0, r[2]);
-            moveRecord(s, gaussSeidel, h.opposite_particle1, r[3]);
+            moveRecord(s, gaussSeidel, h.edge_particle0, recordAt(s.bendCorr, d.x));
+            moveRecord(s, gaussSeidel, h.edge_particle1, recordAt(s.bendCorr, d.y));
+            moveRecord(s, gaussSeidel, h.opposite_particle0, recordAt(s.bendCorr, d.z));
+            moveRecord(s, gaussSeidel, h.opposite_particle1, recordAt(s.bendCorr, d.w));
         }
     } else if constexpr (kFam == kFamJoints) {
         solveJointAt(s, dt, relax, c);
@@ -2851,16 +2837,17 @@ __device__ __forceinline__ void colourConstraint(const Scene &s, float dt, float
     } else if constexpr (kFam == kFamDistances) {
         solveDistanceAt(s, dt, relax, c);
         const cn_strand_distance dc = s.dists[c];
-        moveRecord(s, gaussSeidel, dc.particle_a, s.distCorr[2 * size_t(c)]);
-        moveRecord(s, gaussSeidel, dc.particle_b, s.distCorr[2 * size_t(c) + 1]);
+        const uint2 d = reinterpret_cast<const uint2 *>(s.distDst)[c];
+        moveRecord(s, gaussSeidel, dc.particle_a, recordAt(s.distCorr, d.x));
+        moveRecord(s, gaussSeidel, dc.particle_b, recordAt(s.distCorr, d.y));
     } else {
         solveTet(s, dt, relax, c);
         const cn_soft_tet t = s.tets[c];
-        const float4 *r = s.tetCorr + 4 * size_t(c);
-        moveRecord(s, gaussSeidel, t.particle_indices[0], r[0]);
-        moveRecord(s, gaussSeidel, t.particle_indices[1], r[1]);
-        moveRecord(s, gaussSeidel, t.particle_indices[2], r[2]);
-        moveRecord(s, gaussSeidel, t.particle_indices[3], r[3]);
+        const uint4 d = reinterpret_cast<const uint4 *>(s.tetDst)[c];
+        moveRecord(s, gaussSeidel, t.particle_indices[0], recordAt(s.tetCorr, d.x));
+        moveRecord(s, gaussSeidel, t.particle_indices[1], recordAt(s.tetCorr, d.y));
+        moveRecord(s, gaussSeidel, t.particle_indices[2], recordAt(s.tetCorr, d.z));
+        moveRecord(s, gaussSeidel, t.particle_indices[3], recordAt(s.tetCorr, d.w));
     }
 }
 
@@ -2983,21 +2970,21 @@ __device__ __forceinline__ void fusedFamily(const Scene &s, float dt, float rela
         cg::this_cluster().sync();
         if constexpr (kFam == kFamEdges) {
             for (uint32_t i = s.edgeWin.x + tid; i < s.edgeWin.y; i += nth)
-                applyPairAt(s, s.edgeRanges, s.edgeInc, s.edgeCorr, i);
+                applyGatherAt(s, s.edgeRanges, s.edgeCorr, i);
         } else if constexpr (kFam == kFamSegments) {
             const uint32_t m = s.N > s.S ? s.N : s.S;
             for (uint32_t i = tid; i < m; i += nth) applySegmentsAt(s, i);
         } else if constexpr (kFam == kFamBends) {
             for (uint32_t i = s.bendWin.x + tid; i < s.bendWin.y; i += nth)
-                applyQuadAt(s, s.bendRanges, s.bendInc, s.bendCorr, i);
+                applyGatherAt(s, s.bendRanges, s.bendCorr, i);
         } else if constexpr (kFam == kFamJoints) {
             for (uint32_t g = tid; g < s.S; g += nth) applyJointsAt(s, g);
         } else if constexpr (kFam == kFamDistances) {
             for (uint32_t i = s.segWin.x + tid; i < s.segWin.y; i += nth)
-                applyPairAt(s, s.segRanges, s.segInc, s.distCorr, i);
+                applyGatherAt(s, s.segRanges, s.distCorr, i);
         } else {
             for (uint32_t i = s.tetWin.x + tid; i < s.tetWin.y; i += nth)
-                applyQuadAt(s, s.tetRanges, s.tetInc, s.tetCorr, i);
+                applyGatherAt(s, s.tetRanges, s.tetCorr, i);
         }
         cg::this_cluster().sync();
     } else {
@@ -3077,13 +3064,13 @@ __global__ void __launch_bounds__(kBatchFusedThreads, 2) k_batchFusedIterations(
                 if (s.E) {
                     for (uint32_t e = er.x + tid; e < er.y; e += nth) solveEdge(s, dt, relax, e);
                     cl.sync();
-                    for (uint32_t i = pr.x + tid; i < pr.y; i += nth) applyPairAt(s, s.edgeRanges, s.edgeInc, s.edgeCorr, i);
+                    for (uint32_t i = pr.x + tid; i < pr.y; i += nth) applyGatherAt(s, s.edgeRanges, s.edgeCorr, i);
                     cl.sync();
                 }
                 if (s.T) {
                     for (uint32_t t = tr.x + tid; t < tr.y; t += nth) solveTet(s, dt, relax, t);
                     cl.sync();
-                    for (uint32_t i = pr.x + tid; i < pr.y; i += nth) applyQuadAt(s, s.tetRanges, s.tetInc, s.tetCorr, i);
+                    for (uint32_t i = pr.x + tid; i < pr.y; i += nth) applyGatherAt(s, s.tetRanges, s.tetCorr, i);
                     cl.sync();
                 }
             }
@@ -3243,7 +3230,7 @@ void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t
     const float relax = c.softInternalRelaxation;
     if (s.E) {
         launchPdl(k_solveEdges, gridFor(s.wE, s.E), kThreads, st, s, dt, relax);
-        launchPdl(k_applyPair, applyGrid(s, s.edgeWin), kThreads, st, s, s.edgeRanges, s.edgeInc, s.edgeCorr, s.edgeWin);
+        launchPdl(k_applyGather, applyGrid(s, s.edgeWin), kThreads, st, s, s.edgeRanges, s.edgeCorr, s.edgeWin);
     }
     if (s.S) {
         launchPdl(k_solveSegments, blocksFor(s.S), kThreads, st, s, dt, relax);
@@ -3252,7 +3239,7 @@ void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t
     if (s.Bn || s.D) {
         if (s.Bn) launchPdl(k_solveBends, blocksFor(s.Bn), kThreads, st, s, dt, relax);
         if (s.D) launchPdl(k_solveDihedrals, blocksFor(s.D), kThreads, st, s, dt, relax);
-        launchPdl(k_applyQuad, applyGrid(s, s.bendWin), kThreads, st, s, s.bendRanges, s.bendInc, s.bendCorr, s.bendWin);
+        launchPdl(k_applyGather, applyGrid(s, s.bendWin), kThreads, st, s, s.bendRanges, s.bendCorr, s.bendWin);
     }
     if (s.J) {
         launchPdl(k_solveJoints, blocksFor(s.J), kThreads, st, s, dt, relax);
@@ -3260,11 +3247,11 @@ void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t
     }
     if (s.SD) {
         launchPdl(k_solveDistances, blocksFor(s.SD), kThreads, st, s, dt, relax);
-        launchPdl(k_applyPair, applyGrid(s, s.segWin), kThreads, st, s, s.segRanges, s.segInc, s.distCorr, s.segWin);
+        launchPdl(k_applyGather, applyGrid(s, s.segWin), kThreads, st, s, s.segRanges, s.distCorr, s.segWin);
     }
     if (s.T) {
         launchPdl(k_solveTets, gridFor(s.wT, s.T), kThreads, st, s, dt, relax);
-        launchPdl(k_applyQuad, applyGrid(s, s.tetWin), kThreads, st, s, s.tetRanges, s.tetInc, s.tetCorr, s.tetWin);
+        launchPdl(k_applyGather, applyGrid(s, s.tetWin), kThreads, st, s, s.tetRanges, s.tetCorr, s.tetWin);
     }
 }
 

@@ -160,11 +160,15 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
     s.joints = a.take<cn_strand_joint>(s.J);
     s.dists = a.take<cn_strand_distance>(s.SD);
     s.segOrient = a.take<float4>(s.S);
-    s.edgeRanges = a.take<uint2>(N); s.edgeInc = a.take<uint2>(edgeI.inc.size());
-    s.bendRanges = a.take<uint2>(N); s.bendInc = a.take<uint2>(bendI.inc.size());
-    s.tetRanges = a.take<uint2>(N); s.tetInc = a.take<uint2>(tetI.inc.size());
+    s.edgeRanges = a.take<uint2>(N);
+    s.bendRanges = a.take<uint2>(N);
+    s.tetRanges = a.take<uint2>(N);
     s.segRanges = a.take<uint2>(N); s.segInc = a.take<uint2>(segI.inc.size());
     s.segJointRanges = a.take<uint2>(s.S); s.segJointInc = a.take<uint2>(jointI.inc.size());
+    s.edgeDst = a.take<uint32_t>(size_t(s.E) * 2);
+    s.bendDst = a.take<uint32_t>(size_t(s.Bn + s.D) * 4);
+    s.tetDst = a.take<uint32_t>(size_t(s.T) * 4);
+    s.distDst = a.take<uint32_t>(size_t(s.SD) * 2);
     s.edgeLambda = a.take<float>(s.E);
     s.bendLambda = a.take<float>(s.Bn + s.D);
     s.tetLambda = a.take<float>(s.T);
@@ -176,7 +180,9 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
     s.tetCorr = a.take<float4>(size_t(s.T) * 4);
     s.segCorr = a.take<float4>(size_t(s.S) * 3);
     s.jointCorr = a.take<float4>(size_t(s.J) * 2);
-    s.distCorr = a.take<float4>(size_t(s.SD) * 2);
+    // the distance gather walks every strand-segment incidence entry: slots of segments without a
+    // distance constraint stay zero
+    s.distCorr = a.take<float4>(s.SD ? std::max<size_t>(size_t(s.SD) * 2, segI.inc.size()) : 0);
     s.posCorr = a.take<float4>(N);
     s.velCorr = a.take<float4>(N);
     for (uint32_t f = 0; f < cn::kFamilies; ++f) {
@@ -878,15 +884,24 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     s.tetWin = window(tetI);
     s.segWin = window(segI);
     CN_CUDA(up(s.edgeRanges, edgeI.ranges.data(), edgeI.ranges.size(), st));
-    CN_CUDA(up(s.edgeInc, edgeI.inc.data(), edgeI.inc.size(), st));
     CN_CUDA(up(s.bendRanges, bendI.ranges.data(), bendI.ranges.size(), st));
-    CN_CUDA(up(s.bendInc, bendI.inc.data(), bendI.inc.size(), st));
     CN_CUDA(up(s.tetRanges, tetI.ranges.data(), tetI.ranges.size(), st));
-    CN_CUDA(up(s.tetInc, tetI.inc.data(), tetI.inc.size(), st));
     CN_CUDA(up(s.segRanges, segI.ranges.data(), segI.ranges.size(), st));
     CN_CUDA(up(s.segInc, segI.inc.data(), segI.inc.size(), st));
     CN_CUDA(up(s.segJointRanges, jointI.ranges.data(), jointI.ranges.size(), st));
     CN_CUDA(up(s.segJointInc, jointI.inc.data(), jointI.inc.size(), st));
+    CN_CUDA(up(const_cast<uint32_t *>(s.edgeDst), edgeI.dst.data(), edgeI.dst.size(), st));
+    CN_CUDA(up(const_cast<uint32_t *>(s.bendDst), bendI.dst.data(), bendI.dst.size(), st));
+    CN_CUDA(up(const_cast<uint32_t *>(s.tetDst), tetI.dst.data(), tetI.dst.size(), st));
+    {
+        // strand distance c's records go to segment c's gather slots (none past the segments)
+        std::vector<uint32_t> distDst(size_t(s.SD) * 2, 0xffffffffu);
+        for (uint32_t c = 0; c < std::min(s.SD, s.S); ++c) {
+            distDst[2 * size_t(c)] = segI.dst[2 * size_t(c)];
+            distDst[2 * size_t(c) + 1] = segI.dst[2 * size_t(c) + 1];
+        }
+        CN_CUDA(up(const_cast<uint32_t *>(s.distDst), distDst.data(), distDst.size(), st));
+    }
     for (uint32_t f = 0; f < cn::kFamilies; ++f) {
         const cn::Colouring &col = sv->colouring[f];
         if (!col.colours()) continue;

@@ -122,11 +122,11 @@ def test_autotune_keeps_state_and_results():
 def test_server_results_equal_alone_and_in_the_mix_with_evictions():
     pool = small_pool(6)
     # a budget that holds two or three of the six scenes: admissions must evict idle scenes
-    # (the batch charges 120 + 4 x 72 B per particle, 84 B per edge, 132 B per tet, 272 B per
+    # (the batch charges 120 + 4 x 72 B per particle, 76 B per edge, 116 B per tet, 272 B per
     # body and 216 B per collider)
     def scene_bytes(sc):
         c = sc.world.counts()
-        return c["particles"] * (120 + 288) + c["edges"] * 84 + c["tets"] * 132 + 2 * 272 + 2 * 216
+        return c["particles"] * (120 + 288) + c["edges"] * 76 + c["tets"] * 116 + 2 * 272 + 2 * 216
     largest = max(scene_bytes(sc) for sc in pool)
     b = Batch(batch_desc(serving.serving_solver_desc(), memory_budget_bytes=int(2.5 * largest),
                          particle_capacity=20000))
