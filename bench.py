@@ -83,6 +83,7 @@ class ClockSampler:
     FIELDS = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    MEM_FIELDS = ",clocks.mem,clocks.max.mem"
 
     def __init__(self, uuid: str | None):
         self.uuid = uuid
@@ -90,8 +91,16 @@ class ClockSampler:
         self.lines: list[str] = []
 
     def start(self):
+        fields = self.FIELDS
+        try:  # the memory clock too, where this nvidia-smi knows the fields
+            probe = subprocess.run(["nvidia-smi", f"--query-gpu={fields}{self.MEM_FIELDS}", "--format=csv,noheader,nounits"],
+                                   capture_output=True, text=True, timeout=20)
+            if probe.returncode == 0:
+                fields += self.MEM_FIELDS
+        except (FileNotFoundError, subprocess.TimeoutExpired):
+            pass
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={fields}", "--format=csv,noheader,nounits",
                                           "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except FileNotFoundError:
             self.proc = None
@@ -111,7 +120,7 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        sm, smax, reasons = [], [], set()
+        sm, smax, mem, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.lines:
             parts = [p.strip() for p in line.split(",")]
@@ -124,11 +133,15 @@ class ClockSampler:
                 smax.append(float(parts[2]))
             except ValueError:
                 continue
+            try:
+                mem.append(float(parts[9]))
+            except (ValueError, IndexError):
+                pass
             for name, flag in zip(names, parts[5:9]):
                 if flag.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "mem_mhz": statistics.median(mem) if mem else None, "reasons": sorted(reasons), "samples": len(sm)}
 
 
 def peaks():

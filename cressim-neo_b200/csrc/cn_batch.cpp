@@ -311,8 +311,9 @@ void enqueueTick(cn_batch *b, float frameDt, cudaStream_t st)
             const bool runSoft = (s.E || s.T) && it < b->softIt;
             const bool runRigid = it < b->contactIt;
             if (!runSoft && !runRigid) break;
-            if (runSoft) cn::launchSoftIteration(s, dt, c, st);
-            if (runRigid) cn::launchContacts(s, c, false, true, st);
+            // the rigid contacts run in the tet gather's pass when there is a tet family
+            const bool contactsDone = runSoft && cn::launchSoftIteration(s, dt, c, st, runRigid);
+            if (runRigid && !contactsDone) cn::launchContacts(s, c, false, true, st);
         }
         cn::launchUpdateVelocities(s, dt, nullptr, st);
         if (b->contactIt) cn::launchRigidContactVelocities(s, b->contactIt, c, st);

@@ -48,7 +48,7 @@ struct DeviceMeta {
     uint32_t rigidContactSlots;       // kRigidPairContacts x rigidRigidPairCount + proxy contact slots
     uint32_t proxyContactSlots;       // min(required, capacity) proxy particle -> body contact slots
     uint32_t requiredProxyContacts;   // proxy candidates (GpuProxyRigidContactMeta.requiredContactCount)
-    uint32_t reserved[1];
+    uint32_t activeParticleContactsLast; // activeParticleContacts of the last completed contact pass
 };
 
 // Rigid-rigid contact point of a collider pair (GpuRigidContact, physics_rigid_types.hlsli):
@@ -374,7 +374,11 @@ void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const C
 void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st);
 // Vorticity confinement (after launchFluidNeighborsOnly's post-update lists): curl, then force.
 void launchFluidVorticity(const Scene &s, float dt, cudaStream_t st);
-void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st);
+// One iteration of the soft families (gather schedule).  With `rigidContacts` (an iteration whose
+// particle-rigid contacts follow the soft families directly: no particle-particle contacts) and
+// a tet family, those contacts run in the tet gather's pass; returns true when they did, and the
+// caller launches them itself otherwise.
+bool launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st, bool rigidContacts = false);
 // The XPBD schedule of a solver: CN_XPBD_* and, for the coloured schedules, each family's colour
 // count and colour start offsets into Scene::colOrder (host copies for the per-colour launches,
 // device copies for the fused kernel).
@@ -384,7 +388,8 @@ struct XpbdPlan {
     const uint32_t *hostStarts[kFamilies] = {};
     const uint32_t *devStarts[kFamilies] = {};
 };
-void launchSoftIteration(const Scene &s, float dt, const Config &c, const XpbdPlan &plan, cudaStream_t st);
+bool launchSoftIteration(const Scene &s, float dt, const Config &c, const XpbdPlan &plan, cudaStream_t st,
+                         bool rigidContacts = false);
 // Fused iterations: one thread-block cluster runs every iteration of a substep (soft families in
 // `plan`'s schedule, then the particle-rigid contacts when `rigid`), phases separated by cluster
 // barriers.  fusedIterationsShape() is {0, 0} when the cluster launch is unavailable.

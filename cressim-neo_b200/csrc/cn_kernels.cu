@@ -1794,15 +1794,6 @@ __device__ __forceinline__ void particleContactGenerateAt(const Scene &s, uint32
     s.particleContacts[pi] = out;
 }
 
-__global__ void __launch_bounds__(kThreads) k_particleContactGenerate(Scene s)
-{
-    pdlEnter();
-    if (blockIdx.x == 0 && threadIdx.x == 0) s.meta_->activeParticleContacts = 0u;
-    // a fixed grid strides over the pairs that exist (a device count), not the capacity
-    const uint32_t count = s.meta_->particlePairCount;
-    for (uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x; pi < count; pi += gridDim.x * blockDim.x)
-        particleContactGenerateAt(s, pi);
-}
 
 // The rigid side of a proxy particle in a particle-particle contact: its body (inverse mass only
 // for a dynamic body), the contact point at the body's predicted pose and its lever arm.
@@ -1907,13 +1898,20 @@ __device__ __forceinline__ void particleContactSolveAt(const Scene &s, const Con
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_particleContactSolve(Scene s, Config cfg)
+// physics_particle_generate_explicit_contacts + physics_particle_solve_explicit_contacts, one pass:
+// a pair's solve reads only its own contact and the two positions, which no pair changes (the
+// corrections are summed into posCorr), so generating and solving it in the same thread gives the
+// two-pass results.  The active-contact count is published and cleared by the position-correction
+// apply that follows every such pass.
+__global__ void __launch_bounds__(kThreads) k_particleContacts(Scene s, Config cfg)
 {
     pdlEnter();
     // a fixed grid strides over the pairs that exist (a device count), not the capacity
     const uint32_t count = s.meta_->particlePairCount;
-    for (uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x; pi < count; pi += gridDim.x * blockDim.x)
+    for (uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x; pi < count; pi += gridDim.x * blockDim.x) {
+        particleContactGenerateAt(s, pi);
         particleContactSolveAt(s, cfg, pi);
+    }
 }
 
 // Particle-rigid contact for candidate pair `pi`: physics_particle_rigid_generate_contacts.cs.hlsl:29-210
@@ -2134,18 +2132,48 @@ __global__ void __launch_bounds__(kThreads) k_rigidContacts(Scene s, Config cfg,
     forEachElem(s.wP, s.N, [&](uint32_t i) { rigidContactsAt(s, cfg, applyDirect, i); });
 }
 
-// physics_particle_apply_position_corrections.cs.hlsl:8-30
-__global__ void __launch_bounds__(kThreads) k_applyPositionCorrections(Scene s)
+// The tet family's gather and the particle-rigid contacts that follow it, in one pass, for
+// iterations without particle-particle contacts: a particle's rigid contacts read only its own
+// position, its candidate pairs and the colliders, so running them in the same thread right after
+// its gather (over the same particles as the two per-phase kernels: the tet window, then every
+// particle) gives their results bit for bit with one launch and one pass over x fewer.
+__global__ void __launch_bounds__(kThreads) k_applyTetsRigidContacts(Scene s, Config cfg)
 {
     pdlEnter();
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= s.N) return;
+    forEachElem(s.wP, s.N, [&](uint32_t i) {
+        if (s.wP.tiles || (i >= s.tetWin.x && i < s.tetWin.y)) applyGatherAt(s, s.tetRanges, s.tetCorr, i);
+        rigidContactsAt(s, cfg, true, i);
+    });
+}
+
+// physics_particle_apply_position_corrections.cs.hlsl:8-30
+__device__ __forceinline__ void applyPositionCorrectionAt(const Scene &s, uint32_t i)
+{
     const f3 c = xyz(s.posCorr[i]);
     s.posCorr[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 p = s.x[i];
     if (p.w <= kEps) return;
     s.x[i] = mk4(xyz(p) + c, p.w);
 }
+
+// The particle-particle pass of this iteration is complete: its active-contact count becomes the
+// reported one and the counter starts again at zero for the next pass.
+__device__ __forceinline__ void publishParticleContactCount(const Scene &s)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        s.meta_->activeParticleContactsLast = s.meta_->activeParticleContacts;
+        s.meta_->activeParticleContacts = 0u;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_applyPositionCorrections(Scene s)
+{
+    pdlEnter();
+    publishParticleContactCount(s);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < s.N) applyPositionCorrectionAt(s, i);
+}
+
 
 // ------------------------------------------------------------------------------------------
 // Velocity update and velocity-level passes
@@ -3106,12 +3134,10 @@ inline unsigned applyGrid(const Scene &s, uint2 win)
     return s.wP.tiles ? gridFor(s.wP, s.N) : blocksFor(win.y > win.x ? win.y - win.x : 0u);
 }
 
-void launchSoftIteration(const Scene &s, float dt, const Config &c, const XpbdPlan &plan, cudaStream_t st)
+bool launchSoftIteration(const Scene &s, float dt, const Config &c, const XpbdPlan &plan, cudaStream_t st,
+                         bool rigidContacts)
 {
-    if (plan.schedule == CN_XPBD_GATHER) {
-        launchSoftIteration(s, dt, c, st);
-        return;
-    }
+    if (plan.schedule == CN_XPBD_GATHER) return launchSoftIteration(s, dt, c, st, rigidContacts);
     const float relax = c.softInternalRelaxation;
     launchColourFamily<kFamEdges>(s, dt, relax, plan, st);
     launchColourFamily<kFamSegments>(s, dt, relax, plan, st);
@@ -3119,6 +3145,7 @@ void launchSoftIteration(const Scene &s, float dt, const Config &c, const XpbdPl
     launchColourFamily<kFamJoints>(s, dt, relax, plan, st);
     launchColourFamily<kFamDistances>(s, dt, relax, plan, st);
     launchColourFamily<kFamTets>(s, dt, relax, plan, st);
+    return false;
 }
 
 FusedShape fusedIterationsShape()
@@ -3225,7 +3252,7 @@ void launchBatchFusedIterations(const Scene &s, const Config &c, float dt, const
     cudaLaunchKernelEx(&cfg, k_batchFusedIterations, s, c, dt, plan);
 }
 
-void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st)
+bool launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st, bool rigidContacts)
 {
     const float relax = c.softInternalRelaxation;
     if (s.E) {
@@ -3251,8 +3278,13 @@ void launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t
     }
     if (s.T) {
         launchPdl(k_solveTets, gridFor(s.wT, s.T), kThreads, st, s, dt, relax);
+        if (rigidContacts && s.N) {
+            launchPdl(k_applyTetsRigidContacts, gridFor(s.wP, s.N), kThreads, st, s, c);
+            return true;
+        }
         launchPdl(k_applyGather, applyGrid(s, s.tetWin), kThreads, st, s, s.tetRanges, s.tetCorr, s.tetWin);
     }
+    return false;
 }
 
 void launchContacts(const Scene &s, const Config &c, bool particleContacts, bool rigidContacts,
@@ -3260,8 +3292,7 @@ void launchContacts(const Scene &s, const Config &c, bool particleContacts, bool
 {
     if (particleContacts) {
         const uint32_t cap = s.particlePairCapacity;
-        launchPdl(k_particleContactGenerate, pairGrid(cap), kThreads, st, s);
-        launchPdl(k_particleContactSolve, pairGrid(cap), kThreads, st, s, c);
+        launchPdl(k_particleContacts, pairGrid(cap), kThreads, st, s, c);
     }
     if (rigidContacts) launchPdl(k_rigidContacts, gridFor(s.wP, s.N), kThreads, st, s, c, !particleContacts);
     if (particleContacts) launchPdl(k_applyPositionCorrections, blocksFor(s.N), kThreads, st, s);

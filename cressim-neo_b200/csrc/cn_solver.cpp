@@ -481,8 +481,14 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
                 probe(sv, "fluid_delta_apply_clamp", st,
                       [&] { cn::launchFluidDeltaApplyClamp(s, it, dt, c, sv->writeFluidDebug, st); });
             }
-            if (runSoft) probe(sv, "soft_constraints", st, [&] { cn::launchSoftIteration(s, dt, c, sv->plan, st); });
-            if (runPP || runRigid) probe(sv, "contacts", st, [&] { cn::launchContacts(s, c, runPP, runRigid, st); });
+            // without particle-particle contacts the rigid contacts run in the tet gather's pass
+            bool contactsDone = false;
+            if (runSoft)
+                probe(sv, "soft_constraints", st, [&] {
+                    contactsDone = cn::launchSoftIteration(s, dt, c, sv->plan, st, runRigid && !runPP);
+                });
+            if ((runPP || runRigid) && !contactsDone)
+                probe(sv, "contacts", st, [&] { cn::launchContacts(s, c, runPP, runRigid, st); });
             // finalRigidContactDepenetration (physics_solver.cpp:1111-1117)
             if (runRigidRigid) probe(sv, "rigid_depenetration", st, [&] { cn::launchRigidDepenetration(s, c, st); });
             // applyRigidCorrections (physics_solver.cpp:1170-1177); with only static and kinematic
@@ -999,7 +1005,7 @@ CN_API cn_status cn_solver_validate_meta(cn_solver *sv, cn_meta *out)
     out->required_particle_particle_candidate_count = m.requiredParticlePairs;
     out->particle_particle_candidate_overflow = m.requiredParticlePairs > sv->s.particlePairCapacity ? 1u : 0u;
     out->fluid_boundary_candidate_overflow = m.boundaryMaskOverflow;
-    out->active_particle_contact_count = m.activeParticleContacts;
+    out->active_particle_contact_count = m.activeParticleContactsLast;
     out->fluid_neighbor_truncations = m.neighborTruncations;
     out->device_wait_timeouts = m.waitTimeouts;
     out->rigid_rigid_candidate_count = m.rigidRigidPairCount;

@@ -10,7 +10,7 @@ CPU:
   and at relaxation 0.5 ends closer to its converged state after the same few iterations.
 GPU:
 * fused iterations (one thread-block cluster kernel per substep) are bit-identical with the
-  per-phase kernels, and the 16^3 cube's frame graph shrinks from 1,102 kernels;
+  per-phase kernels, and the 16^3 cube's frame graph shrinks from ~900 kernels to ~110;
 * both coloured schedules are bit-identical with the oracle's restatement, fused and per colour
   (tolerance only for the scene whose bends go through acos);
 * colour Jacobi stays within 1e-5 of the gather schedule on the full 16^3 cube.
@@ -176,7 +176,7 @@ def test_cube_runs_fused_and_its_graph_shrinks():
         else:
             assert info["fused_iterations"] == 0
         s.close()
-    assert kernels[FUSED_OFF] > 1000 and kernels[FUSED_ON] < 200, kernels
+    assert kernels[FUSED_OFF] > 800 and kernels[FUSED_ON] < 200, kernels
 
 
 def _tissue_run(make, frames=4):
