@@ -536,7 +536,8 @@ class Solver:
     def schedule_info(self) -> dict:
         """The XPBD schedule in use: xpbd_schedule, fused_iterations (1: one cluster kernel per
         substep), cluster_ctas, threads_per_cta, colours per family (edges, strand segments,
-        bends + dihedrals, strand joints, strand distances, tets)."""
+        bends + dihedrals, strand joints, strand distances, tets), branches (iteration work on
+        side streams: 1 fluid chain, 2 strand families, 4 cloth bends)."""
         v = _abi.ScheduleInfo()
         _check(self._lib.cn_solver_schedule_info(self._h, C.byref(v)))
         out = {name: getattr(v, name) for name, _ in _abi.ScheduleInfo._fields_}

@@ -39,7 +39,7 @@ class SoftSettings(C.Structure):
 
 class ScheduleInfo(C.Structure):
     _fields_ = [("xpbd_schedule", u32), ("fused_iterations", u32), ("cluster_ctas", u32),
-                ("threads_per_cta", u32), ("colours", u32 * 6)]
+                ("threads_per_cta", u32), ("colours", u32 * 6), ("branches", u32)]
 
 
 class FluidSettings(C.Structure):

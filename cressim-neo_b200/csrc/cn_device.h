@@ -379,6 +379,10 @@ void launchFluidVorticity(const Scene &s, float dt, cudaStream_t st);
 // a tet family, those contacts run in the tet gather's pass; returns true when they did, and the
 // caller launches them itself otherwise.
 bool launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st, bool rigidContacts = false);
+// The same for the families whose bit (1 << kFam*) is set in `families`, in the family order.
+bool launchSoftFamilies(const Scene &s, float dt, const Config &c, cudaStream_t st, uint32_t families,
+                        bool rigidContacts = false);
+constexpr uint32_t kAllFamilies = (1u << kFamilies) - 1u;
 // The XPBD schedule of a solver: CN_XPBD_* and, for the coloured schedules, each family's colour
 // count and colour start offsets into Scene::colOrder (host copies for the per-colour launches,
 // device copies for the fused kernel).

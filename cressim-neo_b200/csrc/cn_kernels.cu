@@ -1628,10 +1628,13 @@ __global__ void __launch_bounds__(kThreads) k_solveSegments(Scene s, float dt, f
     if (g < s.S) solveSegmentAt(s, dt, relax, g);
 }
 
-// physics_strand_apply_segment_corrections.cs.hlsl:11-43
-__device__ __forceinline__ void applySegmentsAt(const Scene &s, uint32_t i)
+// physics_strand_apply_segment_corrections.cs.hlsl:11-43.  Thread i applies particle segWin.x + i
+// of the segments' particle window (the others have no segment records) and renormalises
+// segment i's orientation.
+__device__ __forceinline__ void applySegmentsAt(const Scene &s, uint32_t t)
 {
-    if (i < s.N) {
+    const uint32_t i = s.segWin.x + t;
+    if (i < s.segWin.y) {
         const float4 p = s.x[i];
         if (p.w > kEps) {
             const uint2 r = s.segRanges[i];
@@ -1643,7 +1646,12 @@ __device__ __forceinline__ void applySegmentsAt(const Scene &s, uint32_t i)
             s.x[i] = mk4(xyz(p) + total, p.w);
         }
     }
-    if (i < s.S) s.segOrient[i] = qNormalize(add4(s.segOrient[i], s.segCorr[3 * size_t(i) + 2]));
+    if (t < s.S) s.segOrient[t] = qNormalize(add4(s.segOrient[t], s.segCorr[3 * size_t(t) + 2]));
+}
+__host__ __device__ __forceinline__ uint32_t segmentApplyThreads(const Scene &s)
+{
+    const uint32_t w = s.segWin.y > s.segWin.x ? s.segWin.y - s.segWin.x : 0u;
+    return w > s.S ? w : s.S;
 }
 
 __global__ void __launch_bounds__(kThreads) k_applySegments(Scene s)
@@ -3000,7 +3008,7 @@ __device__ __forceinline__ void fusedFamily(const Scene &s, float dt, float rela
             for (uint32_t i = s.edgeWin.x + tid; i < s.edgeWin.y; i += nth)
                 applyGatherAt(s, s.edgeRanges, s.edgeCorr, i);
         } else if constexpr (kFam == kFamSegments) {
-            const uint32_t m = s.N > s.S ? s.N : s.S;
+            const uint32_t m = segmentApplyThreads(s);
             for (uint32_t i = tid; i < m; i += nth) applySegmentsAt(s, i);
         } else if constexpr (kFam == kFamBends) {
             for (uint32_t i = s.bendWin.x + tid; i < s.bendWin.y; i += nth)
@@ -3254,29 +3262,36 @@ void launchBatchFusedIterations(const Scene &s, const Config &c, float dt, const
 
 bool launchSoftIteration(const Scene &s, float dt, const Config &c, cudaStream_t st, bool rigidContacts)
 {
+    return launchSoftFamilies(s, dt, c, st, kAllFamilies, rigidContacts);
+}
+
+bool launchSoftFamilies(const Scene &s, float dt, const Config &c, cudaStream_t st, uint32_t families,
+                        bool rigidContacts)
+{
     const float relax = c.softInternalRelaxation;
-    if (s.E) {
+    auto on = [&](uint32_t f) { return ((families >> f) & 1u) != 0u; };
+    if (s.E && on(kFamEdges)) {
         launchPdl(k_solveEdges, gridFor(s.wE, s.E), kThreads, st, s, dt, relax);
         launchPdl(k_applyGather, applyGrid(s, s.edgeWin), kThreads, st, s, s.edgeRanges, s.edgeCorr, s.edgeWin);
     }
-    if (s.S) {
+    if (s.S && on(kFamSegments)) {
         launchPdl(k_solveSegments, blocksFor(s.S), kThreads, st, s, dt, relax);
-        launchPdl(k_applySegments, blocksFor(s.N > s.S ? s.N : s.S), kThreads, st, s);
+        launchPdl(k_applySegments, blocksFor(segmentApplyThreads(s)), kThreads, st, s);
     }
-    if (s.Bn || s.D) {
+    if ((s.Bn || s.D) && on(kFamBends)) {
         if (s.Bn) launchPdl(k_solveBends, blocksFor(s.Bn), kThreads, st, s, dt, relax);
         if (s.D) launchPdl(k_solveDihedrals, blocksFor(s.D), kThreads, st, s, dt, relax);
         launchPdl(k_applyGather, applyGrid(s, s.bendWin), kThreads, st, s, s.bendRanges, s.bendCorr, s.bendWin);
     }
-    if (s.J) {
+    if (s.J && on(kFamJoints)) {
         launchPdl(k_solveJoints, blocksFor(s.J), kThreads, st, s, dt, relax);
         launchPdl(k_applyJoints, blocksFor(s.S), kThreads, st, s);
     }
-    if (s.SD) {
+    if (s.SD && on(kFamDistances)) {
         launchPdl(k_solveDistances, blocksFor(s.SD), kThreads, st, s, dt, relax);
         launchPdl(k_applyGather, applyGrid(s, s.segWin), kThreads, st, s, s.segRanges, s.distCorr, s.segWin);
     }
-    if (s.T) {
+    if (s.T && on(kFamTets)) {
         launchPdl(k_solveTets, gridFor(s.wT, s.T), kThreads, st, s, dt, relax);
         if (rigidContacts && s.N) {
             launchPdl(k_applyTetsRigidContacts, gridFor(s.wP, s.N), kThreads, st, s, c);

@@ -75,6 +75,12 @@ struct cn_solver {
     bool fused = false;
     cn::FusedShape fusedShape{};
     bool fusedShapeQueried = false;
+    // Concurrent branches of an iteration (gather schedule): families and the fluid chain whose
+    // particles are disjoint run on side streams forked from and joined to the frame's stream,
+    // each particle seeing the same updates in the same order.
+    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, joinFluid = nullptr, joinStrands = nullptr, afterEdges = nullptr, joinBends = nullptr;
+    bool branchFluid = false, branchStrands = false, branchBends = false;
 };
 
 namespace {
@@ -410,6 +416,35 @@ cn_status uploadSurfaceRender(cn_solver *sv, const cn_world_soa &w, cudaStream_t
     return CN_OK;
 }
 
+// One iteration's soft families with the strand families on a side stream and, once the edges
+// are applied, the cloth bends on another, joined back before the stream goes on (each particle's
+// families still in the order of physics_solver.cpp:915-1019).
+void launchSoftBranches(cn_solver *sv, float dt, cudaStream_t st)
+{
+    const cn::Scene &s = sv->s;
+    const cn::Config &c = sv->cfg;
+    const uint32_t strandFams = (1u << cn::kFamSegments) | (1u << cn::kFamJoints) | (1u << cn::kFamDistances);
+    uint32_t mainFams = cn::kAllFamilies;
+    if (sv->branchStrands) {
+        cudaStreamWaitEvent(sv->side[1], sv->fork, 0);
+        cn::launchSoftFamilies(s, dt, c, sv->side[1], strandFams);
+        cudaEventRecord(sv->joinStrands, sv->side[1]);
+        mainFams &= ~strandFams;
+    }
+    if (sv->branchBends) {
+        cn::launchSoftFamilies(s, dt, c, st, mainFams & (1u << cn::kFamEdges));
+        cudaEventRecord(sv->afterEdges, st);
+        cudaStreamWaitEvent(sv->side[2], sv->afterEdges, 0);
+        cn::launchSoftFamilies(s, dt, c, sv->side[2], 1u << cn::kFamBends);
+        cudaEventRecord(sv->joinBends, sv->side[2]);
+        cn::launchSoftFamilies(s, dt, c, st, mainFams & ~((1u << cn::kFamEdges) | (1u << cn::kFamBends)));
+        cudaStreamWaitEvent(st, sv->joinBends, 0);
+    } else {
+        cn::launchSoftFamilies(s, dt, c, st, mainFams);
+    }
+    if (sv->branchStrands) cudaStreamWaitEvent(st, sv->joinStrands, 0);
+}
+
 void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
 {
     const cn::Scene &s = sv->s;
@@ -472,21 +507,32 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             const bool runRigid = sv->rigidPossible && it < sv->contactIt;
             const bool runRigidRigid = sv->rigidRigid && it < sv->rrIt;
             if (!runFluid && !runSoft && !runPP && !runRigid && !runRigidRigid) break; // remaining iterations are empty
+            // fork: the fluid chain and the branched soft families leave the frame's stream here
+            const bool fluidBranch = sv->branchFluid && runFluid && runSoft;
+            const bool softBranches = runSoft && (sv->branchStrands || sv->branchBends);
+            if (fluidBranch || softBranches) cudaEventRecord(sv->fork, st);
+            const cudaStream_t fst = fluidBranch ? sv->side[0] : st;
+            if (fluidBranch) cudaStreamWaitEvent(fst, sv->fork, 0);
             if (runFluid) {
                 if (it == 0 || cn::fluidGatherEachIteration(s))
-                    probe(sv, "fluid_gather", st, [&] { cn::launchFluidGather(s, it, st); });
+                    probe(sv, "fluid_gather", fst, [&] { cn::launchFluidGather(s, it, fst); });
                 // the first iteration of a substep also records the superset lists when they are on
-                probe(sv, (it == 0 && s.sup && !sv->walkCells) ? "fluid_neighbors_superset" : "fluid_neighbors_density", st,
-                      [&] { cn::launchFluidNeighborsDensity(s, c, it, sv->walkCells, st); });
-                probe(sv, "fluid_delta_apply_clamp", st,
-                      [&] { cn::launchFluidDeltaApplyClamp(s, it, dt, c, sv->writeFluidDebug, st); });
+                probe(sv, (it == 0 && s.sup && !sv->walkCells) ? "fluid_neighbors_superset" : "fluid_neighbors_density", fst,
+                      [&] { cn::launchFluidNeighborsDensity(s, c, it, sv->walkCells, fst); });
+                probe(sv, "fluid_delta_apply_clamp", fst,
+                      [&] { cn::launchFluidDeltaApplyClamp(s, it, dt, c, sv->writeFluidDebug, fst); });
             }
-            // without particle-particle contacts the rigid contacts run in the tet gather's pass
+            if (fluidBranch) cudaEventRecord(sv->joinFluid, fst);
+            // without particle-particle contacts (and without soft branches) the rigid contacts run
+            // in the tet gather's pass
             bool contactsDone = false;
-            if (runSoft)
+            if (runSoft && softBranches)
+                probe(sv, "soft_constraints", st, [&] { launchSoftBranches(sv, dt, st); });
+            else if (runSoft)
                 probe(sv, "soft_constraints", st, [&] {
                     contactsDone = cn::launchSoftIteration(s, dt, c, sv->plan, st, runRigid && !runPP);
                 });
+            if (fluidBranch) cudaStreamWaitEvent(st, sv->joinFluid, 0);
             if ((runPP || runRigid) && !contactsDone)
                 probe(sv, "contacts", st, [&] { cn::launchContacts(s, c, runPP, runRigid, st); });
             // finalRigidContactDepenetration (physics_solver.cpp:1111-1117)
@@ -601,10 +647,15 @@ CN_API cn_status cn_solver_create(const cn_solver_desc *desc, int device, cn_sol
     cn_solver *sv = new cn_solver();
     sv->desc = *desc;
     sv->device = device;
-    const cudaError_t e = cudaStreamCreateWithFlags(&sv->ownStream, cudaStreamNonBlocking);
+    cudaError_t e = cudaStreamCreateWithFlags(&sv->ownStream, cudaStreamNonBlocking);
+    for (cudaStream_t &x : sv->side)
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
+    for (cudaEvent_t *ev : {&sv->fork, &sv->joinFluid, &sv->joinStrands, &sv->afterEdges, &sv->joinBends})
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     if (e != cudaSuccess) {
-        delete sv;
-        return setError(CN_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+        cudaGetLastError();
+        cn_solver_destroy(sv);
+        return setError(CN_ERR_CUDA, std::string("cn_solver_create: ") + cudaGetErrorString(e));
     }
     *out = sv;
     return CN_OK;
@@ -614,9 +665,13 @@ CN_API void cn_solver_destroy(cn_solver *sv)
 {
     if (!sv) return;
     cudaSetDevice(sv->device);
-    cudaStreamSynchronize(sv->ownStream);
+    if (sv->ownStream) cudaStreamSynchronize(sv->ownStream);
     releaseBuffers(sv);
-    cudaStreamDestroy(sv->ownStream);
+    if (sv->ownStream) cudaStreamDestroy(sv->ownStream);
+    for (cudaStream_t x : sv->side)
+        if (x) cudaStreamDestroy(x);
+    for (cudaEvent_t ev : {sv->fork, sv->joinFluid, sv->joinStrands, sv->afterEdges, sv->joinBends})
+        if (ev) cudaEventDestroy(ev);
     delete sv;
 }
 
@@ -955,6 +1010,27 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
         const uint64_t most = std::max({uint64_t(N), uint64_t(s.E), uint64_t(s.Bn) + s.D, uint64_t(s.T), uint64_t(s.S),
                                         uint64_t(s.J), uint64_t(s.SD)});
         sv->fused = cap > 0 && most <= cap;
+    }
+    // Concurrent branches (per-phase gather schedule): the strand families beside the others, the
+    // cloth bends beside the tets once the edges are applied, and the fluid chain beside the soft
+    // families, whenever the particle windows they write are disjoint.
+    {
+        auto disjoint = [](uint2 a, uint2 b) { return a.y <= a.x || b.y <= b.x || a.y <= b.x || b.y <= a.x; };
+        const bool perPhase = sv->plan.schedule == CN_XPBD_GATHER && !sv->fused;
+        const bool strands = s.S || s.J || s.SD, others = s.E || s.Bn || s.D || s.T;
+        sv->branchStrands = perPhase && strands && others && disjoint(s.segWin, s.edgeWin) &&
+                            disjoint(s.segWin, s.bendWin) && disjoint(s.segWin, s.tetWin);
+        sv->branchBends = perPhase && (s.Bn || s.D) && s.T && disjoint(s.bendWin, s.tetWin) &&
+                          (!strands || sv->branchStrands);
+        uint2 fluidWin = make_uint2(N, 0u);
+        for (uint32_t i = 0; i < N; ++i)
+            if (w->kinds[i] == CN_PARTICLE_FLUID) {
+                fluidWin.x = std::min(fluidWin.x, i);
+                fluidWin.y = i + 1;
+            }
+        sv->branchFluid = perPhase && sv->hasFluid && (strands || others) && disjoint(fluidWin, s.edgeWin) &&
+                          disjoint(fluidWin, s.bendWin) && disjoint(fluidWin, s.tetWin) &&
+                          disjoint(fluidWin, s.segWin);
     }
     sv->hostX = w->positions_inv_mass;
     sv->hostV = w->velocities;
@@ -1367,6 +1443,7 @@ CN_API cn_status cn_solver_schedule_info(cn_solver *sv, cn_schedule_info *out)
     out->cluster_ctas = sv->fused ? sv->fusedShape.ctas : 0u;
     out->threads_per_cta = sv->fused ? sv->fusedShape.threads : 0u;
     for (uint32_t f = 0; f < cn::kFamilies; ++f) out->colours[f] = sv->plan.colours[f];
+    out->branches = (sv->branchFluid ? 1u : 0u) | (sv->branchStrands ? 2u : 0u) | (sv->branchBends ? 4u : 0u);
     return CN_OK;
 }
 

@@ -653,6 +653,8 @@ typedef struct cn_schedule_info {
     uint32_t threads_per_cta;
     uint32_t colours[6];        /* colours per family: edges, strand segments, bends + dihedrals,
                                  * strand joints, strand distances, tets (0 under CN_XPBD_GATHER) */
+    uint32_t branches;          /* iteration work run concurrently on side streams (disjoint particles):
+                                 * 1 the fluid chain, 2 the strand families, 4 the cloth bends */
 } cn_schedule_info;
 CN_API cn_status cn_solver_schedule_info(cn_solver *solver, cn_schedule_info *out);
 

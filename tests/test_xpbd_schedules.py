@@ -308,3 +308,19 @@ def test_programmatic_dependent_launch_changes_no_bits(tmp_path):
         subprocess.run([sys.executable, str(script), str(root), str(dst)], env=env, check=True, timeout=600)
         out[flag] = np.load(dst)
     _bits(out["1"], out["0"], "pdl on / off")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name, branches", [("cloth_and_strand", 2), ("cloth_on_tissue", 6), ("mixed_small", 7),
+                                            ("xpbd_cube_8", 0)])
+def test_concurrent_branches_where_particles_are_disjoint(name, branches):
+    """The golden scenes run their disjoint work on side streams (their golden tests then hold
+    the branched schedule to the oracle bit for bit)."""
+    seen = {}
+
+    def make(desc, soa):
+        s = _solver()(desc, soa)
+        seen["info"] = s.schedule_info()
+        return s
+    make_golden.run(make, name, frames=1)
+    assert seen["info"]["branches"] == branches, seen
