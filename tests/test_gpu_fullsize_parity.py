@@ -3,7 +3,7 @@
 * The PBF dam break at its benchmark size (128 x 64 x 128 = 1,048,576 particles) for one frame:
   the sorted (cellKey, index) pairs, the cell-range table, the neighbour counts and lists of the
   last fluid iteration and the particle state are compared with the oracle bit for bit (the
-  north-star bars are bit-exact keys / permutations / lists and 1e-5 on the state; both sides
+  parity bars are bit-exact keys / permutations / lists and 1e-5 on the state; both sides
   evaluate the same float32 expressions without contraction, so the state is bit-identical too).
 * The superset-filter schedule (the default from the second fluid iteration on) against the
   27-cell walk in every iteration, bit for bit, at full size for two frames.
