@@ -157,6 +157,13 @@ struct cn_batch {
     uint32_t clusterCtas = 0, clusters = 0;
     uint2 *dScenes = nullptr;
     uint2 *hScenes[2] = {nullptr, nullptr};
+    // admission: scene images are copied and scattered on the upload stream; the next tick waits
+    // for the last one
+    cudaStream_t upStream = nullptr;
+    cudaEvent_t upDone = nullptr;
+    uint8_t *dStage = nullptr;
+    size_t stageBytes = 0;
+    bool uploadPending = false;
 };
 
 namespace {
@@ -360,6 +367,178 @@ void releaseScene(cn_batch *b, BatchScene &sc)
 
 } // namespace
 
+namespace cn {
+
+cn_status buildSceneImage(const cn_world_soa &w, uint32_t rigidPairsPerParticle, SceneImage &img)
+{
+    const uint32_t N = w.particle_count;
+    if (N == 0) return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_add_scene: empty scene");
+    if (!w.positions_inv_mass || !w.velocities || !w.radii || !w.kinds || !w.metadata || !w.material_indices ||
+        !w.owner_types || !w.owner_indices)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_add_scene: missing particle array");
+    // The batch runs the soft-tissue families: edges, tets, static / kinematic colliders.
+    if (w.bend_count || w.dihedral_count || w.strand_segment_count || w.strand_joint_count || w.strand_distance_count)
+        return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: cloth and strand constraints are not batched");
+    std::vector<uint32_t> groups;
+    for (uint32_t i = 0; i < N; ++i) {
+        if (w.kinds[i] == CN_PARTICLE_FLUID)
+            return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: fluid particles are not batched");
+        if (w.owner_types[i] == CN_OWNER_RIGID_BODY)
+            return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: rigid proxy particles are not batched");
+        const uint32_t ph = w.metadata[4 * i + 1];
+        if (ph & CN_PHASE_SELF_COLLIDE)
+            return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: self-colliding bodies are not batched");
+        const uint32_t g = ph & CN_PHASE_GROUP_MASK;
+        if (std::find(groups.begin(), groups.end(), g) == groups.end()) groups.push_back(g);
+    }
+    if (groups.size() > 1)
+        return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: scenes with particle-particle contacts are not batched");
+    for (uint32_t k = 0; k < w.rigid_body_count; ++k)
+        if (w.body_types[k] == CN_BODY_DYNAMIC) return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: dynamic rigid bodies");
+    std::vector<uint32_t> order;
+    colliderQueryOrder(w, order);
+    const Incidence edgeI = buildIncidence(N, w.edge_count, 2, [&](uint32_t c, uint32_t k) {
+        return k == 0 ? w.edges[c].particle_a : w.edges[c].particle_b;
+    });
+    const Incidence tetI = buildIncidence(N, w.tet_count, 4, [&](uint32_t c, uint32_t k) {
+        return w.tets[c].particle_indices[k];
+    });
+
+    AdmitImage &L = img.layout;
+    L = AdmitImage{};
+    L.N = N;
+    L.E = w.edge_count;
+    L.T = w.tet_count;
+    L.B = w.rigid_body_count;
+    L.C = w.collider_count;
+    L.CI = w.body_collider_index_count;
+    L.M = std::max<uint32_t>(w.contact_material_count, 1u);
+    L.queryCount = uint32_t(order.size());
+    const size_t sizes[kAdmSegments] = {
+        16ull * N, 16ull * N, 4ull * N, 4ull * N, 16ull * N, 4ull * N, 4ull * N, 4ull * N, 8ull * N, 8ull * N,
+        sizeof(cn_soft_edge) * L.E, 8ull * L.E, sizeof(cn_soft_tet) * L.T, 16ull * L.T, 16ull * L.M,
+        16ull * L.B, 16ull * L.B, 16ull * L.B, 16ull * L.B, 16ull * L.B, 16ull * L.B, 4ull * L.B, 16ull * L.B,
+        16ull * L.B, 4ull * L.B, 8ull * L.B, 4ull * L.CI, sizeof(cn_collider_geometry) * L.C,
+        sizeof(cn_collider_broadphase) * L.C, 16ull * L.C, 4ull * L.queryCount};
+    size_t at = 0;
+    for (uint32_t k = 0; k < kAdmSegments; ++k) {
+        L.off[k] = at;
+        at += (sizes[k] + 15) & ~size_t(15);
+    }
+    img.bytes.assign(at, 0);
+    auto put = [&](uint32_t seg, const void *src, size_t bytes) {
+        if (bytes && src) std::memcpy(img.bytes.data() + L.off[seg], src, bytes);
+    };
+    put(kAdmRadii, w.radii, 4ull * N);
+    put(kAdmKinds, w.kinds, 4ull * N);
+    put(kAdmMeta, w.metadata, 16ull * N);
+    put(kAdmMatIdx, w.material_indices, 4ull * N);
+    put(kAdmOwnerTypes, w.owner_types, 4ull * N);
+    put(kAdmOwnerIdx, w.owner_indices, 4ull * N);
+    put(kAdmEdgeRanges, edgeI.ranges.data(), 8ull * N);
+    put(kAdmTetRanges, tetI.ranges.data(), 8ull * N);
+    put(kAdmEdges, w.edges, sizeof(cn_soft_edge) * L.E);
+    put(kAdmEdgeDst, edgeI.dst.data(), 8ull * L.E);
+    put(kAdmTets, w.tets, sizeof(cn_soft_tet) * L.T);
+    put(kAdmTetDst, tetI.dst.data(), 16ull * L.T);
+    put(kAdmMaterials, w.contact_materials, 16ull * w.contact_material_count);
+    put(kAdmBodyScale, w.body_scales, 16ull * L.B);
+    put(kAdmBodyInvI, w.body_inverse_inertia, 16ull * L.B);
+    put(kAdmBodyType, w.body_types, 4ull * L.B);
+    put(kAdmBodyColRanges, w.body_collider_ranges, 8ull * L.B);
+    put(kAdmBodyColIdx, w.body_collider_indices, 4ull * L.CI);
+    put(kAdmColGeo, w.collider_geometry, sizeof(cn_collider_geometry) * L.C);
+    put(kAdmColBp, w.collider_broadphase, sizeof(cn_collider_broadphase) * L.C);
+    put(kAdmColMat, w.collider_materials, 16ull * L.C);
+    put(kAdmQueryOrder, order.data(), 4ull * L.queryCount);
+    refreshSceneImage(w, img);
+    img.budgetBytes = N * kBytesPerParticle + uint64_t(L.E) * kBytesPerEdge + uint64_t(L.T) * kBytesPerTet +
+                      uint64_t(L.B) * kBytesPerBody + uint64_t(L.C) * kBytesPerCollider +
+                      uint64_t(N) * rigidPairsPerParticle * 72u;
+    return CN_OK;
+}
+
+void refreshSceneImage(const cn_world_soa &w, SceneImage &img)
+{
+    const AdmitImage &L = img.layout;
+    auto put = [&](uint32_t seg, const void *src, size_t bytes) {
+        if (bytes && src) std::memcpy(img.bytes.data() + L.off[seg], src, bytes);
+    };
+    put(kAdmX, w.positions_inv_mass, 16ull * L.N);
+    put(kAdmV, w.velocities, 16ull * L.N);
+    put(kAdmBodyPos, w.body_positions_inv_mass, 16ull * L.B);
+    put(kAdmBodyRot, w.body_orientations, 16ull * L.B);
+    put(kAdmBodyLin, w.body_linear_velocities, 16ull * L.B);
+    put(kAdmBodyAng, w.body_angular_velocities, 16ull * L.B);
+    put(kAdmKinPos, w.body_kinematic_target_positions, 16ull * L.B);
+    put(kAdmKinRot, w.body_kinematic_target_orientations, 16ull * L.B);
+    put(kAdmKinFlags, w.body_kinematic_target_flags, 4ull * L.B);
+}
+
+cn_status batchAdmitImage(cn_batch *b, const SceneImage &img, uint32_t *scene_id)
+{
+    const AdmitImage &L = img.layout;
+    if (b->bytesAdmitted + img.budgetBytes > b->desc.memory_budget_bytes)
+        return setError(CN_ERR_CAPACITY, "cn_batch_add_scene: the device-memory budget is full");
+    BatchScene sc;
+    bool ok = b->aP.alloc(L.N, sc.p.start);
+    sc.p.count = ok ? L.N : 0;
+    auto take = [&](RangeAlloc &ra, uint32_t n, Range &r) {
+        if (!ok) return;
+        ok = ra.alloc(n, r.start);
+        r.count = ok ? n : 0;
+    };
+    take(b->aE, L.E, sc.e);
+    take(b->aT, L.T, sc.t);
+    take(b->aEI, L.E * 2u, sc.ei);
+    take(b->aTI, L.T * 4u, sc.ti);
+    take(b->aB, L.B, sc.b);
+    take(b->aC, L.C, sc.c);
+    take(b->aCI, L.CI, sc.ci);
+    take(b->aM, L.M, sc.m);
+    if (!ok) {
+        releaseScene(b, sc);
+        return setError(CN_ERR_CAPACITY, "cn_batch_add_scene: the pool has no room for this scene");
+    }
+    sc.live = true;
+    sc.queryCount = L.queryCount;
+    sc.bytes = img.budgetBytes;
+    b->bytesAdmitted += img.budgetBytes;
+    CN_CUDA(cudaSetDevice(b->device));
+    // One transfer into the staging buffer (grown when a larger scene arrives), then the scatter;
+    // both on the upload stream, which the next tick waits for.
+    const size_t bytes = img.bytes.size();
+    if (bytes > b->stageBytes) {
+        const size_t cap = std::max(bytes, 2 * b->stageBytes);
+        CN_CUDA(cudaStreamSynchronize(b->upStream));
+        if (b->dStage) cudaFree(b->dStage);
+        b->dStage = nullptr;
+        b->stageBytes = 0;
+        CN_CUDA(cudaMalloc(&b->dStage, cap));
+        b->stageBytes = cap;
+    }
+    CN_CUDA(cudaMemcpyAsync(b->dStage, img.bytes.data(), bytes, cudaMemcpyHostToDevice, b->upStream));
+    AdmitImage a = L;
+    a.img = b->dStage;
+    a.p0 = sc.p.start; a.e0 = sc.e.start; a.t0 = sc.t.start; a.ei0 = sc.ei.start; a.ti0 = sc.ti.start;
+    a.b0 = sc.b.start; a.c0 = sc.c.start; a.ci0 = sc.ci.start; a.m0 = sc.m.start;
+    launchAdmitScene(b->s, a, b->upStream);
+    CN_CUDA(cudaGetLastError());
+    CN_CUDA(cudaEventRecord(b->upDone, b->upStream));
+    b->uploadPending = true;
+    uint32_t id = 0;
+    while (id < b->scenes.size() && b->scenes[id].live) ++id;
+    if (id == b->scenes.size()) b->scenes.emplace_back();
+    b->scenes[id] = sc;
+    *scene_id = id;
+    clearError();
+    return CN_OK;
+}
+
+uint32_t batchRigidPairsPerParticle(const cn_batch *b) { return b->desc.rigid_pairs_per_particle; }
+
+} // namespace cn
+
 extern "C" {
 
 CN_API void cn_batch_desc_defaults(cn_batch_desc *d)
@@ -428,6 +607,8 @@ CN_API cn_status cn_batch_create(const cn_batch_desc *d, int device, cn_batch **
     a.reset(static_cast<uint8_t *>(b->arena));
     layoutPool(b, a);
     cudaStreamCreateWithFlags(&b->ownStream, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&b->upStream, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&b->upDone, cudaEventDisableTiming);
     cudaMemsetAsync(b->arena, 0, b->arenaBytes, b->ownStream);
     for (int k = 0; k < 2; ++k) cudaEventCreateWithFlags(&b->stageDone[k], cudaEventDisableTiming);
     const cn_status st = allocWorkLists(b);
@@ -480,168 +661,19 @@ CN_API void cn_batch_destroy(cn_batch *b)
         if (b->stageDone[k]) cudaEventDestroy(b->stageDone[k]);
     }
     if (b->ownStream) cudaStreamDestroy(b->ownStream);
+    if (b->upStream) cudaStreamDestroy(b->upStream);
+    if (b->upDone) cudaEventDestroy(b->upDone);
+    if (b->dStage) cudaFree(b->dStage);
     delete b;
 }
 
 CN_API cn_status cn_batch_add_scene(cn_batch *b, const cn_world_soa *w, uint32_t *scene_id)
 {
     if (!b || !w || !scene_id) return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_add_scene: null argument");
-    const uint32_t N = w->particle_count;
-    if (N == 0) return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_add_scene: empty scene");
-    if (!w->positions_inv_mass || !w->velocities || !w->radii || !w->kinds || !w->metadata || !w->material_indices ||
-        !w->owner_types || !w->owner_indices)
-        return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_add_scene: missing particle array");
-    // The batch runs the soft-tissue families: edges, tets, static / kinematic colliders.
-    if (w->bend_count || w->dihedral_count || w->strand_segment_count || w->strand_joint_count ||
-        w->strand_distance_count)
-        return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: cloth and strand constraints are not batched");
-    std::vector<uint32_t> groups;
-    for (uint32_t i = 0; i < N; ++i) {
-        if (w->kinds[i] == CN_PARTICLE_FLUID)
-            return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: fluid particles are not batched");
-        if (w->owner_types[i] == CN_OWNER_RIGID_BODY)
-            return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: rigid proxy particles are not batched");
-        const uint32_t ph = w->metadata[4 * i + 1];
-        if (ph & CN_PHASE_SELF_COLLIDE)
-            return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: self-colliding bodies are not batched");
-        const uint32_t g = ph & CN_PHASE_GROUP_MASK;
-        if (std::find(groups.begin(), groups.end(), g) == groups.end()) groups.push_back(g);
-    }
-    if (groups.size() > 1)
-        return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: scenes with particle-particle contacts are not batched");
-    for (uint32_t k = 0; k < w->rigid_body_count; ++k)
-        if (w->body_types[k] == CN_BODY_DYNAMIC)
-            return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: dynamic rigid bodies");
-    std::vector<uint32_t> order;
-    cn::colliderQueryOrder(*w, order);
-
-    BatchScene sc;
-    const uint64_t bytes = N * kBytesPerParticle + uint64_t(w->edge_count) * kBytesPerEdge +
-                           uint64_t(w->tet_count) * kBytesPerTet + uint64_t(w->rigid_body_count) * kBytesPerBody +
-                           uint64_t(w->collider_count) * kBytesPerCollider +
-                           uint64_t(N) * b->desc.rigid_pairs_per_particle * 72u;
-    if (b->bytesAdmitted + bytes > b->desc.memory_budget_bytes)
-        return setError(CN_ERR_CAPACITY, "cn_batch_add_scene: the device-memory budget is full");
-    const uint32_t nCI = std::max(w->body_collider_index_count, 0u);
-    bool ok = b->aP.alloc(N, sc.p.start);
-    sc.p.count = ok ? N : 0;
-    auto take = [&](RangeAlloc &ra, uint32_t n, Range &r) {
-        if (!ok) return;
-        ok = ra.alloc(n, r.start);
-        r.count = ok ? n : 0;
-    };
-    take(b->aE, w->edge_count, sc.e);
-    take(b->aT, w->tet_count, sc.t);
-    take(b->aEI, w->edge_count * 2u, sc.ei);
-    take(b->aTI, w->tet_count * 4u, sc.ti);
-    take(b->aB, w->rigid_body_count, sc.b);
-    take(b->aC, w->collider_count, sc.c);
-    take(b->aCI, nCI, sc.ci);
-    take(b->aM, std::max<uint32_t>(w->contact_material_count, 1u), sc.m);
-    if (!ok) {
-        releaseScene(b, sc);
-        return setError(CN_ERR_CAPACITY, "cn_batch_add_scene: the pool has no room for this scene");
-    }
-    sc.live = true;
-    sc.queryCount = uint32_t(order.size());
-    sc.bytes = bytes;
-    b->bytesAdmitted += bytes;
-
-    // Rebased host copies.
-    const uint32_t p0 = sc.p.start, e0 = sc.e.start, t0 = sc.t.start, b0 = sc.b.start, c0 = sc.c.start;
-    const uint32_t ci0 = sc.ci.start, m0 = sc.m.start;
-    std::vector<uint32_t> matIdx(w->material_indices, w->material_indices + N);
-    for (auto &m : matIdx) m += m0;
-    std::vector<uint32_t> ownerIdx(w->owner_indices, w->owner_indices + N);
-    for (uint32_t i = 0; i < N; ++i)
-        if (w->owner_types[i] == CN_OWNER_RIGID_BODY) ownerIdx[i] += b0;
-    std::vector<float4> xprev(N);
-    for (uint32_t i = 0; i < N; ++i)
-        xprev[i] = make_float4(w->positions_inv_mass[4 * i], w->positions_inv_mass[4 * i + 1],
-                               w->positions_inv_mass[4 * i + 2], 0.0f);
-    std::vector<cn_soft_edge> edges(w->edges, w->edges + w->edge_count);
-    for (auto &e : edges) { e.particle_a += p0; e.particle_b += p0; }
-    std::vector<cn_soft_tet> tets(w->tets, w->tets + w->tet_count);
-    for (auto &t : tets)
-        for (int k = 0; k < 4; ++k) t.particle_indices[k] += p0;
-    const cn::Incidence edgeI = cn::buildIncidence(N, w->edge_count, 2, [&](uint32_t c, uint32_t k) {
-        return k == 0 ? w->edges[c].particle_a : w->edges[c].particle_b;
-    });
-    const cn::Incidence tetI = cn::buildIncidence(N, w->tet_count, 4, [&](uint32_t c, uint32_t k) {
-        return w->tets[c].particle_indices[k];
-    });
-    std::vector<uint2> eRanges(edgeI.ranges), tRanges(tetI.ranges);
-    for (auto &r : eRanges) r.x += sc.ei.start;
-    for (auto &r : tRanges) r.x += sc.ti.start;
-    // gather slots, rebased with the scene's incidence ranges
-    std::vector<uint32_t> eDst(edgeI.dst), tDst(tetI.dst);
-    for (auto &d : eDst)
-        if (d != 0xffffffffu) d += sc.ei.start;
-    for (auto &d : tDst)
-        if (d != 0xffffffffu) d += sc.ti.start;
-    std::vector<uint2> colRange(N, make_uint2(c0, c0 + sc.queryCount));
-    std::vector<uint32_t> queryOrder(order);
-    for (auto &q : queryOrder) q += c0;
-    std::vector<cn_collider_broadphase> bp(w->collider_broadphase, w->collider_broadphase + w->collider_count);
-    for (auto &x : bp) x.owner_body += b0;
-    std::vector<uint2> bodyColRanges(w->rigid_body_count);
-    for (uint32_t k = 0; k < w->rigid_body_count; ++k) {
-        const uint32_t *r = w->body_collider_ranges + 2 * k;
-        bodyColRanges[k] = make_uint2(r[0] + ci0, r[1]);
-    }
-    std::vector<uint32_t> bodyColIdx(w->body_collider_indices, w->body_collider_indices + nCI);
-    for (auto &x : bodyColIdx) x += c0;
-    std::vector<float4> materials(sc.m.count, make_float4(0.f, 0.f, 0.f, 0.f));
-    for (uint32_t k = 0; k < w->contact_material_count; ++k)
-        materials[k] = make_float4(w->contact_materials[4 * k], w->contact_materials[4 * k + 1],
-                                   w->contact_materials[4 * k + 2], w->contact_materials[4 * k + 3]);
-
-    cn::Scene &s = b->s;
-    cudaStream_t st = b->ownStream;
-    CN_CUDA(cudaSetDevice(b->device));
-    CN_CUDA(upTo(s.x + p0, reinterpret_cast<const float4 *>(w->positions_inv_mass), N, st));
-    CN_CUDA(upTo(s.v + p0, reinterpret_cast<const float4 *>(w->velocities), N, st));
-    CN_CUDA(upTo(s.xprev + p0, xprev.data(), N, st));
-    CN_CUDA(upTo(const_cast<float *>(s.radii) + p0, w->radii, N, st));
-    CN_CUDA(upTo(const_cast<uint32_t *>(s.kinds) + p0, w->kinds, N, st));
-    CN_CUDA(upTo(const_cast<uint4 *>(s.meta) + p0, reinterpret_cast<const uint4 *>(w->metadata), N, st));
-    CN_CUDA(upTo(const_cast<uint32_t *>(s.matIdx) + p0, matIdx.data(), N, st));
-    CN_CUDA(cudaMemsetAsync(const_cast<uint32_t *>(s.fluidMatIdx) + p0, 0, sizeof(uint32_t) * N, st));
-    CN_CUDA(upTo(const_cast<uint32_t *>(s.ownerTypes) + p0, w->owner_types, N, st));
-    CN_CUDA(upTo(const_cast<uint32_t *>(s.ownerIdx) + p0, ownerIdx.data(), N, st));
-    CN_CUDA(upTo(const_cast<uint2 *>(s.edgeRanges) + p0, eRanges.data(), N, st));
-    CN_CUDA(upTo(const_cast<uint2 *>(s.tetRanges) + p0, tRanges.data(), N, st));
-    CN_CUDA(upTo(const_cast<uint2 *>(s.pColRange) + p0, colRange.data(), N, st));
-    CN_CUDA(upTo(const_cast<cn_soft_edge *>(s.edges) + e0, edges.data(), edges.size(), st));
-    CN_CUDA(upTo(const_cast<cn_soft_tet *>(s.tets) + t0, tets.data(), tets.size(), st));
-    CN_CUDA(upTo(const_cast<uint32_t *>(s.edgeDst) + size_t(e0) * 2, eDst.data(), eDst.size(), st));
-    CN_CUDA(upTo(const_cast<uint32_t *>(s.tetDst) + size_t(t0) * 4, tDst.data(), tDst.size(), st));
-    CN_CUDA(upTo(const_cast<float4 *>(s.contactMaterials) + m0, materials.data(), materials.size(), st));
-    const uint32_t nb = w->rigid_body_count, nc = w->collider_count;
-    CN_CUDA(upTo(s.bodyPos + b0, reinterpret_cast<const float4 *>(w->body_positions_inv_mass), nb, st));
-    CN_CUDA(upTo(s.bodyRot + b0, reinterpret_cast<const float4 *>(w->body_orientations), nb, st));
-    CN_CUDA(upTo(s.bodyLin + b0, reinterpret_cast<const float4 *>(w->body_linear_velocities), nb, st));
-    CN_CUDA(upTo(s.bodyAng + b0, reinterpret_cast<const float4 *>(w->body_angular_velocities), nb, st));
-    CN_CUDA(upTo(const_cast<float4 *>(s.bodyScale) + b0, reinterpret_cast<const float4 *>(w->body_scales), nb, st));
-    CN_CUDA(upTo(const_cast<float4 *>(s.bodyInvInertia) + b0, reinterpret_cast<const float4 *>(w->body_inverse_inertia), nb, st));
-    CN_CUDA(upTo(const_cast<uint32_t *>(s.bodyType) + b0, w->body_types, nb, st));
-    CN_CUDA(upTo(s.bodyKinPos + b0, reinterpret_cast<const float4 *>(w->body_kinematic_target_positions), nb, st));
-    CN_CUDA(upTo(s.bodyKinRot + b0, reinterpret_cast<const float4 *>(w->body_kinematic_target_orientations), nb, st));
-    CN_CUDA(upTo(s.bodyKinFlags + b0, w->body_kinematic_target_flags, nb, st));
-    CN_CUDA(upTo(const_cast<uint2 *>(s.bodyColRanges) + b0, bodyColRanges.data(), nb, st));
-    CN_CUDA(upTo(const_cast<uint32_t *>(s.bodyColIdx) + ci0, bodyColIdx.data(), bodyColIdx.size(), st));
-    CN_CUDA(upTo(const_cast<cn_collider_geometry *>(s.colGeo) + c0, w->collider_geometry, nc, st));
-    CN_CUDA(upTo(const_cast<cn_collider_broadphase *>(s.colBp) + c0, bp.data(), nc, st));
-    CN_CUDA(upTo(const_cast<float4 *>(s.colMat) + c0, reinterpret_cast<const float4 *>(w->collider_materials), nc, st));
-    CN_CUDA(upTo(const_cast<uint32_t *>(s.colQueryOrder) + c0, queryOrder.data(), queryOrder.size(), st));
-    CN_CUDA(cudaStreamSynchronize(st)); // the host copies above go out of scope
-    uint32_t id = 0;
-    while (id < b->scenes.size() && b->scenes[id].live) ++id;
-    if (id == b->scenes.size()) b->scenes.emplace_back();
-    b->scenes[id] = sc;
-    *scene_id = id;
-    cn::clearError();
-    return CN_OK;
+    cn::SceneImage img;
+    const cn_status st = cn::buildSceneImage(*w, b->desc.rigid_pairs_per_particle, img);
+    if (st != CN_OK) return st;
+    return cn::batchAdmitImage(b, img, scene_id);
 }
 
 CN_API cn_status cn_batch_remove_scene(cn_batch *b, uint32_t scene_id)
@@ -725,6 +757,10 @@ CN_API cn_status cn_batch_step(cn_batch *b, const uint32_t *scene_ids, uint32_t 
     b->pendingTargets.erase(b->pendingTargets.begin(), b->pendingTargets.begin() + nt);
     const cn_status gs = ensureGraph(b, frame_dt);
     if (gs != CN_OK) return gs;
+    if (b->uploadPending) { // admitted scenes' uploads land before this tick reads the pool
+        CN_CUDA(cudaStreamWaitEvent(st, b->upDone, 0));
+        b->uploadPending = false;
+    }
     for (int f = 0; f < 5; ++f)
         if (counts[f])
             CN_CUDA(cudaMemcpyAsync(b->dTiles + b->tileOffset[f], tiles + b->tileOffset[f], size_t(counts[f]) * sizeof(uint2),

@@ -434,6 +434,25 @@ void launchRigidContactVelocitiesDynamic(const Scene &s, uint32_t iterations, co
 // (physics_particle_sync_rigid_proxy_particles.cs.hlsl; the predict does it for the first time).
 void launchSyncRigidProxies(const Scene &s, cudaStream_t st);
 
+// ---------------------------------------------------------------- batch admission (cn_batch.cpp)
+// A scene's upload image: every per-element array a batch pool holds for it, with the scene's own
+// (0-based) indices, each segment 16-byte aligned in one host buffer.  Admission copies the image
+// to a device staging buffer in one transfer and k_admitScene scatters it into the pool ranges,
+// adding the scene's range offsets to every index field.
+enum AdmitSegment : uint32_t {
+    kAdmX, kAdmV, kAdmRadii, kAdmKinds, kAdmMeta, kAdmMatIdx, kAdmOwnerTypes, kAdmOwnerIdx, kAdmEdgeRanges,
+    kAdmTetRanges, kAdmEdges, kAdmEdgeDst, kAdmTets, kAdmTetDst, kAdmMaterials, kAdmBodyPos, kAdmBodyRot,
+    kAdmBodyLin, kAdmBodyAng, kAdmBodyScale, kAdmBodyInvI, kAdmBodyType, kAdmKinPos, kAdmKinRot, kAdmKinFlags,
+    kAdmBodyColRanges, kAdmBodyColIdx, kAdmColGeo, kAdmColBp, kAdmColMat, kAdmQueryOrder, kAdmSegments
+};
+struct AdmitImage {
+    const uint8_t *img = nullptr;          // the staging copy on the device
+    uint64_t off[kAdmSegments] = {};       // byte offset of each segment
+    uint32_t N = 0, E = 0, T = 0, B = 0, C = 0, CI = 0, M = 0, queryCount = 0;
+    uint32_t p0 = 0, e0 = 0, t0 = 0, ei0 = 0, ti0 = 0, b0 = 0, c0 = 0, ci0 = 0, m0 = 0; // pool offsets
+};
+void launchAdmitScene(const Scene &s, const AdmitImage &a, cudaStream_t st);
+
 // ---------------------------------------------------------------- rigid-rigid contacts (cn_rigid.cu)
 // Scratch of the rigid broadphase and grouping (sort + scan), in bytes, for C colliders and
 // `pairs` candidate pairs.

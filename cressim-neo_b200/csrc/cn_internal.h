@@ -133,6 +133,20 @@ template <class F> Colouring colourGreedy(uint32_t n, uint32_t constraints, uint
     return out;
 }
 
+// A batch scene's upload image (cn_batch.cpp): validated soft-tissue content in the pool's array
+// layouts with the scene's own indices, and the device bytes it is charged against the budget.
+struct SceneImage {
+    std::vector<uint8_t> bytes;
+    AdmitImage layout;
+    uint64_t budgetBytes = 0;
+};
+cn_status buildSceneImage(const cn_world_soa &w, uint32_t rigidPairsPerParticle, SceneImage &img);
+// Copies the mutable state (particles, bodies, kinematic targets) of `w` into the image.
+void refreshSceneImage(const cn_world_soa &w, SceneImage &img);
+// Admits the image into the batch (ranges, one transfer, the device-side scatter).
+cn_status batchAdmitImage(cn_batch *b, const SceneImage &img, uint32_t *scene_id);
+uint32_t batchRigidPairsPerParticle(const cn_batch *b);
+
 // Solver constants of one substep, from the PhysicsSolverDesc mirror.
 inline Config configFromDesc(const cn_solver_desc &d)
 {

@@ -1060,8 +1060,14 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidNeighborsDen
                             if (kExtras && st > kEps) normal += spikyGradK(delta, dist, h, invH, kW);
                         }
                     };
-                    if (!check) {
-                        for (uint32_t c = start; c < end; ++c) visit(c, ld4(&s.P[c]));
+                    if (!check) { // two candidates' positions in flight, visited in order
+                        uint32_t c = start;
+                        for (; c + 1u < end; c += 2u) {
+                            const float4 q0 = ld4(&s.P[c]), q1 = ld4(&s.P[c + 1u]);
+                            visit(c, q0);
+                            visit(c + 1u, q1);
+                        }
+                        if (c < end) visit(c, ld4(&s.P[c]));
                     } else {
                         for (uint32_t c = start; c < end; ++c) {
                             const int4 ce = __ldg(&s.cCell[c]);
@@ -3214,6 +3220,86 @@ void launchFusedIterations(const Scene &s, const Config &c, float dt, const Xpbd
     if (plan.schedule == CN_XPBD_COLOUR_JACOBI) fusedLaunch<CN_XPBD_COLOUR_JACOBI>(s, c, dt, fp, shape, st);
     else if (plan.schedule == CN_XPBD_COLOUR_GAUSS_SEIDEL) fusedLaunch<CN_XPBD_COLOUR_GAUSS_SEIDEL>(s, c, dt, fp, shape, st);
     else fusedLaunch<CN_XPBD_GATHER>(s, c, dt, fp, shape, st);
+}
+
+// Scatters an admitted scene's upload image into its pool ranges, rebasing every index field:
+// particle indices by p0, incidence positions by ei0 / ti0, bodies by b0, colliders by c0, body
+// collider lists by ci0, materials by m0 (the host rebasing of cn_batch_add_scene, on the device).
+__global__ void __launch_bounds__(kThreads) k_admitScene(Scene s, AdmitImage a)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    auto seg = [&](uint32_t k) { return a.img + a.off[k]; };
+    auto f4 = [&](uint32_t k) { return reinterpret_cast<const float4 *>(seg(k)); };
+    auto u32 = [&](uint32_t k) { return reinterpret_cast<const uint32_t *>(seg(k)); };
+    auto u2 = [&](uint32_t k) { return reinterpret_cast<const uint2 *>(seg(k)); };
+    if (i < a.N) {
+        const uint32_t p = a.p0 + i;
+        const float4 x = f4(kAdmX)[i];
+        s.x[p] = x;
+        s.v[p] = f4(kAdmV)[i];
+        s.xprev[p] = make_float4(x.x, x.y, x.z, 0.0f);
+        const_cast<float *>(s.radii)[p] = reinterpret_cast<const float *>(seg(kAdmRadii))[i];
+        const_cast<uint32_t *>(s.kinds)[p] = u32(kAdmKinds)[i];
+        const_cast<uint4 *>(s.meta)[p] = reinterpret_cast<const uint4 *>(seg(kAdmMeta))[i];
+        const_cast<uint32_t *>(s.matIdx)[p] = u32(kAdmMatIdx)[i] + a.m0;
+        const_cast<uint32_t *>(s.fluidMatIdx)[p] = 0u;
+        const uint32_t ot = u32(kAdmOwnerTypes)[i];
+        const_cast<uint32_t *>(s.ownerTypes)[p] = ot;
+        const_cast<uint32_t *>(s.ownerIdx)[p] = u32(kAdmOwnerIdx)[i] + (ot == CN_OWNER_RIGID_BODY ? a.b0 : 0u);
+        const uint2 er = u2(kAdmEdgeRanges)[i], tr = u2(kAdmTetRanges)[i];
+        const_cast<uint2 *>(s.edgeRanges)[p] = make_uint2(er.x + a.ei0, er.y);
+        const_cast<uint2 *>(s.tetRanges)[p] = make_uint2(tr.x + a.ti0, tr.y);
+        const_cast<uint2 *>(s.pColRange)[p] = make_uint2(a.c0, a.c0 + a.queryCount);
+    }
+    if (i < a.E) {
+        cn_soft_edge e = reinterpret_cast<const cn_soft_edge *>(seg(kAdmEdges))[i];
+        e.particle_a += a.p0;
+        e.particle_b += a.p0;
+        const_cast<cn_soft_edge *>(s.edges)[a.e0 + i] = e;
+        const uint2 d = u2(kAdmEdgeDst)[i];
+        reinterpret_cast<uint2 *>(const_cast<uint32_t *>(s.edgeDst))[a.e0 + i] =
+            make_uint2(d.x == kNoSlot ? kNoSlot : d.x + a.ei0, d.y == kNoSlot ? kNoSlot : d.y + a.ei0);
+    }
+    if (i < a.T) {
+        cn_soft_tet t = reinterpret_cast<const cn_soft_tet *>(seg(kAdmTets))[i];
+        for (int k = 0; k < 4; ++k) t.particle_indices[k] += a.p0;
+        const_cast<cn_soft_tet *>(s.tets)[a.t0 + i] = t;
+        const uint4 d = reinterpret_cast<const uint4 *>(seg(kAdmTetDst))[i];
+        auto rb = [&](uint32_t v) { return v == kNoSlot ? kNoSlot : v + a.ti0; };
+        reinterpret_cast<uint4 *>(const_cast<uint32_t *>(s.tetDst))[a.t0 + i] = make_uint4(rb(d.x), rb(d.y), rb(d.z), rb(d.w));
+    }
+    if (i < a.M) const_cast<float4 *>(s.contactMaterials)[a.m0 + i] = f4(kAdmMaterials)[i];
+    if (i < a.B) {
+        const uint32_t b = a.b0 + i;
+        s.bodyPos[b] = f4(kAdmBodyPos)[i];
+        s.bodyRot[b] = f4(kAdmBodyRot)[i];
+        s.bodyLin[b] = f4(kAdmBodyLin)[i];
+        s.bodyAng[b] = f4(kAdmBodyAng)[i];
+        const_cast<float4 *>(s.bodyScale)[b] = f4(kAdmBodyScale)[i];
+        const_cast<float4 *>(s.bodyInvInertia)[b] = f4(kAdmBodyInvI)[i];
+        const_cast<uint32_t *>(s.bodyType)[b] = u32(kAdmBodyType)[i];
+        s.bodyKinPos[b] = f4(kAdmKinPos)[i];
+        s.bodyKinRot[b] = f4(kAdmKinRot)[i];
+        s.bodyKinFlags[b] = u32(kAdmKinFlags)[i];
+        const uint2 r = u2(kAdmBodyColRanges)[i];
+        const_cast<uint2 *>(s.bodyColRanges)[b] = make_uint2(r.x + a.ci0, r.y);
+    }
+    if (i < a.CI) const_cast<uint32_t *>(s.bodyColIdx)[a.ci0 + i] = u32(kAdmBodyColIdx)[i] + a.c0;
+    if (i < a.C) {
+        const uint32_t c = a.c0 + i;
+        const_cast<cn_collider_geometry *>(s.colGeo)[c] = reinterpret_cast<const cn_collider_geometry *>(seg(kAdmColGeo))[i];
+        cn_collider_broadphase bp = reinterpret_cast<const cn_collider_broadphase *>(seg(kAdmColBp))[i];
+        bp.owner_body += a.b0;
+        const_cast<cn_collider_broadphase *>(s.colBp)[c] = bp;
+        const_cast<float4 *>(s.colMat)[c] = f4(kAdmColMat)[i];
+    }
+    if (i < a.queryCount) const_cast<uint32_t *>(s.colQueryOrder)[a.c0 + i] = u32(kAdmQueryOrder)[i] + a.c0;
+}
+
+void launchAdmitScene(const Scene &s, const AdmitImage &a, cudaStream_t st)
+{
+    const uint32_t n = std::max({a.N, a.E, a.T, a.B, a.C, a.CI, a.M, a.queryCount, 1u});
+    k_admitScene<<<blocksFor(n), kThreads, 0, st>>>(s, a);
 }
 
 uint32_t batchFusedClusters(uint32_t ctas)

@@ -126,6 +126,10 @@ struct SceneSlot {
     SceneSlot(const SceneSlot &) = delete;
     SceneSlot &operator=(const SceneSlot &) = delete;
     SceneStore store;
+    // the scene's upload image, built at registration; admission refreshes its state sections
+    cn::SceneImage image;
+    cn_status imageStatus = CN_OK;
+    std::string imageError;
     bool resident = false;
     uint32_t batchId = 0;
     std::deque<Request> queue;
@@ -168,7 +172,12 @@ bool admit(cn_server *srv, uint32_t id)
     SceneSlot &sc = *srv->scenes[id];
     for (;;) {
         uint32_t bid = 0;
-        const cn_status st = cn_batch_add_scene(srv->batch, &sc.store.soa, &bid);
+        if (sc.imageStatus != CN_OK) {
+            cn::setError(sc.imageStatus, sc.imageError);
+            return false;
+        }
+        cn::refreshSceneImage(sc.store.soa, sc.image);
+        const cn_status st = cn::batchAdmitImage(srv->batch, sc.image, &bid);
         if (st == CN_OK) {
             sc.resident = true;
             sc.batchId = bid;
@@ -256,7 +265,11 @@ CN_API cn_status cn_server_register_scene(cn_server *srv, const cn_world_soa *w,
 {
     if (!srv || !w || !scene) return setError(CN_ERR_INVALID_ARGUMENT, "cn_server_register_scene: null argument");
     srv->scenes.push_back(std::make_unique<SceneSlot>());
-    srv->scenes.back()->store.assign(*w);
+    SceneSlot &sc = *srv->scenes.back();
+    sc.store.assign(*w);
+    sc.imageStatus = cn::buildSceneImage(sc.store.soa, cn::batchRigidPairsPerParticle(srv->batch), sc.image);
+    if (sc.imageStatus != CN_OK) sc.imageError = cn_last_error();
+    cn::clearError();
     *scene = uint32_t(srv->scenes.size() - 1);
     return CN_OK;
 }
