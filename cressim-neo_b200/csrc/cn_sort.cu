@@ -327,6 +327,36 @@ __global__ void __launch_bounds__(kScanThreads) k_scanDown(const uint32_t *__res
     }
 }
 
+// Small inputs (at most kScanSingleMax elements): one CTA walks the chunks with a running carry,
+// the same integers in one launch instead of three.
+constexpr uint32_t kScanSingleMax = 8u * kScanChunk;
+__global__ void __launch_bounds__(kScanThreads) k_scanSingle(const uint32_t *__restrict__ in, uint32_t n,
+                                                             uint32_t *__restrict__ out, uint32_t *total)
+{
+    uint32_t carry = 0;
+    for (uint32_t chunk = 0; chunk < n; chunk += kScanChunk) {
+        const uint32_t base = chunk + threadIdx.x * kScanItems;
+        uint32_t vals[kScanItems];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) {
+            const uint32_t idx = base + i;
+            vals[i] = idx < n ? in[idx] : 0u;
+            sum += vals[i];
+        }
+        uint32_t t;
+        uint32_t prefix = blockExclusiveScan(sum, t) + carry;
+#pragma unroll
+        for (int i = 0; i < kScanItems; ++i) {
+            const uint32_t idx = base + i;
+            if (idx < n) out[idx] = prefix;
+            prefix += vals[i];
+        }
+        carry += t;
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+
 } // namespace
 
 size_t radixSortScratchBytes(uint32_t n)
@@ -371,6 +401,10 @@ void exclusiveScan(const uint32_t *in, uint32_t *out, uint32_t n, uint32_t *tota
 {
     if (n == 0) {
         if (total) cudaMemsetAsync(total, 0, sizeof(uint32_t), st);
+        return;
+    }
+    if (n <= kScanSingleMax) {
+        k_scanSingle<<<1, kScanThreads, 0, st>>>(in, n, out, total);
         return;
     }
     uint32_t *partials = static_cast<uint32_t *>(scratch);
