@@ -385,28 +385,45 @@ def run_served(args, stream, sh, rank: int = 0, world: int = 1) -> dict:
         sv.close()
     del solvers
 
-    # batched: every scene resident, autotuned schedule, saturated ticks
+    # batched: every scene resident, created with colour tables so that the autotuner times the
+    # gather schedule (per-phase and fused) against colour Jacobi; saturated ticks
+    from cn_physics._abi import XPBD_COLOUR_JACOBI, XPBD_GATHER
     budget = 120 << 30
-    bd = batch_desc(desc, memory_budget_bytes=budget, max_scenes=len(pool) + 8, particle_capacity=P + 4096,
+    bdesc = type(desc).from_buffer_copy(desc)
+    bdesc.soft.xpbd_schedule = XPBD_COLOUR_JACOBI
+    bd = batch_desc(bdesc, memory_budget_bytes=budget, max_scenes=len(pool) + 8, particle_capacity=P + 4096,
                     edge_capacity=E + 4096, tet_capacity=T + 4096)
     b = Batch(bd)
     ids = [b.add_scene(sc.world.soa()) for sc in pool]
     tune = b.autotune(ids, dt)
-    b.step(ids, dt, sh)
-    torch.cuda.synchronize()
-    ticks = []
-    for _ in range(5):
-        if world > 1:
-            dist.barrier()
-        ev[0].record(stream)
+
+    def time_ticks(n=5):
         b.step(ids, dt, sh)
-        ev[1].record(stream)
         torch.cuda.synchronize()
-        ticks.append(max_over_ranks(ev[0].elapsed_time(ev[1]), world))
+        out = []
+        for _ in range(n):
+            if world > 1:
+                dist.barrier()
+            ev[0].record(stream)
+            b.step(ids, dt, sh)
+            ev[1].record(stream)
+            torch.cuda.synchronize()
+            out.append(max_over_ranks(ev[0].elapsed_time(ev[1]), world))
+        return out
+
+    ticks = time_ticks()
     tick_ms = float(np.median(ticks))
+    # both schedules at the tuned tile shape, per-phase kernels (the state moves on: timing only)
+    by_schedule = {}
+    b.set_fused(0)
+    for name, sched in (("gather", XPBD_GATHER), ("colour_jacobi", XPBD_COLOUR_JACOBI)):
+        b.set_xpbd_schedule(sched)
+        by_schedule[name] = round(float(np.median(time_ticks(3))), 3)
     b.close()
 
     # served: a fresh batch (same schedule) behind the server, Poisson load in real time
+    bdesc.soft.xpbd_schedule = tune["xpbd_schedule"]
+    bd.solver = bdesc
     bd.tile_elements, bd.blocks_per_sm = tune["tile_elements"], tune["blocks_per_sm"]
     bd.fused_cluster_ctas = tune["cluster_ctas"]
     b = Batch(bd)
@@ -453,7 +470,10 @@ def run_served(args, stream, sh, rank: int = 0, world: int = 1) -> dict:
         "batched": {"value": round(batched_rate, 1), "tick_ms_p50": round(tick_ms, 3),
                     "tick_ms_max": round(max(ticks), 3), "schedule": {"tile_elements": tune["tile_elements"],
                                                                       "blocks_per_sm": tune["blocks_per_sm"],
-                                                                      "fused_cluster_ctas": tune["cluster_ctas"]},
+                                                                      "fused_cluster_ctas": tune["cluster_ctas"],
+                                                                      "xpbd_schedule": ["gather", "colour_jacobi"][
+                                                                          tune["xpbd_schedule"]]},
+                    "tick_ms_per_phase_by_xpbd_schedule": by_schedule,
                     "autotune_candidates": tune["candidates"]},
         "batched_over_plain": round(batched_rate / plain_rate, 2),
         "served": {"offered_frames_per_s": args.serve_rate, "arrival_window_s": args.serve_seconds,

@@ -678,14 +678,20 @@ class Batch:
         cluster of that many CTAs per scene at a time."""
         _check(self._lib.cn_batch_set_fused(self._h, cluster_ctas))
 
+    def set_xpbd_schedule(self, schedule: int) -> None:
+        """XPBD_GATHER, or (in a batch created with a coloured schedule) XPBD_COLOUR_JACOBI /
+        XPBD_COLOUR_GAUSS_SEIDEL for the next ticks."""
+        _check(self._lib.cn_batch_set_xpbd_schedule(self._h, schedule))
+
     def autotune(self, scenes: Sequence[int], dt: float) -> dict:
         ids = np.ascontiguousarray(np.asarray(scenes, dtype=np.uint32))
         t = _abi.BatchTuning()
         _check(self._lib.cn_batch_autotune(self._h, _u32(ids), ids.size, dt, C.byref(t)))
         return {"tile_elements": t.tile_elements, "blocks_per_sm": t.blocks_per_sm, "tick_ms": t.tick_ms,
-                "cluster_ctas": t.cluster_ctas,
+                "cluster_ctas": t.cluster_ctas, "xpbd_schedule": t.xpbd_schedule,
                 "candidates": [(t.candidates[k].tile_elements, t.candidates[k].blocks_per_sm,
-                                round(t.candidates[k].tick_ms, 4), t.candidates[k].cluster_ctas)
+                                round(t.candidates[k].tick_ms, 4), t.candidates[k].cluster_ctas,
+                                t.candidates[k].xpbd_schedule)
                                for k in range(t.candidate_count)]}
 
 

@@ -239,17 +239,20 @@ class BatchDesc(C.Structure):
 class BatchStats(C.Structure):
     _fields_ = [("resident_scenes", u32), ("particles_used", u32), ("particle_capacity", u32),
                 ("edges_used", u32), ("edge_capacity", u32), ("tets_used", u32), ("tet_capacity", u32),
-                ("tile_elements", u32), ("grid_blocks", u32), ("fused_cluster_ctas", u32), ("budget_bytes", u64),
+                ("tile_elements", u32), ("grid_blocks", u32), ("fused_cluster_ctas", u32), ("xpbd_schedule", u32),
+                ("reserved0", u32), ("budget_bytes", u64),
                 ("budget_used_bytes", u64), ("pool_bytes", u64), ("ticks", u64)]
 
 
 class BatchCandidate(C.Structure):
-    _fields_ = [("tile_elements", u32), ("blocks_per_sm", u32), ("tick_ms", f32), ("cluster_ctas", u32)]
+    _fields_ = [("tile_elements", u32), ("blocks_per_sm", u32), ("tick_ms", f32), ("cluster_ctas", u32),
+                ("xpbd_schedule", u32)]
 
 
 class BatchTuning(C.Structure):
     _fields_ = [("tile_elements", u32), ("blocks_per_sm", u32), ("tick_ms", f32), ("candidate_count", u32),
-                ("candidates", BatchCandidate * 24), ("cluster_ctas", u32), ("reserved", u32 * 3)]
+                ("candidates", BatchCandidate * 24), ("cluster_ctas", u32), ("xpbd_schedule", u32),
+                ("reserved", u32 * 2)]
 
 
 class ServerDesc(C.Structure):
@@ -339,6 +342,7 @@ SIGNATURES = [
     ("cn_batch_get_stats", C.c_int, [C.c_void_p, C.POINTER(BatchStats)]),
     ("cn_batch_set_schedule", C.c_int, [C.c_void_p, u32, u32]),
     ("cn_batch_set_fused", C.c_int, [C.c_void_p, u32]),
+    ("cn_batch_set_xpbd_schedule", C.c_int, [C.c_void_p, u32]),
     ("cn_batch_autotune", C.c_int, [C.c_void_p, P_u32, u32, f32, C.POINTER(BatchTuning)]),
     ("cn_solver_export_dlpack", C.c_int, [C.c_void_p, C.c_char_p, C.POINTER(C.c_void_p)]),
     ("cn_solver_update_world", C.c_int, [C.c_void_p, C.POINTER(WorldSoA), u32]),

@@ -8,7 +8,9 @@
 // writes the tick's work lists (element ranges of the chosen scenes, cut into tiles) and staged
 // kinematic targets, and replays one CUDA graph whose kernels stride over those lists with a
 // fixed grid.  The graph is captured once per frame dt; the tile size and grid are tuned by
-// cn_batch_autotune on the resident scenes.
+// cn_batch_autotune on the resident scenes.  A batch created with a coloured XPBD schedule also
+// holds each scene's edge and tet colourings (made as a solver of its own makes them), and its
+// colour passes run one kernel per colour over all stepped scenes.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -91,7 +93,8 @@ struct Range {
 };
 struct BatchScene {
     bool live = false;
-    Range p, e, t, ei, ti, b, c, ci, m;
+    Range p, e, t, ei, ti, b, c, ci, m, k;
+    uint32_t edgeColours = 0;
     uint32_t queryCount = 0; // colliders in its query order (a prefix-free range starting at c.start)
     uint64_t bytes = 0;
 };
@@ -128,8 +131,13 @@ struct cn_batch {
     size_t arenaBytes = 0;
     uint32_t *scanScratch = nullptr;
     size_t scanScratchBytes = 0;
-    uint32_t P = 0, E = 0, T = 0, B = 0, C = 0, M = 0, pairCap = 0;
-    RangeAlloc aP, aE, aT, aEI, aTI, aB, aC, aCI, aM;
+    uint32_t P = 0, E = 0, T = 0, B = 0, C = 0, M = 0, pairCap = 0, K = 0;
+    RangeAlloc aP, aE, aT, aEI, aTI, aB, aC, aCI, aM, aK;
+    // XPBD schedule: the running one, and whether the pool holds colour tables (a batch created
+    // with a coloured schedule); colours = the most any resident scene's edges / tets need
+    uint32_t schedule = CN_XPBD_GATHER;
+    bool coloured = false;
+    uint32_t colours[2] = {0, 0};
     std::vector<BatchScene> scenes;
     uint64_t bytesAdmitted = 0;
     // work lists: 5 tile regions + 6 counters (5 lists + targets) on the device and in two pinned
@@ -152,8 +160,8 @@ struct cn_batch {
     uint32_t tileElems = 256, blocksPerSm = 8, smCount = 148, grid = 0;
     uint64_t ticks = 0;
     // persistent fused iterations: CTAs per scene cluster (0: per-phase kernels), clusters of the
-    // grid, and the tick's scene list (per stepped scene its particle, edge and tet ranges;
-    // counter 6 = scenes, counter 7 = the next scene to take, both staged with the work lists)
+    // grid; the tick's scene list (cn::kSceneListStride uint2 per stepped scene; counter 6 =
+    // scenes, counter 7 = the next scene to take, both staged with the work lists)
     uint32_t clusterCtas = 0, clusters = 0;
     uint2 *dScenes = nullptr;
     uint2 *hScenes[2] = {nullptr, nullptr};
@@ -215,7 +223,7 @@ cn_status allocWorkLists(cn_batch *b)
         if (b->hScenes[k]) cudaFreeHost(b->hScenes[k]);
     b->dScenes = nullptr;
     b->hScenes[0] = b->hScenes[1] = nullptr;
-    const size_t sceneListBytes = size_t(3) * std::max<uint32_t>(b->desc.max_scenes, 1u) * sizeof(uint2);
+    const size_t sceneListBytes = size_t(cn::kSceneListStride) * std::max<uint32_t>(b->desc.max_scenes, 1u) * sizeof(uint2);
     CN_CUDA(cudaMalloc(&b->dScenes, sceneListBytes));
     for (int k = 0; k < 2; ++k) CN_CUDA(cudaMallocHost(&b->hScenes[k], sceneListBytes));
     CN_CUDA(cudaMalloc(&b->dTiles, size_t(b->tileTotal) * sizeof(uint2)));
@@ -283,6 +291,12 @@ void layoutPool(cn_batch *b, cn::Arena &a)
     s.rigidPairs = a.take<uint2>(b->pairCap);
     s.rigidContacts = a.take<cn::RigidContact>(b->pairCap);
     s.meta_ = a.take<cn::DeviceMeta>(1);
+    if (b->coloured) {
+        s.colOrder[cn::kFamEdges] = a.take<uint32_t>(E);
+        s.colOrder[cn::kFamTets] = a.take<uint32_t>(T);
+        s.softAcc = a.take<float4>(P);
+        s.batchColStarts = a.take<uint32_t>(b->K);
+    }
     b->scanScratchBytes = (size_t(2) * P + 4) * sizeof(uint32_t) + cn::scanScratchBytes(std::max<uint32_t>(P, 1u));
     b->scanScratch = a.take<uint32_t>(b->scanScratchBytes / sizeof(uint32_t));
 }
@@ -318,6 +332,14 @@ void enqueueTick(cn_batch *b, float frameDt, cudaStream_t st)
             const bool runSoft = (s.E || s.T) && it < b->softIt;
             const bool runRigid = it < b->contactIt;
             if (!runSoft && !runRigid) break;
+            if (b->schedule != CN_XPBD_GATHER) {
+                // one kernel per colour over every stepped scene, then the contacts
+                if (runSoft)
+                    cn::launchBatchColourIteration(s, dt, c, b->schedule, b->colours, b->dScenes, b->dCounts + 6,
+                                                   b->grid, st);
+                if (runRigid) cn::launchContacts(s, c, false, true, st);
+                continue;
+            }
             // the rigid contacts run in the tet gather's pass when there is a tet family
             const bool contactsDone = runSoft && cn::launchSoftIteration(s, dt, c, st, runRigid);
             if (runRigid && !contactsDone) cn::launchContacts(s, c, false, true, st);
@@ -361,6 +383,7 @@ void releaseScene(cn_batch *b, BatchScene &sc)
     b->aC.release(sc.c.start, sc.c.count);
     b->aCI.release(sc.ci.start, sc.ci.count);
     b->aM.release(sc.m.start, sc.m.count);
+    b->aK.release(sc.k.start, sc.k.count);
     b->bytesAdmitted -= sc.bytes;
     sc = BatchScene{};
 }
@@ -369,7 +392,7 @@ void releaseScene(cn_batch *b, BatchScene &sc)
 
 namespace cn {
 
-cn_status buildSceneImage(const cn_world_soa &w, uint32_t rigidPairsPerParticle, SceneImage &img)
+cn_status buildSceneImage(const cn_world_soa &w, uint32_t rigidPairsPerParticle, bool coloured, SceneImage &img)
 {
     const uint32_t N = w.particle_count;
     if (N == 0) return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_add_scene: empty scene");
@@ -403,9 +426,33 @@ cn_status buildSceneImage(const cn_world_soa &w, uint32_t rigidPairsPerParticle,
     const Incidence tetI = buildIncidence(N, w.tet_count, 4, [&](uint32_t c, uint32_t k) {
         return w.tets[c].particle_indices[k];
     });
+    // coloured schedules: the colourings a solver of this scene makes, and per family the words
+    // colours, particle window, colour starts
+    Colouring edgeCol, tetCol;
+    std::vector<uint32_t> colWords;
+    if (coloured) {
+        edgeCol = colourGreedy(N, w.edge_count, 2, [&](uint32_t c, uint32_t k) {
+            return k == 0 ? w.edges[c].particle_a : w.edges[c].particle_b;
+        });
+        tetCol = colourGreedy(N, w.tet_count, 4, [&](uint32_t c, uint32_t k) { return w.tets[c].particle_indices[k]; });
+        if (edgeCol.colours() > kBatchMaxColours || tetCol.colours() > kBatchMaxColours)
+            return setError(CN_ERR_UNSUPPORTED, "cn_batch_add_scene: more than " + std::to_string(kBatchMaxColours) +
+                                                    " colours in one constraint family");
+        const Colouring *fam[2] = {&edgeCol, &tetCol};
+        const uint2 win[2] = {incidenceWindow(edgeI), incidenceWindow(tetI)};
+        for (int f = 0; f < 2; ++f) {
+            colWords.push_back(fam[f]->colours());
+            colWords.push_back(win[f].x);
+            colWords.push_back(win[f].y);
+            if (fam[f]->colours()) colWords.insert(colWords.end(), fam[f]->starts.begin(), fam[f]->starts.end());
+            else colWords.push_back(0u);
+        }
+    }
 
     AdmitImage &L = img.layout;
     L = AdmitImage{};
+    img.colours[0] = edgeCol.colours();
+    img.colours[1] = tetCol.colours();
     L.N = N;
     L.E = w.edge_count;
     L.T = w.tet_count;
@@ -414,12 +461,14 @@ cn_status buildSceneImage(const cn_world_soa &w, uint32_t rigidPairsPerParticle,
     L.CI = w.body_collider_index_count;
     L.M = std::max<uint32_t>(w.contact_material_count, 1u);
     L.queryCount = uint32_t(order.size());
+    L.colWords = uint32_t(colWords.size());
     const size_t sizes[kAdmSegments] = {
         16ull * N, 16ull * N, 4ull * N, 4ull * N, 16ull * N, 4ull * N, 4ull * N, 4ull * N, 8ull * N, 8ull * N,
         sizeof(cn_soft_edge) * L.E, 8ull * L.E, sizeof(cn_soft_tet) * L.T, 16ull * L.T, 16ull * L.M,
         16ull * L.B, 16ull * L.B, 16ull * L.B, 16ull * L.B, 16ull * L.B, 16ull * L.B, 4ull * L.B, 16ull * L.B,
         16ull * L.B, 4ull * L.B, 8ull * L.B, 4ull * L.CI, sizeof(cn_collider_geometry) * L.C,
-        sizeof(cn_collider_broadphase) * L.C, 16ull * L.C, 4ull * L.queryCount};
+        sizeof(cn_collider_broadphase) * L.C, 16ull * L.C, 4ull * L.queryCount, 4ull * edgeCol.order.size(),
+        4ull * tetCol.order.size(), 4ull * L.colWords};
     size_t at = 0;
     for (uint32_t k = 0; k < kAdmSegments; ++k) {
         L.off[k] = at;
@@ -451,10 +500,15 @@ cn_status buildSceneImage(const cn_world_soa &w, uint32_t rigidPairsPerParticle,
     put(kAdmColBp, w.collider_broadphase, sizeof(cn_collider_broadphase) * L.C);
     put(kAdmColMat, w.collider_materials, 16ull * L.C);
     put(kAdmQueryOrder, order.data(), 4ull * L.queryCount);
+    put(kAdmEdgeColOrder, edgeCol.order.data(), 4ull * edgeCol.order.size());
+    put(kAdmTetColOrder, tetCol.order.data(), 4ull * tetCol.order.size());
+    put(kAdmColStarts, colWords.data(), 4ull * L.colWords);
     refreshSceneImage(w, img);
     img.budgetBytes = N * kBytesPerParticle + uint64_t(L.E) * kBytesPerEdge + uint64_t(L.T) * kBytesPerTet +
                       uint64_t(L.B) * kBytesPerBody + uint64_t(L.C) * kBytesPerCollider +
                       uint64_t(N) * rigidPairsPerParticle * 72u;
+    if (coloured) // colour orders, the colour-Jacobi sums, the colour tables
+        img.budgetBytes += 4ull * (L.E + L.T) + 16ull * N + 4ull * L.colWords;
     return CN_OK;
 }
 
@@ -478,6 +532,8 @@ void refreshSceneImage(const cn_world_soa &w, SceneImage &img)
 cn_status batchAdmitImage(cn_batch *b, const SceneImage &img, uint32_t *scene_id)
 {
     const AdmitImage &L = img.layout;
+    if ((L.colWords != 0u) != b->coloured)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_add_scene: the scene image does not match the batch's schedule");
     if (b->bytesAdmitted + img.budgetBytes > b->desc.memory_budget_bytes)
         return setError(CN_ERR_CAPACITY, "cn_batch_add_scene: the device-memory budget is full");
     BatchScene sc;
@@ -496,12 +552,24 @@ cn_status batchAdmitImage(cn_batch *b, const SceneImage &img, uint32_t *scene_id
     take(b->aC, L.C, sc.c);
     take(b->aCI, L.CI, sc.ci);
     take(b->aM, L.M, sc.m);
+    take(b->aK, L.colWords, sc.k);
     if (!ok) {
         releaseScene(b, sc);
         return setError(CN_ERR_CAPACITY, "cn_batch_add_scene: the pool has no room for this scene");
     }
     sc.live = true;
     sc.queryCount = L.queryCount;
+    if (b->coloured) {
+        const uint32_t ce = img.colours[0], ct = img.colours[1];
+        sc.edgeColours = ce;
+        if (ce > b->colours[0] || ct > b->colours[1]) { // the tick's graph runs more colour passes
+            b->colours[0] = std::max(b->colours[0], ce);
+            b->colours[1] = std::max(b->colours[1], ct);
+            CN_CUDA(cudaSetDevice(b->device));
+            CN_CUDA(cudaDeviceSynchronize()); // no tick of the old graph in flight
+            releaseGraph(b);
+        }
+    }
     sc.bytes = img.budgetBytes;
     b->bytesAdmitted += img.budgetBytes;
     CN_CUDA(cudaSetDevice(b->device));
@@ -521,7 +589,7 @@ cn_status batchAdmitImage(cn_batch *b, const SceneImage &img, uint32_t *scene_id
     AdmitImage a = L;
     a.img = b->dStage;
     a.p0 = sc.p.start; a.e0 = sc.e.start; a.t0 = sc.t.start; a.ei0 = sc.ei.start; a.ti0 = sc.ti.start;
-    a.b0 = sc.b.start; a.c0 = sc.c.start; a.ci0 = sc.ci.start; a.m0 = sc.m.start;
+    a.b0 = sc.b.start; a.c0 = sc.c.start; a.ci0 = sc.ci.start; a.m0 = sc.m.start; a.k0 = sc.k.start;
     launchAdmitScene(b->s, a, b->upStream);
     CN_CUDA(cudaGetLastError());
     CN_CUDA(cudaEventRecord(b->upDone, b->upStream));
@@ -536,6 +604,7 @@ cn_status batchAdmitImage(cn_batch *b, const SceneImage &img, uint32_t *scene_id
 }
 
 uint32_t batchRigidPairsPerParticle(const cn_batch *b) { return b->desc.rigid_pairs_per_particle; }
+bool batchColoured(const cn_batch *b) { return b->coloured; }
 
 } // namespace cn
 
@@ -564,9 +633,14 @@ CN_API cn_status cn_batch_create(const cn_batch_desc *d, int device, cn_batch **
         return setError(CN_ERR_NO_DEVICE, "cn_batch_create: no CUDA device");
     }
     if (device < 0 || device >= count) return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_create: bad device");
-    if (d->solver.soft.xpbd_schedule != CN_XPBD_GATHER)
-        return setError(CN_ERR_UNSUPPORTED, "cn_batch_create: a batch runs the gather XPBD schedule");
+    const uint32_t schedule = d->solver.soft.xpbd_schedule;
+    if (schedule > CN_XPBD_COLOUR_GAUSS_SEIDEL)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_create: unknown soft.xpbd_schedule");
+    if (schedule != CN_XPBD_GATHER && d->fused_cluster_ctas)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_create: the fused iterations run the gather schedule");
     auto *b = new cn_batch();
+    b->schedule = schedule;
+    b->coloured = schedule != CN_XPBD_GATHER;
     b->desc = *d;
     b->device = device;
     CN_CUDA(cudaSetDevice(device));
@@ -593,6 +667,10 @@ CN_API cn_status cn_batch_create(const cn_batch_desc *d, int device, cn_batch **
     b->pairCap = std::max<uint32_t>(P * std::max<uint32_t>(d->rigid_pairs_per_particle, 1u), 64u);
     b->aP.reset(P); b->aE.reset(E); b->aT.reset(T); b->aEI.reset(E * 2u); b->aTI.reset(T * 4u);
     b->aB.reset(B); b->aC.reset(C); b->aCI.reset(C); b->aM.reset(b->M);
+    // colour-table words: a scene takes edge colours + tet colours + 8 <= its edges + tets + 8
+    // particles' worth
+    b->K = b->coloured ? uint32_t(std::min<uint64_t>(8ull * P + uint64_t(E) + T, 0xffffffffull)) : 0u;
+    b->aK.reset(b->K);
     cn::Arena a;
     a.reset(nullptr);
     layoutPool(b, a);
@@ -671,7 +749,7 @@ CN_API cn_status cn_batch_add_scene(cn_batch *b, const cn_world_soa *w, uint32_t
 {
     if (!b || !w || !scene_id) return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_add_scene: null argument");
     cn::SceneImage img;
-    const cn_status st = cn::buildSceneImage(*w, b->desc.rigid_pairs_per_particle, img);
+    const cn_status st = cn::buildSceneImage(*w, b->desc.rigid_pairs_per_particle, b->coloured, img);
     if (st != CN_OK) return st;
     return cn::batchAdmitImage(b, img, scene_id);
 }
@@ -737,9 +815,11 @@ CN_API cn_status cn_batch_step(cn_batch *b, const uint32_t *scene_ids, uint32_t 
         if (id >= b->scenes.size() || !b->scenes[id].live)
             return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_step: scene " + std::to_string(id) + " is not resident");
         const BatchScene &sc = b->scenes[id];
-        sceneList[3 * n] = make_uint2(sc.p.start, sc.p.start + sc.p.count);
-        sceneList[3 * n + 1] = make_uint2(sc.e.start, sc.e.start + sc.e.count);
-        sceneList[3 * n + 2] = make_uint2(sc.t.start, sc.t.start + sc.t.count);
+        uint2 *row = sceneList + size_t(cn::kSceneListStride) * n;
+        row[0] = make_uint2(sc.p.start, sc.p.start + sc.p.count);
+        row[1] = make_uint2(sc.e.start, sc.e.start + sc.e.count);
+        row[2] = make_uint2(sc.t.start, sc.t.start + sc.t.count);
+        row[3] = make_uint2(sc.k.start, sc.k.start + sc.edgeColours + 4u); // edge, tet colour tables
         const Range fam[5] = {sc.p, sc.e, sc.t, sc.b, sc.c};
         for (int f = 0; f < 5; ++f) {
             const uint32_t step = f >= 3 ? std::max<uint32_t>(fam[f].count, 1u) : te;
@@ -767,8 +847,9 @@ CN_API cn_status cn_batch_step(cn_batch *b, const uint32_t *scene_ids, uint32_t 
                                     cudaMemcpyHostToDevice, st));
     CN_CUDA(cudaMemcpyAsync(b->dCounts, counts, 8 * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     if (nt) CN_CUDA(cudaMemcpyAsync(b->dTargets, targets, size_t(nt) * sizeof(cn::BodyTarget), cudaMemcpyHostToDevice, st));
-    if (count && b->clusterCtas)
-        CN_CUDA(cudaMemcpyAsync(b->dScenes, sceneList, size_t(3) * count * sizeof(uint2), cudaMemcpyHostToDevice, st));
+    if (count && (b->clusterCtas || b->schedule != CN_XPBD_GATHER))
+        CN_CUDA(cudaMemcpyAsync(b->dScenes, sceneList, size_t(cn::kSceneListStride) * count * sizeof(uint2),
+                                cudaMemcpyHostToDevice, st));
     CN_CUDA(cudaEventRecord(b->stageDone[k], st));
     CN_CUDA(cudaGraphLaunch(b->graphExec, st));
     CN_CUDA(cudaGetLastError());
@@ -831,6 +912,24 @@ CN_API cn_status cn_batch_get_stats(cn_batch *b, cn_batch_stats *out)
     out->tile_elements = b->tileElems;
     out->grid_blocks = b->grid;
     out->fused_cluster_ctas = b->clusterCtas;
+    out->xpbd_schedule = b->schedule;
+    return CN_OK;
+}
+
+CN_API cn_status cn_batch_set_xpbd_schedule(cn_batch *b, uint32_t schedule)
+{
+    if (!b) return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_set_xpbd_schedule: null batch");
+    if (schedule > CN_XPBD_COLOUR_GAUSS_SEIDEL)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_set_xpbd_schedule: unknown schedule");
+    if (schedule != CN_XPBD_GATHER && !b->coloured)
+        return setError(CN_ERR_UNSUPPORTED, "cn_batch_set_xpbd_schedule: the batch was created without colour tables");
+    if (schedule != CN_XPBD_GATHER && b->clusterCtas)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_set_xpbd_schedule: the fused iterations run the gather schedule");
+    if (schedule == b->schedule) return CN_OK;
+    CN_CUDA(cudaSetDevice(b->device));
+    CN_CUDA(cudaDeviceSynchronize());
+    b->schedule = schedule;
+    releaseGraph(b);
     return CN_OK;
 }
 
@@ -839,6 +938,8 @@ CN_API cn_status cn_batch_set_fused(cn_batch *b, uint32_t cluster_ctas)
     if (!b) return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_set_fused: null batch");
     if (cluster_ctas != 0u && cluster_ctas != 1u && cluster_ctas != 2u && cluster_ctas != 4u && cluster_ctas != 8u)
         return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_set_fused: cluster_ctas is 0, 1, 2, 4 or 8");
+    if (cluster_ctas && b->schedule != CN_XPBD_GATHER)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_set_fused: the fused iterations run the gather schedule");
     CN_CUDA(cudaSetDevice(b->device));
     CN_CUDA(cudaDeviceSynchronize());
     uint32_t clusters = 0;
@@ -866,8 +967,8 @@ CN_API cn_status cn_batch_set_schedule(cn_batch *b, uint32_t tile_elements, uint
     return allocWorkLists(b);
 }
 
-// Times one tick of the given scenes under each (tile size, blocks per SM) candidate and keeps
-// the fastest.  Each candidate's ticks run on copies of the state that are then discarded: the
+// Times one tick of the given scenes under each (tile size, blocks per SM) candidate, the fused
+// iterations and, in a colour-Jacobi batch, colour Jacobi, and keeps the fastest.  Each candidate's ticks run on copies of the state that are then discarded: the
 // scenes' particles, velocities and bodies are restored afterwards.
 CN_API cn_status cn_batch_autotune(cn_batch *b, const uint32_t *scene_ids, uint32_t count, float frame_dt,
                                    cn_batch_tuning *out)
@@ -900,7 +1001,9 @@ CN_API cn_status cn_batch_autotune(cn_batch *b, const uint32_t *scene_ids, uint3
     const uint32_t blocks[] = {4, 8, 16, 32};
     const uint32_t clusterSizes[] = {1, 2, 4, 8};
     float best = 1e30f;
-    uint32_t bestTile = b->tileElems, bestBlocks = b->blocksPerSm, bestCtas = 0;
+    uint32_t bestTile = b->tileElems, bestBlocks = b->blocksPerSm, bestCtas = 0, bestSchedule = b->schedule;
+    const uint32_t created = b->desc.solver.soft.xpbd_schedule;
+    const uint32_t tileSchedule = created == CN_XPBD_COLOUR_GAUSS_SEIDEL ? created : uint32_t(CN_XPBD_GATHER);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -908,7 +1011,7 @@ CN_API cn_status cn_batch_autotune(cn_batch *b, const uint32_t *scene_ids, uint3
     uint32_t n = 0;
     const uint32_t capacity = uint32_t(sizeof(out->candidates) / sizeof(out->candidates[0]));
     // warm-up (capture + first replay), then three timed ticks; the state is restored after
-    auto trial = [&](uint32_t te, uint32_t bps, uint32_t ctas) -> cn_status {
+    auto trial = [&](uint32_t te, uint32_t bps, uint32_t ctas, uint32_t schedule) -> cn_status {
         cn_status st = cn_batch_step(b, scene_ids, count, frame_dt, b->ownStream);
         if (st != CN_OK) return st;
         cudaEventRecord(e0, b->ownStream);
@@ -918,32 +1021,43 @@ CN_API cn_status cn_batch_autotune(cn_batch *b, const uint32_t *scene_ids, uint3
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, e0, e1);
         ms /= 3.0f;
-        if (n < capacity) out->candidates[n++] = cn_batch_candidate{te, bps, ms, ctas};
+        if (n < capacity) out->candidates[n++] = cn_batch_candidate{te, bps, ms, ctas, schedule};
         if (ms < best) {
             best = ms;
             bestTile = te;
             bestBlocks = bps;
             bestCtas = ctas;
+            bestSchedule = schedule;
         }
         const cudaError_t e = save(false);
         return e == cudaSuccess ? CN_OK : setError(CN_ERR_CUDA, std::string("cn_batch_autotune: ") + cudaGetErrorString(e));
     };
     cn_status st = cn_batch_set_fused(b, 0);
+    if (st == CN_OK) st = cn_batch_set_xpbd_schedule(b, tileSchedule);
     for (uint32_t te : tiles)
         for (uint32_t bps : blocks) {
             if (st == CN_OK) st = cn_batch_set_schedule(b, te, bps);
-            if (st == CN_OK) st = trial(te, bps, 0);
+            if (st == CN_OK) st = trial(te, bps, 0, tileSchedule);
         }
-    // the persistent fused iterations, with the other phases at the best tile schedule so far
+    // the persistent fused iterations (gather), with the other phases at the best tile schedule
     const uint32_t tileForFused = bestTile, blocksForFused = bestBlocks;
     if (st == CN_OK) st = cn_batch_set_schedule(b, tileForFused, blocksForFused);
     for (uint32_t ctas : clusterSizes) {
-        if (st != CN_OK) break;
+        if (st != CN_OK || tileSchedule != CN_XPBD_GATHER) break;
         if (cn_batch_set_fused(b, ctas) != CN_OK) {
             cn::clearError(); // clusters of this size cannot be formed: not a candidate
             continue;
         }
-        st = trial(tileForFused, blocksForFused, ctas);
+        st = trial(tileForFused, blocksForFused, ctas, CN_XPBD_GATHER);
+    }
+    // colour Jacobi at the best tile size, its colour passes over grids of 4 .. 32 blocks per SM
+    if (st == CN_OK && created == CN_XPBD_COLOUR_JACOBI) {
+        st = cn_batch_set_fused(b, 0);
+        if (st == CN_OK) st = cn_batch_set_xpbd_schedule(b, CN_XPBD_COLOUR_JACOBI);
+        for (uint32_t bps : blocks) {
+            if (st == CN_OK) st = cn_batch_set_schedule(b, tileForFused, bps);
+            if (st == CN_OK) st = trial(tileForFused, bps, 0, CN_XPBD_COLOUR_JACOBI);
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -951,7 +1065,10 @@ CN_API cn_status cn_batch_autotune(cn_batch *b, const uint32_t *scene_ids, uint3
     out->tile_elements = bestTile;
     out->blocks_per_sm = bestBlocks;
     out->cluster_ctas = bestCtas;
+    out->xpbd_schedule = bestSchedule;
     out->tick_ms = best;
+    if (st == CN_OK) st = cn_batch_set_fused(b, 0);
+    if (st == CN_OK) st = cn_batch_set_xpbd_schedule(b, bestSchedule);
     if (st == CN_OK) st = cn_batch_set_schedule(b, bestTile, bestBlocks);
     if (st == CN_OK) st = cn_batch_set_fused(b, bestCtas);
     CN_CUDA(save(false));

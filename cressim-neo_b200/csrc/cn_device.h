@@ -150,6 +150,9 @@ struct Scene {
     const uint32_t *colOrder[kFamilies] = {};
     float4 *softAcc = nullptr;
     float4 *orientAcc = nullptr;
+    // a batch's colour tables, per admitted scene and family (edges, then tets) a run of words:
+    // colours, the family's particle window [lo, hi), then colours + 1 starts (scene-local)
+    uint32_t *batchColStarts = nullptr;
 
     // ---- rigid bodies / colliders ----
     uint32_t B = 0, C = 0;
@@ -401,9 +404,13 @@ struct FusedShape {
     uint32_t ctas = 0, threads = 0;
 };
 FusedShape fusedIterationsShape();
+// A batch tick's stepped scenes: kSceneListStride uint2 per scene -- its particle, edge and tet
+// ranges [x, y), then the word offsets of its edge and tet colour tables in Scene::batchColStarts.
+constexpr uint32_t kSceneListStride = 4u;
+constexpr uint32_t kBatchMaxColours = 256u;
+constexpr uint32_t kColWordsHeader = 3u; // colours, window lo, window hi
 // A batch tick's iterations as one persistent kernel (cn_batch): `clusters` clusters of `ctas`
-// CTAs, each taking stepped scenes from `next` (zero at the tick's start) until `sceneCount`;
-// scenes[3 j .. 3 j + 2] = scene j's particle, edge and tet ranges [x, y).
+// CTAs, each taking stepped scenes from `next` (zero at the tick's start) until `sceneCount`.
 struct BatchFusedPlan {
     uint32_t iterations, softIterations, contactIterations;
     const uint2 *scenes;
@@ -414,6 +421,12 @@ struct BatchFusedPlan {
 uint32_t batchFusedClusters(uint32_t ctas);
 void launchBatchFusedIterations(const Scene &s, const Config &c, float dt, const BatchFusedPlan &plan, uint32_t ctas,
                                 uint32_t clusters, cudaStream_t st);
+// One iteration of a batch's edge and tet families under a coloured schedule: per family and
+// colour k < maxColours[family] one kernel over the stepped scenes (`scenes`, `sceneCount`), the
+// grid's blocks split evenly over the scenes' colour-k constraints; colour Jacobi then adds each
+// scene's sums to x over the family's particle window.
+void launchBatchColourIteration(const Scene &s, float dt, const Config &c, uint32_t schedule, const uint32_t maxColours[2],
+                                const uint2 *scenes, const uint32_t *sceneCount, uint32_t grid, cudaStream_t st);
 void launchFusedIterations(const Scene &s, const Config &c, float dt, const XpbdPlan &plan, uint32_t iterations,
                            uint32_t softIterations, uint32_t contactIterations, bool rigid, const FusedShape &shape,
                            cudaStream_t st);
@@ -443,13 +456,15 @@ enum AdmitSegment : uint32_t {
     kAdmX, kAdmV, kAdmRadii, kAdmKinds, kAdmMeta, kAdmMatIdx, kAdmOwnerTypes, kAdmOwnerIdx, kAdmEdgeRanges,
     kAdmTetRanges, kAdmEdges, kAdmEdgeDst, kAdmTets, kAdmTetDst, kAdmMaterials, kAdmBodyPos, kAdmBodyRot,
     kAdmBodyLin, kAdmBodyAng, kAdmBodyScale, kAdmBodyInvI, kAdmBodyType, kAdmKinPos, kAdmKinRot, kAdmKinFlags,
-    kAdmBodyColRanges, kAdmBodyColIdx, kAdmColGeo, kAdmColBp, kAdmColMat, kAdmQueryOrder, kAdmSegments
+    kAdmBodyColRanges, kAdmBodyColIdx, kAdmColGeo, kAdmColBp, kAdmColMat, kAdmQueryOrder, kAdmEdgeColOrder,
+    kAdmTetColOrder, kAdmColStarts, kAdmSegments
 };
 struct AdmitImage {
     const uint8_t *img = nullptr;          // the staging copy on the device
     uint64_t off[kAdmSegments] = {};       // byte offset of each segment
     uint32_t N = 0, E = 0, T = 0, B = 0, C = 0, CI = 0, M = 0, queryCount = 0;
     uint32_t p0 = 0, e0 = 0, t0 = 0, ei0 = 0, ti0 = 0, b0 = 0, c0 = 0, ci0 = 0, m0 = 0; // pool offsets
+    uint32_t colWords = 0, k0 = 0;         // colour-table words (0: none) and their pool offset
 };
 void launchAdmitScene(const Scene &s, const AdmitImage &a, cudaStream_t st);
 

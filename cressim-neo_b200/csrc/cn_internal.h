@@ -82,6 +82,17 @@ template <class F> Incidence buildIncidence(uint32_t n, uint32_t constraints, ui
         }
     return out;
 }
+// The particles a family touches, as one window [lo, hi) over its incidence ranges ((0, 0) when none).
+inline uint2 incidenceWindow(const Incidence &I)
+{
+    uint32_t lo = uint32_t(I.ranges.size()), hi = 0;
+    for (uint32_t i = 0; i < I.ranges.size(); ++i)
+        if (I.ranges[i].y) {
+            lo = std::min(lo, i);
+            hi = i + 1;
+        }
+    return lo < hi ? make_uint2(lo, hi) : make_uint2(0u, 0u);
+}
 
 // Greedy graph colouring of one constraint family: constraint c, in ascending order, takes the
 // lowest colour no earlier constraint sharing one of its elements has (elementOf(c, k) >= n is
@@ -139,13 +150,17 @@ struct SceneImage {
     std::vector<uint8_t> bytes;
     AdmitImage layout;
     uint64_t budgetBytes = 0;
+    uint32_t colours[2] = {0, 0}; // edge and tet colours (coloured schedules)
 };
-cn_status buildSceneImage(const cn_world_soa &w, uint32_t rigidPairsPerParticle, SceneImage &img);
+// `coloured`: the image also carries the scene's edge and tet colourings (a batch created with a
+// coloured XPBD schedule).
+cn_status buildSceneImage(const cn_world_soa &w, uint32_t rigidPairsPerParticle, bool coloured, SceneImage &img);
 // Copies the mutable state (particles, bodies, kinematic targets) of `w` into the image.
 void refreshSceneImage(const cn_world_soa &w, SceneImage &img);
 // Admits the image into the batch (ranges, one transfer, the device-side scatter).
 cn_status batchAdmitImage(cn_batch *b, const SceneImage &img, uint32_t *scene_id);
 uint32_t batchRigidPairsPerParticle(const cn_batch *b);
+bool batchColoured(const cn_batch *b);
 
 // Solver constants of one substep, from the PhysicsSolverDesc mirror.
 inline Config configFromDesc(const cn_solver_desc &d)

@@ -3100,7 +3100,8 @@ __global__ void __launch_bounds__(kBatchFusedThreads, 2) k_batchFusedIterations(
         const uint32_t j = *cl.map_shared_rank(&taken, 0);
         cl.sync(); // every thread has its copy before the leader takes the next one
         if (j >= count) break;
-        const uint2 pr = plan.scenes[3u * j], er = plan.scenes[3u * j + 1u], tr = plan.scenes[3u * j + 2u];
+        const uint2 pr = plan.scenes[kSceneListStride * j], er = plan.scenes[kSceneListStride * j + 1u],
+                    tr = plan.scenes[kSceneListStride * j + 2u];
         for (uint32_t it = 0; it < plan.iterations; ++it) {
             if ((s.E || s.T) && it < plan.softIterations) {
                 if (s.E) {
@@ -3294,12 +3295,85 @@ __global__ void __launch_bounds__(kThreads) k_admitScene(Scene s, AdmitImage a)
         const_cast<float4 *>(s.colMat)[c] = f4(kAdmColMat)[i];
     }
     if (i < a.queryCount) const_cast<uint32_t *>(s.colQueryOrder)[a.c0 + i] = u32(kAdmQueryOrder)[i] + a.c0;
+    if (a.colWords) {
+        if (i < a.E) const_cast<uint32_t *>(s.colOrder[kFamEdges])[a.e0 + i] = u32(kAdmEdgeColOrder)[i] + a.e0;
+        if (i < a.T) const_cast<uint32_t *>(s.colOrder[kFamTets])[a.t0 + i] = u32(kAdmTetColOrder)[i] + a.t0;
+        if (i < a.colWords) s.batchColStarts[a.k0 + i] = u32(kAdmColStarts)[i];
+    }
 }
 
 void launchAdmitScene(const Scene &s, const AdmitImage &a, cudaStream_t st)
 {
-    const uint32_t n = std::max({a.N, a.E, a.T, a.B, a.C, a.CI, a.M, a.queryCount, 1u});
+    const uint32_t n = std::max({a.N, a.E, a.T, a.B, a.C, a.CI, a.M, a.queryCount, a.colWords, 1u});
     k_admitScene<<<blocksFor(n), kThreads, 0, st>>>(s, a);
+}
+
+// The blocks of a batch colour pass: `chunks` blocks per stepped scene (the grid split evenly),
+// block w taking scene w / chunks and every chunks-th stride of its range.
+template <class F>
+__device__ __forceinline__ void forSceneChunks(const uint32_t *sceneCount, F &&f)
+{
+    const uint32_t n = *sceneCount;
+    if (n == 0u) return;
+    const uint32_t chunks = max(gridDim.x / n, 1u);
+    for (uint32_t w = blockIdx.x; w < n * chunks; w += gridDim.x) f(w / chunks, w % chunks, chunks);
+}
+
+// Colour k of one family over a batch tick's stepped scenes: each scene's colour-k range of its
+// colour order (global constraint indices), scenes with fewer colours skipped.
+template <uint32_t kFam, bool kGaussSeidel>
+__global__ void __launch_bounds__(kThreads) k_colourSolveBatch(Scene s, float dt, float relax, uint32_t k,
+                                                               const uint2 *scenes, const uint32_t *sceneCount)
+{
+    pdlEnter();
+    forSceneChunks(sceneCount, [&](uint32_t j, uint32_t part, uint32_t chunks) {
+        const uint2 range = scenes[kSceneListStride * j + (kFam == kFamEdges ? 1u : 2u)];
+        const uint2 bases = scenes[kSceneListStride * j + 3u];
+        const uint32_t *words = s.batchColStarts + (kFam == kFamEdges ? bases.x : bases.y);
+        if (k >= words[0]) return;
+        const uint32_t *starts = words + kColWordsHeader;
+        const uint32_t b = range.x + starts[k], e = range.x + starts[k + 1u];
+        for (uint32_t q = b + part * blockDim.x + threadIdx.x; q < e; q += chunks * blockDim.x)
+            colourConstraint<kFam>(s, dt, relax, kGaussSeidel, s.colOrder[kFam][q]);
+    });
+}
+
+// End of a batch colour-Jacobi family: each stepped scene's sums added over the family's window.
+template <uint32_t kFam>
+__global__ void __launch_bounds__(kThreads) k_colourJacobiApplyBatch(Scene s, const uint2 *scenes,
+                                                                     const uint32_t *sceneCount)
+{
+    pdlEnter();
+    forSceneChunks(sceneCount, [&](uint32_t j, uint32_t part, uint32_t chunks) {
+        const uint32_t p0 = scenes[kSceneListStride * j].x;
+        const uint2 bases = scenes[kSceneListStride * j + 3u];
+        const uint32_t *words = s.batchColStarts + (kFam == kFamEdges ? bases.x : bases.y);
+        if (words[0] == 0u) return;
+        const uint32_t b = p0 + words[1], e = p0 + words[2];
+        for (uint32_t i = b + part * blockDim.x + threadIdx.x; i < e; i += chunks * blockDim.x)
+            colourJacobiApplyAt(s, i);
+    });
+}
+
+template <uint32_t kFam>
+void launchBatchColourFamily(const Scene &s, float dt, float relax, bool gs, uint32_t colours, const uint2 *scenes,
+                             const uint32_t *sceneCount, uint32_t grid, cudaStream_t st)
+{
+    if ((kFam == kFamEdges ? s.E : s.T) == 0u) return;
+    for (uint32_t k = 0; k < colours; ++k) {
+        if (gs) launchPdl(k_colourSolveBatch<kFam, true>, grid, kThreads, st, s, dt, relax, k, scenes, sceneCount);
+        else launchPdl(k_colourSolveBatch<kFam, false>, grid, kThreads, st, s, dt, relax, k, scenes, sceneCount);
+    }
+    if (!gs) launchPdl(k_colourJacobiApplyBatch<kFam>, grid, kThreads, st, s, scenes, sceneCount);
+}
+
+void launchBatchColourIteration(const Scene &s, float dt, const Config &c, uint32_t schedule, const uint32_t maxColours[2],
+                                const uint2 *scenes, const uint32_t *sceneCount, uint32_t grid, cudaStream_t st)
+{
+    const bool gs = schedule == CN_XPBD_COLOUR_GAUSS_SEIDEL;
+    const float relax = c.softInternalRelaxation;
+    launchBatchColourFamily<kFamEdges>(s, dt, relax, gs, maxColours[0], scenes, sceneCount, grid, st);
+    launchBatchColourFamily<kFamTets>(s, dt, relax, gs, maxColours[1], scenes, sceneCount, grid, st);
 }
 
 uint32_t batchFusedClusters(uint32_t ctas)

@@ -267,7 +267,8 @@ CN_API cn_status cn_server_register_scene(cn_server *srv, const cn_world_soa *w,
     srv->scenes.push_back(std::make_unique<SceneSlot>());
     SceneSlot &sc = *srv->scenes.back();
     sc.store.assign(*w);
-    sc.imageStatus = cn::buildSceneImage(sc.store.soa, cn::batchRigidPairsPerParticle(srv->batch), sc.image);
+    sc.imageStatus = cn::buildSceneImage(sc.store.soa, cn::batchRigidPairsPerParticle(srv->batch),
+                                          cn::batchColoured(srv->batch), sc.image);
     if (sc.imageStatus != CN_OK) sc.imageError = cn_last_error();
     cn::clearError();
     *scene = uint32_t(srv->scenes.size() - 1);

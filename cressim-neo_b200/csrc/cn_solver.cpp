@@ -931,19 +931,10 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     CN_CUDA(up(s.joints, w->strand_joints, s.J, st));
     CN_CUDA(up(s.dists, w->strand_distances, s.SD, st));
     CN_CUDA(up(s.segOrient, w->strand_segment_orientations, s.S, st));
-    auto window = [](const cn::Incidence &I) {
-        uint32_t lo = uint32_t(I.ranges.size()), hi = 0;
-        for (uint32_t i = 0; i < I.ranges.size(); ++i)
-            if (I.ranges[i].y) {
-                lo = std::min(lo, i);
-                hi = i + 1;
-            }
-        return lo < hi ? make_uint2(lo, hi) : make_uint2(0u, 0u);
-    };
-    s.edgeWin = window(edgeI);
-    s.bendWin = window(bendI);
-    s.tetWin = window(tetI);
-    s.segWin = window(segI);
+    s.edgeWin = cn::incidenceWindow(edgeI);
+    s.bendWin = cn::incidenceWindow(bendI);
+    s.tetWin = cn::incidenceWindow(tetI);
+    s.segWin = cn::incidenceWindow(segI);
     CN_CUDA(up(s.edgeRanges, edgeI.ranges.data(), edgeI.ranges.size(), st));
     CN_CUDA(up(s.bendRanges, bendI.ranges.data(), bendI.ranges.size(), st));
     CN_CUDA(up(s.tetRanges, tetI.ranges.data(), tetI.ranges.size(), st));

@@ -693,7 +693,9 @@ CN_API cn_status cn_solver_debug_read(cn_solver *solver, cn_debug_buffer which, 
 /* edges + tets, static / kinematic colliders) live in one device pool, each  */
 /* in its own index ranges, and any subset of them is stepped by one tick:    */
 /* one CUDA graph whose kernels stride over per-scene work tiles.  A scene    */
-/* stepped in a batch gets the same bits as in a cn_solver of its own.       */
+/* stepped in a batch gets the same bits as in a cn_solver of its own under  */
+/* the same XPBD schedule (solver.soft.xpbd_schedule: gather, or a coloured  */
+/* schedule, for which the pool also holds each scene's colourings).         */
 /* ------------------------------------------------------------------------ */
 typedef struct cn_batch cn_batch;
 
@@ -716,19 +718,24 @@ typedef struct cn_batch_stats {
     uint32_t resident_scenes;
     uint32_t particles_used, particle_capacity, edges_used, edge_capacity, tets_used, tet_capacity;
     uint32_t tile_elements, grid_blocks, fused_cluster_ctas;
+    uint32_t xpbd_schedule, reserved0; /* the running XPBD schedule (CN_XPBD_*) */
     uint64_t budget_bytes, budget_used_bytes, pool_bytes, ticks;
 } cn_batch_stats;
 
 /* cluster_ctas: 0 for the per-phase iteration kernels, else the CTAs per scene of the persistent
- * fused iterations (cn_batch_desc.fused_cluster_ctas). */
-typedef struct cn_batch_candidate { uint32_t tile_elements, blocks_per_sm; float tick_ms; uint32_t cluster_ctas; } cn_batch_candidate;
+ * fused iterations (cn_batch_desc.fused_cluster_ctas); xpbd_schedule: CN_XPBD_*. */
+typedef struct cn_batch_candidate {
+    uint32_t tile_elements, blocks_per_sm;
+    float tick_ms;
+    uint32_t cluster_ctas, xpbd_schedule;
+} cn_batch_candidate;
 typedef struct cn_batch_tuning {
     uint32_t tile_elements, blocks_per_sm;
     float tick_ms;
     uint32_t candidate_count;
     cn_batch_candidate candidates[24];
-    uint32_t cluster_ctas;
-    uint32_t reserved[3];
+    uint32_t cluster_ctas, xpbd_schedule;
+    uint32_t reserved[2];
 } cn_batch_tuning;
 
 CN_API void cn_batch_desc_defaults(cn_batch_desc *desc);
@@ -756,9 +763,16 @@ CN_API cn_status cn_batch_set_schedule(cn_batch *batch, uint32_t tile_elements, 
 /* 0: per-phase iteration kernels; 1, 2, 4 or 8: the persistent fused iterations with clusters of
  * that many CTAs.  CN_ERR_UNSUPPORTED when the device cannot form such clusters. */
 CN_API cn_status cn_batch_set_fused(cn_batch *batch, uint32_t cluster_ctas);
+/* The XPBD schedule of the next ticks: CN_XPBD_GATHER always; a coloured one only in a batch
+ * created with a coloured schedule (CN_ERR_UNSUPPORTED otherwise) and with the per-phase kernels
+ * (cluster_ctas 0). */
+CN_API cn_status cn_batch_set_xpbd_schedule(cn_batch *batch, uint32_t schedule);
 /* Times a tick of `scenes` for each (tile size, blocks per SM) candidate of the per-phase
  * kernels, then for the persistent fused iterations with clusters of 1, 2, 4 and 8 CTAs (at the
- * best tile schedule), keeps the fastest and restores the scenes' state. */
+ * best tile schedule), keeps the fastest and restores the scenes' state.  In a batch created with
+ * colour Jacobi it also times colour Jacobi at the best tile size (its results equal the gather
+ * schedule's up to the order of each particle's sum, within 1e-5); under Gauss-Seidel, a
+ * different iteration, only the tile candidates are timed, all under Gauss-Seidel. */
 CN_API cn_status cn_batch_autotune(cn_batch *batch, const uint32_t *scenes, uint32_t count, float frame_dt,
                                    cn_batch_tuning *out);
 

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from cn_physics import Batch, Server, Solver, batch_desc, serving
+from cn_physics._abi import XPBD_COLOUR_GAUSS_SEIDEL, XPBD_COLOUR_JACOBI, XPBD_GATHER
 from conftest import has_gpu
 
 DT = 1.0 / 60.0
@@ -28,8 +29,14 @@ def targets_for(scene, frames, seed):
     return np.stack(out)
 
 
-def own_solver_run(scene, targets):
-    sv = Solver(serving.serving_solver_desc())
+def solver_desc_with(schedule):
+    d = serving.serving_solver_desc()
+    d.soft.xpbd_schedule = schedule
+    return d
+
+
+def own_solver_run(scene, targets, desc=None):
+    sv = Solver(desc if desc is not None else serving.serving_solver_desc())
     sv.sync_world(scene.world.soa())
     for tg in targets:
         sv.set_kinematic_target(scene.tool, tg[:3], tg[3:])
@@ -37,6 +44,23 @@ def own_solver_run(scene, targets):
     x, v, _ = sv.read_particles()
     sv.close()
     return x, v
+
+
+# Scenes 0 and 2 stepped every tick; 1 and 3 only on some ticks (they catch up afterwards).
+MIXED_TICKS = [[0, 1, 2, 3], [0, 2], [0, 2, 3], [0, 1, 2], [0, 2], [0, 1, 2, 3], [1, 3], [1, 3], [1, 3], [1]]
+
+
+def run_mixed_ticks(b, pool, ids, tg, frames):
+    done = [0] * len(pool)
+    for tick in MIXED_TICKS:
+        step = [k for k in tick if done[k] < frames]
+        for k in step:
+            t = tg[k][done[k]]
+            b.set_kinematic_target(ids[k], pool[k].tool, t[:3], t[3:])
+        b.step([ids[k] for k in step], DT)
+        for k in step:
+            done[k] += 1
+    assert done == [frames] * len(pool)
 
 
 def test_pool_generator_counts():
@@ -78,18 +102,7 @@ def test_batched_scene_equals_its_own_solver_and_is_independent_of_the_mix(clust
                          fused_cluster_ctas=cluster_ctas))
     assert b.stats()["fused_cluster_ctas"] == cluster_ctas
     ids = [b.add_scene(sc.world.soa()) for sc in pool]
-    # scenes 0 and 2 stepped every tick; 1 and 3 only on some ticks (they catch up afterwards)
-    done = [0] * len(pool)
-    schedule = [[0, 1, 2, 3], [0, 2], [0, 2, 3], [0, 1, 2], [0, 2], [0, 1, 2, 3], [1, 3], [1, 3], [1, 3], [1]]
-    for tick in schedule:
-        step = [k for k in tick if done[k] < frames]
-        for k in step:
-            t = tg[k][done[k]]
-            b.set_kinematic_target(ids[k], pool[k].tool, t[:3], t[3:])
-        b.step([ids[k] for k in step], DT)
-        for k in step:
-            done[k] += 1
-    assert done == [frames] * len(pool)
+    run_mixed_ticks(b, pool, ids, tg, frames)
     for k in range(len(pool)):
         x, v = b.read_particles(ids[k])
         assert np.array_equal(x, ref[k][0]) and np.array_equal(v, ref[k][1]), f"scene {k}"
@@ -116,6 +129,83 @@ def test_autotune_keeps_state_and_results():
         x, v = b.read_particles(ids[k])
         assert np.array_equal(x, ref[k][0]) and np.array_equal(v, ref[k][1])
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("schedule", [XPBD_COLOUR_JACOBI, XPBD_COLOUR_GAUSS_SEIDEL])
+def test_batched_scene_equals_its_own_solver_under_coloured_schedules(schedule):
+    """A batch created with a coloured schedule: one kernel per colour over the stepped scenes,
+    each scene's colour-k constraints and colour-Jacobi window its own solver's.  A scene removed
+    and a new one admitted into the freed colour tables also match."""
+    pool = small_pool(5)
+    frames = 5
+    desc = solver_desc_with(schedule)
+    tg = [targets_for(sc, frames, seed=30 + k) for k, sc in enumerate(pool)]
+    ref = [own_solver_run(sc, tg[k], desc) for k, sc in enumerate(pool)]
+    b = Batch(batch_desc(desc, memory_budget_bytes=1 << 30, particle_capacity=30000))
+    assert b.stats()["xpbd_schedule"] == schedule
+    ids = [b.add_scene(sc.world.soa()) for sc in pool[:4]]
+    run_mixed_ticks(b, pool[:4], ids, tg[:4], frames)
+    for k in range(4):
+        x, v = b.read_particles(ids[k])
+        assert np.array_equal(x, ref[k][0]) and np.array_equal(v, ref[k][1]), f"scene {k}"
+    b.remove_scene(ids[1])
+    new = b.add_scene(pool[4].world.soa())
+    for f in range(frames):
+        b.set_kinematic_target(new, pool[4].tool, tg[4][f][:3], tg[4][f][3:])
+        b.step([new, ids[0]], DT)
+    x, v = b.read_particles(new)
+    assert np.array_equal(x, ref[4][0]) and np.array_equal(v, ref[4][1])
+    b.close()
+
+
+@pytest.mark.gpu
+def test_coloured_batch_switches_to_gather_and_autotune_picks_a_schedule():
+    """A colour-Jacobi batch also runs the gather schedule (bit-identical to gather solvers); its
+    autotuner times both and the chosen one still equals its solvers bit for bit; colour Jacobi
+    and gather agree within 1e-5 (only the order of each particle's sum differs)."""
+    pool = small_pool(3)
+    frames = 3
+    tg = [targets_for(sc, frames, seed=40 + k) for k, sc in enumerate(pool)]
+    ref = {s: [own_solver_run(sc, tg[k], solver_desc_with(s)) for k, sc in enumerate(pool)]
+           for s in (XPBD_GATHER, XPBD_COLOUR_JACOBI)}
+    for k in range(len(pool)):
+        np.testing.assert_allclose(ref[XPBD_COLOUR_JACOBI][k][0], ref[XPBD_GATHER][k][0], rtol=0, atol=1e-5)
+    b = Batch(batch_desc(solver_desc_with(XPBD_COLOUR_JACOBI), memory_budget_bytes=1 << 30,
+                         particle_capacity=10000))
+    ids = [b.add_scene(sc.world.soa()) for sc in pool]
+    tune = b.autotune(ids, DT)
+    cands = tune["candidates"]
+    cj = [c for c in cands if c[4] == XPBD_COLOUR_JACOBI]
+    assert len(cj) == 4 and all(c[3] == 0 for c in cj), cands
+    assert tune["xpbd_schedule"] in (XPBD_GATHER, XPBD_COLOUR_JACOBI)
+    assert b.stats()["xpbd_schedule"] == tune["xpbd_schedule"]
+    for mode in (XPBD_GATHER, XPBD_COLOUR_JACOBI):
+        b.set_fused(0)
+        b.set_xpbd_schedule(mode)
+        ids2 = [b.add_scene(sc.world.soa()) for sc in pool]
+        for f in range(frames):
+            for k in range(len(pool)):
+                b.set_kinematic_target(ids2[k], pool[k].tool, tg[k][f][:3], tg[k][f][3:])
+            b.step(ids2, DT)
+        for k in range(len(pool)):
+            x, v = b.read_particles(ids2[k])
+            assert np.array_equal(x, ref[mode][k][0]) and np.array_equal(v, ref[mode][k][1]), (mode, k)
+            b.remove_scene(ids2[k])
+    b.close()
+
+
+@pytest.mark.gpu
+def test_gather_batch_refuses_coloured_schedules():
+    from cn_physics import CNError
+    b = Batch(batch_desc(serving.serving_solver_desc(), memory_budget_bytes=1 << 28, particle_capacity=4000))
+    with pytest.raises(CNError):
+        b.set_xpbd_schedule(XPBD_COLOUR_JACOBI)
+    b.set_xpbd_schedule(XPBD_GATHER)
+    b.close()
+    with pytest.raises(CNError):   # the fused iterations run the gather schedule
+        Batch(batch_desc(solver_desc_with(XPBD_COLOUR_JACOBI), memory_budget_bytes=1 << 28,
+                         particle_capacity=4000, fused_cluster_ctas=2))
 
 
 @pytest.mark.gpu

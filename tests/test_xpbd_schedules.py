@@ -264,7 +264,7 @@ def test_gpu_colour_jacobi_cube16_within_tolerance_of_gather():
 
 
 @pytest.mark.gpu
-def test_coloured_schedule_info_and_batch_rejection():
+def test_coloured_schedule_info_and_batch_schedule():
     w, desc, dt = scenes.xpbd_cube(n=8, spacing=1.0 / 8.0)
     desc.soft.xpbd_schedule = XPBD_COLOUR_GAUSS_SEIDEL
     s = Solver(desc)
@@ -274,6 +274,10 @@ def test_coloured_schedule_info_and_batch_rejection():
     assert info["colours"]["edges"] >= 1 and info["colours"]["tets"] >= 1
     s.close()
     from cn_physics import Batch, batch_desc
+    b = Batch(batch_desc(desc, memory_budget_bytes=1 << 28))   # a batch holds the colour tables too
+    assert b.stats()["xpbd_schedule"] == XPBD_COLOUR_GAUSS_SEIDEL
+    b.close()
+    desc.soft.xpbd_schedule = 7
     with pytest.raises(CNError):
         Batch(batch_desc(desc, memory_budget_bytes=1 << 28))
 
