@@ -55,7 +55,7 @@ class SolverDesc(C.Structure):
                 ("rigid_rigid_contact_iterations", u32), ("contact", ContactSettings),
                 ("rigid", RigidSettings), ("joints", JointSettings), ("soft", SoftSettings),
                 ("fluid", FluidSettings), ("enable_blocking_readback", u32),
-                ("max_fluid_neighborhood", u32)]
+                ("max_fluid_neighborhood", u32), ("particle_rigid_pairs_per_particle", u32)]
 
 
 class FluidMaterial(C.Structure):

@@ -162,6 +162,12 @@ cn_status batchAdmitImage(cn_batch *b, const SceneImage &img, uint32_t *scene_id
 uint32_t batchRigidPairsPerParticle(const cn_batch *b);
 bool batchColoured(const cn_batch *b);
 
+// Particle-rigid candidate pairs per particle (0 reads as the reference's 8).
+inline uint32_t rigidPairsPerParticle(const cn_solver_desc &d)
+{
+    return d.particle_rigid_pairs_per_particle ? d.particle_rigid_pairs_per_particle : 8u;
+}
+
 // Solver constants of one substep, from the PhysicsSolverDesc mirror.
 inline Config configFromDesc(const cn_solver_desc &d)
 {

@@ -231,7 +231,7 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
         // pairs per collider; proxy contact slots: 8 per proxy, the particle-rigid candidate rate
         const uint32_t P = std::max<uint32_t>(64u, 32u * C);
         s.rrCapacity = P;
-        s.proxyCapacity = sv->proxyContacts ? std::max<uint32_t>(64u, 8u * sv->nProxy) : 0u;
+        s.proxyCapacity = sv->proxyContacts ? std::max<uint32_t>(64u, cn::rigidPairsPerParticle(sv->desc) * sv->nProxy) : 0u;
         s.rrCount = a.take<uint32_t>(C); s.rrOffset = a.take<uint32_t>(C);
         s.rrStage = a.take<uint2>(size_t(C) * 64u); // kPairStage per collider
         const uint32_t K = P * cn::kRigidPairContacts + s.proxyCapacity;
@@ -334,7 +334,7 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
     if (sv->rigidPossible || sv->proxyContacts) {
         s.candCount = a.take<uint32_t>(N);
         s.candOffset = a.take<uint32_t>(N);
-        s.rigidPairCapacity = std::max<uint32_t>(N * 8u, 64u);
+        s.rigidPairCapacity = std::max<uint32_t>(N * cn::rigidPairsPerParticle(sv->desc), 64u);
         s.rigidPairs = a.take<uint2>(s.rigidPairCapacity);
         s.rigidContacts = a.take<cn::RigidContact>(s.rigidPairCapacity);
     }
@@ -631,6 +631,7 @@ CN_API void cn_solver_desc_defaults(cn_solver_desc *d)
     d->fluid.max_under_density_ratio = 0.0f;
     d->enable_blocking_readback = 1u;
     d->max_fluid_neighborhood = 128u;
+    d->particle_rigid_pairs_per_particle = 8u;
 }
 
 CN_API cn_status cn_solver_create(const cn_solver_desc *desc, int device, cn_solver **out)
@@ -686,6 +687,9 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     if (N > (1u << 29)) return setError(CN_ERR_CAPACITY, "cn_solver_sync_world: more than 2^29 particles");
     if (sv->desc.max_fluid_neighborhood > 1024u)
         return setError(CN_ERR_INVALID_ARGUMENT, "max_fluid_neighborhood above 1024");
+    if (sv->desc.particle_rigid_pairs_per_particle > 256u ||
+        uint64_t(N) * cn::rigidPairsPerParticle(sv->desc) >= (uint64_t(1) << 32))
+        return setError(CN_ERR_INVALID_ARGUMENT, "particle_rigid_pairs_per_particle above 256 or 2^32 pairs");
     CN_CUDA(cudaSetDevice(sv->device));
     CN_CUDA(cudaStreamSynchronize(sv->ownStream));
     releaseBuffers(sv);

@@ -140,6 +140,11 @@ typedef struct cn_solver_desc {
     cn_fluid_settings fluid;
     uint32_t enable_blocking_readback; /* 1: step() copies x and v back into the synced host arrays */
     uint32_t max_fluid_neighborhood;   /* 128 (kDefaultFluidMaxNeighborhood) */
+    /* Particle-rigid candidate pairs (and proxy contact slots) per particle: 8, the reference's
+     * fixed rate (max(particles x 8, 64), physics_scene_gpu_state.cpp:726-727); 0 reads as 8.  No
+     * reference counterpart as a setting: raise it for scenes whose particles touch more
+     * colliders, where cn_solver_validate_meta reports the overflow. */
+    uint32_t particle_rigid_pairs_per_particle;
 } cn_solver_desc;
 
 /* Fills the reference's defaults (physics_solver.h:22-143). */

@@ -917,7 +917,9 @@ void buildParticleRigidCandidates(cno_solver &s)
             per[i].push_back(b);
         }
     }
-    const uint32_t cap = std::max<uint32_t>(N * 8u, 64u);
+    // max(particles x 8, 64) (physics_scene_gpu_state.cpp:726-727); the rate is a setting here
+    const uint32_t rate = s.desc.particle_rigid_pairs_per_particle ? s.desc.particle_rigid_pairs_per_particle : 8u;
+    const uint32_t cap = std::max<uint32_t>(N * rate, 64u);
     s.rigidPairs.clear();
     uint64_t required = 0;
     for (uint32_t i = 0; i < N; ++i)
@@ -2803,7 +2805,8 @@ void proxyRigidContacts(cno_solver &s)
 {
     uint32_t proxyCands = 0;
     while (proxyCands < s.rigidPairs.size() && s.rigidPairs[proxyCands].first < s.nProxy) ++proxyCands;
-    const uint32_t cap = std::max<uint32_t>(64u, 8u * s.nProxy);
+    const uint32_t cap = std::max<uint32_t>(
+        64u, (s.desc.particle_rigid_pairs_per_particle ? s.desc.particle_rigid_pairs_per_particle : 8u) * s.nProxy);
     const uint32_t used = std::min(proxyCands, cap);
     s.requiredProxyContacts = proxyCands;
     s.proxyContactSlots = used;

@@ -59,6 +59,7 @@ def reference_desc(**overrides):
     d.fluid.max_under_density_ratio = 0.0
     d.enable_blocking_readback = 1
     d.max_fluid_neighborhood = 128
+    d.particle_rigid_pairs_per_particle = 8
     for k, v in overrides.items():
         setattr(d, k, v)
     return d

@@ -262,3 +262,61 @@ def test_incremental_update_moves_proxy_points():
     p, q = gpu.read_rigid_bodies()[:2]
     want = np.array([qrot(q[b], local[k, :3]) + p[b, :3] for k in range(27)])
     np.testing.assert_allclose(x[:27, :3], want, atol=2e-5)
+
+
+def crowded_proxies():
+    """A 4 x 4 x 4 proxy body (64 proxies of radius 0.02) inside a lattice of small static spheres
+    0.025 apart: each proxy is a candidate of ~166 bodies (10,648 pairs), far more than the
+    reference's fixed 8 pairs per particle."""
+    w = World()
+    g = (np.arange(9) - 4.0) * 0.025
+    for x in g:
+        for y in g:
+            for z in g:
+                s = w.add_rigid_body("static", position=(float(x), 0.5 + float(y), float(z)))
+                w.add_collider(s, "sphere", (0.008,), friction=0.5)
+    b = w.add_rigid_body("kinematic", position=(0.0, 0.5, 0.0))
+    w.set_rigid_proxy_particles(b, lattice(4, 0.04), 0.02, friction=0.5)
+    return w, b
+
+
+@pytest.mark.parametrize("rate", [0, 8, 192])
+def test_particle_rigid_candidate_rate_sizes_the_pair_buffer_in_the_oracle(rate):
+    """particle_rigid_pairs_per_particle: 0 and 8 are the reference's max(particles x 8, 64) pairs
+    (an overflow here), 192 holds every candidate."""
+    w, _ = crowded_proxies()
+    soa = w.soa()
+    ora = cn_oracle.Oracle(solver_desc(**DESC, particle_rigid_pairs_per_particle=rate), soa)
+    ora.step(1.0 / 60.0)
+    m = ora.meta()
+    cap = max(64 * (rate or 8), 64)
+    assert m["required_rigid_pairs"] > 8 * 64, m
+    assert m["rigid_pairs"] == min(m["required_rigid_pairs"], cap), m
+    ora.close()
+
+
+@pytest.mark.gpu
+def test_particle_rigid_candidate_rate_matches_the_oracle_and_clears_the_overflow():
+    w, _ = crowded_proxies()
+    for rate, status in ((0, "CAPACITY"), (192, "OK")):
+        desc = solver_desc(**DESC, particle_rigid_pairs_per_particle=rate)
+        gpu, ora = pair(w, desc)
+        gpu.step(1.0 / 60.0)
+        ora.step(1.0 / 60.0)
+        m, om = gpu.validate_gpu_meta(), ora.meta()
+        assert m["status"] == status, m
+        assert m["required_particle_rigid_candidate_count"] == om["required_rigid_pairs"]
+        assert m["required_proxy_rigid_contact_count"] == om["required_proxy_contacts"]
+        xg, xo = gpu.read_particles()[0], ora.read_particles()[0]
+        assert np.abs(xg - xo).max() < 1e-5
+        gpu.close()
+        ora.close()
+
+
+@pytest.mark.gpu
+def test_particle_rigid_candidate_rate_is_bounded():
+    s = Solver(solver_desc(**DESC, particle_rigid_pairs_per_particle=1000))
+    w, _ = proxy_drop()
+    with pytest.raises(CNError):
+        s.sync_world(w.soa())
+    s.close()
