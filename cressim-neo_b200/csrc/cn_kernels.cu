@@ -927,6 +927,9 @@ __device__ __forceinline__ bool neighborAllowed(const Scene &s, uint32_t tag, ui
 //         mixes several cells looks its runs up itself);
 // mode 1: as mode 0, and also record every candidate within h * (1 + margin) ("superset", in
 //         traversal order) for the later iterations of this substep;
+// mode 3: record the superset only (no list, no density): the first iteration's list and density
+//         then come from the mode 2 filter over it, which visits the same candidates in the same
+//         order with the same distances, so the list and the sums are those of mode 1;
 // mode 2: filter the superset instead of walking the cells.  Cells are fixed for the substep and
 //         positions move only by the accumulated delta, so while 2 * max|delta| < margin * h every
 //         neighbour of this iteration is in the superset, and filtering it in order yields exactly
@@ -949,14 +952,15 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidNeighborsDen
     if (slot >= s.N) return;
     const uint32_t info = s.sInfo[slot];
     if ((info & kFluidBit) == 0u) {
-        if (density) s.Cs[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (density && mode != 3u) s.Cs[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
         return;
     }
     const float4 self = s.P[slot];
     if ((__float_as_uint(self.w) & kFluidBit) == 0u) { // invMass <= kEps
+        if (mode == 1u || mode == 3u) s.supCount[slot] = 0u;
+        if (mode == 3u) return;
         if (density) s.Cs[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
         s.nbrCount[slot] = 0u;
-        if (mode == 1u) s.supCount[slot] = 0u;
         return;
     }
     const uint32_t maxN = s.maxNbr;
@@ -1012,7 +1016,7 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidNeighborsDen
         const uint32_t myGroup = infoGroup(info);
         const bool selfCompat = (m.w & m.z) != 0u;
         const int4 e = s.cCell[slot];
-        const bool buildSup = mode == 1u;
+        const bool buildSup = mode == 1u || mode == 3u;
         const float supR = h * (1.0f + s.supMargin);
         const float sup2 = supR * supR;
         const float rec2 = buildSup ? (sup2 > h2 ? sup2 : h2) : h2;
@@ -1051,7 +1055,7 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidNeighborsDen
                             if (supN < s.supCap) __stcs(&sup[supN * lstr], c); // written once, read later
                             ++supN;
                         }
-                        if (d2 >= h2) return;
+                        if (mode == 3u || d2 >= h2) return;
                         if (count >= maxN) { truncated = 1; return; }
                         __stcs(&out[count++ * lstr], c);
                         if (density) {
@@ -1077,6 +1081,7 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidNeighborsDen
                     }
                 }
         if (buildSup) s.supCount[slot] = supN; // > supCap marks an overflowed superset
+        if (mode == 3u) return;
     }
     s.nbrCount[slot] = count;
     if (truncated) atomicAdd(&s.meta_->neighborTruncations, 1u);
@@ -2734,6 +2739,10 @@ void launchParticleCandidates(const Scene &s, uint32_t *scanTmp, size_t, cudaStr
     k_particleCandidates<true><<<blocksFor(s.N), kThreads, 0, st>>>(s, total);
 }
 
+// The first iteration of a substep as a superset-only cell walk plus the filter of the later
+// iterations (true), or one walk that also builds the list and the density (false).
+constexpr bool kSplitSupersetBuild = true;
+
 // Positions of iteration k: buffer A (s.P) for even k, B (s.Pb) for odd k when double-buffered.
 inline Scene withPositions(const Scene &s, uint32_t iter)
 {
@@ -2764,10 +2773,14 @@ void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter,
     if (s.sup == nullptr || walkCells) {
         if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<0u, true>, g, kThreads, st, sp, c, true, iter, Dk);
         else launchPdl(k_fluidNeighborsDensity<0u, false>, g, kThreads, st, sp, c, true, iter, Dk);
-    } else if (iter == 0) {
+    } else if (iter == 0 && !kSplitSupersetBuild) {
         if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<1u, true>, g, kThreads, st, sp, c, true, iter, Dk);
         else launchPdl(k_fluidNeighborsDensity<1u, false>, g, kThreads, st, sp, c, true, iter, Dk);
     } else {
+        if (iter == 0) { // the superset, then the filter below
+            if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<3u, true>, g, kThreads, st, sp, c, true, iter, Dk);
+            else launchPdl(k_fluidNeighborsDensity<3u, false>, g, kThreads, st, sp, c, true, iter, Dk);
+        }
         if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<2u, true>, g, kThreads, st, sp, c, true, iter, Dk);
         else launchPdl(k_fluidNeighborsDensity<2u, false>, g, kThreads, st, sp, c, true, iter, Dk);
     }
