@@ -13,6 +13,7 @@ Python or CPU implementation of the substep in this package.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -626,9 +627,12 @@ class Batch:
         _check(self._lib.cn_batch_create(C.byref(self.desc), device, C.byref(h)))
         self._h = h
         self._sizes = {}
+        self._servers = weakref.WeakSet()   # servers over this batch, closed before it
 
     def close(self):
         if getattr(self, "_h", None):
+            for srv in list(getattr(self, "_servers", ())):
+                srv.close()
             self._lib.cn_batch_destroy(self._h)
             self._h = None
 
@@ -710,10 +714,13 @@ class Server:
         _check(self._lib.cn_server_create(batch._h, C.byref(d), batch.desc.solver.substeps, C.byref(h)))
         self._h = h
         self._sizes = []
+        batch._servers.add(self)
 
     def close(self):
+        # a server is destroyed before its batch (the batch's close() closes it first)
         if getattr(self, "_h", None):
-            self._lib.cn_server_destroy(self._h)
+            if getattr(self.batch, "_h", None):
+                self._lib.cn_server_destroy(self._h)
             self._h = None
 
     def __del__(self):

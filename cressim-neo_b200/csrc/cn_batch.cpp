@@ -93,6 +93,7 @@ struct Range {
 };
 struct BatchScene {
     bool live = false;
+    uint64_t stepStamp = 0; // the cn_batch_step call that last listed it (duplicate check)
     Range p, e, t, ei, ti, b, c, ci, m, k;
     uint32_t edgeColours = 0;
     uint32_t queryCount = 0; // colliders in its query order (a prefix-free range starting at c.start)
@@ -158,7 +159,7 @@ struct cn_batch {
     float graphDt = -1.0f;
     uint32_t substeps = 1, softIt = 1, contactIt = 1, maxIt = 1;
     uint32_t tileElems = 256, blocksPerSm = 8, smCount = 148, grid = 0;
-    uint64_t ticks = 0;
+    uint64_t ticks = 0, stepCalls = 0;
     // persistent fused iterations: CTAs per scene cluster (0: per-phase kernels), clusters of the
     // grid; the tick's scene list (cn::kSceneListStride uint2 per stepped scene; counter 6 =
     // scenes, counter 7 = the next scene to take, both staged with the work lists)
@@ -529,6 +530,40 @@ void refreshSceneImage(const cn_world_soa &w, SceneImage &img)
     put(kAdmKinFlags, w.body_kinematic_target_flags, 4ull * L.B);
 }
 
+// The device side of an admission: a recapture when the scene brings more colours than the tick's
+// graph passes over, one transfer into the staging buffer (grown when a larger scene arrives),
+// then the scatter into the scene's ranges; all on the upload stream, which the next tick waits for.
+static cudaError_t uploadScene(cn_batch *b, const SceneImage &img, const BatchScene &sc)
+{
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e != cudaSuccess) return e;
+    if (b->coloured && (img.colours[0] > b->colours[0] || img.colours[1] > b->colours[1])) {
+        b->colours[0] = std::max(b->colours[0], img.colours[0]);
+        b->colours[1] = std::max(b->colours[1], img.colours[1]);
+        if ((e = cudaDeviceSynchronize()) != cudaSuccess) return e; // no tick of the old graph in flight
+        releaseGraph(b);
+    }
+    const size_t bytes = img.bytes.size();
+    if (bytes > b->stageBytes) {
+        const size_t cap = std::max(bytes, 2 * b->stageBytes);
+        if ((e = cudaStreamSynchronize(b->upStream)) != cudaSuccess) return e;
+        if (b->dStage) cudaFree(b->dStage);
+        b->dStage = nullptr;
+        b->stageBytes = 0;
+        if ((e = cudaMalloc(&b->dStage, cap)) != cudaSuccess) return e;
+        b->stageBytes = cap;
+    }
+    if ((e = cudaMemcpyAsync(b->dStage, img.bytes.data(), bytes, cudaMemcpyHostToDevice, b->upStream)) != cudaSuccess)
+        return e;
+    AdmitImage a = img.layout;
+    a.img = b->dStage;
+    a.p0 = sc.p.start; a.e0 = sc.e.start; a.t0 = sc.t.start; a.ei0 = sc.ei.start; a.ti0 = sc.ti.start;
+    a.b0 = sc.b.start; a.c0 = sc.c.start; a.ci0 = sc.ci.start; a.m0 = sc.m.start; a.k0 = sc.k.start;
+    launchAdmitScene(b->s, a, b->upStream);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return cudaEventRecord(b->upDone, b->upStream);
+}
+
 cn_status batchAdmitImage(cn_batch *b, const SceneImage &img, uint32_t *scene_id)
 {
     const AdmitImage &L = img.layout;
@@ -559,40 +594,15 @@ cn_status batchAdmitImage(cn_batch *b, const SceneImage &img, uint32_t *scene_id
     }
     sc.live = true;
     sc.queryCount = L.queryCount;
-    if (b->coloured) {
-        const uint32_t ce = img.colours[0], ct = img.colours[1];
-        sc.edgeColours = ce;
-        if (ce > b->colours[0] || ct > b->colours[1]) { // the tick's graph runs more colour passes
-            b->colours[0] = std::max(b->colours[0], ce);
-            b->colours[1] = std::max(b->colours[1], ct);
-            CN_CUDA(cudaSetDevice(b->device));
-            CN_CUDA(cudaDeviceSynchronize()); // no tick of the old graph in flight
-            releaseGraph(b);
-        }
-    }
+    sc.edgeColours = img.colours[0];
     sc.bytes = img.budgetBytes;
     b->bytesAdmitted += img.budgetBytes;
-    CN_CUDA(cudaSetDevice(b->device));
-    // One transfer into the staging buffer (grown when a larger scene arrives), then the scatter;
-    // both on the upload stream, which the next tick waits for.
-    const size_t bytes = img.bytes.size();
-    if (bytes > b->stageBytes) {
-        const size_t cap = std::max(bytes, 2 * b->stageBytes);
-        CN_CUDA(cudaStreamSynchronize(b->upStream));
-        if (b->dStage) cudaFree(b->dStage);
-        b->dStage = nullptr;
-        b->stageBytes = 0;
-        CN_CUDA(cudaMalloc(&b->dStage, cap));
-        b->stageBytes = cap;
+    const cudaError_t e = uploadScene(b, img, sc);
+    if (e != cudaSuccess) { // the ranges and the budget go back; the pool keeps no part of the scene
+        releaseScene(b, sc);
+        return setError(e == cudaErrorMemoryAllocation ? CN_ERR_OUT_OF_MEMORY : CN_ERR_CUDA,
+                        std::string("cn_batch_add_scene: ") + cudaGetErrorString(e));
     }
-    CN_CUDA(cudaMemcpyAsync(b->dStage, img.bytes.data(), bytes, cudaMemcpyHostToDevice, b->upStream));
-    AdmitImage a = L;
-    a.img = b->dStage;
-    a.p0 = sc.p.start; a.e0 = sc.e.start; a.t0 = sc.t.start; a.ei0 = sc.ei.start; a.ti0 = sc.ti.start;
-    a.b0 = sc.b.start; a.c0 = sc.c.start; a.ci0 = sc.ci.start; a.m0 = sc.m.start; a.k0 = sc.k.start;
-    launchAdmitScene(b->s, a, b->upStream);
-    CN_CUDA(cudaGetLastError());
-    CN_CUDA(cudaEventRecord(b->upDone, b->upStream));
     b->uploadPending = true;
     uint32_t id = 0;
     while (id < b->scenes.size() && b->scenes[id].live) ++id;
@@ -810,11 +820,15 @@ CN_API cn_status cn_batch_step(cn_batch *b, const uint32_t *scene_ids, uint32_t 
     if (count > std::max<uint32_t>(b->desc.max_scenes, 1u))
         return setError(CN_ERR_CAPACITY, "cn_batch_step: more scenes than max_scenes");
     uint2 *sceneList = b->hScenes[k];
+    const uint64_t stamp = ++b->stepCalls;
     for (uint32_t n = 0; n < count; ++n) {
         const uint32_t id = scene_ids[n];
         if (id >= b->scenes.size() || !b->scenes[id].live)
             return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_step: scene " + std::to_string(id) + " is not resident");
-        const BatchScene &sc = b->scenes[id];
+        BatchScene &sc = b->scenes[id];
+        if (sc.stepStamp == stamp)
+            return setError(CN_ERR_INVALID_ARGUMENT, "cn_batch_step: scene " + std::to_string(id) + " is listed twice");
+        sc.stepStamp = stamp;
         uint2 *row = sceneList + size_t(cn::kSceneListStride) * n;
         row[0] = make_uint2(sc.p.start, sc.p.start + sc.p.count);
         row[1] = make_uint2(sc.e.start, sc.e.start + sc.e.count);

@@ -166,7 +166,10 @@ struct cn_server {
 namespace {
 
 // Makes `id` resident, evicting idle resident scenes (least recently stepped first) when the
-// budget or the pool is full.  Returns false if it has to wait for room.
+// budget or the pool is full.  Returns false if it has to wait for room.  A scene already taken
+// into the tick being assembled (lastTick = the coming tick) is not idle even when that tick
+// issues its request's last frame: evicting it would drop it from the tick and hand its batch id
+// to the scene being admitted, which the tick would then step twice.
 bool admit(cn_server *srv, uint32_t id)
 {
     SceneSlot &sc = *srv->scenes[id];
@@ -188,7 +191,7 @@ bool admit(cn_server *srv, uint32_t id)
         int victim = -1;
         for (uint32_t k = 0; k < srv->scenes.size(); ++k) {
             const SceneSlot &o = *srv->scenes[k];
-            if (!o.resident || !o.queue.empty() || k == id) continue;
+            if (!o.resident || !o.queue.empty() || k == id || o.lastTick > srv->tickCount) continue;
             if (victim < 0 || o.lastTick < srv->scenes[victim]->lastTick) victim = int(k);
         }
         if (victim < 0) return false;

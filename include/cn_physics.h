@@ -807,6 +807,7 @@ typedef struct cn_server_stats {
 CN_API void cn_server_desc_defaults(cn_server_desc *desc);
 /* `substeps` is the batch's substep count (used for the particle-substep count). */
 CN_API cn_status cn_server_create(cn_batch *batch, const cn_server_desc *desc, uint32_t substeps, cn_server **out);
+/* Removes the server's resident scenes from its batch: call it before cn_batch_destroy of that batch. */
 CN_API void cn_server_destroy(cn_server *server);
 CN_API cn_status cn_server_register_scene(cn_server *server, const cn_world_soa *world, uint32_t *out_scene);
 /* Makes a registered scene resident ahead of its requests (evicting idle scenes if needed);

@@ -239,3 +239,97 @@ def test_server_results_equal_alone_and_in_the_mix_with_evictions():
         assert np.array_equal(x, x_ref) and np.array_equal(v, v_ref), f"scene {k}"
     srv.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_server_over_a_gauss_seidel_batch_with_evictions_equals_own_solvers():
+    """The server's admission images carry the colourings when its batch runs a coloured schedule:
+    scenes evicted and admitted again under a budget of about two scenes still equal solvers of
+    their own under Gauss-Seidel."""
+    pool = small_pool(6)
+    desc = solver_desc_with(XPBD_COLOUR_GAUSS_SEIDEL)
+
+    def scene_bytes(sc):   # the gather budget terms plus colour orders, sums and tables
+        c = sc.world.counts()
+        return (c["particles"] * (120 + 288 + 16) + c["edges"] * (76 + 4) + c["tets"] * (116 + 4)
+                + 2 * 272 + 2 * 216 + 4 * 200)
+    largest = max(scene_bytes(sc) for sc in pool)
+    b = Batch(batch_desc(desc, memory_budget_bytes=int(2.5 * largest), particle_capacity=20000))
+    srv = Server(b, DT)
+    ids = [srv.register(sc.world.soa()) for sc in pool]
+    # the request stream of the gather server test, which evicts under this budget
+    req = serving.poisson_requests(pool, steps_per_second=600.0, duration_s=0.15, seed=5)
+    per_scene = {k: [] for k in range(len(pool))}
+    for r in req:
+        per_scene[r.scene].append(r.targets)
+    out = serving.serve(srv, pool, ids, req)
+    st = out["stats"]
+    assert out["requests"] == len(req) and st["pending"] == 0 and st["evictions"] > 0, st
+    for k, sc in enumerate(pool):
+        if not per_scene[k]:
+            continue
+        x_ref, v_ref = own_solver_run(sc, np.concatenate(per_scene[k]), desc)
+        x, v = srv.read_particles(ids[k])
+        assert np.array_equal(x, x_ref) and np.array_equal(v, v_ref), f"scene {k}"
+    srv.close()
+    b.close()
+
+
+def serve_in_groups(srv, pool, ids, req, group, ticks_between):
+    """Submits `group` requests, then ticks `ticks_between` times, until all are done: a fixed
+    interleaving of submissions, admissions, evictions and ticks (no wall clock)."""
+    nxt = 0
+    while nxt < len(req) or srv.stats()["pending"]:
+        for _ in range(group):
+            if nxt < len(req):
+                r = req[nxt]
+                srv.submit(ids[r.scene], r.steps, tool_body=pool[r.scene].tool, targets=r.targets)
+                nxt += 1
+        for _ in range(ticks_between):
+            srv.tick(0)
+    srv.drain(0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("schedule", [XPBD_GATHER, XPBD_COLOUR_GAUSS_SEIDEL])
+def test_server_interleavings_with_evictions_equal_own_solvers(schedule):
+    """Fixed interleavings in which a request's last frame empties a scene's queue while its tick
+    is being assembled, and a later scene of the same tick needs room: the scene already in the
+    tick is not evicted (it used to be, and its batch id went to the admitted scene, which the tick
+    then stepped twice)."""
+    pool = small_pool(6)
+    desc = solver_desc_with(schedule)
+    req = serving.poisson_requests(pool, steps_per_second=600.0, duration_s=0.15, seed=5)
+    per_scene = {k: [] for k in range(len(pool))}
+    for r in req:
+        per_scene[r.scene].append(r.targets)
+    ref = {k: own_solver_run(pool[k], np.concatenate(t), desc) for k, t in per_scene.items() if t}
+
+    def scene_bytes(sc):
+        c = sc.world.counts()
+        return (c["particles"] * (120 + 288 + 16) + c["edges"] * (76 + 4) + c["tets"] * (116 + 4)
+                + 2 * 272 + 2 * 216 + 4 * 200)
+    largest = max(scene_bytes(sc) for sc in pool)
+    for group, ticks_between in ((1, 1), (2, 2), (100, 1)):
+        b = Batch(batch_desc(desc, memory_budget_bytes=int(2.5 * largest), particle_capacity=20000))
+        srv = Server(b, DT)
+        ids = [srv.register(sc.world.soa()) for sc in pool]
+        serve_in_groups(srv, pool, ids, req, group, ticks_between)
+        assert srv.stats()["evictions"] > 0
+        for k, (x_ref, v_ref) in ref.items():
+            x, v = srv.read_particles(ids[k])
+            assert np.array_equal(x, x_ref) and np.array_equal(v, v_ref), (group, ticks_between, k)
+        srv.close()
+        b.close()
+
+
+@pytest.mark.gpu
+def test_batch_step_rejects_a_scene_listed_twice():
+    from cn_physics import CNError
+    pool = small_pool(2)
+    b = Batch(batch_desc(serving.serving_solver_desc(), memory_budget_bytes=1 << 28, particle_capacity=4000))
+    ids = [b.add_scene(sc.world.soa()) for sc in pool]
+    with pytest.raises(CNError):
+        b.step([ids[0], ids[1], ids[0]], DT)
+    b.step(ids, DT)
+    b.close()
