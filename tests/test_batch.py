@@ -333,3 +333,54 @@ def test_batch_step_rejects_a_scene_listed_twice():
         b.step([ids[0], ids[1], ids[0]], DT)
     b.step(ids, DT)
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("schedule", [XPBD_GATHER, XPBD_COLOUR_JACOBI])
+def test_random_admissions_removals_and_step_subsets_equal_own_solvers(schedule):
+    """Seeded random sequence of adds (fragmenting the pool's ranges and colour tables), removals,
+    targets and step subsets over eight small scenes; every resident instance equals a solver of
+    its own that ran the same frames with the same targets."""
+    rng = np.random.default_rng(7)
+    desc = solver_desc_with(schedule)
+    dims = [(3, 3, 3), (5, 2, 4), (4, 4, 2), (2, 3, 6), (6, 2, 2), (3, 5, 3), (4, 2, 5), (2, 2, 2)]
+    pool = [serving.tissue_scene(d, seed=50 + k) for k, d in enumerate(dims)]
+    # room for about four of the eight scenes (589 particles, 1,260 tets in all)
+    b = Batch(batch_desc(desc, memory_budget_bytes=1 << 28, particle_capacity=330, edge_capacity=2400,
+                         tet_capacity=700, max_scenes=8))
+    full = 0
+    live = {}   # scene index -> (batch id, targets stepped so far)
+    for op in range(60):
+        k = int(rng.integers(len(pool)))
+        if k not in live:
+            try:
+                live[k] = (b.add_scene(pool[k].world.soa()), [])
+            except Exception:   # the pool is full: drop a random resident scene instead
+                full += 1
+                victim = int(rng.choice(list(live)))
+                b.remove_scene(live.pop(victim)[0])
+            continue
+        if rng.random() < 0.15:
+            b.remove_scene(live.pop(k)[0])
+            continue
+        step = [j for j in live if rng.random() < 0.6] or [k]
+        for j in step:
+            pose = pool[j].tool_pose + rng.normal(0.0, 0.003, 3).astype(np.float32)
+            tg = np.concatenate([pose, [0.0, 0.0, 0.7071068, 0.7071068]]).astype(np.float32)
+            b.set_kinematic_target(live[j][0], pool[j].tool, tg[:3], tg[3:])
+            live[j][1].append(tg)
+        b.step([live[j][0] for j in step], DT)
+    checked = 0
+    for k, (bid, tgs) in live.items():
+        x, v = b.read_particles(bid)
+        if tgs:
+            x_ref, v_ref = own_solver_run(pool[k], np.stack(tgs), desc)
+        else:
+            sv = Solver(desc)
+            sv.sync_world(pool[k].world.soa())
+            x_ref, v_ref, _ = sv.read_particles()
+            sv.close()
+        assert np.array_equal(x, x_ref) and np.array_equal(v, v_ref), (k, len(tgs))
+        checked += 1
+    assert checked >= 2 and full >= 3, (checked, full)
+    b.close()
