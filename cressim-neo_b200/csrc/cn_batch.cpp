@@ -293,8 +293,9 @@ void layoutPool(cn_batch *b, cn::Arena &a)
     s.rigidContacts = a.take<cn::RigidContact>(b->pairCap);
     s.meta_ = a.take<cn::DeviceMeta>(1);
     if (b->coloured) {
-        s.colOrder[cn::kFamEdges] = a.take<uint32_t>(E);
-        s.colOrder[cn::kFamTets] = a.take<uint32_t>(T);
+        s.edgesC = a.take<cn_soft_edge>(E);
+        s.tetsC = a.take<cn_soft_tet>(T);
+        s.tetRecC = a.take<float4>(size_t(T) * 4);
         s.softAcc = a.take<float4>(P);
         s.batchColStarts = a.take<uint32_t>(b->K);
     }
@@ -508,8 +509,9 @@ cn_status buildSceneImage(const cn_world_soa &w, uint32_t rigidPairsPerParticle,
     img.budgetBytes = N * kBytesPerParticle + uint64_t(L.E) * kBytesPerEdge + uint64_t(L.T) * kBytesPerTet +
                       uint64_t(L.B) * kBytesPerBody + uint64_t(L.C) * kBytesPerCollider +
                       uint64_t(N) * rigidPairsPerParticle * 72u;
-    if (coloured) // colour orders, the colour-Jacobi sums, the colour tables
-        img.budgetBytes += 4ull * (L.E + L.T) + 16ull * N + 4ull * L.colWords;
+    if (coloured) // colour-ordered edges and tets with the tets' records, the colour-Jacobi sums, the tables
+        img.budgetBytes += sizeof(cn_soft_edge) * uint64_t(L.E) + (sizeof(cn_soft_tet) + 64ull) * L.T + 16ull * N +
+                           4ull * L.colWords;
     return CN_OK;
 }
 

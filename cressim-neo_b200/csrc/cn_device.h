@@ -153,6 +153,12 @@ struct Scene {
     // a batch's colour tables, per admitted scene and family (edges, then tets) a run of words:
     // colours, the family's particle window [lo, hi), then colours + 1 starts (scene-local)
     uint32_t *batchColStarts = nullptr;
+    // a coloured batch's edges and tets in colour order (pool position e0 + i holds the scene's
+    // i-th constraint in colour order; lambdas share that indexing under a coloured schedule) and
+    // each tet's last corrections in the same order
+    const cn_soft_edge *edgesC = nullptr;
+    const cn_soft_tet *tetsC = nullptr;
+    float4 *tetRecC = nullptr;
 
     // ---- rigid bodies / colliders ----
     uint32_t B = 0, C = 0;

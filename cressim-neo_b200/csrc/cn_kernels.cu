@@ -1341,32 +1341,40 @@ __device__ __forceinline__ float4 recordAt(const float4 *corr, uint32_t slot)
     return slot != kNoSlot ? corr[slot] : make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
-// physics_soft_solve_edge_constraints.cs.hlsl:10-74
+// physics_soft_solve_edge_constraints.cs.hlsl:10-74: one edge's corrections (zero when it is
+// disabled or degenerate) and, when it returns true, its new lambda.
+__device__ __forceinline__ bool edgeSolve(const Scene &s, float dt, float relax, const cn_soft_edge &ed, float lambda,
+                                          float &newLambda, float4 &cA, float4 &cB)
+{
+    cA = make_float4(0.f, 0.f, 0.f, 0.f);
+    cB = cA;
+    if (ed.enabled == 0u) return false;
+    const float4 a = s.x[ed.particle_a], b = s.x[ed.particle_b];
+    const float wA = a.w, wB = b.w, wSum = wA + wB;
+    const f3 delta = xyz(b) - xyz(a);
+    const float l2 = dot(delta, delta);
+    if (!(wSum > kEps && l2 > kEps)) return false;
+    const float len = sqrtf(l2);
+    const f3 gA = -delta / len;
+    const f3 gB = -gA;
+    const float alpha = mx(ed.compliance, 0.0f) / mx(dt * dt, kEps);
+    const float Cv = len - ed.rest_length;
+    const float den = wSum + alpha;
+    if (!(den > kEps)) return false;
+    const float dl = -(Cv + alpha * lambda) / den;
+    newLambda = lambda + dl;
+    cA = mk4(wA * dl * gA * relax, 0.0f);
+    cB = mk4(wB * dl * gB * relax, 0.0f);
+    return true;
+}
+
 __device__ __forceinline__ void solveEdge(const Scene &s, float dt, float relax, uint32_t e)
 {
     const cn_soft_edge ed = s.edges[e];
     const float lambda = s.edgeLambda[e]; // with the record: one round trip fewer
-    float4 cA = make_float4(0.f, 0.f, 0.f, 0.f), cB = cA;
-    if (ed.enabled != 0u) {
-        const float4 a = s.x[ed.particle_a], b = s.x[ed.particle_b];
-        const float wA = a.w, wB = b.w, wSum = wA + wB;
-        const f3 delta = xyz(b) - xyz(a);
-        const float l2 = dot(delta, delta);
-        if (wSum > kEps && l2 > kEps) {
-            const float len = sqrtf(l2);
-            const f3 gA = -delta / len;
-            const f3 gB = -gA;
-            const float alpha = mx(ed.compliance, 0.0f) / mx(dt * dt, kEps);
-            const float Cv = len - ed.rest_length;
-            const float den = wSum + alpha;
-            if (den > kEps) {
-                const float dl = -(Cv + alpha * lambda) / den;
-                s.edgeLambda[e] = lambda + dl;
-                cA = mk4(wA * dl * gA * relax, 0.0f);
-                cB = mk4(wB * dl * gB * relax, 0.0f);
-            }
-        }
-    }
+    float newLambda;
+    float4 cA, cB;
+    if (edgeSolve(s, dt, relax, ed, lambda, newLambda, cA, cB)) s.edgeLambda[e] = newLambda;
     const uint2 d = reinterpret_cast<const uint2 *>(s.edgeDst)[e];
     putRecord(s.edgeCorr, d.x, cA);
     putRecord(s.edgeCorr, d.y, cB);
@@ -1417,15 +1425,15 @@ __global__ void __launch_bounds__(kThreads) k_applyGather(Scene s, const uint2 *
     if (i < win.y) applyGatherAt(s, ranges, corr, i);
 }
 
-// physics_soft_solve_tet_constraints.cs.hlsl:15-87
-__device__ __forceinline__ void solveTet(const Scene &s, float dt, float relax, uint32_t t)
+// physics_soft_solve_tet_constraints.cs.hlsl:15-87: one tet's four corrections and its new
+// lambda; false when the tet keeps its previous corrections (no weight, or a degenerate one).
+__device__ __forceinline__ bool tetSolve(const Scene &s, float dt, float relax, const cn_soft_tet &tet, float lambda,
+                                         float &newLambda, float4 c[4])
 {
-    const cn_soft_tet tet = s.tets[t];
-    const float lambda = s.tetLambda[t]; // with the record: one round trip fewer
     const float4 q0 = s.x[tet.particle_indices[0]], q1 = s.x[tet.particle_indices[1]];
     const float4 q2 = s.x[tet.particle_indices[2]], q3 = s.x[tet.particle_indices[3]];
     const float w0 = q0.w, w1 = q1.w, w2 = q2.w, w3 = q3.w;
-    if ((w0 + w1 + w2 + w3) <= kEps) return; // keeps the previous correction record
+    if ((w0 + w1 + w2 + w3) <= kEps) return false;
     const f3 p0 = xyz(q0), p1 = xyz(q1), p2 = xyz(q2), p3 = xyz(q3);
     const float sv = dot(cross(p1 - p0, p2 - p0), p3 - p0) / 6.0f;
     const float vs = (sv >= 0.0f) ? 1.0f : -1.0f;
@@ -1437,14 +1445,29 @@ __device__ __forceinline__ void solveTet(const Scene &s, float dt, float relax, 
     const float sg = w0 * dot(g0, g0) + w1 * dot(g1, g1) + w2 * dot(g2, g2) + w3 * dot(g3, g3);
     const float alpha = mx(tet.compliance, 0.0f) / mx(dt * dt, kEps);
     const float den = sg + alpha;
-    if (den <= kEps) return;
+    if (den <= kEps) return false;
     const float dl = -(Cv + alpha * lambda) / den;
-    s.tetLambda[t] = lambda + dl;
+    newLambda = lambda + dl;
+    c[0] = mk4(w0 * dl * g0 * relax, 0.0f);
+    c[1] = mk4(w1 * dl * g1 * relax, 0.0f);
+    c[2] = mk4(w2 * dl * g2 * relax, 0.0f);
+    c[3] = mk4(w3 * dl * g3 * relax, 0.0f);
+    return true;
+}
+
+__device__ __forceinline__ void solveTet(const Scene &s, float dt, float relax, uint32_t t)
+{
+    const cn_soft_tet tet = s.tets[t];
+    const float lambda = s.tetLambda[t]; // with the record: one round trip fewer
+    float newLambda;
+    float4 c[4];
+    if (!tetSolve(s, dt, relax, tet, lambda, newLambda, c)) return; // keeps the previous records
+    s.tetLambda[t] = newLambda;
     const uint4 d = reinterpret_cast<const uint4 *>(s.tetDst)[t];
-    putRecord(s.tetCorr, d.x, mk4(w0 * dl * g0 * relax, 0.0f));
-    putRecord(s.tetCorr, d.y, mk4(w1 * dl * g1 * relax, 0.0f));
-    putRecord(s.tetCorr, d.z, mk4(w2 * dl * g2 * relax, 0.0f));
-    putRecord(s.tetCorr, d.w, mk4(w3 * dl * g3 * relax, 0.0f));
+    putRecord(s.tetCorr, d.x, c[0]);
+    putRecord(s.tetCorr, d.y, c[1]);
+    putRecord(s.tetCorr, d.z, c[2]);
+    putRecord(s.tetCorr, d.w, c[3]);
 }
 
 __global__ void __launch_bounds__(kThreads) k_solveTets(Scene s, float dt, float relax)
@@ -2906,6 +2929,37 @@ __device__ __forceinline__ void colourConstraint(const Scene &s, float dt, float
     }
 }
 
+// A coloured batch's constraint at colour position q (its edges and tets stored in colour order):
+// the same per-constraint solve, its lambda at q, the corrections moved from registers; a tet that
+// keeps its previous corrections takes them from its colour-ordered record.  Same values, same
+// order of the moves as colourConstraint.
+template <uint32_t kFam>
+__device__ __forceinline__ void colourConstraintOrdered(const Scene &s, float dt, float relax, bool gaussSeidel, uint32_t q)
+{
+    float newLambda;
+    if constexpr (kFam == kFamEdges) {
+        const cn_soft_edge ed = s.edgesC[q];
+        float4 cA, cB;
+        if (edgeSolve(s, dt, relax, ed, s.edgeLambda[q], newLambda, cA, cB)) s.edgeLambda[q] = newLambda;
+        moveRecord(s, gaussSeidel, ed.particle_a, cA);
+        moveRecord(s, gaussSeidel, ed.particle_b, cB);
+    } else {
+        const cn_soft_tet t = s.tetsC[q];
+        float4 c[4];
+        float4 *rec = s.tetRecC + 4 * size_t(q);
+        if (tetSolve(s, dt, relax, t, s.tetLambda[q], newLambda, c)) {
+            s.tetLambda[q] = newLambda;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) rec[k] = c[k];
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) c[k] = rec[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) moveRecord(s, gaussSeidel, t.particle_indices[k], c[k]);
+    }
+}
+
 // End of a colour-Jacobi family: x += the family's sum (particles with invMass > kEps), sum
 // cleared; for joints the orientation sum, then the normalisation every segment gets.
 __device__ __forceinline__ void colourJacobiApplyAt(const Scene &s, uint32_t i)
@@ -3265,22 +3319,33 @@ __global__ void __launch_bounds__(kThreads) k_admitScene(Scene s, AdmitImage a)
         const_cast<uint2 *>(s.tetRanges)[p] = make_uint2(tr.x + a.ti0, tr.y);
         const_cast<uint2 *>(s.pColRange)[p] = make_uint2(a.c0, a.c0 + a.queryCount);
     }
-    if (i < a.E) {
-        cn_soft_edge e = reinterpret_cast<const cn_soft_edge *>(seg(kAdmEdges))[i];
+    // a scene starts with zero correction records, as a solver's freshly cleared arena
+    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    auto edgeAt = [&](uint32_t k) {
+        cn_soft_edge e = reinterpret_cast<const cn_soft_edge *>(seg(kAdmEdges))[k];
         e.particle_a += a.p0;
         e.particle_b += a.p0;
-        const_cast<cn_soft_edge *>(s.edges)[a.e0 + i] = e;
+        return e;
+    };
+    auto tetAt = [&](uint32_t k) {
+        cn_soft_tet t = reinterpret_cast<const cn_soft_tet *>(seg(kAdmTets))[k];
+        for (int j = 0; j < 4; ++j) t.particle_indices[j] += a.p0;
+        return t;
+    };
+    if (i < a.E) {
+        const_cast<cn_soft_edge *>(s.edges)[a.e0 + i] = edgeAt(i);
         const uint2 d = u2(kAdmEdgeDst)[i];
         reinterpret_cast<uint2 *>(const_cast<uint32_t *>(s.edgeDst))[a.e0 + i] =
             make_uint2(d.x == kNoSlot ? kNoSlot : d.x + a.ei0, d.y == kNoSlot ? kNoSlot : d.y + a.ei0);
+        s.edgeCorr[a.ei0 + 2u * i] = zero4;
+        s.edgeCorr[a.ei0 + 2u * i + 1u] = zero4;
     }
     if (i < a.T) {
-        cn_soft_tet t = reinterpret_cast<const cn_soft_tet *>(seg(kAdmTets))[i];
-        for (int k = 0; k < 4; ++k) t.particle_indices[k] += a.p0;
-        const_cast<cn_soft_tet *>(s.tets)[a.t0 + i] = t;
+        const_cast<cn_soft_tet *>(s.tets)[a.t0 + i] = tetAt(i);
         const uint4 d = reinterpret_cast<const uint4 *>(seg(kAdmTetDst))[i];
         auto rb = [&](uint32_t v) { return v == kNoSlot ? kNoSlot : v + a.ti0; };
         reinterpret_cast<uint4 *>(const_cast<uint32_t *>(s.tetDst))[a.t0 + i] = make_uint4(rb(d.x), rb(d.y), rb(d.z), rb(d.w));
+        for (uint32_t k = 0; k < 4u; ++k) s.tetCorr[a.ti0 + 4u * i + k] = zero4;
     }
     if (i < a.M) const_cast<float4 *>(s.contactMaterials)[a.m0 + i] = f4(kAdmMaterials)[i];
     if (i < a.B) {
@@ -3308,9 +3373,12 @@ __global__ void __launch_bounds__(kThreads) k_admitScene(Scene s, AdmitImage a)
         const_cast<float4 *>(s.colMat)[c] = f4(kAdmColMat)[i];
     }
     if (i < a.queryCount) const_cast<uint32_t *>(s.colQueryOrder)[a.c0 + i] = u32(kAdmQueryOrder)[i] + a.c0;
-    if (a.colWords) {
-        if (i < a.E) const_cast<uint32_t *>(s.colOrder[kFamEdges])[a.e0 + i] = u32(kAdmEdgeColOrder)[i] + a.e0;
-        if (i < a.T) const_cast<uint32_t *>(s.colOrder[kFamTets])[a.t0 + i] = u32(kAdmTetColOrder)[i] + a.t0;
+    if (a.colWords) { // the colour-ordered copies, colour tables and records
+        if (i < a.E) const_cast<cn_soft_edge *>(s.edgesC)[a.e0 + i] = edgeAt(u32(kAdmEdgeColOrder)[i]);
+        if (i < a.T) {
+            const_cast<cn_soft_tet *>(s.tetsC)[a.t0 + i] = tetAt(u32(kAdmTetColOrder)[i]);
+            for (uint32_t k = 0; k < 4u; ++k) s.tetRecC[4u * (size_t(a.t0) + i) + k] = zero4;
+        }
         if (i < a.colWords) s.batchColStarts[a.k0 + i] = u32(kAdmColStarts)[i];
     }
 }
@@ -3333,7 +3401,7 @@ __device__ __forceinline__ void forSceneChunks(const uint32_t *sceneCount, F &&f
 }
 
 // Colour k of one family over a batch tick's stepped scenes: each scene's colour-k range of its
-// colour order (global constraint indices), scenes with fewer colours skipped.
+// colour-ordered constraints (contiguous), scenes with fewer colours skipped.
 template <uint32_t kFam, bool kGaussSeidel>
 __global__ void __launch_bounds__(kThreads) k_colourSolveBatch(Scene s, float dt, float relax, uint32_t k,
                                                                const uint2 *scenes, const uint32_t *sceneCount)
@@ -3347,7 +3415,7 @@ __global__ void __launch_bounds__(kThreads) k_colourSolveBatch(Scene s, float dt
         const uint32_t *starts = words + kColWordsHeader;
         const uint32_t b = range.x + starts[k], e = range.x + starts[k + 1u];
         for (uint32_t q = b + part * blockDim.x + threadIdx.x; q < e; q += chunks * blockDim.x)
-            colourConstraint<kFam>(s, dt, relax, kGaussSeidel, s.colOrder[kFam][q]);
+            colourConstraintOrdered<kFam>(s, dt, relax, kGaussSeidel, q);
     });
 }
 
