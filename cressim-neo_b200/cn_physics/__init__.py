@@ -434,7 +434,9 @@ class World:
                 "tets": ("tets", s.tet_count, np.uint32, 8), "edges": ("edges", s.edge_count, np.uint32, 8),
                 "dihedrals": ("dihedrals", s.dihedral_count, np.uint32, 8),
                 "segments": ("strand_segments", s.strand_segment_count, np.uint32, 8),
-                "joints": ("strand_joints", s.strand_joint_count, np.uint32, 8)}[name]
+                "joints": ("strand_joints", s.strand_joint_count, np.uint32, 8),
+                "body_inverse_inertia": ("body_inverse_inertia", s.rigid_body_count, np.float32, 4),
+                "body_types": ("body_types", s.rigid_body_count, np.uint32, 1)}[name]
         return _view(getattr(s, spec[0]), spec[1], spec[2], spec[3])
 
 

@@ -38,6 +38,10 @@ using cn::setError;
 struct cn_solver {
     cn_solver_desc desc{};
     int device = 0;
+    // what cn_solver_update_world may not change: the constraints' particle (segment) indices,
+    // which the incidence tables and colourings are built from, and the body types
+    uint64_t topologyHash = 0;
+    std::vector<uint32_t> bodyTypes;
     cudaStream_t ownStream = nullptr;
     cn::Scene s{};
     cn::Config cfg{};
@@ -676,6 +680,31 @@ CN_API void cn_solver_destroy(cn_solver *sv)
     delete sv;
 }
 
+// FNV-1a over the particle (segment) indices of every constraint record: the incidence tables,
+// gather slots and colourings of the synced world are built from them.
+static uint64_t topologyHash(const cn_world_soa &w)
+{
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint32_t v) {
+        for (int k = 0; k < 4; ++k) {
+            h ^= (v >> (8 * k)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    };
+    for (uint32_t c = 0; c < w.edge_count; ++c) { mix(w.edges[c].particle_a); mix(w.edges[c].particle_b); }
+    for (uint32_t c = 0; c < w.bend_count; ++c) { mix(w.bends[c].particle0); mix(w.bends[c].particle1); mix(w.bends[c].particle2); }
+    for (uint32_t c = 0; c < w.dihedral_count; ++c) {
+        const cn_cloth_dihedral &d = w.dihedrals[c];
+        mix(d.edge_particle0); mix(d.edge_particle1); mix(d.opposite_particle0); mix(d.opposite_particle1);
+    }
+    for (uint32_t c = 0; c < w.tet_count; ++c)
+        for (int k = 0; k < 4; ++k) mix(w.tets[c].particle_indices[k]);
+    for (uint32_t c = 0; c < w.strand_segment_count; ++c) { mix(w.strand_segments[c].particle_a); mix(w.strand_segments[c].particle_b); }
+    for (uint32_t c = 0; c < w.strand_joint_count; ++c) { mix(w.strand_joints[c].segment_a); mix(w.strand_joints[c].segment_b); }
+    for (uint32_t c = 0; c < w.strand_distance_count; ++c) { mix(w.strand_distances[c].particle_a); mix(w.strand_distances[c].particle_b); }
+    return h;
+}
+
 CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
 {
     if (!sv || !w) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_sync_world: null argument");
@@ -1033,6 +1062,8 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     sv->fluidMaterialCapacity = w->fluid_material_count;
     sv->surfIdxCapacity = w->surface_render ? w->surface_render->vertex_triangle_index_count : 0u;
     sv->cellRangeCapacity = cn::nextPow2(std::max<uint32_t>(N * 2u, 1u));
+    sv->topologyHash = topologyHash(*w);
+    sv->bodyTypes.assign(w->body_types, w->body_types + w->rigid_body_count);
     sv->synced = true;
     ++sv->bindingGeneration;
     cn::clearError();
@@ -1263,6 +1294,12 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
             CN_CUDA(up(s.proxyLocal, w->rigid_proxy_local_positions, s.nProxy, st));
         }
     }
+    if ((flags & CN_SYNC_CONSTRAINTS) && topologyHash(*w) != sv->topologyHash)
+        return setError(CN_ERR_INVALID_ARGUMENT,
+                        "cn_solver_update_world: constraint particle indices changed; use cn_solver_sync_world");
+    if ((flags & CN_SYNC_RIGID_BODIES) && (s.B && (!w->body_types ||
+                                                   !std::equal(sv->bodyTypes.begin(), sv->bodyTypes.end(), w->body_types))))
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: body types changed; use cn_solver_sync_world");
     if (flags & CN_SYNC_CONSTRAINTS) {
         // records only: incidence tables depend on the particle indices, which must not change
         CN_CUDA(up(s.edges, w->edges, s.E, st));
@@ -1279,6 +1316,7 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
         CN_CUDA(up(s.bodyLin, w->body_linear_velocities, s.B, st));
         CN_CUDA(up(s.bodyAng, w->body_angular_velocities, s.B, st));
         CN_CUDA(up(s.bodyScale, w->body_scales, s.B, st));
+        CN_CUDA(up(s.bodyInvInertia, w->body_inverse_inertia, s.B, st));
         CN_CUDA(up(s.bodyKinPos, w->body_kinematic_target_positions, s.B, st));
         CN_CUDA(up(s.bodyKinRot, w->body_kinematic_target_orientations, s.B, st));
         CN_CUDA(up(s.bodyKinFlags, w->body_kinematic_target_flags, s.B, st));

@@ -593,8 +593,10 @@ CN_API cn_status cn_solver_export_dlpack(cn_solver *solver, const char *buffer, 
 typedef enum cn_sync_flags {
     CN_SYNC_PARTICLE_STATE = 1,     /* positions / inverse masses, velocities */
     CN_SYNC_PARTICLE_ATTRIBUTES = 2,/* radii, metadata, material indices, contact / fluid materials */
-    CN_SYNC_CONSTRAINTS = 4,        /* edge, bend, dihedral, tet and strand records */
-    CN_SYNC_RIGID_BODIES = 8,       /* body poses, velocities, scales, kinematic targets */
+    CN_SYNC_CONSTRAINTS = 4,        /* edge, bend, dihedral, tet and strand records; their particle
+                                     * (segment) indices must be the synced ones (else refused) */
+    CN_SYNC_RIGID_BODIES = 8,       /* body poses, velocities, scales, inverse inertia, kinematic
+                                     * targets; body types must be the synced ones (else refused) */
     CN_SYNC_COLLIDERS = 16,         /* collider geometry, broadphase records, materials */
     CN_SYNC_SURFACE_RENDER = 32     /* surface render bindings, normals, triangles (same counts) */
 } cn_sync_flags;

@@ -78,3 +78,62 @@ def test_step_io_equals_write_step_read():
         b.step(dt)
     xb, vb, _ = b.read_particles()
     assert np.array_equal(xh.numpy(), xb) and np.array_equal(vh.numpy(), vb)
+
+
+def body_on_ground_with_tissue():
+    from cn_physics import World
+    w = World()
+    w.add_soft_body_grid((0.2, 0.1, 0.2), 0.05, position=(0.6, 0.06, 0.0), radius=0.02)
+    scenes.ground(w)
+    tilt = (0.0871557, 0.0, 0.0, 0.9961947)   # 10 degrees about x: lands on an edge
+    b = w.add_rigid_body("dynamic", position=(0.0, 0.15, 0.0), orientation=tilt, mass=1.0,
+                         inverse_inertia=(3.0, 2.0, 1.0))
+    w.add_collider(b, "box", (0.1, 0.05, 0.2), friction=0.5)
+    w.soa()
+    return w, b
+
+
+def test_incremental_body_update_includes_the_inverse_inertia():
+    """CN_SYNC_RIGID_BODIES uploads the inverse inertia too (as uploadRigidBodyRange,
+    physics_scene_gpu_state.cpp:2702-2730): a box landing on an edge after the update moves as in
+    a fresh sync of the updated world."""
+    from cn_physics import solver_desc
+    w, b = body_on_ground_with_tissue()
+    desc = solver_desc(substeps=4, default_iterations=10)
+    a = Solver(desc)
+    a.sync_world(w)
+    w.array("body_inverse_inertia")[b, :3] = (30.0, 20.0, 10.0)
+    a.update_world(w, "rigid_bodies")
+    fresh = Solver(desc)
+    fresh.sync_world(w)
+    for _ in range(30):
+        a.step(1.0 / 60.0)
+        fresh.step(1.0 / 60.0)
+    for u, v in zip(a.read_rigid_bodies(), fresh.read_rigid_bodies()):
+        assert np.array_equal(u, v)
+    # the inertia matters here: the same frames with the synced inertia end elsewhere
+    w.array("body_inverse_inertia")[b, :3] = (3.0, 2.0, 1.0)
+    old = Solver(desc)
+    old.sync_world(w)
+    for _ in range(30):
+        old.step(1.0 / 60.0)
+    assert not np.array_equal(old.read_rigid_bodies()[1], fresh.read_rigid_bodies()[1])
+
+
+def test_incremental_update_refuses_topology_and_body_type_changes():
+    """The incidence tables and colourings are built from the constraints' particle indices, and
+    the structural flags from the body types: changing either through cn_solver_update_world is
+    refused (a full cn_solver_sync_world rebuilds them)."""
+    from cn_physics import CNError, solver_desc
+    w, b = body_on_ground_with_tissue()
+    a = Solver(solver_desc(substeps=2))
+    a.sync_world(w)
+    edges = w.array("edges")
+    edges[0, [0, 1]] = edges[0, [1, 0]]
+    with pytest.raises(CNError):
+        a.update_world(w, "constraints")
+    edges[0, [0, 1]] = edges[0, [1, 0]]
+    a.update_world(w, "constraints")            # same indices: accepted
+    w.array("body_types")[b] = 1                 # dynamic -> kinematic
+    with pytest.raises(CNError):
+        a.update_world(w, "rigid_bodies")
