@@ -42,6 +42,7 @@ struct cn_solver {
     // which the incidence tables and colourings are built from, and the body types
     uint64_t topologyHash = 0;
     std::vector<uint32_t> bodyTypes;
+    uint32_t attributeStructure = 0; // attributeStructure() of the synced world
     cudaStream_t ownStream = nullptr;
     cn::Scene s{};
     cn::Config cfg{};
@@ -705,6 +706,37 @@ static uint64_t topologyHash(const cn_world_soa &w)
     return h;
 }
 
+// The structural choices that the particle attributes make at sync: particle-particle contacts
+// possible (a self-colliding solid particle or several solid groups), vorticity confinement, and the
+// fluid kernels built with the cohesion / surface-tension terms.
+static uint32_t attributeStructure(const cn_world_soa &w)
+{
+    bool anyFluid = false, anySelf = false;
+    uint32_t firstGroup = 0xffffffffu, groups = 0;
+    for (uint32_t i = 0; i < w.particle_count; ++i) {
+        if (w.kinds[i] == CN_PARTICLE_FLUID) {
+            anyFluid = true;
+            continue;
+        }
+        const uint32_t ph = w.metadata[4 * i + 1];
+        if (ph & CN_PHASE_SELF_COLLIDE) anySelf = true;
+        const uint32_t g = ph & CN_PHASE_GROUP_MASK;
+        if (groups == 0) {
+            firstGroup = g;
+            groups = 1;
+        } else if (g != firstGroup) {
+            groups = 2;
+        }
+    }
+    uint32_t bits = (anySelf || groups > 1) ? 1u : 0u;
+    for (uint32_t m = 0; m < w.fluid_material_count; ++m) {
+        const cn_fluid_material &fm = w.fluid_materials[m];
+        if (anyFluid && fm.vorticity_confinement > 1.0e-6f) bits |= 2u;
+        if (fm.cohesion > 0.0f || fm.surface_tension > 1.0e-6f) bits |= 4u;
+    }
+    return bits;
+}
+
 CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
 {
     if (!sv || !w) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_sync_world: null argument");
@@ -1063,6 +1095,7 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
     sv->surfIdxCapacity = w->surface_render ? w->surface_render->vertex_triangle_index_count : 0u;
     sv->cellRangeCapacity = cn::nextPow2(std::max<uint32_t>(N * 2u, 1u));
     sv->topologyHash = topologyHash(*w);
+    sv->attributeStructure = attributeStructure(*w);
     sv->bodyTypes.assign(w->body_types, w->body_types + w->rigid_body_count);
     sv->synced = true;
     ++sv->bindingGeneration;
@@ -1294,6 +1327,10 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
             CN_CUDA(up(s.proxyLocal, w->rigid_proxy_local_positions, s.nProxy, st));
         }
     }
+    if ((flags & CN_SYNC_PARTICLE_ATTRIBUTES) && attributeStructure(*w) != sv->attributeStructure)
+        return setError(CN_ERR_INVALID_ARGUMENT,
+                        "cn_solver_update_world: the attributes change which contact or fluid terms run "
+                        "(self-collision, solid groups, vorticity, cohesion / surface tension); use cn_solver_sync_world");
     if ((flags & CN_SYNC_CONSTRAINTS) && topologyHash(*w) != sv->topologyHash)
         return setError(CN_ERR_INVALID_ARGUMENT,
                         "cn_solver_update_world: constraint particle indices changed; use cn_solver_sync_world");

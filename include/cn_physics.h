@@ -592,7 +592,10 @@ CN_API cn_status cn_solver_export_dlpack(cn_solver *solver, const char *buffer, 
  * binding_generation stay as they are. */
 typedef enum cn_sync_flags {
     CN_SYNC_PARTICLE_STATE = 1,     /* positions / inverse masses, velocities */
-    CN_SYNC_PARTICLE_ATTRIBUTES = 2,/* radii, metadata, material indices, contact / fluid materials */
+    CN_SYNC_PARTICLE_ATTRIBUTES = 2,/* radii, metadata, material indices, contact / fluid materials;
+                                     * refused when they change which contact or fluid terms run
+                                     * (self-collision or solid groups, vorticity, cohesion / surface
+                                     * tension) */
     CN_SYNC_CONSTRAINTS = 4,        /* edge, bend, dihedral, tet and strand records; their particle
                                      * (segment) indices must be the synced ones (else refused) */
     CN_SYNC_RIGID_BODIES = 8,       /* body poses, velocities, scales, inverse inertia, kinematic

@@ -137,3 +137,29 @@ def test_incremental_update_refuses_topology_and_body_type_changes():
     w.array("body_types")[b] = 1                 # dynamic -> kinematic
     with pytest.raises(CNError):
         a.update_world(w, "rigid_bodies")
+
+
+def test_incremental_attribute_update_equals_a_fresh_sync_unless_it_changes_the_kernels():
+    """A fluid material's viscosity uploaded in place gives the bits of a fresh sync; switching
+    surface tension on would need the kernels built with those terms, so the update is refused."""
+    from cn_physics import CNError
+    w, desc, dt = scenes.dam_break(nx=12, ny=8, nz=12, box=(1.2, 0.8, 1.2))
+    import ctypes as C
+    from cn_physics import _abi
+    soa = w.soa()
+    fm = C.cast(C.c_void_p(soa.fluid_materials), C.POINTER(_abi.FluidMaterial))
+    a = Solver(desc)
+    a.sync_world(soa)
+    fm[0].viscosity = fm[0].viscosity * 4.0
+    a.update_world(soa, "particle_attributes")
+    fresh = Solver(desc)
+    fresh.sync_world(soa)
+    for _ in range(3):
+        a.step(dt)
+        fresh.step(dt)
+    xa, va, _ = a.read_particles()
+    xf, vf, _ = fresh.read_particles()
+    assert np.array_equal(xa, xf) and np.array_equal(va, vf)
+    fm[0].surface_tension = 0.5
+    with pytest.raises(CNError):
+        a.update_world(soa, "particle_attributes")
