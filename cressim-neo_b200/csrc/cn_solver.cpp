@@ -43,6 +43,7 @@ struct cn_solver {
     uint64_t topologyHash = 0;
     std::vector<uint32_t> bodyTypes;
     uint32_t attributeStructure = 0; // attributeStructure() of the synced world
+    std::vector<uint32_t> queryOrder; // the colliders queried (enabled, of a present body), in order
     cudaStream_t ownStream = nullptr;
     cn::Scene s{};
     cn::Config cfg{};
@@ -845,6 +846,7 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
 
     std::vector<uint32_t> order;
     const uint32_t moving = cn::colliderQueryOrder(*w, order);
+    sv->queryOrder = order;
     // useInitialRigidContactSolve (physics_solver.cpp:512-514) for scenes where a body can move:
     // collider pairs of the rigid broadphase, or proxy particles against colliders
     sv->rigidRigid = anyDynamic && rrIt > 0 && ((order.size() >= 2 && moving > 0) || (nProxy > 0 && w->collider_count > 0));
@@ -1303,6 +1305,36 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
         const std::string err = checkSurfaceRender(*w);
         if (!err.empty()) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: " + err);
     }
+    // everything that is refused is refused before anything is uploaded
+    if (flags & CN_SYNC_PARTICLE_ATTRIBUTES) {
+        if (w->contact_material_count > std::max<uint32_t>(sv->contactMaterialCapacity, 1u) ||
+            w->fluid_material_count > std::max<uint32_t>(sv->fluidMaterialCapacity, 1u))
+            return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: more materials than synced; use cn_solver_sync_world");
+        if (s.nProxy && !w->rigid_proxy_local_positions)
+            return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: rigid proxy local positions missing");
+    }
+    if ((flags & CN_SYNC_RIGID_BODIES) && s.nProxy && !w->body_proxy_contact_materials)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: proxy contact materials missing");
+    if ((flags & CN_SYNC_SURFACE_RENDER) && w->surface_render &&
+        w->surface_render->vertex_triangle_index_count > sv->surfIdxCapacity)
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: more incident-triangle indices than synced");
+    if ((flags & CN_SYNC_PARTICLE_ATTRIBUTES) && attributeStructure(*w) != sv->attributeStructure)
+        return setError(CN_ERR_INVALID_ARGUMENT,
+                        "cn_solver_update_world: the attributes change which contact or fluid terms run "
+                        "(self-collision, solid groups, vorticity, cohesion / surface tension); use cn_solver_sync_world");
+    if (flags & CN_SYNC_COLLIDERS) {
+        std::vector<uint32_t> order;
+        cn::colliderQueryOrder(*w, order);
+        if (order != sv->queryOrder)
+            return setError(CN_ERR_INVALID_ARGUMENT,
+                            "cn_solver_update_world: colliders enabled, disabled or moved to other bodies; use cn_solver_sync_world");
+    }
+    if ((flags & CN_SYNC_CONSTRAINTS) && topologyHash(*w) != sv->topologyHash)
+        return setError(CN_ERR_INVALID_ARGUMENT,
+                        "cn_solver_update_world: constraint particle indices changed; use cn_solver_sync_world");
+    if ((flags & CN_SYNC_RIGID_BODIES) && (s.B && (!w->body_types ||
+                                                   !std::equal(sv->bodyTypes.begin(), sv->bodyTypes.end(), w->body_types))))
+        return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: body types changed; use cn_solver_sync_world");
     CN_CUDA(cudaSetDevice(sv->device));
     CN_CUDA(cudaDeviceSynchronize()); // frames in flight read these buffers
     cudaStream_t st = sv->ownStream;
@@ -1316,27 +1348,10 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
         CN_CUDA(up(s.meta, w->metadata, N, st));
         CN_CUDA(up(s.matIdx, w->material_indices, N, st));
         CN_CUDA(up(s.fluidMatIdx, w->fluid_material_indices, N, st));
-        if (w->contact_material_count > std::max<uint32_t>(sv->contactMaterialCapacity, 1u) ||
-            w->fluid_material_count > std::max<uint32_t>(sv->fluidMaterialCapacity, 1u))
-            return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: more materials than synced; use cn_solver_sync_world");
         CN_CUDA(up(s.contactMaterials, w->contact_materials, w->contact_material_count, st));
         CN_CUDA(up(s.fluidMaterials, w->fluid_materials, w->fluid_material_count, st));
-        if (s.nProxy) {
-            if (!w->rigid_proxy_local_positions)
-                return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: rigid proxy local positions missing");
-            CN_CUDA(up(s.proxyLocal, w->rigid_proxy_local_positions, s.nProxy, st));
-        }
+        if (s.nProxy) CN_CUDA(up(s.proxyLocal, w->rigid_proxy_local_positions, s.nProxy, st));
     }
-    if ((flags & CN_SYNC_PARTICLE_ATTRIBUTES) && attributeStructure(*w) != sv->attributeStructure)
-        return setError(CN_ERR_INVALID_ARGUMENT,
-                        "cn_solver_update_world: the attributes change which contact or fluid terms run "
-                        "(self-collision, solid groups, vorticity, cohesion / surface tension); use cn_solver_sync_world");
-    if ((flags & CN_SYNC_CONSTRAINTS) && topologyHash(*w) != sv->topologyHash)
-        return setError(CN_ERR_INVALID_ARGUMENT,
-                        "cn_solver_update_world: constraint particle indices changed; use cn_solver_sync_world");
-    if ((flags & CN_SYNC_RIGID_BODIES) && (s.B && (!w->body_types ||
-                                                   !std::equal(sv->bodyTypes.begin(), sv->bodyTypes.end(), w->body_types))))
-        return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: body types changed; use cn_solver_sync_world");
     if (flags & CN_SYNC_CONSTRAINTS) {
         // records only: incidence tables depend on the particle indices, which must not change
         CN_CUDA(up(s.edges, w->edges, s.E, st));
@@ -1357,11 +1372,7 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
         CN_CUDA(up(s.bodyKinPos, w->body_kinematic_target_positions, s.B, st));
         CN_CUDA(up(s.bodyKinRot, w->body_kinematic_target_orientations, s.B, st));
         CN_CUDA(up(s.bodyKinFlags, w->body_kinematic_target_flags, s.B, st));
-        if (s.nProxy) {
-            if (!w->body_proxy_contact_materials)
-                return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: proxy contact materials missing");
-            CN_CUDA(up(s.bodyProxyMat, w->body_proxy_contact_materials, s.B, st));
-        }
+        if (s.nProxy) CN_CUDA(up(s.bodyProxyMat, w->body_proxy_contact_materials, s.B, st));
     }
     if (flags & CN_SYNC_COLLIDERS) {
         CN_CUDA(up(s.colGeo, w->collider_geometry, s.C, st));
@@ -1369,10 +1380,7 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
         CN_CUDA(up(s.colMat, w->collider_materials, s.C, st));
     }
     if (flags & CN_SYNC_SURFACE_RENDER) {
-        // the index-array length may differ at equal vertex counts: it must fit the synced one
-        const cn_surface_render_data *sr = w->surface_render;
-        if (sr && sr->vertex_triangle_index_count > sv->surfIdxCapacity)
-            return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_update_world: more incident-triangle indices than synced");
+        // the index-array length may differ at equal vertex counts (checked above to fit the synced one)
         const cn_status r = uploadSurfaceRender(sv, *w, st);
         if (r != CN_OK) return r;
     }

@@ -600,7 +600,8 @@ typedef enum cn_sync_flags {
                                      * (segment) indices must be the synced ones (else refused) */
     CN_SYNC_RIGID_BODIES = 8,       /* body poses, velocities, scales, inverse inertia, kinematic
                                      * targets; body types must be the synced ones (else refused) */
-    CN_SYNC_COLLIDERS = 16,         /* collider geometry, broadphase records, materials */
+    CN_SYNC_COLLIDERS = 16,         /* collider geometry, broadphase records, materials; refused
+                                     * when colliders are enabled, disabled or change bodies */
     CN_SYNC_SURFACE_RENDER = 32     /* surface render bindings, normals, triangles (same counts) */
 } cn_sync_flags;
 CN_API cn_status cn_solver_update_world(cn_solver *solver, const cn_world_soa *world, uint32_t flags);

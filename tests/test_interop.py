@@ -163,3 +163,30 @@ def test_incremental_attribute_update_equals_a_fresh_sync_unless_it_changes_the_
     fm[0].surface_tension = 0.5
     with pytest.raises(CNError):
         a.update_world(soa, "particle_attributes")
+
+
+def test_refused_incremental_update_uploads_nothing():
+    """Disabling a collider changes the colliders that are queried: refused (a full sync rebuilds
+    the query order), and the particle state flagged in the same call is not uploaded either."""
+    import ctypes as C
+    from cn_physics import CNError, solver_desc
+    w, b = body_on_ground_with_tissue()
+    desc = solver_desc(substeps=2, default_iterations=8)
+    soa = w.soa()
+    a, ref = Solver(desc), Solver(desc)
+    a.sync_world(soa)
+    ref.sync_world(soa)
+    w.velocities()[:, 0] += 1.0
+    words = np.ctypeslib.as_array(C.cast(C.c_void_p(soa.collider_broadphase), C.POINTER(C.c_uint32)),
+                                  (soa.collider_count, 8))
+    enabled = 5   # cn_collider_broadphase.enabled_flag
+    assert words[:, enabled].all()
+    words[-1, enabled] = 0
+    with pytest.raises(CNError):
+        a.update_world(soa, "particle_state", "colliders")
+    for _ in range(3):
+        a.step(1.0 / 60.0)
+        ref.step(1.0 / 60.0)
+    xa, va, _ = a.read_particles()
+    xr, vr, _ = ref.read_particles()
+    assert np.array_equal(xa, xr) and np.array_equal(va, vr)
