@@ -984,8 +984,10 @@ CN_API cn_status cn_batch_set_schedule(cn_batch *b, uint32_t tile_elements, uint
 }
 
 // Times one tick of the given scenes under each (tile size, blocks per SM) candidate, the fused
-// iterations and, in a colour-Jacobi batch, colour Jacobi, and keeps the fastest.  Each candidate's ticks run on copies of the state that are then discarded: the
-// scenes' particles, velocities and bodies are restored afterwards.
+// iterations and, in a colour-Jacobi batch, colour Jacobi, and keeps the fastest.  The trial
+// ticks' effects are discarded: the scenes' particles, velocities and bodies are restored from
+// host copies, and the correction records (which a tet that keeps its previous corrections
+// re-applies) from a device copy.
 CN_API cn_status cn_batch_autotune(cn_batch *b, const uint32_t *scene_ids, uint32_t count, float frame_dt,
                                    cn_batch_tuning *out)
 {
@@ -1011,6 +1013,30 @@ CN_API cn_status cn_batch_autotune(cn_batch *b, const uint32_t *scene_ids, uint3
         return cudaSuccess;
     };
     CN_CUDA(save(true));
+    // the correction records, kept on the device (edge and tet gather slots, colour-ordered tet records)
+    struct DevItem { void *dev; size_t bytes; };
+    const DevItem records[] = {{s.edgeCorr, sizeof(float4) * 2 * size_t(b->E)},
+                               {s.tetCorr, sizeof(float4) * 4 * size_t(b->T)},
+                               {s.tetRecC, s.tetRecC ? sizeof(float4) * 4 * size_t(b->T) : 0}};
+    size_t recordBytes = 0;
+    for (const DevItem &it : records) recordBytes += it.bytes;
+    uint8_t *recordCopy = nullptr;
+    CN_CUDA(cudaMalloc(&recordCopy, std::max<size_t>(recordBytes, 16)));
+    auto copyRecords = [&](bool toCopy) -> cudaError_t {
+        size_t at = 0;
+        for (const DevItem &it : records) {
+            if (!it.bytes) continue;
+            const cudaError_t e = toCopy ? cudaMemcpy(recordCopy + at, it.dev, it.bytes, cudaMemcpyDeviceToDevice)
+                                         : cudaMemcpy(it.dev, recordCopy + at, it.bytes, cudaMemcpyDeviceToDevice);
+            if (e != cudaSuccess) return e;
+            at += it.bytes;
+        }
+        return cudaSuccess;
+    };
+    if (copyRecords(true) != cudaSuccess) {
+        cudaFree(recordCopy);
+        return setError(CN_ERR_CUDA, "cn_batch_autotune: cannot copy the correction records");
+    }
     const std::vector<cn::BodyTarget> staged = b->pendingTargets;
     b->pendingTargets.clear();
     const uint32_t tiles[] = {128, 256, 512, 1024};
@@ -1045,7 +1071,8 @@ CN_API cn_status cn_batch_autotune(cn_batch *b, const uint32_t *scene_ids, uint3
             bestCtas = ctas;
             bestSchedule = schedule;
         }
-        const cudaError_t e = save(false);
+        cudaError_t e = save(false);
+        if (e == cudaSuccess) e = copyRecords(false);
         return e == cudaSuccess ? CN_OK : setError(CN_ERR_CUDA, std::string("cn_batch_autotune: ") + cudaGetErrorString(e));
     };
     cn_status st = cn_batch_set_fused(b, 0);
@@ -1087,7 +1114,9 @@ CN_API cn_status cn_batch_autotune(cn_batch *b, const uint32_t *scene_ids, uint3
     if (st == CN_OK) st = cn_batch_set_xpbd_schedule(b, bestSchedule);
     if (st == CN_OK) st = cn_batch_set_schedule(b, bestTile, bestBlocks);
     if (st == CN_OK) st = cn_batch_set_fused(b, bestCtas);
-    CN_CUDA(save(false));
+    const cudaError_t restored = save(false) == cudaSuccess ? copyRecords(false) : cudaErrorUnknown;
+    cudaFree(recordCopy);
+    if (restored != cudaSuccess) return setError(CN_ERR_CUDA, "cn_batch_autotune: cannot restore the scenes' state");
     b->pendingTargets = staged;
     b->ticks = 0;
     return st;
