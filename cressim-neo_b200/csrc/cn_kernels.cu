@@ -2960,6 +2960,25 @@ __device__ __forceinline__ void colourConstraintOrdered(const Scene &s, float dt
     }
 }
 
+// Colour position q of family kFam: the colour-ordered edges and tets where the scene holds them,
+// else the constraint the colour order names.
+template <uint32_t kFam>
+__device__ __forceinline__ void colourAt(const Scene &s, float dt, float relax, bool gaussSeidel, uint32_t q)
+{
+    if constexpr (kFam == kFamEdges) {
+        if (s.edgesC) {
+            colourConstraintOrdered<kFamEdges>(s, dt, relax, gaussSeidel, q);
+            return;
+        }
+    } else if constexpr (kFam == kFamTets) {
+        if (s.tetsC) {
+            colourConstraintOrdered<kFamTets>(s, dt, relax, gaussSeidel, q);
+            return;
+        }
+    }
+    colourConstraint<kFam>(s, dt, relax, gaussSeidel, s.colOrder[kFam][q]);
+}
+
 // End of a colour-Jacobi family: x += the family's sum (particles with invMass > kEps), sum
 // cleared; for joints the orientation sum, then the normalisation every segment gets.
 __device__ __forceinline__ void colourJacobiApplyAt(const Scene &s, uint32_t i)
@@ -2982,7 +3001,7 @@ __global__ void __launch_bounds__(kThreads) k_colourSolve(Scene s, float dt, flo
 {
     pdlEnter();
     const uint32_t k = begin + blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < end) colourConstraint<kFam>(s, dt, relax, kGaussSeidel, s.colOrder[kFam][k]);
+    if (k < end) colourAt<kFam>(s, dt, relax, kGaussSeidel, k);
 }
 
 __global__ void __launch_bounds__(kThreads) k_colourJacobiApply(Scene s, uint2 win)
@@ -3098,11 +3117,10 @@ __device__ __forceinline__ void fusedFamily(const Scene &s, float dt, float rela
         cg::this_cluster().sync();
     } else {
         constexpr bool gs = kSchedule == CN_XPBD_COLOUR_GAUSS_SEIDEL;
-        const uint32_t *order = s.colOrder[kFam];
         const uint32_t *starts = plan.starts[kFam];
         for (uint32_t k = 0; k < plan.colours[kFam]; ++k) {
             const uint32_t b = starts[k], e = starts[k + 1];
-            for (uint32_t j = b + tid; j < e; j += nth) colourConstraint<kFam>(s, dt, relax, gs, order[j]);
+            for (uint32_t j = b + tid; j < e; j += nth) colourAt<kFam>(s, dt, relax, gs, j);
             cg::this_cluster().sync();
         }
         if constexpr (!gs) {

@@ -44,6 +44,8 @@ struct cn_solver {
     std::vector<uint32_t> bodyTypes;
     uint32_t attributeStructure = 0; // attributeStructure() of the synced world
     std::vector<uint32_t> queryOrder; // the colliders queried (enabled, of a present body), in order
+    std::vector<cn_soft_edge> edgesC; // host staging of the colour-ordered copies (coloured schedules)
+    std::vector<cn_soft_tet> tetsC;
     cudaStream_t ownStream = nullptr;
     cn::Scene s{};
     cn::Config cfg{};
@@ -203,6 +205,12 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
         sv->plan.devStarts[f] = col.colours() ? a.take<uint32_t>(col.starts.size()) : nullptr;
     }
     const bool coloured = sv->plan.schedule != CN_XPBD_GATHER;
+    // the coloured schedules read the edges and tets in colour order (a colour is a contiguous
+    // range); their lambdas are indexed by colour position and the tets' last corrections sit in
+    // the tet records, by colour position, which the gather schedule would use otherwise
+    s.edgesC = coloured && s.E ? a.take<cn_soft_edge>(s.E) : nullptr;
+    s.tetsC = coloured && s.T ? a.take<cn_soft_tet>(s.T) : nullptr;
+    s.tetRecC = s.tetsC ? s.tetCorr : nullptr;
     s.softAcc = coloured ? a.take<float4>(N) : nullptr;
     s.orientAcc = coloured ? a.take<float4>(w.strand_segment_count) : nullptr;
     s.B = w.rigid_body_count;
@@ -738,6 +746,29 @@ static uint32_t attributeStructure(const cn_world_soa &w)
     return bits;
 }
 
+// The edges and tets in colour order, for the coloured schedules.
+static cudaError_t uploadColourOrdered(cn_solver *sv, const cn_world_soa &w, cudaStream_t st)
+{
+    const cn::Scene &s = sv->s;
+    if (s.edgesC) {
+        const std::vector<uint32_t> &order = sv->colouring[cn::kFamEdges].order;
+        sv->edgesC.resize(order.size());
+        for (size_t i = 0; i < order.size(); ++i) sv->edgesC[i] = w.edges[order[i]];
+        const cudaError_t e = cudaMemcpyAsync(const_cast<cn_soft_edge *>(s.edgesC), sv->edgesC.data(),
+                                              sizeof(cn_soft_edge) * order.size(), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+    }
+    if (s.tetsC) {
+        const std::vector<uint32_t> &order = sv->colouring[cn::kFamTets].order;
+        sv->tetsC.resize(order.size());
+        for (size_t i = 0; i < order.size(); ++i) sv->tetsC[i] = w.tets[order[i]];
+        const cudaError_t e = cudaMemcpyAsync(const_cast<cn_soft_tet *>(s.tetsC), sv->tetsC.data(),
+                                              sizeof(cn_soft_tet) * order.size(), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
 {
     if (!sv || !w) return setError(CN_ERR_INVALID_ARGUMENT, "cn_solver_sync_world: null argument");
@@ -1027,6 +1058,7 @@ CN_API cn_status cn_solver_sync_world(cn_solver *sv, const cn_world_soa *w)
         CN_CUDA(up(const_cast<uint32_t *>(s.colOrder[f]), col.order.data(), col.order.size(), st));
         CN_CUDA(up(const_cast<uint32_t *>(sv->plan.devStarts[f]), col.starts.data(), col.starts.size(), st));
     }
+    CN_CUDA(uploadColourOrdered(sv, *w, st));
     CN_CUDA(up(s.bodyPos, w->body_positions_inv_mass, s.B, st));
     CN_CUDA(up(s.bodyRot, w->body_orientations, s.B, st));
     CN_CUDA(up(s.bodyLin, w->body_linear_velocities, s.B, st));
@@ -1361,6 +1393,7 @@ CN_API cn_status cn_solver_update_world(cn_solver *sv, const cn_world_soa *w, ui
         CN_CUDA(up(s.segs, w->strand_segments, s.S, st));
         CN_CUDA(up(s.joints, w->strand_joints, s.J, st));
         CN_CUDA(up(s.dists, w->strand_distances, s.SD, st));
+        CN_CUDA(uploadColourOrdered(sv, *w, st)); // the coloured schedules' copies of the records
     }
     if (flags & CN_SYNC_RIGID_BODIES) {
         CN_CUDA(up(s.bodyPos, w->body_positions_inv_mass, s.B, st));

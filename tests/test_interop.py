@@ -190,3 +190,24 @@ def test_refused_incremental_update_uploads_nothing():
     xa, va, _ = a.read_particles()
     xr, vr, _ = ref.read_particles()
     assert np.array_equal(xa, xr) and np.array_equal(va, vr)
+
+
+def test_incremental_constraint_update_under_a_coloured_schedule_equals_a_fresh_sync():
+    """The coloured schedules read colour-ordered copies of the edges and tets: an in-place update
+    of the tet compliances refreshes them."""
+    from cn_physics._abi import XPBD_COLOUR_GAUSS_SEIDEL
+    w, desc, dt = scenes.xpbd_cube(n=6, spacing=0.1)
+    desc.soft.xpbd_schedule = XPBD_COLOUR_GAUSS_SEIDEL
+    a = Solver(desc)
+    a.sync_world(w)
+    tets = w.array("tets").view(np.float32)
+    tets[:, 5] = tets[:, 5] * 0.25 + 1e-7
+    a.update_world(w, "constraints")
+    fresh = Solver(desc)
+    fresh.sync_world(w)
+    for _ in range(3):
+        a.step(dt)
+        fresh.step(dt)
+    xa, va, _ = a.read_particles()
+    xf, vf, _ = fresh.read_particles()
+    assert np.array_equal(xa, xf) and np.array_equal(va, vf)
