@@ -748,6 +748,13 @@ __global__ void __launch_bounds__(kThreads) k_particleCandidates(Scene s, const 
                     }
                     const uint32_t c = s.valsA[slot];
                     if (c <= i) continue;
+                    // the filters are independent of one another: the distance test, which
+                    // rejects most candidates, comes first, so the metadata loads and the
+                    // adjacency scan run for the pairs in contact range only
+                    const f3 op = xyz(s.x[c]);
+                    const float cr = r + s.radii[c];
+                    const f3 d = op - pos;
+                    if (!(dot(d, d) <= cr * cr)) continue;
                     const uint4 om = s.meta[c];
                     if (om.x != m.x) continue;
                     if ((m.w & om.z) == 0u || (om.w & m.z) == 0u) continue;
@@ -759,10 +766,6 @@ __global__ void __launch_bounds__(kThreads) k_particleCandidates(Scene s, const 
                         const bool b = (om.y & CN_PHASE_SELF_COLLIDE) != 0u;
                         if (!a || !b || isAdjacent(s, i, c)) continue;
                     }
-                    const f3 op = xyz(s.x[c]);
-                    const float cr = r + s.radii[c];
-                    const f3 d = op - pos;
-                    if (!(dot(d, d) <= cr * cr)) continue;
                     if (kEmit) {
                         if (write >= s.particlePairCapacity) return;
                         s.particlePairs[write++] = make_uint2(i, c);
