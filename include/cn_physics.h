@@ -754,7 +754,8 @@ CN_API cn_status cn_batch_create(const cn_batch_desc *desc, int cuda_device, cn_
 CN_API void cn_batch_destroy(cn_batch *batch);
 /* Admits one scene (a world SoA with 0-based indices).  CN_ERR_CAPACITY when the budget or the
  * pool has no room; CN_ERR_UNSUPPORTED for fluid, cloth, strand, self-colliding or dynamic-body
- * content.  The upload is asynchronous: the scene's arrays go to the device in one transfer and
+ * content, and in a batch created with a coloured schedule for an edge or tet family that needs
+ * more than 256 colours.  The upload is asynchronous: the scene's arrays go to the device in one transfer and
  * are scattered into its pool ranges on the batch's upload stream, which the next cn_batch_step
  * waits for; the SoA may be reused as soon as the call returns. */
 CN_API cn_status cn_batch_add_scene(cn_batch *batch, const cn_world_soa *world, uint32_t *out_scene);
