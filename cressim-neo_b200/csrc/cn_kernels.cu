@@ -33,6 +33,9 @@ constexpr bool kInterleavedLists = true;
 constexpr bool kInterleavedLists = false;
 #endif
 inline unsigned blocksFor(size_t n) { return n == 0 ? 1u : unsigned((n + kThreads - 1) / kThreads); }
+// Block size of the fluid neighbour and delta kernels.
+constexpr uint32_t kFluidThreads = 128u;
+inline unsigned fluidBlocksFor(size_t n) { return n == 0 ? 1u : unsigned((n + kFluidThreads - 1) / kFluidThreads); }
 // Grid of a kernel that strides over a device-counted list of capacity n: 16 blocks per SM at most.
 inline unsigned pairGrid(size_t n) { return std::min<unsigned>(blocksFor(n), 148u * 16u); }
 // Per-slot fluid word: bit 31 = fluid particle, bits 16..30 = fluid material, bits 0..15 = filter
@@ -947,7 +950,7 @@ __device__ __forceinline__ bool neighborAllowed(const Scene &s, uint32_t tag, ui
 // (fewer live registers: the kernels then run at 5 blocks of 256 per SM without spills -- the
 // filter 10 %, the superset build 5 % faster than the full build, measured).
 template <uint32_t mode, bool kExtras>
-__global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidNeighborsDensity(Scene s, Config cfg, bool density,
+__global__ void __launch_bounds__(kFluidThreads, (kExtras ? 4 : 5) * (256 / kFluidThreads)) k_fluidNeighborsDensity(Scene s, Config cfg, bool density,
                                                                                     uint32_t iter, float4 *Dk)
 {
     pdlEnter();
@@ -1120,7 +1123,7 @@ __global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidNeighborsDen
 // kExtras false: no fluid material of the scene has cohesion or surface tension, so those terms
 // are zero for every pair and the kernel is built without them (fewer live registers).
 template <bool kExtras>
-__global__ void __launch_bounds__(kThreads, kExtras ? 4 : 5) k_fluidDeltaApplyClamp(Scene s, Config cfg, const float4 *Xs,
+__global__ void __launch_bounds__(kFluidThreads, (kExtras ? 4 : 5) * (256 / kFluidThreads)) k_fluidDeltaApplyClamp(Scene s, Config cfg, const float4 *Xs,
                                                                    const float4 *Dcur, float4 *Dnext,
                                                                    uint32_t iter, float dt, bool writeDx,
                                                                    float4 *Pnext)
@@ -2795,20 +2798,20 @@ void launchFluidNeighborsDensity(const Scene &s, const Config &c, uint32_t iter,
     if (s.N == 0) return;
     const Scene sp = withPositions(s, iter);
     float4 *Dk = (iter & 1u) ? s.Db : s.Da;
-    const unsigned g = blocksFor(s.N);
+    const unsigned g = fluidBlocksFor(s.N);
     if (s.sup == nullptr || walkCells) {
-        if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<0u, true>, g, kThreads, st, sp, c, true, iter, Dk);
-        else launchPdl(k_fluidNeighborsDensity<0u, false>, g, kThreads, st, sp, c, true, iter, Dk);
+        if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<0u, true>, g, kFluidThreads, st, sp, c, true, iter, Dk);
+        else launchPdl(k_fluidNeighborsDensity<0u, false>, g, kFluidThreads, st, sp, c, true, iter, Dk);
     } else if (iter == 0 && !kSplitSupersetBuild) {
-        if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<1u, true>, g, kThreads, st, sp, c, true, iter, Dk);
-        else launchPdl(k_fluidNeighborsDensity<1u, false>, g, kThreads, st, sp, c, true, iter, Dk);
+        if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<1u, true>, g, kFluidThreads, st, sp, c, true, iter, Dk);
+        else launchPdl(k_fluidNeighborsDensity<1u, false>, g, kFluidThreads, st, sp, c, true, iter, Dk);
     } else {
         if (iter == 0) { // the superset, then the filter below
-            if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<3u, true>, g, kThreads, st, sp, c, true, iter, Dk);
-            else launchPdl(k_fluidNeighborsDensity<3u, false>, g, kThreads, st, sp, c, true, iter, Dk);
+            if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<3u, true>, g, kFluidThreads, st, sp, c, true, iter, Dk);
+            else launchPdl(k_fluidNeighborsDensity<3u, false>, g, kFluidThreads, st, sp, c, true, iter, Dk);
         }
-        if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<2u, true>, g, kThreads, st, sp, c, true, iter, Dk);
-        else launchPdl(k_fluidNeighborsDensity<2u, false>, g, kThreads, st, sp, c, true, iter, Dk);
+        if (s.fluidExtras) launchPdl(k_fluidNeighborsDensity<2u, true>, g, kFluidThreads, st, sp, c, true, iter, Dk);
+        else launchPdl(k_fluidNeighborsDensity<2u, false>, g, kFluidThreads, st, sp, c, true, iter, Dk);
     }
 }
 
@@ -2820,10 +2823,10 @@ void launchFluidDeltaApplyClamp(const Scene &s, uint32_t iter, float dt, const C
     float4 *Dnext = (iter & 1u) ? s.Da : s.Db;
     float4 *Pnext = s.Pb ? ((iter & 1u) ? s.P : s.Pb) : nullptr;
     if (s.fluidExtras)
-        launchPdl(k_fluidDeltaApplyClamp<true>, blocksFor(s.N), kThreads, st, withPositions(s, iter), c, s.Xs, Dcur, Dnext,
+        launchPdl(k_fluidDeltaApplyClamp<true>, fluidBlocksFor(s.N), kFluidThreads, st, withPositions(s, iter), c, s.Xs, Dcur, Dnext,
                                                                       iter, dt, writeDebug, Pnext);
     else
-        launchPdl(k_fluidDeltaApplyClamp<false>, blocksFor(s.N), kThreads, st, withPositions(s, iter), c, s.Xs, Dcur, Dnext,
+        launchPdl(k_fluidDeltaApplyClamp<false>, fluidBlocksFor(s.N), kFluidThreads, st, withPositions(s, iter), c, s.Xs, Dcur, Dnext,
                                                                        iter, dt, writeDebug, Pnext);
 }
 
@@ -2848,7 +2851,7 @@ void launchFluidNeighborsOnly(const Scene &s, cudaStream_t st)
     // Positions after the velocity update; the accumulated delta was folded into x.
     launchPdl(k_fluidGather, blocksFor(s.N), kThreads, st, s, s.Xs, s.Da, 0u, nullptr, nullptr);
     Config dummy{};
-    launchPdl(k_fluidNeighborsDensity<0u, false>, blocksFor(s.N), kThreads, st, s, dummy, false, 0u, nullptr);
+    launchPdl(k_fluidNeighborsDensity<0u, false>, fluidBlocksFor(s.N), kFluidThreads, st, s, dummy, false, 0u, nullptr);
 }
 
 // ------------------------------------------------------------------------------------------
