@@ -66,10 +66,13 @@ template <class F> __device__ __forceinline__ void forEachElem(const WorkList &w
 }
 inline unsigned gridFor(const WorkList &w, size_t n) { return w.tiles ? w.grid : blocksFor(n); }
 
-// The soft families' solves and gathers and the particle-rigid contacts run in blocks of 128: a
-// small scene's few hundred to few thousand elements then spread over more SMs (the 16^3 cube's
-// frame 3.30 -> 3.06 ms).  Their grids count blocks of that size; a batch keeps its work-list grid.
-constexpr int kSoftThreads = 128;
+// The soft families' solves and gathers, the colour passes and the particle-rigid contacts run in
+// small blocks: a single world's few hundred to few thousand elements then spread over more SMs
+// (64 threads: the 16^3 cube's frame 3.30 -> 2.94 ms), a batch's work-list grid in blocks of 128
+// (its tick is 8 % slower with 64).
+constexpr int kSoftThreads = 64;
+constexpr int kSoftBatchThreads = 128;
+inline unsigned softThreads(const Scene &s) { return s.wP.tiles ? kSoftBatchThreads : kSoftThreads; }
 inline unsigned softBlocksFor(size_t n) { return n == 0 ? 1u : unsigned((n + kSoftThreads - 1) / kSoftThreads); }
 inline unsigned softGridFor(const WorkList &w, size_t n) { return w.tiles ? w.grid : softBlocksFor(n); }
 inline unsigned softApplyGrid(const Scene &s, uint2 win)
@@ -3064,15 +3067,15 @@ void launchColourFamily(const Scene &s, float dt, float relax, const XpbdPlan &p
     for (uint32_t k = 0; k < plan.colours[kFam]; ++k) {
         const uint32_t b = starts[k], e = starts[k + 1];
         if (e <= b) continue;
-        if (gs) launchPdl(k_colourSolve<kFam, true>, softBlocksFor(e - b), kSoftThreads, st, s, dt, relax, b, e);
-        else launchPdl(k_colourSolve<kFam, false>, softBlocksFor(e - b), kSoftThreads, st, s, dt, relax, b, e);
+        if (gs) launchPdl(k_colourSolve<kFam, true>, softBlocksFor(e - b), softThreads(s), st, s, dt, relax, b, e);
+        else launchPdl(k_colourSolve<kFam, false>, softBlocksFor(e - b), softThreads(s), st, s, dt, relax, b, e);
     }
     if (gs) return;
     if (kFam == kFamJoints) {
-        launchPdl(k_colourJacobiOrient, softBlocksFor(s.S), kSoftThreads, st, s);
+        launchPdl(k_colourJacobiOrient, softBlocksFor(s.S), softThreads(s), st, s);
     } else {
         const uint2 win = familyWindow(s, kFam);
-        if (win.y > win.x) launchPdl(k_colourJacobiApply, softBlocksFor(win.y - win.x), kSoftThreads, st, s, win);
+        if (win.y > win.x) launchPdl(k_colourJacobiApply, softBlocksFor(win.y - win.x), softThreads(s), st, s, win);
     }
 }
 
@@ -3548,33 +3551,33 @@ bool launchSoftFamilies(const Scene &s, float dt, const Config &c, cudaStream_t 
     const float relax = c.softInternalRelaxation;
     auto on = [&](uint32_t f) { return ((families >> f) & 1u) != 0u; };
     if (s.E && on(kFamEdges)) {
-        launchPdl(k_solveEdges, softGridFor(s.wE, s.E), kSoftThreads, st, s, dt, relax);
-        launchPdl(k_applyGather, softApplyGrid(s, s.edgeWin), kSoftThreads, st, s, s.edgeRanges, s.edgeCorr, s.edgeWin);
+        launchPdl(k_solveEdges, softGridFor(s.wE, s.E), softThreads(s), st, s, dt, relax);
+        launchPdl(k_applyGather, softApplyGrid(s, s.edgeWin), softThreads(s), st, s, s.edgeRanges, s.edgeCorr, s.edgeWin);
     }
     if (s.S && on(kFamSegments)) {
-        launchPdl(k_solveSegments, softBlocksFor(s.S), kSoftThreads, st, s, dt, relax);
-        launchPdl(k_applySegments, softBlocksFor(segmentApplyThreads(s)), kSoftThreads, st, s);
+        launchPdl(k_solveSegments, softBlocksFor(s.S), softThreads(s), st, s, dt, relax);
+        launchPdl(k_applySegments, softBlocksFor(segmentApplyThreads(s)), softThreads(s), st, s);
     }
     if ((s.Bn || s.D) && on(kFamBends)) {
-        if (s.Bn) launchPdl(k_solveBends, softBlocksFor(s.Bn), kSoftThreads, st, s, dt, relax);
-        if (s.D) launchPdl(k_solveDihedrals, softBlocksFor(s.D), kSoftThreads, st, s, dt, relax);
-        launchPdl(k_applyGather, softApplyGrid(s, s.bendWin), kSoftThreads, st, s, s.bendRanges, s.bendCorr, s.bendWin);
+        if (s.Bn) launchPdl(k_solveBends, softBlocksFor(s.Bn), softThreads(s), st, s, dt, relax);
+        if (s.D) launchPdl(k_solveDihedrals, softBlocksFor(s.D), softThreads(s), st, s, dt, relax);
+        launchPdl(k_applyGather, softApplyGrid(s, s.bendWin), softThreads(s), st, s, s.bendRanges, s.bendCorr, s.bendWin);
     }
     if (s.J && on(kFamJoints)) {
-        launchPdl(k_solveJoints, softBlocksFor(s.J), kSoftThreads, st, s, dt, relax);
-        launchPdl(k_applyJoints, softBlocksFor(s.S), kSoftThreads, st, s);
+        launchPdl(k_solveJoints, softBlocksFor(s.J), softThreads(s), st, s, dt, relax);
+        launchPdl(k_applyJoints, softBlocksFor(s.S), softThreads(s), st, s);
     }
     if (s.SD && on(kFamDistances)) {
-        launchPdl(k_solveDistances, softBlocksFor(s.SD), kSoftThreads, st, s, dt, relax);
-        launchPdl(k_applyGather, softApplyGrid(s, s.segWin), kSoftThreads, st, s, s.segRanges, s.distCorr, s.segWin);
+        launchPdl(k_solveDistances, softBlocksFor(s.SD), softThreads(s), st, s, dt, relax);
+        launchPdl(k_applyGather, softApplyGrid(s, s.segWin), softThreads(s), st, s, s.segRanges, s.distCorr, s.segWin);
     }
     if (s.T && on(kFamTets)) {
-        launchPdl(k_solveTets, softGridFor(s.wT, s.T), kSoftThreads, st, s, dt, relax);
+        launchPdl(k_solveTets, softGridFor(s.wT, s.T), softThreads(s), st, s, dt, relax);
         if (rigidContacts && s.N) {
-            launchPdl(k_applyTetsRigidContacts, softGridFor(s.wP, s.N), kSoftThreads, st, s, c);
+            launchPdl(k_applyTetsRigidContacts, softGridFor(s.wP, s.N), softThreads(s), st, s, c);
             return true;
         }
-        launchPdl(k_applyGather, softApplyGrid(s, s.tetWin), kSoftThreads, st, s, s.tetRanges, s.tetCorr, s.tetWin);
+        launchPdl(k_applyGather, softApplyGrid(s, s.tetWin), softThreads(s), st, s, s.tetRanges, s.tetCorr, s.tetWin);
     }
     return false;
 }
@@ -3586,7 +3589,7 @@ void launchContacts(const Scene &s, const Config &c, bool particleContacts, bool
         const uint32_t cap = s.particlePairCapacity;
         launchPdl(k_particleContacts, pairGrid(cap), kThreads, st, s, c);
     }
-    if (rigidContacts) launchPdl(k_rigidContacts, softGridFor(s.wP, s.N), kSoftThreads, st, s, c, !particleContacts);
+    if (rigidContacts) launchPdl(k_rigidContacts, softGridFor(s.wP, s.N), softThreads(s), st, s, c, !particleContacts);
     if (particleContacts) launchPdl(k_applyPositionCorrections, blocksFor(s.N), kThreads, st, s);
 }
 
