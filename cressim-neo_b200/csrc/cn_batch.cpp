@@ -334,17 +334,20 @@ void enqueueTick(cn_batch *b, float frameDt, cudaStream_t st)
             const bool runSoft = (s.E || s.T) && it < b->softIt;
             const bool runRigid = it < b->contactIt;
             if (!runSoft && !runRigid) break;
+            // the contact records are read after the iterations: written by the last contact pass only
+            cn::Scene si = s;
+            si.storeRigidContacts = it + 1 == b->contactIt ? 1u : 0u;
             if (b->schedule != CN_XPBD_GATHER) {
                 // one kernel per colour over every stepped scene, then the contacts
                 if (runSoft)
                     cn::launchBatchColourIteration(s, dt, c, b->schedule, b->colours, b->dScenes, b->dCounts + 6,
                                                    b->grid, st);
-                if (runRigid) cn::launchContacts(s, c, false, true, st);
+                if (runRigid) cn::launchContacts(si, c, false, true, st);
                 continue;
             }
             // the rigid contacts run in the tet gather's pass when there is a tet family
-            const bool contactsDone = runSoft && cn::launchSoftIteration(s, dt, c, st, runRigid);
-            if (runRigid && !contactsDone) cn::launchContacts(s, c, false, true, st);
+            const bool contactsDone = runSoft && cn::launchSoftIteration(si, dt, c, st, runRigid);
+            if (runRigid && !contactsDone) cn::launchContacts(si, c, false, true, st);
         }
         cn::launchUpdateVelocities(s, dt, nullptr, st);
         if (b->contactIt) cn::launchRigidContactVelocities(s, b->contactIt, c, st);

@@ -202,6 +202,9 @@ struct Scene {
     const float4 *bodyProxyMat = nullptr;  // per body: its proxies' contact material
     // dynamic bodies: corrections summed (float atomics) over a pass, applied per body after it
     uint32_t hasDynamic = 0;
+    // the particle-rigid contact pass writes its contact records (read by the velocity passes after
+    // the iterations): the iteration loops set it for their last contact iteration only
+    uint32_t storeRigidContacts = 1;
     float4 *bodyTransCorr = nullptr, *bodyRotCorr = nullptr, *bodyLinVelCorr = nullptr, *bodyAngVelCorr = nullptr;
     // Per collider, the world frame the fluid boundary queries use this substep (4 float4:
     // centre + shape/enabled word, orientation, shape extents, capsule end).

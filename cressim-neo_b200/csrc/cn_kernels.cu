@@ -1412,11 +1412,11 @@ __global__ void __launch_bounds__(kThreads) k_solveEdges(Scene s, float dt, floa
 // with the range and the records as the only dependent loads.
 constexpr uint32_t kGatherBatch = 8u;
 
-__device__ __forceinline__ void applyGatherAt(const Scene &s, const uint2 *ranges, const float4 *corr, uint32_t i)
+// x + the particle's records summed in list order (x itself for a particle without weight).
+__device__ __forceinline__ float4 gatheredPosition(const uint2 *ranges, const float4 *corr, uint32_t i, const float4 p)
 {
-    const float4 p = s.x[i];
     const uint2 r = ranges[i];
-    if (p.w <= kEps) return;
+    if (p.w <= kEps) return p;
     f3 total{0.f, 0.f, 0.f};
     for (uint32_t k = 0; k < r.y; k += kGatherBatch) {
         float4 c[kGatherBatch];
@@ -1427,7 +1427,13 @@ __device__ __forceinline__ void applyGatherAt(const Scene &s, const uint2 *range
         for (uint32_t j = 0; j < kGatherBatch; ++j)
             if (k + j < r.y) total += xyz(c[j]);
     }
-    s.x[i] = mk4(xyz(p) + total, p.w);
+    return mk4(xyz(p) + total, p.w);
+}
+
+__device__ __forceinline__ void applyGatherAt(const Scene &s, const uint2 *ranges, const float4 *corr, uint32_t i)
+{
+    const float4 p = s.x[i];
+    if (p.w > kEps) s.x[i] = gatheredPosition(ranges, corr, i, p);
 }
 
 // physics_soft_apply_edge_corrections.cs.hlsl:9-35, physics_soft_apply_tet_corrections.cs.hlsl:9-50,
@@ -2148,11 +2154,12 @@ __device__ __forceinline__ ContactCorrection solveRigidContact(const Scene &s, c
 // Generate + solve every candidate pair of particle i (pairs are particle-major), then either
 // accumulate into posCorr (explicit contacts present) or apply directly
 // (physics_particle_apply_position_corrections.cs.hlsl:8-30).
-__device__ __forceinline__ void rigidContactsAt(const Scene &s, const Config &cfg, bool applyDirect, uint32_t i)
+// Particle i's contacts from its position sp (its x, or the value the fused gather just computed).
+__device__ __forceinline__ void rigidContactsFrom(const Scene &s, const Config &cfg, bool applyDirect, uint32_t i,
+                                                  const float4 sp)
 {
     const uint32_t cnt = s.candCount[i];
     const uint32_t off = s.candOffset[i]; // with the count: one round trip fewer
-    const float4 sp = s.x[i];
     f3 corr{0.f, 0.f, 0.f};
     bool any = false;
     if (cnt) {
@@ -2163,7 +2170,7 @@ __device__ __forceinline__ void rigidContactsAt(const Scene &s, const Config &cf
             if (pi >= lim) break;
             const uint2 pr = s.rigidPairs[pi]; // pr.x == i: pairs are emitted particle-major
             const RigidContact c = generateRigidContact(s, i, pr.y, pt);
-            s.rigidContacts[pi] = c;
+            if (s.storeRigidContacts) s.rigidContacts[pi] = c;
             if (!c.active) continue;
             const ContactCorrection d = solveRigidContact(s, cfg, c, sp, pt);
             // the particle's float-atomic order of the reference == pair order here
@@ -2188,6 +2195,11 @@ __device__ __forceinline__ void rigidContactsAt(const Scene &s, const Config &cf
     }
 }
 
+__device__ __forceinline__ void rigidContactsAt(const Scene &s, const Config &cfg, bool applyDirect, uint32_t i)
+{
+    rigidContactsFrom(s, cfg, applyDirect, i, s.x[i]);
+}
+
 __global__ void __launch_bounds__(kThreads) k_rigidContacts(Scene s, Config cfg, bool applyDirect)
 {
     pdlEnter();
@@ -2202,9 +2214,11 @@ __global__ void __launch_bounds__(kThreads) k_rigidContacts(Scene s, Config cfg,
 __global__ void __launch_bounds__(kThreads) k_applyTetsRigidContacts(Scene s, Config cfg)
 {
     pdlEnter();
+    // the gathered position goes to the contacts in registers: x is read and written once
     forEachElem(s.wP, s.N, [&](uint32_t i) {
-        if (s.wP.tiles || (i >= s.tetWin.x && i < s.tetWin.y)) applyGatherAt(s, s.tetRanges, s.tetCorr, i);
-        rigidContactsAt(s, cfg, true, i);
+        float4 p = s.x[i];
+        if (s.wP.tiles || (i >= s.tetWin.x && i < s.tetWin.y)) p = gatheredPosition(s.tetRanges, s.tetCorr, i, p);
+        rigidContactsFrom(s, cfg, true, i, p);
     });
 }
 

@@ -538,17 +538,20 @@ void enqueueFrame(cn_solver *sv, float frameDt, cudaStream_t st)
             }
             if (fluidBranch) cudaEventRecord(sv->joinFluid, fst);
             // without particle-particle contacts (and without soft branches) the rigid contacts run
-            // in the tet gather's pass
+            // in the tet gather's pass; their records are read after the iterations, so only the last
+            // contact pass writes them
+            cn::Scene si = s;
+            si.storeRigidContacts = it + 1 == sv->contactIt ? 1u : 0u;
             bool contactsDone = false;
             if (runSoft && softBranches)
                 probe(sv, "soft_constraints", st, [&] { launchSoftBranches(sv, dt, st); });
             else if (runSoft)
                 probe(sv, "soft_constraints", st, [&] {
-                    contactsDone = cn::launchSoftIteration(s, dt, c, sv->plan, st, runRigid && !runPP);
+                    contactsDone = cn::launchSoftIteration(si, dt, c, sv->plan, st, runRigid && !runPP);
                 });
             if (fluidBranch) cudaStreamWaitEvent(st, sv->joinFluid, 0);
             if ((runPP || runRigid) && !contactsDone)
-                probe(sv, "contacts", st, [&] { cn::launchContacts(s, c, runPP, runRigid, st); });
+                probe(sv, "contacts", st, [&] { cn::launchContacts(si, c, runPP, runRigid, st); });
             // finalRigidContactDepenetration (physics_solver.cpp:1111-1117)
             if (runRigidRigid) probe(sv, "rigid_depenetration", st, [&] { cn::launchRigidDepenetration(s, c, st); });
             // applyRigidCorrections (physics_solver.cpp:1170-1177); with only static and kinematic
