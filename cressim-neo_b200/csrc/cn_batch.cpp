@@ -115,7 +115,7 @@ inline float fromBits(uint32_t u)
 
 // Device bytes one element of each family takes in the pool (used for the budget accounting).
 constexpr uint64_t kBytesPerParticle = 3 * 16 + 6 * 4 + 16 + 2 * 8 + 2 * 4 + 8;
-constexpr uint64_t kBytesPerEdge = 32 + 4 + 2 * 16 + 2 * 4;
+constexpr uint64_t kBytesPerEdge = 16 + 4 + 2 * 16 + 2 * 4;
 constexpr uint64_t kBytesPerTet = 32 + 4 + 4 * 16 + 4 * 4;
 constexpr uint64_t kBytesPerBody = 16 * 16 + 8 + 8;
 constexpr uint64_t kBytesPerCollider = 48 + 32 + 16 + 3 * 16 + 4 * 16 + 4 + 4;
@@ -258,7 +258,7 @@ void layoutPool(cn_batch *b, cn::Arena &a)
     s.contactMaterials = a.take<float4>(std::max<uint32_t>(b->M, 1u));
     s.fluidMaterials = a.take<cn_fluid_material>(1);
     s.E = E; s.T = T;
-    s.edges = a.take<cn_soft_edge>(E);
+    s.edgesP = a.take<cn::PackedEdge>(E);
     s.tets = a.take<cn_soft_tet>(T);
     s.edgeRanges = a.take<uint2>(P);
     s.tetRanges = a.take<uint2>(P);
@@ -293,7 +293,7 @@ void layoutPool(cn_batch *b, cn::Arena &a)
     s.rigidContacts = a.take<cn::RigidContact>(b->pairCap);
     s.meta_ = a.take<cn::DeviceMeta>(1);
     if (b->coloured) {
-        s.edgesC = a.take<cn_soft_edge>(E);
+        s.edgesC = a.take<cn::PackedEdge>(E);
         s.tetsC = a.take<cn_soft_tet>(T);
         s.tetRecC = a.take<float4>(size_t(T) * 4);
         s.softAcc = a.take<float4>(P);
@@ -513,7 +513,7 @@ cn_status buildSceneImage(const cn_world_soa &w, uint32_t rigidPairsPerParticle,
                       uint64_t(L.B) * kBytesPerBody + uint64_t(L.C) * kBytesPerCollider +
                       uint64_t(N) * rigidPairsPerParticle * 72u;
     if (coloured) // colour-ordered edges and tets with the tets' records, the colour-Jacobi sums, the tables
-        img.budgetBytes += sizeof(cn_soft_edge) * uint64_t(L.E) + (sizeof(cn_soft_tet) + 64ull) * L.T + 16ull * N +
+        img.budgetBytes += sizeof(cn::PackedEdge) * uint64_t(L.E) + (sizeof(cn_soft_tet) + 64ull) * L.T + 16ull * N +
                            4ull * L.colWords;
     return CN_OK;
 }

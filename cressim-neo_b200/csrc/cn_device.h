@@ -86,6 +86,17 @@ struct WorkList {
 constexpr uint32_t kFamilies = 6u;
 enum : uint32_t { kFamEdges = 0u, kFamSegments = 1u, kFamBends = 2u, kFamJoints = 3u, kFamDistances = 4u, kFamTets = 5u };
 
+// An edge as the solves read it, 16 bytes instead of the record's 32: particle b's top bit marks a
+// disabled edge (particle indices stay below 2^29).
+struct PackedEdge {
+    uint32_t a, b;
+    float rest, compliance;
+};
+__host__ __device__ inline PackedEdge packEdge(const cn_soft_edge &e)
+{
+    return PackedEdge{e.particle_a, e.particle_b | (e.enabled ? 0u : 0x80000000u), e.rest_length, e.compliance};
+}
+
 struct Scene {
     // per-tick work lists of a batch (all null for a single world)
     WorkList wP, wE, wT, wB, wC;      // particles, edges, tets, rigid bodies, colliders
@@ -156,8 +167,10 @@ struct Scene {
     // a coloured batch's edges and tets in colour order (pool position e0 + i holds the scene's
     // i-th constraint in colour order; lambdas share that indexing under a coloured schedule) and
     // each tet's last corrections in the same order
-    const cn_soft_edge *edgesC = nullptr;
+    const PackedEdge *edgesC = nullptr;
     const cn_soft_tet *tetsC = nullptr;
+    // a batch's edges, packed (its pool has no scene view that would need the record layout)
+    const PackedEdge *edgesP = nullptr;
     float4 *tetRecC = nullptr;
 
     // ---- rigid bodies / colliders ----

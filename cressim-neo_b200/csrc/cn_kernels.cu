@@ -1363,13 +1363,13 @@ __device__ __forceinline__ float4 recordAt(const float4 *corr, uint32_t slot)
 
 // physics_soft_solve_edge_constraints.cs.hlsl:10-74: one edge's corrections (zero when it is
 // disabled or degenerate) and, when it returns true, its new lambda.
-__device__ __forceinline__ bool edgeSolve(const Scene &s, float dt, float relax, const cn_soft_edge &ed, float lambda,
+__device__ __forceinline__ bool edgeSolve(const Scene &s, float dt, float relax, const PackedEdge &ed, float lambda,
                                           float &newLambda, float4 &cA, float4 &cB)
 {
     cA = make_float4(0.f, 0.f, 0.f, 0.f);
     cB = cA;
-    if (ed.enabled == 0u) return false;
-    const float4 a = s.x[ed.particle_a], b = s.x[ed.particle_b];
+    if (ed.b >> 31) return false; // disabled
+    const float4 a = s.x[ed.a], b = s.x[ed.b];
     const float wA = a.w, wB = b.w, wSum = wA + wB;
     const f3 delta = xyz(b) - xyz(a);
     const float l2 = dot(delta, delta);
@@ -1378,7 +1378,7 @@ __device__ __forceinline__ bool edgeSolve(const Scene &s, float dt, float relax,
     const f3 gA = -delta / len;
     const f3 gB = -gA;
     const float alpha = mx(ed.compliance, 0.0f) / mx(dt * dt, kEps);
-    const float Cv = len - ed.rest_length;
+    const float Cv = len - ed.rest;
     const float den = wSum + alpha;
     if (!(den > kEps)) return false;
     const float dl = -(Cv + alpha * lambda) / den;
@@ -1390,7 +1390,7 @@ __device__ __forceinline__ bool edgeSolve(const Scene &s, float dt, float relax,
 
 __device__ __forceinline__ void solveEdge(const Scene &s, float dt, float relax, uint32_t e)
 {
-    const cn_soft_edge ed = s.edges[e];
+    const PackedEdge ed = s.edgesP ? s.edgesP[e] : packEdge(s.edges[e]);
     const float lambda = s.edgeLambda[e]; // with the record: one round trip fewer
     float newLambda;
     float4 cA, cB;
@@ -2972,11 +2972,11 @@ __device__ __forceinline__ void colourConstraintOrdered(const Scene &s, float dt
 {
     float newLambda;
     if constexpr (kFam == kFamEdges) {
-        const cn_soft_edge ed = s.edgesC[q];
+        const PackedEdge ed = s.edgesC[q];
         float4 cA, cB;
         if (edgeSolve(s, dt, relax, ed, s.edgeLambda[q], newLambda, cA, cB)) s.edgeLambda[q] = newLambda;
-        moveRecord(s, gaussSeidel, ed.particle_a, cA);
-        moveRecord(s, gaussSeidel, ed.particle_b, cB);
+        moveRecord(s, gaussSeidel, ed.a, cA);
+        moveRecord(s, gaussSeidel, ed.b & 0x7fffffffu, cB);
     } else {
         const cn_soft_tet t = s.tetsC[q];
         float4 c[4];
@@ -3386,7 +3386,7 @@ __global__ void __launch_bounds__(kThreads) k_admitScene(Scene s, AdmitImage a)
         return t;
     };
     if (i < a.E) {
-        const_cast<cn_soft_edge *>(s.edges)[a.e0 + i] = edgeAt(i);
+        const_cast<PackedEdge *>(s.edgesP)[a.e0 + i] = packEdge(edgeAt(i));
         const uint2 d = u2(kAdmEdgeDst)[i];
         reinterpret_cast<uint2 *>(const_cast<uint32_t *>(s.edgeDst))[a.e0 + i] =
             make_uint2(d.x == kNoSlot ? kNoSlot : d.x + a.ei0, d.y == kNoSlot ? kNoSlot : d.y + a.ei0);
@@ -3427,7 +3427,7 @@ __global__ void __launch_bounds__(kThreads) k_admitScene(Scene s, AdmitImage a)
     }
     if (i < a.queryCount) const_cast<uint32_t *>(s.colQueryOrder)[a.c0 + i] = u32(kAdmQueryOrder)[i] + a.c0;
     if (a.colWords) { // the colour-ordered copies, colour tables and records
-        if (i < a.E) const_cast<cn_soft_edge *>(s.edgesC)[a.e0 + i] = edgeAt(u32(kAdmEdgeColOrder)[i]);
+        if (i < a.E) const_cast<PackedEdge *>(s.edgesC)[a.e0 + i] = packEdge(edgeAt(u32(kAdmEdgeColOrder)[i]));
         if (i < a.T) {
             const_cast<cn_soft_tet *>(s.tetsC)[a.t0 + i] = tetAt(u32(kAdmTetColOrder)[i]);
             for (uint32_t k = 0; k < 4u; ++k) s.tetRecC[4u * (size_t(a.t0) + i) + k] = zero4;

@@ -44,7 +44,7 @@ struct cn_solver {
     std::vector<uint32_t> bodyTypes;
     uint32_t attributeStructure = 0; // attributeStructure() of the synced world
     std::vector<uint32_t> queryOrder; // the colliders queried (enabled, of a present body), in order
-    std::vector<cn_soft_edge> edgesC; // host staging of the colour-ordered copies (coloured schedules)
+    std::vector<cn::PackedEdge> edgesC; // host staging of the colour-ordered copies (coloured schedules)
     std::vector<cn_soft_tet> tetsC;
     cudaStream_t ownStream = nullptr;
     cn::Scene s{};
@@ -208,7 +208,7 @@ void layout(cn_solver *sv, cn::Arena &a, const cn_world_soa &w, const cn::Incide
     // the coloured schedules read the edges and tets in colour order (a colour is a contiguous
     // range); their lambdas are indexed by colour position and the tets' last corrections sit in
     // the tet records, by colour position, which the gather schedule would use otherwise
-    s.edgesC = coloured && s.E ? a.take<cn_soft_edge>(s.E) : nullptr;
+    s.edgesC = coloured && s.E ? a.take<cn::PackedEdge>(s.E) : nullptr;
     s.tetsC = coloured && s.T ? a.take<cn_soft_tet>(s.T) : nullptr;
     s.tetRecC = s.tetsC ? s.tetCorr : nullptr;
     s.softAcc = coloured ? a.take<float4>(N) : nullptr;
@@ -756,9 +756,9 @@ static cudaError_t uploadColourOrdered(cn_solver *sv, const cn_world_soa &w, cud
     if (s.edgesC) {
         const std::vector<uint32_t> &order = sv->colouring[cn::kFamEdges].order;
         sv->edgesC.resize(order.size());
-        for (size_t i = 0; i < order.size(); ++i) sv->edgesC[i] = w.edges[order[i]];
-        const cudaError_t e = cudaMemcpyAsync(const_cast<cn_soft_edge *>(s.edgesC), sv->edgesC.data(),
-                                              sizeof(cn_soft_edge) * order.size(), cudaMemcpyHostToDevice, st);
+        for (size_t i = 0; i < order.size(); ++i) sv->edgesC[i] = cn::packEdge(w.edges[order[i]]);
+        const cudaError_t e = cudaMemcpyAsync(const_cast<cn::PackedEdge *>(s.edgesC), sv->edgesC.data(),
+                                              sizeof(cn::PackedEdge) * order.size(), cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return e;
     }
     if (s.tetsC) {

@@ -212,11 +212,11 @@ def test_gather_batch_refuses_coloured_schedules():
 def test_server_results_equal_alone_and_in_the_mix_with_evictions():
     pool = small_pool(6)
     # a budget that holds two or three of the six scenes: admissions must evict idle scenes
-    # (the batch charges 120 + 4 x 72 B per particle, 76 B per edge, 116 B per tet, 272 B per
+    # (the batch charges 120 + 4 x 72 B per particle, 60 B per edge, 116 B per tet, 272 B per
     # body and 216 B per collider)
     def scene_bytes(sc):
         c = sc.world.counts()
-        return c["particles"] * (120 + 288) + c["edges"] * 76 + c["tets"] * 116 + 2 * 272 + 2 * 216
+        return c["particles"] * (120 + 288) + c["edges"] * 60 + c["tets"] * 116 + 2 * 272 + 2 * 216
     largest = max(scene_bytes(sc) for sc in pool)
     b = Batch(batch_desc(serving.serving_solver_desc(), memory_budget_bytes=int(2.5 * largest),
                          particle_capacity=20000))
@@ -251,7 +251,7 @@ def test_server_over_a_gauss_seidel_batch_with_evictions_equals_own_solvers():
 
     def scene_bytes(sc):   # the gather budget terms plus colour orders, sums and tables
         c = sc.world.counts()
-        return (c["particles"] * (120 + 288 + 16) + c["edges"] * (76 + 4) + c["tets"] * (116 + 4)
+        return (c["particles"] * (120 + 288 + 16) + c["edges"] * (60 + 16) + c["tets"] * (116 + 96)
                 + 2 * 272 + 2 * 216 + 4 * 200)
     largest = max(scene_bytes(sc) for sc in pool)
     b = Batch(batch_desc(desc, memory_budget_bytes=int(2.5 * largest), particle_capacity=20000))
@@ -304,11 +304,12 @@ def test_server_interleavings_with_evictions_equal_own_solvers(schedule):
     for r in req:
         per_scene[r.scene].append(r.targets)
     ref = {k: own_solver_run(pool[k], np.concatenate(t), desc) for k, t in per_scene.items() if t}
+    coloured = schedule != XPBD_GATHER
 
-    def scene_bytes(sc):
+    def scene_bytes(sc):   # the batch's budget charge, with the colour tables under a coloured schedule
         c = sc.world.counts()
-        return (c["particles"] * (120 + 288 + 16) + c["edges"] * (76 + 4) + c["tets"] * (116 + 4)
-                + 2 * 272 + 2 * 216 + 4 * 200)
+        return (c["particles"] * (120 + 288 + 16 * coloured) + c["edges"] * (60 + 16 * coloured)
+                + c["tets"] * (116 + 96 * coloured) + 2 * 272 + 2 * 216 + 4 * 200 * coloured)
     largest = max(scene_bytes(sc) for sc in pool)
     for group, ticks_between in ((1, 1), (2, 2), (100, 1)):
         b = Batch(batch_desc(desc, memory_budget_bytes=int(2.5 * largest), particle_capacity=20000))
