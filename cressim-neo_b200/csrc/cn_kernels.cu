@@ -2162,7 +2162,10 @@ __device__ __forceinline__ void rigidContactsFrom(const Scene &s, const Config &
     const uint32_t off = s.candOffset[i]; // with the count: one round trip fewer
     f3 corr{0.f, 0.f, 0.f};
     bool any = false;
-    if (cnt) {
+    // A particle without weight takes no correction, and with no dynamic body nothing receives
+    // its contacts' shares: only the stored records (the last contact iteration) need them.
+    const bool inert = sp.w <= kEps && !s.hasDynamic && !s.storeRigidContacts;
+    if (cnt && !inert) {
         const uint32_t lim = s.meta_->rigidPairCount;
         const ContactParticle pt = loadContactParticle(s, i, sp);
         for (uint32_t k = 0; k < cnt; ++k) {
